@@ -1,0 +1,147 @@
+/*
+ * vring_b200.h -- C ABI of the B200 (sm_100a) implementation of vring's
+ * single-rank RK3 fractional-step core.
+ *
+ * The reference's surface is a set of Fortran module subroutines that each
+ * take `type(run) :: var` (loop.F90:26, momentum_coef.F90:24/71,
+ * momentum_terms_swirl.F90:15/78/137/177, step.F90:17, divergence.F90:16/69/239,
+ * poisson_solve.F90:13, tripar.F90:11/120, trithom.F90:6, btrithom.F90:5,
+ * part_tools.F90:95/144/199/228/374).  Derived types with allocatable
+ * components are not C-interoperable, so the state lives in an opaque
+ * context that owns all device memory; fields cross the boundary as plain
+ * double arrays in the reference's Fortran layouts (column-major, theta
+ * fastest, the reference's ghost extents).  INTEGRATION.md shows the
+ * ISO_C_BINDING module a Fortran caller binds these with.
+ *
+ * Conventions: every function returns VR_OK (0) or a VR_ERR_* code;
+ * vr_last_error() gives a message.  Work is queued on the context's own CUDA
+ * stream; calls that return host data synchronise that stream.  One host
+ * thread per context; separate contexts may run concurrently.
+ */
+#ifndef VRING_B200_H
+#define VRING_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VR_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define VR_API __attribute__((visibility("default")))
+#else
+#define VR_API
+#endif
+
+enum vr_status {
+  VR_OK = 0,
+  VR_ERR_DESC = 1,      /* invalid descriptor or sizes                       */
+  VR_ERR_OOM = 2,       /* device or host allocation failed                  */
+  VR_ERR_CUDA = 3,      /* a CUDA runtime call failed                        */
+  VR_ERR_NONFINITE = 4, /* NaN/Inf found (the reference stops: divergence.F90:396) */
+  VR_ERR_TIMEOUT = 5,   /* a bounded device wait gave up                     */
+  VR_ERR_FIELD = 6,     /* unknown field id or extents that do not match     */
+  VR_ERR_STATE = 7,     /* call made in a state that does not allow it       */
+  VR_ERR_ARG = 8,       /* invalid argument                                  */
+  VR_ERR_CAPACITY = 9,  /* particle slots exhausted                          */
+  VR_ERR_NODEVICE = 10  /* no usable CUDA device                             */
+};
+
+enum vr_precision { VR_FP64 = 0, VR_MIXED = 1 };
+enum vr_theta_wavenumber {
+  VR_WTH_EXACT = 0,    /* m^2, the reference's 'wvnex' (poisson_solve.F90:287)   */
+  VR_WTH_MODIFIED = 1  /* 2/dth^2 (1 - cos(2 pi m / N)): the discrete div-grad   */
+};
+enum vr_inflow {
+  VR_INFLOW_OFF = 0,       /* corr1s/corr2s/corr3s = 0                          */
+  VR_INFLOW_REFERENCE = 1  /* piston pulse profile() (gen_tools_swirl.F90:159)  */
+};
+
+/* Run descriptor: ===Mesh=== and ===Para=== of inp.txt (mesh_tools.F90:86-93,
+ * para_tools.F90:68-86) plus the device-side switches. */
+typedef struct vr_desc {
+  int32_t abi_version;      /* VR_ABI_VERSION                                   */
+  int32_t ntheta, nr, nz;   /* global cells (one rank: local == global)         */
+  double rmax, zmax;        /* maxr, maxz                                       */
+  double dt, re, pe, slip;  /* dt, Re, Pe, slip                                 */
+  int32_t precision;        /* vr_precision                                     */
+  int32_t theta_wavenumber; /* vr_theta_wavenumber                              */
+  int32_t inflow;           /* vr_inflow                                        */
+  int32_t device;           /* CUDA device ordinal                              */
+  int32_t flags;            /* reserved, 0                                      */
+} vr_desc;
+
+/* Field ids (the reference names; solu_toolsII.F90:10-68, solp_tools.F90:8-30).
+ * Extents (Fortran, first index fastest):
+ *   ghosted 3-D  (nth, 0:nr+2, 0:nz+2): Q1..Q3, DQ1..DQ3, RU1..RU3, PRES
+ *   PRG          (nth, nr, nz, 3)
+ *   RHS          (nth, nr, nz)        -- divq output / Poisson right-hand side
+ *   DPH          (nth, 0:nr+1, 0:nz+1)
+ *   2-D          (nth, 1:nr+1): CORR3S, CORR3N, CSORT, TCONV
+ *                (nth, 0:nr+2): DQ3NO                                         */
+enum vr_field {
+  VR_F_Q1 = 0, VR_F_Q2 = 1, VR_F_Q3 = 2, VR_F_DQ1 = 3, VR_F_DQ2 = 4, VR_F_DQ3 = 5,
+  VR_F_RU1 = 6, VR_F_RU2 = 7, VR_F_RU3 = 8, VR_F_PRES = 11, VR_F_PRG = 12,
+  VR_F_RHS = 13, VR_F_DPH = 15, VR_F_DQ3NO = 19, VR_F_CORR3S = 22, VR_F_CORR3N = 23,
+  VR_F_CSORT = 24, VR_F_TCONV = 25
+};
+
+typedef struct vr_ctx vr_ctx;
+
+/* ---- lifetime (main.F90:39-68: create_mesh_a, alct_solu/solp, prep_poisson) */
+VR_API int vr_create(const vr_desc *desc, vr_ctx **out);
+VR_API int vr_destroy(vr_ctx *ctx);
+VR_API const char *vr_last_error(const vr_ctx *ctx);
+VR_API int vr_sync(vr_ctx *ctx);
+
+/* ---- state transfer (host arrays in the Fortran layouts listed above) ----- */
+VR_API int vr_field_extents(const vr_ctx *ctx, int32_t field, int64_t ext[4]);
+VR_API int vr_set_field(vr_ctx *ctx, int32_t field, const double *host, const int64_t ext[4]);
+VR_API int vr_get_field(vr_ctx *ctx, int32_t field, double *host, const int64_t ext[4]);
+/* para%irkstep, para%ntime, para%nstep (loop.F90:51-53, :65) */
+VR_API int vr_set_clock(vr_ctx *ctx, int32_t irkstep, double ntime, int64_t nstep);
+VR_API int vr_get_clock(const vr_ctx *ctx, int32_t *irkstep, double *ntime, int64_t *nstep);
+
+/* ---- the reference's per-routine surface, one call each ------------------ */
+VR_API int vr_ucoeff(vr_ctx *ctx);        /* momentum_coef.F90:24-69                   */
+VR_API int vr_coesys(vr_ctx *ctx);        /* momentum_coef.F90:71-538                  */
+VR_API int vr_hdnbc(vr_ctx *ctx);         /* momentum_terms_swirl.F90:177-296          */
+VR_API int vr_hdnl1(vr_ctx *ctx);         /* momentum_terms_swirl.F90:15-77  -> DQ1    */
+VR_API int vr_hdnl2(vr_ctx *ctx);         /* momentum_terms_swirl.F90:78-135 -> DQ2    */
+VR_API int vr_hdnl3(vr_ctx *ctx);         /* momentum_terms_swirl.F90:137-174 -> DQ3   */
+VR_API int vr_step(vr_ctx *ctx);          /* step.F90:17-210 (+ solqi/solqj/solqk)     */
+VR_API int vr_divq(vr_ctx *ctx);          /* divergence.F90:16-67 -> RHS               */
+VR_API int vr_laplace_solve(vr_ctx *ctx); /* poisson_solve.F90:13-32 -> DPH            */
+VR_API int vr_upsol(vr_ctx *ctx);         /* divergence.F90:69-236                     */
+VR_API int vr_uppres(vr_ctx *ctx);        /* divergence.F90:239-480                    */
+
+/* ---- fused paths --------------------------------------------------------- */
+/* One RK substep irk (loop.F90:63-130 without particles), fused kernels. */
+VR_API int vr_substep(vr_ctx *ctx, int32_t irk);
+/* nsteps time steps (loop.F90:47-130): ntime += dt, substeps 1..3, as one CUDA
+ * graph per substep replayed; particle classes attached with vr_part_attach
+ * advance at substep 1 (loop.F90:66-68). */
+VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
+
+/* ---- diagnostics --------------------------------------------------------- */
+/* max over cells of |div q| in FP64 (the divq stencil without 1/(alpha dt)) */
+VR_API int vr_max_divergence(vr_ctx *ctx, double *out);
+/* number of non-finite values in q1..q3 and pres; VR_ERR_NONFINITE if any */
+VR_API int vr_check_finite(vr_ctx *ctx, int64_t *count);
+
+/* ---- batched tridiagonal solvers (host arrays) --------------------------- */
+/* tripar.F90:120-145 / trithom.F90:6-29: nbatch independent systems of size n,
+ * system b at offset b*n in every array; aa(1) and cc(n) are not used. */
+VR_API int vr_solve_lap_thom(const double *rhs, double *sol, const double *aa, const double *bb,
+                      const double *cc, int32_t n, int32_t nbatch);
+/* btrithom.F90:5-71: block tridiagonal, n blocks of size m, identity
+ * off-diagonal blocks, tridiagonal diagonal blocks (b1 sub, b2 diag, b3 super) */
+VR_API int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
+                       const double *b3, int32_t m, int32_t n, int32_t nbatch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VRING_B200_H */

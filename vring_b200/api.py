@@ -1,0 +1,210 @@
+"""ctypes binding of ``lib/libvring_b200.so`` and the host-side mirror of the
+reference's subroutine surface.
+
+``Run`` stands for the reference's ``type(run) :: var`` (run.F90:14-22): it
+owns one device context and exposes the routines of the RK3 core under the
+reference's names (``ucoeff``, ``coesys``, ``hdnbc``, ``hdnl1``..``hdnl3``,
+``step``, ``divq``, ``laplace_solve``, ``upsol``, ``uppres``, ``iterate``).
+Fields are numpy arrays in the reference's Fortran layouts.
+
+There is no CPU path: if the CUDA library cannot be loaded, or no device is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libvring_b200.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "vring_b200.h")
+
+VR_ABI_VERSION = 1
+STATUS = {0: "VR_OK", 1: "VR_ERR_DESC", 2: "VR_ERR_OOM", 3: "VR_ERR_CUDA", 4: "VR_ERR_NONFINITE",
+          5: "VR_ERR_TIMEOUT", 6: "VR_ERR_FIELD", 7: "VR_ERR_STATE", 8: "VR_ERR_ARG",
+          9: "VR_ERR_CAPACITY", 10: "VR_ERR_NODEVICE"}
+FIELD_ID = {"q1": 0, "q2": 1, "q3": 2, "dq1": 3, "dq2": 4, "dq3": 5, "ru1": 6, "ru2": 7, "ru3": 8,
+            "pres": 11, "prg": 12, "rhs": 13, "dph": 15, "dq3no": 19, "corr3s": 22, "corr3n": 23,
+            "csort": 24, "tconv": 25}
+PRECISION = {"fp64": 0, "mixed": 1}
+WTH = {"exact": 0, "wvnex": 0, "modified": 1}
+INFLOW = {"off": 0, "reference": 1}
+
+
+class VrError(RuntimeError):
+    def __init__(self, code: int, msg: str = ""):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+class Desc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("ntheta", C.c_int32), ("nr", C.c_int32),
+                ("nz", C.c_int32), ("rmax", C.c_double), ("zmax", C.c_double), ("dt", C.c_double),
+                ("re", C.c_double), ("pe", C.c_double), ("slip", C.c_double),
+                ("precision", C.c_int32), ("theta_wavenumber", C.c_int32), ("inflow", C.c_int32),
+                ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+def declared_symbols(header: str = HEADER) -> list[str]:
+    """Every entry point ``include/vring_b200.h`` declares with VR_API."""
+    txt = open(header).read()
+    return re.findall(r"VR_API\s+[\w\s\*]+?\b(vr_\w+)\s*\(", txt)
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises when it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libvring_b200.so is not built (run vring_b200.build.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, dp = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        L.vr_create.argtypes = [C.POINTER(Desc), C.POINTER(vp)]
+        L.vr_destroy.argtypes = [vp]
+        L.vr_last_error.restype = C.c_char_p
+        L.vr_last_error.argtypes = [vp]
+        L.vr_sync.argtypes = [vp]
+        L.vr_field_extents.argtypes = [vp, i32, C.POINTER(i64)]
+        L.vr_set_field.argtypes = [vp, i32, vp, C.POINTER(i64)]
+        L.vr_get_field.argtypes = [vp, i32, vp, C.POINTER(i64)]
+        L.vr_set_clock.argtypes = [vp, i32, dp, i64]
+        L.vr_get_clock.argtypes = [vp, C.POINTER(i32), C.POINTER(dp), C.POINTER(i64)]
+        for n in ("ucoeff", "coesys", "hdnbc", "hdnl1", "hdnl2", "hdnl3", "step", "divq",
+                  "laplace_solve", "upsol", "uppres"):
+            getattr(L, "vr_" + n).argtypes = [vp]
+        L.vr_substep.argtypes = [vp, i32]
+        L.vr_iterate.argtypes = [vp, i32]
+        L.vr_max_divergence.argtypes = [vp, C.POINTER(dp)]
+        L.vr_check_finite.argtypes = [vp, C.POINTER(i64)]
+        L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
+        L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Run:
+    """One single-rank vring run resident on a B200 (the reference's type(run))."""
+
+    def __init__(self, ntheta, nr, nz, rmax, zmax, dt, re, pe=1.0, slip=0.0, precision="fp64",
+                 theta_wavenumber="exact", inflow="off", device=0):
+        self.desc = Desc(VR_ABI_VERSION, ntheta, nr, nz, rmax, zmax, dt, re, pe, slip,
+                         PRECISION[precision], WTH[theta_wavenumber], INFLOW[inflow], device, 0)
+        self._h = C.c_void_p()
+        rc = lib().vr_create(C.byref(self.desc), C.byref(self._h))
+        if rc:
+            raise VrError(rc, "vr_create(%dx%dx%d)" % (ntheta, nr, nz))
+        self.ntheta, self.nr, self.nz = ntheta, nr, nz
+        self.dt = dt
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().vr_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc, what):
+        if rc:
+            msg = lib().vr_last_error(self._h)
+            raise VrError(rc, "%s: %s" % (what, msg.decode() if msg else ""))
+
+    # -- state ----------------------------------------------------------------
+    def extents(self, name: str) -> tuple:
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        return tuple(int(e) for e in ext)
+
+    def get(self, name: str) -> np.ndarray:
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        shape = tuple(int(e) for e in ext)
+        a = np.empty(shape, dtype=np.float64, order="F")
+        self._chk(lib().vr_get_field(self._h, FIELD_ID[name], _p(a), ext), "get " + name)
+        return a if shape[3] > 1 else a[..., 0]
+
+    def set(self, name: str, value) -> None:
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        shape = tuple(int(e) for e in ext)
+        a = np.asfortranarray(np.broadcast_to(np.asarray(value, dtype=np.float64),
+                                              shape if shape[3] > 1 else shape[:3]))
+        self._chk(lib().vr_set_field(self._h, FIELD_ID[name], _p(a), ext), "set " + name)
+
+    def set_clock(self, irkstep: int, ntime: float, nstep: int = 0):
+        self._chk(lib().vr_set_clock(self._h, irkstep, ntime, nstep), "set_clock")
+
+    @property
+    def clock(self):
+        irk, t, n = C.c_int32(), C.c_double(), C.c_int64()
+        self._chk(lib().vr_get_clock(self._h, C.byref(irk), C.byref(t), C.byref(n)), "get_clock")
+        return irk.value, t.value, n.value
+
+    # -- the reference's routines --------------------------------------------
+    def __getattr__(self, name):
+        if name in ("ucoeff", "coesys", "hdnbc", "hdnl1", "hdnl2", "hdnl3", "step", "divq",
+                    "laplace_solve", "upsol", "uppres", "sync"):
+            fn = getattr(lib(), "vr_" + name)
+            return lambda: self._chk(fn(self._h), name)
+        raise AttributeError(name)
+
+    def substep(self, irk: int):
+        self._chk(lib().vr_substep(self._h, irk), "substep")
+
+    def iterate(self, nsteps: int):
+        self._chk(lib().vr_iterate(self._h, nsteps), "iterate")
+
+    def max_divergence(self) -> float:
+        v = C.c_double()
+        self._chk(lib().vr_max_divergence(self._h, C.byref(v)), "max_divergence")
+        return v.value
+
+    def count_nonfinite(self) -> int:
+        n = C.c_int64()
+        rc = lib().vr_check_finite(self._h, C.byref(n))
+        if rc not in (0, 4):
+            self._chk(rc, "check_finite")
+        return n.value
+
+
+def solve_lap_thom(rhs, aa, bb, cc):
+    """Batched Thomas solve on the GPU (tripar.F90:120-145); 2-D inputs are
+    (nbatch, n) with one system per row."""
+    arrs = [np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64) for x in (rhs, aa, bb, cc)]
+    nb, n = arrs[0].shape
+    sol = np.empty_like(arrs[0])
+    rc = lib().vr_solve_lap_thom(_p(arrs[0]), _p(sol), _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), n, nb)
+    if rc:
+        raise VrError(rc, "vr_solve_lap_thom")
+    return sol.reshape(np.shape(rhs))
+
+
+def solve_lap_bthom(rhs, b1, b2, b3, m, n):
+    """Batched block Thomas (btrithom.F90:5-71); inputs (nbatch, m*n)."""
+    arrs = [np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64) for x in (rhs, b1, b2, b3)]
+    nb = arrs[0].shape[0]
+    sol = np.empty_like(arrs[0])
+    rc = lib().vr_solve_lap_bthom(_p(arrs[0]), _p(sol), _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), m, n, nb)
+    if rc:
+        raise VrError(rc, "vr_solve_lap_bthom")
+    return sol.reshape(np.shape(rhs))

@@ -1,0 +1,156 @@
+// vr_internal.cuh -- shared definitions of the sm_100a implementation.
+//
+// Storage: every field keeps the reference's Fortran layout in HBM
+// (column-major, theta fastest) so the C ABI copies it without reshaping:
+//   ghosted 3-D fields  (nth, 0:nr+2, 0:nz+2)   solu_toolsII.F90:88-111
+//   prg                 (nth, nr, nz, 3)        solu_toolsII.F90:113
+//   rhs / spectral work (nth, nr, nz)           solp_tools.F90:53-55
+//   dph                 (nth, 0:nr+1, 0:nz+1)   solp_tools.F90:57
+// A warp spans consecutive theta cells, so every stencil row and every batch
+// of tridiagonal lines along r or z is read with full 128-byte sectors.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/vring_b200.h"
+
+namespace vr {
+
+// ---------------------------------------------------------------------------
+// geometry + metric coefficients, passed by value to the stencil kernels
+// ---------------------------------------------------------------------------
+struct Geo {
+  int nth, nr, nz, nrc, nzc;
+  int J3, K3;  // ghosted j extent (nr+3) and k extent (nz+3)
+  int pl;      // nth * J3: k stride of ghosted fields
+  int dpl;     // nth * (nr+2): k stride of dph
+  double dx1, dx2, dx3, dx1q, dx2q, dx3q, axsym, dt, re, slip, dtheta, dr, dz;
+  // device vectors indexed by the Fortran j (allocated 0..nr+2)
+  const double *rm, *rc, *irm, *qc;
+  const double *h1d11, *h1d22d, *h1d22n, *h1dare, *h2d11, *h2d22m, *h2d22p, *h2dare;
+  const double *s1t11, *s1t2n, *s1t2s, *s1t2c, *s2t11, *s2t2p, *s2t2m, *s2t2c;
+  const double *s3t2n, *s3t2s;
+};
+
+__host__ __device__ inline int I3(const Geo &g, int i, int j, int k) {
+  return (i - 1) + g.nth * (j + g.J3 * k);
+}
+__host__ __device__ inline int IPRG(const Geo &g, int i, int j, int k, int m) {
+  return (i - 1) + g.nth * ((j - 1) + g.nr * ((k - 1) + g.nz * (m - 1)));
+}
+__host__ __device__ inline int IRS(const Geo &g, int i, int j, int k) {
+  return (i - 1) + g.nth * ((j - 1) + g.nr * (k - 1));
+}
+__host__ __device__ inline int IDP(const Geo &g, int i, int j, int k) {
+  return (i - 1) + g.nth * (j + (g.nr + 2) * k);
+}
+__host__ __device__ inline int I2O(const Geo &g, int i, int j) { return (i - 1) + g.nth * (j - 1); }
+__host__ __device__ inline int I2Z(const Geo &g, int i, int j) { return (i - 1) + g.nth * j; }
+
+// RK3 coefficients of one substep (para_tools.F90:103-113)
+struct Rk {
+  double gam, rom, alm;
+};
+
+// Precomputed factorisation of one batched tridiagonal family whose matrix
+// is shared by every line: g_j = (f_j - a_j g_{j-1}) ib_j,
+// x_j = g_j - c_j ib_j x_{j+1}; arrays indexed 0..n-1.
+struct Tri {
+  const double *a, *c, *ib;
+  int n;
+};
+
+// Factorisation of the periodic theta solve of step.F90:487-534 (tripij) for
+// one family: per row j, inner unknowns i = 1..N-1 and the bordering unknown N.
+//   inv[j*N + i-1]   1/pivot               (i = 1..N-1)
+//   pp[j*N + i-1]    scaled super-diagonal (i = 1..N-2)
+//   zz[j*N + i-1]    border response       (i = 1..N-1)
+//   sub[j], sup[j]   the constant sub/super diagonal (-acc), za2[j] denominator
+struct TriPer {
+  const double *inv, *pp, *zz, *sub, *sup, *za2;
+};
+
+// ---------------------------------------------------------------------------
+// the context behind vr_ctx*
+// ---------------------------------------------------------------------------
+struct HostCoef;  // ucoeff/coesys vectors in double, host side
+
+}  // namespace vr
+
+struct vr_ctx {
+  vr_desc d;
+  int dev;
+  cudaStream_t stream;
+  vr::Geo geo;
+  // clock
+  int irk;
+  double ntime;
+  int64_t nstep;
+  double crkgam[4], crkrom[4], crkalm[4];
+  // device fields
+  double *q[3], *dq[3], *ru[3], *qrhs[3];
+  double *prg, *pres, *rhs, *dph, *spec;
+  double *csort, *dq3no, *corr3n, *corr3s, *tconv;
+  // device coefficient storage (one allocation) and family tables
+  double *dcoef;
+  size_t dcoef_len;
+  vr::Tri rtri[4][3], ztri[4][3];          // [irk][component]
+  vr::TriPer ttri[4][2];                   // [irk][0: s1t11 (q1,q3), 1: s2t11 (q2)]
+  const double *pois_ib;                   // (nth/2+1, nr, nz) -> [kz][j][mm]
+  const double *pois_a, *pois_c;           // aa/cc with aa(1)=0, cc(nr)=0
+  const double *tw_th;                     // theta twiddles (cos, sin) 2*nth
+  const double *tw_z;                      // z twiddles for FFT (cos,sin) n and DCT shifts
+  // host-side copies needed for hdnbc scalars
+  double *h_rc, *h_rm, *h_da, *h_qc;
+  // diagnostics scratch
+  double *d_red;
+  unsigned long long *d_count;
+  // CUDA graphs for the fused substeps (one per irk), built lazily
+  cudaGraphExec_t graph[4];
+  bool graph_ok[4];
+  std::string err;
+};
+
+namespace vr {
+
+// error helpers ------------------------------------------------------------
+int set_err(vr_ctx *c, int code, const std::string &msg);
+#define VR_CUDA(c, call)                                                            \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return vr::set_err((c), VR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define VR_LAUNCH_CHECK(c)                                                          \
+  do {                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                            \
+    if (e_ != cudaSuccess)                                                          \
+      return vr::set_err((c), VR_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+// kernel launchers (return cudaError_t of the launch) -----------------------
+cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);
+cudaError_t launch_hdnl(vr_ctx *c, int comp);
+cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h);
+cudaError_t launch_tsweep(vr_ctx *c, int comp);
+cudaError_t launch_rsweep(vr_ctx *c, int comp);
+cudaError_t launch_zsweep(vr_ctx *c, int comp);
+cudaError_t launch_divq(vr_ctx *c, const Rk &rk);
+cudaError_t launch_poisson(vr_ctx *c);
+cudaError_t launch_upsol(vr_ctx *c, const Rk &rk);
+cudaError_t launch_uppres(vr_ctx *c, const Rk &rk);
+cudaError_t launch_maxdiv(vr_ctx *c, double *d_out);
+cudaError_t launch_count_nonfinite(vr_ctx *c, unsigned long long *d_out);
+
+// batched tridiagonal kernels on raw device arrays (vr_solve_lap_thom)
+cudaError_t launch_thomas_batched(const double *rhs, double *sol, const double *aa,
+                                  const double *bb, const double *cc, int n, int nbatch,
+                                  cudaStream_t s);
+cudaError_t launch_bthom_batched(const double *rhs, double *sol, const double *b1,
+                                 const double *b2, const double *b3, int m, int n, int nbatch,
+                                 double *work, cudaStream_t s);
+
+}  // namespace vr

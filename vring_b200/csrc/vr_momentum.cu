@@ -1,0 +1,603 @@
+// vr_momentum.cu -- explicit momentum terms, RK right-hand sides and the
+// implicit (approximate-factorisation) sweeps of step.F90.
+//
+// Stencil kernels map threadIdx.x to theta, so each warp reads 32
+// consecutive theta cells (256 contiguous bytes) of every neighbour row; the
+// neighbour rows in r and z come from L1/L2.
+//
+// Sweeps:
+//  * theta (tripij, periodic): one warp per (r, z) line; each lane owns a
+//    contiguous chunk of the line, the two first-order recurrences of the
+//    factorised solve are composed per chunk and combined with a warp
+//    shuffle scan, so loads/stores are fully coalesced and no lane waits on
+//    a serial chain longer than its chunk.
+//  * r and z (solqj / solqk): a CTA stages a tile of LT lines x n unknowns
+//    (LT consecutive theta, one line per theta) in shared memory with
+//    coalesced row loads, every line is split into CH chunks solved with the
+//    same chunk-composition, and the tile is written back row by row.
+// The matrices are identical for every line of a family (they depend on the
+// substep and on r or z only), so their Thomas factorisation is computed once
+// on the host (vr_ctx.cu) and the kernels only run the two substitutions.
+#include <cuda_runtime.h>
+
+#include "vr_internal.cuh"
+
+namespace vr {
+
+__device__ __forceinline__ double ld(const double *p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// hdnbc (momentum_terms_swirl.F90:177-296), one thread per (ic, jc<=nrc)
+// ---------------------------------------------------------------------------
+__global__ void k_hdnbc(Geo g, Rk rk, double cs, double cor, const double *__restrict__ q3,
+                        double *csort, double *tconv, double *corr3n, double *dq3no,
+                        double *corr3s) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (ic > g.nth || jc > g.nrc) return;
+  int o = I2O(g, ic, jc);
+  corr3s[o] = (jc <= g.nr && g.rc[jc] <= (double)0.4999f) ? cs : 0.0;
+  double q3n = q3[I3(g, ic, jc, g.nzc)], q3m = q3[I3(g, ic, jc, g.nz)];
+  double cso = csort[o];
+  if (jc <= g.nr && q3n > 0.0) {
+    cso = (double)0.6f * q3n;
+    csort[o] = cso;
+  }
+  double tc = -cso * g.dx3 * (q3n - q3m);
+  tconv[o] = tc;
+  int oz = I2Z(g, ic, jc);
+  double c3n = (rk.gam * tc + rk.rom * dq3no[oz]) * g.dt;
+  dq3no[oz] = tc;
+  corr3n[o] = c3n + g.qc[jc] * cor;
+}
+
+cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double cs, double cor) {
+  const Geo &g = c->geo;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nrc + 3) / 4);
+  k_hdnbc<<<gr, b, 0, c->stream>>>(g, rk, cs, cor, c->q[2], c->csort, c->tconv, c->corr3n, c->dq3no,
+                                   c->corr3s);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// explicit terms.  The south values q1s/q2s/q3s are zero: hdnbc sets them to
+// 0 every substep (momentum_terms_swirl.F90:216-223).
+// ---------------------------------------------------------------------------
+struct QV {
+  const double *__restrict__ q1, *__restrict__ q2, *__restrict__ q3;
+};
+
+// hdnl1 at (i, j+1/2, k+1/2), momentum_terms_swirl.F90:29-68
+__device__ __forceinline__ double h1_at(const Geo &g, const QV &q, int ic, int ip, int im, int jc, int kc) {
+  const double *q1 = q.q1, *q2 = q.q2, *q3 = q.q3;
+  int jm = jc > 1 ? jc - 1 : 1;
+  double q1c = ld(q1 + I3(g, ic, jc, kc));
+  double q1p = ld(q1 + I3(g, ip, jc, kc)), q1m = ld(q1 + I3(g, im, jc, kc));
+  double qnn = q1p + q1c, qss = q1m + q1c;
+  double h11 = (qnn * qnn - qss * qss) * g.h1d11[jc];
+  double q2cn = ld(q2 + I3(g, ic, jc + 1, kc)), q2mn = ld(q2 + I3(g, im, jc + 1, kc));
+  double q2c = ld(q2 + I3(g, ic, jc, kc)), q2m = ld(q2 + I3(g, im, jc, kc));
+  qnn = (q2cn + q2mn) * (ld(q1 + I3(g, ic, jc + 1, kc)) + q1c);
+  qss = (q1c + ld(q1 + I3(g, ic, jm, kc))) * (q2c + q2m);
+  double h12d = (qnn - qss) * g.h1d22d[jc];
+  qnn = (q1p + q1c) * (q2cn + q2c);
+  qss = (q1c + q1m) * (q2mn + q2m);
+  double h12n = (qnn + qss) * g.h1d22n[jc];
+  qnn = 0.25 * (ld(q3 + I3(g, ic, jc, kc + 1)) + ld(q3 + I3(g, im, jc, kc + 1))) *
+        (ld(q1 + I3(g, ic, jc, kc + 1)) + q1c);
+  if (kc == 1)
+    qss = 0.0;  // 0.5*(q3s+q3s)*q1s
+  else
+    qss = 0.25 * (ld(q3 + I3(g, ic, jc, kc)) + ld(q3 + I3(g, im, jc, kc))) *
+          (q1c + ld(q1 + I3(g, ic, jc, kc - 1)));
+  double h13 = (qnn - qss) * g.dx3;
+  double d1q2 = ((q2cn + q2c) - (q2mn + q2m)) * g.h1dare[jc];
+  return d1q2 - (h11 + (h12d + h12n) + h13);
+}
+
+// hdnl2 at (i+1/2, j, k+1/2), j >= 2, momentum_terms_swirl.F90:94-128
+__device__ __forceinline__ double h2_at(const Geo &g, const QV &q, int ic, int ip, int im, int jc, int kc) {
+  const double *q1 = q.q1, *q2 = q.q2, *q3 = q.q3;
+  double q1p = ld(q1 + I3(g, ip, jc, kc)), q1pm = ld(q1 + I3(g, ip, jc - 1, kc));
+  double q1c = ld(q1 + I3(g, ic, jc, kc)), q1cm = ld(q1 + I3(g, ic, jc - 1, kc));
+  double q2c = ld(q2 + I3(g, ic, jc, kc));
+  double qnn = (q1p + q1pm) * (ld(q2 + I3(g, ip, jc, kc)) + q2c);
+  double qss = (q1c + q1cm) * (q2c + ld(q2 + I3(g, im, jc, kc)));
+  double h21 = (qnn - qss) * g.h2d11[jc];
+  qnn = ld(q2 + I3(g, ic, jc + 1, kc)) + q2c;
+  qss = q2c + ld(q2 + I3(g, ic, jc - 1, kc));
+  double h22 = qnn * qnn * g.h2d22p[jc] - qss * qss * g.h2d22m[jc];
+  qnn = 0.5 * (q1c + q1p);
+  qss = 0.5 * (q1cm + q1pm);
+  double h11n = 0.25 * (qnn + qss) * (qnn + qss);
+  qnn = 0.25 * (ld(q3 + I3(g, ic, jc, kc + 1)) + ld(q3 + I3(g, ic, jc - 1, kc + 1))) *
+        (ld(q2 + I3(g, ic, jc, kc + 1)) + q2c);
+  if (kc == 1)
+    qss = 0.0;
+  else
+    qss = 0.25 * (ld(q3 + I3(g, ic, jc, kc)) + ld(q3 + I3(g, ic, jc - 1, kc))) *
+          (q2c + ld(q2 + I3(g, ic, jc, kc - 1)));
+  double h23 = (qnn - qss) * g.dx3;
+  double d1q1 = -((q1p + q1pm) - (q1c + q1cm)) * g.h2dare[jc];
+  return d1q1 - (h21 + h22 + h23 - h11n);
+}
+
+// hdnl3 at (i+1/2, j+1/2, k), k >= 2, momentum_terms_swirl.F90:150-171
+__device__ __forceinline__ double h3_at(const Geo &g, const QV &q, int ic, int ip, int im, int jc, int kc) {
+  const double *q1 = q.q1, *q2 = q.q2, *q3 = q.q3;
+  int jm = jc > 1 ? jc - 1 : 1;
+  double q3c = ld(q3 + I3(g, ic, jc, kc));
+  double qnn = (ld(q3 + I3(g, ic, jc + 1, kc)) + q3c) *
+               (ld(q2 + I3(g, ic, jc + 1, kc)) + ld(q2 + I3(g, ic, jc + 1, kc - 1)));
+  double qss = (ld(q3 + I3(g, ic, jm, kc)) + q3c) * (ld(q2 + I3(g, ic, jc, kc)) + ld(q2 + I3(g, ic, jc, kc - 1)));
+  double h32 = (qnn - qss) * g.h1d22d[jc];
+  qnn = (q3c + ld(q3 + I3(g, ip, jc, kc))) * (ld(q1 + I3(g, ip, jc, kc)) + ld(q1 + I3(g, ip, jc, kc - 1)));
+  qss = (ld(q3 + I3(g, im, jc, kc)) + q3c) * (ld(q1 + I3(g, ic, jc, kc)) + ld(q1 + I3(g, ic, jc, kc - 1)));
+  double h31 = (qnn - qss) * g.h1d11[jc];
+  double q3p = ld(q3 + I3(g, ic, jc, kc + 1)), q3m = ld(q3 + I3(g, ic, jc, kc - 1));
+  qnn = 0.25 * (q3c + q3p) * (q3c + q3p);
+  qss = 0.25 * (q3c + q3m) * (q3c + q3m);
+  double h33 = (qnn - qss) * g.dx3;
+  return -(h31 + h32 + h33);
+}
+
+__global__ void k_hdnl(Geo g, QV q, int comp, double *__restrict__ dq) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  if (comp == 1) dq[I3(g, ic, jc, kc)] = h1_at(g, q, ic, ip, im, jc, kc);
+  if (comp == 2 && jc >= 2) dq[I3(g, ic, jc, kc)] = h2_at(g, q, ic, ip, im, jc, kc);
+  if (comp == 3 && kc >= 2) dq[I3(g, ic, jc, kc)] = h3_at(g, q, ic, ip, im, jc, kc);
+}
+
+cudaError_t launch_hdnl(vr_ctx *c, int comp) {
+  const Geo &g = c->geo;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  k_hdnl<<<gr, b, 0, c->stream>>>(g, QV{c->q[0], c->q[1], c->q[2]}, comp, c->dq[comp - 1]);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// RK right-hand sides of step.F90:32-165 for all three components at once
+// (q is not modified by step, so one pass reads it for all three).  With
+// INLINE_H the explicit terms H are computed here (fused hdnl1-3 + RHS);
+// otherwise they are read from dq (written by vr_hdnl1..3).  ru <- H.
+// ---------------------------------------------------------------------------
+struct RhsArgs {
+  QV q;
+  const double *__restrict__ dqh[3];  // H when not inlined
+  double *ru[3];
+  const double *__restrict__ prg;
+  double *qrhs[3];
+};
+
+template <bool INLINE_H>
+__global__ void k_rhs(Geo g, Rk rk, RhsArgs a) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  int jm = jc > 1 ? jc - 1 : 1;
+  const double *q1 = a.q.q1, *q2 = a.q.q2, *q3 = a.q.q3;
+  int o = I3(g, ic, jc, kc);
+  double are = rk.alm / g.re;
+  // ---- q1 (step.F90:32-63)
+  {
+    double h = INLINE_H ? h1_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[0] + o);
+    double qc = ld(q1 + o);
+    double d11 = (ld(q1 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q1 + I3(g, im, jc, kc))) * g.s1t11[jc];
+    double d33;
+    if (kc == 1)
+      d33 = 4.0 / 3.0 * (ld(q1 + I3(g, ic, jc, kc + 1)) - 3.0 * qc + 2.0 * 0.0) * g.dx3q;
+    else
+      d33 = (ld(q1 + I3(g, ic, jc, kc + 1)) - 2.0 * qc + ld(q1 + I3(g, ic, jc, kc - 1))) * g.dx3q;
+    double qnn = (ld(q1 + I3(g, ic, jc + 1, kc)) * g.irm[jc + 1] - qc * g.irm[jc]) * g.s1t2n[jc];
+    double qss = (qc * g.irm[jc] - ld(q1 + I3(g, ic, jm, kc)) * g.irm[jm]) * g.s1t2s[jc];
+    double d22 = (qnn - qss) * g.s1t2c[jc];
+    double r = ld(a.ru[0] + o);
+    a.qrhs[0][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 1)) +
+                    are * (d11 + d33 + d22)) * g.dt;
+    a.ru[0][o] = h;
+  }
+  // ---- q3 (step.F90:93-116), k >= 2
+  if (kc >= 2) {
+    double h = INLINE_H ? h3_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[2] + o);
+    double qc = ld(q3 + o);
+    double d11 = (ld(q3 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q3 + I3(g, im, jc, kc))) * g.s1t11[jc];
+    double d33 = (ld(q3 + I3(g, ic, jc, kc + 1)) - 2.0 * qc + ld(q3 + I3(g, ic, jc, kc - 1))) * g.dx3q;
+    double qnn = (ld(q3 + I3(g, ic, jc + 1, kc)) - qc) * g.s3t2n[jc];
+    double qss = (qc - ld(q3 + I3(g, ic, jm, kc))) * g.s3t2s[jc];
+    double d22 = qnn - qss;
+    double r = ld(a.ru[2] + o);
+    a.qrhs[2][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 3)) +
+                    are * (d11 + d33 + d22)) * g.dt;
+    a.ru[2][o] = h;
+  }
+  // ---- q2 (step.F90:144-165), j >= 2
+  if (jc >= 2) {
+    double h = INLINE_H ? h2_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[1] + o);
+    double qc = ld(q2 + o);
+    double d11 = (ld(q2 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q2 + I3(g, im, jc, kc))) * g.s2t11[jc];
+    double d33;
+    if (kc == 1)
+      d33 = 4.0 / 3.0 * (ld(q2 + I3(g, ic, jc, kc + 1)) - 3.0 * qc + 2.0 * 0.0) * g.dx3q;
+    else
+      d33 = (ld(q2 + I3(g, ic, jc, kc + 1)) - 2.0 * qc + ld(q2 + I3(g, ic, jc, kc - 1))) * g.dx3q;
+    double d22 = ld(q2 + I3(g, ic, jc + 1, kc)) * g.s2t2p[jc] - qc * g.s2t2c[jc] +
+                 ld(q2 + I3(g, ic, jc - 1, kc)) * g.s2t2m[jc];
+    double r = ld(a.ru[1] + o);
+    a.qrhs[1][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 2)) +
+                    are * (d11 + d33 + d22)) * g.dt;
+    a.ru[1][o] = h;
+  }
+}
+
+cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h) {
+  const Geo &g = c->geo;
+  RhsArgs a;
+  a.q = QV{c->q[0], c->q[1], c->q[2]};
+  for (int n = 0; n < 3; n++) {
+    a.dqh[n] = c->dq[n];
+    a.ru[n] = c->ru[n];
+    a.qrhs[n] = c->qrhs[n];
+  }
+  a.prg = c->prg;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  if (inline_h)
+    k_rhs<true><<<gr, b, 0, c->stream>>>(g, rk, a);
+  else
+    k_rhs<false><<<gr, b, 0, c->stream>>>(g, rk, a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// theta sweep (solqi + tripij, step.F90:212-263, 487-534), warp per line
+// ---------------------------------------------------------------------------
+// Affine map y_out = C + M * y_in, composed left-to-right along the line.
+struct Aff {
+  double M, C;
+};
+__device__ __forceinline__ Aff aff_then(const Aff &first, const Aff &second) {
+  return Aff{second.M * first.M, second.C + second.M * first.C};
+}
+
+constexpr int kTMaxE = 32;  // elements per lane: ntheta <= 1025
+
+__global__ void k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nlines_j, int nlines) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nlines) return;
+  int jc = jb + warp % nlines_j;
+  int kc = kb + warp / nlines_j;
+  const int N = g.nth;
+  double *line = f + I3(g, 1, jc, kc);
+  const double *inv = t.inv + (size_t)jc * N, *pp = t.pp + (size_t)jc * N, *zz = t.zz + (size_t)jc * N;
+  const double A = t.sub[jc];
+  const int inner = N - 1;
+  const int E = (inner + 31) / 32;
+  const int i0 = lane * E;  // 0-based inner index of the first owned element
+  double y[kTMaxE];
+  int cnt = inner - i0;
+  cnt = cnt < 0 ? 0 : (cnt > E ? E : cnt);
+  // forward: y_i = (f_i - A y_{i-1}) inv_i
+  Aff fw{1.0, 0.0};
+#pragma unroll
+  for (int e = 0; e < kTMaxE; e++) {
+    if (e < cnt) {
+      int i = i0 + e;
+      double fi = line[i];
+      double iv = ld(inv + i);
+      y[e] = fi;
+      fw.C = (fi - A * fw.C) * iv;
+      fw.M = -A * iv * fw.M;
+    }
+  }
+  // inclusive scan of the chunk maps across lanes
+  Aff acc = fw;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    Aff o{__shfl_up_sync(0xffffffffu, acc.M, d), __shfl_up_sync(0xffffffffu, acc.C, d)};
+    if (lane >= d) acc = aff_then(o, acc);
+  }
+  double yin = __shfl_up_sync(0xffffffffu, acc.C, 1);
+  if (lane == 0) yin = 0.0;
+  {
+    double yp = yin;
+#pragma unroll
+    for (int e = 0; e < kTMaxE; e++) {
+      if (e < cnt) {
+        int i = i0 + e;
+        yp = (y[e] - A * yp) * ld(inv + i);
+        y[e] = yp;
+      }
+    }
+  }
+  // backward: w_i = y_i - pp_i w_{i+1}, w beyond the inner range = 0
+  Aff bw{1.0, 0.0};
+#pragma unroll
+  for (int e = kTMaxE - 1; e >= 0; e--) {
+    if (e < cnt) {
+      int i = i0 + e;
+      double p = ld(pp + i);
+      bw.C = y[e] - p * bw.C;
+      bw.M = -p * bw.M;
+    }
+  }
+  acc = bw;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    Aff o{__shfl_down_sync(0xffffffffu, acc.M, d), __shfl_down_sync(0xffffffffu, acc.C, d)};
+    if (lane + d < 32) acc = aff_then(o, acc);
+  }
+  double win = __shfl_down_sync(0xffffffffu, acc.C, 1);
+  if (lane == 31) win = 0.0;
+  {
+    double wp = win;
+#pragma unroll
+    for (int e = kTMaxE - 1; e >= 0; e--) {
+      if (e < cnt) {
+        int i = i0 + e;
+        wp = y[e] - ld(pp + i) * wp;
+        y[e] = wp;
+      }
+    }
+  }
+  // bordering unknown N (step.F90:526-533)
+  int last_lane = (inner - 1) / E;
+  int last_e = (inner - 1) - last_lane * E;
+  double w1 = __shfl_sync(0xffffffffu, y[0], 0);
+  double wl = 0.0;
+#pragma unroll
+  for (int e = 0; e < kTMaxE; e++)
+    if (e == last_e) wl = y[e];
+  wl = __shfl_sync(0xffffffffu, wl, last_lane);
+  double fN = line[N - 1];
+  double za1 = fN - t.sup[jc] * w1 - A * wl;
+  double xN = za1 / t.za2[jc];
+#pragma unroll
+  for (int e = 0; e < kTMaxE; e++) {
+    if (e < cnt) {
+      int i = i0 + e;
+      line[i] = y[e] + ld(zz + i) * xN;
+    }
+  }
+  if (lane == 0) line[N - 1] = xN;
+}
+
+cudaError_t launch_tsweep(vr_ctx *c, int comp) {
+  const Geo &g = c->geo;
+  int jb = comp == 2 ? 2 : 1, kb = comp == 3 ? 2 : 1;
+  int nj = g.nr - jb + 1, nk = g.nz - kb + 1;
+  int nlines = nj * nk;
+  int threads = 128;
+  int blocks = (int)(((long long)nlines * 32 + threads - 1) / threads);
+  const TriPer &t = c->ttri[c->irk][comp == 2 ? 1 : 0];
+  k_tsweep<<<blocks, threads, 0, c->stream>>>(g, t, c->qrhs[comp - 1], jb, kb, nj, nlines);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// r / z sweeps on a shared-memory tile of LT lines x n unknowns
+// ---------------------------------------------------------------------------
+// Per-line coefficients of a shared-matrix family.
+struct CoefShared {
+  const double *a, *c, *ib;
+  __device__ __forceinline__ double A(int, int e) const { return ld(a + e); }
+  __device__ __forceinline__ double Cc(int, int e) const { return ld(c + e); }
+  __device__ __forceinline__ double IB(int, int e) const { return ld(ib + e); }
+};
+
+// Solve the LT lines of tile[e*LD + l] (e = 0..n-1) in place.  Threads
+// (l, ch) = (t % LT, t / LT) own the chunk [ch*CL, ch*CL + CL).
+template <int LT, int CH, class Coef>
+__device__ void tile_solve(double *tile, int LD, int n, const Coef &cf, double *sM, double *sC) {
+  const int t = threadIdx.x;
+  const int l = t % LT, ch = t / LT;
+  const int CL = (n + CH - 1) / CH;
+  const int e0 = ch * CL;
+  const int e1 = min(n, e0 + CL);
+  // forward pass 1: chunk map with zero input
+  double M = 1.0, Cv = 0.0;
+  for (int e = e0; e < e1; e++) {
+    double ib = cf.IB(l, e), a = cf.A(l, e);
+    Cv = (tile[e * LD + l] - a * Cv) * ib;
+    M = -a * ib * M;
+  }
+  sM[ch * LT + l] = M;
+  sC[ch * LT + l] = Cv;
+  __syncthreads();
+  if (ch == 0) {  // sequential combine over the CH chunks of line l
+    double y = 0.0;
+    for (int k = 0; k < CH; k++) {
+      double m = sM[k * LT + l], cc = sC[k * LT + l];
+      sC[k * LT + l] = y;  // input of chunk k
+      y = cc + m * y;
+    }
+  }
+  __syncthreads();
+  double y = sC[ch * LT + l];
+  for (int e = e0; e < e1; e++) {
+    y = (tile[e * LD + l] - cf.A(l, e) * y) * cf.IB(l, e);
+    tile[e * LD + l] = y;
+  }
+  __syncthreads();
+  // backward: x_e = g_e - (c_e ib_e) x_{e+1}
+  M = 1.0;
+  Cv = 0.0;
+  for (int e = e1 - 1; e >= e0; e--) {
+    double u = cf.Cc(l, e) * cf.IB(l, e);
+    Cv = tile[e * LD + l] - u * Cv;
+    M = -u * M;
+  }
+  sM[ch * LT + l] = M;
+  sC[ch * LT + l] = Cv;
+  __syncthreads();
+  if (ch == 0) {
+    double x = 0.0;
+    for (int k = CH - 1; k >= 0; k--) {
+      double m = sM[k * LT + l], cc = sC[k * LT + l];
+      sC[k * LT + l] = x;  // input (x beyond the chunk end) of chunk k
+      x = cc + m * x;
+    }
+  }
+  __syncthreads();
+  double x = sC[ch * LT + l];
+  for (int e = e1 - 1; e >= e0; e--) {
+    x = tile[e * LD + l] - cf.Cc(l, e) * cf.IB(l, e) * x;
+    tile[e * LD + l] = x;
+  }
+  __syncthreads();
+}
+
+// Line sweep parameters.  Element e of line (i, m2) sits at
+//   (i-1) + s2 * m2 + se * (e0 + e)
+// in every ghosted array; the tile covers theta cells i0+1 .. i0+LT.
+struct SweepArgs {
+  const double *in;
+  double *out;
+  const double *add;   // out = add + x when non-null, else out = x
+  int s2, se, e0, n;   // strides, first element index, unknowns per line
+  int m2_0;            // first value of the second line index
+  // boundary right-hand sides for element 0 / n-1 (z sweeps): from a 2-D
+  // (nth, nrc) array indexed with the line's (i, m2), or the constant 0
+  const double *bc_lo, *bc_hi;
+  int bc_lo_on, bc_hi_on;
+  int mode;  // 0 plain; 1: z sweep of q1/q3 (slip ghost at j = nr+1);
+             // 2: r sweep of q2 (axis row j=1 and wall ghost j=nr+1)
+  double slip;
+  int nrc, nr, nth, J3;
+};
+
+template <int LT, int CH>
+__global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgs s, CoefShared cf) {
+  extern __shared__ double smem[];
+  const int LD = LT + 1;
+  double *tile = smem;
+  double *sM = tile + (size_t)s.n * LD;
+  double *sC = sM + LT * CH;
+  const int i0 = blockIdx.x * LT;  // 0-based theta of the first line
+  const int m2 = s.m2_0 + blockIdx.y;
+  const int nthreads = LT * CH;
+  const int nl = min(LT, s.nth - i0);
+  // load rows
+  for (int idx = threadIdx.x; idx < s.n * LT; idx += nthreads) {
+    int e = idx / LT, l = idx % LT;
+    double v = 0.0;
+    if (l < nl) {
+      v = s.in[(i0 + l) + s.s2 * m2 + s.se * (s.e0 + e)];
+      if (e == 0 && s.bc_lo_on) v = s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
+      if (e == s.n - 1 && s.bc_hi_on) v = s.bc_hi ? s.bc_hi[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
+    }
+    tile[e * LD + l] = v;
+  }
+  __syncthreads();
+  tile_solve<LT, CH>(tile, LD, s.n, cf, sM, sC);
+  for (int idx = threadIdx.x; idx < s.n * LT; idx += nthreads) {
+    int e = idx / LT, l = idx % LT;
+    if (l >= nl) continue;
+    int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
+    double x = tile[e * LD + l];
+    double v = s.add ? s.add[o] + x : x;
+    s.out[o] = v;
+    if (s.mode == 1 && m2 == s.nr)  // dq(ic, nrc, kc) = slip * dq(ic, nr, kc)
+      s.out[o + s.nth] = s.slip * v;
+    if (s.mode == 2) {
+      if (e == 0)  // dq2(ic, 1, kc) = stri(1) + q2(ic, 1, kc) with stri(1) = 0
+        s.out[o - s.se] = s.add[o - s.se] + 0.0;
+      if (e == s.n - 1)  // dq2(ic, nrc, kc) = 0.0*slip*dq2(ic, nr, kc)
+        s.out[o + s.se] = 0.0 * s.slip * v;
+    }
+  }
+}
+
+template <int LT, int CH>
+static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared &cf, int nm2) {
+  size_t sm = sizeof(double) * ((size_t)s.n * (LT + 1) + 2 * LT * CH);
+  cudaError_t e = cudaFuncSetAttribute(k_linesweep<LT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm);
+  if (e) return e;
+  dim3 gr((s.nth + LT - 1) / LT, nm2);
+  k_linesweep<LT, CH><<<gr, LT * CH, sm, c->stream>>>(s, cf);
+  return cudaGetLastError();
+}
+
+// tile width by line length so the tile fits the 227 KB of shared memory
+static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared &cf, int nm2) {
+  if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
+  if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);
+  return run_linesweep<4, 64>(c, s, cf, nm2);
+}
+
+// solqj (step.F90:266-358): lines (ic, kc) along j.
+cudaError_t launch_rsweep(vr_ctx *c, int comp) {
+  const Geo &g = c->geo;
+  const Tri &t = c->rtri[c->irk][comp - 1];
+  SweepArgs s{};
+  s.in = c->qrhs[comp - 1];
+  s.s2 = g.pl;
+  s.se = g.nth;
+  s.n = t.n;
+  s.nth = g.nth;
+  s.nr = g.nr;
+  s.nrc = g.nrc;
+  s.J3 = g.J3;
+  s.slip = g.slip;
+  int nm2;
+  if (comp == 2) {  // rows 2..nr (Dirichlet rows 1 and nrc), kc = 1..nzc, dq2 = q2 + x
+    s.out = c->dq[1];
+    s.add = c->q[1];
+    s.e0 = 2;
+    s.m2_0 = 1;
+    nm2 = g.nzc;
+    s.mode = 2;
+  } else {  // q1: kc = 1..nz ; q3: kc = 2..nz (kc = 1 is replaced by the z sweep's row)
+    s.out = c->qrhs[comp - 1];
+    s.add = nullptr;
+    s.e0 = 1;
+    s.m2_0 = comp == 3 ? 2 : 1;
+    nm2 = g.nz - s.m2_0 + 1;
+    s.mode = 0;
+  }
+  return dispatch_linesweep(c, s, CoefShared{t.a, t.c, t.ib}, nm2);
+}
+
+// solqk (step.F90:360-485): lines (ic, jc) along k = 1..nzc.
+cudaError_t launch_zsweep(vr_ctx *c, int comp) {
+  const Geo &g = c->geo;
+  const Tri &t = c->ztri[c->irk][comp - 1];
+  SweepArgs s{};
+  s.in = c->qrhs[comp - 1];
+  s.s2 = g.nth;
+  s.se = g.pl;
+  s.e0 = 1;
+  s.n = t.n;
+  s.nth = g.nth;
+  s.nr = g.nr;
+  s.nrc = g.nrc;
+  s.J3 = g.J3;
+  s.slip = g.slip;
+  s.bc_lo_on = 1;  // corr1s/corr2s/corr3s; the first two are identically 0
+  s.bc_hi_on = 1;  // 0*corr1n, 0*corr2n, corr3n
+  s.bc_lo = comp == 3 ? c->corr3s : nullptr;
+  s.bc_hi = comp == 3 ? c->corr3n : nullptr;
+  int nm2;
+  if (comp == 2) {  // lines jc = 2..nr; jc = 1 and nrc are replaced by solqj's Dirichlet rows
+    s.out = c->qrhs[1];
+    s.add = nullptr;
+    s.m2_0 = 2;
+    nm2 = g.nr - 1;
+    s.mode = 0;
+  } else {  // lines jc = 1..nr; jc = nrc is the slip ghost
+    s.out = c->dq[comp - 1];
+    s.add = c->q[comp - 1];
+    s.m2_0 = 1;
+    nm2 = g.nr;
+    s.mode = 1;
+  }
+  return dispatch_linesweep(c, s, CoefShared{t.a, t.c, t.ib}, nm2);
+}
+
+}  // namespace vr

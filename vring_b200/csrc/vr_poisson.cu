@@ -1,0 +1,394 @@
+// vr_poisson.cu -- pressure Poisson solve of poisson_solve.F90 (fftp path):
+//   theta: packed real DFT [a0, a1, b1, a2, b2, ...] (fastfouriertransform.F90:10-48)
+//   z:     DCT-II scaled 1/(2 nz) (REDFT10), inverse DCT-III (REDFT01)
+//          (fastfouriertransform.F90:250-339)
+//   r:     one tridiagonal solve per (theta mode, z mode) (poisson_solve.F90:270-323)
+//   back:  DCT-III along z, inverse packed DFT along theta, copied into dph.
+//
+// Power-of-two lengths run radix-2 FFTs in shared memory (twiddles computed
+// on the host in double); other lengths use the direct sums.  The radial
+// factorisation depends only on (theta mode, z mode) and is built once at
+// vr_create; the solve streams the right-hand side through a shared-memory
+// tile and runs the two substitutions chunk-parallel (see vr_momentum.cu).
+#include <cuda_runtime.h>
+
+#include "vr_internal.cuh"
+
+namespace vr {
+
+__device__ __forceinline__ int brev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
+
+__host__ __device__ inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+static int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
+// In-place radix-2 FFT of LPB lines of length n held in (re, im) with the
+// input already in bit-reversed order; sign -1 forward, +1 backward.
+// tw holds (cos, sin)(2 pi p / n) for p = 0..n-1.
+__device__ void smem_fft(double *re, double *im, int n, int lpb, const double *__restrict__ tw, int sign) {
+  const int half = n >> 1;
+  for (int h = 1; h < n; h <<= 1) {
+    int step = n / (2 * h);
+    for (int idx = threadIdx.x; idx < lpb * half; idx += blockDim.x) {
+      int l = idx / half, b = idx % half;
+      int grp = b / h, pos = b % h;
+      int i1 = l * n + grp * 2 * h + pos, i2 = i1 + h;
+      double wr = __ldg(tw + 2 * (pos * step)), wi = sign * __ldg(tw + 2 * (pos * step) + 1);
+      double xr = re[i2], xi = im[i2];
+      double tr = xr * wr - xi * wi, ti = xr * wi + xi * wr;
+      double ar = re[i1], ai = im[i1];
+      re[i2] = ar - tr;
+      im[i2] = ai - ti;
+      re[i1] = ar + tr;
+      im[i1] = ai + ti;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// theta transforms on lines of nth contiguous values
+// ---------------------------------------------------------------------------
+__global__ void k_fft_fwd(const double *__restrict__ in, double *__restrict__ out, int N, int logn,
+                          int lpb, int nlines, const double *__restrict__ tw) {
+  extern __shared__ double sm[];
+  double *re = sm, *im = sm + lpb * N;
+  int line0 = blockIdx.x * lpb;
+  int nl = min(lpb, nlines - line0);
+  for (int idx = threadIdx.x; idx < lpb * N; idx += blockDim.x) {
+    int l = idx / N, n = idx % N;
+    double v = l < nl ? in[(size_t)(line0 + l) * N + n] : 0.0;
+    re[l * N + brev(n, logn)] = v;
+    im[l * N + brev(n, logn)] = 0.0;
+  }
+  __syncthreads();
+  smem_fft(re, im, N, lpb, tw, -1);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    int l = idx / N, s = idx % N;  // output slot s (0-based)
+    double v;
+    if (s == 0) {
+      v = re[l * N] / N;
+    } else if (s & 1) {  // a_k, k = (s+1)/2
+      int k = (s + 1) >> 1;
+      v = 2.0 * re[l * N + k] / N;
+    } else {  // b_k, k = s/2 (k < N/2)
+      int k = s >> 1;
+      v = -2.0 * im[l * N + k] / N;
+    }
+    out[(size_t)(line0 + l) * N + s] = v;
+  }
+}
+
+// inverse: packed -> values; writes into dph(i, j, k) (j = 1..nr, k = 1..nz)
+__global__ void k_fft_bwd(const double *__restrict__ in, double *__restrict__ dph, Geo g, int logn, int lpb,
+                          int nlines, const double *__restrict__ tw) {
+  extern __shared__ double sm[];
+  const int N = g.nth;
+  double *re = sm, *im = sm + lpb * N;
+  int line0 = blockIdx.x * lpb;
+  int nl = min(lpb, nlines - line0);
+  for (int idx = threadIdx.x; idx < lpb * N; idx += blockDim.x) {
+    int l = idx / N, k = idx % N;
+    double fr = 0.0, fi = 0.0;
+    if (l < nl) {
+      const double *p = in + (size_t)(line0 + l) * N;
+      int kk = k <= N / 2 ? k : N - k;  // Hermitian extension
+      if (kk == 0) {
+        fr = p[0];
+      } else {
+        fr = p[2 * kk - 1] / 2.0;
+        fi = (2 * kk < N) ? -1.0 * p[2 * kk] / 2.0 : 0.0;
+      }
+      if (k > N / 2) fi = -fi;
+      if (2 * kk == N) fi = 0.0;
+    }
+    re[l * N + brev(k, logn)] = fr;
+    im[l * N + brev(k, logn)] = fi;
+  }
+  __syncthreads();
+  smem_fft(re, im, N, lpb, tw, +1);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    int l = idx / N, n = idx % N;
+    int L = line0 + l;  // L = (j-1) + nr*(k-1)
+    int j = 1 + L % g.nr, k = 1 + L / g.nr;
+    dph[IDP(g, n + 1, j, k)] = re[l * N + n];
+  }
+}
+
+// direct sums for lengths that are not powers of two
+__global__ void k_dft_fwd_direct(const double *__restrict__ in, double *__restrict__ out, int N, int nlines) {
+  int L = blockIdx.x;
+  if (L >= nlines) return;
+  const double *x = in + (size_t)L * N;
+  for (int s = threadIdx.x; s < N; s += blockDim.x) {
+    int k = (s + 1) >> 1;
+    double acc = 0.0;
+    for (int j = 0; j < N; j++) {
+      double sn, cs;
+      sincospi(2.0 * (double)(((long long)j * k) % N) / N, &sn, &cs);
+      acc += x[j] * ((s == 0 || (s & 1)) ? cs : -sn);
+    }
+    out[(size_t)L * N + s] = (s == 0) ? acc / N : (s & 1) ? 2.0 * acc / N : -2.0 * acc / N;
+  }
+}
+
+__global__ void k_dft_bwd_direct(const double *__restrict__ in, double *__restrict__ dph, Geo g, int nlines) {
+  int L = blockIdx.x;
+  if (L >= nlines) return;
+  const int N = g.nth;
+  const double *p = in + (size_t)L * N;
+  int j = 1 + L % g.nr, k = 1 + L / g.nr;
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    double s = p[0];
+    for (int kk = 1; kk <= N / 2; kk++) {
+      double sn, cs;
+      sincospi(2.0 * (double)(((long long)n * kk) % N) / N, &sn, &cs);
+      double fr = p[2 * kk - 1] / 2.0, fi = (2 * kk < N) ? -1.0 * p[2 * kk] / 2.0 : 0.0;
+      if (2 * kk == N)
+        s += fr * cs;
+      else
+        s += 2.0 * (fr * cs - fi * sn);
+    }
+    dph[IDP(g, n + 1, j, k)] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z transforms on lines (slot, j) of the (nth, nr, nz) spectral array,
+// stride nth*nr; a tile holds LT consecutive slots at fixed j.
+// ---------------------------------------------------------------------------
+template <int LT>
+__global__ void k_dct(double *__restrict__ a, Geo g, int logn, int dir, const double *__restrict__ twz) {
+  extern __shared__ double sm[];
+  const int n = g.nz;
+  double *re = sm, *im = sm + LT * n, *xr = sm + 2 * LT * n;
+  const int i0 = blockIdx.x * LT, j = blockIdx.y;  // j 0-based
+  const int nl = min(LT, g.nth - i0);
+  const size_t s2 = (size_t)g.nth * g.nr;
+  const double *shift = twz + 2 * n;  // (cos, sin)(pi k / (2n))
+  for (int idx = threadIdx.x; idx < LT * n; idx += blockDim.x) {
+    int k = idx / LT, l = idx % LT;
+    xr[l * n + k] = l < nl ? a[(i0 + l) + (size_t)g.nth * j + s2 * k] : 0.0;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < LT * n; idx += blockDim.x) {
+    int l = idx / n, k = idx % n;
+    double vr, vi;
+    int pos;
+    if (dir > 0) {  // v_p = x_{2p}, v_{n-1-p} = x_{2p+1}
+      vr = xr[l * n + k];
+      vi = 0.0;
+      pos = (k & 1) ? n - 1 - (k >> 1) : (k >> 1);
+    } else {  // V_k = e^{i pi k/(2n)} (X_k - i X_{n-k}) / 2
+      double x0 = xr[l * n + k] / 2.0, x1 = (k == 0) ? 0.0 : -xr[l * n + n - k] / 2.0;
+      double cr = __ldg(shift + 2 * k), ci = __ldg(shift + 2 * k + 1);
+      vr = x0 * cr - x1 * ci;
+      vi = x0 * ci + x1 * cr;
+      pos = k;
+    }
+    re[l * n + brev(pos, logn)] = vr;
+    im[l * n + brev(pos, logn)] = vi;
+  }
+  __syncthreads();
+  smem_fft(re, im, n, LT, twz, dir > 0 ? -1 : +1);
+  for (int idx = threadIdx.x; idx < LT * n; idx += blockDim.x) {
+    int k = idx / LT, l = idx % LT;
+    if (l >= nl) continue;
+    double v;
+    if (dir > 0) {
+      double cr = __ldg(shift + 2 * k), ci = __ldg(shift + 2 * k + 1);
+      v = 2.0 * (re[l * n + k] * cr + im[l * n + k] * ci) / (2.0 * n * 1);
+    } else {
+      v = (k & 1) ? 2.0 * re[l * n + n - 1 - (k >> 1)] : 2.0 * re[l * n + (k >> 1)];
+    }
+    a[(i0 + l) + (size_t)g.nth * j + s2 * k] = v;
+  }
+}
+
+__global__ void k_dct_direct(double *__restrict__ a, Geo g, int dir) {
+  extern __shared__ double sm[];
+  const int n = g.nz;
+  const int slot = blockIdx.x, j = blockIdx.y;
+  const size_t s2 = (size_t)g.nth * g.nr;
+  double *x = sm;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) x[k] = a[slot + (size_t)g.nth * j + s2 * k];
+  __syncthreads();
+  double y[8];
+  int cnt = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double s = 0.0;
+    if (dir > 0) {
+      for (int p = 0; p < n; p++) s += x[p] * cospi((double)(((long long)(2 * p + 1) * k) % (4 * n)) / (2.0 * n));
+      s = 2.0 * s / (2.0 * n * 1);
+    } else {
+      s = x[0];
+      for (int p = 1; p < n; p++) s += 2.0 * x[p] * cospi((double)(((long long)p * (2 * k + 1)) % (4 * n)) / (2.0 * n));
+    }
+    y[cnt++] = s;
+  }
+  __syncthreads();
+  cnt = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) a[slot + (size_t)g.nth * j + s2 * k] = y[cnt++];
+}
+
+// ---------------------------------------------------------------------------
+// radial solves: lines (slot, kz) along j, per-line factorisation from the
+// (kz, j, mode) table; slot s (1-based) carries mode m = s/2.
+// ---------------------------------------------------------------------------
+template <int LT, int CH>
+__device__ void tile_solve_pois(double *tile, int LD, int n, const double *__restrict__ pa,
+                                const double *__restrict__ pc, const double *__restrict__ ib, int nm,
+                                int mm0, double *sM, double *sC) {
+  // identical to tile_solve of vr_momentum.cu with per-line ib
+  const int t = threadIdx.x;
+  const int l = t % LT, ch = t / LT;
+  const int CL = (n + CH - 1) / CH;
+  const int e0 = ch * CL, e1 = min(n, e0 + CL);
+  const int mm = min((mm0 + l + 1) / 2, nm - 1);  // mode of slot i0+l+1 (padding lines clamped)
+  auto IB = [&](int e) { return __ldg(ib + (size_t)e * nm + mm); };
+  double M = 1.0, Cv = 0.0;
+  for (int e = e0; e < e1; e++) {
+    double b = IB(e), a = __ldg(pa + e);
+    Cv = (tile[e * LD + l] - a * Cv) * b;
+    M = -a * b * M;
+  }
+  sM[ch * LT + l] = M;
+  sC[ch * LT + l] = Cv;
+  __syncthreads();
+  if (ch == 0) {
+    double y = 0.0;
+    for (int k = 0; k < CH; k++) {
+      double m = sM[k * LT + l], cc = sC[k * LT + l];
+      sC[k * LT + l] = y;
+      y = cc + m * y;
+    }
+  }
+  __syncthreads();
+  double y = sC[ch * LT + l];
+  for (int e = e0; e < e1; e++) {
+    y = (tile[e * LD + l] - __ldg(pa + e) * y) * IB(e);
+    tile[e * LD + l] = y;
+  }
+  __syncthreads();
+  M = 1.0;
+  Cv = 0.0;
+  for (int e = e1 - 1; e >= e0; e--) {
+    double u = __ldg(pc + e) * IB(e);
+    Cv = tile[e * LD + l] - u * Cv;
+    M = -u * M;
+  }
+  sM[ch * LT + l] = M;
+  sC[ch * LT + l] = Cv;
+  __syncthreads();
+  if (ch == 0) {
+    double x = 0.0;
+    for (int k = CH - 1; k >= 0; k--) {
+      double m = sM[k * LT + l], cc = sC[k * LT + l];
+      sC[k * LT + l] = x;
+      x = cc + m * x;
+    }
+  }
+  __syncthreads();
+  double x = sC[ch * LT + l];
+  for (int e = e1 - 1; e >= e0; e--) {
+    x = tile[e * LD + l] - __ldg(pc + e) * IB(e) * x;
+    tile[e * LD + l] = x;
+  }
+  __syncthreads();
+}
+
+template <int LT, int CH>
+__global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g, const double *__restrict__ pa,
+                                                   const double *__restrict__ pc, const double *__restrict__ pib) {
+  extern __shared__ double sm[];
+  const int LD = LT + 1, n = g.nr, nm = g.nth / 2 + 1;
+  double *tile = sm, *sM = tile + (size_t)n * LD, *sC = sM + LT * CH;
+  const int i0 = blockIdx.x * LT, kz = blockIdx.y;
+  const int nl = min(LT, g.nth - i0);
+  const size_t base = (size_t)g.nth * g.nr * kz;
+  for (int idx = threadIdx.x; idx < n * LT; idx += LT * CH) {
+    int e = idx / LT, l = idx % LT;
+    tile[e * LD + l] = l < nl ? a[base + (i0 + l) + (size_t)g.nth * e] : 0.0;
+  }
+  __syncthreads();
+  tile_solve_pois<LT, CH>(tile, LD, n, pa, pc, pib + (size_t)kz * n * nm, nm, i0, sM, sC);
+  for (int idx = threadIdx.x; idx < n * LT; idx += LT * CH) {
+    int e = idx / LT, l = idx % LT;
+    if (l < nl) a[base + (i0 + l) + (size_t)g.nth * e] = tile[e * LD + l];
+  }
+}
+
+template <int LT, int CH>
+static cudaError_t run_radial(vr_ctx *c) {
+  const Geo &g = c->geo;
+  size_t sm = sizeof(double) * ((size_t)g.nr * (LT + 1) + 2 * LT * CH);
+  cudaError_t e = cudaFuncSetAttribute(k_radial<LT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  k_radial<LT, CH><<<dim3((g.nth + LT - 1) / LT, g.nz), LT * CH, sm, c->stream>>>(c->spec, g, c->pois_a, c->pois_c,
+                                                                                c->pois_ib);
+  return cudaGetLastError();
+}
+
+template <int LT>
+static cudaError_t run_dct(vr_ctx *c, int dir) {
+  const Geo &g = c->geo;
+  size_t sm = sizeof(double) * 3 * LT * g.nz;
+  cudaError_t e = cudaFuncSetAttribute(k_dct<LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  k_dct<LT><<<dim3((g.nth + LT - 1) / LT, g.nr), 256, sm, c->stream>>>(c->spec, g, ilog2(g.nz), dir, c->tw_z);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_poisson(vr_ctx *c) {
+  const Geo &g = c->geo;
+  cudaError_t e;
+  const int N = g.nth, nlines = g.nr * g.nz;
+  // theta forward: rhs -> spec
+  if (is_pow2(N)) {
+    int lpb = N >= 1024 ? 1 : 1024 / N;
+    size_t sm = sizeof(double) * 2 * lpb * N;
+    if ((e = cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_fwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->rhs, c->spec, N, ilog2(N), lpb, nlines,
+                                                                c->tw_th);
+  } else {
+    k_dft_fwd_direct<<<nlines, 64, 0, c->stream>>>(c->rhs, c->spec, N, nlines);
+  }
+  if ((e = cudaGetLastError())) return e;
+  // z forward DCT
+  if (is_pow2(g.nz)) {
+    if ((e = g.nz <= 1024 ? run_dct<8>(c, +1) : run_dct<4>(c, +1))) return e;
+  } else {
+    k_dct_direct<<<dim3(N, g.nr), 64, sizeof(double) * g.nz, c->stream>>>(c->spec, g, +1);
+  }
+  if ((e = cudaGetLastError())) return e;
+  // radial solves
+  if (g.nr <= 640)
+    e = run_radial<16, 16>(c);
+  else if (g.nr <= 1600)
+    e = run_radial<8, 32>(c);
+  else
+    e = run_radial<4, 64>(c);
+  if (e) return e;
+  // z backward
+  if (is_pow2(g.nz)) {
+    if ((e = g.nz <= 1024 ? run_dct<8>(c, -1) : run_dct<4>(c, -1))) return e;
+  } else {
+    k_dct_direct<<<dim3(N, g.nr), 64, sizeof(double) * g.nz, c->stream>>>(c->spec, g, -1);
+  }
+  if ((e = cudaGetLastError())) return e;
+  // theta backward -> dph
+  if (is_pow2(N)) {
+    int lpb = N >= 1024 ? 1 : 1024 / N;
+    size_t sm = sizeof(double) * 2 * lpb * N;
+    if ((e = cudaFuncSetAttribute(k_fft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_bwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->spec, c->dph, g, ilog2(N), lpb, nlines, c->tw_th);
+  } else {
+    k_dft_bwd_direct<<<nlines, 64, 0, c->stream>>>(c->spec, c->dph, g, nlines);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace vr

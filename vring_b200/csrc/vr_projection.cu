@@ -1,0 +1,226 @@
+// vr_projection.cu -- divergence, velocity projection and pressure update of
+// divergence.F90 (divq :16-67, upsol :69-236, uppres :239-480) plus the
+// FP64 diagnostics (max |div q|, non-finite count).
+//
+// uppres builds three auxiliary gradient fields (qcap) and applies a
+// Laplacian-type stencil to each; here every qcap value is recomputed from
+// dph inside the one kernel that updates prg and pres, so qcap never goes
+// to HBM: the pass reads dph once (neighbours from L1/L2) and prg/pres once.
+#include <cuda_runtime.h>
+
+#include "vr_internal.cuh"
+
+namespace vr {
+
+__device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// divq: rhs = -div(dq) / (alpha dt)
+// ---------------------------------------------------------------------------
+__global__ void k_divq(Geo g, double inv_adt, const double *__restrict__ dq1, const double *__restrict__ dq2,
+                       const double *__restrict__ dq3, double *__restrict__ rhs) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  int ip = ic < g.nth ? ic + 1 : 1;
+  int o = I3(g, ic, jc, kc);
+  double irm = g.irm[jc];
+  double d = (ldg(dq1 + I3(g, ip, jc, kc)) - ldg(dq1 + o)) * g.dx1 * g.axsym * irm +
+             (ldg(dq2 + o + g.nth) - ldg(dq2 + o)) * g.dx2 * irm +
+             (ldg(dq3 + o + g.pl) - ldg(dq3 + o)) * g.dx3;
+  rhs[IRS(g, ic, jc, kc)] = -d * inv_adt;
+}
+
+cudaError_t launch_divq(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  k_divq<<<gr, b, 0, c->stream>>>(g, 1.0 / (rk.alm * g.dt), c->dq[0], c->dq[1], c->dq[2], c->rhs);
+  return cudaGetLastError();
+}
+
+// dph with the north ghost dph(nzc) = dph(nz) (divergence.F90:93-99, 254-258)
+__device__ __forceinline__ double dphv(const Geo &g, const double *__restrict__ dph, int i, int j, int k) {
+  return ldg(dph + IDP(g, i, j, k == g.nzc ? g.nz : k));
+}
+
+// ---------------------------------------------------------------------------
+// upsol (divergence.F90:69-236): one thread per (ic, jc = 0..nrc, kc = 1..nzc)
+// ---------------------------------------------------------------------------
+__global__ void k_upsol(Geo g, double adt, const double *__restrict__ dq1, const double *__restrict__ dq2,
+                        const double *__restrict__ dq3, const double *__restrict__ dph, double *__restrict__ q1,
+                        double *__restrict__ q2, double *__restrict__ q3, double *__restrict__ dphw) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = blockIdx.y * blockDim.y + threadIdx.y;  // 0..nrc
+  int kc = 1 + blockIdx.z;                          // 1..nzc
+  if (ic > g.nth || jc > g.nrc) return;
+  int im = ic > 1 ? ic - 1 : g.nth;
+  int o = I3(g, ic, jc, kc);
+  if (kc == g.nzc && jc >= 1 && jc <= g.nr) dphw[IDP(g, ic, jc, g.nzc)] = ldg(dph + IDP(g, ic, jc, g.nz));
+  // q1
+  if (jc >= 1) {
+    int j = jc <= g.nr ? jc : g.nr;
+    double v = ldg(dq1 + I3(g, ic, j, kc)) -
+               (adt * g.dx1 * g.irm[j]) * (dphv(g, dph, ic, j, kc) - dphv(g, dph, im, j, kc));
+    q1[o] = jc <= g.nr ? v : g.slip * v;
+  }
+  // q2
+  if (jc >= 1) {
+    if (jc == 1 || jc == g.nrc) {
+      q2[o] = 0.0;
+    } else {
+      q2[o] = ldg(dq2 + o) - adt * g.rc[jc] * g.dx2 * (dphv(g, dph, ic, jc, kc) - dphv(g, dph, ic, jc - 1, kc));
+    }
+  }
+  // q3
+  if (kc == 1) {
+    q3[o] = ldg(dq3 + o);  // jc = 0..nrc: imposed south value
+  } else if (jc >= 1) {
+    int j = jc <= g.nr ? jc : g.nr;
+    double v = ldg(dq3 + I3(g, ic, j, kc)) - adt * g.dx3 * (dphv(g, dph, ic, j, kc) - dphv(g, dph, ic, j, kc - 1));
+    q3[o] = jc <= g.nr ? v : g.slip * v;
+  }
+}
+
+cudaError_t launch_upsol(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nrc + 1 + 3) / 4, g.nzc);
+  k_upsol<<<gr, b, 0, c->stream>>>(g, rk.alm * g.dt, c->dq[0], c->dq[1], c->dq[2], c->dph, c->q[0], c->q[1],
+                                   c->q[2], c->dph);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// uppres (divergence.F90:239-480)
+// ---------------------------------------------------------------------------
+// gradient components of phi (the reference's qcap for each direction)
+__device__ __forceinline__ double gth(const Geo &g, const double *dph, int i, int j, int k) {
+  int im = i > 1 ? i - 1 : g.nth;
+  return (dphv(g, dph, i, j, k) - dphv(g, dph, im, j, k)) * g.dx1 * g.irm[j];
+}
+__device__ __forceinline__ double grr(const Geo &g, const double *dph, int i, int j, int k) {
+  if (j <= 1 || j >= g.nrc) return 0.0;  // qcap(ic,1,:) = qcap(ic,nrc,:) = 0
+  return (dphv(g, dph, i, j, k) - dphv(g, dph, i, j - 1, k)) * g.dx2 * g.rc[j];
+}
+__device__ __forceinline__ double gzz(const Geo &g, const double *dph, int i, int j, int k) {
+  if (k <= 1) return 0.0;  // qcap(ic,jc,1) = 0
+  return (dphv(g, dph, i, j, k) - dphv(g, dph, i, j, k - 1)) * g.dx3;
+}
+
+__global__ void k_uppres(Geo g, double be, const double *__restrict__ dph, double *__restrict__ prg,
+                         double *__restrict__ pres) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  int km = kc == 1 ? 1 : (kc == g.nz ? g.nz : kc - 1);  // kmv (mesh_tools.F90:272-280)
+  int kp = kc + 1;
+  int jm = jc > 1 ? jc - 1 : 1, jp = jc < g.nr ? jc + 1 : g.nr;  // jmv, jpv
+  // theta component (divergence.F90:270-311)
+  {
+    double c0 = gth(g, dph, ic, jc, kc);
+    double d11 = (gth(g, dph, ip, jc, kc) - 2.0 * c0 + gth(g, dph, im, jc, kc)) * g.s1t11[jc];
+    double d33 = (gth(g, dph, ic, jc, kp) - 2.0 * c0 + gth(g, dph, ic, jc, km)) * g.dx3q;
+    double qnn = gth(g, dph, ic, jp, kc) * g.irm[jc + 1] - c0 * g.irm[jc];
+    double qss = c0 * g.irm[jc] - gth(g, dph, ic, jm, kc) * g.irm[jm];
+    double d22 = (qnn * g.s1t2n[jc] - qss * g.s1t2s[jc]) * g.s1t2c[jc];
+    int o = IPRG(g, ic, jc, kc, 1);
+    prg[o] = prg[o] + c0 - be * (d11 + d33 + d22);
+  }
+  // r component, jc >= 2 (divergence.F90:315-373)
+  if (jc >= 2) {
+    double c0 = grr(g, dph, ic, jc, kc);
+    double d11 = (grr(g, dph, ip, jc, kc) - 2.0 * c0 + grr(g, dph, im, jc, kc)) * g.s2t11[jc];
+    double d33 = (grr(g, dph, ic, jc, kp) - 2.0 * c0 + grr(g, dph, ic, jc, km)) * g.dx3q;
+    double qnn = grr(g, dph, ic, jc + 1, kc) - c0;
+    double qss = c0 - grr(g, dph, ic, jc - 1, kc);
+    double d22 = qnn * g.s2t2p[jc] - qss * g.s2t2m[jc];
+    int o = IPRG(g, ic, jc, kc, 2);
+    prg[o] = prg[o] + c0 - be * (d11 + d22 + d33);
+  }
+  // z component, kc >= 2 (divergence.F90:378-439)
+  if (kc >= 2) {
+    double c0 = gzz(g, dph, ic, jc, kc);
+    double d11 = (gzz(g, dph, ip, jc, kc) - 2.0 * c0 + gzz(g, dph, im, jc, kc)) * g.s1t11[jc];
+    double d33 = (gzz(g, dph, ic, jc, kc + 1) - 2.0 * c0 + gzz(g, dph, ic, jc, kc - 1)) * g.dx3q;
+    double qnn = gzz(g, dph, ic, jp, kc) - c0;
+    double qss = c0 - gzz(g, dph, ic, jm, kc);
+    double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
+    int o = IPRG(g, ic, jc, kc, 3);
+    prg[o] = prg[o] + c0 - be * (d11 + d22 + d33);
+  }
+  // pressure (divergence.F90:445-476)
+  {
+    double p0 = dphv(g, dph, ic, jc, kc);
+    double d11 = (dphv(g, dph, ip, jc, kc) + dphv(g, dph, im, jc, kc) - 2.0 * p0) * g.s1t11[jc];
+    double qnn = dphv(g, dph, ic, jp, kc) - p0;
+    double qss = p0 - dphv(g, dph, ic, jm, kc);
+    double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
+    double d33 = (dphv(g, dph, ic, jc, kp) + dphv(g, dph, ic, jc, km) - 2.0 * p0) * g.dx3q;
+    int o = I3(g, ic, jc, kc);
+    pres[o] = pres[o] + p0 - be * (d11 + d22 + d33);
+  }
+}
+
+cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  double be = 0.5 * (rk.alm * g.dt) / g.re;
+  k_uppres<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// diagnostics
+// ---------------------------------------------------------------------------
+__global__ void k_zero(double *p, unsigned long long *q) {
+  if (p) *p = 0.0;
+  if (q) *q = 0ull;
+}
+
+__global__ void k_maxdiv(Geo g, const double *__restrict__ q1, const double *__restrict__ q2,
+                         const double *__restrict__ q3, double *out) {
+  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  int kc = 1 + blockIdx.z;
+  double v = 0.0;
+  if (ic <= g.nth && jc <= g.nr) {
+    int ip = ic < g.nth ? ic + 1 : 1;
+    int o = I3(g, ic, jc, kc);
+    double irm = g.irm[jc];
+    v = fabs((ldg(q1 + I3(g, ip, jc, kc)) - ldg(q1 + o)) * g.dx1 * g.axsym * irm +
+             (ldg(q2 + o + g.nth) - ldg(q2 + o)) * g.dx2 * irm + (ldg(q3 + o + g.pl) - ldg(q3 + o)) * g.dx3);
+    if (v != v) v = __longlong_as_double(0x7ff0000000000000ll);  // NaN reports as +inf
+  }
+  for (int s = 16; s; s >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, s));
+  if ((threadIdx.x & 31) == 0)
+    atomicMax((unsigned long long *)out, (unsigned long long)__double_as_longlong(v));
+}
+
+cudaError_t launch_maxdiv(vr_ctx *c, double *d_out) {
+  const Geo &g = c->geo;
+  k_zero<<<1, 1, 0, c->stream>>>(d_out, nullptr);
+  dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  k_maxdiv<<<gr, b, 0, c->stream>>>(g, c->q[0], c->q[1], c->q[2], d_out);
+  return cudaGetLastError();
+}
+
+__global__ void k_nonfinite(const double *__restrict__ a, size_t n, unsigned long long *cnt) {
+  unsigned long long local = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(ldg(a + i))) local++;
+  for (int s = 16; s; s >>= 1) local += __shfl_down_sync(0xffffffffu, local, s);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(cnt, local);
+}
+
+cudaError_t launch_count_nonfinite(vr_ctx *c, unsigned long long *d_out) {
+  const Geo &g = c->geo;
+  size_t n3 = (size_t)g.nth * g.J3 * g.K3;
+  k_zero<<<1, 1, 0, c->stream>>>(nullptr, d_out);
+  const double *f[4] = {c->q[0], c->q[1], c->q[2], c->pres};
+  for (const double *p : f) k_nonfinite<<<4 * 148, 256, 0, c->stream>>>(p, n3, d_out);
+  return cudaGetLastError();
+}
+
+}  // namespace vr
