@@ -35,7 +35,18 @@ def assert_field_close(gpu, orc, name, rel=1e-12, floor=1e-300):
     r = orc.field(name)
     assert g.shape == r.shape, (name, g.shape, r.shape)
     scale = max(np.abs(r).max(), floor)
-    err = np.abs(g - r).max()
-    assert err <= rel * scale, "%s: max |gpu - oracle| = %.3e, scale %.3e (rel %.2e)" % (
-        name, err, scale, err / scale)
+    d = np.abs(g - r)
+    err = d.max()
+    where = np.unravel_index(np.argmax(d), d.shape)
+    assert err <= rel * scale, "%s: max |gpu - oracle| = %.3e at %s, scale %.3e (rel %.2e)" % (
+        name, err, where, scale, err / scale)
     return err / scale
+
+
+def prep(orc, gpu, irk=1, ntime=0.0, nstep=0):
+    """Set the clock and build the substep's coefficients on both sides
+    (loop.F90:71-74 calls ucoeff and coesys before every substep)."""
+    for o in (orc, gpu):
+        o.set_clock(irk, ntime, nstep)
+        o.ucoeff()
+        o.coesys()

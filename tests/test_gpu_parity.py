@@ -10,7 +10,7 @@ field (1e-11 where a near-singular Poisson mode amplifies round-off).
 import numpy as np
 import pytest
 
-from parity_util import STATE, assert_field_close, copy_to_gpu, make_pair, seed_random
+from parity_util import STATE, assert_field_close, copy_to_gpu, make_pair, prep, seed_random
 
 pytestmark = pytest.mark.gpu
 
@@ -30,8 +30,7 @@ def _pair(grid, **kw):
 def test_hdnbc(grid, irk):
     orc, gpu = _pair(grid, inflow="reference")
     seed_random(orc, gpu, ["q3", "csort", "dq3no"], seed=irk)
-    for o in (orc, gpu):
-        o.set_clock(irk, 0.15, 3)
+    prep(orc, gpu, irk, 0.15, 3)
     orc.hdnbc()
     gpu.hdnbc()
     for n in ("csort", "tconv", "corr3n", "dq3no", "corr3s"):
@@ -42,6 +41,7 @@ def test_hdnbc(grid, irk):
 def test_hdnl(grid, comp):
     orc, gpu = _pair(grid)
     seed_random(orc, gpu, ["q1", "q2", "q3", "dq1", "dq2", "dq3"], seed=comp)
+    prep(orc, gpu)
     getattr(orc, "hdnl%d" % comp)()
     getattr(gpu, "hdnl%d" % comp)()
     assert_field_close(gpu, orc, "dq%d" % comp)
@@ -53,8 +53,7 @@ def test_step(grid, irk, slip):
     orc, gpu = _pair(grid, slip=slip)
     seed_random(orc, gpu, ["q1", "q2", "q3", "dq1", "dq2", "dq3", "ru1", "ru2", "ru3", "prg",
                            "corr3s", "corr3n"], seed=10 + irk)
-    for o in (orc, gpu):
-        o.set_clock(irk, 0.0, 0)
+    prep(orc, gpu, irk)
     orc.step()
     gpu.step()
     for n in ("dq1", "dq2", "dq3", "ru1", "ru2", "ru3"):
@@ -65,8 +64,7 @@ def test_step(grid, irk, slip):
 def test_divq(grid, irk):
     orc, gpu = _pair(grid)
     seed_random(orc, gpu, ["dq1", "dq2", "dq3"], seed=20 + irk)
-    for o in (orc, gpu):
-        o.set_clock(irk, 0.0, 0)
+    prep(orc, gpu, irk)
     orc.divq()
     gpu.divq()
     assert_field_close(gpu, orc, "rhs")
@@ -76,6 +74,7 @@ def test_divq(grid, irk):
 def test_laplace_solve(grid, wth):
     orc, gpu = _pair(grid, wth=wth)
     seed_random(orc, gpu, ["rhs"], seed=30)
+    prep(orc, gpu)
     orc.laplace_solve()
     gpu.laplace_solve()
     nth, nr, nz = grid
@@ -88,8 +87,7 @@ def test_laplace_solve(grid, wth):
 def test_upsol(grid, irk):
     orc, gpu = _pair(grid)
     seed_random(orc, gpu, ["q1", "q2", "q3", "dq1", "dq2", "dq3", "dph"], seed=40 + irk)
-    for o in (orc, gpu):
-        o.set_clock(irk, 0.0, 0)
+    prep(orc, gpu, irk)
     orc.upsol()
     gpu.upsol()
     for n in ("q1", "q2", "q3", "dph"):
@@ -100,8 +98,7 @@ def test_upsol(grid, irk):
 def test_uppres(grid, irk):
     orc, gpu = _pair(grid)
     seed_random(orc, gpu, ["dph", "prg", "pres"], seed=50 + irk)
-    for o in (orc, gpu):
-        o.set_clock(irk, 0.0, 0)
+    prep(orc, gpu, irk)
     orc.uppres()
     gpu.uppres()
     for n in ("prg", "pres", "dph"):
@@ -121,8 +118,7 @@ def _ring_state(orc, gpu, grid, seed=0):
 def test_fused_substep_matches_routine_sequence(grid, wth):
     orc, gpu = _pair(grid, wth=wth)
     _ring_state(orc, gpu, grid)
-    for o in (orc, gpu):
-        o.set_clock(1, 2e-3, 0)
+    prep(orc, gpu, 1, 2e-3, 0)
     orc.substep(1)
     gpu.substep(1)
     for n in STATE + ["dph", "rhs"]:

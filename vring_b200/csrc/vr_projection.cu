@@ -108,7 +108,7 @@ __device__ __forceinline__ double gzz(const Geo &g, const double *dph, int i, in
 }
 
 __global__ void k_uppres(Geo g, double be, const double *__restrict__ dph, double *__restrict__ prg,
-                         double *__restrict__ pres) {
+                         double *__restrict__ pres, double *__restrict__ dphw) {
   int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   int kc = 1 + blockIdx.z;
@@ -117,6 +117,9 @@ __global__ void k_uppres(Geo g, double be, const double *__restrict__ dph, doubl
   int km = kc == 1 ? 1 : (kc == g.nz ? g.nz : kc - 1);  // kmv (mesh_tools.F90:272-280)
   int kp = kc + 1;
   int jm = jc > 1 ? jc - 1 : 1, jp = jc < g.nr ? jc + 1 : g.nr;  // jmv, jpv
+  // the north ghost of dph is read through dphv(); it is also stored, as the
+  // reference does (divergence.F90:254-258)
+  if (kc == g.nz) dphw[IDP(g, ic, jc, g.nzc)] = ldg(dph + IDP(g, ic, jc, g.nz));
   // theta component (divergence.F90:270-311)
   {
     double c0 = gth(g, dph, ic, jc, kc);
@@ -167,7 +170,7 @@ cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   double be = 0.5 * (rk.alm * g.dt) / g.re;
-  k_uppres<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres);
+  k_uppres<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
   return cudaGetLastError();
 }
 
