@@ -1,0 +1,294 @@
+#!/usr/bin/env python
+"""Throughput of the RK3 fractional-step core on one vortex ring.
+
+Workload (the configuration the headline metric is quoted on): a Gaussian-core
+vortex ring (R = 1, sigma = 0.2, Gamma = 1, z0 = 3, seeded noise 1e-4) on the
+cylindrical staggered grid Nr x Ntheta x Nz = 256 x 128 x 512, r in [0, 4],
+z in [0, 12], Re = 3000, dt = 5e-4, free slip at r = 4 (slip = 1), the
+reference's z boundaries (wall + convective outflow) and the discrete theta
+wavenumber in the Poisson solve (max |div u| at round-off).  One step = one
+RK3 time step (3 substeps).  FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent replica per GPU (a single ring does not shard at
+this size); value = cells x steps of all ranks / max-over-ranks time.
+--impl reference times the CPU restatement of the same path (OpenMP over all
+host cores) on the same configuration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-RK3-steps/s at 256×128×512, mixed vs FP64 on B200 at max|div u|≤1e-9"
+UNIT = "Mcell-RK3-steps/s"
+NTH, NR, NZ = 128, 256, 512
+RMAX, ZMAX, DT, RE, SLIP = 4.0, 12.0, 5e-4, 3000.0, 1.0
+WORKLOAD = ("vortex ring, Nr x Ntheta x Nz = 256 x 128 x 512, r<=4, z<=12, Re 3000, dt 5e-4, "
+            "free slip, reference z boundaries, discrete theta wavenumber, FP64")
+# algorithmic 8-byte words per interior cell and substep, by kernel family
+# (each field word read or written once per logical phase of the reference):
+#   A rhs 15 | B theta 6, r 7, z 8 | C divq 4 | D fft 4, dct 4, radial 2 | E upsol 7 | F uppres 9
+WORDS = {"rhs": 15, "tsweep": 6, "rsweep": 7, "zsweep": 8, "divq": 4, "fft": 4, "dct": 4,
+         "radial": 2, "upsol": 7, "uppres": 9}
+WORDS_PER_CELL_STEP = 3 * sum(WORDS.values())  # 198 words = 1584 B
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """DRAM bytes per launch from the committed ncu summaries (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def ring_state():
+    from vring_b200.synthetic import ring_fields
+    return ring_fields(NTH, NR, NZ, RMAX, ZMAX, R=1.0, sigma=0.2, gamma=1.0, z0=3.0, noise=1e-4, seed=0)
+
+
+def cpu_reference(steps, budget_s, q=None):
+    """The CPU restatement on the same workload, all host threads; returns
+    (Mcell-steps/s, steps timed, threads)."""
+    from oracle import oracle as O
+    q = q if q is not None else ring_state()
+    o = O.Oracle(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, 1, 0, 0)
+    for n, a in zip(("q1", "q2", "q3"), q):
+        o.field(n)[...] = a
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        o.iterate(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return NTH * NR * NZ * done / el / 1e6, done, os.cpu_count()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    q = ring_state()
+    # untimed warm-up bounded to one step, then a bounded timed sample
+    if args.warmup > 0:
+        cpu_reference(1, 1e9, q)
+    val, done, cores = cpu_reference(args.steps, 150.0, q)
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ]},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d RK3 steps of the full 256x128x512 workload (CPU FP64 "
+                                       "restatement, OpenMP, %d threads)" % (done, cores)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import vring_b200 as V
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    q = ring_state()
+    run = V.Run(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, theta_wavenumber="modified", device=local)
+    for n, a in zip(("q1", "q2", "q3"), q):
+        run.set(n, a)
+    stream = torch.cuda.current_stream()
+    run.set_stream(stream.cuda_stream)
+    ncell = NTH * NR * NZ
+
+    for _ in range(args.warmup):
+        run.iterate(1)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, inputs resident in HBM ---------------------
+    clocks = ClockSampler(local)
+    run.profile(True)
+    n0 = run.launch_count
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        run.iterate(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = run.launch_count - n0
+    prof = run.profile_read()
+    run.profile(False)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = world * ncell * args.steps / (ms_max / 1e3) / 1e6
+    maxdiv = run.max_divergence()
+    nonfinite = run.count_nonfinite()
+
+    # ---- end to end: per step, velocity in from pinned host memory, one step
+    # through the C ABI, velocity back to pinned host memory ------------------
+    pins = [torch.empty(int(torch.tensor(a.shape).prod()), dtype=torch.float64, pin_memory=True)
+            for a in q]
+    for p, a in zip(pins, q):
+        p.numpy()[:] = a.ravel(order="F")
+    run.set_stream(0)
+    for p, n in zip(pins, ("q1", "q2", "q3")):  # warm the copy path once
+        run.set_ptr(n, p.data_ptr())
+    run.iterate(1)
+    run.sync()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        for p, n in zip(pins, ("q1", "q2", "q3")):
+            run.set_ptr(n, p.data_ptr())
+        run.iterate(1)
+        for p, n in zip(pins, ("q1", "q2", "q3")):
+            run.get_ptr(n, p.data_ptr())
+    run.sync()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    bytes_q = sum(p.numel() for p in pins) * 8
+    e2e_val = world * ncell * args.e2e_steps / e2e_s / 1e6
+
+    # ---- roofline of the dominant kernel family -------------------------------
+    peak, peak_kind = peaks()
+    fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
+    tot_ms, nl = prof[fam]
+    per_sub = nl / (3 * args.steps)  # launches of this family per substep
+    bytes_per_launch = WORDS[fam] / per_sub * ncell * 8
+    achieved = bytes_per_launch / (tot_ms / nl / 1e3) / 1e9
+    traffic = traffic_table().get(fam)
+    step_ideal_ms = WORDS_PER_CELL_STEP * 8 * ncell / (peak * 1e9) * 1e3
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ],
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"},
+            "max_div_u": maxdiv, "nonfinite": nonfinite,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": bytes_q,
+                    "d2h_bytes_per_step": bytes_q,
+                    "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1), "
+                            "q1,q2,q3 device->host; other state stays resident in the context"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "traffic": traffic,
+                         "step_frac": step_ideal_ms / (ms_max / args.steps)},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
+            "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, done, cores = cpu_reference(3, 20.0, q)
+        line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": "%d RK3 steps of the full workload (CPU FP64 restatement, "
+                                          "OpenMP, %d threads)" % (done, cores)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    run.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

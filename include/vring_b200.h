@@ -95,6 +95,10 @@ VR_API int vr_create(const vr_desc *desc, vr_ctx **out);
 VR_API int vr_destroy(vr_ctx *ctx);
 VR_API const char *vr_last_error(const vr_ctx *ctx);
 VR_API int vr_sync(vr_ctx *ctx);
+/* Queue the context's work on a caller's CUDA stream (cudaStream_t passed as
+ * void*; NULL returns to the context's own stream). */
+VR_API int vr_set_stream(vr_ctx *ctx, void *cuda_stream);
+VR_API int vr_get_stream(const vr_ctx *ctx, void **cuda_stream);
 
 /* ---- state transfer (host arrays in the Fortran layouts listed above) ----- */
 VR_API int vr_field_extents(const vr_ctx *ctx, int32_t field, int64_t ext[4]);
@@ -130,6 +134,14 @@ VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
 VR_API int vr_max_divergence(vr_ctx *ctx, double *out);
 /* number of non-finite values in q1..q3 and pres; VR_ERR_NONFINITE if any */
 VR_API int vr_check_finite(vr_ctx *ctx, int64_t *count);
+/* kernels launched by this context so far */
+VR_API int vr_launch_count(const vr_ctx *ctx, int64_t *n);
+/* per-kernel-family event timing on the context's stream: vr_profile(ctx, 1)
+ * starts recording (and clears), vr_profile_read sums one family:
+ * 0 hdnbc, 1 hdnl, 2 rhs, 3 theta sweep, 4 r sweep, 5 z sweep, 6 divq,
+ * 7 theta FFT, 8 z DCT, 9 radial Poisson solve, 10 upsol, 11 uppres, 12 diag */
+VR_API int vr_profile(vr_ctx *ctx, int32_t enable);
+VR_API int vr_profile_read(vr_ctx *ctx, int32_t kind, double *total_ms, int64_t *launches);
 
 /* ---- batched tridiagonal solvers (host arrays) --------------------------- */
 /* tripar.F90:120-145 / trithom.F90:6-29: nbatch independent systems of size n,

@@ -82,6 +82,11 @@ def lib():
         L.vr_iterate.argtypes = [vp, i32]
         L.vr_max_divergence.argtypes = [vp, C.POINTER(dp)]
         L.vr_check_finite.argtypes = [vp, C.POINTER(i64)]
+        L.vr_set_stream.argtypes = [vp, vp]
+        L.vr_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.vr_launch_count.argtypes = [vp, C.POINTER(i64)]
+        L.vr_profile.argtypes = [vp, i32]
+        L.vr_profile_read.argtypes = [vp, i32, C.POINTER(dp), C.POINTER(i64)]
         L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
         _lib = L
@@ -150,6 +155,43 @@ class Run:
         a = np.asfortranarray(np.broadcast_to(np.asarray(value, dtype=np.float64),
                                               shape if shape[3] > 1 else shape[:3]))
         self._chk(lib().vr_set_field(self._h, FIELD_ID[name], _p(a), ext), "set " + name)
+
+    def set_ptr(self, name: str, host_ptr: int) -> None:
+        """Copy a field from a raw host address (e.g. pinned memory)."""
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        self._chk(lib().vr_set_field(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext), "set " + name)
+
+    def get_ptr(self, name: str, host_ptr: int) -> None:
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        self._chk(lib().vr_get_field(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext), "get " + name)
+
+    def set_stream(self, cuda_stream_handle: int) -> None:
+        """Queue the context's work on a caller's CUDA stream (0: its own)."""
+        self._chk(lib().vr_set_stream(self._h, C.c_void_p(cuda_stream_handle or None)), "set_stream")
+
+    @property
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._chk(lib().vr_launch_count(self._h, C.byref(n)), "launch_count")
+        return n.value
+
+    PROFILE_KINDS = ["hdnbc", "hdnl", "rhs", "tsweep", "rsweep", "zsweep", "divq", "fft", "dct",
+                     "radial", "upsol", "uppres", "diag"]
+
+    def profile(self, enable: bool) -> None:
+        self._chk(lib().vr_profile(self._h, 1 if enable else 0), "profile")
+
+    def profile_read(self) -> dict:
+        """{family: (total_ms, launches)} of the kernels recorded since profile(True)."""
+        out = {}
+        for k, name in enumerate(self.PROFILE_KINDS):
+            t, n = C.c_double(), C.c_int64()
+            self._chk(lib().vr_profile_read(self._h, k, C.byref(t), C.byref(n)), "profile_read")
+            if n.value:
+                out[name] = (t.value, n.value)
+        return out
 
     def set_clock(self, irkstep: int, ntime: float, nstep: int = 0):
         self._chk(lib().vr_set_clock(self._h, irkstep, ntime, nstep), "set_clock")

@@ -20,6 +20,29 @@ int set_err(vr_ctx *c, int code, const std::string &msg) {
   return code;
 }
 
+LaunchScope::LaunchScope(vr_ctx *ctx, int kind) : c(ctx), slot(-1) {
+  c->nlaunch++;
+  if (!c->prof_on) return;
+  if (c->prof_used * 2 + 2 > c->prof_ev.size()) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+      cudaEventDestroy(a);
+      return;
+    }
+    c->prof_ev.push_back(a);
+    c->prof_ev.push_back(b);
+    c->prof_kind.push_back(kind);
+  }
+  slot = (int)c->prof_used++;
+  c->prof_kind[slot] = kind;
+  cudaEventRecord(c->prof_ev[2 * slot], c->stream);
+}
+
+LaunchScope::~LaunchScope() {
+  if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], c->stream);
+}
+
 // default-kind (real*4) literal of the reference, widened as gfortran does
 static inline double sp(float x) { return (double)x; }
 
@@ -281,7 +304,8 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
     return code;
   };
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
+  c->stream = c->own_stream;
   c->crkgam[1] = 8.0 / 15.0;
   c->crkgam[2] = 5.0 / 12.0;
   c->crkgam[3] = 3.0 / 4.0;
@@ -498,16 +522,62 @@ extern "C" int vr_destroy(vr_ctx *c) {
   for (double *p : ptrs)
     if (p) cudaFree(p);
   if (c->d_count) cudaFree(c->d_count);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   delete[] c->h_rc;
   delete[] c->h_rm;
   delete[] c->h_da;
   delete[] c->h_qc;
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return VR_OK;
 }
 
 extern "C" const char *vr_last_error(const vr_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" int vr_set_stream(vr_ctx *c, void *stream) {
+  if (!c) return VR_ERR_ARG;
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return VR_OK;
+}
+
+extern "C" int vr_get_stream(const vr_ctx *c, void **stream) {
+  if (!c || !stream) return VR_ERR_ARG;
+  *stream = (void *)c->stream;
+  return VR_OK;
+}
+
+extern "C" int vr_launch_count(const vr_ctx *c, int64_t *n) {
+  if (!c || !n) return VR_ERR_ARG;
+  *n = c->nlaunch;
+  return VR_OK;
+}
+
+extern "C" int vr_profile(vr_ctx *c, int32_t enable) {
+  if (!c) return VR_ERR_ARG;
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->prof_on = enable != 0;
+  c->prof_used = 0;
+  return VR_OK;
+}
+
+extern "C" int vr_profile_read(vr_ctx *c, int32_t kind, double *total_ms, int64_t *launches) {
+  if (!c || kind < 0 || kind >= vr::PK_N) return VR_ERR_ARG;
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  double t = 0.0;
+  int64_t n = 0;
+  for (size_t s = 0; s < c->prof_used; s++) {
+    if (c->prof_kind[s] != kind) continue;
+    float ms = 0.f;
+    VR_CUDA(c, cudaEventElapsedTime(&ms, c->prof_ev[2 * s], c->prof_ev[2 * s + 1]));
+    t += ms;
+    n++;
+  }
+  if (total_ms) *total_ms = t;
+  if (launches) *launches = n;
+  return VR_OK;
+}
 
 extern "C" int vr_sync(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;

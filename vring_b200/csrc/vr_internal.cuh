@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/vring_b200.h"
 
@@ -111,6 +112,13 @@ struct vr_ctx {
   // CUDA graphs for the fused substeps (one per irk), built lazily
   cudaGraphExec_t graph[4];
   bool graph_ok[4];
+  cudaStream_t own_stream;  // the context's stream; `stream` may be a caller's
+  // launch accounting and optional per-kernel event timing
+  int64_t nlaunch;
+  bool prof_on;
+  std::vector<cudaEvent_t> prof_ev;  // pairs (start, stop)
+  std::vector<int> prof_kind;
+  size_t prof_used;
   std::string err;
 };
 
@@ -130,6 +138,21 @@ int set_err(vr_ctx *c, int code, const std::string &msg);
     if (e_ != cudaSuccess)                                                          \
       return vr::set_err((c), VR_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
   } while (0)
+
+// kernel families for vr_profile_read
+enum ProfKind {
+  PK_HDNBC = 0, PK_HDNL, PK_RHS, PK_TSWEEP, PK_RSWEEP, PK_ZSWEEP, PK_DIVQ, PK_FFT, PK_DCT,
+  PK_RADIAL, PK_UPSOL, PK_UPPRES, PK_DIAG, PK_N
+};
+
+// Counts one kernel launch; with profiling on, brackets it with events on the
+// context's stream.
+struct LaunchScope {
+  vr_ctx *c;
+  int slot;
+  LaunchScope(vr_ctx *ctx, int kind);
+  ~LaunchScope();
+};
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);

@@ -54,6 +54,7 @@ __global__ void k_hdnbc(Geo g, Rk rk, double cs, double cor, const double *__res
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double cs, double cor) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nrc + 3) / 4);
+  LaunchScope ls(c, PK_HDNBC);
   k_hdnbc<<<gr, b, 0, c->stream>>>(g, rk, cs, cor, c->q[2], c->csort, c->tconv, c->corr3n, c->dq3no,
                                    c->corr3s);
   return cudaGetLastError();
@@ -155,6 +156,7 @@ __global__ void k_hdnl(Geo g, QV q, int comp, double *__restrict__ dq) {
 cudaError_t launch_hdnl(vr_ctx *c, int comp) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  LaunchScope ls(c, PK_HDNL);
   k_hdnl<<<gr, b, 0, c->stream>>>(g, QV{c->q[0], c->q[1], c->q[2]}, comp, c->dq[comp - 1]);
   return cudaGetLastError();
 }
@@ -246,6 +248,7 @@ cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h) {
   }
   a.prg = c->prg;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  LaunchScope ls(c, PK_RHS);
   if (inline_h)
     k_rhs<true><<<gr, b, 0, c->stream>>>(g, rk, a);
   else
@@ -375,6 +378,7 @@ cudaError_t launch_tsweep(vr_ctx *c, int comp) {
   int threads = 128;
   int blocks = (int)(((long long)nlines * 32 + threads - 1) / threads);
   const TriPer &t = c->ttri[c->irk][comp == 2 ? 1 : 0];
+  LaunchScope ls(c, PK_TSWEEP);
   k_tsweep<<<blocks, threads, 0, c->stream>>>(g, t, c->qrhs[comp - 1], jb, kb, nj, nlines);
   return cudaGetLastError();
 }
@@ -520,6 +524,7 @@ static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared
                                        (int)sm);
   if (e) return e;
   dim3 gr((s.nth + LT - 1) / LT, nm2);
+  LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
   k_linesweep<LT, CH><<<gr, LT * CH, sm, c->stream>>>(s, cf);
   return cudaGetLastError();
 }

@@ -327,6 +327,7 @@ static cudaError_t run_radial(vr_ctx *c) {
   size_t sm = sizeof(double) * ((size_t)g.nr * (LT + 1) + 2 * LT * CH);
   cudaError_t e = cudaFuncSetAttribute(k_radial<LT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
+  LaunchScope ls(c, PK_RADIAL);
   k_radial<LT, CH><<<dim3((g.nth + LT - 1) / LT, g.nz), LT * CH, sm, c->stream>>>(c->spec, g, c->pois_a, c->pois_c,
                                                                                 c->pois_ib);
   return cudaGetLastError();
@@ -338,6 +339,7 @@ static cudaError_t run_dct(vr_ctx *c, int dir) {
   size_t sm = sizeof(double) * 3 * LT * g.nz;
   cudaError_t e = cudaFuncSetAttribute(k_dct<LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
+  LaunchScope ls(c, PK_DCT);
   k_dct<LT><<<dim3((g.nth + LT - 1) / LT, g.nr), 256, sm, c->stream>>>(c->spec, g, ilog2(g.nz), dir, c->tw_z);
   return cudaGetLastError();
 }
@@ -351,9 +353,11 @@ cudaError_t launch_poisson(vr_ctx *c) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
     if ((e = cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    LaunchScope ls(c, PK_FFT);
     k_fft_fwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->rhs, c->spec, N, ilog2(N), lpb, nlines,
                                                                 c->tw_th);
   } else {
+    LaunchScope ls(c, PK_FFT);
     k_dft_fwd_direct<<<nlines, 64, 0, c->stream>>>(c->rhs, c->spec, N, nlines);
   }
   if ((e = cudaGetLastError())) return e;
@@ -361,6 +365,7 @@ cudaError_t launch_poisson(vr_ctx *c) {
   if (is_pow2(g.nz)) {
     if ((e = g.nz <= 1024 ? run_dct<8>(c, +1) : run_dct<4>(c, +1))) return e;
   } else {
+    LaunchScope ls(c, PK_DCT);
     k_dct_direct<<<dim3(N, g.nr), 64, sizeof(double) * g.nz, c->stream>>>(c->spec, g, +1);
   }
   if ((e = cudaGetLastError())) return e;
@@ -376,6 +381,7 @@ cudaError_t launch_poisson(vr_ctx *c) {
   if (is_pow2(g.nz)) {
     if ((e = g.nz <= 1024 ? run_dct<8>(c, -1) : run_dct<4>(c, -1))) return e;
   } else {
+    LaunchScope ls(c, PK_DCT);
     k_dct_direct<<<dim3(N, g.nr), 64, sizeof(double) * g.nz, c->stream>>>(c->spec, g, -1);
   }
   if ((e = cudaGetLastError())) return e;
@@ -384,8 +390,10 @@ cudaError_t launch_poisson(vr_ctx *c) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
     if ((e = cudaFuncSetAttribute(k_fft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    LaunchScope ls(c, PK_FFT);
     k_fft_bwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->spec, c->dph, g, ilog2(N), lpb, nlines, c->tw_th);
   } else {
+    LaunchScope ls(c, PK_FFT);
     k_dft_bwd_direct<<<nlines, 64, 0, c->stream>>>(c->spec, c->dph, g, nlines);
   }
   return cudaGetLastError();

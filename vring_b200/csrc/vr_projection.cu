@@ -35,6 +35,7 @@ __global__ void k_divq(Geo g, double inv_adt, const double *__restrict__ dq1, co
 cudaError_t launch_divq(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
+  LaunchScope ls(c, PK_DIVQ);
   k_divq<<<gr, b, 0, c->stream>>>(g, 1.0 / (rk.alm * g.dt), c->dq[0], c->dq[1], c->dq[2], c->rhs);
   return cudaGetLastError();
 }
@@ -85,6 +86,7 @@ __global__ void k_upsol(Geo g, double adt, const double *__restrict__ dq1, const
 cudaError_t launch_upsol(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nrc + 1 + 3) / 4, g.nzc);
+  LaunchScope ls(c, PK_UPSOL);
   k_upsol<<<gr, b, 0, c->stream>>>(g, rk.alm * g.dt, c->dq[0], c->dq[1], c->dq[2], c->dph, c->q[0], c->q[1],
                                    c->q[2], c->dph);
   return cudaGetLastError();
@@ -170,6 +172,7 @@ cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   double be = 0.5 * (rk.alm * g.dt) / g.re;
+  LaunchScope ls(c, PK_UPPRES);
   k_uppres<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
   return cudaGetLastError();
 }
@@ -203,6 +206,7 @@ __global__ void k_maxdiv(Geo g, const double *__restrict__ q1, const double *__r
 
 cudaError_t launch_maxdiv(vr_ctx *c, double *d_out) {
   const Geo &g = c->geo;
+  LaunchScope ls(c, PK_DIAG);
   k_zero<<<1, 1, 0, c->stream>>>(d_out, nullptr);
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   k_maxdiv<<<gr, b, 0, c->stream>>>(g, c->q[0], c->q[1], c->q[2], d_out);
@@ -220,6 +224,7 @@ __global__ void k_nonfinite(const double *__restrict__ a, size_t n, unsigned lon
 cudaError_t launch_count_nonfinite(vr_ctx *c, unsigned long long *d_out) {
   const Geo &g = c->geo;
   size_t n3 = (size_t)g.nth * g.J3 * g.K3;
+  LaunchScope ls(c, PK_DIAG);
   k_zero<<<1, 1, 0, c->stream>>>(nullptr, d_out);
   const double *f[4] = {c->q[0], c->q[1], c->q[2], c->pres};
   for (const double *p : f) k_nonfinite<<<4 * 148, 256, 0, c->stream>>>(p, n3, d_out);
