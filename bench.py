@@ -192,7 +192,9 @@ def main():
     run = V.Run(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, theta_wavenumber="modified", device=local)
     for n, a in zip(("q1", "q2", "q3"), q):
         run.set(n, a)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by the library and the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     run.set_stream(stream.cuda_stream)
     ncell = NTH * NR * NZ
 

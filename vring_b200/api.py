@@ -168,7 +168,9 @@ class Run:
         self._chk(lib().vr_get_field(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext), "get " + name)
 
     def set_stream(self, cuda_stream_handle: int) -> None:
-        """Queue the context's work on a caller's CUDA stream (0: its own)."""
+        """Queue the context's work on a caller's CUDA stream; 0 (which is also
+        the handle of the legacy default stream) selects the context's own
+        stream, so pass a created stream."""
         self._chk(lib().vr_set_stream(self._h, C.c_void_p(cuda_stream_handle or None)), "set_stream")
 
     @property
