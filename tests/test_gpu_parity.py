@@ -1,10 +1,11 @@
 """GPU parity: every routine of the RK3 core through the C ABI against the CPU
 restatement on the same seeded state.
 
-Grids cover the transform paths: power-of-two theta and z (radix-2 FFT and
-FFT-based DCT), odd theta (the reference's own case; direct DFT), even
-non-power-of-two theta (Nyquist slot, direct DFT) and non-power-of-two z
-(direct DCT).  Tolerance: FP64, max |gpu - oracle| <= 1e-12 x max |oracle| per
+Grids cover the transform paths: power-of-two theta and z below 32 (shared
+memory radix-2 FFT), from 32 up (warp-register FFT and DCT), odd theta (the
+reference's own case; direct DFT), even non-power-of-two theta (Nyquist slot,
+direct DFT) and non-power-of-two z (direct DCT); the last tests run the
+production transform sizes (theta 128, z 512) on a thin radial grid.  Tolerance: FP64, max |gpu - oracle| <= 1e-12 x max |oracle| per
 field (1e-11 where a near-singular Poisson mode amplifies round-off).
 """
 import numpy as np
@@ -14,7 +15,7 @@ from parity_util import STATE, assert_field_close, copy_to_gpu, make_pair, prep,
 
 pytestmark = pytest.mark.gpu
 
-GRIDS = [(16, 16, 32), (9, 12, 20), (12, 16, 24)]
+GRIDS = [(16, 16, 32), (9, 12, 20), (12, 16, 24), (32, 8, 64), (64, 12, 128)]
 
 
 @pytest.fixture(params=GRIDS, ids=lambda g: "x".join(map(str, g)))
@@ -176,3 +177,23 @@ def test_batched_thomas_and_block_thomas():
     for i in range(4):
         ref = O.solve_lap_bthom(rr[i], b1[i], b2[i], b3[i], m, nblk)
         np.testing.assert_allclose(xs[i], ref, rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("wth", ["exact", "modified"])
+def test_production_transform_sizes(wth):
+    grid = (128, 8, 512)
+    orc, gpu = _pair(grid, wth=wth)
+    seed_random(orc, gpu, ["rhs"], seed=60)
+    prep(orc, gpu)
+    orc.laplace_solve()
+    gpu.laplace_solve()
+    g = gpu.get("dph")[:, 1:9, 1:513]
+    r = orc.field("dph")[:, 1:9, 1:513]
+    assert np.abs(g - r).max() <= 1e-11 * np.abs(r).max()
+    orc, gpu = _pair(grid, wth=wth)
+    _ring_state(orc, gpu, grid)
+    prep(orc, gpu, 1, 5e-4, 0)
+    orc.substep(1)
+    gpu.substep(1)
+    for n in STATE + ["dph", "rhs"]:
+        assert_field_close(gpu, orc, n, rel=1e-11)

@@ -267,38 +267,52 @@ __device__ __forceinline__ Aff aff_then(const Aff &first, const Aff &second) {
   return Aff{second.M * first.M, second.C + second.M * first.C};
 }
 
-constexpr int kTMaxE = 32;  // elements per lane: ntheta <= 1025
+// One block = 8 warps = 8 lines (j, k..k+7) sharing row j's factorisation,
+// which is staged in shared memory once; each warp stages its line through a
+// padded shared buffer (coalesced global access, conflict-free chunk reads)
+// and solves it with the chunked affine scan: lane l owns the E contiguous
+// inner unknowns [l E, l E + E).
+__host__ __device__ __forceinline__ int tpad(int i) { return i + (i >> 4); }
 
-__global__ void k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nlines_j, int nlines) {
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= nlines) return;
-  int jc = jb + warp % nlines_j;
-  int kc = kb + warp / nlines_j;
+template <int E>
+__global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nk) {
+  extern __shared__ double sm[];
   const int N = g.nth;
-  double *line = f + I3(g, 1, jc, kc);
-  const double *inv = t.inv + (size_t)jc * N, *pp = t.pp + (size_t)jc * N, *zz = t.zz + (size_t)jc * N;
+  const int SPN = tpad(N) + 1;
+  double *cinv = sm, *cpp = sm + SPN, *czz = sm + 2 * SPN, *lines = sm + 3 * SPN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int jc = jb + blockIdx.y;
+  const int kc = kb + blockIdx.x * 8 + warp;
+  const bool active = kc < kb + nk;
+  for (int i = threadIdx.x; i < N; i += 256) {
+    cinv[tpad(i)] = __ldg(t.inv + (size_t)jc * N + i);
+    cpp[tpad(i)] = __ldg(t.pp + (size_t)jc * N + i);
+    czz[tpad(i)] = __ldg(t.zz + (size_t)jc * N + i);
+  }
+  double *sl = lines + (size_t)warp * SPN;
+  double *line = f + I3(g, 1, jc, active ? kc : kb);
+  if (active)
+    for (int i = lane; i < N; i += 32) sl[tpad(i)] = line[i];
+  __syncthreads();
+  if (!active) return;
   const double A = t.sub[jc];
   const int inner = N - 1;
-  const int E = (inner + 31) / 32;
-  const int i0 = lane * E;  // 0-based inner index of the first owned element
-  double y[kTMaxE];
+  const int i0 = lane * E;
   int cnt = inner - i0;
   cnt = cnt < 0 ? 0 : (cnt > E ? E : cnt);
+  double y[E];
   // forward: y_i = (f_i - A y_{i-1}) inv_i
   Aff fw{1.0, 0.0};
 #pragma unroll
-  for (int e = 0; e < kTMaxE; e++) {
+  for (int e = 0; e < E; e++) {
     if (e < cnt) {
-      int i = i0 + e;
-      double fi = line[i];
-      double iv = ld(inv + i);
+      int i = tpad(i0 + e);
+      double fi = sl[i], iv = cinv[i];
       y[e] = fi;
       fw.C = (fi - A * fw.C) * iv;
       fw.M = -A * iv * fw.M;
     }
   }
-  // inclusive scan of the chunk maps across lanes
   Aff acc = fw;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -307,24 +321,19 @@ __global__ void k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb
   }
   double yin = __shfl_up_sync(0xffffffffu, acc.C, 1);
   if (lane == 0) yin = 0.0;
-  {
-    double yp = yin;
 #pragma unroll
-    for (int e = 0; e < kTMaxE; e++) {
-      if (e < cnt) {
-        int i = i0 + e;
-        yp = (y[e] - A * yp) * ld(inv + i);
-        y[e] = yp;
-      }
+  for (int e = 0; e < E; e++) {
+    if (e < cnt) {
+      yin = (y[e] - A * yin) * cinv[tpad(i0 + e)];
+      y[e] = yin;
     }
   }
-  // backward: w_i = y_i - pp_i w_{i+1}, w beyond the inner range = 0
+  // backward: w_i = y_i - pp_i w_{i+1}
   Aff bw{1.0, 0.0};
 #pragma unroll
-  for (int e = kTMaxE - 1; e >= 0; e--) {
+  for (int e = E - 1; e >= 0; e--) {
     if (e < cnt) {
-      int i = i0 + e;
-      double p = ld(pp + i);
+      double p = cpp[tpad(i0 + e)];
       bw.C = y[e] - p * bw.C;
       bw.M = -p * bw.M;
     }
@@ -337,50 +346,56 @@ __global__ void k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb
   }
   double win = __shfl_down_sync(0xffffffffu, acc.C, 1);
   if (lane == 31) win = 0.0;
-  {
-    double wp = win;
 #pragma unroll
-    for (int e = kTMaxE - 1; e >= 0; e--) {
-      if (e < cnt) {
-        int i = i0 + e;
-        wp = y[e] - ld(pp + i) * wp;
-        y[e] = wp;
-      }
+  for (int e = E - 1; e >= 0; e--) {
+    if (e < cnt) {
+      win = y[e] - cpp[tpad(i0 + e)] * win;
+      y[e] = win;
     }
   }
   // bordering unknown N (step.F90:526-533)
-  int last_lane = (inner - 1) / E;
-  int last_e = (inner - 1) - last_lane * E;
+  const int last_lane = (inner - 1) / E, last_e = (inner - 1) - last_lane * E;
   double w1 = __shfl_sync(0xffffffffu, y[0], 0);
   double wl = 0.0;
 #pragma unroll
-  for (int e = 0; e < kTMaxE; e++)
+  for (int e = 0; e < E; e++)
     if (e == last_e) wl = y[e];
   wl = __shfl_sync(0xffffffffu, wl, last_lane);
-  double fN = line[N - 1];
-  double za1 = fN - t.sup[jc] * w1 - A * wl;
-  double xN = za1 / t.za2[jc];
+  const double fN = sl[tpad(N - 1)];
+  const double xN = (fN - t.sup[jc] * w1 - A * wl) / t.za2[jc];
+  __syncwarp();
 #pragma unroll
-  for (int e = 0; e < kTMaxE; e++) {
-    if (e < cnt) {
-      int i = i0 + e;
-      line[i] = y[e] + ld(zz + i) * xN;
-    }
-  }
-  if (lane == 0) line[N - 1] = xN;
+  for (int e = 0; e < E; e++)
+    if (e < cnt) sl[tpad(i0 + e)] = y[e] + czz[tpad(i0 + e)] * xN;
+  if (lane == 0) sl[tpad(N - 1)] = xN;
+  __syncwarp();
+  for (int i = lane; i < N; i += 32) line[i] = sl[tpad(i)];
+}
+
+template <int E>
+static cudaError_t run_tsweep(vr_ctx *c, const TriPer &t, double *f, int jb, int kb, int nj, int nk) {
+  const int SPN = tpad(c->geo.nth) + 1;
+  size_t sm = sizeof(double) * (size_t)SPN * (3 + 8);
+  cudaError_t e = cudaFuncSetAttribute(k_tsweep<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  LaunchScope ls(c, PK_TSWEEP);
+  k_tsweep<E><<<dim3((nk + 7) / 8, nj), 256, sm, c->stream>>>(c->geo, t, f, jb, kb, nk);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tsweep(vr_ctx *c, int comp) {
   const Geo &g = c->geo;
   int jb = comp == 2 ? 2 : 1, kb = comp == 3 ? 2 : 1;
   int nj = g.nr - jb + 1, nk = g.nz - kb + 1;
-  int nlines = nj * nk;
-  int threads = 128;
-  int blocks = (int)(((long long)nlines * 32 + threads - 1) / threads);
   const TriPer &t = c->ttri[c->irk][comp == 2 ? 1 : 0];
-  LaunchScope ls(c, PK_TSWEEP);
-  k_tsweep<<<blocks, threads, 0, c->stream>>>(g, t, c->qrhs[comp - 1], jb, kb, nj, nlines);
-  return cudaGetLastError();
+  double *f = c->qrhs[comp - 1];
+  int E = (g.nth - 1 + 31) / 32;
+  if (E <= 1) return run_tsweep<1>(c, t, f, jb, kb, nj, nk);
+  if (E <= 2) return run_tsweep<2>(c, t, f, jb, kb, nj, nk);
+  if (E <= 4) return run_tsweep<4>(c, t, f, jb, kb, nj, nk);
+  if (E <= 8) return run_tsweep<8>(c, t, f, jb, kb, nj, nk);
+  if (E <= 16) return run_tsweep<16>(c, t, f, jb, kb, nj, nk);
+  return run_tsweep<32>(c, t, f, jb, kb, nj, nk);
 }
 
 // ---------------------------------------------------------------------------

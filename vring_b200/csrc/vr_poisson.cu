@@ -12,6 +12,7 @@
 // tile and runs the two substitutions chunk-parallel (see vr_momentum.cu).
 #include <cuda_runtime.h>
 
+#include "vr_fft.cuh"
 #include "vr_internal.cuh"
 
 namespace vr {
@@ -153,6 +154,219 @@ __global__ void k_dft_bwd_direct(const double *__restrict__ in, double *__restri
         s += 2.0 * (fr * cs - fi * sn);
     }
     dph[IDP(g, n + 1, j, k)] = s;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// warp-register transforms (power-of-two lengths >= 32)
+// ---------------------------------------------------------------------------
+// theta forward: one warp per pair of lines (a, b) transformed as a + i b;
+// 8 warps per block; shared memory only for the bit-reversed reorder.
+template <int E>
+__global__ void __launch_bounds__(256) k_fft_fwd_w(const double *__restrict__ in, double *__restrict__ out,
+                                                   int nlines, const double *__restrict__ tw) {
+  constexpr int N = 32 * E, LOGN = Log2N<E>::v, SP = N + N / 32;
+  extern __shared__ double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *sre = sm + (size_t)warp * 2 * SP, *sim = sre + SP;
+  const int la = (blockIdx.x * 8 + warp) * 2;
+  if (la >= nlines) return;
+  const bool hasb = la + 1 < nlines;
+  const double *pa = in + (size_t)la * N, *pb = pa + N;
+  double re[E], im[E];
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    re[j] = pa[lane + 32 * j];
+    im[j] = hasb ? pb[lane + 32 * j] : 0.0;
+  }
+  warp_fft_dif<E>(re, im, tw, lane);
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    int k = spad(brev_n(lane + 32 * j, LOGN));
+    sre[k] = re[j];
+    sim[k] = im[j];
+  }
+  __syncwarp();
+  double *oa = out + (size_t)la * N, *ob = oa + N;
+  const double invn = 1.0 / N;
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    int s = lane + 32 * j;
+    double va, vb;
+    if (s == 0) {
+      va = sre[0] * invn;
+      vb = sim[0] * invn;
+    } else {
+      int k = (s + 1) >> 1, km = N - k;
+      double zr = sre[spad(k)], zi = sim[spad(k)], mr = sre[spad(km & (N - 1))], mi = sim[spad(km & (N - 1))];
+      if (s & 1) {  // 2 Re A_k / N, 2 Re B_k / N
+        va = (zr + mr) * invn;
+        vb = (zi + mi) * invn;
+      } else {  // -2 Im A_k / N, -2 Im B_k / N
+        va = -(zi - mi) * invn;
+        vb = (zr - mr) * invn;
+      }
+    }
+    oa[s] = va;
+    if (hasb) ob[s] = vb;
+  }
+}
+
+// theta inverse: packed lines -> values, written into dph rows
+template <int E>
+__global__ void __launch_bounds__(256) k_fft_bwd_w(const double *__restrict__ in, double *__restrict__ dph, Geo g,
+                                                   int nlines, const double *__restrict__ tw) {
+  constexpr int N = 32 * E, LOGN = Log2N<E>::v, SP = N + N / 32;
+  extern __shared__ double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *sa = sm + (size_t)warp * 2 * SP, *sb = sa + SP;
+  const int la = (blockIdx.x * 8 + warp) * 2;
+  if (la >= nlines) return;
+  const bool hasb = la + 1 < nlines;
+  const double *pa = in + (size_t)la * N, *pb = pa + N;
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    sa[lane + 32 * j] = pa[lane + 32 * j];
+    sb[lane + 32 * j] = hasb ? pb[lane + 32 * j] : 0.0;
+  }
+  __syncwarp();
+  // Z_k = A_k + i B_k with the Hermitian spectra of the two packed lines
+  double re[E], im[E];
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    int k = lane + 32 * j;
+    int kk = k <= N / 2 ? k : N - k;
+    double ar, ai, br, bi;
+    if (kk == 0) {
+      ar = sa[0];
+      ai = 0.0;
+      br = sb[0];
+      bi = 0.0;
+    } else {
+      ar = sa[2 * kk - 1] / 2.0;
+      br = sb[2 * kk - 1] / 2.0;
+      ai = (2 * kk < N) ? -1.0 * sa[2 * kk] / 2.0 : 0.0;
+      bi = (2 * kk < N) ? -1.0 * sb[2 * kk] / 2.0 : 0.0;
+      if (k > N / 2) {
+        ai = -ai;
+        bi = -bi;
+      }
+    }
+    re[j] = ar - bi;      // Re Z
+    im[j] = -(ai + br);   // -Im Z: inverse transform as conj(DFT(conj Z))
+  }
+  warp_fft_dif<E>(re, im, tw, lane);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    int m = spad(brev_n(lane + 32 * j, LOGN));
+    sa[m] = re[j];
+    sb[m] = -im[j];
+  }
+  __syncwarp();
+  const int ja = 1 + la % g.nr, ka = 1 + la / g.nr;
+  double *da = dph + IDP(g, 1, ja, ka);
+  double *db = nullptr;
+  if (hasb) {
+    int lb = la + 1;
+    db = dph + IDP(g, 1, 1 + lb % g.nr, 1 + lb / g.nr);
+  }
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    int n = lane + 32 * j;
+    da[n] = sa[spad(n)];
+    if (hasb) db[n] = sb[spad(n)];
+  }
+}
+
+// z transforms: a CTA stages LT columns (consecutive theta, fixed r) x nz in
+// shared memory with 128-byte row loads; warp w transforms columns 2w, 2w+1
+// as one complex sequence (Makhoul's even/odd reordering turns the DCT into
+// an N-point FFT plus a quarter-wave shift).
+template <int E, int LT>
+__global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g, int dir,
+                                                   const double *__restrict__ twz) {
+  constexpr int N = 32 * E, LOGN = Log2N<E>::v, LD = LT + 1;
+  extern __shared__ double tile[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i0 = blockIdx.x * LT, j = blockIdx.y;  // j 0-based radial index
+  const int nl = min(LT, g.nth - i0);
+  const size_t s2 = (size_t)g.nth * g.nr;
+  double *base = a + i0 + (size_t)g.nth * j;
+  for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
+    int k = idx / LT, l = idx % LT;
+    tile[k * LD + l] = l < nl ? base[l + s2 * k] : 0.0;
+  }
+  __syncthreads();
+  const double *shift = twz + 2 * N;  // cos, sin (pi k / (2N))
+  const int ca = 2 * warp, cb = ca + 1;
+  double re[E], im[E];
+  if (dir > 0) {
+    // z_n = v^a_n + i v^b_n, v_n = x_{2n} (n < N/2), v_{N-1-n} = x_{2n+1}
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int n = lane + 32 * q;
+      int src = n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1;
+      re[q] = tile[src * LD + ca];
+      im[q] = tile[src * LD + cb];
+    }
+    __syncwarp();
+    warp_fft_dif<E>(re, im, twz, lane);
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int k = brev_n(lane + 32 * q, LOGN);
+      tile[k * LD + ca] = re[q];
+      tile[k * LD + cb] = im[q];
+    }
+    __syncwarp();
+    // y_k = 2 Re(e^{-i pi k/(2N)} V_k) / (2N)
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int k = lane + 32 * q, km = (N - k) & (N - 1);
+      double zr = tile[k * LD + ca], zi = tile[k * LD + cb];
+      double mr = tile[km * LD + ca], mi = tile[km * LD + cb];
+      double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);  // V^a = (Z_k + conj Z_{N-k}) / 2
+      double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);  // V^b = -i (Z_k - conj Z_{N-k}) / 2
+      double c = __ldg(shift + 2 * k), s = __ldg(shift + 2 * k + 1);
+      re[q] = 2.0 * (var_ * c + vai * s) / (2.0 * N * 1);
+      im[q] = 2.0 * (vbr * c + vbi * s) / (2.0 * N * 1);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int k = lane + 32 * q;
+      tile[k * LD + ca] = re[q];
+      tile[k * LD + cb] = im[q];
+    }
+  } else {
+    // W_k = V^a_k + i V^b_k, V_k = e^{i pi k/(2N)} (X_k - i X_{N-k}) / 2
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int k = lane + 32 * q;
+      double c = __ldg(shift + 2 * k), s = __ldg(shift + 2 * k + 1);
+      double xa = tile[k * LD + ca] / 2.0, xb = tile[k * LD + cb] / 2.0;
+      double ya = k == 0 ? 0.0 : -tile[(N - k) * LD + ca] / 2.0, yb = k == 0 ? 0.0 : -tile[(N - k) * LD + cb] / 2.0;
+      double var_ = xa * c - ya * s, vai = xa * s + ya * c;
+      double vbr = xb * c - yb * s, vbi = xb * s + yb * c;
+      re[q] = var_ - vbi;     // Re W
+      im[q] = -(vai + vbr);   // -Im W (inverse as conj(DFT(conj W)))
+    }
+    __syncwarp();
+    warp_fft_dif<E>(re, im, twz, lane);
+    // slot of point n holds conj(w_m), m = brev(n); w_m = v^a_m + i v^b_m
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      int m = brev_n(lane + 32 * q, LOGN);
+      int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+      tile[o * LD + ca] = 2.0 * re[q];
+      tile[o * LD + cb] = -2.0 * im[q];
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
+    int k = idx / LT, l = idx % LT;
+    if (l < nl) base[l + s2 * k] = tile[k * LD + l];
   }
 }
 
@@ -344,12 +558,72 @@ static cudaError_t run_dct(vr_ctx *c, int dir) {
   return cudaGetLastError();
 }
 
+template <int E>
+static cudaError_t run_fft_w(vr_ctx *c, int dir) {
+  const Geo &g = c->geo;
+  constexpr int N = 32 * E, SP = N + N / 32;
+  const int nlines = g.nr * g.nz;
+  size_t sm = sizeof(double) * 8 * 2 * SP;
+  int blocks = (nlines + 15) / 16;
+  cudaError_t e;
+  LaunchScope ls(c, PK_FFT);
+  if (dir > 0) {
+    if ((e = cudaFuncSetAttribute(k_fft_fwd_w<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_fwd_w<E><<<blocks, 256, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th);
+  } else {
+    if ((e = cudaFuncSetAttribute(k_fft_bwd_w<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_bwd_w<E><<<blocks, 256, sm, c->stream>>>(c->spec, c->dph, g, nlines, c->tw_th);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t fft_warp_dispatch(vr_ctx *c, int dir, bool *done) {
+  *done = true;
+  switch (c->geo.nth) {
+    case 32: return run_fft_w<1>(c, dir);
+    case 64: return run_fft_w<2>(c, dir);
+    case 128: return run_fft_w<4>(c, dir);
+    case 256: return run_fft_w<8>(c, dir);
+    case 512: return run_fft_w<16>(c, dir);
+    case 1024: return run_fft_w<32>(c, dir);
+    default: *done = false; return cudaSuccess;
+  }
+}
+
+template <int E, int LT>
+static cudaError_t run_dct_w(vr_ctx *c, int dir) {
+  const Geo &g = c->geo;
+  constexpr int N = 32 * E;
+  size_t sm = sizeof(double) * (size_t)N * (LT + 1);
+  cudaError_t e = cudaFuncSetAttribute(k_dct_w<E, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  LaunchScope ls(c, PK_DCT);
+  k_dct_w<E, LT><<<dim3((g.nth + LT - 1) / LT, g.nr), LT * 16, sm, c->stream>>>(c->spec, g, dir, c->tw_z);
+  return cudaGetLastError();
+}
+
+static cudaError_t dct_warp_dispatch(vr_ctx *c, int dir, bool *done) {
+  *done = true;
+  switch (c->geo.nz) {
+    case 32: return run_dct_w<1, 16>(c, dir);
+    case 64: return run_dct_w<2, 16>(c, dir);
+    case 128: return run_dct_w<4, 16>(c, dir);
+    case 256: return run_dct_w<8, 16>(c, dir);
+    case 512: return run_dct_w<16, 16>(c, dir);
+    case 1024: return run_dct_w<32, 8>(c, dir);
+    default: *done = false; return cudaSuccess;
+  }
+}
+
 cudaError_t launch_poisson(vr_ctx *c) {
   const Geo &g = c->geo;
   cudaError_t e;
   const int N = g.nth, nlines = g.nr * g.nz;
   // theta forward: rhs -> spec
-  if (is_pow2(N)) {
+  bool done = false;
+  if ((e = fft_warp_dispatch(c, +1, &done))) return e;
+  if (done) {
+  } else if (is_pow2(N)) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
     if ((e = cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
@@ -362,7 +636,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
   }
   if ((e = cudaGetLastError())) return e;
   // z forward DCT
-  if (is_pow2(g.nz)) {
+  if ((e = dct_warp_dispatch(c, +1, &done))) return e;
+  if (done) {
+  } else if (is_pow2(g.nz)) {
     if ((e = g.nz <= 1024 ? run_dct<8>(c, +1) : run_dct<4>(c, +1))) return e;
   } else {
     LaunchScope ls(c, PK_DCT);
@@ -378,7 +654,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
     e = run_radial<4, 64>(c);
   if (e) return e;
   // z backward
-  if (is_pow2(g.nz)) {
+  if ((e = dct_warp_dispatch(c, -1, &done))) return e;
+  if (done) {
+  } else if (is_pow2(g.nz)) {
     if ((e = g.nz <= 1024 ? run_dct<8>(c, -1) : run_dct<4>(c, -1))) return e;
   } else {
     LaunchScope ls(c, PK_DCT);
@@ -386,7 +664,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
   }
   if ((e = cudaGetLastError())) return e;
   // theta backward -> dph
-  if (is_pow2(N)) {
+  if ((e = fft_warp_dispatch(c, -1, &done))) return e;
+  if (done) {
+  } else if (is_pow2(N)) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
     if ((e = cudaFuncSetAttribute(k_fft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
