@@ -227,27 +227,32 @@ def main():
 
     # ---- end to end: per step, velocity in from pinned host memory, one step
     # through the C ABI, velocity back to pinned host memory ------------------
-    pins = [torch.empty(int(torch.tensor(a.shape).prod()), dtype=torch.float64, pin_memory=True)
-            for a in q]
-    for p, a in zip(pins, q):
-        p.numpy()[:] = a.ravel(order="F")
-    run.set_stream(0)
-    for p, n in zip(pins, ("q1", "q2", "q3")):  # warm the copy path once
-        run.set_ptr(n, p.data_ptr())
-    run.iterate(1)
-    run.sync()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        for p, n in zip(pins, ("q1", "q2", "q3")):
+    e2e = None
+    if args.e2e_steps > 0:
+        pins = [torch.empty(int(torch.tensor(a.shape).prod()), dtype=torch.float64, pin_memory=True)
+                for a in q]
+        for p, a in zip(pins, q):
+            p.numpy()[:] = a.ravel(order="F")
+        run.set_stream(0)
+        for p, n in zip(pins, ("q1", "q2", "q3")):  # warm the copy path once
             run.set_ptr(n, p.data_ptr())
         run.iterate(1)
-        for p, n in zip(pins, ("q1", "q2", "q3")):
-            run.get_ptr(n, p.data_ptr())
-    run.sync()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    bytes_q = sum(p.numel() for p in pins) * 8
-    e2e_val = world * ncell * args.e2e_steps / e2e_s / 1e6
+        run.sync()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            for p, n in zip(pins, ("q1", "q2", "q3")):
+                run.set_ptr(n, p.data_ptr())
+            run.iterate(1)
+            for p, n in zip(pins, ("q1", "q2", "q3")):
+                run.get_ptr(n, p.data_ptr())
+        run.sync()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        bytes_q = sum(p.numel() for p in pins) * 8
+        e2e = {"value": world * ncell * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": bytes_q, "d2h_bytes_per_step": bytes_q,
+               "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1), "
+                       "q1,q2,q3 device->host; other state stays resident in the context"}
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
@@ -266,10 +271,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"},
             "max_div_u": maxdiv, "nonfinite": nonfinite,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": bytes_q,
-                    "d2h_bytes_per_step": bytes_q,
-                    "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1), "
-                            "q1,q2,q3 device->host; other state stays resident in the context"},
+            "e2e": e2e,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
