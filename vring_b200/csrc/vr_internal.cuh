@@ -51,6 +51,16 @@ __host__ __device__ inline int IDP(const Geo &g, int i, int j, int k) {
 __host__ __device__ inline int I2O(const Geo &g, int i, int j) { return (i - 1) + g.nth * (j - 1); }
 __host__ __device__ inline int I2Z(const Geo &g, int i, int j) { return (i - 1) + g.nth * j; }
 
+// asynchronous 8-byte global -> shared copies (cp.async, sm_80+): a CTA puts
+// a whole tile in flight before waiting once
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // RK3 coefficients of one substep (para_tools.F90:103-113)
 struct Rk {
   double gam, rom, alm;

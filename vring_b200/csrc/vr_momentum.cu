@@ -176,19 +176,22 @@ struct RhsArgs {
 };
 
 template <bool INLINE_H>
-__global__ void k_rhs(Geo g, Rk rk, RhsArgs a) {
+__global__ void __launch_bounds__(128) k_rhs(Geo g, Rk rk, RhsArgs a) {
   int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   int kc = 1 + blockIdx.z;
   if (ic > g.nth || jc > g.nr) return;
   int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
   int jm = jc > 1 ? jc - 1 : 1;
-  const double *q1 = a.q.q1, *q2 = a.q.q2, *q3 = a.q.q3;
-  int o = I3(g, ic, jc, kc);
-  double are = rk.alm / g.re;
-  // ---- q1 (step.F90:32-63)
-  {
-    double h = INLINE_H ? h1_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[0] + o);
+  const double *__restrict__ q1 = a.q.q1, *__restrict__ q2 = a.q.q2, *__restrict__ q3 = a.q.q3;
+  const int o = I3(g, ic, jc, kc);
+  const double are = rk.alm / g.re;
+  const bool do3 = kc >= 2, do2 = jc >= 2;
+  // every load and every result first; the six stores come last so the
+  // compiler can keep all loads in flight together
+  double h1, h2 = 0.0, h3 = 0.0, r1, r2 = 0.0, r3 = 0.0;
+  {  // q1 (step.F90:32-63)
+    h1 = INLINE_H ? h1_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[0] + o);
     double qc = ld(q1 + o);
     double d11 = (ld(q1 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q1 + I3(g, im, jc, kc))) * g.s1t11[jc];
     double d33;
@@ -199,28 +202,22 @@ __global__ void k_rhs(Geo g, Rk rk, RhsArgs a) {
     double qnn = (ld(q1 + I3(g, ic, jc + 1, kc)) * g.irm[jc + 1] - qc * g.irm[jc]) * g.s1t2n[jc];
     double qss = (qc * g.irm[jc] - ld(q1 + I3(g, ic, jm, kc)) * g.irm[jm]) * g.s1t2s[jc];
     double d22 = (qnn - qss) * g.s1t2c[jc];
-    double r = ld(a.ru[0] + o);
-    a.qrhs[0][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 1)) +
-                    are * (d11 + d33 + d22)) * g.dt;
-    a.ru[0][o] = h;
+    r1 = (rk.gam * h1 + rk.rom * ld(a.ru[0] + o) - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 1)) +
+          are * (d11 + d33 + d22)) * g.dt;
   }
-  // ---- q3 (step.F90:93-116), k >= 2
-  if (kc >= 2) {
-    double h = INLINE_H ? h3_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[2] + o);
+  if (do3) {  // q3 (step.F90:93-116), k >= 2
+    h3 = INLINE_H ? h3_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[2] + o);
     double qc = ld(q3 + o);
     double d11 = (ld(q3 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q3 + I3(g, im, jc, kc))) * g.s1t11[jc];
     double d33 = (ld(q3 + I3(g, ic, jc, kc + 1)) - 2.0 * qc + ld(q3 + I3(g, ic, jc, kc - 1))) * g.dx3q;
     double qnn = (ld(q3 + I3(g, ic, jc + 1, kc)) - qc) * g.s3t2n[jc];
     double qss = (qc - ld(q3 + I3(g, ic, jm, kc))) * g.s3t2s[jc];
     double d22 = qnn - qss;
-    double r = ld(a.ru[2] + o);
-    a.qrhs[2][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 3)) +
-                    are * (d11 + d33 + d22)) * g.dt;
-    a.ru[2][o] = h;
+    r3 = (rk.gam * h3 + rk.rom * ld(a.ru[2] + o) - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 3)) +
+          are * (d11 + d33 + d22)) * g.dt;
   }
-  // ---- q2 (step.F90:144-165), j >= 2
-  if (jc >= 2) {
-    double h = INLINE_H ? h2_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[1] + o);
+  if (do2) {  // q2 (step.F90:144-165), j >= 2
+    h2 = INLINE_H ? h2_at(g, a.q, ic, ip, im, jc, kc) : ld(a.dqh[1] + o);
     double qc = ld(q2 + o);
     double d11 = (ld(q2 + I3(g, ip, jc, kc)) - 2.0 * qc + ld(q2 + I3(g, im, jc, kc))) * g.s2t11[jc];
     double d33;
@@ -230,10 +227,18 @@ __global__ void k_rhs(Geo g, Rk rk, RhsArgs a) {
       d33 = (ld(q2 + I3(g, ic, jc, kc + 1)) - 2.0 * qc + ld(q2 + I3(g, ic, jc, kc - 1))) * g.dx3q;
     double d22 = ld(q2 + I3(g, ic, jc + 1, kc)) * g.s2t2p[jc] - qc * g.s2t2c[jc] +
                  ld(q2 + I3(g, ic, jc - 1, kc)) * g.s2t2m[jc];
-    double r = ld(a.ru[1] + o);
-    a.qrhs[1][o] = (rk.gam * h + rk.rom * r - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 2)) +
-                    are * (d11 + d33 + d22)) * g.dt;
-    a.ru[1][o] = h;
+    r2 = (rk.gam * h2 + rk.rom * ld(a.ru[1] + o) - rk.alm * ld(a.prg + IPRG(g, ic, jc, kc, 2)) +
+          are * (d11 + d33 + d22)) * g.dt;
+  }
+  a.qrhs[0][o] = r1;
+  a.ru[0][o] = h1;
+  if (do3) {
+    a.qrhs[2][o] = r3;
+    a.ru[2][o] = h3;
+  }
+  if (do2) {
+    a.qrhs[1][o] = r2;
+    a.ru[1][o] = h2;
   }
 }
 
@@ -285,14 +290,15 @@ __global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restr
   const int kc = kb + blockIdx.x * 8 + warp;
   const bool active = kc < kb + nk;
   for (int i = threadIdx.x; i < N; i += 256) {
-    cinv[tpad(i)] = __ldg(t.inv + (size_t)jc * N + i);
-    cpp[tpad(i)] = __ldg(t.pp + (size_t)jc * N + i);
-    czz[tpad(i)] = __ldg(t.zz + (size_t)jc * N + i);
+    cp_async8(cinv + tpad(i), t.inv + (size_t)jc * N + i);
+    cp_async8(cpp + tpad(i), t.pp + (size_t)jc * N + i);
+    cp_async8(czz + tpad(i), t.zz + (size_t)jc * N + i);
   }
   double *sl = lines + (size_t)warp * SPN;
   double *line = f + I3(g, 1, jc, active ? kc : kb);
   if (active)
-    for (int i = lane; i < N; i += 32) sl[tpad(i)] = line[i];
+    for (int i = lane; i < N; i += 32) cp_async8(sl + tpad(i), line + i);
+  cp_async_wait_all();
   __syncthreads();
   if (!active) return;
   const double A = t.sub[jc];
@@ -501,16 +507,20 @@ __global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgs s, CoefShared cf
   const int m2 = s.m2_0 + blockIdx.y;
   const int nthreads = LT * CH;
   const int nl = min(LT, s.nth - i0);
-  // load rows
+  // load rows: every element of the tile in flight at once (cp.async)
   for (int idx = threadIdx.x; idx < s.n * LT; idx += nthreads) {
     int e = idx / LT, l = idx % LT;
-    double v = 0.0;
-    if (l < nl) {
-      v = s.in[(i0 + l) + s.s2 * m2 + s.se * (s.e0 + e)];
-      if (e == 0 && s.bc_lo_on) v = s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
-      if (e == s.n - 1 && s.bc_hi_on) v = s.bc_hi ? s.bc_hi[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
-    }
-    tile[e * LD + l] = v;
+    if (l < nl)
+      cp_async8(tile + e * LD + l, s.in + ((i0 + l) + s.s2 * m2 + s.se * (s.e0 + e)));
+    else
+      tile[e * LD + l] = 0.0;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (threadIdx.x < nl) {  // boundary right-hand sides replace rows 0 / n-1
+    int l = threadIdx.x;
+    if (s.bc_lo_on) tile[l] = s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
+    if (s.bc_hi_on) tile[(s.n - 1) * LD + l] = s.bc_hi ? s.bc_hi[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
   }
   __syncthreads();
   tile_solve<LT, CH>(tile, LD, s.n, cf, sM, sC);

@@ -296,8 +296,12 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
   double *base = a + i0 + (size_t)g.nth * j;
   for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
     int k = idx / LT, l = idx % LT;
-    tile[k * LD + l] = l < nl ? base[l + s2 * k] : 0.0;
+    if (l < nl)
+      cp_async8(tile + k * LD + l, base + l + s2 * k);
+    else
+      tile[k * LD + l] = 0.0;
   }
+  cp_async_wait_all();
   __syncthreads();
   const double *shift = twz + 2 * N;  // cos, sin (pi k / (2N))
   const int ca = 2 * warp, cb = ca + 1;
@@ -525,8 +529,12 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
   const size_t base = (size_t)g.nth * g.nr * kz;
   for (int idx = threadIdx.x; idx < n * LT; idx += LT * CH) {
     int e = idx / LT, l = idx % LT;
-    tile[e * LD + l] = l < nl ? a[base + (i0 + l) + (size_t)g.nth * e] : 0.0;
+    if (l < nl)
+      cp_async8(tile + e * LD + l, a + base + (i0 + l) + (size_t)g.nth * e);
+    else
+      tile[e * LD + l] = 0.0;
   }
+  cp_async_wait_all();
   __syncthreads();
   tile_solve_pois<LT, CH>(tile, LD, n, pa, pc, pib + (size_t)kz * n * nm, nm, i0, sM, sC);
   for (int idx = threadIdx.x; idx < n * LT; idx += LT * CH) {
