@@ -20,6 +20,7 @@
 // on the host (vr_ctx.cu) and the kernels only run the two substitutions.
 #include <cuda_runtime.h>
 
+#include "vr_chunk.cuh"
 #include "vr_internal.cuh"
 
 namespace vr {
@@ -554,8 +555,50 @@ static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared
   return cudaGetLastError();
 }
 
-// tile width by line length so the tile fits the 227 KB of shared memory
+// Line policy of k_chunk for the momentum sweeps (same addressing and boundary
+// rules as k_linesweep).
+struct MomLine {
+  SweepArgs s;
+  const double *a, *c, *ib;
+  int n, i0, m2;
+  __device__ void begin_block() {
+    i0 = blockIdx.x * 32;
+    m2 = s.m2_0 + blockIdx.y;
+  }
+  __device__ bool line_active(int l) const { return i0 + l < s.nth; }
+  __device__ double load(int l, int e) const {
+    if (e == 0 && s.bc_lo_on) return s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
+    if (e == n - 1 && s.bc_hi_on) return s.bc_hi ? s.bc_hi[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
+    return s.in[(i0 + l) + s.s2 * m2 + s.se * (s.e0 + e)];
+  }
+  __device__ double A(int, int e) const { return __ldg(a + e); }
+  __device__ double Cc(int, int e) const { return __ldg(c + e); }
+  __device__ double IB(int, int e) const { return __ldg(ib + e); }
+  __device__ void store(int l, int e, double x) const {
+    int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
+    double v = s.add ? s.add[o] + x : x;
+    s.out[o] = v;
+    if (s.mode == 1 && m2 == s.nr) s.out[o + s.nth] = s.slip * v;
+    if (s.mode == 2) {
+      if (e == 0) s.out[o - s.se] = s.add[o - s.se] + 0.0;
+      if (e == n - 1) s.out[o + s.se] = 0.0 * s.slip * v;
+    }
+  }
+};
+
+// register-resident chunked sweep up to 544 unknowns per line, else a
+// shared-memory tile sized to fit the 227 KB of shared memory
 static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared &cf, int nm2) {
+  if (chunk_bucket(s.n)) {
+    MomLine p;
+    p.s = s;
+    p.a = cf.a;
+    p.c = cf.c;
+    p.ib = cf.ib;
+    p.n = s.n;
+    LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
+    return launch_chunk(p, dim3((s.nth + 31) / 32, nm2), c->stream);
+  }
   if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
   if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);
   return run_linesweep<4, 64>(c, s, cf, nm2);

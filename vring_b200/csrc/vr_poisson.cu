@@ -12,6 +12,7 @@
 // tile and runs the two substitutions chunk-parallel (see vr_momentum.cu).
 #include <cuda_runtime.h>
 
+#include "vr_chunk.cuh"
 #include "vr_fft.cuh"
 #include "vr_internal.cuh"
 
@@ -543,6 +544,26 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
   }
 }
 
+// Line policy of k_chunk for the radial solves: lines (slot, kz) along j with
+// the factorisation of mode m = slot/2 (poisson_solve.F90:164-167).
+struct PoisLine {
+  double *a;
+  const double *pa, *pc, *pib;
+  int n, nth, nm, i0, kz;
+  __device__ void begin_block() {
+    i0 = blockIdx.x * 32;
+    kz = blockIdx.y;
+  }
+  __device__ bool line_active(int l) const { return i0 + l < nth; }
+  __device__ int mm(int l) const { return min((i0 + l + 1) / 2, nm - 1); }
+  __device__ size_t off(int l, int e) const { return (size_t)nth * n * kz + (i0 + l) + (size_t)nth * e; }
+  __device__ double load(int l, int e) const { return a[off(l, e)]; }
+  __device__ double A(int, int e) const { return __ldg(pa + e); }
+  __device__ double Cc(int, int e) const { return __ldg(pc + e); }
+  __device__ double IB(int l, int e) const { return __ldg(pib + ((size_t)kz * n + e) * nm + mm(l)); }
+  __device__ void store(int l, int e, double x) const { a[off(l, e)] = x; }
+};
+
 template <int LT, int CH>
 static cudaError_t run_radial(vr_ctx *c) {
   const Geo &g = c->geo;
@@ -654,7 +675,18 @@ cudaError_t launch_poisson(vr_ctx *c) {
   }
   if ((e = cudaGetLastError())) return e;
   // radial solves
-  if (g.nr <= 640)
+  if (chunk_bucket(g.nr)) {
+    PoisLine p;
+    p.a = c->spec;
+    p.pa = c->pois_a;
+    p.pc = c->pois_c;
+    p.pib = c->pois_ib;
+    p.n = g.nr;
+    p.nth = g.nth;
+    p.nm = g.nth / 2 + 1;
+    LaunchScope ls(c, PK_RADIAL);
+    if ((e = launch_chunk(p, dim3((N + 31) / 32, g.nz), c->stream))) return e;
+  } else if (g.nr <= 640)
     e = run_radial<16, 16>(c);
   else if (g.nr <= 1600)
     e = run_radial<8, 32>(c);
