@@ -304,6 +304,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
     return code;
   };
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
   c->stream = c->own_stream;
   c->crkgam[1] = 8.0 / 15.0;

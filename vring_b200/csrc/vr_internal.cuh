@@ -94,6 +94,7 @@ struct HostCoef;  // ucoeff/coesys vectors in double, host side
 struct vr_ctx {
   vr_desc d;
   int dev;
+  int nsm;  // streaming multiprocessors of the device
   cudaStream_t stream;
   vr::Geo geo;
   // clock

@@ -289,6 +289,9 @@ template <int E, int LT>
 __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g, int dir,
                                                    const double *__restrict__ twz) {
   constexpr int N = 32 * E, LOGN = Log2N<E>::v, LD = LT + 1;
+  // row k of the tile starts at k*LD + k/16: the bit-reversed scatter of the
+  // FFT output then spreads over the banks
+  auto row = [](int k) { return k * LD + (k >> 4); };
   extern __shared__ double tile[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i0 = blockIdx.x * LT, j = blockIdx.y;  // j 0-based radial index
@@ -298,9 +301,9 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
   for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
     int k = idx / LT, l = idx % LT;
     if (l < nl)
-      cp_async8(tile + k * LD + l, base + l + s2 * k);
+      cp_async8(tile + row(k) + l, base + l + s2 * k);
     else
-      tile[k * LD + l] = 0.0;
+      tile[row(k) + l] = 0.0;
   }
   cp_async_wait_all();
   __syncthreads();
@@ -313,24 +316,24 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     for (int q = 0; q < E; q++) {
       int n = lane + 32 * q;
       int src = n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1;
-      re[q] = tile[src * LD + ca];
-      im[q] = tile[src * LD + cb];
+      re[q] = tile[row(src) + ca];
+      im[q] = tile[row(src) + cb];
     }
     __syncwarp();
     warp_fft_dif<E>(re, im, twz, lane);
 #pragma unroll
     for (int q = 0; q < E; q++) {
       int k = brev_n(lane + 32 * q, LOGN);
-      tile[k * LD + ca] = re[q];
-      tile[k * LD + cb] = im[q];
+      tile[row(k) + ca] = re[q];
+      tile[row(k) + cb] = im[q];
     }
     __syncwarp();
     // y_k = 2 Re(e^{-i pi k/(2N)} V_k) / (2N)
 #pragma unroll
     for (int q = 0; q < E; q++) {
       int k = lane + 32 * q, km = (N - k) & (N - 1);
-      double zr = tile[k * LD + ca], zi = tile[k * LD + cb];
-      double mr = tile[km * LD + ca], mi = tile[km * LD + cb];
+      double zr = tile[row(k) + ca], zi = tile[row(k) + cb];
+      double mr = tile[row(km) + ca], mi = tile[row(km) + cb];
       double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);  // V^a = (Z_k + conj Z_{N-k}) / 2
       double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);  // V^b = -i (Z_k - conj Z_{N-k}) / 2
       double c = __ldg(shift + 2 * k), s = __ldg(shift + 2 * k + 1);
@@ -341,8 +344,8 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
 #pragma unroll
     for (int q = 0; q < E; q++) {
       int k = lane + 32 * q;
-      tile[k * LD + ca] = re[q];
-      tile[k * LD + cb] = im[q];
+      tile[row(k) + ca] = re[q];
+      tile[row(k) + cb] = im[q];
     }
   } else {
     // W_k = V^a_k + i V^b_k, V_k = e^{i pi k/(2N)} (X_k - i X_{N-k}) / 2
@@ -350,8 +353,8 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     for (int q = 0; q < E; q++) {
       int k = lane + 32 * q;
       double c = __ldg(shift + 2 * k), s = __ldg(shift + 2 * k + 1);
-      double xa = tile[k * LD + ca] / 2.0, xb = tile[k * LD + cb] / 2.0;
-      double ya = k == 0 ? 0.0 : -tile[(N - k) * LD + ca] / 2.0, yb = k == 0 ? 0.0 : -tile[(N - k) * LD + cb] / 2.0;
+      double xa = tile[row(k) + ca] / 2.0, xb = tile[row(k) + cb] / 2.0;
+      double ya = k == 0 ? 0.0 : -tile[row((N - k)) + ca] / 2.0, yb = k == 0 ? 0.0 : -tile[row((N - k)) + cb] / 2.0;
       double var_ = xa * c - ya * s, vai = xa * s + ya * c;
       double vbr = xb * c - yb * s, vbi = xb * s + yb * c;
       re[q] = var_ - vbi;     // Re W
@@ -364,14 +367,14 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     for (int q = 0; q < E; q++) {
       int m = brev_n(lane + 32 * q, LOGN);
       int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
-      tile[o * LD + ca] = 2.0 * re[q];
-      tile[o * LD + cb] = -2.0 * im[q];
+      tile[row(o) + ca] = 2.0 * re[q];
+      tile[row(o) + cb] = -2.0 * im[q];
     }
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
     int k = idx / LT, l = idx % LT;
-    if (l < nl) base[l + s2 * k] = tile[k * LD + l];
+    if (l < nl) base[l + s2 * k] = tile[row(k) + l];
   }
 }
 
@@ -549,15 +552,16 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
 struct PoisLine {
   double *a;
   const double *pa, *pc, *pib;
-  int n, nth, nm, i0, kz;
-  __device__ void begin_block() {
-    i0 = blockIdx.x * 32;
-    kz = blockIdx.y;
+  int n, nth, nm, nbx, i0, kz;
+  __device__ void set_tile(int tile) {
+    i0 = (tile % nbx) * 32;
+    kz = tile / nbx;
   }
   __device__ bool line_active(int l) const { return i0 + l < nth; }
   __device__ int mm(int l) const { return min((i0 + l + 1) / 2, nm - 1); }
   __device__ size_t off(int l, int e) const { return (size_t)nth * n * kz + (i0 + l) + (size_t)nth * e; }
-  __device__ double load(int l, int e) const { return a[off(l, e)]; }
+  __device__ const double *gptr(int l, int e) const { return a + off(l, e); }
+  __device__ double fix(int, int, double v) const { return v; }
   __device__ double A(int, int e) const { return __ldg(pa + e); }
   __device__ double Cc(int, int e) const { return __ldg(pc + e); }
   __device__ double IB(int l, int e) const { return __ldg(pib + ((size_t)kz * n + e) * nm + mm(l)); }
@@ -623,7 +627,7 @@ template <int E, int LT>
 static cudaError_t run_dct_w(vr_ctx *c, int dir) {
   const Geo &g = c->geo;
   constexpr int N = 32 * E;
-  size_t sm = sizeof(double) * (size_t)N * (LT + 1);
+  size_t sm = sizeof(double) * ((size_t)N * (LT + 1) + N / 16 + 1);
   cudaError_t e = cudaFuncSetAttribute(k_dct_w<E, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   LaunchScope ls(c, PK_DCT);
@@ -684,8 +688,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
     p.n = g.nr;
     p.nth = g.nth;
     p.nm = g.nth / 2 + 1;
+    p.nbx = (N + 31) / 32;
     LaunchScope ls(c, PK_RADIAL);
-    if ((e = launch_chunk(p, dim3((N + 31) / 32, g.nz), c->stream))) return e;
+    if ((e = launch_chunk(p, p.nbx * g.nz, c->nsm, c->stream))) return e;
   } else if (g.nr <= 640)
     e = run_radial<16, 16>(c);
   else if (g.nr <= 1600)
