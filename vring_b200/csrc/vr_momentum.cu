@@ -6,12 +6,14 @@
 // neighbour rows in r and z come from L1/L2.
 //
 // Sweeps:
-//  * theta (tripij, periodic): one thread per (r, z) line; a block stages its
-//    lines and the row's factorisation in shared memory (cp.async) and every
-//    thread runs the reference's sequential recurrences on its line.
+//  * theta (tripij, periodic): one warp per (r, z) line, 8 lines of one r row
+//    per block sharing the row's factorisation in shared memory; each lane
+//    owns a contiguous chunk of the line, the two first-order recurrences of
+//    the factorised solve are composed per chunk and chained with a warp
+//    shuffle scan.
 //  * r and z (solqj / solqk): k_chunk (vr_chunk.cuh) keeps 32 neighbouring
-//    lines x 32 chunks in registers, pipelined over tiles; lines longer than
-//    544 unknowns use a shared-memory tile with the same chunk composition.
+//    lines x 32 chunks in registers; lines longer than 544 unknowns use a
+//    shared-memory tile with the same chunk composition.
 // The matrices are identical for every line of a family (they depend on the
 // substep and on r or z only), so their Thomas factorisation is computed once
 // on the host (vr_ctx.cu) and the kernels only run the two substitutions.
@@ -262,68 +264,128 @@ cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h) {
 // ---------------------------------------------------------------------------
 // theta sweep (solqi + tripij, step.F90:212-263, 487-534), warp per line
 // ---------------------------------------------------------------------------
-// One thread per line: a block takes LPB lines (j, k..k+LPB-1) that share
-// row j's factorisation.  The rows and the lines stream into shared memory
-// with cp.async (each line is nth contiguous values), every thread runs the
-// reference's sequential recurrences on its own line (row stride nth+1 keeps
-// the 32 lines of a warp on distinct banks), and the tile is written back
-// with coalesced stores.
-template <int LPB>
-__global__ void __launch_bounds__(LPB) k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nk) {
-  extern __shared__ double sm[];
-  const int N = g.nth, LD = N + 1;
-  double *cinv = sm, *cpp = cinv + N, *czz = cpp + N, *tile = czz + N;
-  const int jc = jb + blockIdx.y;
-  const int k0 = kb + blockIdx.x * LPB;
-  const int nl = min(LPB, kb + nk - k0);
-  const int tid = threadIdx.x;
-  for (int i = tid; i < N; i += LPB) {
-    cp_async8(cinv + i, t.inv + (size_t)jc * N + i);
-    cp_async8(cpp + i, t.pp + (size_t)jc * N + i);
-    cp_async8(czz + i, t.zz + (size_t)jc * N + i);
-  }
-  for (int idx = tid; idx < nl * N; idx += LPB) {
-    int l = idx / N, i = idx - l * N;
-    cp_async8(tile + l * LD + i, f + I3(g, 1 + i, jc, k0 + l));
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  if (tid < nl) {
-    double *x = tile + tid * LD;
-    const double A = t.sub[jc];
-    // forward over the inner unknowns 1..N-1 (step.F90:497-513)
-    double y = x[0] * cinv[0];
-    x[0] = y;
-    for (int i = 1; i <= N - 2; i++) {
-      y = (x[i] - A * y) * cinv[i];
-      x[i] = y;
-    }
-    // backward (step.F90:516-525)
-    double w = x[N - 2];
-    for (int i = N - 3; i >= 0; i--) {
-      w = x[i] - cpp[i] * w;
-      x[i] = w;
-    }
-    // bordering unknown N (step.F90:526-533)
-    const double xN = (x[N - 1] - t.sup[jc] * x[0] - A * x[N - 2]) / t.za2[jc];
-    for (int i = 0; i <= N - 2; i++) x[i] = x[i] + czz[i] * xN;
-    x[N - 1] = xN;
-  }
-  __syncthreads();
-  for (int idx = tid; idx < nl * N; idx += LPB) {
-    int l = idx / N, i = idx - l * N;
-    f[I3(g, 1 + i, jc, k0 + l)] = tile[l * LD + i];
-  }
+// Affine map y_out = C + M * y_in, composed left-to-right along the line.
+struct Aff {
+  double M, C;
+};
+__device__ __forceinline__ Aff aff_then(const Aff &first, const Aff &second) {
+  return Aff{second.M * first.M, second.C + second.M * first.C};
 }
 
-template <int LPB>
+// One block = 8 warps = 8 lines (j, k..k+7) sharing row j's factorisation,
+// which is staged in shared memory once; each warp stages its line through a
+// padded shared buffer (coalesced global access, conflict-free chunk reads)
+// and solves it with the chunked affine scan: lane l owns the E contiguous
+// inner unknowns [l E, l E + E).
+__host__ __device__ __forceinline__ int tpad(int i) { return i + (i >> 4); }
+
+template <int E>
+__global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nk) {
+  extern __shared__ double sm[];
+  const int N = g.nth;
+  const int SPN = tpad(N) + 1;
+  double *cinv = sm, *cpp = sm + SPN, *czz = sm + 2 * SPN, *lines = sm + 3 * SPN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int jc = jb + blockIdx.y;
+  const int kc = kb + blockIdx.x * 8 + warp;
+  const bool active = kc < kb + nk;
+  for (int i = threadIdx.x; i < N; i += 256) {
+    cp_async8(cinv + tpad(i), t.inv + (size_t)jc * N + i);
+    cp_async8(cpp + tpad(i), t.pp + (size_t)jc * N + i);
+    cp_async8(czz + tpad(i), t.zz + (size_t)jc * N + i);
+  }
+  double *sl = lines + (size_t)warp * SPN;
+  double *line = f + I3(g, 1, jc, active ? kc : kb);
+  if (active)
+    for (int i = lane; i < N; i += 32) cp_async8(sl + tpad(i), line + i);
+  cp_async_wait_all();
+  __syncthreads();
+  if (!active) return;
+  const double A = t.sub[jc];
+  const int inner = N - 1;
+  const int i0 = lane * E;
+  int cnt = inner - i0;
+  cnt = cnt < 0 ? 0 : (cnt > E ? E : cnt);
+  double y[E];
+  // forward: y_i = (f_i - A y_{i-1}) inv_i
+  Aff fw{1.0, 0.0};
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if (e < cnt) {
+      int i = tpad(i0 + e);
+      double fi = sl[i], iv = cinv[i];
+      y[e] = fi;
+      fw.C = (fi - A * fw.C) * iv;
+      fw.M = -A * iv * fw.M;
+    }
+  }
+  Aff acc = fw;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    Aff o{__shfl_up_sync(0xffffffffu, acc.M, d), __shfl_up_sync(0xffffffffu, acc.C, d)};
+    if (lane >= d) acc = aff_then(o, acc);
+  }
+  double yin = __shfl_up_sync(0xffffffffu, acc.C, 1);
+  if (lane == 0) yin = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if (e < cnt) {
+      yin = (y[e] - A * yin) * cinv[tpad(i0 + e)];
+      y[e] = yin;
+    }
+  }
+  // backward: w_i = y_i - pp_i w_{i+1}
+  Aff bw{1.0, 0.0};
+#pragma unroll
+  for (int e = E - 1; e >= 0; e--) {
+    if (e < cnt) {
+      double p = cpp[tpad(i0 + e)];
+      bw.C = y[e] - p * bw.C;
+      bw.M = -p * bw.M;
+    }
+  }
+  acc = bw;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    Aff o{__shfl_down_sync(0xffffffffu, acc.M, d), __shfl_down_sync(0xffffffffu, acc.C, d)};
+    if (lane + d < 32) acc = aff_then(o, acc);
+  }
+  double win = __shfl_down_sync(0xffffffffu, acc.C, 1);
+  if (lane == 31) win = 0.0;
+#pragma unroll
+  for (int e = E - 1; e >= 0; e--) {
+    if (e < cnt) {
+      win = y[e] - cpp[tpad(i0 + e)] * win;
+      y[e] = win;
+    }
+  }
+  // bordering unknown N (step.F90:526-533)
+  const int last_lane = (inner - 1) / E, last_e = (inner - 1) - last_lane * E;
+  double w1 = __shfl_sync(0xffffffffu, y[0], 0);
+  double wl = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; e++)
+    if (e == last_e) wl = y[e];
+  wl = __shfl_sync(0xffffffffu, wl, last_lane);
+  const double fN = sl[tpad(N - 1)];
+  const double xN = (fN - t.sup[jc] * w1 - A * wl) / t.za2[jc];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < E; e++)
+    if (e < cnt) sl[tpad(i0 + e)] = y[e] + czz[tpad(i0 + e)] * xN;
+  if (lane == 0) sl[tpad(N - 1)] = xN;
+  __syncwarp();
+  for (int i = lane; i < N; i += 32) line[i] = sl[tpad(i)];
+}
+
+template <int E>
 static cudaError_t run_tsweep(vr_ctx *c, const TriPer &t, double *f, int jb, int kb, int nj, int nk) {
-  const int N = c->geo.nth;
-  size_t sm = sizeof(double) * ((size_t)3 * N + (size_t)LPB * (N + 1));
-  cudaError_t e = cudaFuncSetAttribute(k_tsweep<LPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const int SPN = tpad(c->geo.nth) + 1;
+  size_t sm = sizeof(double) * (size_t)SPN * (3 + 8);
+  cudaError_t e = cudaFuncSetAttribute(k_tsweep<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   LaunchScope ls(c, PK_TSWEEP);
-  k_tsweep<LPB><<<dim3((nk + LPB - 1) / LPB, nj), LPB, sm, c->stream>>>(c->geo, t, f, jb, kb, nk);
+  k_tsweep<E><<<dim3((nk + 7) / 8, nj), 256, sm, c->stream>>>(c->geo, t, f, jb, kb, nk);
   return cudaGetLastError();
 }
 
@@ -333,9 +395,13 @@ cudaError_t launch_tsweep(vr_ctx *c, int comp) {
   int nj = g.nr - jb + 1, nk = g.nz - kb + 1;
   const TriPer &t = c->ttri[c->irk][comp == 2 ? 1 : 0];
   double *f = c->qrhs[comp - 1];
-  if (g.nth <= 192) return run_tsweep<64>(c, t, f, jb, kb, nj, nk);
-  if (g.nth <= 640) return run_tsweep<32>(c, t, f, jb, kb, nj, nk);
-  return run_tsweep<16>(c, t, f, jb, kb, nj, nk);
+  int E = (g.nth - 1 + 31) / 32;
+  if (E <= 1) return run_tsweep<1>(c, t, f, jb, kb, nj, nk);
+  if (E <= 2) return run_tsweep<2>(c, t, f, jb, kb, nj, nk);
+  if (E <= 4) return run_tsweep<4>(c, t, f, jb, kb, nj, nk);
+  if (E <= 8) return run_tsweep<8>(c, t, f, jb, kb, nj, nk);
+  if (E <= 16) return run_tsweep<16>(c, t, f, jb, kb, nj, nk);
+  return run_tsweep<32>(c, t, f, jb, kb, nj, nk);
 }
 
 // ---------------------------------------------------------------------------
@@ -533,7 +599,7 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgs &s, const CoefS
     p.n = s.n;
     p.nbx = (s.nth + 31) / 32;
     LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
-    return launch_chunk(p, p.nbx * nm2, c->nsm, c->stream);
+    return launch_chunk(p, p.nbx * nm2, c->stream);
   }
   if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
   if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);

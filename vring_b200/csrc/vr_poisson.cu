@@ -690,7 +690,7 @@ cudaError_t launch_poisson(vr_ctx *c) {
     p.nm = g.nth / 2 + 1;
     p.nbx = (N + 31) / 32;
     LaunchScope ls(c, PK_RADIAL);
-    if ((e = launch_chunk(p, p.nbx * g.nz, c->nsm, c->stream))) return e;
+    if ((e = launch_chunk(p, p.nbx * g.nz, c->stream))) return e;
   } else if (g.nr <= 640)
     e = run_radial<16, 16>(c);
   else if (g.nr <= 1600)
