@@ -124,9 +124,9 @@ VR_API int vr_uppres(vr_ctx *ctx);        /* divergence.F90:239-480             
 /* ---- fused paths --------------------------------------------------------- */
 /* One RK substep irk (loop.F90:63-130 without particles), fused kernels. */
 VR_API int vr_substep(vr_ctx *ctx, int32_t irk);
-/* nsteps time steps (loop.F90:47-130): ntime += dt, substeps 1..3, as one CUDA
- * graph per substep replayed; particle classes attached with vr_part_attach
- * advance at substep 1 (loop.F90:66-68). */
+/* nsteps time steps (loop.F90:47-130): ntime += dt, substeps 1..3, all
+ * kernels enqueued on the context's stream; particle classes attached with
+ * vr_part_attach advance before substep 1 (loop.F90:65-68). */
 VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
 
 /* ---- diagnostics --------------------------------------------------------- */
@@ -139,9 +139,52 @@ VR_API int vr_launch_count(const vr_ctx *ctx, int64_t *n);
 /* per-kernel-family event timing on the context's stream: vr_profile(ctx, 1)
  * starts recording (and clears), vr_profile_read sums one family:
  * 0 hdnbc, 1 hdnl, 2 rhs, 3 theta sweep, 4 r sweep, 5 z sweep, 6 divq,
- * 7 theta FFT, 8 z DCT, 9 radial Poisson solve, 10 upsol, 11 uppres, 12 diag */
+ * 7 theta FFT, 8 z DCT, 9 radial Poisson solve, 10 upsol, 11 uppres, 12 diag,
+ * 13 particles */
 VR_API int vr_profile(vr_ctx *ctx, int32_t enable);
 VR_API int vr_profile_read(vr_ctx *ctx, int32_t kind, double *total_ms, int64_t *launches);
+
+/* ---- Lagrangian particles (part_tools.F90) ------------------------------- */
+/* One particle class (type part): state u(naloc, 117) and v(naloc, 3) stored
+ * column-major on the device exactly as the reference declares them, the free
+ * list isfre(naloc)/ifree, and the counters npart, nlast, nfree, nids.
+ * u: 1-3 position, 4-6 velocity, 7-15 Jacobian, 16-24 its rate, 25-51
+ * Hessian, 52-78 its rate, 79-81 fluid velocity, 82-90 its gradient, 91-117
+ * its second derivatives at the particle; v: 1 time, 2 concentration, 3 id.
+ * Classes must be destroyed before their context (vr_destroy returns
+ * VR_ERR_STATE while any exists). */
+typedef struct vr_part vr_part;
+/* init_part (part_tools.F90:228-359): class id 1..8 sets the radius, the
+ * Stokes number and nsubdt; mode 0 inertial particles, 1 tracers */
+VR_API int vr_part_create(vr_ctx *ctx, int32_t id, int32_t naloc, int32_t mode, vr_part **out);
+VR_API int vr_part_destroy(vr_part *part);
+/* radius, Stokes number, concentration scale and Euler substeps per step */
+VR_API int vr_part_info(const vr_part *part, double *radius, double *stokes, double *conc,
+                        int32_t *nsubdt);
+/* injc_part (part_tools.F90:144-197); the slot used (1-based) in *ip;
+ * VR_ERR_CAPACITY when all naloc slots are taken */
+VR_API int vr_injc_part(vr_part *part, double x, double y, double z, double c, double u, double v,
+                        double w, int32_t icall, int32_t *ip);
+/* remv_part (part_tools.F90:199-225), ip 1-based */
+VR_API int vr_remv_part(vr_part *part, int32_t ip);
+/* iter_part (part_tools.F90:374-1164) on one rank: nsubdt explicit Euler
+ * substeps of dt/nsubdt in the context's current velocity field; particles
+ * that leave 0 <= z <= zmax, r <= rmax are removed. Enqueued on the
+ * context's stream; the free list is brought up to date by the next call
+ * that reads or changes it. */
+VR_API int vr_iter_part(vr_part *part, int32_t irkstep);
+/* on != 0: vr_iterate advances this class once per time step */
+VR_API int vr_part_attach(vr_part *part, int32_t on);
+/* whole-class state in the reference's layout; isfre may be NULL (all live);
+ * slots nlast+1..naloc are ignored */
+VR_API int vr_part_set_state(vr_part *part, const double *u, const double *v, const int32_t *isfre,
+                             int32_t nlast);
+/* any pointer may be NULL; counts = {npart, nlast, nfree, nids} */
+VR_API int vr_part_get_state(vr_part *part, double *u, double *v, int32_t *isfre, int32_t counts[4]);
+/* interpolated fluid velocity, gradient and Hessian (Cartesian components,
+ * part_tools.F90:521-797) at n points xyz[3n]; out[39n] per point: u_i,
+ * du_i/dx_j at 3+i+3j, d2u_i/dx_j dx_k at 12+i+3j+9k; cells[3n] = (it, ir, iz) */
+VR_API int vr_part_probe(vr_part *part, const double *xyz, int32_t n, double *out, int32_t *cells);
 
 /* ---- batched tridiagonal solvers (host arrays) --------------------------- */
 /* tripar.F90:120-145 / trithom.F90:6-29: nbatch independent systems of size n,

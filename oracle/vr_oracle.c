@@ -1741,6 +1741,14 @@ static void part_eval(orc_ctx *c, orc_part *p, double x, double y, double z, dou
     if (c->nth == 1) it = 1;
     int ir = (int)floor(r / c->dr) + 1;
     int iz = (int)floor(z / c->dz) + 1;
+    /* mesh lookups stay inside the stored vectors for points off the mesh
+     * (a no-op for 0 <= r <= rmax, 0 <= z <= zmax) */
+    if (!(it >= 1)) it = 1;
+    if (it > c->nth + 1) it = c->nth + 1;
+    if (ir < 0) ir = 0;
+    if (ir > c->nr + 2) ir = c->nr + 2;
+    if (iz < 0) iz = 0;
+    if (iz > c->nz + 1) iz = c->nz + 1;
     for (int f3 = -1; f3 <= 1; f3++)
       for (int f2 = -1; f2 <= 1; f2++)
         for (int f1 = -1; f1 <= 1; f1++) {

@@ -1,0 +1,198 @@
+"""GPU particles (part_tools.F90) against the oracle, through the C ABI.
+
+- the reference's dertest known answers (u_theta = 0, u_r = r^2, u_z = 1 on
+  the dertest r-z mesh) interpolated by the CUDA kernel;
+- interpolation/transform at random points of a vortex-ring field: cell
+  indices bit-exact, values to 1e-12;
+- iter_part (inertial and tracer classes) over several calls, with particles
+  leaving the domain: state arrays, free list and counters;
+- injc_part / remv_part slot bookkeeping;
+- particles attached to vr_iterate, advanced before substep 1 of every step.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests.parity_util import make_pair
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "dertest_kat.npz")
+
+
+def _ring(orc, gpu, nth, nr, nz, seed=0):
+    from vring_b200.synthetic import ring_fields
+    q1, q2, q3 = ring_fields(nth, nr, nz, 4.0, 12.0, noise=1e-3, seed=seed)
+    for n, a in (("q1", q1), ("q2", q2), ("q3", q3)):
+        orc.field(n)[...] = a
+        gpu.set(n, a)
+
+
+def test_dertest_kat_on_gpu():
+    """The dertest dumps (8 significant digits) through the CUDA kernel. The
+    dumps come from an axisymmetric run (ntheta = 1); the field is independent
+    of theta, so the same answers hold on an 8-cell theta mesh."""
+    import vring_b200 as V
+    g = np.load(GOLD)
+    _, nr, nz, rmax, zmax = g["mesh"]
+    run = V.Run(8, int(nr), int(nz), float(rmax), float(zmax), 1e-3, 1000.0)
+    ext = run.extents("q2")
+    dr = float(rmax) / int(nr)
+    rc = (np.arange(ext[1]) - 1.0) * dr
+    q2 = np.broadcast_to((rc ** 3)[None, :, None], ext[:3])
+    run.set("q1", 0.0)
+    run.set("q2", q2)
+    run.set("q3", 1.0)
+    p = V.Part(run, 1, 4, 0)
+    vel, dvel, dd, _ = p.probe(g["pos"])
+    got = np.concatenate([vel, dvel.reshape(-1, 9, order="F"), dd[:, 0].reshape(-1, 9, order="F"),
+                          dd[:, 1].reshape(-1, 9, order="F"), dd[:, 2].reshape(-1, 9, order="F")], 1)
+    ref = np.concatenate([g["vel"], g["dvel"], g["ddvel1"], g["ddvel2"], g["ddvel3"]], 1)
+    np.testing.assert_allclose(got, ref, rtol=2e-7, atol=2e-13)
+    p.close()
+
+
+@pytest.mark.parametrize("grid", [(16, 16, 32), (12, 24, 40)])
+def test_probe_matches_oracle(grid):
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = grid
+    orc, gpu = make_pair(nth, nr, nz)
+    _ring(orc, gpu, nth, nr, nz, seed=3)
+    op = O.OraclePart(orc, 3, 8, 0)
+    gp = V.Part(gpu, 3, 8, 0)
+    rng = np.random.default_rng(7)
+    n = 600
+    r = rng.uniform(0.02, 3.98, n)
+    th = rng.uniform(0, 2 * np.pi, n)
+    z = rng.uniform(0.01, 11.99, n)
+    xyz = np.stack([r * np.cos(th), r * np.sin(th), z], 1)
+    # points on cell faces and the theta = 0 / pi seams
+    dr, dz = 4.0 / nr, 12.0 / nz
+    extra = np.array([[dr * 5, 0.0, dz * 7], [-dr * 3, 0.0, dz * 2], [0.0, dr * 4, dz * 3],
+                      [0.0, -dr * 4, dz * 3], [dr * 2, -1e-13, 6.0], [1e-3, 1e-3, 0.5]])
+    xyz = np.concatenate([xyz, extra])
+    vel, dvel, dd, cells = gp.probe(xyz)
+    for i, pt in enumerate(xyz):
+        idx, _ = op.cell(*pt)
+        assert tuple(cells[i]) == tuple(idx), (i, pt, cells[i], idx)
+        ref = op.probe(*pt)
+        got = np.concatenate([vel[i], dvel[i].reshape(-1, order="F"), dd[i].reshape(-1, order="F")])
+        scale = max(np.abs(ref).max(), 1e-30)
+        err = np.abs(got - ref).max()
+        assert err <= 1e-12 * scale, (i, pt, err / scale)
+    gp.close()
+
+
+def _inject_cloud(ps, n, seed, out_frac=0.1):
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.3, 3.6, n)
+    th = rng.uniform(0, 2 * np.pi, n)
+    z = rng.uniform(0.5, 11.5, n)
+    w = rng.uniform(-0.5, 0.5, n)
+    nout = int(out_frac * n)
+    z[:nout] = 11.97          # inertial: these leave through z = zmax within a step
+    w[:nout] = 40.0
+    r[nout:2 * nout] = 4.0005  # start just beyond r = rmax: removed after one substep
+    slots = []
+    for i in range(n):
+        s = [p.injc(r[i] * np.cos(th[i]), r[i] * np.sin(th[i]), z[i], 0.1, -0.1, w[i]) for p in ps]
+        assert s[0] == s[1]
+        slots.append(s[0])
+    return slots
+
+
+def _compare_parts(op, gp, rel=1e-11):
+    u, v, isf, cnt = gp.state()
+    assert cnt == {"npart": op.npart, "nlast": op.nlast, "nfree": op.nfree, "nids": op.nids}
+    ou, ov = op.u, op.v
+    assert np.array_equal(isf[:op.nlast] != 0, op.isfre[1:op.nlast + 1] != 0)
+    scale = np.maximum(np.abs(ou).max(axis=0), 1e-30)
+    err = (np.abs(u - ou) / scale).max()
+    assert err <= rel, err
+    np.testing.assert_array_equal(v, ov)
+
+
+@pytest.mark.parametrize("pid,mode", [(4, 0), (8, 0), (6, 1)])
+def test_iter_part_matches_oracle(pid, mode):
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = 16, 32, 64
+    orc, gpu = make_pair(nth, nr, nz, dt=1e-3)
+    _ring(orc, gpu, nth, nr, nz, seed=5)
+    naloc = 700
+    op = O.OraclePart(orc, pid, naloc, mode)
+    gp = V.Part(gpu, pid, naloc, mode)
+    assert (gp.nsubdt, gp.st, gp.r, gp.c) == (op.nsubdt, op.st, op.r, op.c)
+    _inject_cloud([op, gp], 600, seed=pid)
+    for call in range(3):
+        op.iter_part(1)
+        gp.iter_part(1)
+        _compare_parts(op, gp)
+    assert op.npart < 600          # the fast particles left through z = zmax
+    # refill freed slots after removals
+    _inject_cloud([op, gp], 50, seed=11, out_frac=0.0)
+    op.iter_part(1)
+    gp.iter_part(1)
+    _compare_parts(op, gp)
+    gp.close()
+
+
+def test_inject_remove_bookkeeping():
+    from oracle import oracle as O
+    import vring_b200 as V
+    orc, gpu = make_pair(8, 16, 32)
+    op = O.OraclePart(orc, 2, 12, 0)
+    gp = V.Part(gpu, 2, 12, 0)
+    seq = [("i", 1.0), ("i", 1.1), ("i", 1.2), ("i", 1.3), ("r", 2), ("r", 4), ("i", 1.4),
+           ("r", 1), ("i", 1.5), ("i", 1.6), ("r", 3), ("r", 2), ("i", 1.7), ("i", 1.8)]
+    for op_, a in seq:
+        if op_ == "i":
+            s0 = op.injc(a, 0.5, 2.0, 0.1, 0.2, 0.3, icall=1)
+            s1 = gp.injc(a, 0.5, 2.0, 0.1, 0.2, 0.3, icall=1)
+            assert s0 == s1
+        else:
+            op.remv(a)
+            gp.remv(a)
+        _compare_parts(op, gp, rel=0.0)
+    # capacity: the GPU refuses the slot past naloc
+    while gp.counts["nlast"] < 12 or gp.counts["nfree"] > 0:
+        gp.injc(1.0, 1.0, 1.0)
+    with pytest.raises(V.VrError) as e:
+        gp.injc(1.0, 1.0, 1.0)
+    assert e.value.code == 9
+    gp.close()
+
+
+def test_iterate_with_attached_particles():
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = 16, 32, 64
+    orc, gpu = make_pair(nth, nr, nz, dt=1e-3, wth="modified")
+    _ring(orc, gpu, nth, nr, nz, seed=9)
+    op = O.OraclePart(orc, 5, 300, 0)
+    gp = V.Part(gpu, 5, 300, 0)
+    _inject_cloud([op, gp], 250, seed=2)
+    gp.attach(True)
+    gpu.iterate(3)
+    for _ in range(3):      # loop.F90:65-68: iter_part, then the three substeps
+        op.iter_part(1)
+        orc.iterate(1)
+    _compare_parts(op, gp, rel=1e-10)
+    for n in ("q1", "q2", "q3"):
+        g, r = gpu.get(n), orc.field(n)
+        assert np.abs(g - r).max() <= 1e-10 * np.abs(r).max()
+    gp.attach(False)
+    gp.close()
+
+
+def test_context_refuses_destroy_with_live_particles():
+    import vring_b200 as V
+    from vring_b200.api import lib
+    run = V.Run(8, 16, 32, 4.0, 12.0, 1e-3, 1000.0)
+    p = V.Part(run, 1, 4, 0)
+    assert lib().vr_destroy(run._h) == 7
+    p.close()
+    run.close()
+    assert not run._h

@@ -87,6 +87,16 @@ def lib():
         L.vr_launch_count.argtypes = [vp, C.POINTER(i64)]
         L.vr_profile.argtypes = [vp, i32]
         L.vr_profile_read.argtypes = [vp, i32, C.POINTER(dp), C.POINTER(i64)]
+        L.vr_part_create.argtypes = [vp, i32, i32, i32, C.POINTER(vp)]
+        L.vr_part_destroy.argtypes = [vp]
+        L.vr_part_info.argtypes = [vp, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp), C.POINTER(i32)]
+        L.vr_injc_part.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, i32, C.POINTER(i32)]
+        L.vr_remv_part.argtypes = [vp, i32]
+        L.vr_iter_part.argtypes = [vp, i32]
+        L.vr_part_attach.argtypes = [vp, i32]
+        L.vr_part_set_state.argtypes = [vp, vp, vp, vp, i32]
+        L.vr_part_get_state.argtypes = [vp, vp, vp, vp, C.POINTER(i32)]
+        L.vr_part_probe.argtypes = [vp, vp, i32, vp, vp]
         L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
         _lib = L
@@ -113,8 +123,8 @@ class Run:
 
     # -- lifetime -------------------------------------------------------------
     def close(self):
-        if self._h:
-            lib().vr_destroy(self._h)
+        # a context with live particle classes refuses (VR_ERR_STATE) and is kept
+        if self._h and lib().vr_destroy(self._h) == 0:
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -180,7 +190,7 @@ class Run:
         return n.value
 
     PROFILE_KINDS = ["hdnbc", "hdnl", "rhs", "tsweep", "rsweep", "zsweep", "divq", "fft", "dct",
-                     "radial", "upsol", "uppres", "diag"]
+                     "radial", "upsol", "uppres", "diag", "part"]
 
     def profile(self, enable: bool) -> None:
         self._chk(lib().vr_profile(self._h, 1 if enable else 0), "profile")
@@ -252,3 +262,86 @@ def solve_lap_bthom(rhs, b1, b2, b3, m, n):
     if rc:
         raise VrError(rc, "vr_solve_lap_bthom")
     return sol.reshape(np.shape(rhs))
+
+
+class Part:
+    """One particle class on a Run (part_tools.F90 ``type part``).
+
+    ``u`` (naloc, 117) and ``v`` (naloc, 3) are the reference's state arrays;
+    slots are 1-based in ``injc``/``remv`` as in the reference.
+    """
+
+    NVAR = 117
+
+    def __init__(self, run: Run, pid: int, naloc: int, mode: int = 0):
+        self.run, self.naloc = run, naloc
+        self._h = C.c_void_p()
+        run._chk(lib().vr_part_create(run._h, pid, naloc, mode, C.byref(self._h)), "vr_part_create")
+        r, st, c, ns = C.c_double(), C.c_double(), C.c_double(), C.c_int32()
+        self._chk(lib().vr_part_info(self._h, C.byref(r), C.byref(st), C.byref(c), C.byref(ns)))
+        self.r, self.st, self.c, self.nsubdt = r.value, st.value, c.value, ns.value
+
+    def _chk(self, rc, what="particles"):
+        self.run._chk(rc, what)
+
+    def close(self):
+        if self._h:
+            lib().vr_part_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def injc(self, x, y, z, u=0.0, v=0.0, w=0.0, c=None, icall=1) -> int:
+        ip = C.c_int32()
+        self._chk(lib().vr_injc_part(self._h, x, y, z, self.c if c is None else c, u, v, w, icall,
+                                     C.byref(ip)), "injc_part")
+        return ip.value
+
+    def remv(self, ip: int) -> None:
+        self._chk(lib().vr_remv_part(self._h, ip), "remv_part")
+
+    def iter_part(self, irk: int = 1) -> None:
+        self._chk(lib().vr_iter_part(self._h, irk), "iter_part")
+
+    def attach(self, on: bool = True) -> None:
+        self._chk(lib().vr_part_attach(self._h, 1 if on else 0), "part_attach")
+
+    def set_state(self, u, v, isfre=None, nlast=None) -> None:
+        u = np.asfortranarray(u, dtype=np.float64)
+        v = np.asfortranarray(v, dtype=np.float64)
+        assert u.shape == (self.naloc, self.NVAR) and v.shape == (self.naloc, 3)
+        isf = None if isfre is None else np.ascontiguousarray(isfre, dtype=np.int32)
+        self._chk(lib().vr_part_set_state(self._h, _p(u), _p(v), None if isf is None else _p(isf),
+                                          self.naloc if nlast is None else nlast), "part_set_state")
+
+    def state(self):
+        """(u, v, isfre, {npart, nlast, nfree, nids}) copied to the host."""
+        u = np.empty((self.naloc, self.NVAR), dtype=np.float64, order="F")
+        v = np.empty((self.naloc, 3), dtype=np.float64, order="F")
+        isf = np.empty(self.naloc, dtype=np.int32)
+        cnt = (C.c_int32 * 4)()
+        self._chk(lib().vr_part_get_state(self._h, _p(u), _p(v), _p(isf), cnt), "part_get_state")
+        return u, v, isf, dict(zip(("npart", "nlast", "nfree", "nids"), list(cnt)))
+
+    @property
+    def counts(self) -> dict:
+        cnt = (C.c_int32 * 4)()
+        self._chk(lib().vr_part_get_state(self._h, None, None, None, cnt), "part_get_state")
+        return dict(zip(("npart", "nlast", "nfree", "nids"), list(cnt)))
+
+    def probe(self, xyz):
+        """Interpolated velocity (n,3), gradient (n,3,3) [i,j] = du_i/dx_j,
+        Hessian (n,3,3,3) and cell indices (n,3) at points xyz (n,3)."""
+        xyz = np.ascontiguousarray(np.atleast_2d(xyz), dtype=np.float64)
+        n = xyz.shape[0]
+        out = np.empty((n, 39), dtype=np.float64)
+        cells = np.empty((n, 3), dtype=np.int32)
+        self._chk(lib().vr_part_probe(self._h, _p(xyz), n, _p(out), _p(cells)), "part_probe")
+        vel = out[:, :3]
+        dvel = out[:, 3:12].reshape(n, 3, 3, order="F")
+        ddvel = out[:, 12:].reshape(n, 3, 3, 3, order="F")
+        return vel, dvel, ddvel, cells

@@ -513,6 +513,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
 
 extern "C" int vr_destroy(vr_ctx *c) {
   if (!c) return VR_OK;
+  if (c->nparts > 0) return set_err(c, VR_ERR_STATE, "vr_destroy: particle classes of this context still exist");
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int i = 0; i < 4; i++)
@@ -523,6 +524,7 @@ extern "C" int vr_destroy(vr_ctx *c) {
   for (double *p : ptrs)
     if (p) cudaFree(p);
   if (c->d_count) cudaFree(c->d_count);
+  if (c->part_mesh) cudaFree(c->part_mesh);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   delete[] c->h_rc;
   delete[] c->h_rm;
@@ -840,6 +842,11 @@ extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
   for (int s = 0; s < nsteps; s++) {
     c->ntime = c->d.dt + c->ntime;
     for (int irk = 1; irk <= 3; irk++) {
+      if (irk == 1)  // loop.F90:65-70: particles advance once per step, before ucoeff
+        for (vr_part *p : c->parts) {
+          int rc = vr_part_enqueue(p);
+          if (rc) return rc;
+        }
       int rc = enqueue_substep(c, irk);
       if (rc) return rc;
     }

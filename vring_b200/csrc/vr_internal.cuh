@@ -91,6 +91,8 @@ struct HostCoef;  // ucoeff/coesys vectors in double, host side
 
 }  // namespace vr
 
+struct vr_part;
+
 struct vr_ctx {
   vr_desc d;
   int dev;
@@ -131,6 +133,11 @@ struct vr_ctx {
   std::vector<int> prof_kind;
   size_t prof_used;
   std::string err;
+  // particle classes: theta/z mesh vectors (thc, thm, zm, zc), the classes
+  // advanced by vr_iterate, and the number of live classes of this context
+  double *part_mesh;
+  std::vector<vr_part *> parts;
+  int nparts;
 };
 
 namespace vr {
@@ -153,7 +160,7 @@ int set_err(vr_ctx *c, int code, const std::string &msg);
 // kernel families for vr_profile_read
 enum ProfKind {
   PK_HDNBC = 0, PK_HDNL, PK_RHS, PK_TSWEEP, PK_RSWEEP, PK_ZSWEEP, PK_DIVQ, PK_FFT, PK_DCT,
-  PK_RADIAL, PK_UPSOL, PK_UPPRES, PK_DIAG, PK_N
+  PK_RADIAL, PK_UPSOL, PK_UPPRES, PK_DIAG, PK_PART, PK_N
 };
 
 // Counts one kernel launch; with profiling on, brackets it with events on the
@@ -164,6 +171,9 @@ struct LaunchScope {
   LaunchScope(vr_ctx *ctx, int kind);
   ~LaunchScope();
 };
+
+// enqueue the nsubdt Euler substeps of one particle class (vr_particles.cu)
+int vr_part_enqueue(vr_part *p);
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);
