@@ -46,7 +46,8 @@ enum vr_status {
   VR_ERR_STATE = 7,     /* call made in a state that does not allow it       */
   VR_ERR_ARG = 8,       /* invalid argument                                  */
   VR_ERR_CAPACITY = 9,  /* particle slots exhausted                          */
-  VR_ERR_NODEVICE = 10  /* no usable CUDA device                             */
+  VR_ERR_NODEVICE = 10, /* no usable CUDA device                             */
+  VR_ERR_SCRATCH = 11   /* larger than a no-allocation entry's fixed scratch */
 };
 
 enum vr_precision { VR_FP64 = 0, VR_MIXED = 1 };
@@ -195,6 +196,21 @@ VR_API int vr_solve_lap_thom(const double *rhs, double *sol, const double *aa, c
  * off-diagonal blocks, tridiagonal diagonal blocks (b1 sub, b2 diag, b3 super) */
 VR_API int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
                        const double *b3, int32_t m, int32_t n, int32_t nbatch);
+
+/* No counterpart in the reference: solve_lap_thom on device arrays that
+ * allocates nothing.  rhs, sol, aa, bb, cc are device pointers of the current
+ * device (n * nbatch doubles each, the layout of vr_solve_lap_thom); the work
+ * is enqueued on cuda_stream (NULL: the legacy default stream) and the call
+ * returns without waiting.  The gamm scratch is a fixed array of
+ * VR_THOM_NOALLOC_MAX doubles (4 MiB) per device inside the library:
+ * n * nbatch above that returns VR_ERR_SCRATCH.  The first call on a device
+ * looks the array up (and may load the module); make it before any stream
+ * capture.  Calls on one device share the array, so calls that may run at the
+ * same time race: order them, e.g. on one stream.  The scratch need not start
+ * at zero. */
+#define VR_THOM_NOALLOC_MAX (1 << 19)
+VR_API int vr_solve_lap_thom_noalloc(const double *rhs, double *sol, const double *aa, const double *bb,
+                                     const double *cc, int32_t n, int32_t nbatch, void *cuda_stream);
 
 #ifdef __cplusplus
 }

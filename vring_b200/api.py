@@ -25,7 +25,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "vring_b200.h")
 VR_ABI_VERSION = 1
 STATUS = {0: "VR_OK", 1: "VR_ERR_DESC", 2: "VR_ERR_OOM", 3: "VR_ERR_CUDA", 4: "VR_ERR_NONFINITE",
           5: "VR_ERR_TIMEOUT", 6: "VR_ERR_FIELD", 7: "VR_ERR_STATE", 8: "VR_ERR_ARG",
-          9: "VR_ERR_CAPACITY", 10: "VR_ERR_NODEVICE"}
+          9: "VR_ERR_CAPACITY", 10: "VR_ERR_NODEVICE", 11: "VR_ERR_SCRATCH"}
 FIELD_ID = {"q1": 0, "q2": 1, "q3": 2, "dq1": 3, "dq2": 4, "dq3": 5, "ru1": 6, "ru2": 7, "ru3": 8,
             "pres": 11, "prg": 12, "rhs": 13, "dph": 15, "dq3no": 19, "corr3s": 22, "corr3n": 23,
             "csort": 24, "tconv": 25}
@@ -99,6 +99,7 @@ def lib():
         L.vr_part_probe.argtypes = [vp, vp, i32, vp, vp]
         L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
+        L.vr_solve_lap_thom_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, i32, vp]
         _lib = L
     return _lib
 
@@ -345,3 +346,19 @@ class Part:
         dvel = out[:, 3:12].reshape(n, 3, 3, order="F")
         ddvel = out[:, 12:].reshape(n, 3, 3, 3, order="F")
         return vel, dvel, ddvel, cells
+
+
+THOM_NOALLOC_MAX = 1 << 19
+
+
+def solve_lap_thom_noalloc(rhs_ptr: int, sol_ptr: int, aa_ptr: int, bb_ptr: int, cc_ptr: int,
+                           n: int, nbatch: int, cuda_stream: int = 0) -> None:
+    """``vr_solve_lap_thom_noalloc``: the batched Thomas solve on device
+    arrays (raw device addresses of n*nbatch doubles each), enqueued on
+    ``cuda_stream`` without any device allocation; its scratch is a fixed
+    array of THOM_NOALLOC_MAX doubles per device shared by all calls."""
+    rc = lib().vr_solve_lap_thom_noalloc(C.c_void_p(rhs_ptr), C.c_void_p(sol_ptr), C.c_void_p(aa_ptr),
+                                         C.c_void_p(bb_ptr), C.c_void_p(cc_ptr), n, nbatch,
+                                         C.c_void_p(cuda_stream or None))
+    if rc:
+        raise VrError(rc, "vr_solve_lap_thom_noalloc(n=%d, nbatch=%d)" % (n, nbatch))

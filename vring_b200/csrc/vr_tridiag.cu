@@ -4,6 +4,7 @@
 // Host arrays in, host arrays out; the device copies are made per call.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <vector>
 
 #include "vr_internal.cuh"
@@ -177,6 +178,48 @@ extern "C" int vr_solve_lap_thom(const double *rhs, double *sol, const double *a
   for (double *p : d)
     if (p) cudaFree(p);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// vr_solve_lap_thom_noalloc: the batched Thomas solve on caller-owned device
+// arrays, with its gamm scratch in a fixed array of this library instead of a
+// per-call allocation.  It is meant for hosts that size all device memory once
+// at start-up and then run a time loop that must not allocate: a per-call
+// cudaMallocAsync can fail with out-of-memory halfway through a long run when
+// other work has taken the pool, and it adds allocator work to every call.
+// The scratch is one file-scope array per device, shared by every call on
+// that device.  Every call writes the scratch rows it later reads, so nothing
+// in it needs to start at zero; two calls that execute at the same time on
+// one device (different streams or host threads) use the same rows and
+// corrupt each other's results, so such calls must be ordered, e.g. on one
+// stream.  The array's address is looked up once per device on the first call
+// (cudaGetSymbolAddress), which may load the module; make that first call
+// before any stream capture.
+static __device__ __align__(256) double g_thom_scratch[VR_THOM_NOALLOC_MAX];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<double *> g_thom_scratch_ptr[kMaxDevices];
+}  // namespace
+
+extern "C" int vr_solve_lap_thom_noalloc(const double *rhs, double *sol, const double *aa, const double *bb,
+                                         const double *cc, int32_t n, int32_t nbatch, void *cuda_stream) {
+  if (!rhs || !sol || !aa || !bb || !cc || n < 1 || nbatch < 1) return VR_ERR_ARG;
+  if ((int64_t)n * nbatch > (int64_t)VR_THOM_NOALLOC_MAX) return VR_ERR_SCRATCH;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return VR_ERR_NODEVICE;
+  if (dev >= kMaxDevices) return VR_ERR_ARG;
+  double *gamm = g_thom_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!gamm) {
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_thom_scratch);
+    if (e != cudaSuccess || !addr) return VR_ERR_CUDA;
+    gamm = static_cast<double *>(addr);
+    g_thom_scratch_ptr[dev].store(gamm, std::memory_order_release);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+  k_thomas<<<(nbatch + 127) / 128, 128, 0, s>>>(rhs, sol, aa, bb, cc, gamm, n, nbatch);
+  return cudaGetLastError() == cudaSuccess ? VR_OK : VR_ERR_CUDA;
 }
 
 extern "C" int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
