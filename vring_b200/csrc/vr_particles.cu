@@ -33,7 +33,7 @@ struct vr_part {
   int id, naloc, nvar, nsubdt, mode;
   double r, st, c;
   // device
-  double *u, *v, *tab;  // tab: mint(9,27) then xint(27,3)
+  double *u, *v;
   int *isfre, *gone;    // gone[ip-1] = substep serial at removal, -1 alive
   int *d_nremoved;
   // host bookkeeping (part_tools.F90 type part)
@@ -82,10 +82,23 @@ __device__ __forceinline__ double part_theta(double x, double y, double r) {
   return __dadd_rn(vr_acos(__ddiv_rn(-x, r)), pi4);
 }
 
+// Closed form of the least-squares operator mint = (X^T X)^{-1} X^T of the
+// 27-point stencil for the basis (t, r, z, t^2, tr, r^2, rz, z^2, zt) on
+// offsets {-d, 0, d}^3 (part_tools.F90:295-357), and the stencil products of
+// xint.  Row entries depend only on the offset pattern, so the kernel applies
+// mint as signed sums instead of a 9 x 27 table.
+struct PartCoef {
+  double lin[3];    // rows t, r, z: o_a / (18 d_a)
+  double sq[3][8];  // rows t^2, r^2, z^2 at pattern 4[o_a != 0] + 2[o_b != 0] + [o_c != 0], b = a+1, c = a+2
+  double cr[3];     // rows tr, rz, zt: o_a o_b / (12 d_a d_b)
+  double pr[9];     // d1, d2, d3, d1 d1, d1 d2, d2 d2, d2 d3, d3 d3, d3 d1
+};
+
 struct PartGeo {
   Geo g;
   const double *thc, *thm, *rm, *rc, *zm, *zc;  // 1-based device vectors
   double dtheta, dr, dz, zmax, rmax;
+  PartCoef C;
 };
 
 __device__ __forceinline__ void part_cell(const PartGeo &P, double x, double y, double z, int &it, int &ir, int &iz,
@@ -98,26 +111,91 @@ __device__ __forceinline__ void part_cell(const PartGeo &P, double x, double y, 
   iz = (int)floor(__ddiv_rn(z, P.dz)) + 1;
 }
 
-// stencil sample of component ivar (part_tools.F90:587-590); indices clamped
-// to the stored extents (reached only by particles already out of range)
-__device__ __forceinline__ double part_sample(const PartGeo &P, const double *q1, const double *q2,
-                                              const double *q3, int ivar, int it, int ir, int iz) {
-  ir = ir < 0 ? 0 : (ir > P.g.nr + 2 ? P.g.nr + 2 : ir);
-  iz = iz < 0 ? 0 : (iz > P.g.nz + 2 ? P.g.nz + 2 : iz);
-  int o = I3(P.g, it, ir, iz);
-  if (ivar == 1) return __ldg(q1 + o);
-  if (ivar == 3) return __ldg(q3 + o);
-  double rcv = P.rc[ir];
-  return rcv > (double)0.0001f ? __ldg(q2 + o) / rcv : 0.0;
+// One Richardson pass of the reference's fit (part_tools.F90:600-620):
+// mp = -mint (X a - y); the first pass starts from a = 0.
+template <bool FIRST>
+__device__ __forceinline__ void ls_pass(const PartCoef &C, const double (&y)[27], const double (&a)[9],
+                                        double (&mp)[9]) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) mp[i] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 27; k++) {
+    const int o1 = k % 3 - 1, o2 = (k / 3) % 3 - 1, o3 = k / 9 - 1;
+    double r = 0.0;
+    if (!FIRST) {  // X a at offset k, in the reference's term order
+      if (o1) r = r + (o1 * C.pr[0]) * a[0];
+      if (o2) r = r + (o2 * C.pr[1]) * a[1];
+      if (o3) r = r + (o3 * C.pr[2]) * a[2];
+      if (o1) r = r + C.pr[3] * a[3];
+      if (o1 * o2) r = r + ((o1 * o2) * C.pr[4]) * a[4];
+      if (o2) r = r + C.pr[5] * a[5];
+      if (o2 * o3) r = r + ((o2 * o3) * C.pr[6]) * a[6];
+      if (o3) r = r + C.pr[7] * a[7];
+      if (o3 * o1) r = r + ((o3 * o1) * C.pr[8]) * a[8];
+    }
+    const double e = r - y[k];
+    const int n1 = o1 != 0, n2 = o2 != 0, n3 = o3 != 0;
+    if (o1) mp[0] = mp[0] - (o1 * C.lin[0]) * e;
+    if (o2) mp[1] = mp[1] - (o2 * C.lin[1]) * e;
+    if (o3) mp[2] = mp[2] - (o3 * C.lin[2]) * e;
+    if (n1 | n2 | n3) {
+      mp[3] = mp[3] - C.sq[0][4 * n1 + 2 * n2 + n3] * e;
+      mp[5] = mp[5] - C.sq[1][4 * n2 + 2 * n3 + n1] * e;
+      mp[7] = mp[7] - C.sq[2][4 * n3 + 2 * n1 + n2] * e;
+    }
+    if (o1 * o2) mp[4] = mp[4] - ((o1 * o2) * C.cr[0]) * e;
+    if (o2 * o3) mp[6] = mp[6] - ((o2 * o3) * C.cr[1]) * e;
+    if (o3 * o1) mp[8] = mp[8] - ((o3 * o1) * C.cr[2]) * e;
+  }
 }
 
-// interpolated velocity, gradient and Hessian in Cartesian components at
-// (x, y, z) (part_tools.F90:521-797)
-__device__ void part_eval(const PartGeo &P, const double *q1, const double *q2, const double *q3,
-                          const double *__restrict__ tab, double x, double y, double z, double vel[3],
-                          double dvel[3][3], double ddvel[3][3][3], int cell[3]) {
-  const double *mint = tab, *xint = tab + 243;
-  double r, theta;
+// quadratic coefficients of one component: Richardson iteration from zero,
+// at most 100 passes, stopping when |mp| < 1e-6 (single-precision literal)
+__device__ __forceinline__ void ls_fit(const PartCoef &C, const double (&y)[27], double (&a)[9]) {
+  double mp[9];
+  ls_pass<true>(C, y, a, mp);
+  double nn = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    a[i] = mp[i];
+    nn += mp[i] * mp[i];
+  }
+  if (sqrt(nn) < (double)0.000001f) return;
+#pragma unroll 1
+  for (int iint = 2; iint <= 100; iint++) {
+    ls_pass<false>(C, y, a, mp);
+    nn = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      a[i] = a[i] + mp[i];
+      nn += mp[i] * mp[i];
+    }
+    if (sqrt(nn) < (double)0.000001f) return;
+  }
+}
+
+// ---- three threads per particle ------------------------------------------
+// A block holds 32 particles in three warps; warp w fits component w of the
+// velocity (q1, q2/rc, q3) at the particle, then owns row w of every output:
+// u_w, du_w/dx_j, d2u_w/dx_j dx_k and row w of the position, velocity,
+// Jacobian and Hessian updates.  Shared memory carries the fitted components
+// and the old Jacobian/Hessian rows between the warps, so each warp's global
+// accesses are rows of u (32 consecutive particles).
+
+constexpr int kPartPerBlock = 32;
+
+struct PartShared {
+  double cv[39][kPartPerBlock];   // component kd: ff, dff(3), ddff(3,3) at 13 kd + t
+  double jac[9][kPartPerBlock];   // old Jacobian, m + 3 j
+  double hes[27][kPartPerBlock];  // old Hessian, m + 3 j + 9 k
+  double pos[3][kPartPerBlock];   // new position
+};
+
+// Fit component kd at (x, y, z) and write ff, dff and ddff (the first 13
+// rows of M FI, part_tools.F90:653-683) to cv[13 kd ..][p].
+__device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
+                                               double y, double z, double (*cv)[kPartPerBlock], int p,
+                                               int (&cell)[3], double &r, double &theta) {
   int it, ir, iz;
   part_cell(P, x, y, z, it, ir, iz, r, theta);
   // keep the mesh lookups inside the stored vectors for points off the mesh
@@ -128,293 +206,323 @@ __device__ void part_eval(const PartGeo &P, const double *q1, const double *q2, 
   cell[0] = it;
   cell[1] = ir;
   cell[2] = iz;
-  double ff[3], dff[3][3], ddff[3][3][3];
-  double sn = sin(theta), cs = cos(theta);
-  double sn2 = sin(2.0 * theta), cs2 = cos(2.0 * theta);
-  for (int ivar = 1; ivar <= 3; ivar++) {
-    double yint[27];
-    for (int f3 = -1; f3 <= 1; f3++)
-      for (int f2 = -1; f2 <= 1; f2++)
-        for (int f1 = -1; f1 <= 1; f1++) {
-          int iv = (f1 + 1) + 3 * (f2 + 1) + 9 * (f3 + 1);
-          int itof = it + f1;
-          if (itof > P.g.nth) itof = 1;
-          if (itof < 1) itof = P.g.nth;
-          yint[iv] = part_sample(P, q1, q2, q3, ivar, itof, ir + f2, iz + f3);
+  double yv[27];
+  {
+    int ith[3], jr[3], kz[3];
+#pragma unroll
+    for (int f = -1; f <= 1; f++) {
+      int t = it + f;
+      if (t > P.g.nth) t = 1;
+      if (t < 1) t = P.g.nth;
+      ith[f + 1] = t - 1;
+      int j = ir + f, k = iz + f;
+      jr[f + 1] = j < 0 ? 0 : (j > P.g.nr + 2 ? P.g.nr + 2 : j);
+      kz[f + 1] = k < 0 ? 0 : (k > P.g.nz + 2 ? P.g.nz + 2 : k);
+    }
+    const double tiny = (double)0.0001f;
+#pragma unroll
+    for (int f3 = 0; f3 < 3; f3++)
+#pragma unroll
+      for (int f2 = 0; f2 < 3; f2++) {
+        const double *row = q + (size_t)P.g.nth * (jr[f2] + (size_t)P.g.J3 * kz[f3]);
+#pragma unroll
+        for (int f1 = 0; f1 < 3; f1++) yv[f1 + 3 * f2 + 9 * f3] = __ldg(row + ith[f1]);
+        if (kd == 1) {  // q2 / rc, zero where rc <= 1e-4 (part_tools.F90:587-590)
+          const double rcv = __ldg(P.rc + jr[f2]);
+          const double irc = rcv > tiny ? 1.0 / rcv : 0.0;
+#pragma unroll
+          for (int f1 = 0; f1 < 3; f1++) yv[f1 + 3 * f2 + 9 * f3] *= irc;
         }
-    double y0 = yint[13];
-    for (int iv = 0; iv < 27; iv++) yint[iv] = yint[iv] - y0;
-    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int iint = 1; iint <= 100; iint++) {
-      double mp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int k = 0; k < 27; k++) {
-        double x1 = __ldg(xint + k), x2 = __ldg(xint + 27 + k), x3 = __ldg(xint + 54 + k);
-        double rk = x1 * a[0] + x2 * a[1] + x3 * a[2] + x1 * x1 * a[3] + x1 * x2 * a[4] + x2 * x2 * a[5] +
-                    x2 * x3 * a[6] + x3 * x3 * a[7] + x3 * x1 * a[8];
-        double d = rk - yint[k];
-#pragma unroll
-        for (int i = 0; i < 9; i++) mp[i] = mp[i] - __ldg(mint + i + 9 * k) * d;
       }
-      double nn = 0.0;
-#pragma unroll
-      for (int i = 0; i < 9; i++) {
-        a[i] = a[i] + mp[i];
-        nn += mp[i] * mp[i];
-      }
-      if (sqrt(nn) < (double)0.000001f) break;
-    }
-    double dtp, drp, dzp;
-    if (ivar == 1) {
-      dtp = theta - P.thc[it];
-      drp = r - P.rm[ir];
-      dzp = z - P.zm[iz];
-    } else if (ivar == 2) {
-      dtp = theta - P.thm[it];
-      drp = r - P.rc[ir];
-      dzp = z - P.zm[iz];
-    } else {
-      dtp = theta - P.thm[it];
-      drp = r - P.rm[ir];
-      dzp = z - P.zc[iz];
-    }
-    const double twopi = 6.283185307179586;
-    if (dtp > P.dtheta) dtp = dtp - twopi;
-    if (dtp < -P.dtheta) dtp = dtp + twopi;
-    double f = dtp * a[0] + drp * a[1] + dzp * a[2] + dtp * dtp * a[3] + dtp * drp * a[4] + drp * drp * a[5] +
-               drp * dzp * a[6] + dzp * dzp * a[7] + dzp * dtp * a[8] + y0;
-    double FI[12];
-    FI[0] = a[0] + 2.0 * dtp * a[3] + drp * a[4] + dzp * a[8];  // ft
-    FI[1] = a[1] + dtp * a[4] + 2.0 * drp * a[5] + dzp * a[6];  // fr
-    FI[2] = a[2] + drp * a[6] + 2.0 * dzp * a[7] + dtp * a[8];  // fz
-    FI[3] = 2.0 * a[3];                                         // ftt
-    FI[4] = drp * a[4];                                         // ftr
-    FI[5] = dzp * a[8];                                         // ftz
-    FI[6] = a[4];                                               // frt
-    FI[7] = 2.0 * a[5];                                         // frr
-    FI[8] = a[6];                                               // frz
-    FI[9] = a[8];                                               // fzt
-    FI[10] = a[6];                                              // fzr
-    FI[11] = 2.0 * a[7];                                        // fzz
-    const double r2 = r * r;
-    ff[ivar - 1] = f;
-    // rows 1..3 of M (part_tools.F90:672-674)
-    dff[ivar - 1][0] = -sn / r * FI[0] + cs * FI[1];
-    dff[ivar - 1][1] = cs / r * FI[0] + sn * FI[1];
-    dff[ivar - 1][2] = FI[2];
-    // rows 4..12 of M (part_tools.F90:675-683): ddff(id1, id2) = row 3+id1+3(id2-1)
-    double R4 = sn2 / r2 * FI[0] + sn * sn / r * FI[1] + sn * sn / r2 * FI[3] + (-cs * sn / r) * FI[4] +
-                (-cs * sn / r) * FI[6] + cs * cs * FI[7];
-    double R5 = -cs2 / r2 * FI[0] + (-cs * sn / r) * FI[1] + (-cs * sn / r2) * FI[3] + (-sn * sn / r) * FI[4] +
-                cs * cs / r * FI[6] + cs * sn * FI[7];
-    double R6 = -sn / r * FI[5] + cs * FI[8];
-    double R7 = -cs2 / r2 * FI[0] + (-cs * sn / r) * FI[1] + (-cs * sn / r2) * FI[3] + cs * cs / r * FI[4] +
-                (-sn * sn / r) * FI[6] + cs * sn * FI[7];
-    double R8 = -sn2 / r2 * FI[0] + cs * cs / r * FI[1] + cs * cs / r2 * FI[3] + cs * sn / r * FI[4] +
-                cs * sn / r * FI[6] + sn * sn * FI[7];
-    double R9 = cs / r * FI[5] + sn * FI[8];
-    double R10 = -sn / r * FI[9] + cs * FI[10];
-    double R11 = cs / r * FI[9] + sn * FI[10];
-    double R12 = FI[11];
-    ddff[ivar - 1][0][0] = R4;
-    ddff[ivar - 1][1][0] = R5;
-    ddff[ivar - 1][2][0] = R6;
-    ddff[ivar - 1][0][1] = R7;
-    ddff[ivar - 1][1][1] = R8;
-    ddff[ivar - 1][2][1] = R9;
-    ddff[ivar - 1][0][2] = R10;
-    ddff[ivar - 1][1][2] = R11;
-    ddff[ivar - 1][2][2] = R12;
   }
+  const double y0 = yv[13];
+#pragma unroll
+  for (int k = 0; k < 27; k++) yv[k] = yv[k] - y0;
+  double a[9];
+  ls_fit(P.C, yv, a);
+  double dtp, drp, dzp;
+  if (kd == 0) {
+    dtp = theta - __ldg(P.thc + it);
+    drp = r - __ldg(P.rm + ir);
+    dzp = z - __ldg(P.zm + iz);
+  } else if (kd == 1) {
+    dtp = theta - __ldg(P.thm + it);
+    drp = r - __ldg(P.rc + ir);
+    dzp = z - __ldg(P.zm + iz);
+  } else {
+    dtp = theta - __ldg(P.thm + it);
+    drp = r - __ldg(P.rm + ir);
+    dzp = z - __ldg(P.zc + iz);
+  }
+  const double twopi = 6.283185307179586;
+  if (dtp > P.dtheta) dtp = dtp - twopi;
+  if (dtp < -P.dtheta) dtp = dtp + twopi;
+  const double ff = dtp * a[0] + drp * a[1] + dzp * a[2] + dtp * dtp * a[3] + dtp * drp * a[4] +
+                    drp * drp * a[5] + drp * dzp * a[6] + dzp * dzp * a[7] + dzp * dtp * a[8] + y0;
+  const double ft = a[0] + 2.0 * dtp * a[3] + drp * a[4] + dzp * a[8];
+  const double fr = a[1] + dtp * a[4] + 2.0 * drp * a[5] + dzp * a[6];
+  const double fz = a[2] + drp * a[6] + 2.0 * dzp * a[7] + dtp * a[8];
+  const double ftt = 2.0 * a[3], ftr = drp * a[4], ftz = dzp * a[8], frt = a[4], frr = 2.0 * a[5];
+  const double frz = a[6], fzt = a[8], fzr = a[6], fzz = 2.0 * a[7];
+  double sn, cs, sn2, cs2;
+  sincos(theta, &sn, &cs);
+  sincos(2.0 * theta, &sn2, &cs2);
+  const double ir1 = 1.0 / r, ir2 = 1.0 / (r * r);
+  const double m_snr = -sn * ir1, m_csr = cs * ir1;
+  const double m30 = sn2 * ir2, m31 = sn * sn * ir1, m33 = sn * sn * ir2, m34 = -cs * sn * ir1, m37 = cs * cs;
+  const double m40 = -cs2 * ir2, m43 = -cs * sn * ir2, m44 = -sn * sn * ir1, m46 = cs * cs * ir1, m47 = cs * sn;
+  const double m70 = -sn2 * ir2, m73 = cs * cs * ir2, m74 = cs * sn * ir1, m77 = sn * sn;
+  double(*o)[kPartPerBlock] = cv + 13 * kd;
+  o[0][p] = ff;
+  o[1][p] = m_snr * ft + cs * fr;                                                     // dff 1
+  o[2][p] = m_csr * ft + sn * fr;                                                     // dff 2
+  o[3][p] = fz;                                                                       // dff 3
+  o[4][p] = m30 * ft + m31 * fr + m33 * ftt + m34 * ftr + m34 * frt + m37 * frr;      // ddff(1,1)
+  o[5][p] = m40 * ft + m34 * fr + m43 * ftt + m44 * ftr + m46 * frt + m47 * frr;      // ddff(2,1)
+  o[6][p] = m_snr * ftz + cs * frz;                                                   // ddff(3,1)
+  o[7][p] = m40 * ft + m34 * fr + m43 * ftt + m46 * ftr + m44 * frt + m47 * frr;      // ddff(1,2)
+  o[8][p] = m70 * ft + m46 * fr + m73 * ftt + m74 * ftr + m74 * frt + m77 * frr;      // ddff(2,2)
+  o[9][p] = m_csr * ftz + sn * frz;                                                   // ddff(3,2)
+  o[10][p] = m_snr * fzt + cs * fzr;                                                  // ddff(1,3)
+  o[11][p] = m_csr * fzt + sn * fzr;                                                  // ddff(2,3)
+  o[12][p] = fzz;                                                                     // ddff(3,3)
+}
+
+// Row id of the Cartesian velocity, gradient and Hessian from the three
+// fitted components (part_tools.F90:730-797), in the reference's summation
+// order over components.
+__device__ __forceinline__ void part_cart_row(double r, double theta, int id, const double (*cv)[kPartPerBlock],
+                                              int p, double &vel, double (&dvel)[3], double (&ddvel)[3][3]) {
+  double sn, cs;
+  sincos(theta, &sn, &cs);
   const double rs = r > (double)0.000001f ? r : (double)0.000001f;
-  const double NM[3][3] = {{-sn, cs, 0.0}, {cs, sn, 0.0}, {0.0, 0.0, 1.0}};
-  // DNMAT(a,b,c), zero outside a,b,c in {1,2} x {1,2} x {1,2}
-  double DN[3][3][3] = {};
-  DN[0][0][0] = cs * sn / rs;
-  DN[0][0][1] = sn * sn / rs;
-  DN[0][1][0] = sn * sn / rs;
-  DN[0][1][1] = -cs * sn / rs;
-  DN[1][0][0] = -cs * cs / rs;
-  DN[1][0][1] = -sn * cs / rs;
-  DN[1][1][0] = -sn * cs / rs;
-  DN[1][1][1] = cs * cs / rs;
-  const double rs2 = rs * rs;
-  const double A1 = sn * (-2.0 * (cs * cs) + sn * sn) / rs2, A2 = -3.0 * cs * (sn * sn) / rs2;
-  const double A3 = cs * (cs * cs - 2.0 * (sn * sn)) / rs2, A4 = 3.0 * (cs * cs) * sn / rs2;
-  // DDNMAT(a,b,c,d) for a,b,c,d in {1,2}
-  double DDN[2][2][2][2] = {{{{A1, A2}, {A2, -A1}}, {{A3, -A1}, {-A1, -A3}}},
-                            {{{A3, -A1}, {-A1, -A3}}, {{A4, -A3}, {-A3, -A4}}}};
-  for (int id = 0; id < 3; id++) {
-    double s = 0.0;
-    for (int jd = 0; jd < 3; jd++) s = s + ff[jd] * NM[id][jd];
-    vel[id] = s;
+  const double irs = 1.0 / rs, irs2 = 1.0 / (rs * rs);
+  const double A1 = sn * (-2.0 * (cs * cs) + sn * sn) * irs2, A2 = -3.0 * cs * (sn * sn) * irs2;
+  const double A3 = cs * (cs * cs - 2.0 * (sn * sn)) * irs2, A4 = 3.0 * (cs * cs) * sn * irs2;
+  // DN(a, b, kd) for b = id, a = 1, 2 and kd = 1, 2 (zero elsewhere)
+  double dnb[2][2];  // [a][kd]
+  if (id == 0) {
+    dnb[0][0] = cs * sn * irs;  // DN(1,1,1)
+    dnb[0][1] = sn * sn * irs;  // DN(1,1,2)
+    dnb[1][0] = -cs * cs * irs; // DN(2,1,1)
+    dnb[1][1] = -sn * cs * irs; // DN(2,1,2)
+  } else {
+    dnb[0][0] = sn * sn * irs;  // DN(1,2,1)
+    dnb[0][1] = -cs * sn * irs; // DN(1,2,2)
+    dnb[1][0] = -sn * cs * irs; // DN(2,2,1)
+    dnb[1][1] = cs * cs * irs;  // DN(2,2,2)
   }
-  for (int id = 0; id < 3; id++)
-    for (int jd = 0; jd < 3; jd++) {
-      double s = 0.0;
-      for (int kd = 0; kd < 3; kd++) s = s + dff[kd][jd] * NM[id][kd] + ff[kd] * DN[jd][id][kd];
-      dvel[id][jd] = s;
+  // DDN(l, j, id, kd) for l, j, kd in {1, 2}
+  double ddnb[2][2][2];  // [l][j][kd]
+  if (id == 0) {
+    ddnb[0][0][0] = A1;  ddnb[0][0][1] = A2;
+    ddnb[0][1][0] = A3;  ddnb[0][1][1] = -A1;
+    ddnb[1][0][0] = A3;  ddnb[1][0][1] = -A1;
+    ddnb[1][1][0] = A4;  ddnb[1][1][1] = -A3;
+  } else {
+    ddnb[0][0][0] = A2;  ddnb[0][0][1] = -A1;
+    ddnb[0][1][0] = -A1; ddnb[0][1][1] = -A3;
+    ddnb[1][0][0] = -A1; ddnb[1][0][1] = -A3;
+    ddnb[1][1][0] = -A3; ddnb[1][1][1] = -A4;
+  }
+  // NM(id, kd)
+  const double nm0 = id == 0 ? -sn : (id == 1 ? cs : 0.0);
+  const double nm1 = id == 0 ? cs : (id == 1 ? sn : 0.0);
+  const double nm2 = id == 2 ? 1.0 : 0.0;
+  vel = 0.0;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    dvel[j] = 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; l++) ddvel[j][l] = 0.0;
+  }
+#pragma unroll
+  for (int kd = 0; kd < 3; kd++) {
+    const double(*c)[kPartPerBlock] = cv + 13 * kd;
+    const double nmk = kd == 0 ? nm0 : (kd == 1 ? nm1 : nm2);
+    const double f = c[0][p];
+    const double df[3] = {c[1][p], c[2][p], c[3][p]};
+    vel = vel + f * nmk;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const double dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : 0.0;
+      dvel[j] = dvel[j] + df[j] * nmk + f * dn_j;
     }
-  for (int id = 0; id < 3; id++)
-    for (int jd = 0; jd < 3; jd++)
-      for (int ld = 0; ld < 3; ld++) {
-        double s = 0.0;
-        for (int kd = 0; kd < 3; kd++) {
-          double ddn = (ld < 2 && jd < 2 && id < 2 && kd < 2) ? DDN[ld][jd][id][kd] : 0.0;
-          s = s + ddff[kd][jd][ld] * NM[id][kd] + dff[kd][jd] * DN[ld][id][kd] + dff[kd][ld] * DN[jd][id][kd] +
-              ff[kd] * ddn;
-        }
-        ddvel[id][jd][ld] = s;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) {
+        const double ddf = c[4 + j + 3 * l][p];
+        const double dn_l = (kd < 2 && l < 2 && id < 2) ? dnb[l][kd < 2 ? kd : 0] : 0.0;
+        const double dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : 0.0;
+        const double d4 = (kd < 2 && l < 2 && j < 2 && id < 2) ? ddnb[l < 2 ? l : 0][j < 2 ? j : 0][kd < 2 ? kd : 0]
+                                                                : 0.0;
+        ddvel[j][l] = ddvel[j][l] + ddf * nmk + df[j] * dn_l + df[l] * dn_j + f * d4;
       }
+  }
 }
 
 #define PUo(ip, iv) ((size_t)((ip) - 1) + (size_t)naloc * ((iv) - 1))
 
-// one Euler substep of every live particle (part_tools.F90:517-959) and the
-// out-of-range test (:962-987)
-__global__ void __launch_bounds__(128) k_iter_part(PartGeo P, const double *__restrict__ q1,
-                                                   const double *__restrict__ q2, const double *__restrict__ q3,
-                                                   const double *__restrict__ tab, double *__restrict__ u,
-                                                   double *__restrict__ v, int *__restrict__ isfre,
-                                                   int *__restrict__ gone, int naloc, int nlast, int mode,
-                                                   double inv_st, double partdt, int serial, int *nremoved) {
-  int ip = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip > nlast || isfre[ip - 1] != 0) return;
-  double vel[3], dvel[3][3], ddvel[3][3][3];
-  int cell[3];
-  part_eval(P, q1, q2, q3, tab, u[PUo(ip, 1)], u[PUo(ip, 2)], u[PUo(ip, 3)], vel, dvel, ddvel, cell);
-  if (mode == 1) {  // tracer: dx/dt = u(x)
-    for (int i = 0; i < 3; i++) u[PUo(ip, 1 + i)] = u[PUo(ip, 1 + i)] + vel[i] * partdt;
-    for (int i = 0; i < 3; i++) u[PUo(ip, 4 + i)] = vel[i];
-  } else {
-    double jac[3][3];
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) jac[i][j] = u[PUo(ip, 6 + (i + 1) + 3 * j)];
-    // positions and velocities
-    double ddt_pos[3], ddt_vel[3];
-    for (int i = 0; i < 3; i++) {
-      ddt_pos[i] = u[PUo(ip, 4 + i)];
-      ddt_vel[i] = inv_st * (vel[i] - u[PUo(ip, 4 + i)]);
+// One Euler substep of every live particle (part_tools.F90:517-959) and the
+// out-of-range test and removal (:962-987).
+__global__ void __launch_bounds__(96) k_iter_part(PartGeo P, const double *__restrict__ q1,
+                                                  const double *__restrict__ q2, const double *__restrict__ q3,
+                                                  double *__restrict__ u, double *__restrict__ v,
+                                                  int *__restrict__ isfre, int *__restrict__ gone, int naloc,
+                                                  int nlast, int mode, double inv_st, double partdt, int serial,
+                                                  int *nremoved) {
+  __shared__ PartShared S;
+  const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ip = 1 + blockIdx.x * kPartPerBlock + p;
+  const bool live = ip <= nlast && isfre[ip - 1] == 0;
+  double r = 0.0, theta = 0.0;
+  if (live) {
+    const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
+    int cell[3];
+    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta);
+    if (mode != 1) {
+#pragma unroll
+      for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
+#pragma unroll
+      for (int jk = 0; jk < 9; jk++) S.hes[w + 3 * jk][p] = u[PUo(ip, 25 + w + 3 * jk)];
     }
-    // Jacobian and its rate
-    double ddt_jac[9], ddt_jrt[9];
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) {
-        int o = i + 3 * j;
-        ddt_jac[o] = u[PUo(ip, 16 + o)];
-        double sumj = jac[0][j] * dvel[i][0] + jac[1][j] * dvel[i][1] + jac[2][j] * dvel[i][2];
-        ddt_jrt[o] = inv_st * (sumj - u[PUo(ip, 16 + o)]);
-      }
-    // Hessian and its rate
-    double ddt_hrt[27];
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++)
-        for (int k = 0; k < 3; k++) {
-          int o = i + 3 * j + 9 * k;
-          double h0 = u[PUo(ip, 25 + 0 + 3 * j + 9 * k)], h1 = u[PUo(ip, 25 + 1 + 3 * j + 9 * k)],
-                 h2 = u[PUo(ip, 25 + 2 + 3 * j + 9 * k)];
-          double sumh = h0 * dvel[i][0] + h1 * dvel[i][1] + h2 * dvel[i][2] +
-                        jac[0][j] * jac[0][k] * ddvel[i][0][0] + jac[1][j] * jac[0][k] * ddvel[i][1][0] +
-                        jac[2][j] * jac[0][k] * ddvel[i][2][0] + jac[0][j] * jac[1][k] * ddvel[i][0][1] +
-                        jac[0][j] * jac[2][k] * ddvel[i][0][2] + jac[1][j] * jac[1][k] * ddvel[i][1][1] +
-                        jac[1][j] * jac[2][k] * ddvel[i][1][2] + jac[2][j] * jac[1][k] * ddvel[i][2][1] +
-                        jac[2][j] * jac[2][k] * ddvel[i][2][2];
-          ddt_hrt[o] = inv_st * (sumh - u[PUo(ip, 52 + o)]);
-        }
-    // Euler update (part_tools.F90:926-930), in the reference's variable order
-    for (int i = 0; i < 3; i++) u[PUo(ip, 1 + i)] = u[PUo(ip, 1 + i)] + ddt_pos[i] * partdt;
-    for (int i = 0; i < 3; i++) u[PUo(ip, 4 + i)] = u[PUo(ip, 4 + i)] + ddt_vel[i] * partdt;
-    for (int o = 0; o < 9; o++) u[PUo(ip, 7 + o)] = u[PUo(ip, 7 + o)] + ddt_jac[o] * partdt;
-    for (int o = 0; o < 9; o++) u[PUo(ip, 16 + o)] = u[PUo(ip, 16 + o)] + ddt_jrt[o] * partdt;
-    for (int o = 0; o < 27; o++) {
-      double hrt = u[PUo(ip, 52 + o)];
-      u[PUo(ip, 25 + o)] = u[PUo(ip, 25 + o)] + hrt * partdt;  // d(hes)/dt = hrt (old value)
-    }
-    for (int o = 0; o < 27; o++) u[PUo(ip, 52 + o)] = u[PUo(ip, 52 + o)] + ddt_hrt[o] * partdt;
   }
-  for (int i = 0; i < 3; i++) u[PUo(ip, 79 + i)] = vel[i];
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) u[PUo(ip, 78 + 3 + (i + 1) + 3 * j)] = dvel[i][j];
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++)
-      for (int k = 0; k < 3; k++) u[PUo(ip, 78 + 3 + 9 + (i + 1) + 3 * j + 9 * k)] = ddvel[i][j][k];
+  __syncthreads();
+  double pw = 0.0;
+  if (live) {
+    double vel, dvel[3], ddvel[3][3];
+    part_cart_row(r, theta, w, S.cv, p, vel, dvel, ddvel);
+    pw = u[PUo(ip, 1 + w)];
+    if (mode == 1) {  // tracer: dx/dt = u(x)
+      pw = pw + vel * partdt;
+      u[PUo(ip, 1 + w)] = pw;
+      u[PUo(ip, 4 + w)] = vel;
+    } else {
+      // Stokes drag on position, velocity, Jacobian and Hessian
+      // (part_tools.F90:836-870), explicit Euler (:926-930), row w
+      const double pv = u[PUo(ip, 4 + w)];
+      pw = pw + pv * partdt;
+      u[PUo(ip, 1 + w)] = pw;
+      u[PUo(ip, 4 + w)] = pv + (inv_st * (vel - pv)) * partdt;
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const double jr = u[PUo(ip, 16 + w + 3 * j)];
+        const double sumj = S.jac[0 + 3 * j][p] * dvel[0] + S.jac[1 + 3 * j][p] * dvel[1] +
+                            S.jac[2 + 3 * j][p] * dvel[2];
+        u[PUo(ip, 7 + w + 3 * j)] = S.jac[w + 3 * j][p] + jr * partdt;
+        u[PUo(ip, 16 + w + 3 * j)] = jr + (inv_st * (sumj - jr)) * partdt;
+      }
+#pragma unroll 1
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          const int oj = 3 * j + 9 * k;
+          const double jc0 = S.jac[0 + 3 * j][p], jc1 = S.jac[1 + 3 * j][p], jc2 = S.jac[2 + 3 * j][p];
+          const double kc0 = S.jac[0 + 3 * k][p], kc1 = S.jac[1 + 3 * k][p], kc2 = S.jac[2 + 3 * k][p];
+          const double h0 = S.hes[0 + oj][p], h1 = S.hes[1 + oj][p], h2 = S.hes[2 + oj][p];
+          const double hw = w == 0 ? h0 : (w == 1 ? h1 : h2);
+          const double hr = u[PUo(ip, 52 + w + oj)];
+          const double sumh = h0 * dvel[0] + h1 * dvel[1] + h2 * dvel[2] + jc0 * kc0 * ddvel[0][0] +
+                              jc1 * kc0 * ddvel[1][0] + jc2 * kc0 * ddvel[2][0] + jc0 * kc1 * ddvel[0][1] +
+                              jc0 * kc2 * ddvel[0][2] + jc1 * kc1 * ddvel[1][1] + jc1 * kc2 * ddvel[1][2] +
+                              jc2 * kc1 * ddvel[2][1] + jc2 * kc2 * ddvel[2][2];
+          u[PUo(ip, 25 + w + oj)] = hw + hr * partdt;
+          u[PUo(ip, 52 + w + oj)] = hr + (inv_st * (sumh - hr)) * partdt;
+        }
+    }
+    // fluid velocity and its derivatives at the particle (part_tools.F90:940-958)
+    u[PUo(ip, 79 + w)] = vel;
+#pragma unroll
+    for (int j = 0; j < 3; j++) u[PUo(ip, 82 + w + 3 * j)] = dvel[j];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) u[PUo(ip, 91 + w + 3 * j + 9 * k)] = ddvel[j][k];
+    S.pos[w][p] = pw;
+  }
+  __syncthreads();
+  if (!live) return;
   // out of the domain: removed (single rank: nothing migrates)
-  double x = u[PUo(ip, 1)], y = u[PUo(ip, 2)], z = u[PUo(ip, 3)];
-  double r = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
-  if ((z > P.zmax) || (z < 0.0) || (r > P.rmax) || (r < 0.0)) {
-    for (int iv = 1; iv <= 117; iv++) u[PUo(ip, iv)] = 0.0;
-    for (int iv = 0; iv < 3; iv++) v[(size_t)(ip - 1) + (size_t)naloc * iv] = 0.0;
-    isfre[ip - 1] = 1;
-    gone[ip - 1] = serial;
-    atomicAdd(nremoved, 1);
+  const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+  const double rp = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
+  if ((z > P.zmax) || (z < 0.0) || (rp > P.rmax) || (rp < 0.0)) {
+#pragma unroll 1
+    for (int iv = 1 + 39 * w; iv <= 39 * (w + 1); iv++) u[PUo(ip, iv)] = 0.0;
+    if (w == 0) {
+#pragma unroll
+      for (int iv = 0; iv < 3; iv++) v[(size_t)(ip - 1) + (size_t)naloc * iv] = 0.0;
+      isfre[ip - 1] = 1;
+      gone[ip - 1] = serial;
+      atomicAdd(nremoved, 1);
+    }
   }
 }
 
 // interpolation at arbitrary points (the dertest known answers)
-__global__ void k_part_probe(PartGeo P, const double *__restrict__ q1, const double *__restrict__ q2,
-                             const double *__restrict__ q3, const double *__restrict__ tab,
-                             const double *__restrict__ xyz, int n, double *__restrict__ out,
-                             int *__restrict__ cells) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double vel[3], dvel[3][3], ddvel[3][3][3];
-  int cell[3];
-  part_eval(P, q1, q2, q3, tab, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], vel, dvel, ddvel, cell);
+__global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__restrict__ q1,
+                                                   const double *__restrict__ q2, const double *__restrict__ q3,
+                                                   const double *__restrict__ xyz, int n, double *__restrict__ out,
+                                                   int *__restrict__ cells) {
+  __shared__ double cv[39][kPartPerBlock];
+  const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kPartPerBlock + p;
+  const bool act = i < n;
+  double r = 0.0, theta = 0.0;
+  if (act) {
+    const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+    int cell[3];
+    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta);
+    if (w == 0)
+      for (int a = 0; a < 3; a++) cells[3 * (size_t)i + a] = cell[a];
+  }
+  __syncthreads();
+  if (!act) return;
+  double vel, dvel[3], ddvel[3][3];
+  part_cart_row(r, theta, w, cv, p, vel, dvel, ddvel);
   double *o = out + 39 * (size_t)i;
-  for (int a = 0; a < 3; a++) o[a] = vel[a];
-  for (int b = 0; b < 3; b++)
-    for (int a = 0; a < 3; a++) o[3 + a + 3 * b] = dvel[a][b];
+  o[w] = vel;
+  for (int b = 0; b < 3; b++) o[3 + w + 3 * b] = dvel[b];
   for (int c = 0; c < 3; c++)
-    for (int b = 0; b < 3; b++)
-      for (int a = 0; a < 3; a++) o[12 + a + 3 * b + 9 * c] = ddvel[a][b][c];
-  for (int a = 0; a < 3; a++) cells[3 * i + a] = cell[a];
+    for (int b = 0; b < 3; b++) o[12 + w + 3 * b + 9 * c] = ddvel[b][c];
 }
 
-// The least-squares operator mint = (X^T X)^{-1} X^T of the 27-point stencil
-// for the basis (t, r, z, t^2, tr, r^2, rz, z^2, zt) and the offsets xint, in
-// the reduced fractions of its closed form (part_tools.F90:295-357).
-static void build_tables(double dx, double dy, double dz, std::vector<double> &tab) {
-  tab.assign(243 + 81, 0.0);
-  double *mint = tab.data(), *xint = tab.data() + 243;
-  double d[3] = {dx, dy, dz};
-  for (int i3 = -1; i3 <= 1; i3++)
-    for (int i2 = -1; i2 <= 1; i2++)
-      for (int i1 = -1; i1 <= 1; i1++) {
-        int iv = (i1 + 1) + 3 * (i2 + 1) + 9 * (i3 + 1);
-        int o[3] = {i1, i2, i3};
-        for (int a = 0; a < 3; a++) xint[iv + 27 * a] = o[a] == 0 ? 0.0 : o[a] * d[a];
-        for (int a = 0; a < 3; a++) {  // linear rows: o / (18 d)
-          double val = 0.0;
-          if (o[a] == 1) val = 1.0 / (18.0 * d[a]);
-          if (o[a] == -1) val = -(1.0 / (18.0 * d[a]));
-          mint[a + 9 * iv] = val;
+// PartCoef from the mesh spacings, each entry computed as the reference's
+// reduced fraction (part_tools.F90:295-357)
+static void part_coef(double d1, double d2, double d3, PartCoef &C) {
+  const double d[3] = {d1, d2, d3};
+  for (int a = 0; a < 3; a++) C.lin[a] = 1.0 / (18.0 * d[a]);
+  for (int a = 0; a < 3; a++)
+    for (int pat = 0; pat < 8; pat++) {
+      int na = (pat >> 2) & 1, nb = (pat >> 1) & 1, nc = pat & 1;
+      int num = 5 * na - 2 * nb - 2 * nc, den = 42;
+      double val = 0.0;
+      if (num != 0) {
+        int g = std::abs(num), h = den;
+        while (h) {
+          int t = g % h;
+          g = h;
+          h = t;
         }
-        const int sq_row[3] = {3, 5, 7};
-        for (int a = 0; a < 3; a++) {  // square rows: (5[o_a] - 2[o_b] - 2[o_c]) / (42 d_a^2)
-          int num = 5 * (o[a] != 0) - 2 * (o[(a + 1) % 3] != 0) - 2 * (o[(a + 2) % 3] != 0), den = 42;
-          double val = 0.0;
-          if (num != 0) {
-            int gcd = std::abs(num), h = den;
-            while (h) {
-              int t = gcd % h;
-              gcd = h;
-              h = t;
-            }
-            num /= gcd;
-            den /= gcd;
-            val = num > 0 ? (double)num / ((double)den * (d[a] * d[a])) : -((double)(-num) / ((double)den * (d[a] * d[a])));
-          }
-          mint[sq_row[a] + 9 * iv] = val;
-        }
-        const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0}, row[3] = {4, 6, 8};
-        for (int q = 0; q < 3; q++) {  // cross rows: o_a o_b / (12 d_a d_b)
-          int sgn = o[pa[q]] * o[pb[q]];
-          double den = q == 2 ? 12.0 * d[0] * d[2] : 12.0 * d[pa[q]] * d[pb[q]];
-          double val = 0.0;
-          if (sgn == 1) val = 1.0 / den;
-          if (sgn == -1) val = -(1.0 / den);
-          mint[row[q] + 9 * iv] = val;
-        }
+        num /= g;
+        den /= g;
+        val = num > 0 ? (double)num / ((double)den * (d[a] * d[a]))
+                      : -((double)(-num) / ((double)den * (d[a] * d[a])));
       }
+      C.sq[a][pat] = val;
+    }
+  C.cr[0] = 1.0 / (12.0 * d[0] * d[1]);
+  C.cr[1] = 1.0 / (12.0 * d[1] * d[2]);
+  C.cr[2] = 1.0 / (12.0 * d[0] * d[2]);
+  C.pr[0] = d1;
+  C.pr[1] = d2;
+  C.pr[2] = d3;
+  C.pr[3] = d1 * d1;
+  C.pr[4] = d1 * d2;
+  C.pr[5] = d2 * d2;
+  C.pr[6] = d2 * d3;
+  C.pr[7] = d3 * d3;
+  C.pr[8] = d3 * d1;
 }
 
 }  // namespace vr
@@ -435,6 +543,7 @@ static int part_geo(vr_ctx *c, PartGeo &P) {
   P.thm = c->part_mesh + (c->geo.nth + 2);
   P.zm = c->part_mesh + 2 * (c->geo.nth + 2);
   P.zc = c->part_mesh + 2 * (c->geo.nth + 2) + (c->geo.nz + 3);
+  part_coef(c->geo.dtheta, c->geo.dr, c->geo.dz, P.C);
   return VR_OK;
 }
 
@@ -482,12 +591,9 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
   p->c = (double)(1.0e6f * (0.02f * 0.02f * 0.02f));
   static const int nsub[10] = {20, 10, 10, 5, 5, 5, 5, 5, 5, 5};
   p->nsubdt = (id >= 1 && id <= 10) ? nsub[id - 1] : 5;
-  std::vector<double> tab;
-  build_tables(c->geo.dtheta, c->geo.dr, c->geo.dz, tab);
   size_t nu = (size_t)naloc * 117, nv = (size_t)naloc * 3;
   bool ok = cudaMalloc(&p->u, nu * sizeof(double)) == cudaSuccess &&
             cudaMalloc(&p->v, nv * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&p->tab, tab.size() * sizeof(double)) == cudaSuccess &&
             cudaMalloc(&p->isfre, naloc * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&p->gone, naloc * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&p->d_nremoved, sizeof(int)) == cudaSuccess;
@@ -500,7 +606,6 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
   cudaMemset(p->isfre, 0, naloc * sizeof(int));
   cudaMemset(p->gone, 0xff, naloc * sizeof(int));
   cudaMemset(p->d_nremoved, 0, sizeof(int));
-  cudaMemcpy(p->tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   p->ifree.assign(naloc + 2, 0);
   p->h_isfre.assign(naloc + 1, 0);
   VR_CUDA(c, cudaDeviceSynchronize());
@@ -520,7 +625,6 @@ extern "C" int vr_part_destroy(vr_part *p) {
   }
   cudaFree(p->u);
   cudaFree(p->v);
-  cudaFree(p->tab);
   cudaFree(p->isfre);
   cudaFree(p->gone);
   cudaFree(p->d_nremoved);
@@ -654,7 +758,7 @@ int vr::vr_part_enqueue(vr_part *p) {
   for (int s = 0; s < p->nsubdt; s++) {
     if (p->nlast <= 0) break;
     LaunchScope ls(c, PK_PART);
-    k_iter_part<<<(p->nlast + 127) / 128, 128, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], p->tab, p->u, p->v,
+    k_iter_part<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
                                                               p->isfre, p->gone, p->naloc, p->nlast, p->mode,
                                                               inv_st, partdt, p->serial++, p->d_nremoved);
     cudaError_t e = cudaGetLastError();
@@ -744,7 +848,7 @@ extern "C" int vr_part_probe(vr_part *p, const double *xyz, int32_t n, double *o
     rc = VR_ERR_OOM;
   if (!rc && cudaMemcpy(dx, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice)) rc = VR_ERR_CUDA;
   if (!rc) {
-    k_part_probe<<<(n + 127) / 128, 128, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], p->tab, dx, n, dout, dcell);
+    k_part_probe<<<(n + kPartPerBlock - 1) / kPartPerBlock, 96, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], dx, n, dout, dcell);
     if (cudaGetLastError() || cudaStreamSynchronize(c->stream)) rc = VR_ERR_CUDA;
   }
   if (!rc && cudaMemcpy(out, dout, sizeof(double) * 39 * n, cudaMemcpyDeviceToHost)) rc = VR_ERR_CUDA;
