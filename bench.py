@@ -6,8 +6,10 @@ vortex ring (R = 1, sigma = 0.2, Gamma = 1, z0 = 3, seeded noise 1e-4) on the
 cylindrical staggered grid Nr x Ntheta x Nz = 256 x 128 x 512, r in [0, 4],
 z in [0, 12], Re = 3000, dt = 5e-4, free slip at r = 4 (slip = 1), the
 reference's z boundaries (wall + convective outflow) and the discrete theta
-wavenumber in the Poisson solve (max |div u| at round-off).  One step = one
-RK3 time step (3 substeps).  FP64.
+wavenumber in the Poisson solve (max |div u| at round-off), with 1,048,576
+tracer particles uniform in area over r in [0.3, 1.7], z in [2, 4] (seed 0).
+One step = one RK3 time step: the particle advance (iter_part, nsubdt Euler
+substeps) and the three field substeps.  FP64.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,8 +36,11 @@ METRIC = "Mcell-RK3-steps/s at 256×128×512, mixed vs FP64 on B200 at max|div u
 UNIT = "Mcell-RK3-steps/s"
 NTH, NR, NZ = 128, 256, 512
 RMAX, ZMAX, DT, RE, SLIP = 4.0, 12.0, 5e-4, 3000.0, 1.0
+NPART, PART_CLASS, PART_MODE = 1048576, 8, 1  # tracers (u_p = u(x_p)), class 8: nsubdt 5
+PART_R, PART_Z = (0.3, 1.7), (2.0, 4.0)
 WORKLOAD = ("vortex ring, Nr x Ntheta x Nz = 256 x 128 x 512, r<=4, z<=12, Re 3000, dt 5e-4, "
-            "free slip, reference z boundaries, discrete theta wavenumber, FP64")
+            "free slip, reference z boundaries, discrete theta wavenumber, 1,048,576 tracer "
+            "particles (5 Euler substeps per step), FP64")
 # algorithmic 8-byte words per interior cell and substep, by kernel family
 # (each field word read or written once per logical phase of the reference):
 #   A rhs 15 | B theta 6, r 7, z 8 | C divq 4 | D fft 4, dct 4, radial 2 | E upsol 7 | F uppres 9
@@ -112,22 +117,50 @@ def ring_state():
     return ring_fields(NTH, NR, NZ, RMAX, ZMAX, R=1.0, sigma=0.2, gamma=1.0, z0=3.0, noise=1e-4, seed=0)
 
 
-def cpu_reference(steps, budget_s, q=None):
-    """The CPU restatement on the same workload, all host threads; returns
-    (Mcell-steps/s, steps timed, threads)."""
+def particle_state(n, seed=0):
+    """u(n, 117), v(n, 3) of n particles injected at rest (injc_part layout)."""
+    import numpy as np
+    from vring_b200.synthetic import annulus_particles
+    x, y, z = annulus_particles(n, PART_R[0], PART_R[1], PART_Z[0], PART_Z[1], seed=seed)
+    u = np.zeros((n, 117), order="F")
+    v = np.zeros((n, 3), order="F")
+    u[:, 0], u[:, 1], u[:, 2] = x, y, z
+    u[:, 6] = u[:, 10] = u[:, 14] = 1.0
+    return u, v
+
+
+def cpu_reference(steps, budget_s, q=None, part_sample=65536):
+    """The CPU restatement on the same workload, all host threads.  The field
+    steps run at full size; the particle advance runs on the first
+    part_sample particles of the same cloud and is scaled to 1,048,576.
+    Returns (Mcell-steps/s, steps timed, threads, sample text)."""
     from oracle import oracle as O
     q = q if q is not None else ring_state()
     o = O.Oracle(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, 1, 0, 0)
     for n, a in zip(("q1", "q2", "q3"), q):
         o.field(n)[...] = a
-    done, t0 = 0, time.perf_counter()
+    pu, pv = particle_state(NPART)
+    op = O.OraclePart(o, PART_CLASS, part_sample, PART_MODE)
+    op.u[...] = pu[:part_sample]
+    op.v[...] = pv[:part_sample]
+    op._s.nlast = op._s.npart = part_sample
+    done, t_field, t_part, t0 = 0, 0.0, 0.0, time.perf_counter()
     while done < steps:
+        ta = time.perf_counter()
+        op.iter_part(1)
+        tb = time.perf_counter()
         o.iterate(1)
+        tc = time.perf_counter()
+        t_part += tb - ta
+        t_field += tc - tb
         done += 1
-        if time.perf_counter() - t0 > budget_s:
+        if tc - t0 > budget_s:
             break
-    el = time.perf_counter() - t0
-    return NTH * NR * NZ * done / el / 1e6, done, os.cpu_count()
+    step_s = (t_field + t_part * NPART / part_sample) / done
+    sample = ("%d RK3 steps of the full 256x128x512 field workload plus the particle advance of "
+              "%d of the 1,048,576 particles scaled by %d (CPU FP64 restatement, OpenMP, %d threads)"
+              % (done, part_sample, NPART // part_sample, os.cpu_count()))
+    return NTH * NR * NZ / step_s / 1e6, done, os.cpu_count(), sample
 
 
 def run_reference(args):
@@ -138,14 +171,13 @@ def run_reference(args):
     # untimed warm-up bounded to one step, then a bounded timed sample
     if args.warmup > 0:
         cpu_reference(1, 1e9, q)
-    val, done, cores = cpu_reference(args.steps, 150.0, q)
+    val, done, cores, sample = cpu_reference(args.steps, 150.0, q)
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ]},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "%d RK3 steps of the full 256x128x512 workload (CPU FP64 "
-                                       "restatement, OpenMP, %d threads)" % (done, cores)},
+                             "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -154,7 +186,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -192,6 +224,11 @@ def main():
     run = V.Run(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, theta_wavenumber="modified", device=local)
     for n, a in zip(("q1", "q2", "q3"), q):
         run.set(n, a)
+    part = V.Part(run, PART_CLASS, NPART, PART_MODE)
+    pu, pv = particle_state(NPART)
+    part.set_state(pu, pv, None, NPART)
+    del pu, pv
+    part.attach(True)  # advanced by vr_iterate before substep 1 of every step
     # a dedicated (non-default) stream shared by the library and the events
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -251,8 +288,9 @@ def main():
         bytes_q = sum(p.numel() for p in pins) * 8
         e2e = {"value": world * ncell * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": bytes_q, "d2h_bytes_per_step": bytes_q,
-               "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1), "
-                       "q1,q2,q3 device->host; other state stays resident in the context"}
+               "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1) "
+                       "(particles included), q1,q2,q3 device->host; pressure, RK history and "
+                       "particle state stay resident in the context"}
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
@@ -264,13 +302,21 @@ def main():
     traffic = traffic_table().get(fam)
     step_ideal_ms = WORDS_PER_CELL_STEP * 8 * ncell / (peak * 1e9) * 1e3
 
+    part_ms = prof.get("part", (0.0, 0))[0]
+    counts = part.counts
+    particles = {"n": NPART, "mode": "tracer", "class": PART_CLASS, "nsubdt": part.nsubdt,
+                 "live_after": counts["npart"], "ms_per_step": part_ms / args.steps,
+                 "share_of_step": part_ms / ms if ms > 0 else None,
+                 "value": NPART * args.steps / (part_ms / 1e3) if part_ms > 0 else None,
+                 "unit": "particle-steps/s (particle kernel time)",
+                 "substeps_per_s": NPART * part.nsubdt * args.steps / (part_ms / 1e3) if part_ms > 0 else None}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ],
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"},
-            "max_div_u": maxdiv, "nonfinite": nonfinite,
+            "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak,
@@ -281,12 +327,12 @@ def main():
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        val, done, cores = cpu_reference(3, 20.0, q)
+        val, done, cores, sample = cpu_reference(3, 20.0, q)
         line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": "%d RK3 steps of the full workload (CPU FP64 restatement, "
-                                          "OpenMP, %d threads)" % (done, cores)}
+                                "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    part.close()
     run.close()
     if dist is not None:
         dist.barrier()

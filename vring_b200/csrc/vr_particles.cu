@@ -92,6 +92,7 @@ struct PartCoef {
   double sq[3][8];  // rows t^2, r^2, z^2 at pattern 4[o_a != 0] + 2[o_b != 0] + [o_c != 0], b = a+1, c = a+2
   double cr[3];     // rows tr, rz, zt: o_a o_b / (12 d_a d_b)
   double pr[9];     // d1, d2, d3, d1 d1, d1 d2, d2 d2, d2 d3, d3 d3, d3 d1
+  double ymax_one_pass;  // max |y| below which the second pass is rounding noise under the stop tolerance
 };
 
 struct PartGeo {
@@ -149,8 +150,14 @@ __device__ __forceinline__ void ls_pass(const PartCoef &C, const double (&y)[27]
   }
 }
 
-// quadratic coefficients of one component: Richardson iteration from zero,
-// at most 100 passes, stopping when |mp| < 1e-6 (single-precision literal)
+// Quadratic coefficients of one component: the reference's Richardson
+// iteration from zero, at most 100 passes, stopping when |mp| < 1e-6
+// (single-precision literal).  mint X = I, so the first pass is already the
+// least-squares solution and the second pass only adds the rounding error of
+// the first, bounded by a multiple of eps |mint| max|y|.  When max|y| is below
+// the bound at which that correction stays under the stop tolerance
+// (C.ymax_one_pass), the reference stops after the second pass with a
+// rounding-level change; the kernel stops after the first.
 __device__ __forceinline__ void ls_fit(const PartCoef &C, const double (&y)[27], double (&a)[9]) {
   double mp[9];
   ls_pass<true>(C, y, a, mp);
@@ -161,6 +168,10 @@ __device__ __forceinline__ void ls_fit(const PartCoef &C, const double (&y)[27],
     nn += mp[i] * mp[i];
   }
   if (sqrt(nn) < (double)0.000001f) return;
+  double ym = 0.0;
+#pragma unroll
+  for (int k = 0; k < 27; k++) ym = fmax(ym, fabs(y[k]));
+  if (ym < C.ymax_one_pass) return;  // NaN/Inf fail the test and take the full loop
 #pragma unroll 1
   for (int iint = 2; iint <= 100; iint++) {
     ls_pass<false>(C, y, a, mp);
@@ -195,7 +206,8 @@ struct PartShared {
 // rows of M FI, part_tools.F90:653-683) to cv[13 kd ..][p].
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
                                                double y, double z, double (*cv)[kPartPerBlock], int p,
-                                               int (&cell)[3], double &r, double &theta) {
+                                               int (&cell)[3], double &r, double &theta, double &sn,
+                                               double &cs) {
   int it, ir, iz;
   part_cell(P, x, y, z, it, ir, iz, r, theta);
   // keep the mesh lookups inside the stored vectors for points off the mesh
@@ -264,9 +276,8 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   const double fz = a[2] + drp * a[6] + 2.0 * dzp * a[7] + dtp * a[8];
   const double ftt = 2.0 * a[3], ftr = drp * a[4], ftz = dzp * a[8], frt = a[4], frr = 2.0 * a[5];
   const double frz = a[6], fzt = a[8], fzr = a[6], fzz = 2.0 * a[7];
-  double sn, cs, sn2, cs2;
   sincos(theta, &sn, &cs);
-  sincos(2.0 * theta, &sn2, &cs2);
+  const double sn2 = 2.0 * sn * cs, cs2 = (cs - sn) * (cs + sn);  // sin 2theta, cos 2theta
   const double ir1 = 1.0 / r, ir2 = 1.0 / (r * r);
   const double m_snr = -sn * ir1, m_csr = cs * ir1;
   const double m30 = sn2 * ir2, m31 = sn * sn * ir1, m33 = sn * sn * ir2, m34 = -cs * sn * ir1, m37 = cs * cs;
@@ -291,10 +302,9 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
 // Row id of the Cartesian velocity, gradient and Hessian from the three
 // fitted components (part_tools.F90:730-797), in the reference's summation
 // order over components.
-__device__ __forceinline__ void part_cart_row(double r, double theta, int id, const double (*cv)[kPartPerBlock],
-                                              int p, double &vel, double (&dvel)[3], double (&ddvel)[3][3]) {
-  double sn, cs;
-  sincos(theta, &sn, &cs);
+__device__ __forceinline__ void part_cart_row(double r, double sn, double cs, int id,
+                                              const double (*cv)[kPartPerBlock], int p, double &vel,
+                                              double (&dvel)[3], double (&ddvel)[3][3]) {
   const double rs = r > (double)0.000001f ? r : (double)0.000001f;
   const double irs = 1.0 / rs, irs2 = 1.0 / (rs * rs);
   const double A1 = sn * (-2.0 * (cs * cs) + sn * sn) * irs2, A2 = -3.0 * cs * (sn * sn) * irs2;
@@ -366,7 +376,7 @@ __device__ __forceinline__ void part_cart_row(double r, double theta, int id, co
 
 // One Euler substep of every live particle (part_tools.F90:517-959) and the
 // out-of-range test and removal (:962-987).
-__global__ void __launch_bounds__(96) k_iter_part(PartGeo P, const double *__restrict__ q1,
+__global__ void __launch_bounds__(96, 5) k_iter_part(PartGeo P, const double *__restrict__ q1,
                                                   const double *__restrict__ q2, const double *__restrict__ q3,
                                                   double *__restrict__ u, double *__restrict__ v,
                                                   int *__restrict__ isfre, int *__restrict__ gone, int naloc,
@@ -376,11 +386,11 @@ __global__ void __launch_bounds__(96) k_iter_part(PartGeo P, const double *__res
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ip = 1 + blockIdx.x * kPartPerBlock + p;
   const bool live = ip <= nlast && isfre[ip - 1] == 0;
-  double r = 0.0, theta = 0.0;
+  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0;
   if (live) {
     const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
     int cell[3];
-    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta);
+    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs);
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -392,7 +402,7 @@ __global__ void __launch_bounds__(96) k_iter_part(PartGeo P, const double *__res
   double pw = 0.0;
   if (live) {
     double vel, dvel[3], ddvel[3][3];
-    part_cart_row(r, theta, w, S.cv, p, vel, dvel, ddvel);
+    part_cart_row(r, sn, cs, w, S.cv, p, vel, dvel, ddvel);
     pw = u[PUo(ip, 1 + w)];
     if (mode == 1) {  // tracer: dx/dt = u(x)
       pw = pw + vel * partdt;
@@ -468,18 +478,18 @@ __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__re
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * kPartPerBlock + p;
   const bool act = i < n;
-  double r = 0.0, theta = 0.0;
+  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0;
   if (act) {
     const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
     int cell[3];
-    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta);
+    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs);
     if (w == 0)
       for (int a = 0; a < 3; a++) cells[3 * (size_t)i + a] = cell[a];
   }
   __syncthreads();
   if (!act) return;
   double vel, dvel[3], ddvel[3][3];
-  part_cart_row(r, theta, w, cv, p, vel, dvel, ddvel);
+  part_cart_row(r, sn, cs, w, cv, p, vel, dvel, ddvel);
   double *o = out + 39 * (size_t)i;
   o[w] = vel;
   for (int b = 0; b < 3; b++) o[3 + w + 3 * b] = dvel[b];
@@ -523,6 +533,17 @@ static void part_coef(double d1, double d2, double d3, PartCoef &C) {
   C.pr[6] = d2 * d3;
   C.pr[7] = d3 * d3;
   C.pr[8] = d3 * d1;
+  // Second-pass correction: |mp2_i| <~ 8000 eps |mint_i| max|y| (the first
+  // pass's own rounding plus that of the residual X a - y, whose terms are
+  // each at most 30 max|y|); the threshold keeps sqrt(sum mp2^2) below 1e-7,
+  // a tenth of the stop tolerance.
+  double mmax = 0.0;
+  for (int a = 0; a < 3; a++) {
+    mmax = std::max(mmax, C.lin[a]);
+    mmax = std::max(mmax, C.cr[a]);
+    for (int pat = 0; pat < 8; pat++) mmax = std::max(mmax, std::fabs(C.sq[a][pat]));
+  }
+  C.ymax_one_pass = 1e-7 / (3.0 * 8000.0 * mmax * 2.220446049250313e-16);
 }
 
 }  // namespace vr
