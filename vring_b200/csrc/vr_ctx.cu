@@ -20,7 +20,8 @@ int set_err(vr_ctx *c, int code, const std::string &msg) {
   return code;
 }
 
-LaunchScope::LaunchScope(vr_ctx *ctx, int kind) : c(ctx), slot(-1) {
+LaunchScope::LaunchScope(vr_ctx *ctx, int kind, cudaStream_t stream)
+    : c(ctx), slot(-1), s(stream ? stream : ctx->stream) {
   c->nlaunch++;
   if (!c->prof_on) return;
   if (c->prof_used * 2 + 2 > c->prof_ev.size()) {
@@ -36,11 +37,11 @@ LaunchScope::LaunchScope(vr_ctx *ctx, int kind) : c(ctx), slot(-1) {
   }
   slot = (int)c->prof_used++;
   c->prof_kind[slot] = kind;
-  cudaEventRecord(c->prof_ev[2 * slot], c->stream);
+  cudaEventRecord(c->prof_ev[2 * slot], s);
 }
 
 LaunchScope::~LaunchScope() {
-  if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], c->stream);
+  if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], s);
 }
 
 // default-kind (real*4) literal of the reference, widened as gfortran does
@@ -841,12 +842,13 @@ extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
   VR_CUDA(c, cudaSetDevice(c->dev));
   for (int s = 0; s < nsteps; s++) {
     c->ntime = c->d.dt + c->ntime;
+    // loop.F90:65-70: particles advance once per step, before ucoeff, in the
+    // velocity at the start of the step
+    for (vr_part *p : c->parts) {
+      int rc = vr_part_enqueue(p, c->stream);
+      if (rc) return rc;
+    }
     for (int irk = 1; irk <= 3; irk++) {
-      if (irk == 1)  // loop.F90:65-70: particles advance once per step, before ucoeff
-        for (vr_part *p : c->parts) {
-          int rc = vr_part_enqueue(p);
-          if (rc) return rc;
-        }
       int rc = enqueue_substep(c, irk);
       if (rc) return rc;
     }

@@ -168,12 +168,14 @@ enum ProfKind {
 struct LaunchScope {
   vr_ctx *c;
   int slot;
-  LaunchScope(vr_ctx *ctx, int kind);
+  cudaStream_t s;
+  LaunchScope(vr_ctx *ctx, int kind, cudaStream_t stream = nullptr);
   ~LaunchScope();
 };
 
-// enqueue the nsubdt Euler substeps of one particle class (vr_particles.cu)
-int vr_part_enqueue(vr_part *p);
+// enqueue the nsubdt Euler substeps of one particle class on stream s
+// (vr_particles.cu)
+int vr_part_enqueue(vr_part *p, cudaStream_t s);
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);

@@ -770,7 +770,7 @@ extern "C" int vr_remv_part(vr_part *p, int32_t ip) {
 }
 
 // enqueue the nsubdt substeps of one call of iter_part
-int vr::vr_part_enqueue(vr_part *p) {
+int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
   vr_ctx *c = p->ctx;
   PartGeo P;
   part_geo(c, P);
@@ -778,8 +778,8 @@ int vr::vr_part_enqueue(vr_part *p) {
   double inv_st = 1.0 / p->st;
   for (int s = 0; s < p->nsubdt; s++) {
     if (p->nlast <= 0) break;
-    LaunchScope ls(c, PK_PART);
-    k_iter_part<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
+    LaunchScope ls(c, PK_PART, stream);
+    k_iter_part<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
                                                               p->isfre, p->gone, p->naloc, p->nlast, p->mode,
                                                               inv_st, partdt, p->serial++, p->d_nremoved);
     cudaError_t e = cudaGetLastError();
@@ -792,7 +792,7 @@ extern "C" int vr_iter_part(vr_part *p, int32_t irk) {
   if (!p) return VR_ERR_ARG;
   (void)irk;  // the reference advances particles at substep 1 only, with Euler
   VR_CUDA(p->ctx, cudaSetDevice(p->ctx->dev));
-  return vr_part_enqueue(p);
+  return vr_part_enqueue(p, p->ctx->stream);
 }
 
 extern "C" int vr_part_attach(vr_part *p, int32_t on) {
@@ -808,6 +808,7 @@ extern "C" int vr_part_set_state(vr_part *p, const double *u, const double *v, c
   if (!p || !u || !v || nlast < 0 || nlast > p->naloc) return VR_ERR_ARG;
   vr_ctx *c = p->ctx;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));  // queued steps may still advance this class
   VR_CUDA(c, cudaMemcpy(p->u, u, sizeof(double) * (size_t)p->naloc * 117, cudaMemcpyHostToDevice));
   VR_CUDA(c, cudaMemcpy(p->v, v, sizeof(double) * (size_t)p->naloc * 3, cudaMemcpyHostToDevice));
   std::vector<int> isf(p->naloc, 0);
