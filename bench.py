@@ -140,6 +140,7 @@ def cpu_reference(steps, budget_s, q=None, part_sample=65536):
     for n, a in zip(("q1", "q2", "q3"), q):
         o.field(n)[...] = a
     pu, pv = particle_state(NPART)
+    part_sample = min(part_sample, NPART)
     op = O.OraclePart(o, PART_CLASS, part_sample, PART_MODE)
     op.u[...] = pu[:part_sample]
     op.v[...] = pv[:part_sample]
@@ -191,7 +192,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NR", "NTHETA", "NZ"), default=None,
+                    help="smaller grid for profiling captures (not the benchmark workload)")
+    ap.add_argument("--nparticles", type=int, default=None,
+                    help="particle count for profiling captures (not the benchmark workload)")
     args = ap.parse_args()
+    global NR, NTH, NZ, NPART, WORKLOAD
+    if args.grid is not None or args.nparticles is not None:
+        if args.grid is not None:
+            NR, NTH, NZ = args.grid
+        if args.nparticles is not None:
+            NPART = args.nparticles
+        WORKLOAD = ("REDUCED profiling case (not the benchmark): vortex ring, Nr x Ntheta x Nz = "
+                    "%d x %d x %d, %d tracer particles, FP64" % (NR, NTH, NZ, NPART))
     if args.impl == "reference":
         return run_reference(args)
 
