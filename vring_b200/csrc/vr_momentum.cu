@@ -242,6 +242,127 @@ __global__ void __launch_bounds__(128) k_rhs(Geo g, Rk rk, RhsArgs a) {
   }
 }
 
+// Fused hdnl1-3 + RHS (INLINE_H path) with every distinct field value loaded
+// once: 27 samples of q1..q3, ru1..3 and prg1..3 per cell.  The arithmetic is
+// that of h1_at/h2_at/h3_at and k_rhs term by term; only the loads are shared.
+// A value that is only used on a boundary row/plane (k-1 at kc = 1, j-1 at
+// jc = 1) is still loaded from the ghost row/plane, which is allocated.
+__global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
+  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  const int jm = jc > 1 ? jc - 1 : 1;
+  const double *__restrict__ q1 = a.q.q1, *__restrict__ q2 = a.q.q2, *__restrict__ q3 = a.q.q3;
+  const int o = I3(g, ic, jc, kc);
+  const int di = ip - ic, dm = im - ic;  // theta neighbour offsets (periodic)
+  const int sj = g.nth, sk = g.pl;       // j and k strides
+  const int ojm = (jm - jc) * sj;        // jm row offset (0 on the axis row)
+  // q1
+  const double A1 = ld(q1 + o), A2 = ld(q1 + o + di), A3 = ld(q1 + o + dm), A4 = ld(q1 + o + sj);
+  const double A5 = ld(q1 + o + ojm), A6 = ld(q1 + o + sk), A7 = ld(q1 + o - sk);
+  const double A8 = ld(q1 + o + di - sj), A9 = ld(q1 + o + di - sk);
+  // q2
+  const double B1 = ld(q2 + o), B2 = ld(q2 + o + di), B3 = ld(q2 + o + dm), B4 = ld(q2 + o + sj);
+  const double B5 = ld(q2 + o - sj), B6 = ld(q2 + o + sk), B7 = ld(q2 + o - sk);
+  const double B8 = ld(q2 + o + dm + sj), B9 = ld(q2 + o + sj - sk);
+  // q3
+  const double C1 = ld(q3 + o), C2 = ld(q3 + o + di), C3 = ld(q3 + o + dm), C4 = ld(q3 + o + sj);
+  const double C5 = ld(q3 + o + ojm), C6 = ld(q3 + o + sk), C7 = ld(q3 + o - sk);
+  const double C8 = ld(q3 + o + dm + sk), C9 = ld(q3 + o - sj + sk);
+  const double ru1 = ld(a.ru[0] + o), ru2 = ld(a.ru[1] + o), ru3 = ld(a.ru[2] + o);
+  const double pg1 = ld(a.prg + IPRG(g, ic, jc, kc, 1)), pg2 = ld(a.prg + IPRG(g, ic, jc, kc, 2));
+  const double pg3 = ld(a.prg + IPRG(g, ic, jc, kc, 3));
+  const double are = rk.alm / g.re;
+  const bool do3 = kc >= 2, do2 = jc >= 2;
+  double h1, h2 = 0.0, h3 = 0.0, r1, r2 = 0.0, r3 = 0.0;
+  {  // hdnl1 (momentum_terms_swirl.F90:29-68)
+    const double q1c = A1, q1p = A2, q1m = A3;
+    double qnn = q1p + q1c, qss = q1m + q1c;
+    const double h11 = (qnn * qnn - qss * qss) * g.h1d11[jc];
+    const double q2cn = B4, q2mn = B8, q2c = B1, q2m = B3;
+    qnn = (q2cn + q2mn) * (A4 + q1c);
+    qss = (q1c + A5) * (q2c + q2m);
+    const double h12d = (qnn - qss) * g.h1d22d[jc];
+    qnn = (q1p + q1c) * (q2cn + q2c);
+    qss = (q1c + q1m) * (q2mn + q2m);
+    const double h12n = (qnn + qss) * g.h1d22n[jc];
+    qnn = 0.25 * (C6 + C8) * (A6 + q1c);
+    qss = kc == 1 ? 0.0 : 0.25 * (C1 + C3) * (q1c + A7);
+    const double h13 = (qnn - qss) * g.dx3;
+    const double d1q2 = ((q2cn + q2c) - (q2mn + q2m)) * g.h1dare[jc];
+    h1 = d1q2 - (h11 + (h12d + h12n) + h13);
+  }
+  {  // RHS q1 (step.F90:32-63)
+    const double qc = A1;
+    const double d11 = (A2 - 2.0 * qc + A3) * g.s1t11[jc];
+    const double d33 = kc == 1 ? 4.0 / 3.0 * (A6 - 3.0 * qc + 2.0 * 0.0) * g.dx3q : (A6 - 2.0 * qc + A7) * g.dx3q;
+    const double qnn = (A4 * g.irm[jc + 1] - qc * g.irm[jc]) * g.s1t2n[jc];
+    const double qss = (qc * g.irm[jc] - A5 * g.irm[jm]) * g.s1t2s[jc];
+    const double d22 = (qnn - qss) * g.s1t2c[jc];
+    r1 = (rk.gam * h1 + rk.rom * ru1 - rk.alm * pg1 + are * (d11 + d33 + d22)) * g.dt;
+  }
+  if (do3) {
+    {  // hdnl3 (momentum_terms_swirl.F90:150-171)
+      const double q3c = C1;
+      double qnn = (C4 + q3c) * (B4 + B9);
+      double qss = (C5 + q3c) * (B1 + B7);
+      const double h32 = (qnn - qss) * g.h1d22d[jc];
+      qnn = (q3c + C2) * (A2 + A9);
+      qss = (C3 + q3c) * (A1 + A7);
+      const double h31 = (qnn - qss) * g.h1d11[jc];
+      qnn = 0.25 * (q3c + C6) * (q3c + C6);
+      qss = 0.25 * (q3c + C7) * (q3c + C7);
+      const double h33 = (qnn - qss) * g.dx3;
+      h3 = -(h31 + h32 + h33);
+    }
+    // RHS q3 (step.F90:93-116)
+    const double qc = C1;
+    const double d11 = (C2 - 2.0 * qc + C3) * g.s1t11[jc];
+    const double d33 = (C6 - 2.0 * qc + C7) * g.dx3q;
+    const double qnn = (C4 - qc) * g.s3t2n[jc];
+    const double qss = (qc - C5) * g.s3t2s[jc];
+    const double d22 = qnn - qss;
+    r3 = (rk.gam * h3 + rk.rom * ru3 - rk.alm * pg3 + are * (d11 + d33 + d22)) * g.dt;
+  }
+  if (do2) {
+    {  // hdnl2 (momentum_terms_swirl.F90:94-128)
+      const double q1p = A2, q1pm = A8, q1c = A1, q1cm = A5, q2c = B1;
+      double qnn = (q1p + q1pm) * (B2 + q2c);
+      double qss = (q1c + q1cm) * (q2c + B3);
+      const double h21 = (qnn - qss) * g.h2d11[jc];
+      qnn = B4 + q2c;
+      qss = q2c + B5;
+      const double h22 = qnn * qnn * g.h2d22p[jc] - qss * qss * g.h2d22m[jc];
+      qnn = 0.5 * (q1c + q1p);
+      qss = 0.5 * (q1cm + q1pm);
+      const double h11n = 0.25 * (qnn + qss) * (qnn + qss);
+      qnn = 0.25 * (C6 + C9) * (B6 + q2c);
+      qss = kc == 1 ? 0.0 : 0.25 * (C1 + C5) * (q2c + B7);
+      const double h23 = (qnn - qss) * g.dx3;
+      const double d1q1 = -((q1p + q1pm) - (q1c + q1cm)) * g.h2dare[jc];
+      h2 = d1q1 - (h21 + h22 + h23 - h11n);
+    }
+    // RHS q2 (step.F90:144-165)
+    const double qc = B1;
+    const double d11 = (B2 - 2.0 * qc + B3) * g.s2t11[jc];
+    const double d33 = kc == 1 ? 4.0 / 3.0 * (B6 - 3.0 * qc + 2.0 * 0.0) * g.dx3q : (B6 - 2.0 * qc + B7) * g.dx3q;
+    const double d22 = B4 * g.s2t2p[jc] - qc * g.s2t2c[jc] + B5 * g.s2t2m[jc];
+    r2 = (rk.gam * h2 + rk.rom * ru2 - rk.alm * pg2 + are * (d11 + d33 + d22)) * g.dt;
+  }
+  a.qrhs[0][o] = r1;
+  a.ru[0][o] = h1;
+  if (do3) {
+    a.qrhs[2][o] = r3;
+    a.ru[2][o] = h3;
+  }
+  if (do2) {
+    a.qrhs[1][o] = r2;
+    a.ru[1][o] = h2;
+  }
+}
+
 cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h) {
   const Geo &g = c->geo;
   RhsArgs a;
@@ -255,7 +376,7 @@ cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h) {
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   LaunchScope ls(c, PK_RHS);
   if (inline_h)
-    k_rhs<true><<<gr, b, 0, c->stream>>>(g, rk, a);
+    k_rhs_fused<<<gr, b, 0, c->stream>>>(g, rk, a);
   else
     k_rhs<false><<<gr, b, 0, c->stream>>>(g, rk, a);
   return cudaGetLastError();
