@@ -168,12 +168,111 @@ __global__ void k_uppres(Geo g, double be, const double *__restrict__ dph, doubl
   }
 }
 
+// uppres with every distinct dph value loaded once.  The gradients of phi
+// (the reference's qcap) are formed from those registers exactly as
+// gth/grr/gzz form them, including the kmv/jmv/jpv index maps and the north
+// ghost dph(nzc) = dph(nz); raw neighbours (j-1, j+1, k-1) are loaded once
+// and the mapped ones are selected from them.
+__global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double *__restrict__ dph,
+                                                  double *__restrict__ prg, double *__restrict__ pres,
+                                                  double *__restrict__ dphw) {
+  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  const int imm = im > 1 ? im - 1 : g.nth;
+  const int jm = jc > 1 ? jc - 1 : 1, jp = jc < g.nr ? jc + 1 : g.nr;  // jmv, jpv
+  const bool kmap = kc == 1 || kc == g.nz;  // kmv(kc) = kc there (mesh_tools.F90:272-280)
+  auto D = [&](int i, int j, int k) { return ldg(dph + IDP(g, i, j, k == g.nzc ? g.nz : k)); };
+  // the read-modify-write operands first: prg1..3 live in one array, so a
+  // load after a store to it could not be moved ahead of that store
+  const int o1 = IPRG(g, ic, jc, kc, 1), o2 = IPRG(g, ic, jc, kc, 2), o3 = IPRG(g, ic, jc, kc, 3);
+  const int op = I3(g, ic, jc, kc);
+  const double pr1 = prg[o1], pr2 = jc >= 2 ? prg[o2] : 0.0, pr3 = kc >= 2 ? prg[o3] : 0.0, ps = pres[op];
+  // plane kc
+  const double d_c = D(ic, jc, kc), d_ip = D(ip, jc, kc), d_im = D(im, jc, kc), d_imm = D(imm, jc, kc);
+  const double d_n = D(ic, jc + 1, kc), d_s = D(ic, jc - 1, kc);
+  const double d_im_n = D(im, jc + 1, kc), d_im_s = D(im, jc - 1, kc), d_ip_s = D(ip, jc - 1, kc);
+  const double d_ss = jc >= 2 ? D(ic, jc - 2, kc) : 0.0;
+  // plane kc + 1 (read through the north-ghost map)
+  const double u_c = D(ic, jc, kc + 1), u_im = D(im, jc, kc + 1), u_s = D(ic, jc - 1, kc + 1);
+  // plane kc - 1 (plane 0 is allocated) and kc - 2
+  const double l_c = D(ic, jc, kc - 1), l_ip = D(ip, jc, kc - 1), l_im = D(im, jc, kc - 1);
+  const double l_n = D(ic, jc + 1, kc - 1), l_s = D(ic, jc - 1, kc - 1);
+  const double ll_c = kc >= 3 ? D(ic, jc, kc - 2) : 0.0;
+  // mapped neighbours
+  const double d_jp = jc == g.nr ? d_c : d_n, d_im_jp = jc == g.nr ? d_im : d_im_n;
+  const double d_jm = jc == 1 ? d_c : d_s, d_im_jm = jc == 1 ? d_im : d_im_s;
+  const double m_c = kmap ? d_c : l_c, m_im = kmap ? d_im : l_im, m_s = kmap ? d_s : l_s;
+  // theta component (divergence.F90:270-311)
+  {
+    const double c0 = (d_c - d_im) * g.dx1 * g.irm[jc];
+    const double gp = (d_ip - d_c) * g.dx1 * g.irm[jc];
+    const double gm = (d_im - d_imm) * g.dx1 * g.irm[jc];
+    const double gkp = (u_c - u_im) * g.dx1 * g.irm[jc];
+    const double gkm = (m_c - m_im) * g.dx1 * g.irm[jc];
+    const double gjp = (d_jp - d_im_jp) * g.dx1 * g.irm[jp];
+    const double gjm = (d_jm - d_im_jm) * g.dx1 * g.irm[jm];
+    const double d11 = (gp - 2.0 * c0 + gm) * g.s1t11[jc];
+    const double d33 = (gkp - 2.0 * c0 + gkm) * g.dx3q;
+    const double qnn = gjp * g.irm[jc + 1] - c0 * g.irm[jc];
+    const double qss = c0 * g.irm[jc] - gjm * g.irm[jm];
+    const double d22 = (qnn * g.s1t2n[jc] - qss * g.s1t2s[jc]) * g.s1t2c[jc];
+    prg[o1] = pr1 + c0 - be * (d11 + d33 + d22);
+  }
+  // r component, jc >= 2 (divergence.F90:315-373); grr = 0 on rows 1 and nrc
+  if (jc >= 2) {
+    const double rcj = g.rc[jc];
+    const double c0 = (d_c - d_s) * g.dx2 * rcj;
+    const double gp = (d_ip - d_ip_s) * g.dx2 * rcj;
+    const double gm = (d_im - d_im_s) * g.dx2 * rcj;
+    const double gkp = (u_c - u_s) * g.dx2 * rcj;
+    const double gkm = (m_c - m_s) * g.dx2 * rcj;
+    const double gn = jc + 1 >= g.nrc ? 0.0 : (d_n - d_c) * g.dx2 * g.rc[jc + 1];
+    const double gs = jc - 1 <= 1 ? 0.0 : (d_s - d_ss) * g.dx2 * g.rc[jc - 1];
+    const double d11 = (gp - 2.0 * c0 + gm) * g.s2t11[jc];
+    const double d33 = (gkp - 2.0 * c0 + gkm) * g.dx3q;
+    const double qnn = gn - c0;
+    const double qss = c0 - gs;
+    const double d22 = qnn * g.s2t2p[jc] - qss * g.s2t2m[jc];
+    prg[o2] = pr2 + c0 - be * (d11 + d22 + d33);
+  }
+  // z component, kc >= 2 (divergence.F90:378-439); gzz = 0 on plane 1
+  if (kc >= 2) {
+    const double c0 = (d_c - l_c) * g.dx3;
+    const double gp = (d_ip - l_ip) * g.dx3;
+    const double gm = (d_im - l_im) * g.dx3;
+    const double gkp = (u_c - d_c) * g.dx3;
+    const double gkm = kc - 1 <= 1 ? 0.0 : (l_c - ll_c) * g.dx3;
+    const double gjp = jc == g.nr ? c0 : (d_n - l_n) * g.dx3;
+    const double gjm = jc == 1 ? c0 : (d_s - l_s) * g.dx3;
+    const double d11 = (gp - 2.0 * c0 + gm) * g.s1t11[jc];
+    const double d33 = (gkp - 2.0 * c0 + gkm) * g.dx3q;
+    const double qnn = gjp - c0;
+    const double qss = c0 - gjm;
+    const double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
+    prg[o3] = pr3 + c0 - be * (d11 + d22 + d33);
+  }
+  // pressure (divergence.F90:445-476)
+  {
+    const double p0 = d_c;
+    const double d11 = (d_ip + d_im - 2.0 * p0) * g.s1t11[jc];
+    const double qnn = d_jp - p0;
+    const double qss = p0 - d_jm;
+    const double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
+    const double d33 = (u_c + m_c - 2.0 * p0) * g.dx3q;
+    pres[op] = ps + p0 - be * (d11 + d22 + d33);
+  }
+  if (kc == g.nz) dphw[IDP(g, ic, jc, g.nzc)] = d_c;
+}
+
 cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   double be = 0.5 * (rk.alm * g.dt) / g.re;
   LaunchScope ls(c, PK_UPPRES);
-  k_uppres<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
+  k_uppres_r<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
   return cudaGetLastError();
 }
 
