@@ -100,6 +100,7 @@ struct PartGeo {
   const double *thc, *thm, *rm, *rc, *zm, *zc;  // 1-based device vectors
   double dtheta, dr, dz, zmax, rmax;
   PartCoef C;
+  const PartCoef *Cg;  // device copy of C for the rare full-iteration path
 };
 
 __device__ __forceinline__ void part_cell(const PartGeo &P, double x, double y, double z, int &it, int &ir, int &iz,
@@ -202,6 +203,46 @@ struct PartShared {
   double pos[3][kPartPerBlock];   // new position
 };
 
+// The 27-point stencil of one component: theta columns (periodic), clamped
+// r rows and z planes, and 1/rc per row for q2/rc (0 where rc <= 1e-4,
+// part_tools.F90:587-590).
+struct Stencil {
+  int ith[3], jr[3], kz[3];
+  double irc[3];
+};
+
+__device__ __forceinline__ double stencil_sample(int nth, int J3, const double *__restrict__ q, int kd,
+                                                 const Stencil &T, int f1, int f2, int f3) {
+  const double v = __ldg(q + (size_t)nth * (T.jr[f2] + (size_t)J3 * T.kz[f3]) + T.ith[f1]);
+  return kd == 1 ? v * T.irc[f2] : v;
+}
+
+// Passes 2..100 of the reference's iteration when the one-pass bound does not
+// hold: the samples are gathered again (this path is rare, so they are not
+// kept in registers on the common path).
+__device__ __noinline__ void ls_more(const PartCoef *__restrict__ Cg, int nth, int J3, const double *__restrict__ q,
+                                     int kd, Stencil T, double y0, double *a9) {
+  double y[27], a[9], mp[9];
+  const PartCoef C = *Cg;
+#pragma unroll
+  for (int k = 0; k < 27; k++) y[k] = stencil_sample(nth, J3, q, kd, T, k % 3, (k / 3) % 3, k / 9) - y0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[i] = a9[i];
+#pragma unroll 1
+  for (int iint = 2; iint <= 100; iint++) {
+    ls_pass<false>(C, y, a, mp);
+    double nn = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      a[i] = a[i] + mp[i];
+      nn += mp[i] * mp[i];
+    }
+    if (sqrt(nn) < (double)0.000001f) break;
+  }
+#pragma unroll
+  for (int i = 0; i < 9; i++) a9[i] = a[i];
+}
+
 // Fit component kd at (x, y, z) and write ff, dff and ddff (the first 13
 // rows of M FI, part_tools.F90:653-683) to cv[13 kd ..][p].
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
@@ -218,40 +259,70 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   cell[0] = it;
   cell[1] = ir;
   cell[2] = iz;
-  double yv[27];
-  {
-    int ith[3], jr[3], kz[3];
+  Stencil T;
 #pragma unroll
-    for (int f = -1; f <= 1; f++) {
-      int t = it + f;
-      if (t > P.g.nth) t = 1;
-      if (t < 1) t = P.g.nth;
-      ith[f + 1] = t - 1;
-      int j = ir + f, k = iz + f;
-      jr[f + 1] = j < 0 ? 0 : (j > P.g.nr + 2 ? P.g.nr + 2 : j);
-      kz[f + 1] = k < 0 ? 0 : (k > P.g.nz + 2 ? P.g.nz + 2 : k);
-    }
+  for (int f = -1; f <= 1; f++) {
+    int t = it + f;
+    if (t > P.g.nth) t = 1;
+    if (t < 1) t = P.g.nth;
+    T.ith[f + 1] = t - 1;
+    int j = ir + f, k = iz + f;
+    T.jr[f + 1] = j < 0 ? 0 : (j > P.g.nr + 2 ? P.g.nr + 2 : j);
+    T.kz[f + 1] = k < 0 ? 0 : (k > P.g.nz + 2 ? P.g.nz + 2 : k);
+    T.irc[f + 1] = 1.0;
+  }
+  if (kd == 1) {
     const double tiny = (double)0.0001f;
 #pragma unroll
-    for (int f3 = 0; f3 < 3; f3++)
-#pragma unroll
-      for (int f2 = 0; f2 < 3; f2++) {
-        const double *row = q + (size_t)P.g.nth * (jr[f2] + (size_t)P.g.J3 * kz[f3]);
-#pragma unroll
-        for (int f1 = 0; f1 < 3; f1++) yv[f1 + 3 * f2 + 9 * f3] = __ldg(row + ith[f1]);
-        if (kd == 1) {  // q2 / rc, zero where rc <= 1e-4 (part_tools.F90:587-590)
-          const double rcv = __ldg(P.rc + jr[f2]);
-          const double irc = rcv > tiny ? 1.0 / rcv : 0.0;
-#pragma unroll
-          for (int f1 = 0; f1 < 3; f1++) yv[f1 + 3 * f2 + 9 * f3] *= irc;
-        }
-      }
+    for (int f = 0; f < 3; f++) {
+      const double rcv = __ldg(P.rc + T.jr[f]);
+      T.irc[f] = rcv > tiny ? 1.0 / rcv : 0.0;
+    }
   }
-  const double y0 = yv[13];
-#pragma unroll
-  for (int k = 0; k < 27; k++) yv[k] = yv[k] - y0;
+  // First pass of the fit (mp = mint y from a = 0), accumulated while the
+  // samples arrive; y_k = sample_k - y0 is not kept.
+  const double y0 = stencil_sample(P.g.nth, P.g.J3, q, kd, T, 1, 1, 1);
   double a[9];
-  ls_fit(P.C, yv, a);
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[i] = 0.0;
+  double ym = 0.0;
+  {
+    const PartCoef &C = P.C;
+#pragma unroll
+    for (int k = 0; k < 27; k++) {
+      if (k == 13) continue;  // y = 0 and every mint entry is 0 at the centre
+      const int o1 = k % 3 - 1, o2 = (k / 3) % 3 - 1, o3 = k / 9 - 1;
+      const double yk = stencil_sample(P.g.nth, P.g.J3, q, kd, T, o1 + 1, o2 + 1, o3 + 1) - y0;
+      ym = fmax(ym, fabs(yk));
+      const double e = 0.0 - yk;
+      const int n1 = o1 != 0, n2 = o2 != 0, n3 = o3 != 0;
+      if (o1) a[0] = a[0] - (o1 * C.lin[0]) * e;
+      if (o2) a[1] = a[1] - (o2 * C.lin[1]) * e;
+      if (o3) a[2] = a[2] - (o3 * C.lin[2]) * e;
+      a[3] = a[3] - C.sq[0][4 * n1 + 2 * n2 + n3] * e;
+      a[5] = a[5] - C.sq[1][4 * n2 + 2 * n3 + n1] * e;
+      a[7] = a[7] - C.sq[2][4 * n3 + 2 * n1 + n2] * e;
+      if (o1 * o2) a[4] = a[4] - ((o1 * o2) * C.cr[0]) * e;
+      if (o2 * o3) a[6] = a[6] - ((o2 * o3) * C.cr[1]) * e;
+      if (o3 * o1) a[8] = a[8] - ((o3 * o1) * C.cr[2]) * e;
+    }
+  }
+  {
+    double nn = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) nn += a[i] * a[i];
+    // stop as the reference does (|mp| < 1e-6), or when the second pass is
+    // provably a rounding-level change under that tolerance (see ls_fit);
+    // NaN/Inf take the full iteration
+    if (!(sqrt(nn) < (double)0.000001f) && !(ym < P.C.ymax_one_pass)) {
+      double at[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) at[i] = a[i];
+      ls_more(P.Cg, P.g.nth, P.g.J3, q, kd, T, y0, at);
+#pragma unroll
+      for (int i = 0; i < 9; i++) a[i] = at[i];
+    }
+  }
   double dtp, drp, dzp;
   if (kd == 0) {
     dtp = theta - __ldg(P.thc + it);
@@ -376,7 +447,10 @@ __device__ __forceinline__ void part_cart_row(double r, double sn, double cs, in
 
 // One Euler substep of every live particle (part_tools.F90:517-959) and the
 // out-of-range test and removal (:962-987).
-__global__ void __launch_bounds__(96, 5) k_iter_part(PartGeo P, const double *__restrict__ q1,
+#ifndef VR_PART_MINB
+#define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const double *__restrict__ q1,
                                                   const double *__restrict__ q2, const double *__restrict__ q3,
                                                   double *__restrict__ u, double *__restrict__ v,
                                                   int *__restrict__ isfre, int *__restrict__ gone, int naloc,
@@ -565,12 +639,17 @@ static int part_geo(vr_ctx *c, PartGeo &P) {
   P.zm = c->part_mesh + 2 * (c->geo.nth + 2);
   P.zc = c->part_mesh + 2 * (c->geo.nth + 2) + (c->geo.nz + 3);
   part_coef(c->geo.dtheta, c->geo.dr, c->geo.dz, P.C);
+  P.Cg = reinterpret_cast<const PartCoef *>(c->part_mesh + 2 * (size_t)(c->geo.nth + 2) +
+                                            2 * (size_t)(c->geo.nz + 3));
   return VR_OK;
 }
 
 static int vr_part_mesh_init(vr_ctx *c) {
   const Geo &g = c->geo;
-  std::vector<double> h(2 * (size_t)(g.nth + 2) + 2 * (size_t)(g.nz + 3), 0.0);
+  // thc, thm, zm, zc, then a copy of the stencil coefficients
+  const size_t nmesh = 2 * (size_t)(g.nth + 2) + 2 * (size_t)(g.nz + 3);
+  static_assert(sizeof(PartCoef) % sizeof(double) == 0, "PartCoef holds doubles only");
+  std::vector<double> h(nmesh + sizeof(PartCoef) / sizeof(double), 0.0);
   double *thc = h.data(), *thm = thc + (g.nth + 2), *zm = thm + (g.nth + 2), *zc = zm + (g.nz + 3);
   for (int i = 1; i <= g.nth; i++) {
     thm[i] = 0.0 + (i - 0.5) * g.dtheta;
@@ -582,6 +661,9 @@ static int vr_part_mesh_init(vr_ctx *c) {
     zm[k] = 0.0 + (k - 0.5) * g.dz;
     zc[k] = 0.0 + (k - 1.0) * g.dz;
   }
+  PartCoef C;
+  part_coef(g.dtheta, g.dr, g.dz, C);
+  std::memcpy(h.data() + nmesh, &C, sizeof(C));
   if (cudaMalloc(&c->part_mesh, sizeof(double) * h.size()) != cudaSuccess) return VR_ERR_OOM;
   if (cudaMemcpy(c->part_mesh, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
     return VR_ERR_CUDA;
