@@ -168,6 +168,17 @@ VR_API int vr_injc_part(vr_part *part, double x, double y, double z, double c, d
                         double w, int32_t icall, int32_t *ip);
 /* remv_part (part_tools.F90:199-225), ip 1-based */
 VR_API int vr_remv_part(vr_part *part, int32_t ip);
+/* inlt_part (part_tools.F90:95-142) on one rank: particles enter through the
+ * south-plane cells with rc < r0 in proportion to the axial flux c a q3 dt
+ * inj / nprcl (inj = 10, nprcl = 0.001); the fractional remainder carries over
+ * per radial row.  Positions come from a splitmix64 stream whose state the
+ * caller holds in *rng_state (the reference's random_number stream cannot be
+ * reproduced).  Synchronous; *ninjected = particles added. */
+VR_API int vr_inlt_part(vr_part *part, double r0, uint64_t *rng_state, int32_t *ninjected);
+/* on != 0: vr_iterate calls inlt_part for this attached class at the start of
+ * every step whose nstep is a multiple of 10 (loop.F90:54-58), with nozzle
+ * radius r0 and a stream seeded with seed */
+VR_API int vr_part_set_inflow(vr_part *part, double r0, uint64_t seed, int32_t on);
 /* iter_part (part_tools.F90:374-1164) on one rank: nsubdt explicit Euler
  * substeps of dt/nsubdt in the context's current velocity field; particles
  * that leave 0 <= z <= zmax, r <= rmax are removed. Enqueued on the

@@ -84,6 +84,10 @@ def lib():
         L.orc_iter_part.argtypes = [vp, vp, i32]
         L.orc_part_probe.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, vp]
         L.orc_part_cell.argtypes = [vp, C.c_double, C.c_double, C.c_double, vp, vp]
+        L.orc_rng_uniform.restype = C.c_double
+        L.orc_rng_uniform.argtypes = [C.POINTER(C.c_uint64)]
+        L.orc_inlt_part.restype = i32
+        L.orc_inlt_part.argtypes = [vp, vp, C.c_double, C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
 
@@ -277,6 +281,16 @@ class OraclePart:
 
     def iter_part(self, irk=1):
         lib().orc_iter_part(self.orc._h, self._h, irk)
+
+    def inlt(self, r0, rng_state):
+        """inlt_part (part_tools.F90:95-142); returns (injected, new rng state)."""
+        st = C.c_uint64(rng_state)
+        n = lib().orc_inlt_part(self.orc._h, self._h, r0, C.byref(st))
+        return n, st.value
+
+    @property
+    def inflow(self):
+        return np.ctypeslib.as_array(self._s.inflow, shape=(self.orc.nr + 2,))
 
     def probe(self, x, y, z):
         out = np.zeros(39)

@@ -1713,6 +1713,52 @@ void orc_remv_part(orc_part *p, int32_t ip) {
   for (int iv = 1; iv <= 3; iv++) PV(p, ip, iv) = 0.0;
 }
 
+/* splitmix64 (Steele, Lea & Flood, "Fast splittable pseudorandom number
+ * generators", OOPSLA 2014): the state advances by the golden-ratio
+ * increment and is mixed with Stafford's variant 13; the top 53 bits give a
+ * uniform double in [0, 1).  It stands in for Fortran random_number, whose
+ * stream cannot be reproduced; the library uses the same sequence. */
+double orc_rng_uniform(uint64_t *state) {
+  uint64_t z = (*state += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* part_tools.F90:95-142 on one rank (ip_a(3) == 0): particles enter through
+ * the south-plane cells with rc < r0 in proportion to the axial flux; inj = 10
+ * and nprcl = 0.001 are init_part's constants (part_tools.F90:275-276), the
+ * fractional remainder carries over in inflow(ir).  Three uniforms per
+ * particle (theta, r, z).  Returns the number injected, -1 when the slots ran
+ * out. */
+int32_t orc_inlt_part(orc_ctx *c, orc_part *p, double r0, uint64_t *rng) {
+  const double nprcl = SP(0.001f);
+  const int inj = 10;
+  int32_t total = 0;
+  for (int ir = 1; ir <= c->nr; ir++) {
+    if (!(c->rc[ir] < r0)) continue;
+    double a = c->dtheta * (c->rc[ir + 1] * c->rc[ir + 1] - c->rc[ir] * c->rc[ir]);
+    for (int it = 1; it <= c->nth; it++) {
+      double ut = 0.0, ur = 0.0; /* the reference zeroes both (part_tools.F90:110-111) */
+      double uz = Q3(it, ir, 1);
+      p->inflow[ir] = p->inflow[ir] + (p->c * a * Q3(it, ir, 1) * c->p.dt * (double)(float)inj / nprcl);
+      int n = (int)floor(p->inflow[ir]);
+      p->inflow[ir] = p->inflow[ir] - (double)(float)n;
+      for (int ip = 1; ip <= n; ip++) {
+        double t = c->thc[it] + c->dtheta * orc_rng_uniform(rng);
+        double r = c->rc[ir] + c->dr * orc_rng_uniform(rng);
+        double z = c->zc[1] + c->dz * orc_rng_uniform(rng);
+        double x = r * cos(t), y = r * sin(t);
+        double u = ur * cos(t) - ut * sin(t), v = ur * sin(t) + ut * cos(t), w = uz;
+        if (orc_injc_part(p, x, y, z, p->c, u, v, w, 1) < 0) return -1;
+        total++;
+      }
+    }
+  }
+  return total;
+}
+
 /* The field sample for component ivar at stencil point (itof, irof, izof),
  * part_tools.F90:587-590.  Indices are clamped to the stored extents; the
  * reference reads outside them only for particles already out of range. */

@@ -116,6 +116,10 @@ int32_t orc_injc_part(orc_part *p, double x, double y, double z, double cc,
                       double u, double v, double w, int32_t icall);
 /* part_tools.F90:199-225 */
 void orc_remv_part(orc_part *p, int32_t ip);
+/* uniform double in [0,1) from a splitmix64 stream (stand-in for random_number) */
+double orc_rng_uniform(uint64_t *state);
+/* part_tools.F90:95-142 (one rank); returns the number injected, -1 when full */
+int32_t orc_inlt_part(orc_ctx *c, orc_part *p, double r0, uint64_t *rng);
 /* part_tools.F90:374-1164 (single rank: no migration) */
 void orc_iter_part(orc_ctx *c, orc_part *p, int32_t irk);
 /* Interpolation + transform at one point (part_tools.F90:521-797):

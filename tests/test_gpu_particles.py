@@ -196,3 +196,62 @@ def test_context_refuses_destroy_with_live_particles():
     p.close()
     run.close()
     assert not run._h
+
+
+def _south_inflow(orc, gpu, seed):
+    rng = np.random.default_rng(seed)
+    q3 = orc.field("q3")
+    q3[:, :, 1] = rng.uniform(0.5, 2.0, size=q3[:, :, 1].shape)
+    gpu.set("q3", q3)
+
+
+def test_inlt_part_matches_oracle():
+    """inlt_part: same slots, positions, velocities, ids and random stream."""
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = 16, 32, 32
+    orc, gpu = make_pair(nth, nr, nz, dt=0.002)
+    _south_inflow(orc, gpu, 4)
+    op = O.OraclePart(orc, 3, 20000, 0)
+    gp = V.Part(gpu, 3, 20000, 0)
+    so, sg = 77, 77
+    for call in range(3):
+        no, so = op.inlt(0.6, so)
+        ng, sg = gp.inlt(0.6, sg)
+        assert (no, so) == (ng, sg) and no > 0
+        _compare_parts(op, gp, rel=1e-15)
+    # removals in between, then refill through the free list
+    for ip in (3, 10, 11, op.nlast):
+        op.remv(ip)
+        gp.remv(ip)
+    no, so = op.inlt(0.6, so)
+    ng, sg = gp.inlt(0.6, sg)
+    assert (no, so) == (ng, sg)
+    _compare_parts(op, gp, rel=1e-15)
+    gp.close()
+
+
+def test_iterate_with_inflow_injection():
+    """vr_iterate with inflow on: inlt_part at nstep = 0, 10, 20 (loop.F90:54-58),
+    then iter_part, then the three substeps, against the same loop on the oracle."""
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = 16, 32, 64
+    orc, gpu = make_pair(nth, nr, nz, dt=1e-3, wth="modified")
+    _ring(orc, gpu, nth, nr, nz, seed=9)
+    _south_inflow(orc, gpu, 5)
+    op = O.OraclePart(orc, 6, 4000, 1)
+    gp = V.Part(gpu, 6, 4000, 1)
+    gp.set_inflow(0.6, 2024, True)
+    gp.attach(True)
+    gpu.iterate(21)
+    so = 2024
+    for step in range(21):
+        if step % 10 == 0:
+            _, so = op.inlt(0.6, so)
+        op.iter_part(1)
+        orc.iterate(1)
+    assert op.nlast > 0
+    _compare_parts(op, gp, rel=1e-10)
+    gp.attach(False)
+    gp.close()

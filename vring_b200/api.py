@@ -92,6 +92,8 @@ def lib():
         L.vr_part_info.argtypes = [vp, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp), C.POINTER(i32)]
         L.vr_injc_part.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, i32, C.POINTER(i32)]
         L.vr_remv_part.argtypes = [vp, i32]
+        L.vr_inlt_part.argtypes = [vp, dp, C.POINTER(C.c_uint64), C.POINTER(i32)]
+        L.vr_part_set_inflow.argtypes = [vp, dp, C.c_uint64, i32]
         L.vr_iter_part.argtypes = [vp, i32]
         L.vr_part_attach.argtypes = [vp, i32]
         L.vr_part_set_state.argtypes = [vp, vp, vp, vp, i32]
@@ -307,6 +309,16 @@ class Part:
 
     def iter_part(self, irk: int = 1) -> None:
         self._chk(lib().vr_iter_part(self._h, irk), "iter_part")
+
+    def inlt(self, r0: float, rng_state: int):
+        """inlt_part (part_tools.F90:95-142); returns (injected, new rng state)."""
+        st, n = C.c_uint64(rng_state), C.c_int32()
+        self._chk(lib().vr_inlt_part(self._h, r0, C.byref(st), C.byref(n)), "inlt_part")
+        return n.value, st.value
+
+    def set_inflow(self, r0: float, seed: int, on: bool = True) -> None:
+        """Inflow injection every 10 steps inside Run.iterate (attached classes)."""
+        self._chk(lib().vr_part_set_inflow(self._h, r0, seed, 1 if on else 0), "part_set_inflow")
 
     def attach(self, on: bool = True) -> None:
         self._chk(lib().vr_part_attach(self._h, 1 if on else 0), "part_attach")

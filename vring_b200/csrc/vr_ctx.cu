@@ -842,6 +842,12 @@ extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
   VR_CUDA(c, cudaSetDevice(c->dev));
   for (int s = 0; s < nsteps; s++) {
     c->ntime = c->d.dt + c->ntime;
+    // loop.F90:54-58: inflow injection every inj = 10 steps
+    if (c->nstep % 10 == 0)
+      for (vr_part *p : c->parts) {
+        int rc = vr_part_inflow_step(p);
+        if (rc) return rc;
+      }
     // loop.F90:65-70: particles advance once per step, before ucoeff, in the
     // velocity at the start of the step
     for (vr_part *p : c->parts) {

@@ -176,6 +176,8 @@ struct LaunchScope {
 // enqueue the nsubdt Euler substeps of one particle class on stream s
 // (vr_particles.cu)
 int vr_part_enqueue(vr_part *p, cudaStream_t s);
+// inlt_part for a class whose inflow injection is on (host, synchronous)
+int vr_part_inflow_step(vr_part *p);
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);

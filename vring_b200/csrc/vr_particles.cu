@@ -28,6 +28,14 @@
 
 #include "vr_internal.cuh"
 
+namespace vr {
+// one injected particle (injc_part, part_tools.F90:144-197)
+struct NewPart {
+  int ip, keep_id;
+  double x, y, z, u, v, w, c, id;
+};
+}  // namespace vr
+
 struct vr_part {
   vr_ctx *ctx;
   int id, naloc, nvar, nsubdt, mode;
@@ -41,6 +49,16 @@ struct vr_part {
   std::vector<int> ifree, h_isfre;
   int serial;  // substeps run so far
   bool counted;  // included in ctx->nparts
+  // injections waiting for one scatter launch, and its device staging buffer
+  std::vector<vr::NewPart> pending;
+  vr::NewPart *d_batch;
+  size_t d_batch_cap;
+  // inlt_part: per-row flux remainder, nozzle radius, random stream, and
+  // whether vr_iterate injects every inj steps
+  std::vector<double> inflow;
+  double r0;
+  uint64_t rng;
+  bool inflow_on;
 };
 
 namespace vr {
@@ -571,6 +589,30 @@ __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__re
     for (int b = 0; b < 3; b++) o[12 + w + 3 * b + 9 * c] = ddvel[b][c];
 }
 
+// Scatter of a batch of injections: every variable of the slot is zeroed,
+// then position, velocity, identity Jacobian, concentration and id are set.
+__global__ void k_inject(const NewPart *__restrict__ b, int n, double *__restrict__ u, double *__restrict__ v,
+                         int *__restrict__ isfre, int naloc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const NewPart P = b[t];
+  const size_t ip = (size_t)P.ip - 1, N = (size_t)naloc;
+  for (int iv = 0; iv < 117; iv++) u[ip + N * iv] = 0.0;
+  u[ip] = P.x;
+  u[ip + N] = P.y;
+  u[ip + 2 * N] = P.z;
+  u[ip + 3 * N] = P.u;
+  u[ip + 4 * N] = P.v;
+  u[ip + 5 * N] = P.w;
+  u[ip + 6 * N] = 1.0;
+  u[ip + 10 * N] = 1.0;
+  u[ip + 14 * N] = 1.0;
+  v[ip] = 0.0;
+  v[ip + N] = P.c;
+  if (!P.keep_id) v[ip + 2 * N] = P.id;
+  isfre[ip] = 0;
+}
+
 // PartCoef from the mesh spacings, each entry computed as the reference's
 // reduced fraction (part_tools.F90:295-357)
 static void part_coef(double d1, double d2, double d3, PartCoef &C) {
@@ -711,6 +753,7 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
   cudaMemset(p->d_nremoved, 0, sizeof(int));
   p->ifree.assign(naloc + 2, 0);
   p->h_isfre.assign(naloc + 1, 0);
+  p->inflow.assign(c->geo.nr + 2, 0.0);
   VR_CUDA(c, cudaDeviceSynchronize());
   c->nparts++;
   p->counted = true;
@@ -731,6 +774,7 @@ extern "C" int vr_part_destroy(vr_part *p) {
   cudaFree(p->isfre);
   cudaFree(p->gone);
   cudaFree(p->d_nremoved);
+  if (p->d_batch) cudaFree(p->d_batch);
   delete p;
   return VR_OK;
 }
@@ -772,14 +816,10 @@ static int part_sync_bookkeeping(vr_part *p) {
   return VR_OK;
 }
 
-extern "C" int vr_injc_part(vr_part *p, double x, double y, double z, double cc, double uu, double vv,
-                            double ww, int32_t icall, int32_t *ipout) {
-  if (!p) return VR_ERR_ARG;
-  vr_ctx *c = p->ctx;
-  VR_CUDA(c, cudaSetDevice(c->dev));
-  int rc = part_sync_bookkeeping(p);
-  if (rc) return rc;
-  // part_tools.F90:144-197
+// injc_part (part_tools.F90:144-197) on the host free list; the device
+// write is queued in p->pending.  Returns the slot or -1 when all are taken.
+static int host_injc(vr_part *p, double x, double y, double z, double cc, double uu, double vv, double ww,
+                     int icall) {
   int ip;
   if (p->nfree > 0) {
     ip = p->ifree[p->nfree];
@@ -787,42 +827,145 @@ extern "C" int vr_injc_part(vr_part *p, double x, double y, double z, double cc,
     p->ifree[p->nfree] = 0;
     p->nfree = p->nfree - 1;
   } else {
-    if (p->nlast + 1 > p->naloc) return set_err(c, VR_ERR_CAPACITY, "particle slots exhausted");
+    if (p->nlast + 1 > p->naloc) return -1;
     p->nlast = p->nlast + 1;
     ip = p->nlast;
     p->h_isfre[ip] = 0;
   }
   p->npart = p->npart + 1;
-  std::vector<double> col(117, 0.0);
-  col[0] = x;
-  col[1] = y;
-  col[2] = z;
-  col[3] = uu;
-  col[4] = vv;
-  col[5] = ww;
-  col[6] = 1.0;
-  col[10] = 1.0;
-  col[14] = 1.0;
-  for (int iv = 0; iv < 117; iv++)
-    VR_CUDA(c, cudaMemcpyAsync(p->u + (size_t)(ip - 1) + (size_t)p->naloc * iv, &col[iv], sizeof(double),
-                               cudaMemcpyHostToDevice, c->stream));
-  double vcol[3] = {0.0, cc, 0.0};
-  if (icall == 1) {
-    p->nids = p->nids + 1;
-    vcol[2] = (double)(float)p->nids;
-  } else {
-    double old = 0.0;
-    VR_CUDA(c, cudaMemcpy(&old, p->v + (size_t)(ip - 1) + (size_t)p->naloc * 2, sizeof(double), cudaMemcpyDeviceToHost));
-    vcol[2] = old;
+  NewPart n;
+  n.ip = ip;
+  n.keep_id = icall != 1;
+  if (icall == 1) p->nids = p->nids + 1;
+  n.id = (double)(float)p->nids;
+  n.x = x;
+  n.y = y;
+  n.z = z;
+  n.u = uu;
+  n.v = vv;
+  n.w = ww;
+  n.c = cc;
+  p->pending.push_back(n);
+  return ip;
+}
+
+// one scatter launch for the queued injections
+static int flush_injections(vr_part *p) {
+  vr_ctx *c = p->ctx;
+  const size_t n = p->pending.size();
+  if (n == 0) return VR_OK;
+  if (n > p->d_batch_cap) {
+    if (p->d_batch) cudaFree(p->d_batch);
+    p->d_batch = nullptr;
+    p->d_batch_cap = 0;
+    size_t cap = std::max<size_t>(n, 1024);
+    if (cudaMalloc(&p->d_batch, cap * sizeof(NewPart)) != cudaSuccess) return set_err(c, VR_ERR_OOM, "injection batch");
+    p->d_batch_cap = cap;
   }
-  for (int iv = 0; iv < 3; iv++)
-    VR_CUDA(c, cudaMemcpyAsync(p->v + (size_t)(ip - 1) + (size_t)p->naloc * iv, &vcol[iv], sizeof(double),
-                               cudaMemcpyHostToDevice, c->stream));
-  int zero = 0;
-  VR_CUDA(c, cudaMemcpyAsync(p->isfre + ip - 1, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  VR_CUDA(c, cudaMemcpyAsync(p->d_batch, p->pending.data(), n * sizeof(NewPart), cudaMemcpyHostToDevice, c->stream));
+  {
+    LaunchScope ls(c, PK_PART);
+    k_inject<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(p->d_batch, (int)n, p->u, p->v, p->isfre, p->naloc);
+  }
+  VR_LAUNCH_CHECK(c);
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));  // the host batch is reused
+  p->pending.clear();
+  return VR_OK;
+}
+
+extern "C" int vr_injc_part(vr_part *p, double x, double y, double z, double cc, double uu, double vv,
+                            double ww, int32_t icall, int32_t *ipout) {
+  if (!p) return VR_ERR_ARG;
+  vr_ctx *c = p->ctx;
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  int rc = part_sync_bookkeeping(p);
+  if (rc) return rc;
+  int ip = host_injc(p, x, y, z, cc, uu, vv, ww, icall);
+  if (ip < 0) return set_err(c, VR_ERR_CAPACITY, "particle slots exhausted");
+  rc = flush_injections(p);
+  if (rc) return rc;
   if (ipout) *ipout = ip;
   return VR_OK;
+}
+
+// splitmix64 (Steele, Lea & Flood, OOPSLA 2014) uniform doubles in [0, 1):
+// the stand-in for Fortran random_number, the same stream as the oracle's
+static double rng_uniform(uint64_t *state) {
+  uint64_t z = (*state += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// inlt_part (part_tools.F90:95-142) on one rank: particles enter through the
+// south-plane cells with rc < r0 in proportion to the axial flux there; the
+// remainder carries over in inflow(ir).  inj = 10 and nprcl = 0.001 are
+// init_part's constants (part_tools.F90:275-276).
+static int part_inlt(vr_part *p, double r0, uint64_t *rng, int *ninj) {
+  vr_ctx *c = p->ctx;
+  const Geo &g = c->geo;
+  int rc = part_sync_bookkeeping(p);
+  if (rc) return rc;
+  const double nprcl = (double)0.001f;
+  const int inj = 10;
+  int nrin = 0;  // rc increases with ir, so the rows with rc < r0 are 1..nrin
+  while (nrin + 1 <= g.nr && c->h_rc[nrin + 1] < r0) nrin++;
+  *ninj = 0;
+  if (nrin == 0) return VR_OK;
+  std::vector<double> q3s((size_t)g.nth * nrin);
+  VR_CUDA(c, cudaMemcpyAsync(q3s.data(), c->q[2] + I3(g, 1, 1, 1), sizeof(double) * q3s.size(),
+                             cudaMemcpyDeviceToHost, c->stream));
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  const double *rcv = c->h_rc;
+  for (int ir = 1; ir <= nrin; ir++) {
+    const double a = g.dtheta * (rcv[ir + 1] * rcv[ir + 1] - rcv[ir] * rcv[ir]);
+    for (int it = 1; it <= g.nth; it++) {
+      const double ut = 0.0, ur = 0.0;  // the reference zeroes both (part_tools.F90:110-111)
+      const double q3 = q3s[(size_t)(it - 1) + (size_t)g.nth * (ir - 1)];
+      const double uz = q3;
+      p->inflow[ir] = p->inflow[ir] + (p->c * a * q3 * g.dt * (double)(float)inj / nprcl);
+      const int n = (int)std::floor(p->inflow[ir]);
+      p->inflow[ir] = p->inflow[ir] - (double)(float)n;
+      const double thc = 0.0 + (it - 1.0) * g.dtheta, zc1 = 0.0 + (1 - 1.0) * g.dz;
+      for (int k = 1; k <= n; k++) {
+        const double t = thc + g.dtheta * rng_uniform(rng);
+        const double r = rcv[ir] + g.dr * rng_uniform(rng);
+        const double z = zc1 + g.dz * rng_uniform(rng);
+        const double x = r * std::cos(t), y = r * std::sin(t);
+        const double u = ur * std::cos(t) - ut * std::sin(t), v = ur * std::sin(t) + ut * std::cos(t), w = uz;
+        if (host_injc(p, x, y, z, p->c, u, v, w, 1) < 0) {
+          flush_injections(p);
+          return set_err(c, VR_ERR_CAPACITY, "particle slots exhausted in inlt_part");
+        }
+        (*ninj)++;
+      }
+    }
+  }
+  return flush_injections(p);
+}
+
+extern "C" int vr_inlt_part(vr_part *p, double r0, uint64_t *rng_state, int32_t *ninjected) {
+  if (!p || !rng_state) return VR_ERR_ARG;
+  VR_CUDA(p->ctx, cudaSetDevice(p->ctx->dev));
+  int n = 0;
+  int rc = part_inlt(p, r0, rng_state, &n);
+  if (ninjected) *ninjected = n;
+  return rc;
+}
+
+extern "C" int vr_part_set_inflow(vr_part *p, double r0, uint64_t seed, int32_t on) {
+  if (!p) return VR_ERR_ARG;
+  p->r0 = r0;
+  p->rng = seed;
+  p->inflow_on = on != 0;
+  return VR_OK;
+}
+
+int vr::vr_part_inflow_step(vr_part *p) {
+  if (!p->inflow_on) return VR_OK;
+  int n = 0;
+  return part_inlt(p, p->r0, &p->rng, &n);
 }
 
 extern "C" int vr_remv_part(vr_part *p, int32_t ip) {
