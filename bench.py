@@ -210,28 +210,13 @@ def main():
 
     import torch
     import vring_b200 as V
+    from vring_b200 import replicas
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = replicas.init("nccl", timeout_s=300.0)
+    rank, world = rep.rank, rep.world
+    barrier, max_over_ranks = rep.barrier, rep.max_over_ranks
 
     q = ring_state()
     run = V.Run(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, theta_wavenumber="modified", device=local)
@@ -271,7 +256,7 @@ def main():
     run.profile(False)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms)
-    value = world * ncell * args.steps / (ms_max / 1e3) / 1e6
+    value = replicas.throughput(ncell * args.steps, world, ms_max / 1e3) / 1e6
     maxdiv = run.max_divergence()
     nonfinite = run.count_nonfinite()
 
@@ -299,7 +284,7 @@ def main():
         run.sync()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
         bytes_q = sum(p.numel() for p in pins) * 8
-        e2e = {"value": world * ncell * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+        e2e = {"value": replicas.throughput(ncell * args.e2e_steps, world, e2e_s) / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": bytes_q, "d2h_bytes_per_step": bytes_q,
                "what": "per step: q1,q2,q3 host->device from pinned memory, vr_iterate(1) "
                        "(particles included), q1,q2,q3 device->host; pressure, RK history and "
@@ -347,9 +332,7 @@ def main():
         print(json.dumps(line), flush=True)
     part.close()
     run.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
