@@ -50,6 +50,7 @@ enum vr_status {
   VR_ERR_SCRATCH = 11   /* larger than a no-allocation entry's fixed scratch */
 };
 
+/* VR_MIXED is reserved: vr_create returns VR_ERR_DESC for it (not built) */
 enum vr_precision { VR_FP64 = 0, VR_MIXED = 1 };
 enum vr_theta_wavenumber {
   VR_WTH_EXACT = 0,    /* m^2, the reference's 'wvnex' (poisson_solve.F90:287)   */

@@ -287,7 +287,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
       (!nz_pow2 && d.nz > 512))
     return VR_ERR_DESC;
   if (!(d.rmax > 0) || !(d.zmax > 0) || !(d.dt > 0) || !(d.re > 0) || !(d.pe > 0)) return VR_ERR_DESC;
-  if (d.precision != VR_FP64 && d.precision != VR_MIXED) return VR_ERR_DESC;
+  if (d.precision != VR_FP64) return VR_ERR_DESC;  // the mixed-precision form is not built
   if (d.theta_wavenumber != VR_WTH_EXACT && d.theta_wavenumber != VR_WTH_MODIFIED) return VR_ERR_DESC;
   if (d.inflow != VR_INFLOW_OFF && d.inflow != VR_INFLOW_REFERENCE) return VR_ERR_DESC;
   int64_t cells = (int64_t)d.ntheta * (d.nr + 3) * (d.nz + 3);
