@@ -47,7 +47,8 @@ enum vr_status {
   VR_ERR_ARG = 8,       /* invalid argument                                  */
   VR_ERR_CAPACITY = 9,  /* particle slots exhausted                          */
   VR_ERR_NODEVICE = 10, /* no usable CUDA device                             */
-  VR_ERR_SCRATCH = 11   /* larger than a no-allocation entry's fixed scratch */
+  VR_ERR_SCRATCH = 11,  /* larger than a no-allocation entry's fixed scratch */
+  VR_ERR_IO = 12        /* a restart file could not be written or read       */
 };
 
 /* VR_MIXED is reserved: vr_create returns VR_ERR_DESC for it (not built) */
@@ -123,6 +124,19 @@ VR_API int vr_laplace_solve(vr_ctx *ctx); /* poisson_solve.F90:13-32 -> DPH     
 VR_API int vr_upsol(vr_ctx *ctx);         /* divergence.F90:69-236                     */
 VR_API int vr_uppres(vr_ctx *ctx);        /* divergence.F90:239-480                    */
 
+/* ---- restart files (run.F90:390-539) -------------------------------------- */
+/* restart_save: the reference's file (gfortran unformatted sequential: a
+ * header record nstep, ntime, ntheta, nr, nz, then one record q1, q2, q3 per
+ * interior cell, theta fastest, then r, then z).  With VR_RESTART_FULL an
+ * extension follows that the reference's reader never reaches: the clock and
+ * every field of the context with its ghosts, for a bit-identical resume. */
+#define VR_RESTART_FULL 1
+VR_API int vr_restart_save(vr_ctx *ctx, const char *path, int32_t flags);
+/* restart_load: q1..q3 on the interior and nstep/ntime from the header (the
+ * reference's nstepi); *full = 1 when an extension was present and the whole
+ * state was restored.  VR_ERR_FIELD when the grid differs. */
+VR_API int vr_restart_load(vr_ctx *ctx, const char *path, int32_t *full);
+
 /* ---- fused paths --------------------------------------------------------- */
 /* One RK substep irk (loop.F90:63-130 without particles), fused kernels. */
 VR_API int vr_substep(vr_ctx *ctx, int32_t irk);
@@ -194,6 +208,12 @@ VR_API int vr_part_set_state(vr_part *part, const double *u, const double *v, co
                              int32_t nlast);
 /* any pointer may be NULL; counts = {npart, nlast, nfree, nids} */
 VR_API int vr_part_get_state(vr_part *part, double *u, double *v, int32_t *isfre, int32_t counts[4]);
+/* a particle class's whole state (arrays, free list, counters, inflow
+ * remainders, random stream) to and from a file; the class loading it must
+ * have the same id, naloc and mode (no reference counterpart: the reference
+ * does not restart particles) */
+VR_API int vr_part_restart_save(vr_part *part, const char *path);
+VR_API int vr_part_restart_load(vr_part *part, const char *path);
 /* interpolated fluid velocity, gradient and Hessian (Cartesian components,
  * part_tools.F90:521-797) at n points xyz[3n]; out[39n] per point: u_i,
  * du_i/dx_j at 3+i+3j, d2u_i/dx_j dx_k at 12+i+3j+9k; cells[3n] = (it, ir, iz) */

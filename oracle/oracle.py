@@ -61,6 +61,7 @@ def lib():
         L.orc_coef.restype = dp
         L.orc_coef.argtypes = [vp, C.c_char_p]
         L.orc_set_clock.argtypes = [vp, i32, C.c_double, i64]
+        L.orc_get_clock.argtypes = [vp, C.POINTER(i32), C.POINTER(C.c_double), C.POINTER(i64)]
         for n in ["ucoeff", "coesys", "hdnbc", "hdnl1", "hdnl2", "hdnl3", "step", "divq",
                   "upsol", "uppres", "laplace_solve"]:
             getattr(L, "orc_" + n).argtypes = [vp]
@@ -84,6 +85,10 @@ def lib():
         L.orc_iter_part.argtypes = [vp, vp, i32]
         L.orc_part_probe.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, vp]
         L.orc_part_cell.argtypes = [vp, C.c_double, C.c_double, C.c_double, vp, vp]
+        L.orc_restart_save.restype = i32
+        L.orc_restart_save.argtypes = [vp, C.c_char_p]
+        L.orc_restart_load.restype = i32
+        L.orc_restart_load.argtypes = [vp, C.c_char_p]
         L.orc_rng_uniform.restype = C.c_double
         L.orc_rng_uniform.argtypes = [C.POINTER(C.c_uint64)]
         L.orc_inlt_part.restype = i32
@@ -152,6 +157,21 @@ class Oracle:
 
     def substep(self, irk: int):
         lib().orc_substep(self._h, irk)
+
+    def restart_save(self, path: str) -> int:
+        """restart_save (run.F90:390-460); 0 on success."""
+        return lib().orc_restart_save(self._h, str(path).encode())
+
+    def restart_load(self, path: str) -> int:
+        """restart_load (run.F90:463-531); 0 on success, -2 on a grid mismatch."""
+        return lib().orc_restart_load(self._h, str(path).encode())
+
+    @property
+    def clock(self):
+        """(irk, ntime, nstep)"""
+        irk, t, n = C.c_int32(), C.c_double(), C.c_int64()
+        lib().orc_get_clock(self._h, C.byref(irk), C.byref(t), C.byref(n))
+        return irk.value, t.value, n.value
 
     def iterate(self, nsteps: int):
         lib().orc_iterate(self._h, nsteps)

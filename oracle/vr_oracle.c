@@ -22,6 +22,7 @@
 #include "vr_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -293,6 +294,12 @@ const double *orc_mesh(orc_ctx *c, int32_t which) {
     case 5: return c->thc;
     default: return NULL;
   }
+}
+
+void orc_get_clock(orc_ctx *c, int32_t *irk, double *ntime, int64_t *nstep) {
+  *irk = c->irk;
+  *ntime = c->ntime;
+  *nstep = c->nstep;
 }
 
 void orc_set_clock(orc_ctx *c, int32_t irk, double ntime, int64_t nstep) {
@@ -2020,4 +2027,81 @@ void orc_iter_part(orc_ctx *c, orc_part *p, int32_t irk) {
     for (int n = 0; n < ndl; n++) orc_remv_part(p, idl[n]);
   }
   free(idl);
+}
+
+/* ======================================================================== */
+/* Restart files: run.F90:390-539                                            */
+/* ======================================================================== */
+/* gfortran unformatted sequential records: the payload framed by its byte
+ * length as a 4-byte little-endian integer before and after. */
+static int orc_rec_write(FILE *f, const void *buf, int32_t n) {
+  if (fwrite(&n, 4, 1, f) != 1 || fwrite(buf, 1, (size_t)n, f) != (size_t)n || fwrite(&n, 4, 1, f) != 1) return -1;
+  return 0;
+}
+static int orc_rec_read(FILE *f, void *buf, int32_t n) {
+  int32_t a = 0, b = 0;
+  if (fread(&a, 4, 1, f) != 1 || a != n) return -1;
+  if (fread(buf, 1, (size_t)n, f) != (size_t)n) return -1;
+  if (fread(&b, 4, 1, f) != 1 || b != n) return -1;
+  return 0;
+}
+
+/* restart_save (run.F90:390-460) on one rank: a header record
+ * (nstep, ntime, nthetag, nrg, nzg) as int32, real64, 3 x int32, then for
+ * iz = 1..nz, ir = 1..nr, ith = 1..ntheta one record (q1, q2, q3). */
+int32_t orc_restart_save(orc_ctx *c, const char *path) {
+  FILE *f = fopen(path, "wb");
+  if (!f) return -1;
+  unsigned char h[24];
+  int32_t nstep = (int32_t)c->nstep, nth = c->nth, nr = c->nr, nz = c->nz;
+  memcpy(h, &nstep, 4);
+  memcpy(h + 4, &c->ntime, 8);
+  memcpy(h + 12, &nth, 4);
+  memcpy(h + 16, &nr, 4);
+  memcpy(h + 20, &nz, 4);
+  int rc = orc_rec_write(f, h, 24);
+  for (int iz = 1; iz <= nz && !rc; iz++)
+    for (int ir = 1; ir <= nr && !rc; ir++)
+      for (int ith = 1; ith <= nth && !rc; ith++) {
+        double q[3] = {Q1(ith, ir, iz), Q2(ith, ir, iz), Q3(ith, ir, iz)};
+        rc = orc_rec_write(f, q, 24);
+      }
+  if (fclose(f) != 0) rc = -1;
+  return rc;
+}
+
+/* restart_load (run.F90:463-531) on one rank: nstepi and ntime from the
+ * header, q1..q3 on the interior; -2 when the grid differs. */
+int32_t orc_restart_load(orc_ctx *c, const char *path) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return -1;
+  unsigned char h[24];
+  int rc = orc_rec_read(f, h, 24);
+  int32_t nstep = 0, nth = 0, nr = 0, nz = 0;
+  double ntime = 0.0;
+  if (!rc) {
+    memcpy(&nstep, h, 4);
+    memcpy(&ntime, h + 4, 8);
+    memcpy(&nth, h + 12, 4);
+    memcpy(&nr, h + 16, 4);
+    memcpy(&nz, h + 20, 4);
+    if (nth != c->nth || nr != c->nr || nz != c->nz) rc = -2;
+  }
+  for (int iz = 1; iz <= c->nz && !rc; iz++)
+    for (int ir = 1; ir <= c->nr && !rc; ir++)
+      for (int ith = 1; ith <= c->nth && !rc; ith++) {
+        double q[3];
+        rc = orc_rec_read(f, q, 24);
+        if (!rc) {
+          Q1(ith, ir, iz) = q[0];
+          Q2(ith, ir, iz) = q[1];
+          Q3(ith, ir, iz) = q[2];
+        }
+      }
+  fclose(f);
+  if (!rc) {
+    c->nstep = nstep;
+    c->ntime = ntime;
+  }
+  return rc;
 }

@@ -51,6 +51,7 @@ double *orc_field(orc_ctx *c, int32_t id, int64_t extents[4]);
 /* mesh_tools.F90:321-350 coordinate vectors (Fortran index = array index). */
 const double *orc_mesh(orc_ctx *c, int32_t which); /* 0 rm,1 rc,2 zm,3 zc,4 thm,5 thc */
 void orc_set_clock(orc_ctx *c, int32_t irk, double ntime, int64_t nstep);
+void orc_get_clock(orc_ctx *c, int32_t *irk, double *ntime, int64_t *nstep);
 
 /* momentum_coef.F90:24-69 / :71-538 */
 void orc_ucoeff(orc_ctx *c);
@@ -129,6 +130,11 @@ void orc_part_probe(orc_ctx *c, orc_part *p, double x, double y, double z, doubl
 void orc_part_cell(orc_ctx *c, double x, double y, double z, int32_t *idx3, double *theta);
 /* acos restated for bit-identical cell indices on CPU and GPU */
 double orc_vr_acos(double x);
+
+/* ---- restart files (run.F90:390-539), gfortran sequential records --- */
+/* 0 on success, -1 on an I/O or format error, -2 on a grid mismatch */
+int32_t orc_restart_save(orc_ctx *c, const char *path);
+int32_t orc_restart_load(orc_ctx *c, const char *path);
 
 #ifdef __cplusplus
 }

@@ -25,7 +25,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "vring_b200.h")
 VR_ABI_VERSION = 1
 STATUS = {0: "VR_OK", 1: "VR_ERR_DESC", 2: "VR_ERR_OOM", 3: "VR_ERR_CUDA", 4: "VR_ERR_NONFINITE",
           5: "VR_ERR_TIMEOUT", 6: "VR_ERR_FIELD", 7: "VR_ERR_STATE", 8: "VR_ERR_ARG",
-          9: "VR_ERR_CAPACITY", 10: "VR_ERR_NODEVICE", 11: "VR_ERR_SCRATCH"}
+          9: "VR_ERR_CAPACITY", 10: "VR_ERR_NODEVICE", 11: "VR_ERR_SCRATCH", 12: "VR_ERR_IO"}
 FIELD_ID = {"q1": 0, "q2": 1, "q3": 2, "dq1": 3, "dq2": 4, "dq3": 5, "ru1": 6, "ru2": 7, "ru3": 8,
             "pres": 11, "prg": 12, "rhs": 13, "dph": 15, "dq3no": 19, "corr3s": 22, "corr3n": 23,
             "csort": 24, "tconv": 25}
@@ -87,6 +87,10 @@ def lib():
         L.vr_launch_count.argtypes = [vp, C.POINTER(i64)]
         L.vr_profile.argtypes = [vp, i32]
         L.vr_profile_read.argtypes = [vp, i32, C.POINTER(dp), C.POINTER(i64)]
+        L.vr_restart_save.argtypes = [vp, C.c_char_p, i32]
+        L.vr_restart_load.argtypes = [vp, C.c_char_p, C.POINTER(i32)]
+        L.vr_part_restart_save.argtypes = [vp, C.c_char_p]
+        L.vr_part_restart_load.argtypes = [vp, C.c_char_p]
         L.vr_part_create.argtypes = [vp, i32, i32, i32, C.POINTER(vp)]
         L.vr_part_destroy.argtypes = [vp]
         L.vr_part_info.argtypes = [vp, C.POINTER(dp), C.POINTER(dp), C.POINTER(dp), C.POINTER(i32)]
@@ -225,6 +229,16 @@ class Run:
             return lambda: self._chk(fn(self._h), name)
         raise AttributeError(name)
 
+    def restart_save(self, path, full: bool = False) -> None:
+        """restart_save (run.F90:390-460); full=True appends the whole state."""
+        self._chk(lib().vr_restart_save(self._h, str(path).encode(), 1 if full else 0), "restart_save")
+
+    def restart_load(self, path) -> bool:
+        """restart_load (run.F90:463-531); True when the whole state was restored."""
+        full = C.c_int32()
+        self._chk(lib().vr_restart_load(self._h, str(path).encode(), C.byref(full)), "restart_load")
+        return bool(full.value)
+
     def substep(self, irk: int):
         self._chk(lib().vr_substep(self._h, irk), "substep")
 
@@ -319,6 +333,12 @@ class Part:
     def set_inflow(self, r0: float, seed: int, on: bool = True) -> None:
         """Inflow injection every 10 steps inside Run.iterate (attached classes)."""
         self._chk(lib().vr_part_set_inflow(self._h, r0, seed, 1 if on else 0), "part_set_inflow")
+
+    def restart_save(self, path) -> None:
+        self._chk(lib().vr_part_restart_save(self._h, str(path).encode()), "part_restart_save")
+
+    def restart_load(self, path) -> None:
+        self._chk(lib().vr_part_restart_load(self._h, str(path).encode()), "part_restart_load")
 
     def attach(self, on: bool = True) -> None:
         self._chk(lib().vr_part_attach(self._h, 1 if on else 0), "part_attach")

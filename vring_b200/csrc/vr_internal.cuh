@@ -11,6 +11,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cstdio>
 #include <stdint.h>
 
 #include <string>
@@ -172,6 +174,14 @@ struct LaunchScope {
   LaunchScope(vr_ctx *ctx, int kind, cudaStream_t stream = nullptr);
   ~LaunchScope();
 };
+
+// gfortran unformatted sequential records (vr_restart.cu): the payload
+// framed by its byte length as a 4-byte little-endian integer on both sides;
+// data_* split an array into records of at most 2^24 doubles
+bool rec_write(FILE *f, const void *buf, size_t n);
+bool rec_read(FILE *f, void *buf, size_t n);
+bool data_write(FILE *f, const double *p, size_t n);
+bool data_read(FILE *f, double *p, size_t n);
 
 // enqueue the nsubdt Euler substeps of one particle class on stream s
 // (vr_particles.cu)

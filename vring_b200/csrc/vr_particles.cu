@@ -1105,3 +1105,94 @@ extern "C" int vr_part_probe(vr_part *p, const double *xyz, int32_t n, double *o
   cudaFree(dcell);
   return rc ? set_err(c, rc, "vr_part_probe") : VR_OK;
 }
+
+// ---- particle class restart --------------------------------------------
+// Records: a tagged header (magic, version, id, naloc, mode, npart, nlast,
+// nfree, nids, serial, inflow_on, nr, r0, rng), ifree(0:naloc+1),
+// isfre(0:naloc), inflow(0:nr+1), then u(naloc, 117) and v(naloc, 3).
+namespace {
+const char kPartMagic[8] = {'V', 'R', 'B', '2', 'P', 'R', 'T', '1'};
+struct PartHead {
+  char magic[8];
+  int32_t version, id, naloc, mode, npart, nlast, nfree, nids, serial, inflow_on, nr, pad;
+  double r0;
+  uint64_t rng;
+};
+}  // namespace
+
+extern "C" int vr_part_restart_save(vr_part *p, const char *path) {
+  if (!p || !path) return VR_ERR_ARG;
+  vr_ctx *c = p->ctx;
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  int rc = part_sync_bookkeeping(p);
+  if (rc) return rc;
+  PartHead h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kPartMagic, 8);
+  h.version = 1;
+  h.id = p->id;
+  h.naloc = p->naloc;
+  h.mode = p->mode;
+  h.npart = p->npart;
+  h.nlast = p->nlast;
+  h.nfree = p->nfree;
+  h.nids = p->nids;
+  h.serial = p->serial;
+  h.inflow_on = p->inflow_on;
+  h.nr = c->geo.nr;
+  h.r0 = p->r0;
+  h.rng = p->rng;
+  std::vector<double> u((size_t)p->naloc * 117), v((size_t)p->naloc * 3);
+  VR_CUDA(c, cudaMemcpy(u.data(), p->u, sizeof(double) * u.size(), cudaMemcpyDeviceToHost));
+  VR_CUDA(c, cudaMemcpy(v.data(), p->v, sizeof(double) * v.size(), cudaMemcpyDeviceToHost));
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return set_err(c, VR_ERR_IO, std::string("cannot open ") + path);
+  bool ok = rec_write(f, &h, sizeof(h)) && rec_write(f, p->ifree.data(), sizeof(int) * p->ifree.size()) &&
+            rec_write(f, p->h_isfre.data(), sizeof(int) * p->h_isfre.size()) &&
+            rec_write(f, p->inflow.data(), sizeof(double) * p->inflow.size()) &&
+            data_write(f, u.data(), u.size()) && data_write(f, v.data(), v.size());
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? VR_OK : set_err(c, VR_ERR_IO, std::string("write failed: ") + path);
+}
+
+extern "C" int vr_part_restart_load(vr_part *p, const char *path) {
+  if (!p || !path) return VR_ERR_ARG;
+  vr_ctx *c = p->ctx;
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return set_err(c, VR_ERR_IO, std::string("cannot open ") + path);
+  PartHead h;
+  bool ok = rec_read(f, &h, sizeof(h)) && !std::memcmp(h.magic, kPartMagic, 8) && h.version == 1;
+  if (ok && (h.naloc != p->naloc || h.id != p->id || h.mode != p->mode || h.nr != c->geo.nr)) {
+    std::fclose(f);
+    return set_err(c, VR_ERR_STATE, "particle restart: class id, naloc, mode or grid differ");
+  }
+  std::vector<int> ifree(p->ifree.size()), isfre(p->h_isfre.size());
+  std::vector<double> inflow(p->inflow.size()), u((size_t)p->naloc * 117), v((size_t)p->naloc * 3);
+  ok = ok && rec_read(f, ifree.data(), sizeof(int) * ifree.size()) &&
+       rec_read(f, isfre.data(), sizeof(int) * isfre.size()) &&
+       rec_read(f, inflow.data(), sizeof(double) * inflow.size()) && data_read(f, u.data(), u.size()) &&
+       data_read(f, v.data(), v.size());
+  std::fclose(f);
+  if (!ok) return set_err(c, VR_ERR_IO, std::string("particle restart: bad file ") + path);
+  p->npart = h.npart;
+  p->nlast = h.nlast;
+  p->nfree = h.nfree;
+  p->nids = h.nids;
+  p->serial = h.serial;
+  p->inflow_on = h.inflow_on != 0;
+  p->r0 = h.r0;
+  p->rng = h.rng;
+  p->ifree = ifree;
+  p->h_isfre = isfre;
+  p->inflow = inflow;
+  std::vector<int> d_isf(p->naloc);
+  for (int i = 0; i < p->naloc; i++) d_isf[i] = isfre[i + 1];
+  VR_CUDA(c, cudaMemcpy(p->u, u.data(), sizeof(double) * u.size(), cudaMemcpyHostToDevice));
+  VR_CUDA(c, cudaMemcpy(p->v, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+  VR_CUDA(c, cudaMemcpy(p->isfre, d_isf.data(), sizeof(int) * d_isf.size(), cudaMemcpyHostToDevice));
+  VR_CUDA(c, cudaMemset(p->gone, 0xff, sizeof(int) * p->naloc));
+  VR_CUDA(c, cudaMemset(p->d_nremoved, 0, sizeof(int)));
+  return VR_OK;
+}
