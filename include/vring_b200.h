@@ -137,6 +137,18 @@ VR_API int vr_restart_save(vr_ctx *ctx, const char *path, int32_t flags);
  * state was restored.  VR_ERR_FIELD when the grid differs. */
 VR_API int vr_restart_load(vr_ctx *ctx, const char *path, int32_t *full);
 
+/* ---- diagnostics of analysis (run.F90:238-388) --------------------------- */
+/* Without the Tecplot files: copies r-row 1 into ghost row 0 of q1..q3 as the
+ * reference does, takes the maxima of the azimuthal vorticity and the swirl
+ * over the core region and the weighted sums for their centroids, updates the
+ * context's para%stat and the centroid speeds over anlstp steps.  out[13] (may
+ * be NULL): ntime, vortmax, swrlmax and the ten analysis.dat columns after
+ * them.  path (may be NULL): the analysis.dat line, (I5,20(E16.8)), written
+ * to a new file at nstep 1 and appended otherwise. */
+VR_API int vr_analysis(vr_ctx *ctx, int32_t anlstp, double out[13], const char *path);
+/* gfortran's E16.8 edit descriptor into buf (17 bytes) */
+VR_API int vr_format_e16_8(double x, char *buf);
+
 /* ---- fused paths --------------------------------------------------------- */
 /* One RK substep irk (loop.F90:63-130 without particles), fused kernels. */
 VR_API int vr_substep(vr_ctx *ctx, int32_t irk);

@@ -85,6 +85,7 @@ def lib():
         L.orc_iter_part.argtypes = [vp, vp, i32]
         L.orc_part_probe.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, vp]
         L.orc_part_cell.argtypes = [vp, C.c_double, C.c_double, C.c_double, vp, vp]
+        L.orc_analysis.argtypes = [vp, i32, vp]
         L.orc_restart_save.restype = i32
         L.orc_restart_save.argtypes = [vp, C.c_char_p]
         L.orc_restart_load.restype = i32
@@ -157,6 +158,13 @@ class Oracle:
 
     def substep(self, irk: int):
         lib().orc_substep(self._h, irk)
+
+    def analysis(self, anlstp: int) -> np.ndarray:
+        """analysis (run.F90:238-388): ntime, vortmax, swrlmax and the ten
+        analysis.dat columns after them."""
+        out = np.zeros(13)
+        lib().orc_analysis(self._h, anlstp, _ptr(out))
+        return out
 
     def restart_save(self, path: str) -> int:
         """restart_save (run.F90:390-460); 0 on success."""

@@ -45,6 +45,7 @@ struct orc_ctx {
   double ntime;
   int64_t nstep;
   double unom0, unom1;
+  double stat[20]; /* para%stat, the analysis accumulators (para_tools.F90:36) */
   /* solu_toolsII.F90 coefficient vectors (Fortran index == array index) */
   double *h1d11, *h1d22d, *h1d22n, *h1dare, *h2d11, *h2d22m, *h2d22p, *h2dare;
   double *s1t11, *s1t2n, *s1t2s, *s1t2c, *s2t11, *s2t2p, *s2t2m, *s2t2c;
@@ -2104,4 +2105,96 @@ int32_t orc_restart_load(orc_ctx *c, const char *path) {
     c->ntime = ntime;
   }
   return rc;
+}
+
+/* ======================================================================== */
+/* analysis: run.F90:238-388                                                 */
+/* ======================================================================== */
+/* One rank, Tecplot output left out.  Copies r-row 1 into ghost row 0 of
+ * q1..q3 for iz = 1..nz (run.F90:305-307), takes in pass 1 the maxima of the
+ * azimuthal vorticity vort = dv/dz - dw/dr and of the swirl q1m over the core
+ * region 0.1 zmax < zm < 0.9 zmax, 0.05 rmax < rm < 0.8 rmax, ir != 1, and in
+ * pass 2 the weighted sums of vort^2 and swrl^2 where they are positive; then
+ * updates para%stat and the centroid speeds stat(9), stat(10) over anlstp
+ * steps.  out[13]: ntime, vortmax, swrlmax and the ten analysis.dat
+ * columns that follow (run.F90:383). */
+void orc_analysis(orc_ctx *c, int32_t anlstp, double *out) {
+  const int nth = c->nth, nr = c->nr, nz = c->nz;
+  for (int iz = 1; iz <= nz; iz++)
+    for (int ith = 1; ith <= nth; ith++) {
+      Q3(ith, 0, iz) = Q3(ith, 1, iz);
+      Q2(ith, 0, iz) = Q2(ith, 1, iz);
+      Q1(ith, 0, iz) = Q1(ith, 1, iz);
+    }
+  const double *rm = c->rm, *zm = c->zm;
+  double vortmaxall = 0.0, swrlmaxall = 0.0;
+  double xvort = 0.0, yvort = 0.0, vvort = 0.0, uvort = 0.0, xswrl = 0.0, yswrl = 0.0, vswrl = 0.0, uswrl = 0.0;
+  for (int ipass = 1; ipass <= 2; ipass++) {
+    double vortmax = SP(-10000.0f), swrlmax = SP(-10000.0f);
+    for (int iz = 1; iz <= nz; iz++)
+      for (int ir = 1; ir <= nr; ir++)
+        for (int ith = 1; ith <= nth; ith++) {
+          int ithp1 = ith + 1;
+          if (ithp1 > nth) ithp1 = 1;
+          double q1m = nth > 1 ? 0.5 * (Q1(ith, ir, iz) + Q1(ithp1, ir, iz)) : 1.0 * Q1(ith, ir, iz);
+          double dwdr = 0.5 * ((Q3(ith, ir + 1, iz) + Q3(ith, ir + 1, iz + 1)) -
+                               (Q3(ith, ir - 1, iz) + Q3(ith, ir - 1, iz + 1))) /
+                        (rm[ir + 1] - rm[ir - 1]);
+          double dvdz = 0.5 * ((Q2(ith, ir, iz + 1) / rm[ir] + Q2(ith, ir + 1, iz + 1) / rm[ir + 1]) -
+                               (Q2(ith, ir + 1, iz - 1) / rm[ir + 1] + Q2(ith, ir, iz - 1) / rm[ir])) /
+                        (zm[iz + 1] - zm[iz - 1]);
+          double vort = +(dvdz - dwdr);
+          double swrl = q1m;
+          if (zm[iz] < SP(0.90f) * c->dzmax && zm[iz] > SP(0.10f) * c->dzmax && rm[ir] < SP(0.80f) * c->drmax &&
+              rm[ir] > c->drmax * SP(0.05f) && ir != 1) {
+            if (ipass == 1) {
+              vortmax = vort > vortmax ? vort : vortmax;
+              swrlmax = swrl > swrlmax ? swrl : swrlmax;
+            } else {
+              if (vort > SP(0.00f) * vortmaxall) {
+                xvort = xvort + zm[iz] * (vort * vort) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                vvort = vvort + (vort * vort) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                yvort = yvort + (vort * vort) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                uvort = uvort + (vort * vort) * c->dx1 * c->dx2 * c->dx3;
+              }
+              if (swrl > SP(0.0f) * swrlmaxall) {
+                xswrl = xswrl + zm[iz] * (swrl * swrl) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                vswrl = vswrl + (swrl * swrl) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                yswrl = yswrl + (swrl * swrl) * rm[ir] * c->dx1 * c->dx2 * c->dx3;
+                uswrl = uswrl + (swrl * swrl) * c->dx1 * c->dx2 * c->dx3;
+              }
+            }
+          }
+        }
+    if (ipass == 1) {
+      vortmaxall = vortmax;
+      swrlmaxall = swrlmax;
+    }
+  }
+  double *st = c->stat;
+  double xvortold = st[0] / st[2], xswrlold = st[4] / st[6];
+  st[0] = xvort;
+  st[1] = yvort;
+  st[2] = vvort;
+  st[3] = uvort;
+  st[4] = xswrl;
+  st[5] = yswrl;
+  st[6] = vswrl;
+  st[7] = uswrl;
+  double xvortnew = st[0] / st[2], xswrlnew = st[4] / st[6];
+  st[8] = (xvortnew - xvortold) / (c->p.dt * anlstp);
+  st[9] = (xswrlnew - xswrlold) / (c->p.dt * anlstp);
+  out[0] = c->ntime;
+  out[1] = vortmaxall;
+  out[2] = swrlmaxall;
+  out[3] = pow(st[0], 1.0) / pow(st[2], 1.0);
+  out[4] = pow(st[1], (double)(1.0f / 2.0f)) / pow(st[3], (double)(1.0f / 2.0f));
+  out[5] = st[2];
+  out[6] = st[3];
+  out[7] = pow(st[4], 1.0) / pow(st[6], 1.0);
+  out[8] = pow(st[5], (double)(1.0f / 2.0f)) / pow(st[7], (double)(1.0f / 2.0f));
+  out[9] = pow(st[6], 1.0);
+  out[10] = pow(st[7], (double)(1.0f / 2.0f));
+  out[11] = st[8];
+  out[12] = st[9];
 }

@@ -131,6 +131,11 @@ void orc_part_cell(orc_ctx *c, double x, double y, double z, int32_t *idx3, doub
 /* acos restated for bit-identical cell indices on CPU and GPU */
 double orc_vr_acos(double x);
 
+/* analysis (run.F90:238-388) on one rank without the Tecplot output:
+ * out[13] = ntime, vortmax, swrlmax and the ten analysis.dat columns after
+ * them; updates the stat accumulators and ghost row 0 of q1..q3 */
+void orc_analysis(orc_ctx *c, int32_t anlstp, double *out);
+
 /* ---- restart files (run.F90:390-539), gfortran sequential records --- */
 /* 0 on success, -1 on an I/O or format error, -2 on a grid mismatch */
 int32_t orc_restart_save(orc_ctx *c, const char *path);

@@ -57,3 +57,18 @@ def test_descriptor_validation_codes():
     bad = Desc(1, 8, 16, 16, 4.0, 12.0, 1e-3, 100.0, 1.0, 0.0, 1, 0, 0, 0, 0)
     assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # VR_MIXED: not built
     assert L.vr_create(None, ctypes.byref(h)) == 8                   # VR_ERR_ARG
+
+
+def test_analysis_line_uses_gfortran_e16_8():
+    """analysis.dat is written with (I5,20(E16.8)) (run.F90:383); the library's
+    formatter follows gfortran's Ew.d layout: 0.d1..d8, exponent letter and a
+    two-digit exponent (three digits and no letter beyond 99)."""
+    from vring_b200.api import format_e16_8 as f
+    assert f(1.0) == "  0.10000000E+01"
+    assert f(-3.141592653589793) == " -0.31415927E+01"
+    assert f(123456789.0) == "  0.12345679E+09"
+    assert f(2.5e-5) == "  0.25000000E-04"
+    assert f(0.0) == "  0.00000000E+00"
+    assert f(1e-101) == "  0.10000000-100"
+    assert f(float("nan")) == "             NaN"
+    assert all(len(f(x)) == 16 for x in (1.0, -1e300, 7e-7, 0.999999999))

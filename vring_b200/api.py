@@ -87,6 +87,8 @@ def lib():
         L.vr_launch_count.argtypes = [vp, C.POINTER(i64)]
         L.vr_profile.argtypes = [vp, i32]
         L.vr_profile_read.argtypes = [vp, i32, C.POINTER(dp), C.POINTER(i64)]
+        L.vr_analysis.argtypes = [vp, i32, vp, C.c_char_p]
+        L.vr_format_e16_8.argtypes = [dp, C.c_char_p]
         L.vr_restart_save.argtypes = [vp, C.c_char_p, i32]
         L.vr_restart_load.argtypes = [vp, C.c_char_p, C.POINTER(i32)]
         L.vr_part_restart_save.argtypes = [vp, C.c_char_p]
@@ -228,6 +230,14 @@ class Run:
             fn = getattr(lib(), "vr_" + name)
             return lambda: self._chk(fn(self._h), name)
         raise AttributeError(name)
+
+    def analysis(self, anlstp: int, path=None) -> np.ndarray:
+        """analysis (run.F90:238-388): ntime, vortmax, swrlmax and the ten
+        analysis.dat columns after them; appends the line to path if given."""
+        out = np.zeros(13)
+        self._chk(lib().vr_analysis(self._h, anlstp, _p(out), None if path is None else str(path).encode()),
+                  "analysis")
+        return out
 
     def restart_save(self, path, full: bool = False) -> None:
         """restart_save (run.F90:390-460); full=True appends the whole state."""
@@ -394,3 +404,12 @@ def solve_lap_thom_noalloc(rhs_ptr: int, sol_ptr: int, aa_ptr: int, bb_ptr: int,
                                          C.c_void_p(cuda_stream or None))
     if rc:
         raise VrError(rc, "vr_solve_lap_thom_noalloc(n=%d, nbatch=%d)" % (n, nbatch))
+
+
+def format_e16_8(x: float) -> str:
+    """gfortran's E16.8 edit descriptor, as the library writes analysis.dat."""
+    buf = C.create_string_buffer(17)
+    rc = lib().vr_format_e16_8(float(x), buf)
+    if rc:
+        raise VrError(rc, "vr_format_e16_8")
+    return buf.value.decode()

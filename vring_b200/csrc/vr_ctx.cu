@@ -526,6 +526,8 @@ extern "C" int vr_destroy(vr_ctx *c) {
     if (p) cudaFree(p);
   if (c->d_count) cudaFree(c->d_count);
   if (c->part_mesh) cudaFree(c->part_mesh);
+  if (c->ana_zm) cudaFree(c->ana_zm);
+  if (c->ana_part) cudaFree(c->ana_part);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   delete[] c->h_rc;
   delete[] c->h_rm;

@@ -140,6 +140,9 @@ struct vr_ctx {
   double *part_mesh;
   std::vector<vr_part *> parts;
   int nparts;
+  // analysis: para%stat (run.F90:365-374), zm on the device, block partials
+  double stat[20];
+  double *ana_zm, *ana_part;
 };
 
 namespace vr {
