@@ -220,6 +220,15 @@ VR_API int vr_part_set_state(vr_part *part, const double *u, const double *v, co
                              int32_t nlast);
 /* any pointer may be NULL; counts = {npart, nlast, nfree, nids} */
 VR_API int vr_part_get_state(vr_part *part, double *u, double *v, int32_t *isfre, int32_t counts[4]);
+/* the dumps of iter_part (part_tools.F90:444-491) into directory dir (NULL:
+ * the working directory): partNNNNNsizeII.dat with a title line, a variables
+ * line and one (200(E20.8)) line per live particle (v, u, and d(1) = det of
+ * the Jacobian), and trajectory_sizeII.dat appended with the particles whose
+ * id is 1 modulo 1000; NNNNN = the context's nstep, II = the class id */
+VR_API int vr_part_dump(vr_part *part, const char *dir);
+/* expstp > 0: vr_iterate writes the dumps of an attached class at the start
+ * of every step whose nstep is a multiple of expstp (0: off) */
+VR_API int vr_part_set_dump(vr_part *part, int32_t expstp, const char *dir);
 /* a particle class's whole state (arrays, free list, counters, inflow
  * remainders, random stream) to and from a file; the class loading it must
  * have the same id, naloc and mode (no reference counterpart: the reference

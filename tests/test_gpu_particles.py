@@ -255,3 +255,80 @@ def test_iterate_with_inflow_injection():
     _compare_parts(op, gp, rel=1e-10)
     gp.attach(False)
     gp.close()
+
+
+def _fortran_e(x, w=20, d=8):
+    """Ew.d as gfortran writes it (independent of the library's formatter)."""
+    if x == 0:
+        s = "0." + "0" * d + "E+00"
+    else:
+        m, e = ("%.*E" % (d - 1, abs(x))).split("E")
+        e = int(e) + 1
+        s = "0." + m.replace(".", "") + ("E%+03d" % e if abs(e) <= 99 else "%+04d" % e)
+    if x < 0:
+        s = "-" + s
+    return s.rjust(w)
+
+
+def test_part_dump_layout(tmp_path):
+    """part_tools.F90:444-491: the part file's header lines, one (200(E20.8))
+    line per live particle with d(1) = det of the Jacobian, and the trajectory
+    file with the particles whose id is 1 modulo 1000."""
+    import vring_b200 as V
+    gpu = V.Run(8, 16, 32, 4.0, 12.0, 1e-3, 1000.0, 1.0, 1.0)
+    naloc = 1300
+    p = V.Part(gpu, 3, naloc, 0)
+    rng = np.random.default_rng(8)
+    u = np.asfortranarray(rng.uniform(-2, 2, (naloc, 117)))
+    v = np.zeros((naloc, 3), order="F")
+    v[:, 1] = p.c
+    v[:, 2] = np.arange(1, naloc + 1)
+    isf = np.zeros(naloc, dtype=np.int32)
+    isf[[5, 600, 999]] = 1           # free slots: not written
+    p.set_state(u, v, isf, 1250)
+    p.dump(tmp_path)
+    lines = (tmp_path / "part00000size03.dat").read_text().split("\n")
+    assert lines[0] == ('title = "particles diameter: '.rjust(32) + _fortran_e(p.r) + " stokes: ".rjust(12)
+                        + _fortran_e(p.st) + '"'.rjust(2))
+    assert lines[1] == ('variables = "id", "time", "c",'.rjust(32) + "".join("   u%03d" % i for i in range(1, 118))
+                        + "".join("   d%03d" % i for i in range(1, 11)))
+    live = [ip for ip in range(1250) if isf[ip] == 0]
+    body = [l for l in lines[2:] if l]
+    assert len(body) == len(live)
+
+    def det(ip):
+        J = u[ip, 6:15].reshape(3, 3, order="F")
+        return np.linalg.det(J)
+
+    for l, ip in zip(body[::97], live[::97]):
+        vals = np.array([float(l[20 * i:20 * (i + 1)]) for i in range(130)])
+        np.testing.assert_allclose(vals[:3], v[ip], rtol=1e-7, atol=0)
+        np.testing.assert_allclose(vals[3:120], u[ip], rtol=1e-7, atol=1e-300)
+        np.testing.assert_allclose(vals[120], det(ip), rtol=1e-7)
+        assert np.all(vals[121:] == 0)
+    traj = (tmp_path / "trajectory_size03.dat").read_text().split("\n")
+    ids = [float(l[40:60]) for l in traj if l]
+    assert ids == [1.0, 1001.0]      # id 1 mod 1000, in slot order
+    last_d = float(body[-1][20 * 120:20 * 121])
+    assert all(float(l[20 * 120:20 * 121]) == last_d for l in traj if l)   # the dump loop's last d
+    assert traj[-2] == "" and traj[-1] == ""
+    p.close()
+
+
+def test_iterate_writes_dumps_every_expstp(tmp_path):
+    import vring_b200 as V
+    from vring_b200.synthetic import ring_fields
+    gpu = V.Run(8, 16, 32, 4.0, 12.0, 1e-3, 1000.0, 1.0, 1.0)
+    for n, a in zip(("q1", "q2", "q3"), ring_fields(8, 16, 32, 4.0, 12.0, seed=1)):
+        gpu.set(n, a)
+    p = V.Part(gpu, 2, 50, 1)
+    for i in range(10):
+        p.injc(1.0 + 0.01 * i, 0.2, 3.0)
+    p.set_dump(2, tmp_path)
+    p.attach(True)
+    gpu.iterate(5)
+    names = sorted(f.name for f in tmp_path.iterdir())
+    assert names == ["part00000size02.dat", "part00002size02.dat", "part00004size02.dat",
+                     "trajectory_size02.dat"]
+    p.attach(False)
+    p.close()

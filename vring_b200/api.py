@@ -91,6 +91,8 @@ def lib():
         L.vr_format_e16_8.argtypes = [dp, C.c_char_p]
         L.vr_restart_save.argtypes = [vp, C.c_char_p, i32]
         L.vr_restart_load.argtypes = [vp, C.c_char_p, C.POINTER(i32)]
+        L.vr_part_dump.argtypes = [vp, C.c_char_p]
+        L.vr_part_set_dump.argtypes = [vp, i32, C.c_char_p]
         L.vr_part_restart_save.argtypes = [vp, C.c_char_p]
         L.vr_part_restart_load.argtypes = [vp, C.c_char_p]
         L.vr_part_create.argtypes = [vp, i32, i32, i32, C.POINTER(vp)]
@@ -343,6 +345,14 @@ class Part:
     def set_inflow(self, r0: float, seed: int, on: bool = True) -> None:
         """Inflow injection every 10 steps inside Run.iterate (attached classes)."""
         self._chk(lib().vr_part_set_inflow(self._h, r0, seed, 1 if on else 0), "part_set_inflow")
+
+    def dump(self, directory=None) -> None:
+        """iter_part's dumps (part_tools.F90:444-491) into directory."""
+        self._chk(lib().vr_part_dump(self._h, None if directory is None else str(directory).encode()), "part_dump")
+
+    def set_dump(self, expstp: int, directory=None) -> None:
+        self._chk(lib().vr_part_set_dump(self._h, expstp, None if directory is None else str(directory).encode()),
+                  "part_set_dump")
 
     def restart_save(self, path) -> None:
         self._chk(lib().vr_part_restart_save(self._h, str(path).encode()), "part_restart_save")

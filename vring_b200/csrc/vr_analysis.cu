@@ -140,34 +140,41 @@ __global__ void k_ana_final(const double *part, int nb, int nv, bool is_max, dou
 
 using namespace vr;
 
-// gfortran's Ew.d edit descriptor for w = 16, d = 8 ("  0.12345678E+01")
-static std::string fmt_e16_8(double x) {
-  char buf[64];
+// gfortran's Ew.d edit descriptor ("  0.12345678E+01" for E16.8): sign,
+// "0.", d significant digits correctly rounded, the exponent with its letter
+// and two digits (three digits and no letter beyond 99), right-justified in w
+std::string vr::fmt_e(double x, int w, int d) {
+  char buf[96];
   if (std::isnan(x)) {
-    std::snprintf(buf, sizeof(buf), "%16s", "NaN");
+    std::snprintf(buf, sizeof(buf), "%*s", w, "NaN");
     return buf;
   }
   if (std::isinf(x)) {
-    std::snprintf(buf, sizeof(buf), "%16s", x < 0 ? "-Infinity" : "Infinity");
+    std::snprintf(buf, sizeof(buf), "%*s", w, x < 0 ? "-Infinity" : "Infinity");
     return buf;
   }
+  std::string digits, eb;
+  int e = 0;
   if (x == 0.0) {
-    std::snprintf(buf, sizeof(buf), "%16s", std::signbit(x) ? "-0.00000000E+00" : "0.00000000E+00");
-    return buf;
+    digits.assign(d, '0');
+  } else {
+    char t[96];
+    std::snprintf(t, sizeof(t), "%.*E", d - 1, std::fabs(x));  // m.mmm..E+xx, correctly rounded
+    e = std::atoi(std::strchr(t, 'E') + 1) + 1;
+    digits = std::string(1, t[0]) + std::string(t + 2, d - 1);
   }
-  char t[64];
-  std::snprintf(t, sizeof(t), "%.7E", std::fabs(x));  // d.dddddddE+xx, correctly rounded
-  const int e = std::atoi(std::strchr(t, 'E') + 1) + 1;
-  std::string digits = std::string(1, t[0]) + std::string(t + 2, 7);
-  char eb[16];
+  char ebuf[16];
   if (std::abs(e) <= 99)
-    std::snprintf(eb, sizeof(eb), "E%c%02d", e < 0 ? '-' : '+', std::abs(e));
+    std::snprintf(ebuf, sizeof(ebuf), "E%c%02d", e < 0 ? '-' : '+', std::abs(e));
   else
-    std::snprintf(eb, sizeof(eb), "%c%03d", e < 0 ? '-' : '+', std::abs(e));
-  std::string s = std::string(x < 0 ? "-" : "") + "0." + digits + eb;
-  std::snprintf(buf, sizeof(buf), "%16s", s.c_str());
+    std::snprintf(ebuf, sizeof(ebuf), "%c%03d", e < 0 ? '-' : '+', std::abs(e));
+  const std::string s = std::string(std::signbit(x) ? "-" : "") + "0." + digits + ebuf;
+  if ((int)s.size() > w) return std::string(w, '*');
+  std::snprintf(buf, sizeof(buf), "%*s", w, s.c_str());
   return buf;
 }
+
+static std::string fmt_e16_8(double x) { return vr::fmt_e(x, 16, 8); }
 
 extern "C" int vr_analysis(vr_ctx *c, int32_t anlstp, double out[13], const char *path) {
   if (!c || anlstp < 1) return VR_ERR_ARG;

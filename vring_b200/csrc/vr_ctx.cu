@@ -851,9 +851,12 @@ extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
         if (rc) return rc;
       }
     // loop.F90:65-70: particles advance once per step, before ucoeff, in the
-    // velocity at the start of the step
+    // velocity at the start of the step; iter_part first writes its dumps
+    // (part_tools.F90:444-491) on dump steps
     for (vr_part *p : c->parts) {
-      int rc = vr_part_enqueue(p, c->stream);
+      int rc = vr_part_dump_step(p);
+      if (rc) return rc;
+      rc = vr_part_enqueue(p, c->stream);
       if (rc) return rc;
     }
     for (int irk = 1; irk <= 3; irk++) {

@@ -178,6 +178,9 @@ struct LaunchScope {
   ~LaunchScope();
 };
 
+// gfortran's Ew.d edit descriptor (vr_analysis.cu)
+std::string fmt_e(double x, int w, int d);
+
 // gfortran unformatted sequential records (vr_restart.cu): the payload
 // framed by its byte length as a 4-byte little-endian integer on both sides;
 // data_* split an array into records of at most 2^24 doubles
@@ -191,6 +194,8 @@ bool data_read(FILE *f, double *p, size_t n);
 int vr_part_enqueue(vr_part *p, cudaStream_t s);
 // inlt_part for a class whose inflow injection is on (host, synchronous)
 int vr_part_inflow_step(vr_part *p);
+// the dump of part_tools.F90:444-491 when this step is a dump step
+int vr_part_dump_step(vr_part *p);
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);

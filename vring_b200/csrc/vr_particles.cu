@@ -59,6 +59,9 @@ struct vr_part {
   double r0;
   uint64_t rng;
   bool inflow_on;
+  // dumps of part_tools.F90:444-491 every dump_every steps into dump_dir
+  int dump_every;
+  std::string dump_dir;
 };
 
 namespace vr {
@@ -1195,4 +1198,90 @@ extern "C" int vr_part_restart_load(vr_part *p, const char *path) {
   VR_CUDA(c, cudaMemset(p->gone, 0xff, sizeof(int) * p->naloc));
   VR_CUDA(c, cudaMemset(p->d_nremoved, 0, sizeof(int)));
   return VR_OK;
+}
+
+// ---- particle dumps (part_tools.F90:444-491) ------------------------------
+// partNNNNNsizeII.dat: a title line, a variables line and one (200(E20.8))
+// line per live particle: v(1:3), u(1:117), d(1:10) with d(1) the
+// determinant of the Jacobian (d(2:10) are never set by the reference and are
+// written as 0).  trajectory_sizeII.dat (appended): the same line for the
+// particles whose id is 1 modulo 1000, carrying the d of the last particle of
+// the dump loop as the reference does, then an empty record.
+static std::string fmt_a(const std::string &s, size_t w) {
+  return s.size() >= w ? s.substr(0, w) : std::string(w - s.size(), ' ') + s;
+}
+
+static std::string fmt_i_pad0(long long v, int w) {
+  char b[32];
+  std::snprintf(b, sizeof(b), "%0*lld", w, v);
+  return (v < 0 || (int)std::strlen(b) > w) ? std::string(w, '*') : std::string(b);
+}
+
+static int part_dump(vr_part *p, const std::string &dir) {
+  vr_ctx *c = p->ctx;
+  int rc = part_sync_bookkeeping(p);
+  if (rc) return rc;
+  const size_t N = (size_t)p->naloc;
+  std::vector<double> u(N * 117), v(N * 3);
+  VR_CUDA(c, cudaMemcpy(u.data(), p->u, sizeof(double) * u.size(), cudaMemcpyDeviceToHost));
+  VR_CUDA(c, cudaMemcpy(v.data(), p->v, sizeof(double) * v.size(), cudaMemcpyDeviceToHost));
+  const std::string t5 = fmt_i_pad0(c->nstep, 5), b2 = fmt_i_pad0(p->id, 2);
+  const std::string base = dir.empty() ? std::string() : dir + "/";
+  const std::string fpart = base + "part" + t5 + "size" + b2 + ".dat";
+  FILE *f = std::fopen(fpart.c_str(), "w");
+  if (!f) return set_err(c, VR_ERR_IO, "cannot open " + fpart);
+  std::string hdr = fmt_a("title = \"particles diameter: ", 32) + fmt_e(p->r, 20, 8) + fmt_a(" stokes: ", 12) +
+                    fmt_e(p->st, 20, 8) + fmt_a("\"", 2) + "\n";
+  hdr += fmt_a("variables = \"id\", \"time\", \"c\",", 32);
+  for (int ii = 1; ii <= 117; ii++) hdr += fmt_a("u", 4) + fmt_i_pad0(ii, 3);
+  for (int ii = 1; ii <= 10; ii++) hdr += fmt_a("d", 4) + fmt_i_pad0(ii, 3);
+  hdr += "\n";
+  bool ok = std::fputs(hdr.c_str(), f) >= 0;
+  double d[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  auto U = [&](size_t ip, int iv) { return u[(ip - 1) + N * (iv - 1)]; };
+  auto line = [&](size_t ip) {
+    std::string l;
+    l.reserve(130 * 20 + 1);
+    for (int ii = 1; ii <= 3; ii++) l += fmt_e(v[(ip - 1) + N * (ii - 1)], 20, 8);
+    for (int ii = 1; ii <= 117; ii++) l += fmt_e(U(ip, ii), 20, 8);
+    for (int ii = 0; ii < 10; ii++) l += fmt_e(d[ii], 20, 8);
+    return l + "\n";
+  };
+  const int j = 6;  // ijac
+  for (int ip = 1; ip <= p->nlast && ok; ip++) {
+    if (p->h_isfre[ip] != 0) continue;
+    d[0] = U(ip, j + 1) * U(ip, j + 5) * U(ip, j + 9) + U(ip, j + 2) * U(ip, j + 6) * U(ip, j + 7) +
+           U(ip, j + 3) * U(ip, j + 4) * U(ip, j + 8) - U(ip, j + 7) * U(ip, j + 5) * U(ip, j + 3) -
+           U(ip, j + 4) * U(ip, j + 2) * U(ip, j + 9) - U(ip, j + 8) * U(ip, j + 6) * U(ip, j + 1);
+    ok = std::fputs(line(ip).c_str(), f) >= 0;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return set_err(c, VR_ERR_IO, "write failed: " + fpart);
+  const std::string ftraj = base + "trajectory_size" + b2 + ".dat";
+  f = std::fopen(ftraj.c_str(), "a");
+  if (!f) return set_err(c, VR_ERR_IO, "cannot open " + ftraj);
+  for (int ip = 1; ip <= p->nlast && ok; ip++)
+    if (p->h_isfre[ip] == 0 && std::fmod(v[(ip - 1) + N * 2] - 1.0, 1000.0) < 0.1)
+      ok = std::fputs(line(ip).c_str(), f) >= 0;
+  ok = ok && std::fputs("\n", f) >= 0;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? VR_OK : set_err(c, VR_ERR_IO, "write failed: " + ftraj);
+}
+
+extern "C" int vr_part_dump(vr_part *p, const char *dir) {
+  if (!p) return VR_ERR_ARG;
+  VR_CUDA(p->ctx, cudaSetDevice(p->ctx->dev));
+  return part_dump(p, dir ? std::string(dir) : std::string());
+}
+
+extern "C" int vr_part_set_dump(vr_part *p, int32_t expstp, const char *dir) {
+  if (!p) return VR_ERR_ARG;
+  p->dump_every = expstp > 0 ? expstp : 0;
+  p->dump_dir = dir ? dir : "";
+  return VR_OK;
+}
+
+int vr::vr_part_dump_step(vr_part *p) {
+  if (p->dump_every <= 0 || p->ctx->nstep % p->dump_every != 0) return VR_OK;
+  return part_dump(p, p->dump_dir);
 }
