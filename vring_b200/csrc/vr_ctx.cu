@@ -765,16 +765,17 @@ extern "C" int vr_hdnl3(vr_ctx *c) {
   return VR_OK;
 }
 
-static cudaError_t sweeps(vr_ctx *c) {
+// theta_done: the theta sweeps already ran inside the fused right-hand side
+static cudaError_t sweeps(vr_ctx *c, bool theta_done = false) {
   cudaError_t e;
   // q1: theta, r, z ; q3: theta, r, z ; q2: theta, z, r (step.F90:72-177)
-  if ((e = launch_tsweep(c, 1))) return e;
+  if (!theta_done && (e = launch_tsweep(c, 1))) return e;
   if ((e = launch_rsweep(c, 1))) return e;
   if ((e = launch_zsweep(c, 1))) return e;
-  if ((e = launch_tsweep(c, 3))) return e;
+  if (!theta_done && (e = launch_tsweep(c, 3))) return e;
   if ((e = launch_rsweep(c, 3))) return e;
   if ((e = launch_zsweep(c, 3))) return e;
-  if ((e = launch_tsweep(c, 2))) return e;
+  if (!theta_done && (e = launch_tsweep(c, 2))) return e;
   if ((e = launch_zsweep(c, 2))) return e;
   return launch_rsweep(c, 2);
 }
@@ -824,8 +825,15 @@ static int enqueue_substep(vr_ctx *c, int irk) {
   double cs, cor;
   hdnbc_scalars(c, &cs, &cor);
   VR_CUDA(c, launch_hdnbc(c, rk, cs, cor));
-  VR_CUDA(c, launch_rhs(c, rk, true));
-  VR_CUDA(c, sweeps(c));
+  cudaError_t fe = launch_rhs_tsweep(c, rk);
+  if (fe == cudaErrorNotSupported) {
+    (void)cudaGetLastError();
+    VR_CUDA(c, launch_rhs(c, rk, true));
+    VR_CUDA(c, sweeps(c));
+  } else {
+    VR_CUDA(c, fe);
+    VR_CUDA(c, sweeps(c, true));
+  }
   VR_CUDA(c, launch_divq(c, rk));
   VR_CUDA(c, launch_poisson(c));
   VR_CUDA(c, launch_upsol(c, rk));

@@ -199,6 +199,7 @@ int vr_part_dump_step(vr_part *p);
 
 // kernel launchers (return cudaError_t of the launch) -----------------------
 cudaError_t launch_hdnbc(vr_ctx *c, const Rk &rk, double corr3s_val, double cor);
+cudaError_t launch_rhs_tsweep(vr_ctx *c, const Rk &rk);
 cudaError_t launch_hdnl(vr_ctx *c, int comp);
 cudaError_t launch_rhs(vr_ctx *c, const Rk &rk, bool inline_h);
 cudaError_t launch_tsweep(vr_ctx *c, int comp);

@@ -247,11 +247,12 @@ __global__ void __launch_bounds__(128) k_rhs(Geo g, Rk rk, RhsArgs a) {
 // that of h1_at/h2_at/h3_at and k_rhs term by term; only the loads are shared.
 // A value that is only used on a boundary row/plane (k-1 at kc = 1, j-1 at
 // jc = 1) is still loaded from the ghost row/plane, which is allocated.
-__global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
-  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int kc = 1 + blockIdx.z;
-  if (ic > g.nth || jc > g.nr) return;
+struct RhsCell {
+  double h1, h2, h3, r1, r2, r3;
+};
+
+__device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsArgs &a, int ic, int jc, int kc,
+                                         RhsCell &out) {
   const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
   const int jm = jc > 1 ? jc - 1 : 1;
   const double *__restrict__ q1 = a.q.q1, *__restrict__ q2 = a.q.q2, *__restrict__ q3 = a.q.q3;
@@ -351,15 +352,26 @@ __global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
     const double d22 = B4 * g.s2t2p[jc] - qc * g.s2t2c[jc] + B5 * g.s2t2m[jc];
     r2 = (rk.gam * h2 + rk.rom * ru2 - rk.alm * pg2 + are * (d11 + d33 + d22)) * g.dt;
   }
-  a.qrhs[0][o] = r1;
-  a.ru[0][o] = h1;
-  if (do3) {
-    a.qrhs[2][o] = r3;
-    a.ru[2][o] = h3;
+  out = RhsCell{h1, h2, h3, r1, r2, r3};
+}
+
+__global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
+  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int kc = 1 + blockIdx.z;
+  if (ic > g.nth || jc > g.nr) return;
+  RhsCell v;
+  rhs_cell(g, rk, a, ic, jc, kc, v);
+  const int o = I3(g, ic, jc, kc);
+  a.qrhs[0][o] = v.r1;
+  a.ru[0][o] = v.h1;
+  if (kc >= 2) {
+    a.qrhs[2][o] = v.r3;
+    a.ru[2][o] = v.h3;
   }
-  if (do2) {
-    a.qrhs[1][o] = r2;
-    a.ru[1][o] = h2;
+  if (jc >= 2) {
+    a.qrhs[1][o] = v.r2;
+    a.ru[1][o] = v.h2;
   }
 }
 
@@ -400,29 +412,13 @@ __device__ __forceinline__ Aff aff_then(const Aff &first, const Aff &second) {
 // inner unknowns [l E, l E + E).
 __host__ __device__ __forceinline__ int tpad(int i) { return i + (i >> 4); }
 
+// Periodic theta solve of one line held in shared memory (sl, padded by
+// tpad) by one warp, with the row's factorisation cinv/cpp/czz (padded) and
+// its scalars A = sub, sup, za2 (tripij's bordered algorithm, step.F90:487-534).
+// Lane l owns the E contiguous inner unknowns [l E, l E + E).
 template <int E>
-__global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nk) {
-  extern __shared__ double sm[];
-  const int N = g.nth;
-  const int SPN = tpad(N) + 1;
-  double *cinv = sm, *cpp = sm + SPN, *czz = sm + 2 * SPN, *lines = sm + 3 * SPN;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int jc = jb + blockIdx.y;
-  const int kc = kb + blockIdx.x * 8 + warp;
-  const bool active = kc < kb + nk;
-  for (int i = threadIdx.x; i < N; i += 256) {
-    cp_async8(cinv + tpad(i), t.inv + (size_t)jc * N + i);
-    cp_async8(cpp + tpad(i), t.pp + (size_t)jc * N + i);
-    cp_async8(czz + tpad(i), t.zz + (size_t)jc * N + i);
-  }
-  double *sl = lines + (size_t)warp * SPN;
-  double *line = f + I3(g, 1, jc, active ? kc : kb);
-  if (active)
-    for (int i = lane; i < N; i += 32) cp_async8(sl + tpad(i), line + i);
-  cp_async_wait_all();
-  __syncthreads();
-  if (!active) return;
-  const double A = t.sub[jc];
+__device__ __forceinline__ void tsolve_warp(int N, const double *cinv, const double *cpp, const double *czz,
+                                            double A, double sup, double za2, double *sl, int lane) {
   const int inner = N - 1;
   const int i0 = lane * E;
   int cnt = inner - i0;
@@ -489,14 +485,133 @@ __global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restr
     if (e == last_e) wl = y[e];
   wl = __shfl_sync(0xffffffffu, wl, last_lane);
   const double fN = sl[tpad(N - 1)];
-  const double xN = (fN - t.sup[jc] * w1 - A * wl) / t.za2[jc];
+  const double xN = (fN - sup * w1 - A * wl) / za2;
   __syncwarp();
 #pragma unroll
   for (int e = 0; e < E; e++)
     if (e < cnt) sl[tpad(i0 + e)] = y[e] + czz[tpad(i0 + e)] * xN;
   if (lane == 0) sl[tpad(N - 1)] = xN;
   __syncwarp();
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restrict__ f, int jb, int kb, int nk) {
+  extern __shared__ double sm[];
+  const int N = g.nth;
+  const int SPN = tpad(N) + 1;
+  double *cinv = sm, *cpp = sm + SPN, *czz = sm + 2 * SPN, *lines = sm + 3 * SPN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int jc = jb + blockIdx.y;
+  const int kc = kb + blockIdx.x * 8 + warp;
+  const bool active = kc < kb + nk;
+  for (int i = threadIdx.x; i < N; i += 256) {
+    cp_async8(cinv + tpad(i), t.inv + (size_t)jc * N + i);
+    cp_async8(cpp + tpad(i), t.pp + (size_t)jc * N + i);
+    cp_async8(czz + tpad(i), t.zz + (size_t)jc * N + i);
+  }
+  double *sl = lines + (size_t)warp * SPN;
+  double *line = f + I3(g, 1, jc, active ? kc : kb);
+  if (active)
+    for (int i = lane; i < N; i += 32) cp_async8(sl + tpad(i), line + i);
+  cp_async_wait_all();
+  __syncthreads();
+  if (!active) return;
+  tsolve_warp<E>(N, cinv, cpp, czz, t.sub[jc], t.sup[jc], t.za2[jc], sl, lane);
   for (int i = lane; i < N; i += 32) line[i] = sl[tpad(i)];
+}
+
+// Fused hdnl1-3 + RHS + theta sweep (solqi, step.F90:212-263) of all three
+// components for a tile of RJ r-rows x RK z-planes and every theta: the
+// right-hand sides go to shared memory, then each warp solves whole theta
+// lines there with the row's factorisation and writes the solved line;
+// qrhs is written once instead of written, read and written again.
+constexpr int kRJ = 1, kRK = 8;
+
+template <int E>
+__global__ void __launch_bounds__(256, 2) k_rhs_tsweep(Geo g, Rk rk, RhsArgs a, TriPer t13, TriPer t2) {
+  extern __shared__ double sm[];
+  const int N = g.nth, SPN = tpad(N) + 1;
+  double *lines = sm;                        // [comp][r][kk], each SPN
+  double *fac = sm + 3 * kRJ * kRK * SPN;    // [fam][r][inv, pp, zz], each SPN
+  const int j0 = 1 + blockIdx.x * kRJ, k0 = 1 + blockIdx.y * kRK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int idx = threadIdx.x; idx < 2 * kRJ * N; idx += blockDim.x) {
+    const int i = idx % N, r = (idx / N) % kRJ, fam = idx / (N * kRJ), jc = j0 + r;
+    if (jc > g.nr) continue;
+    const double *inv = fam ? t2.inv : t13.inv, *pp = fam ? t2.pp : t13.pp, *zz = fam ? t2.zz : t13.zz;
+    double *f = fac + (size_t)(fam * kRJ + r) * 3 * SPN;
+    cp_async8(f + tpad(i), inv + (size_t)jc * N + i);
+    cp_async8(f + SPN + tpad(i), pp + (size_t)jc * N + i);
+    cp_async8(f + 2 * SPN + tpad(i), zz + (size_t)jc * N + i);
+  }
+  for (int idx = threadIdx.x; idx < N * kRJ * kRK; idx += blockDim.x) {
+    const int i = idx % N, r = (idx / N) % kRJ, kk = idx / (N * kRJ);
+    const int jc = j0 + r, kc = k0 + kk;
+    if (jc > g.nr || kc > g.nz) continue;
+    RhsCell v;
+    rhs_cell(g, rk, a, i + 1, jc, kc, v);
+    const int o = I3(g, i + 1, jc, kc);
+    a.ru[0][o] = v.h1;
+    lines[(size_t)((0 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r1;
+    if (kc >= 2) {
+      a.ru[2][o] = v.h3;
+      lines[(size_t)((2 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r3;
+    }
+    if (jc >= 2) {
+      a.ru[1][o] = v.h2;
+      lines[(size_t)((1 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r2;
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int L = warp; L < 3 * kRJ * kRK; L += blockDim.x / 32) {
+    const int comp = L / (kRJ * kRK), r = (L / kRK) % kRJ, kk = L % kRK;
+    const int jc = j0 + r, kc = k0 + kk;
+    if (jc > g.nr || kc > g.nz || (comp == 1 && jc < 2) || (comp == 2 && kc < 2)) continue;
+    const int fam = comp == 1 ? 1 : 0;
+    const double A = fam ? t2.sub[jc] : t13.sub[jc], sup = fam ? t2.sup[jc] : t13.sup[jc];
+    const double za2 = fam ? t2.za2[jc] : t13.za2[jc];
+    const double *f = fac + (size_t)(fam * kRJ + r) * 3 * SPN;
+    double *sl = lines + (size_t)L * SPN;
+    tsolve_warp<E>(N, f, f + SPN, f + 2 * SPN, A, sup, za2, sl, lane);
+    double *dst = (comp == 0 ? a.qrhs[0] : (comp == 1 ? a.qrhs[1] : a.qrhs[2])) + I3(g, 1, jc, kc);
+    for (int i = lane; i < N; i += 32) dst[i] = sl[tpad(i)];
+  }
+}
+
+
+
+template <int E>
+static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgs &a) {
+  const Geo &g = c->geo;
+  const int SPN = tpad(g.nth) + 1;
+  const size_t sm = sizeof(double) * (size_t)SPN * (3 * kRJ * kRK + 2 * kRJ * 3);
+  cudaError_t e = cudaFuncSetAttribute(k_rhs_tsweep<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
+  LaunchScope ls(c, PK_RHS);
+  k_rhs_tsweep<E><<<dim3((g.nr + kRJ - 1) / kRJ, (g.nz + kRK - 1) / kRK), 256, sm, c->stream>>>(g, rk, a, t13, t2);
+  return cudaGetLastError();
+}
+
+// the fused momentum right-hand side and theta sweep; cudaErrorNotSupported
+// for theta lines longer than 257 (then rhs and theta sweep run apart)
+cudaError_t launch_rhs_tsweep(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  RhsArgs a;
+  a.q = QV{c->q[0], c->q[1], c->q[2]};
+  for (int n = 0; n < 3; n++) {
+    a.dqh[n] = c->dq[n];
+    a.ru[n] = c->ru[n];
+    a.qrhs[n] = c->qrhs[n];
+  }
+  a.prg = c->prg;
+  const int E = (g.nth - 1 + 31) / 32;
+  if (E <= 1) return run_rhs_tsweep<1>(c, rk, a);
+  if (E <= 2) return run_rhs_tsweep<2>(c, rk, a);
+  if (E <= 4) return run_rhs_tsweep<4>(c, rk, a);
+  if (E <= 8) return run_rhs_tsweep<8>(c, rk, a);
+  return cudaErrorNotSupported;
 }
 
 template <int E>
