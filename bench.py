@@ -192,6 +192,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NR", "NTHETA", "NZ"), default=None,
                     help="smaller grid for profiling captures (not the benchmark workload)")
     ap.add_argument("--nparticles", type=int, default=None,
@@ -290,6 +291,47 @@ def main():
                        "(particles included), q1,q2,q3 device->host; pressure, RK history and "
                        "particle state stay resident in the context"}
 
+    # ---- the mixed form on the same workload ---------------------------------
+    mixed = None
+    if not args.no_mixed:
+        rm_ = V.Run(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, precision="mixed",
+                    theta_wavenumber="modified", device=local)
+        for n, a in zip(("q1", "q2", "q3"), q):
+            rm_.set(n, a)
+        pm = V.Part(rm_, PART_CLASS, NPART, PART_MODE)
+        pu, pv = particle_state(NPART)
+        pm.set_state(pu, pv, None, NPART)
+        del pu, pv
+        pm.attach(True)
+        rm_.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            rm_.iterate(1)
+        torch.cuda.synchronize()
+        clocks_m = ClockSampler(local)
+        rm_.profile(True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            rm_.iterate(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_m = max_over_ranks(e0.elapsed_time(e1))
+        prof_m = rm_.profile_read()
+        rm_.profile(False)
+        clk_m = clocks_m.stop()
+        value_m = replicas.throughput(ncell * args.steps, world, ms_m / 1e3) / 1e6
+        mixed = {"value": value_m, "unit": UNIT, "ms_per_step": ms_m / args.steps,
+                 "vs_fp64": value_m / value, "max_div_u": rm_.max_divergence(),
+                 "storage": "float: dq, ru, prg, pres; double: q, sweep work arrays, Poisson "
+                            "right-hand side, transforms, dph",
+                 "tolerance": "max|u_mixed - u_fp64| <= 2e-6 max|u| after 5 steps (tests/test_gpu_mixed.py)",
+                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof_m.items())},
+                 "clocks": clk_m}
+        pm.close()
+        rm_.close()
+
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
     fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
@@ -314,7 +356,7 @@ def main():
             "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ],
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"},
-            "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles,
+            "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles, "mixed": mixed,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak,

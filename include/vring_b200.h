@@ -51,7 +51,11 @@ enum vr_status {
   VR_ERR_IO = 12        /* a restart file could not be written or read       */
 };
 
-/* VR_MIXED is reserved: vr_create returns VR_ERR_DESC for it (not built) */
+/* VR_MIXED: dq, ru, prg and pres are stored as float; q1..q3, the sweep work
+ * arrays, the Poisson right-hand side, transforms and dph stay double,
+ * so the projected velocity keeps max|div u| at round-off.  Runs through
+ * vr_substep/vr_iterate only (the per-routine entry points return
+ * VR_ERR_STATE), for ntheta <= 257 and nr, nz <= 543. */
 enum vr_precision { VR_FP64 = 0, VR_MIXED = 1 };
 enum vr_theta_wavenumber {
   VR_WTH_EXACT = 0,    /* m^2, the reference's 'wvnex' (poisson_solve.F90:287)   */

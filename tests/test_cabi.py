@@ -54,8 +54,10 @@ def test_descriptor_validation_codes():
     assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # ntheta < 3
     bad = Desc(1, 8, 16, 16, -4.0, 12.0, 1e-3, 100.0, 1.0, 0.0, 0, 0, 0, 0, 0)
     assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # rmax <= 0
-    bad = Desc(1, 8, 16, 16, 4.0, 12.0, 1e-3, 100.0, 1.0, 0.0, 1, 0, 0, 0, 0)
-    assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # VR_MIXED: not built
+    bad = Desc(1, 300, 16, 16, 4.0, 12.0, 1e-3, 100.0, 1.0, 0.0, 1, 0, 0, 0, 0)
+    assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # VR_MIXED: ntheta > 257
+    bad = Desc(1, 8, 16, 16, 4.0, 12.0, 1e-3, 100.0, 1.0, 0.0, 2, 0, 0, 0, 0)
+    assert L.vr_create(ctypes.byref(bad), ctypes.byref(h)) == 1      # unknown precision
     assert L.vr_create(None, ctypes.byref(h)) == 8                   # VR_ERR_ARG
 
 

@@ -287,7 +287,10 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
       (!nz_pow2 && d.nz > 512))
     return VR_ERR_DESC;
   if (!(d.rmax > 0) || !(d.zmax > 0) || !(d.dt > 0) || !(d.re > 0) || !(d.pe > 0)) return VR_ERR_DESC;
-  if (d.precision != VR_FP64) return VR_ERR_DESC;  // the mixed-precision form is not built
+  if (d.precision != VR_FP64 && d.precision != VR_MIXED) return VR_ERR_DESC;
+  // the mixed form runs the fused substep only: theta lines up to 257 cells
+  // (fused theta sweep) and r/z lines up to 544 unknowns (register sweep)
+  if (d.precision == VR_MIXED && (d.ntheta > 257 || d.nr > 543 || d.nz > 543)) return VR_ERR_DESC;
   if (d.theta_wavenumber != VR_WTH_EXACT && d.theta_wavenumber != VR_WTH_MODIFIED) return VR_ERR_DESC;
   if (d.inflow != VR_INFLOW_OFF && d.inflow != VR_INFLOW_REFERENCE) return VR_ERR_DESC;
   int64_t cells = (int64_t)d.ntheta * (d.nr + 3) * (d.nz + 3);
@@ -299,6 +302,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
   vr_ctx *c = new (std::nothrow) vr_ctx();
   if (!c) return VR_ERR_OOM;
   c->d = d;
+  c->mixed = d.precision == VR_MIXED;
   c->dev = d.device;
   auto fail = [&](int code) {
     vr_destroy(c);
@@ -490,21 +494,20 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
   size_t nrs = (size_t)g.nth * g.nr * g.nz;
   size_t ndp = (size_t)g.nth * (g.nr + 2) * (g.nz + 2);
   size_t n2 = (size_t)g.nth * (g.nrc + 2);
-  double **f3[] = {&c->q[0], &c->q[1], &c->q[2], &c->dq[0], &c->dq[1], &c->dq[2], &c->ru[0],
-                   &c->ru[1], &c->ru[2], &c->qrhs[0], &c->qrhs[1], &c->qrhs[2], &c->pres};
-  for (auto **p : f3) {
-    if (cudaMalloc(p, sizeof(double) * n3) != cudaSuccess) return fail(VR_ERR_OOM);
-    if (cudaMemsetAsync(*p, 0, sizeof(double) * n3, c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
-  }
+  // element size of the fields the mixed form stores as float
+  const size_t lw = c->mixed ? sizeof(float) : sizeof(double);
   struct {
     double **p;
-    size_t n;
-  } other[] = {{&c->prg, 3 * nrs}, {&c->rhs, nrs},   {&c->spec, nrs},  {&c->dph, ndp},
-               {&c->csort, n2},    {&c->dq3no, n2},  {&c->corr3n, n2}, {&c->corr3s, n2},
-               {&c->tconv, n2},    {&c->d_red, 256}};
-  for (auto &o : other) {
-    if (cudaMalloc(o.p, sizeof(double) * o.n) != cudaSuccess) return fail(VR_ERR_OOM);
-    if (cudaMemsetAsync(*o.p, 0, sizeof(double) * o.n, c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
+    size_t n, w;
+  } fl[] = {{&c->q[0], n3, 8},     {&c->q[1], n3, 8},     {&c->q[2], n3, 8},     {&c->dq[0], n3, lw},
+            {&c->dq[1], n3, lw},   {&c->dq[2], n3, lw},   {&c->ru[0], n3, lw},   {&c->ru[1], n3, lw},
+            {&c->ru[2], n3, lw},   {&c->qrhs[0], n3, 8},  {&c->qrhs[1], n3, 8},  {&c->qrhs[2], n3, 8},
+            {&c->pres, n3, lw},    {&c->prg, 3 * nrs, lw}, {&c->rhs, nrs, 8},    {&c->spec, nrs, 8},
+            {&c->dph, ndp, 8},     {&c->csort, n2, 8},    {&c->dq3no, n2, 8},    {&c->corr3n, n2, 8},
+            {&c->corr3s, n2, 8},   {&c->tconv, n2, 8},    {&c->d_red, 256, 8}};
+  for (auto &o : fl) {
+    if (cudaMalloc(o.p, o.w * o.n) != cudaSuccess) return fail(VR_ERR_OOM);
+    if (cudaMemsetAsync(*o.p, 0, o.w * o.n, c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
   }
   if (cudaMalloc(&c->d_count, sizeof(unsigned long long) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
@@ -647,6 +650,11 @@ static int check_ext(vr_ctx *c, int f, const int64_t *ext, double **p, size_t *n
   return VR_OK;
 }
 
+// fields the mixed form stores as float; host arrays stay double
+static bool float_field(const vr_ctx *c, int f) {
+  return c->mixed && ((f >= VR_F_DQ1 && f <= VR_F_RU3) || f == VR_F_PRES || f == VR_F_PRG);
+}
+
 extern "C" int vr_set_field(vr_ctx *c, int32_t f, const double *host, const int64_t ext[4]) {
   if (!c || !host) return VR_ERR_ARG;
   double *p;
@@ -654,6 +662,12 @@ extern "C" int vr_set_field(vr_ctx *c, int32_t f, const double *host, const int6
   int rc = check_ext(c, f, ext, &p, &n);
   if (rc) return rc;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  if (float_field(c, f)) {
+    std::vector<float> t(host, host + n);
+    VR_CUDA(c, cudaMemcpyAsync(p, t.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    VR_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VR_OK;
+  }
   VR_CUDA(c, cudaMemcpyAsync(p, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   VR_CUDA(c, cudaStreamSynchronize(c->stream));
   return VR_OK;
@@ -666,6 +680,13 @@ extern "C" int vr_get_field(vr_ctx *c, int32_t f, double *host, const int64_t ex
   int rc = check_ext(c, f, ext, &p, &n);
   if (rc) return rc;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  if (float_field(c, f)) {
+    std::vector<float> t(n);
+    VR_CUDA(c, cudaMemcpyAsync(t.data(), p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    VR_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n; i++) host[i] = t[i];
+    return VR_OK;
+  }
   VR_CUDA(c, cudaMemcpyAsync(host, p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   VR_CUDA(c, cudaStreamSynchronize(c->stream));
   return VR_OK;
@@ -748,18 +769,21 @@ extern "C" int vr_hdnbc(vr_ctx *c) {
 
 extern "C" int vr_hdnl1(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_hdnl1: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_hdnl(c, 1));
   return VR_OK;
 }
 extern "C" int vr_hdnl2(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_hdnl2: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_hdnl(c, 2));
   return VR_OK;
 }
 extern "C" int vr_hdnl3(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_hdnl3: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_hdnl(c, 3));
   return VR_OK;
@@ -782,6 +806,7 @@ static cudaError_t sweeps(vr_ctx *c, bool theta_done = false) {
 
 extern "C" int vr_step(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_step: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_rhs(c, rk_of(c), false));
   VR_CUDA(c, sweeps(c));
@@ -790,6 +815,7 @@ extern "C" int vr_step(vr_ctx *c) {
 
 extern "C" int vr_divq(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_divq: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_divq(c, rk_of(c)));
   return VR_OK;
@@ -804,6 +830,7 @@ extern "C" int vr_laplace_solve(vr_ctx *c) {
 
 extern "C" int vr_upsol(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_upsol: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_upsol(c, rk_of(c)));
   return VR_OK;
@@ -811,6 +838,7 @@ extern "C" int vr_upsol(vr_ctx *c) {
 
 extern "C" int vr_uppres(vr_ctx *c) {
   if (!c) return VR_ERR_ARG;
+  if (c->mixed) return set_err(c, VR_ERR_STATE, "vr_uppres: the mixed form runs through vr_substep/vr_iterate only");
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_uppres(c, rk_of(c)));
   return VR_OK;

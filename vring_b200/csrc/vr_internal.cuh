@@ -97,6 +97,10 @@ struct vr_part;
 
 struct vr_ctx {
   vr_desc d;
+  // mixed form: dq, ru, prg and pres are stored as float (the pointers below
+  // then address float arrays); q, the sweep work arrays qrhs, the Poisson
+  // arrays and dph stay double
+  bool mixed;
   int dev;
   int nsm;  // streaming multiprocessors of the device
   cudaStream_t stream;

@@ -19,6 +19,8 @@
 // on the host (vr_ctx.cu) and the kernels only run the two substitutions.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "vr_chunk.cuh"
 #include "vr_internal.cuh"
 
@@ -167,13 +169,22 @@ cudaError_t launch_hdnl(vr_ctx *c, int comp) {
 // INLINE_H the explicit terms H are computed here (fused hdnl1-3 + RHS);
 // otherwise they are read from dq (written by vr_hdnl1..3).  ru <- H.
 // ---------------------------------------------------------------------------
-struct RhsArgs {
+// T: storage type of ru and prg (double, or float in the mixed form); the
+// sweep work arrays qrhs stay double
+template <class T>
+struct RhsArgsT {
   QV q;
   const double *__restrict__ dqh[3];  // H when not inlined
-  double *ru[3];
-  const double *__restrict__ prg;
+  T *ru[3];
+  const T *__restrict__ prg;
   double *qrhs[3];
 };
+using RhsArgs = RhsArgsT<double>;
+
+template <class T>
+__device__ __forceinline__ double ldt(const T *p) {
+  return (double)__ldg(p);
+}
 
 template <bool INLINE_H>
 __global__ void __launch_bounds__(128) k_rhs(Geo g, Rk rk, RhsArgs a) {
@@ -251,7 +262,8 @@ struct RhsCell {
   double h1, h2, h3, r1, r2, r3;
 };
 
-__device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsArgs &a, int ic, int jc, int kc,
+template <class T>
+__device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsArgsT<T> &a, int ic, int jc, int kc,
                                          RhsCell &out) {
   const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
   const int jm = jc > 1 ? jc - 1 : 1;
@@ -272,9 +284,9 @@ __device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsAr
   const double C1 = ld(q3 + o), C2 = ld(q3 + o + di), C3 = ld(q3 + o + dm), C4 = ld(q3 + o + sj);
   const double C5 = ld(q3 + o + ojm), C6 = ld(q3 + o + sk), C7 = ld(q3 + o - sk);
   const double C8 = ld(q3 + o + dm + sk), C9 = ld(q3 + o - sj + sk);
-  const double ru1 = ld(a.ru[0] + o), ru2 = ld(a.ru[1] + o), ru3 = ld(a.ru[2] + o);
-  const double pg1 = ld(a.prg + IPRG(g, ic, jc, kc, 1)), pg2 = ld(a.prg + IPRG(g, ic, jc, kc, 2));
-  const double pg3 = ld(a.prg + IPRG(g, ic, jc, kc, 3));
+  const double ru1 = ldt(a.ru[0] + o), ru2 = ldt(a.ru[1] + o), ru3 = ldt(a.ru[2] + o);
+  const double pg1 = ldt(a.prg + IPRG(g, ic, jc, kc, 1)), pg2 = ldt(a.prg + IPRG(g, ic, jc, kc, 2));
+  const double pg3 = ldt(a.prg + IPRG(g, ic, jc, kc, 3));
   const double are = rk.alm / g.re;
   const bool do3 = kc >= 2, do2 = jc >= 2;
   double h1, h2 = 0.0, h3 = 0.0, r1, r2 = 0.0, r3 = 0.0;
@@ -527,8 +539,8 @@ __global__ void __launch_bounds__(256) k_tsweep(Geo g, TriPer t, double *__restr
 // qrhs is written once instead of written, read and written again.
 constexpr int kRJ = 1, kRK = 8;
 
-template <int E>
-__global__ void __launch_bounds__(256, 2) k_rhs_tsweep(Geo g, Rk rk, RhsArgs a, TriPer t13, TriPer t2) {
+template <int E, class T>
+__global__ void __launch_bounds__(256, 2) k_rhs_tsweep(Geo g, Rk rk, RhsArgsT<T> a, TriPer t13, TriPer t2) {
   extern __shared__ double sm[];
   const int N = g.nth, SPN = tpad(N) + 1;
   double *lines = sm;                        // [comp][r][kk], each SPN
@@ -551,14 +563,14 @@ __global__ void __launch_bounds__(256, 2) k_rhs_tsweep(Geo g, Rk rk, RhsArgs a, 
     RhsCell v;
     rhs_cell(g, rk, a, i + 1, jc, kc, v);
     const int o = I3(g, i + 1, jc, kc);
-    a.ru[0][o] = v.h1;
+    a.ru[0][o] = (T)v.h1;
     lines[(size_t)((0 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r1;
     if (kc >= 2) {
-      a.ru[2][o] = v.h3;
+      a.ru[2][o] = (T)v.h3;
       lines[(size_t)((2 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r3;
     }
     if (jc >= 2) {
-      a.ru[1][o] = v.h2;
+      a.ru[1][o] = (T)v.h2;
       lines[(size_t)((1 * kRJ + r) * kRK + kk) * SPN + tpad(i)] = v.r2;
     }
   }
@@ -581,37 +593,42 @@ __global__ void __launch_bounds__(256, 2) k_rhs_tsweep(Geo g, Rk rk, RhsArgs a, 
 
 
 
-template <int E>
-static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgs &a) {
+template <int E, class T>
+static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) {
   const Geo &g = c->geo;
   const int SPN = tpad(g.nth) + 1;
   const size_t sm = sizeof(double) * (size_t)SPN * (3 * kRJ * kRK + 2 * kRJ * 3);
-  cudaError_t e = cudaFuncSetAttribute(k_rhs_tsweep<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = cudaFuncSetAttribute(k_rhs_tsweep<E, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
   LaunchScope ls(c, PK_RHS);
-  k_rhs_tsweep<E><<<dim3((g.nr + kRJ - 1) / kRJ, (g.nz + kRK - 1) / kRK), 256, sm, c->stream>>>(g, rk, a, t13, t2);
+  k_rhs_tsweep<E, T><<<dim3((g.nr + kRJ - 1) / kRJ, (g.nz + kRK - 1) / kRK), 256, sm, c->stream>>>(g, rk, a, t13, t2);
   return cudaGetLastError();
+}
+
+template <class T>
+static cudaError_t launch_rhs_tsweep_t(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  RhsArgsT<T> a;
+  a.q = QV{c->q[0], c->q[1], c->q[2]};
+  for (int n = 0; n < 3; n++) {
+    a.dqh[n] = c->dq[n];
+    a.ru[n] = reinterpret_cast<T *>(c->ru[n]);
+    a.qrhs[n] = c->qrhs[n];
+  }
+  a.prg = reinterpret_cast<const T *>(c->prg);
+  const int E = (g.nth - 1 + 31) / 32;
+  if (E <= 1) return run_rhs_tsweep<1, T>(c, rk, a);
+  if (E <= 2) return run_rhs_tsweep<2, T>(c, rk, a);
+  if (E <= 4) return run_rhs_tsweep<4, T>(c, rk, a);
+  if (E <= 8) return run_rhs_tsweep<8, T>(c, rk, a);
+  return cudaErrorNotSupported;
 }
 
 // the fused momentum right-hand side and theta sweep; cudaErrorNotSupported
 // for theta lines longer than 257 (then rhs and theta sweep run apart)
 cudaError_t launch_rhs_tsweep(vr_ctx *c, const Rk &rk) {
-  const Geo &g = c->geo;
-  RhsArgs a;
-  a.q = QV{c->q[0], c->q[1], c->q[2]};
-  for (int n = 0; n < 3; n++) {
-    a.dqh[n] = c->dq[n];
-    a.ru[n] = c->ru[n];
-    a.qrhs[n] = c->qrhs[n];
-  }
-  a.prg = c->prg;
-  const int E = (g.nth - 1 + 31) / 32;
-  if (E <= 1) return run_rhs_tsweep<1>(c, rk, a);
-  if (E <= 2) return run_rhs_tsweep<2>(c, rk, a);
-  if (E <= 4) return run_rhs_tsweep<4>(c, rk, a);
-  if (E <= 8) return run_rhs_tsweep<8>(c, rk, a);
-  return cudaErrorNotSupported;
+  return c->mixed ? launch_rhs_tsweep_t<float>(c, rk) : launch_rhs_tsweep_t<double>(c, rk);
 }
 
 template <int E>
@@ -716,9 +733,11 @@ __device__ void tile_solve(double *tile, int LD, int n, const Coef &cf, double *
 // Line sweep parameters.  Element e of line (i, m2) sits at
 //   (i-1) + s2 * m2 + se * (e0 + e)
 // in every ghosted array; the tile covers theta cells i0+1 .. i0+LT.
-struct SweepArgs {
+// T: storage type of the output (double, or float for dq in the mixed form)
+template <class T>
+struct SweepArgsT {
   const double *in;
-  double *out;
+  T *out;
   const double *add;   // out = add + x when non-null, else out = x
   int s2, se, e0, n;   // strides, first element index, unknowns per line
   int m2_0;            // first value of the second line index
@@ -731,6 +750,7 @@ struct SweepArgs {
   double slip;
   int nrc, nr, nth, J3;
 };
+using SweepArgs = SweepArgsT<double>;
 
 template <int LT, int CH>
 __global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgs s, CoefShared cf) {
@@ -792,8 +812,9 @@ static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared
 
 // Line policy of k_chunk for the momentum sweeps (same addressing and boundary
 // rules as k_linesweep).
+template <class T>
 struct MomLine {
-  SweepArgs s;
+  SweepArgsT<T> s;
   const double *a, *c, *ib;
   int n, nbx, i0, m2;
   __device__ void set_tile(int tile) {
@@ -814,20 +835,21 @@ struct MomLine {
   __device__ void store(int l, int e, double x) const {
     int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
     double v = s.add ? s.add[o] + x : x;
-    s.out[o] = v;
-    if (s.mode == 1 && m2 == s.nr) s.out[o + s.nth] = s.slip * v;
+    s.out[o] = (T)v;
+    if (s.mode == 1 && m2 == s.nr) s.out[o + s.nth] = (T)(s.slip * v);
     if (s.mode == 2) {
-      if (e == 0) s.out[o - s.se] = s.add[o - s.se] + 0.0;
-      if (e == n - 1) s.out[o + s.se] = 0.0 * s.slip * v;
+      if (e == 0) s.out[o - s.se] = (T)(s.add[o - s.se] + 0.0);
+      if (e == n - 1) s.out[o + s.se] = (T)(0.0 * s.slip * v);
     }
   }
 };
 
 // register-resident chunked sweep up to 544 unknowns per line, else a
 // shared-memory tile sized to fit the 227 KB of shared memory
-static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared &cf, int nm2) {
+template <class T>
+static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const CoefShared &cf, int nm2) {
   if (chunk_bucket(s.n)) {
-    MomLine p;
+    MomLine<T> p;
     p.s = s;
     p.a = cf.a;
     p.c = cf.c;
@@ -837,9 +859,46 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgs &s, const CoefS
     LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
     return launch_chunk(p, p.nbx * nm2, c->stream);
   }
-  if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
-  if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);
-  return run_linesweep<4, 64>(c, s, cf, nm2);
+  if constexpr (std::is_same<T, double>::value) {
+    if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
+    if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);
+    return run_linesweep<4, 64>(c, s, cf, nm2);
+  } else {
+    return cudaErrorNotSupported;  // the mixed form runs lines of at most 544 unknowns
+  }
+}
+
+// solqj (step.F90:266-358): lines (ic, kc) along j.
+// the same sweep with the output in another storage type
+template <class T>
+static SweepArgsT<T> with_out(const SweepArgs &s, T *out) {
+  SweepArgsT<T> r;
+  r.in = s.in;
+  r.out = out;
+  r.add = s.add;
+  r.s2 = s.s2;
+  r.se = s.se;
+  r.e0 = s.e0;
+  r.n = s.n;
+  r.m2_0 = s.m2_0;
+  r.bc_lo = s.bc_lo;
+  r.bc_hi = s.bc_hi;
+  r.bc_lo_on = s.bc_lo_on;
+  r.bc_hi_on = s.bc_hi_on;
+  r.mode = s.mode;
+  r.slip = s.slip;
+  r.nrc = s.nrc;
+  r.nr = s.nr;
+  r.nth = s.nth;
+  r.J3 = s.J3;
+  return r;
+}
+
+// a component's last sweep writes dq, float in the mixed form
+static cudaError_t dispatch_final(vr_ctx *c, SweepArgs &s, double *dq, const CoefShared &cf, int nm2) {
+  if (c->mixed) return dispatch_linesweep(c, with_out(s, reinterpret_cast<float *>(dq)), cf, nm2);
+  s.out = dq;
+  return dispatch_linesweep(c, s, cf, nm2);
 }
 
 // solqj (step.F90:266-358): lines (ic, kc) along j.
@@ -856,23 +915,21 @@ cudaError_t launch_rsweep(vr_ctx *c, int comp) {
   s.nrc = g.nrc;
   s.J3 = g.J3;
   s.slip = g.slip;
-  int nm2;
+  const CoefShared cf{t.a, t.c, t.ib};
   if (comp == 2) {  // rows 2..nr (Dirichlet rows 1 and nrc), kc = 1..nzc, dq2 = q2 + x
-    s.out = c->dq[1];
     s.add = c->q[1];
     s.e0 = 2;
     s.m2_0 = 1;
-    nm2 = g.nzc;
     s.mode = 2;
-  } else {  // q1: kc = 1..nz ; q3: kc = 2..nz (kc = 1 is replaced by the z sweep's row)
-    s.out = c->qrhs[comp - 1];
-    s.add = nullptr;
-    s.e0 = 1;
-    s.m2_0 = comp == 3 ? 2 : 1;
-    nm2 = g.nz - s.m2_0 + 1;
-    s.mode = 0;
+    return dispatch_final(c, s, c->dq[1], cf, g.nzc);
   }
-  return dispatch_linesweep(c, s, CoefShared{t.a, t.c, t.ib}, nm2);
+  // q1: kc = 1..nz ; q3: kc = 2..nz (kc = 1 is replaced by the z sweep's row)
+  s.out = c->qrhs[comp - 1];
+  s.add = nullptr;
+  s.e0 = 1;
+  s.m2_0 = comp == 3 ? 2 : 1;
+  s.mode = 0;
+  return dispatch_linesweep(c, s, cf, g.nz - s.m2_0 + 1);
 }
 
 // solqk (step.F90:360-485): lines (ic, jc) along k = 1..nzc.
@@ -894,21 +951,19 @@ cudaError_t launch_zsweep(vr_ctx *c, int comp) {
   s.bc_hi_on = 1;  // 0*corr1n, 0*corr2n, corr3n
   s.bc_lo = comp == 3 ? c->corr3s : nullptr;
   s.bc_hi = comp == 3 ? c->corr3n : nullptr;
-  int nm2;
+  const CoefShared cf{t.a, t.c, t.ib};
   if (comp == 2) {  // lines jc = 2..nr; jc = 1 and nrc are replaced by solqj's Dirichlet rows
     s.out = c->qrhs[1];
     s.add = nullptr;
     s.m2_0 = 2;
-    nm2 = g.nr - 1;
     s.mode = 0;
-  } else {  // lines jc = 1..nr; jc = nrc is the slip ghost
-    s.out = c->dq[comp - 1];
-    s.add = c->q[comp - 1];
-    s.m2_0 = 1;
-    nm2 = g.nr;
-    s.mode = 1;
+    return dispatch_linesweep(c, s, cf, g.nr - 1);
   }
-  return dispatch_linesweep(c, s, CoefShared{t.a, t.c, t.ib}, nm2);
+  // lines jc = 1..nr; jc = nrc is the slip ghost
+  s.add = c->q[comp - 1];
+  s.m2_0 = 1;
+  s.mode = 1;
+  return dispatch_final(c, s, c->dq[comp - 1], cf, g.nr);
 }
 
 }  // namespace vr

@@ -17,8 +17,16 @@ __device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
 // ---------------------------------------------------------------------------
 // divq: rhs = -div(dq) / (alpha dt)
 // ---------------------------------------------------------------------------
-__global__ void k_divq(Geo g, double inv_adt, const double *__restrict__ dq1, const double *__restrict__ dq2,
-                       const double *__restrict__ dq3, double *__restrict__ rhs) {
+template <class T>
+__device__ __forceinline__ double ldv(const T *p) {
+  return (double)__ldg(p);
+}
+
+// T: storage type of dq (double, or float in the mixed form); the divergence
+// itself is taken in double from the stored values
+template <class T>
+__global__ void k_divq(Geo g, double inv_adt, const T *__restrict__ dq1, const T *__restrict__ dq2,
+                       const T *__restrict__ dq3, double *__restrict__ rhs) {
   int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   int kc = 1 + blockIdx.z;
@@ -26,9 +34,9 @@ __global__ void k_divq(Geo g, double inv_adt, const double *__restrict__ dq1, co
   int ip = ic < g.nth ? ic + 1 : 1;
   int o = I3(g, ic, jc, kc);
   double irm = g.irm[jc];
-  double d = (ldg(dq1 + I3(g, ip, jc, kc)) - ldg(dq1 + o)) * g.dx1 * g.axsym * irm +
-             (ldg(dq2 + o + g.nth) - ldg(dq2 + o)) * g.dx2 * irm +
-             (ldg(dq3 + o + g.pl) - ldg(dq3 + o)) * g.dx3;
+  double d = (ldv(dq1 + I3(g, ip, jc, kc)) - ldv(dq1 + o)) * g.dx1 * g.axsym * irm +
+             (ldv(dq2 + o + g.nth) - ldv(dq2 + o)) * g.dx2 * irm +
+             (ldv(dq3 + o + g.pl) - ldv(dq3 + o)) * g.dx3;
   rhs[IRS(g, ic, jc, kc)] = -d * inv_adt;
 }
 
@@ -36,7 +44,12 @@ cudaError_t launch_divq(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   LaunchScope ls(c, PK_DIVQ);
-  k_divq<<<gr, b, 0, c->stream>>>(g, 1.0 / (rk.alm * g.dt), c->dq[0], c->dq[1], c->dq[2], c->rhs);
+  if (c->mixed)
+    k_divq<float><<<gr, b, 0, c->stream>>>(g, 1.0 / (rk.alm * g.dt), reinterpret_cast<const float *>(c->dq[0]),
+                                           reinterpret_cast<const float *>(c->dq[1]),
+                                           reinterpret_cast<const float *>(c->dq[2]), c->rhs);
+  else
+    k_divq<double><<<gr, b, 0, c->stream>>>(g, 1.0 / (rk.alm * g.dt), c->dq[0], c->dq[1], c->dq[2], c->rhs);
   return cudaGetLastError();
 }
 
@@ -48,8 +61,9 @@ __device__ __forceinline__ double dphv(const Geo &g, const double *__restrict__ 
 // ---------------------------------------------------------------------------
 // upsol (divergence.F90:69-236): one thread per (ic, jc = 0..nrc, kc = 1..nzc)
 // ---------------------------------------------------------------------------
-__global__ void k_upsol(Geo g, double adt, const double *__restrict__ dq1, const double *__restrict__ dq2,
-                        const double *__restrict__ dq3, const double *__restrict__ dph, double *__restrict__ q1,
+template <class T>
+__global__ void k_upsol(Geo g, double adt, const T *__restrict__ dq1, const T *__restrict__ dq2,
+                        const T *__restrict__ dq3, const double *__restrict__ dph, double *__restrict__ q1,
                         double *__restrict__ q2, double *__restrict__ q3, double *__restrict__ dphw) {
   int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int jc = blockIdx.y * blockDim.y + threadIdx.y;  // 0..nrc
@@ -61,7 +75,7 @@ __global__ void k_upsol(Geo g, double adt, const double *__restrict__ dq1, const
   // q1
   if (jc >= 1) {
     int j = jc <= g.nr ? jc : g.nr;
-    double v = ldg(dq1 + I3(g, ic, j, kc)) -
+    double v = ldv(dq1 + I3(g, ic, j, kc)) -
                (adt * g.dx1 * g.irm[j]) * (dphv(g, dph, ic, j, kc) - dphv(g, dph, im, j, kc));
     q1[o] = jc <= g.nr ? v : g.slip * v;
   }
@@ -70,15 +84,15 @@ __global__ void k_upsol(Geo g, double adt, const double *__restrict__ dq1, const
     if (jc == 1 || jc == g.nrc) {
       q2[o] = 0.0;
     } else {
-      q2[o] = ldg(dq2 + o) - adt * g.rc[jc] * g.dx2 * (dphv(g, dph, ic, jc, kc) - dphv(g, dph, ic, jc - 1, kc));
+      q2[o] = ldv(dq2 + o) - adt * g.rc[jc] * g.dx2 * (dphv(g, dph, ic, jc, kc) - dphv(g, dph, ic, jc - 1, kc));
     }
   }
   // q3
   if (kc == 1) {
-    q3[o] = ldg(dq3 + o);  // jc = 0..nrc: imposed south value
+    q3[o] = ldv(dq3 + o);  // jc = 0..nrc: imposed south value
   } else if (jc >= 1) {
     int j = jc <= g.nr ? jc : g.nr;
-    double v = ldg(dq3 + I3(g, ic, j, kc)) - adt * g.dx3 * (dphv(g, dph, ic, j, kc) - dphv(g, dph, ic, j, kc - 1));
+    double v = ldv(dq3 + I3(g, ic, j, kc)) - adt * g.dx3 * (dphv(g, dph, ic, j, kc) - dphv(g, dph, ic, j, kc - 1));
     q3[o] = jc <= g.nr ? v : g.slip * v;
   }
 }
@@ -87,94 +101,28 @@ cudaError_t launch_upsol(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nrc + 1 + 3) / 4, g.nzc);
   LaunchScope ls(c, PK_UPSOL);
-  k_upsol<<<gr, b, 0, c->stream>>>(g, rk.alm * g.dt, c->dq[0], c->dq[1], c->dq[2], c->dph, c->q[0], c->q[1],
-                                   c->q[2], c->dph);
+  if (c->mixed)
+    k_upsol<float><<<gr, b, 0, c->stream>>>(g, rk.alm * g.dt, reinterpret_cast<const float *>(c->dq[0]),
+                                            reinterpret_cast<const float *>(c->dq[1]),
+                                            reinterpret_cast<const float *>(c->dq[2]), c->dph, c->q[0], c->q[1],
+                                            c->q[2], c->dph);
+  else
+    k_upsol<double><<<gr, b, 0, c->stream>>>(g, rk.alm * g.dt, c->dq[0], c->dq[1], c->dq[2], c->dph, c->q[0],
+                                             c->q[1], c->q[2], c->dph);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // uppres (divergence.F90:239-480)
 // ---------------------------------------------------------------------------
-// gradient components of phi (the reference's qcap for each direction)
-__device__ __forceinline__ double gth(const Geo &g, const double *dph, int i, int j, int k) {
-  int im = i > 1 ? i - 1 : g.nth;
-  return (dphv(g, dph, i, j, k) - dphv(g, dph, im, j, k)) * g.dx1 * g.irm[j];
-}
-__device__ __forceinline__ double grr(const Geo &g, const double *dph, int i, int j, int k) {
-  if (j <= 1 || j >= g.nrc) return 0.0;  // qcap(ic,1,:) = qcap(ic,nrc,:) = 0
-  return (dphv(g, dph, i, j, k) - dphv(g, dph, i, j - 1, k)) * g.dx2 * g.rc[j];
-}
-__device__ __forceinline__ double gzz(const Geo &g, const double *dph, int i, int j, int k) {
-  if (k <= 1) return 0.0;  // qcap(ic,jc,1) = 0
-  return (dphv(g, dph, i, j, k) - dphv(g, dph, i, j, k - 1)) * g.dx3;
-}
-
-__global__ void k_uppres(Geo g, double be, const double *__restrict__ dph, double *__restrict__ prg,
-                         double *__restrict__ pres, double *__restrict__ dphw) {
-  int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  int kc = 1 + blockIdx.z;
-  if (ic > g.nth || jc > g.nr) return;
-  int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
-  int km = kc == 1 ? 1 : (kc == g.nz ? g.nz : kc - 1);  // kmv (mesh_tools.F90:272-280)
-  int kp = kc + 1;
-  int jm = jc > 1 ? jc - 1 : 1, jp = jc < g.nr ? jc + 1 : g.nr;  // jmv, jpv
-  // the north ghost of dph is read through dphv(); it is also stored, as the
-  // reference does (divergence.F90:254-258)
-  if (kc == g.nz) dphw[IDP(g, ic, jc, g.nzc)] = ldg(dph + IDP(g, ic, jc, g.nz));
-  // theta component (divergence.F90:270-311)
-  {
-    double c0 = gth(g, dph, ic, jc, kc);
-    double d11 = (gth(g, dph, ip, jc, kc) - 2.0 * c0 + gth(g, dph, im, jc, kc)) * g.s1t11[jc];
-    double d33 = (gth(g, dph, ic, jc, kp) - 2.0 * c0 + gth(g, dph, ic, jc, km)) * g.dx3q;
-    double qnn = gth(g, dph, ic, jp, kc) * g.irm[jc + 1] - c0 * g.irm[jc];
-    double qss = c0 * g.irm[jc] - gth(g, dph, ic, jm, kc) * g.irm[jm];
-    double d22 = (qnn * g.s1t2n[jc] - qss * g.s1t2s[jc]) * g.s1t2c[jc];
-    int o = IPRG(g, ic, jc, kc, 1);
-    prg[o] = prg[o] + c0 - be * (d11 + d33 + d22);
-  }
-  // r component, jc >= 2 (divergence.F90:315-373)
-  if (jc >= 2) {
-    double c0 = grr(g, dph, ic, jc, kc);
-    double d11 = (grr(g, dph, ip, jc, kc) - 2.0 * c0 + grr(g, dph, im, jc, kc)) * g.s2t11[jc];
-    double d33 = (grr(g, dph, ic, jc, kp) - 2.0 * c0 + grr(g, dph, ic, jc, km)) * g.dx3q;
-    double qnn = grr(g, dph, ic, jc + 1, kc) - c0;
-    double qss = c0 - grr(g, dph, ic, jc - 1, kc);
-    double d22 = qnn * g.s2t2p[jc] - qss * g.s2t2m[jc];
-    int o = IPRG(g, ic, jc, kc, 2);
-    prg[o] = prg[o] + c0 - be * (d11 + d22 + d33);
-  }
-  // z component, kc >= 2 (divergence.F90:378-439)
-  if (kc >= 2) {
-    double c0 = gzz(g, dph, ic, jc, kc);
-    double d11 = (gzz(g, dph, ip, jc, kc) - 2.0 * c0 + gzz(g, dph, im, jc, kc)) * g.s1t11[jc];
-    double d33 = (gzz(g, dph, ic, jc, kc + 1) - 2.0 * c0 + gzz(g, dph, ic, jc, kc - 1)) * g.dx3q;
-    double qnn = gzz(g, dph, ic, jp, kc) - c0;
-    double qss = c0 - gzz(g, dph, ic, jm, kc);
-    double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
-    int o = IPRG(g, ic, jc, kc, 3);
-    prg[o] = prg[o] + c0 - be * (d11 + d22 + d33);
-  }
-  // pressure (divergence.F90:445-476)
-  {
-    double p0 = dphv(g, dph, ic, jc, kc);
-    double d11 = (dphv(g, dph, ip, jc, kc) + dphv(g, dph, im, jc, kc) - 2.0 * p0) * g.s1t11[jc];
-    double qnn = dphv(g, dph, ic, jp, kc) - p0;
-    double qss = p0 - dphv(g, dph, ic, jm, kc);
-    double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
-    double d33 = (dphv(g, dph, ic, jc, kp) + dphv(g, dph, ic, jc, km) - 2.0 * p0) * g.dx3q;
-    int o = I3(g, ic, jc, kc);
-    pres[o] = pres[o] + p0 - be * (d11 + d22 + d33);
-  }
-}
-
 // uppres with every distinct dph value loaded once.  The gradients of phi
 // (the reference's qcap) are formed from those registers exactly as
 // gth/grr/gzz form them, including the kmv/jmv/jpv index maps and the north
 // ghost dph(nzc) = dph(nz); raw neighbours (j-1, j+1, k-1) are loaded once
 // and the mapped ones are selected from them.
+template <class T>
 __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double *__restrict__ dph,
-                                                  double *__restrict__ prg, double *__restrict__ pres,
+                                                  T *__restrict__ prg, T *__restrict__ pres,
                                                   double *__restrict__ dphw) {
   const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -189,7 +137,8 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
   // load after a store to it could not be moved ahead of that store
   const int o1 = IPRG(g, ic, jc, kc, 1), o2 = IPRG(g, ic, jc, kc, 2), o3 = IPRG(g, ic, jc, kc, 3);
   const int op = I3(g, ic, jc, kc);
-  const double pr1 = prg[o1], pr2 = jc >= 2 ? prg[o2] : 0.0, pr3 = kc >= 2 ? prg[o3] : 0.0, ps = pres[op];
+  const double pr1 = prg[o1], pr2 = jc >= 2 ? (double)prg[o2] : 0.0, pr3 = kc >= 2 ? (double)prg[o3] : 0.0;
+  const double ps = pres[op];
   // plane kc
   const double d_c = D(ic, jc, kc), d_ip = D(ip, jc, kc), d_im = D(im, jc, kc), d_imm = D(imm, jc, kc);
   const double d_n = D(ic, jc + 1, kc), d_s = D(ic, jc - 1, kc);
@@ -219,7 +168,7 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
     const double qnn = gjp * g.irm[jc + 1] - c0 * g.irm[jc];
     const double qss = c0 * g.irm[jc] - gjm * g.irm[jm];
     const double d22 = (qnn * g.s1t2n[jc] - qss * g.s1t2s[jc]) * g.s1t2c[jc];
-    prg[o1] = pr1 + c0 - be * (d11 + d33 + d22);
+    prg[o1] = (T)(pr1 + c0 - be * (d11 + d33 + d22));
   }
   // r component, jc >= 2 (divergence.F90:315-373); grr = 0 on rows 1 and nrc
   if (jc >= 2) {
@@ -236,7 +185,7 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
     const double qnn = gn - c0;
     const double qss = c0 - gs;
     const double d22 = qnn * g.s2t2p[jc] - qss * g.s2t2m[jc];
-    prg[o2] = pr2 + c0 - be * (d11 + d22 + d33);
+    prg[o2] = (T)(pr2 + c0 - be * (d11 + d22 + d33));
   }
   // z component, kc >= 2 (divergence.F90:378-439); gzz = 0 on plane 1
   if (kc >= 2) {
@@ -252,7 +201,7 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
     const double qnn = gjp - c0;
     const double qss = c0 - gjm;
     const double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
-    prg[o3] = pr3 + c0 - be * (d11 + d22 + d33);
+    prg[o3] = (T)(pr3 + c0 - be * (d11 + d22 + d33));
   }
   // pressure (divergence.F90:445-476)
   {
@@ -262,7 +211,7 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
     const double qss = p0 - d_jm;
     const double d22 = qnn * g.s3t2n[jc] - qss * g.s3t2s[jc];
     const double d33 = (u_c + m_c - 2.0 * p0) * g.dx3q;
-    pres[op] = ps + p0 - be * (d11 + d22 + d33);
+    pres[op] = (T)(ps + p0 - be * (d11 + d22 + d33));
   }
   if (kc == g.nz) dphw[IDP(g, ic, jc, g.nzc)] = d_c;
 }
@@ -272,7 +221,11 @@ cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   double be = 0.5 * (rk.alm * g.dt) / g.re;
   LaunchScope ls(c, PK_UPPRES);
-  k_uppres_r<<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
+  if (c->mixed)
+    k_uppres_r<float><<<gr, b, 0, c->stream>>>(g, be, c->dph, reinterpret_cast<float *>(c->prg),
+                                               reinterpret_cast<float *>(c->pres), c->dph);
+  else
+    k_uppres_r<double><<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
   return cudaGetLastError();
 }
 
@@ -312,10 +265,11 @@ cudaError_t launch_maxdiv(vr_ctx *c, double *d_out) {
   return cudaGetLastError();
 }
 
-__global__ void k_nonfinite(const double *__restrict__ a, size_t n, unsigned long long *cnt) {
+template <class T>
+__global__ void k_nonfinite(const T *__restrict__ a, size_t n, unsigned long long *cnt) {
   unsigned long long local = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    if (!isfinite(ldg(a + i))) local++;
+    if (!isfinite(ldv(a + i))) local++;
   for (int s = 16; s; s >>= 1) local += __shfl_down_sync(0xffffffffu, local, s);
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(cnt, local);
 }
@@ -325,8 +279,12 @@ cudaError_t launch_count_nonfinite(vr_ctx *c, unsigned long long *d_out) {
   size_t n3 = (size_t)g.nth * g.J3 * g.K3;
   LaunchScope ls(c, PK_DIAG);
   k_zero<<<1, 1, 0, c->stream>>>(nullptr, d_out);
-  const double *f[4] = {c->q[0], c->q[1], c->q[2], c->pres};
-  for (const double *p : f) k_nonfinite<<<4 * 148, 256, 0, c->stream>>>(p, n3, d_out);
+  const double *f[3] = {c->q[0], c->q[1], c->q[2]};
+  for (const double *p : f) k_nonfinite<double><<<4 * 148, 256, 0, c->stream>>>(p, n3, d_out);
+  if (c->mixed)
+    k_nonfinite<float><<<4 * 148, 256, 0, c->stream>>>(reinterpret_cast<const float *>(c->pres), n3, d_out);
+  else
+    k_nonfinite<double><<<4 * 148, 256, 0, c->stream>>>(c->pres, n3, d_out);
   return cudaGetLastError();
 }
 
