@@ -51,3 +51,39 @@ def test_mixed_refuses_per_routine_calls_and_converts_fields():
     a = np.random.default_rng(1).uniform(-1, 1, gpu.extents("ru1")[:3])
     gpu.set("ru1", a)
     np.testing.assert_array_equal(gpu.get("ru1"), a.astype(np.float32).astype(np.float64))
+
+
+def test_mixed_particles_against_fp64_oracle():
+    """Mixed form particles: the fit and transforms in float, positions and
+    the state in double; cell indices from the double positions."""
+    from oracle import oracle as O
+    import vring_b200 as V
+    orc, gpu = _pair(16, 32, 64, seed=3)
+    op = O.OraclePart(orc, 4, 300, 0)
+    gp = V.Part(gpu, 4, 300, 0)
+    rng = np.random.default_rng(12)
+    n = 200
+    r = rng.uniform(0.3, 3.5, n)
+    th = rng.uniform(0, 2 * np.pi, n)
+    z = rng.uniform(0.5, 11.5, n)
+    xyz = np.stack([r * np.cos(th), r * np.sin(th), z], 1)
+    vel, dvel, dd, cells = gp.probe(xyz)
+    for i in range(0, n, 7):
+        ref = op.probe(*xyz[i])
+        idx, _ = op.cell(*xyz[i])
+        assert tuple(cells[i]) == tuple(idx)
+        np.testing.assert_allclose(vel[i], ref[:3], rtol=0, atol=1e-5 * np.abs(ref[:3]).max() + 1e-7)
+        np.testing.assert_allclose(dvel[i].reshape(-1, order="F"), ref[3:12], rtol=0,
+                                   atol=1e-4 * np.abs(ref[3:12]).max() + 1e-6)
+    for i in range(n):
+        op.injc(*xyz[i])
+        gp.injc(*xyz[i])
+    for _ in range(3):
+        op.iter_part(1)
+        gp.iter_part(1)
+    u, v, isf, cnt = gp.state()
+    assert cnt["npart"] == op.npart
+    ou = op.u
+    # positions (double state advanced with float velocities): relative to the domain size
+    assert np.abs(u[:n, :3] - ou[:n, :3]).max() <= 1e-9 * 12.0
+    gp.close()

@@ -18,6 +18,7 @@
 // operations (no FMA contraction) and an acos written from its published
 // construction (the same sequence as the CPU restatement).
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include <algorithm>
 #include <cmath>
@@ -116,13 +117,26 @@ struct PartCoef {
   double ymax_one_pass;  // max |y| below which the second pass is rounding noise under the stop tolerance
 };
 
+// the first-pass rows of PartCoef in float, for the mixed form's fit
+struct PartCoefF {
+  float lin[3], sq[3][8], cr[3];
+};
+
 struct PartGeo {
   Geo g;
   const double *thc, *thm, *rm, *rc, *zm, *zc;  // 1-based device vectors
   double dtheta, dr, dz, zmax, rmax;
   PartCoef C;
+  PartCoefF Cf;
   const PartCoef *Cg;  // device copy of C for the rare full-iteration path
 };
+
+template <class R>
+__device__ __forceinline__ const R *coef_lin(const PartGeo &P);
+template <>
+__device__ __forceinline__ const double *coef_lin<double>(const PartGeo &P) { return P.C.lin; }
+template <>
+__device__ __forceinline__ const float *coef_lin<float>(const PartGeo &P) { return P.Cf.lin; }
 
 __device__ __forceinline__ void part_cell(const PartGeo &P, double x, double y, double z, int &it, int &ir, int &iz,
                                           double &r, double &theta) {
@@ -217,8 +231,10 @@ __device__ __forceinline__ void ls_fit(const PartCoef &C, const double (&y)[27],
 
 constexpr int kPartPerBlock = 32;
 
+// R: arithmetic of the fit and the transforms (double; float in the mixed form)
+template <class R>
 struct PartShared {
-  double cv[39][kPartPerBlock];   // component kd: ff, dff(3), ddff(3,3) at 13 kd + t
+  R cv[39][kPartPerBlock];        // component kd: ff, dff(3), ddff(3,3) at 13 kd + t
   double jac[9][kPartPerBlock];   // old Jacobian, m + 3 j
   double hes[27][kPartPerBlock];  // old Hessian, m + 3 j + 9 k
   double pos[3][kPartPerBlock];   // new position
@@ -265,11 +281,17 @@ __device__ __noinline__ void ls_more(const PartCoef *__restrict__ Cg, int nth, i
 }
 
 // Fit component kd at (x, y, z) and write ff, dff and ddff (the first 13
-// rows of M FI, part_tools.F90:653-683) to cv[13 kd ..][p].
+// rows of M FI, part_tools.F90:653-683) to cv[13 kd ..][p].  The cell, theta
+// and the sample differences are double; with R = float (the mixed form) the
+// fit and the transform run in float and stop after the first pass, which is
+// the exact least-squares solution (the reference's further passes correct
+// rounding, below float resolution).
+template <class R>
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
-                                               double y, double z, double (*cv)[kPartPerBlock], int p,
+                                               double y, double z, R (*cv)[kPartPerBlock], int p,
                                                int (&cell)[3], double &r, double &theta, double &sn,
                                                double &cs) {
+  constexpr bool DBL = std::is_same<R, double>::value;
   int it, ir, iz;
   part_cell(P, x, y, z, it, ir, iz, r, theta);
   // keep the mesh lookups inside the stored vectors for points off the mesh
@@ -303,32 +325,34 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   // First pass of the fit (mp = mint y from a = 0), accumulated while the
   // samples arrive; y_k = sample_k - y0 is not kept.
   const double y0 = stencil_sample(P.g.nth, P.g.J3, q, kd, T, 1, 1, 1);
-  double a[9];
+  R a[9];
 #pragma unroll
-  for (int i = 0; i < 9; i++) a[i] = 0.0;
+  for (int i = 0; i < 9; i++) a[i] = 0;
   double ym = 0.0;
   {
-    const PartCoef &C = P.C;
+    const R *lin = coef_lin<R>(P);
+    const R *cr = DBL ? (const R *)P.C.cr : (const R *)P.Cf.cr;
+    const R(*sq)[8] = DBL ? (const R(*)[8])P.C.sq : (const R(*)[8])P.Cf.sq;
 #pragma unroll
     for (int k = 0; k < 27; k++) {
       if (k == 13) continue;  // y = 0 and every mint entry is 0 at the centre
       const int o1 = k % 3 - 1, o2 = (k / 3) % 3 - 1, o3 = k / 9 - 1;
       const double yk = stencil_sample(P.g.nth, P.g.J3, q, kd, T, o1 + 1, o2 + 1, o3 + 1) - y0;
-      ym = fmax(ym, fabs(yk));
-      const double e = 0.0 - yk;
+      if (DBL) ym = fmax(ym, fabs(yk));
+      const R e = (R)(0.0 - yk);
       const int n1 = o1 != 0, n2 = o2 != 0, n3 = o3 != 0;
-      if (o1) a[0] = a[0] - (o1 * C.lin[0]) * e;
-      if (o2) a[1] = a[1] - (o2 * C.lin[1]) * e;
-      if (o3) a[2] = a[2] - (o3 * C.lin[2]) * e;
-      a[3] = a[3] - C.sq[0][4 * n1 + 2 * n2 + n3] * e;
-      a[5] = a[5] - C.sq[1][4 * n2 + 2 * n3 + n1] * e;
-      a[7] = a[7] - C.sq[2][4 * n3 + 2 * n1 + n2] * e;
-      if (o1 * o2) a[4] = a[4] - ((o1 * o2) * C.cr[0]) * e;
-      if (o2 * o3) a[6] = a[6] - ((o2 * o3) * C.cr[1]) * e;
-      if (o3 * o1) a[8] = a[8] - ((o3 * o1) * C.cr[2]) * e;
+      if (o1) a[0] = a[0] - ((R)o1 * lin[0]) * e;
+      if (o2) a[1] = a[1] - ((R)o2 * lin[1]) * e;
+      if (o3) a[2] = a[2] - ((R)o3 * lin[2]) * e;
+      a[3] = a[3] - sq[0][4 * n1 + 2 * n2 + n3] * e;
+      a[5] = a[5] - sq[1][4 * n2 + 2 * n3 + n1] * e;
+      a[7] = a[7] - sq[2][4 * n3 + 2 * n1 + n2] * e;
+      if (o1 * o2) a[4] = a[4] - ((R)(o1 * o2) * cr[0]) * e;
+      if (o2 * o3) a[6] = a[6] - ((R)(o2 * o3) * cr[1]) * e;
+      if (o3 * o1) a[8] = a[8] - ((R)(o3 * o1) * cr[2]) * e;
     }
   }
-  {
+  if constexpr (DBL) {
     double nn = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; i++) nn += a[i] * a[i];
@@ -361,48 +385,53 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   const double twopi = 6.283185307179586;
   if (dtp > P.dtheta) dtp = dtp - twopi;
   if (dtp < -P.dtheta) dtp = dtp + twopi;
-  const double ff = dtp * a[0] + drp * a[1] + dzp * a[2] + dtp * dtp * a[3] + dtp * drp * a[4] +
-                    drp * drp * a[5] + drp * dzp * a[6] + dzp * dzp * a[7] + dzp * dtp * a[8] + y0;
-  const double ft = a[0] + 2.0 * dtp * a[3] + drp * a[4] + dzp * a[8];
-  const double fr = a[1] + dtp * a[4] + 2.0 * drp * a[5] + dzp * a[6];
-  const double fz = a[2] + drp * a[6] + 2.0 * dzp * a[7] + dtp * a[8];
-  const double ftt = 2.0 * a[3], ftr = drp * a[4], ftz = dzp * a[8], frt = a[4], frr = 2.0 * a[5];
-  const double frz = a[6], fzt = a[8], fzr = a[6], fzz = 2.0 * a[7];
+  const R tp = (R)dtp, rp = (R)drp, zp = (R)dzp, two = 2;
+  const R ff = (R)((double)(tp * a[0] + rp * a[1] + zp * a[2] + tp * tp * a[3] + tp * rp * a[4] + rp * rp * a[5] +
+                            rp * zp * a[6] + zp * zp * a[7] + zp * tp * a[8]) + y0);
+  const R ft = a[0] + two * tp * a[3] + rp * a[4] + zp * a[8];
+  const R fr = a[1] + tp * a[4] + two * rp * a[5] + zp * a[6];
+  const R fz = a[2] + rp * a[6] + two * zp * a[7] + tp * a[8];
+  const R ftt = two * a[3], ftr = rp * a[4], ftz = zp * a[8], frt = a[4], frr = two * a[5];
+  const R frz = a[6], fzt = a[8], fzr = a[6], fzz = two * a[7];
   sincos(theta, &sn, &cs);
-  const double sn2 = 2.0 * sn * cs, cs2 = (cs - sn) * (cs + sn);  // sin 2theta, cos 2theta
-  const double ir1 = 1.0 / r, ir2 = 1.0 / (r * r);
-  const double m_snr = -sn * ir1, m_csr = cs * ir1;
-  const double m30 = sn2 * ir2, m31 = sn * sn * ir1, m33 = sn * sn * ir2, m34 = -cs * sn * ir1, m37 = cs * cs;
-  const double m40 = -cs2 * ir2, m43 = -cs * sn * ir2, m44 = -sn * sn * ir1, m46 = cs * cs * ir1, m47 = cs * sn;
-  const double m70 = -sn2 * ir2, m73 = cs * cs * ir2, m74 = cs * sn * ir1, m77 = sn * sn;
-  double(*o)[kPartPerBlock] = cv + 13 * kd;
+  const R s_ = (R)sn, c_ = (R)cs;
+  const R sn2 = two * s_ * c_, cs2 = (c_ - s_) * (c_ + s_);  // sin 2theta, cos 2theta
+  const R ir1 = (R)(1.0 / r), ir2 = (R)(1.0 / (r * r));
+  const R m_snr = -s_ * ir1, m_csr = c_ * ir1;
+  const R m30 = sn2 * ir2, m31 = s_ * s_ * ir1, m33 = s_ * s_ * ir2, m34 = -c_ * s_ * ir1, m37 = c_ * c_;
+  const R m40 = -cs2 * ir2, m43 = -c_ * s_ * ir2, m44 = -s_ * s_ * ir1, m46 = c_ * c_ * ir1, m47 = c_ * s_;
+  const R m70 = -sn2 * ir2, m73 = c_ * c_ * ir2, m74 = c_ * s_ * ir1, m77 = s_ * s_;
+  const R sn_ = s_, cs_ = c_;
+  R(*o)[kPartPerBlock] = cv + 13 * kd;
   o[0][p] = ff;
-  o[1][p] = m_snr * ft + cs * fr;                                                     // dff 1
-  o[2][p] = m_csr * ft + sn * fr;                                                     // dff 2
+  o[1][p] = m_snr * ft + cs_ * fr;                                                    // dff 1
+  o[2][p] = m_csr * ft + sn_ * fr;                                                    // dff 2
   o[3][p] = fz;                                                                       // dff 3
   o[4][p] = m30 * ft + m31 * fr + m33 * ftt + m34 * ftr + m34 * frt + m37 * frr;      // ddff(1,1)
   o[5][p] = m40 * ft + m34 * fr + m43 * ftt + m44 * ftr + m46 * frt + m47 * frr;      // ddff(2,1)
-  o[6][p] = m_snr * ftz + cs * frz;                                                   // ddff(3,1)
+  o[6][p] = m_snr * ftz + cs_ * frz;                                                  // ddff(3,1)
   o[7][p] = m40 * ft + m34 * fr + m43 * ftt + m46 * ftr + m44 * frt + m47 * frr;      // ddff(1,2)
   o[8][p] = m70 * ft + m46 * fr + m73 * ftt + m74 * ftr + m74 * frt + m77 * frr;      // ddff(2,2)
-  o[9][p] = m_csr * ftz + sn * frz;                                                   // ddff(3,2)
-  o[10][p] = m_snr * fzt + cs * fzr;                                                  // ddff(1,3)
-  o[11][p] = m_csr * fzt + sn * fzr;                                                  // ddff(2,3)
+  o[9][p] = m_csr * ftz + sn_ * frz;                                                  // ddff(3,2)
+  o[10][p] = m_snr * fzt + cs_ * fzr;                                                 // ddff(1,3)
+  o[11][p] = m_csr * fzt + sn_ * fzr;                                                 // ddff(2,3)
   o[12][p] = fzz;                                                                     // ddff(3,3)
 }
 
 // Row id of the Cartesian velocity, gradient and Hessian from the three
 // fitted components (part_tools.F90:730-797), in the reference's summation
 // order over components.
-__device__ __forceinline__ void part_cart_row(double r, double sn, double cs, int id,
-                                              const double (*cv)[kPartPerBlock], int p, double &vel,
-                                              double (&dvel)[3], double (&ddvel)[3][3]) {
-  const double rs = r > (double)0.000001f ? r : (double)0.000001f;
-  const double irs = 1.0 / rs, irs2 = 1.0 / (rs * rs);
-  const double A1 = sn * (-2.0 * (cs * cs) + sn * sn) * irs2, A2 = -3.0 * cs * (sn * sn) * irs2;
-  const double A3 = cs * (cs * cs - 2.0 * (sn * sn)) * irs2, A4 = 3.0 * (cs * cs) * sn * irs2;
+template <class R>
+__device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d, int id,
+                                              const R (*cv)[kPartPerBlock], int p, R &vel, R (&dvel)[3],
+                                              R (&ddvel)[3][3]) {
+  const double rsd = r > (double)0.000001f ? r : (double)0.000001f;
+  const R irs = (R)(1.0 / rsd), irs2 = (R)(1.0 / (rsd * rsd));
+  const R sn = (R)sn_d, cs = (R)cs_d, two = 2, three = 3;
+  const R A1 = sn * (-two * (cs * cs) + sn * sn) * irs2, A2 = -three * cs * (sn * sn) * irs2;
+  const R A3 = cs * (cs * cs - two * (sn * sn)) * irs2, A4 = three * (cs * cs) * sn * irs2;
   // DN(a, b, kd) for b = id, a = 1, 2 and kd = 1, 2 (zero elsewhere)
-  double dnb[2][2];  // [a][kd]
+  R dnb[2][2];  // [a][kd]
   if (id == 0) {
     dnb[0][0] = cs * sn * irs;  // DN(1,1,1)
     dnb[0][1] = sn * sn * irs;  // DN(1,1,2)
@@ -415,7 +444,7 @@ __device__ __forceinline__ void part_cart_row(double r, double sn, double cs, in
     dnb[1][1] = cs * cs * irs;  // DN(2,2,2)
   }
   // DDN(l, j, id, kd) for l, j, kd in {1, 2}
-  double ddnb[2][2][2];  // [l][j][kd]
+  R ddnb[2][2][2];  // [l][j][kd]
   if (id == 0) {
     ddnb[0][0][0] = A1;  ddnb[0][0][1] = A2;
     ddnb[0][1][0] = A3;  ddnb[0][1][1] = -A1;
@@ -428,37 +457,38 @@ __device__ __forceinline__ void part_cart_row(double r, double sn, double cs, in
     ddnb[1][1][0] = -A3; ddnb[1][1][1] = -A4;
   }
   // NM(id, kd)
-  const double nm0 = id == 0 ? -sn : (id == 1 ? cs : 0.0);
-  const double nm1 = id == 0 ? cs : (id == 1 ? sn : 0.0);
-  const double nm2 = id == 2 ? 1.0 : 0.0;
-  vel = 0.0;
+  const R zero = 0, one = 1;
+  const R nm0 = id == 0 ? -sn : (id == 1 ? cs : zero);
+  const R nm1 = id == 0 ? cs : (id == 1 ? sn : zero);
+  const R nm2 = id == 2 ? one : zero;
+  vel = 0;
 #pragma unroll
   for (int j = 0; j < 3; j++) {
-    dvel[j] = 0.0;
+    dvel[j] = 0;
 #pragma unroll
-    for (int l = 0; l < 3; l++) ddvel[j][l] = 0.0;
+    for (int l = 0; l < 3; l++) ddvel[j][l] = 0;
   }
 #pragma unroll
   for (int kd = 0; kd < 3; kd++) {
-    const double(*c)[kPartPerBlock] = cv + 13 * kd;
-    const double nmk = kd == 0 ? nm0 : (kd == 1 ? nm1 : nm2);
-    const double f = c[0][p];
-    const double df[3] = {c[1][p], c[2][p], c[3][p]};
+    const R(*c)[kPartPerBlock] = cv + 13 * kd;
+    const R nmk = kd == 0 ? nm0 : (kd == 1 ? nm1 : nm2);
+    const R f = c[0][p];
+    const R df[3] = {c[1][p], c[2][p], c[3][p]};
     vel = vel + f * nmk;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      const double dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : 0.0;
+      const R dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : zero;
       dvel[j] = dvel[j] + df[j] * nmk + f * dn_j;
     }
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
       for (int l = 0; l < 3; l++) {
-        const double ddf = c[4 + j + 3 * l][p];
-        const double dn_l = (kd < 2 && l < 2 && id < 2) ? dnb[l][kd < 2 ? kd : 0] : 0.0;
-        const double dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : 0.0;
-        const double d4 = (kd < 2 && l < 2 && j < 2 && id < 2) ? ddnb[l < 2 ? l : 0][j < 2 ? j : 0][kd < 2 ? kd : 0]
-                                                                : 0.0;
+        const R ddf = c[4 + j + 3 * l][p];
+        const R dn_l = (kd < 2 && l < 2 && id < 2) ? dnb[l][kd < 2 ? kd : 0] : zero;
+        const R dn_j = (kd < 2 && j < 2 && id < 2) ? dnb[j][kd < 2 ? kd : 0] : zero;
+        const R d4 = (kd < 2 && l < 2 && j < 2 && id < 2) ? ddnb[l < 2 ? l : 0][j < 2 ? j : 0][kd < 2 ? kd : 0]
+                                                           : zero;
         ddvel[j][l] = ddvel[j][l] + ddf * nmk + df[j] * dn_l + df[l] * dn_j + f * d4;
       }
   }
@@ -471,13 +501,14 @@ __device__ __forceinline__ void part_cart_row(double r, double sn, double cs, in
 #ifndef VR_PART_MINB
 #define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
 #endif
+template <class R>
 __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const double *__restrict__ q1,
                                                   const double *__restrict__ q2, const double *__restrict__ q3,
                                                   double *__restrict__ u, double *__restrict__ v,
                                                   int *__restrict__ isfre, int *__restrict__ gone, int naloc,
                                                   int nlast, int mode, double inv_st, double partdt, int serial,
                                                   int *nremoved) {
-  __shared__ PartShared S;
+  __shared__ PartShared<R> S;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ip = 1 + blockIdx.x * kPartPerBlock + p;
   const bool live = ip <= nlast && isfre[ip - 1] == 0;
@@ -485,7 +516,7 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
   if (live) {
     const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
     int cell[3];
-    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs);
+    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs);
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -496,8 +527,16 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
   __syncthreads();
   double pw = 0.0;
   if (live) {
-    double vel, dvel[3], ddvel[3][3];
-    part_cart_row(r, sn, cs, w, S.cv, p, vel, dvel, ddvel);
+    R vr_, dvr[3], ddvr[3][3];
+    part_cart_row<R>(r, sn, cs, w, S.cv, p, vr_, dvr, ddvr);
+    const double vel = vr_;
+    double dvel[3], ddvel[3][3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      dvel[j] = dvr[j];
+#pragma unroll
+      for (int l = 0; l < 3; l++) ddvel[j][l] = ddvr[j][l];
+    }
     pw = u[PUo(ip, 1 + w)];
     if (mode == 1) {  // tracer: dx/dt = u(x)
       pw = pw + vel * partdt;
@@ -565,11 +604,12 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
 }
 
 // interpolation at arbitrary points (the dertest known answers)
+template <class R>
 __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__restrict__ q1,
                                                    const double *__restrict__ q2, const double *__restrict__ q3,
                                                    const double *__restrict__ xyz, int n, double *__restrict__ out,
                                                    int *__restrict__ cells) {
-  __shared__ double cv[39][kPartPerBlock];
+  __shared__ R cv[39][kPartPerBlock];
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * kPartPerBlock + p;
   const bool act = i < n;
@@ -577,14 +617,14 @@ __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__re
   if (act) {
     const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
     int cell[3];
-    part_component(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs);
+    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs);
     if (w == 0)
       for (int a = 0; a < 3; a++) cells[3 * (size_t)i + a] = cell[a];
   }
   __syncthreads();
   if (!act) return;
-  double vel, dvel[3], ddvel[3][3];
-  part_cart_row(r, sn, cs, w, cv, p, vel, dvel, ddvel);
+  R vel, dvel[3], ddvel[3][3];
+  part_cart_row<R>(r, sn, cs, w, cv, p, vel, dvel, ddvel);
   double *o = out + 39 * (size_t)i;
   o[w] = vel;
   for (int b = 0; b < 3; b++) o[3 + w + 3 * b] = dvel[b];
@@ -684,6 +724,11 @@ static int part_geo(vr_ctx *c, PartGeo &P) {
   P.zm = c->part_mesh + 2 * (c->geo.nth + 2);
   P.zc = c->part_mesh + 2 * (c->geo.nth + 2) + (c->geo.nz + 3);
   part_coef(c->geo.dtheta, c->geo.dr, c->geo.dz, P.C);
+  for (int a = 0; a < 3; a++) {
+    P.Cf.lin[a] = (float)P.C.lin[a];
+    P.Cf.cr[a] = (float)P.C.cr[a];
+    for (int k = 0; k < 8; k++) P.Cf.sq[a][k] = (float)P.C.sq[a][k];
+  }
   P.Cg = reinterpret_cast<const PartCoef *>(c->part_mesh + 2 * (size_t)(c->geo.nth + 2) +
                                             2 * (size_t)(c->geo.nz + 3));
   return VR_OK;
@@ -1007,7 +1052,8 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
   for (int s = 0; s < p->nsubdt; s++) {
     if (p->nlast <= 0) break;
     LaunchScope ls(c, PK_PART, stream);
-    k_iter_part<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
+    auto kern = c->mixed ? k_iter_part<float> : k_iter_part<double>;
+    kern<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
                                                               p->isfre, p->gone, p->naloc, p->nlast, p->mode,
                                                               inv_st, partdt, p->serial++, p->d_nremoved);
     cudaError_t e = cudaGetLastError();
@@ -1098,7 +1144,8 @@ extern "C" int vr_part_probe(vr_part *p, const double *xyz, int32_t n, double *o
     rc = VR_ERR_OOM;
   if (!rc && cudaMemcpy(dx, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice)) rc = VR_ERR_CUDA;
   if (!rc) {
-    k_part_probe<<<(n + kPartPerBlock - 1) / kPartPerBlock, 96, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], dx, n, dout, dcell);
+    auto kern = c->mixed ? k_part_probe<float> : k_part_probe<double>;
+    kern<<<(n + kPartPerBlock - 1) / kPartPerBlock, 96, 0, c->stream>>>(P, c->q[0], c->q[1], c->q[2], dx, n, dout, dcell);
     if (cudaGetLastError() || cudaStreamSynchronize(c->stream)) rc = VR_ERR_CUDA;
   }
   if (!rc && cudaMemcpy(out, dout, sizeof(double) * 39 * n, cudaMemcpyDeviceToHost)) rc = VR_ERR_CUDA;
