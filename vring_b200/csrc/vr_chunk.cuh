@@ -1,15 +1,15 @@
 // vr_chunk.cuh -- register-resident chunked tridiagonal sweep.
 //
 // A CTA solves 32 lines that lie next to each other in memory (consecutive
-// theta; lane = line), each split into 32 chunks (warp = chunk), so every
-// load and store of a warp is one contiguous 256-byte row and the whole tile
-// goes in flight at once, straight into registers.  The Thomas substitutions
+// theta; lane = line), each split into NCH = 16 or 32 chunks (warp = chunk),
+// so every load and store of a warp is one contiguous 256-byte row and the
+// whole tile goes in flight at once, straight into registers.  The Thomas substitutions
 //   forward   g_e = (f_e - a_e g_{e-1}) ib_e
 //   backward  x_e = g_e - c_e ib_e x_{e+1}
 // are first-order affine recurrences: each thread composes its chunk into one
-// map y_out = C + M y_in; the 32 chunk maps of a line are then chained by one
-// warp with a shuffle scan (the maps are transposed through shared memory so
-// that warp w holds line w), and each thread re-runs its chunk from the exact
+// map y_out = C + M y_in; the NCH chunk maps of a line are then chained with
+// a shuffle scan (the maps are transposed through shared memory so that a
+// warp holds whole lines), and each thread re-runs its chunk from the exact
 // input.  Coefficients are indexed by the position along the line, so a warp
 // reads one broadcast word per element.
 #pragma once
@@ -19,43 +19,48 @@
 
 namespace vr {
 
-// in-place exclusive scan of the 32 chunk maps of line `line` held in
-// sM/sC[chunk][line]; forward (chunk 0 first) or backward (chunk 31 first).
-// On return sC[chunk][line] is the recurrence value entering the chunk.
-template <bool FORWARD>
-__device__ __forceinline__ void chain_chunks(double (*sM)[33], double (*sC)[33], int line, int lane) {
-  double M = sM[lane][line], C = sC[lane][line];
+// In-place exclusive scan of the NCH chunk maps of each line held in
+// sM/sC[chunk][line]; forward (chunk 0 first) or backward (last chunk
+// first).  Every warp scans 32 / NCH lines, NCH lanes per line.  On return
+// sC[chunk][line] is the recurrence value entering the chunk.
+template <bool FORWARD, int NCH>
+__device__ __forceinline__ void chain_chunks(double (*sM)[33], double (*sC)[33], int warp, int lane) {
+  constexpr int LPW = 32 / NCH;  // lines per warp
+  const int ch = lane % NCH, line = warp * LPW + lane / NCH;
+  if (line >= 32) return;  // warps beyond the 32 lines (none when NCH divides 32)
+  double M = sM[ch][line], C = sC[ch][line];
 #pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
+  for (int d = 1; d < NCH; d <<= 1) {
     double om, oc;
     if (FORWARD) {
-      om = __shfl_up_sync(0xffffffffu, M, d);
-      oc = __shfl_up_sync(0xffffffffu, C, d);
-      if (lane >= d) {  // earlier chunks (other) first, then own
+      om = __shfl_up_sync(0xffffffffu, M, d, NCH);
+      oc = __shfl_up_sync(0xffffffffu, C, d, NCH);
+      if (ch >= d) {  // earlier chunks (other) first, then own
         C = C + M * oc;
         M = M * om;
       }
     } else {
-      om = __shfl_down_sync(0xffffffffu, M, d);
-      oc = __shfl_down_sync(0xffffffffu, C, d);
-      if (lane + d < 32) {  // later chunks feed the earlier ones
+      om = __shfl_down_sync(0xffffffffu, M, d, NCH);
+      oc = __shfl_down_sync(0xffffffffu, C, d, NCH);
+      if (ch + d < NCH) {  // later chunks feed the earlier ones
         C = C + M * oc;
         M = M * om;
       }
     }
   }
-  double in = FORWARD ? __shfl_up_sync(0xffffffffu, C, 1) : __shfl_down_sync(0xffffffffu, C, 1);
-  if (FORWARD ? lane == 0 : lane == 31) in = 0.0;
-  sC[lane][line] = in;
+  double in = FORWARD ? __shfl_up_sync(0xffffffffu, C, 1, NCH) : __shfl_down_sync(0xffffffffu, C, 1, NCH);
+  if (FORWARD ? ch == 0 : ch == NCH - 1) in = 0.0;
+  sC[ch][line] = in;
 }
 
-template <int MAXCL, class P>
-__global__ void __launch_bounds__(1024) k_chunk(P p) {
-  __shared__ double sM[32][33], sC[32][33];
+// NCH warps, warp c holding chunk c of the 32 lines (lane = line)
+template <int MAXCL, int NCH, class P>
+__global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
+  __shared__ double sM[NCH][33], sC[NCH][33];
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   p.set_tile(blockIdx.x);
   const int n = p.n;
-  const int CL = (n + 31) / 32;
+  const int CL = (n + NCH - 1) / NCH;
   const int e0 = c * CL;
   int cnt = n - e0;
   cnt = cnt < 0 ? 0 : (cnt > CL ? CL : cnt);
@@ -77,7 +82,7 @@ __global__ void __launch_bounds__(1024) k_chunk(P p) {
   sM[c][lane] = M;
   sC[c][lane] = C;
   __syncthreads();
-  chain_chunks<true>(sM, sC, c, lane);
+  chain_chunks<true, NCH>(sM, sC, c, lane);
   __syncthreads();
   double y = sC[c][lane];
 #pragma unroll
@@ -102,7 +107,7 @@ __global__ void __launch_bounds__(1024) k_chunk(P p) {
   sM[c][lane] = M;
   sC[c][lane] = C;
   __syncthreads();
-  chain_chunks<false>(sM, sC, c, lane);
+  chain_chunks<false, NCH>(sM, sC, c, lane);
   __syncthreads();
   double x = sC[c][lane];
 #pragma unroll
@@ -127,15 +132,28 @@ inline int chunk_bucket(int n) {
   return 0;  // longer lines use the shared-memory tile path
 }
 
+// Lines up to 272 unknowns run as 16 chunks of up to 17 in 512-thread blocks
+// (two blocks per SM, so one block's loads overlap the other's arithmetic);
+// longer lines as 32 chunks in 1024-thread blocks.
+// (for policies with kShortChunks; the radial Poisson lines, whose pivots
+// differ per line, stay with 32 chunks)
 template <class P>
 cudaError_t launch_chunk(const P &p, int ntiles, cudaStream_t s) {
+  if (P::kShortChunks && p.n <= 16 * 8) {
+    k_chunk<8, 16, P><<<ntiles, 512, 0, s>>>(p);
+    return cudaGetLastError();
+  }
+  if (P::kShortChunks && p.n <= 16 * 17) {
+    k_chunk<17, 16, P><<<ntiles, 512, 0, s>>>(p);
+    return cudaGetLastError();
+  }
   switch (chunk_bucket(p.n)) {
-    case 1: k_chunk<1, P><<<ntiles, 1024, 0, s>>>(p); break;
-    case 2: k_chunk<2, P><<<ntiles, 1024, 0, s>>>(p); break;
-    case 4: k_chunk<4, P><<<ntiles, 1024, 0, s>>>(p); break;
-    case 8: k_chunk<8, P><<<ntiles, 1024, 0, s>>>(p); break;
-    case 12: k_chunk<12, P><<<ntiles, 1024, 0, s>>>(p); break;
-    case 17: k_chunk<17, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 1: k_chunk<1, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 2: k_chunk<2, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 4: k_chunk<4, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 8: k_chunk<8, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 12: k_chunk<12, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
+    case 17: k_chunk<17, 32, P><<<ntiles, 1024, 0, s>>>(p); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

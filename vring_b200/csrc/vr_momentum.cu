@@ -814,6 +814,7 @@ static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared
 // rules as k_linesweep).
 template <class T>
 struct MomLine {
+  static constexpr bool kShortChunks = true;
   SweepArgsT<T> s;
   const double *a, *c, *ib;
   int n, nbx, i0, m2;

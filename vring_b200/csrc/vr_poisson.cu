@@ -550,6 +550,7 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
 // Line policy of k_chunk for the radial solves: lines (slot, kz) along j with
 // the factorisation of mode m = slot/2 (poisson_solve.F90:164-167).
 struct PoisLine {
+  static constexpr bool kShortChunks = false;
   double *a;
   const double *pa, *pc, *pib;
   int n, nth, nm, nbx, i0, kz;
