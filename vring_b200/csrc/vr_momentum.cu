@@ -262,31 +262,23 @@ struct RhsCell {
   double h1, h2, h3, r1, r2, r3;
 };
 
-template <class T>
-__device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsArgsT<T> &a, int ic, int jc, int kc,
+// The 27 stencil samples of one cell, named as in rhs_cell, with the RK
+// history and pressure-gradient values of the cell.
+struct RhsSamples {
+  double A1, A2, A3, A4, A5, A6, A7, A8, A9;  // q1
+  double B1, B2, B3, B4, B5, B6, B7, B8, B9;  // q2
+  double C1, C2, C3, C4, C5, C6, C7, C8, C9;  // q3
+  double ru1, ru2, ru3, pg1, pg2, pg3;
+};
+
+// hdnl1-3 and the RK right-hand sides of one cell from its samples
+__device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int kc, const RhsSamples &S,
                                          RhsCell &out) {
-  const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
   const int jm = jc > 1 ? jc - 1 : 1;
-  const double *__restrict__ q1 = a.q.q1, *__restrict__ q2 = a.q.q2, *__restrict__ q3 = a.q.q3;
-  const int o = I3(g, ic, jc, kc);
-  const int di = ip - ic, dm = im - ic;  // theta neighbour offsets (periodic)
-  const int sj = g.nth, sk = g.pl;       // j and k strides
-  const int ojm = (jm - jc) * sj;        // jm row offset (0 on the axis row)
-  // q1
-  const double A1 = ld(q1 + o), A2 = ld(q1 + o + di), A3 = ld(q1 + o + dm), A4 = ld(q1 + o + sj);
-  const double A5 = ld(q1 + o + ojm), A6 = ld(q1 + o + sk), A7 = ld(q1 + o - sk);
-  const double A8 = ld(q1 + o + di - sj), A9 = ld(q1 + o + di - sk);
-  // q2
-  const double B1 = ld(q2 + o), B2 = ld(q2 + o + di), B3 = ld(q2 + o + dm), B4 = ld(q2 + o + sj);
-  const double B5 = ld(q2 + o - sj), B6 = ld(q2 + o + sk), B7 = ld(q2 + o - sk);
-  const double B8 = ld(q2 + o + dm + sj), B9 = ld(q2 + o + sj - sk);
-  // q3
-  const double C1 = ld(q3 + o), C2 = ld(q3 + o + di), C3 = ld(q3 + o + dm), C4 = ld(q3 + o + sj);
-  const double C5 = ld(q3 + o + ojm), C6 = ld(q3 + o + sk), C7 = ld(q3 + o - sk);
-  const double C8 = ld(q3 + o + dm + sk), C9 = ld(q3 + o - sj + sk);
-  const double ru1 = ldt(a.ru[0] + o), ru2 = ldt(a.ru[1] + o), ru3 = ldt(a.ru[2] + o);
-  const double pg1 = ldt(a.prg + IPRG(g, ic, jc, kc, 1)), pg2 = ldt(a.prg + IPRG(g, ic, jc, kc, 2));
-  const double pg3 = ldt(a.prg + IPRG(g, ic, jc, kc, 3));
+  const double A1 = S.A1, A2 = S.A2, A3 = S.A3, A4 = S.A4, A5 = S.A5, A6 = S.A6, A7 = S.A7, A8 = S.A8, A9 = S.A9;
+  const double B1 = S.B1, B2 = S.B2, B3 = S.B3, B4 = S.B4, B5 = S.B5, B6 = S.B6, B7 = S.B7, B8 = S.B8, B9 = S.B9;
+  const double C1 = S.C1, C2 = S.C2, C3 = S.C3, C4 = S.C4, C5 = S.C5, C6 = S.C6, C7 = S.C7, C8 = S.C8, C9 = S.C9;
+  const double ru1 = S.ru1, ru2 = S.ru2, ru3 = S.ru3, pg1 = S.pg1, pg2 = S.pg2, pg3 = S.pg3;
   const double are = rk.alm / g.re;
   const bool do3 = kc >= 2, do2 = jc >= 2;
   double h1, h2 = 0.0, h3 = 0.0, r1, r2 = 0.0, r3 = 0.0;
@@ -365,6 +357,32 @@ __device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsAr
     r2 = (rk.gam * h2 + rk.rom * ru2 - rk.alm * pg2 + are * (d11 + d33 + d22)) * g.dt;
   }
   out = RhsCell{h1, h2, h3, r1, r2, r3};
+}
+
+template <class T>
+__device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsArgsT<T> &a, int ic, int jc, int kc,
+                                         RhsCell &out) {
+  const int ip = ic < g.nth ? ic + 1 : 1, im = ic > 1 ? ic - 1 : g.nth;
+  const int jm = jc > 1 ? jc - 1 : 1;
+  const double *__restrict__ q1 = a.q.q1, *__restrict__ q2 = a.q.q2, *__restrict__ q3 = a.q.q3;
+  const int o = I3(g, ic, jc, kc);
+  const int di = ip - ic, dm = im - ic;  // theta neighbour offsets (periodic)
+  const int sj = g.nth, sk = g.pl;       // j and k strides
+  const int ojm = (jm - jc) * sj;        // jm row offset (0 on the axis row)
+  RhsSamples S;
+  S.A1 = ld(q1 + o), S.A2 = ld(q1 + o + di), S.A3 = ld(q1 + o + dm), S.A4 = ld(q1 + o + sj);
+  S.A5 = ld(q1 + o + ojm), S.A6 = ld(q1 + o + sk), S.A7 = ld(q1 + o - sk);
+  S.A8 = ld(q1 + o + di - sj), S.A9 = ld(q1 + o + di - sk);
+  S.B1 = ld(q2 + o), S.B2 = ld(q2 + o + di), S.B3 = ld(q2 + o + dm), S.B4 = ld(q2 + o + sj);
+  S.B5 = ld(q2 + o - sj), S.B6 = ld(q2 + o + sk), S.B7 = ld(q2 + o - sk);
+  S.B8 = ld(q2 + o + dm + sj), S.B9 = ld(q2 + o + sj - sk);
+  S.C1 = ld(q3 + o), S.C2 = ld(q3 + o + di), S.C3 = ld(q3 + o + dm), S.C4 = ld(q3 + o + sj);
+  S.C5 = ld(q3 + o + ojm), S.C6 = ld(q3 + o + sk), S.C7 = ld(q3 + o - sk);
+  S.C8 = ld(q3 + o + dm + sk), S.C9 = ld(q3 + o - sj + sk);
+  S.ru1 = ldt(a.ru[0] + o), S.ru2 = ldt(a.ru[1] + o), S.ru3 = ldt(a.ru[2] + o);
+  S.pg1 = ldt(a.prg + IPRG(g, ic, jc, kc, 1)), S.pg2 = ldt(a.prg + IPRG(g, ic, jc, kc, 2));
+  S.pg3 = ldt(a.prg + IPRG(g, ic, jc, kc, 3));
+  rhs_eval(g, rk, jc, kc, S, out);
 }
 
 __global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
