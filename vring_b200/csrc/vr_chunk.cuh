@@ -54,12 +54,38 @@ __device__ __forceinline__ void chain_chunks(double (*sM)[33], double (*sC)[33],
 }
 
 // NCH warps, warp c holding chunk c of the 32 lines (lane = line)
+// Policies whose coefficients depend only on the position along the line
+// (kStageCoef) have them staged in shared memory once per block, so the
+// substitution passes read broadcast shared words instead of global ones.
+constexpr int kMaxStaged = 544;
+
 template <int MAXCL, int NCH, class P>
 __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
   __shared__ double sM[NCH][33], sC[NCH][33];
+  __shared__ double sA[P::kStageCoef ? kMaxStaged : 1], sCc[P::kStageCoef ? kMaxStaged : 1],
+      sIB[P::kStageCoef ? kMaxStaged : 1];
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   p.set_tile(blockIdx.x);
   const int n = p.n;
+  if constexpr (P::kStageCoef) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      cp_async8(sA + e, p.a + e);
+      cp_async8(sCc + e, p.c + e);
+      cp_async8(sIB + e, p.ib + e);
+    }
+  }
+  auto A = [&](int l, int e) -> double {
+    if constexpr (P::kStageCoef) return sA[e];
+    else return p.A(l, e);
+  };
+  auto Cc = [&](int l, int e) -> double {
+    if constexpr (P::kStageCoef) return sCc[e];
+    else return p.Cc(l, e);
+  };
+  auto IB = [&](int l, int e) -> double {
+    if constexpr (P::kStageCoef) return sIB[e];
+    else return p.IB(l, e);
+  };
   const int CL = (n + NCH - 1) / NCH;
   const int e0 = c * CL;
   int cnt = n - e0;
@@ -69,12 +95,16 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 #pragma unroll
   for (int t = 0; t < MAXCL; t++)
     if (t < cnt) v[t] = act ? p.fix(lane, e0 + t, *p.gptr(lane, e0 + t)) : 0.0;
+  if constexpr (P::kStageCoef) {
+    cp_async_wait_all();
+    __syncthreads();
+  }
   // forward: chunk map with zero input
   double M = 1.0, C = 0.0;
 #pragma unroll
   for (int t = 0; t < MAXCL; t++) {
     if (t < cnt) {
-      double ib = p.IB(lane, e0 + t), a = p.A(lane, e0 + t);
+      double ib = IB(lane, e0 + t), a = A(lane, e0 + t);
       C = (v[t] - a * C) * ib;
       M = -a * ib * M;
     }
@@ -88,7 +118,7 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 #pragma unroll
   for (int t = 0; t < MAXCL; t++) {
     if (t < cnt) {
-      y = (v[t] - p.A(lane, e0 + t) * y) * p.IB(lane, e0 + t);
+      y = (v[t] - A(lane, e0 + t) * y) * IB(lane, e0 + t);
       v[t] = y;
     }
   }
@@ -98,7 +128,7 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 #pragma unroll
   for (int t = MAXCL - 1; t >= 0; t--) {
     if (t < cnt) {
-      double u = p.Cc(lane, e0 + t) * p.IB(lane, e0 + t);
+      double u = Cc(lane, e0 + t) * IB(lane, e0 + t);
       C = v[t] - u * C;
       M = -u * M;
     }
@@ -113,7 +143,7 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 #pragma unroll
   for (int t = MAXCL - 1; t >= 0; t--) {
     if (t < cnt) {
-      x = v[t] - p.Cc(lane, e0 + t) * p.IB(lane, e0 + t) * x;
+      x = v[t] - Cc(lane, e0 + t) * IB(lane, e0 + t) * x;
       v[t] = x;
     }
   }

@@ -833,6 +833,7 @@ static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared
 template <class T>
 struct MomLine {
   static constexpr bool kShortChunks = true;
+  static constexpr bool kStageCoef = true;  // one factorisation per line family
   SweepArgsT<T> s;
   const double *a, *c, *ib;
   int n, nbx, i0, m2;

@@ -551,6 +551,7 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
 // the factorisation of mode m = slot/2 (poisson_solve.F90:164-167).
 struct PoisLine {
   static constexpr bool kShortChunks = false;
+  static constexpr bool kStageCoef = false;  // the pivots depend on the line's (mode, kz)
   double *a;
   const double *pa, *pc, *pib;
   int n, nth, nm, nbx, i0, kz;
