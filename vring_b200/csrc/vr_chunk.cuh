@@ -62,24 +62,24 @@ constexpr int kMaxStaged = 544;
 template <int MAXCL, int NCH, class P>
 __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
   __shared__ double sM[NCH][33], sC[NCH][33];
-  __shared__ double sA[P::kStageCoef ? kMaxStaged : 1], sCc[P::kStageCoef ? kMaxStaged : 1],
-      sIB[P::kStageCoef ? kMaxStaged : 1];
+  constexpr bool kAC = P::kStageCoef || P::kStageAC;  // sub/super diagonals per position
+  __shared__ double sA[kAC ? kMaxStaged : 1], sCc[kAC ? kMaxStaged : 1], sIB[P::kStageCoef ? kMaxStaged : 1];
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   p.set_tile(blockIdx.x);
   const int n = p.n;
-  if constexpr (P::kStageCoef) {
+  if constexpr (kAC) {
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      cp_async8(sA + e, p.a + e);
-      cp_async8(sCc + e, p.c + e);
-      cp_async8(sIB + e, p.ib + e);
+      cp_async8(sA + e, p.a_ptr() + e);
+      cp_async8(sCc + e, p.c_ptr() + e);
+      if constexpr (P::kStageCoef) cp_async8(sIB + e, p.ib + e);
     }
   }
   auto A = [&](int l, int e) -> double {
-    if constexpr (P::kStageCoef) return sA[e];
+    if constexpr (kAC) return sA[e];
     else return p.A(l, e);
   };
   auto Cc = [&](int l, int e) -> double {
-    if constexpr (P::kStageCoef) return sCc[e];
+    if constexpr (kAC) return sCc[e];
     else return p.Cc(l, e);
   };
   auto IB = [&](int l, int e) -> double {
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 #pragma unroll
   for (int t = 0; t < MAXCL; t++)
     if (t < cnt) v[t] = act ? p.fix(lane, e0 + t, *p.gptr(lane, e0 + t)) : 0.0;
-  if constexpr (P::kStageCoef) {
+  if constexpr (kAC) {
     cp_async_wait_all();
     __syncthreads();
   }

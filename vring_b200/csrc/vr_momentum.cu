@@ -834,6 +834,9 @@ template <class T>
 struct MomLine {
   static constexpr bool kShortChunks = true;
   static constexpr bool kStageCoef = true;  // one factorisation per line family
+  static constexpr bool kStageAC = true;
+  __device__ const double *a_ptr() const { return a; }
+  __device__ const double *c_ptr() const { return c; }
   SweepArgsT<T> s;
   const double *a, *c, *ib;
   int n, nbx, i0, m2;

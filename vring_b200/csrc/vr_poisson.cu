@@ -552,6 +552,9 @@ __global__ void __launch_bounds__(LT *CH) k_radial(double *__restrict__ a, Geo g
 struct PoisLine {
   static constexpr bool kShortChunks = false;
   static constexpr bool kStageCoef = false;  // the pivots depend on the line's (mode, kz)
+  static constexpr bool kStageAC = true;     // aa, cc do not
+  __device__ const double *a_ptr() const { return pa; }
+  __device__ const double *c_ptr() const { return pc; }
   double *a;
   const double *pa, *pc, *pib;
   int n, nth, nm, nbx, i0, kz;
