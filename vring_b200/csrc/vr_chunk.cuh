@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "vr_internal.cuh"
+#include "vr_tma.cuh"
 
 namespace vr {
 
@@ -23,11 +24,11 @@ namespace vr {
 // sM/sC[chunk][line]; forward (chunk 0 first) or backward (last chunk
 // first).  Every warp scans 32 / NCH lines, NCH lanes per line.  On return
 // sC[chunk][line] is the recurrence value entering the chunk.
-template <bool FORWARD, int NCH>
-__device__ __forceinline__ void chain_chunks(double (*sM)[33], double (*sC)[33], int warp, int lane) {
+template <bool FORWARD, int NCH, int LPT = 32>
+__device__ __forceinline__ void chain_chunks(double (*sM)[LPT + 1], double (*sC)[LPT + 1], int warp, int lane) {
   constexpr int LPW = 32 / NCH;  // lines per warp
   const int ch = lane % NCH, line = warp * LPW + lane / NCH;
-  if (line >= 32) return;  // warps beyond the 32 lines (none when NCH divides 32)
+  if (line >= LPT) return;  // warps beyond the tile's lines
   double M = sM[ch][line], C = sC[ch][line];
 #pragma unroll
   for (int d = 1; d < NCH; d <<= 1) {
@@ -152,6 +153,265 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
     for (int t = 0; t < MAXCL; t++)
       if (t < cnt) p.store(lane, e0 + t, v[t]);
   }
+}
+
+// ---------------------------------------------------------------------------
+// TMA-pipelined form.  Persistent CTAs (one per SM) walk the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...; a ring of S shared-memory stages
+// is filled by TMA up to S tiles ahead, so the loads of the next tiles are in
+// flight while the current tile is substituted and stored.  A tile is LPT
+// consecutive theta lines x n positions, loaded as nbox boxes of br
+// positions along the line dimension ldim (1: second array index, 2: third).
+// Thread (warp w, lane) holds line lane % LPT and chunk
+// w * (32 / LPT) + lane / LPT of MAXCL positions, so a warp reads 32 / LPT
+// rows of LPT * 8 contiguous bytes from the stage.
+//
+// Every chunk is full: positions n .. NCH*MAXCL-1 are padding with a = c = 0,
+// pivot 1 and right-hand side 0, which the substitutions carry as exact
+// zeros, so the arithmetic runs without per-position predicates.  The
+// coefficient products of the recurrences, (-a ib) and (c ib), are formed
+// once per CTA; the maps and substitutions use them exactly as the plain
+// kernel forms them.  Per-line pivots (P::kLineIB) and the added field of the
+// final sweeps are read into registers as a tile starts and arrive while the
+// substitutions run.
+// ---------------------------------------------------------------------------
+struct TmaTile {
+  int nbox, br, ldim;
+};
+
+template <int LPT, int NCH, int MAXCL, int S, class P>
+__global__ void __launch_bounds__(LPT *NCH, 1)
+    k_chunk_tma(const __grid_constant__ CUtensorMap tm, P p, int ntiles, TmaTile tt, unsigned *status) {
+  constexpr int NP = NCH * MAXCL;  // padded line length
+  constexpr int NT = LPT * NCH;
+  constexpr bool kLine = P::kLineIB;
+  using OutT = typename P::OutT;
+  extern __shared__ __align__(128) double stage[];
+  __shared__ double sM[NCH][LPT + 1], sC[NCH][LPT + 1];
+  __shared__ double2 sAB[kLine ? 1 : NP];  // (a, ib) per position
+  __shared__ double sMf[kLine ? 1 : NP];   // -a ib
+  __shared__ double sU[kLine ? 1 : NP];    // c ib
+  __shared__ double sA[kLine ? NP : 1], sCc[kLine ? NP : 1];
+  __shared__ __align__(8) uint64_t full[S];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int line = lane % LPT, c = w * (32 / LPT) + lane / LPT;
+  const int n = p.n;
+  const int e0 = c * MAXCL;
+  const bool full_chunk = e0 + MAXCL <= n;
+  const bool has_last = e0 <= n - 1 && n - 1 < e0 + MAXCL;
+  const int slen = tt.nbox * tt.br * LPT;  // doubles per stage
+  auto issue = [&](int s, int tile) {
+    P q = p;
+    q.set_tile(tile);
+    int x, y, z;
+    q.tma_xyz(x, y, z);
+    mbar_expect_tx(&full[s], (unsigned)slen * 8u);
+    for (int b = 0; b < tt.nbox; b++) {
+      const int o = b * tt.br;
+      tma_load_3d(stage + (size_t)s * slen + (size_t)o * LPT, &tm, x, y + (tt.ldim == 1 ? o : 0),
+                  z + (tt.ldim == 2 ? o : 0), &full[s]);
+    }
+  };
+  if (tid == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    mbar_init_fence();
+  }
+  for (int e = tid; e < NP; e += NT) {
+    const bool in = e < n;
+    const double a = in ? p.a_ptr()[e] : 0.0, cc = in ? p.c_ptr()[e] : 0.0;
+    if constexpr (kLine) {
+      sA[e] = a;
+      sCc[e] = cc;
+    } else {
+      const double ib = in ? p.ib[e] : 1.0;
+      sAB[e] = make_double2(a, ib);
+      sMf[e] = -a * ib;
+      sU[e] = cc * ib;
+    }
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int k = 0; k < S; k++) {
+      const int tile = blockIdx.x + k * gridDim.x;
+      if (tile < ntiles) issue(k, tile);
+    }
+
+  bool failed = false;
+  int k = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+    const int s = k % S;
+    p.set_tile(tile);
+    const bool ok = mbar_wait(&full[s], (unsigned)(k / S) & 1u);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    const double *buf = stage + (size_t)s * slen + line;
+    const bool act = p.line_active(line);
+    double v[MAXCL];
+    if (full_chunk) {
+#pragma unroll
+      for (int t = 0; t < MAXCL; t++) v[t] = buf[(e0 + t) * LPT];
+    } else {
+#pragma unroll
+      for (int t = 0; t < MAXCL; t++) v[t] = e0 + t < n ? buf[(e0 + t) * LPT] : 0.0;
+    }
+    // boundary right-hand sides of rows 0 and n-1
+    if (act && c == 0 && p.bc_lo_on()) v[0] = p.bc_lo_val(line);
+    if (act && has_last && p.bc_hi_on()) {
+#pragma unroll
+      for (int t = 0; t < MAXCL; t++)
+        if (e0 + t == n - 1) v[t] = p.bc_hi_val(line);
+    }
+    const bool hadd = p.has_add();
+    const int st = p.stride();
+    double ad[MAXCL];
+    if (act && hadd) {
+      const double *ap = p.add_ptr(line, e0);
+#pragma unroll
+      for (int t = 0; t < MAXCL; t++) ad[t] = (full_chunk || e0 + t < n) ? ap[t * st] : 0.0;
+    }
+    double ibv[kLine ? MAXCL : 1];
+    if constexpr (kLine) {
+      const double *ip = p.ib_ptr(line, e0);
+      const int is = p.ib_stride();
+#pragma unroll
+      for (int t = 0; t < MAXCL; t++) ibv[t] = (act && (full_chunk || e0 + t < n)) ? __ldg(ip + t * is) : 1.0;
+    }
+    __syncthreads();  // stage s has been read by every thread
+    if (tid == 0) {
+      const int nt = tile + S * gridDim.x;
+      if (nt < ntiles) {
+        fence_proxy_async();
+        issue(s, nt);
+      }
+    }
+    // forward: chunk map with zero input
+    double M = 1.0, C = 0.0;
+#pragma unroll
+    for (int t = 0; t < MAXCL; t++) {
+      const int e = e0 + t;
+      if constexpr (kLine) {
+        const double a = sA[e], ib = ibv[t];
+        C = (v[t] - a * C) * ib;
+        M = -a * ib * M;
+      } else {
+        const double2 ab = sAB[e];
+        C = (v[t] - ab.x * C) * ab.y;
+        M = sMf[e] * M;
+      }
+    }
+    sM[c][line] = M;
+    sC[c][line] = C;
+    __syncthreads();
+    chain_chunks<true, NCH, LPT>(sM, sC, w, lane);
+    __syncthreads();
+    double y = sC[c][line];
+#pragma unroll
+    for (int t = 0; t < MAXCL; t++) {
+      const int e = e0 + t;
+      if constexpr (kLine) {
+        y = (v[t] - sA[e] * y) * ibv[t];
+      } else {
+        const double2 ab = sAB[e];
+        y = (v[t] - ab.x * y) * ab.y;
+      }
+      v[t] = y;
+    }
+    // backward
+    M = 1.0;
+    C = 0.0;
+#pragma unroll
+    for (int t = MAXCL - 1; t >= 0; t--) {
+      const int e = e0 + t;
+      const double u = kLine ? sCc[e] * ibv[t] : sU[e];
+      C = v[t] - u * C;
+      M = -u * M;
+    }
+    __syncthreads();  // every thread has read its forward input
+    sM[c][line] = M;
+    sC[c][line] = C;
+    __syncthreads();
+    chain_chunks<false, NCH, LPT>(sM, sC, w, lane);
+    __syncthreads();
+    double x = sC[c][line];
+#pragma unroll
+    for (int t = MAXCL - 1; t >= 0; t--) {
+      const int e = e0 + t;
+      const double u = kLine ? sCc[e] * ibv[t] : sU[e];
+      x = v[t] - u * x;
+      v[t] = x;
+    }
+    if (act) {
+      if (hadd) {
+#pragma unroll
+        for (int t = 0; t < MAXCL; t++) v[t] = ad[t] + v[t];
+      }
+      OutT *op = p.out_ptr(line, e0);
+      if (full_chunk) {
+#pragma unroll
+        for (int t = 0; t < MAXCL; t++) op[t * st] = (OutT)v[t];
+      } else {
+#pragma unroll
+        for (int t = 0; t < MAXCL; t++)
+          if (e0 + t < n) op[t * st] = (OutT)v[t];
+      }
+      if (p.ghost_copy()) {  // slip ghost one row past the line's row
+        const int go = p.ghost_off();
+        const double sl = p.slip();
+#pragma unroll
+        for (int t = 0; t < MAXCL; t++)
+          if (full_chunk || e0 + t < n) op[t * st + go] = (OutT)(sl * v[t]);
+      }
+      if (p.edges()) {  // rows just before the first and after the last position
+        if (c == 0) p.edge_lo(line);
+        if (has_last) {
+#pragma unroll
+          for (int t = 0; t < MAXCL; t++)
+            if (e0 + t == n - 1) p.edge_hi(line, v[t]);
+        }
+      }
+    }
+  }
+  if (failed) {
+    // record the timeout, then let the loads already issued land before the
+    // CTA's shared memory goes away (each wait again bounded)
+    if (tid == 0) {
+      atomicOr(status, 1u);
+      for (int j = k; j < k + S; j++) {
+        const int tile = blockIdx.x + j * gridDim.x;
+        if (tile < ntiles) (void)mbar_wait(&full[j % S], (unsigned)(j / S) & 1u);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Launches the pipelined form when the tile fits: ldim is the array index the
+// lines run along; (d0, d1, d2) the array's extents.  cudaErrorNotSupported
+// when it does not apply (odd theta extent, long lines, encoding refused), so
+// the caller can fall back to k_chunk.
+template <int LPT, int NCH, int MAXCL, int S, class P>
+cudaError_t run_chunk_tma(P p, const void *base, int d0, int d1, int d2, int ldim, int nm2, int nsm,
+                          unsigned *status, cudaStream_t st) {
+  if (p.n < 1 || p.n > NCH * MAXCL || (d0 & 1)) return cudaErrorNotSupported;
+  TmaTile tt;
+  tt.ldim = ldim;
+  tt.nbox = (p.n + 255) / 256;
+  tt.br = (p.n + tt.nbox - 1) / tt.nbox;
+  const size_t dyn = sizeof(double) * (size_t)S * tt.nbox * tt.br * LPT;
+  CUtensorMap tm;
+  if (!encode_tmap_f64_3d(&tm, base, d0, d1, d2, LPT, ldim == 1 ? tt.br : 1, ldim == 2 ? tt.br : 1))
+    return cudaErrorNotSupported;
+  auto kern = k_chunk_tma<LPT, NCH, MAXCL, S, P>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e) return e;
+  p.lpt = LPT;
+  p.nbx = (p.nth_lines() + LPT - 1) / LPT;
+  const int ntiles = p.nbx * nm2;
+  const int grid = ntiles < nsm ? ntiles : nsm;
+  kern<<<grid, LPT * NCH, dyn, st>>>(tm, p, ntiles, tt, status);
+  return cudaGetLastError();
 }
 
 // chunk length bucket: the smallest compiled MAXCL with 32 * MAXCL >= n

@@ -510,6 +510,9 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
     if (cudaMemsetAsync(*o.p, 0, o.w * o.n, c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
   }
   if (cudaMalloc(&c->d_count, sizeof(unsigned long long) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMemsetAsync(c->d_count, 0, sizeof(unsigned long long) * 4, c->stream) != cudaSuccess)
+    return fail(VR_ERR_CUDA);
+  c->d_status = reinterpret_cast<unsigned *>(c->d_count + 3);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
   *out = c;
   return VR_OK;
@@ -920,9 +923,14 @@ extern "C" int vr_check_finite(vr_ctx *c, int64_t *count) {
   if (!c) return VR_ERR_ARG;
   VR_CUDA(c, cudaSetDevice(c->dev));
   VR_CUDA(c, launch_count_nonfinite(c, c->d_count));
-  unsigned long long n = 0;
-  VR_CUDA(c, cudaMemcpyAsync(&n, c->d_count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
+  unsigned long long h[4] = {0, 0, 0, 0};
+  VR_CUDA(c, cudaMemcpyAsync(h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  const unsigned long long n = h[0];
   if (count) *count = (int64_t)n;
+  unsigned status;
+  std::memcpy(&status, &h[3], sizeof(status));
+  if (status & 1u)
+    return set_err(c, VR_ERR_TIMEOUT, "a sweep kernel gave up waiting for its tile loads; results are not valid");
   return n ? set_err(c, VR_ERR_NONFINITE, "non-finite values in q1..q3/pres") : VR_OK;
 }

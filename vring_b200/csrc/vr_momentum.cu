@@ -835,17 +835,53 @@ struct MomLine {
   static constexpr bool kShortChunks = true;
   static constexpr bool kStageCoef = true;  // one factorisation per line family
   static constexpr bool kStageAC = true;
+  static constexpr bool kLineIB = false;
   __device__ const double *a_ptr() const { return a; }
   __device__ const double *c_ptr() const { return c; }
   SweepArgsT<T> s;
   const double *a, *c, *ib;
   int n, nbx, i0, m2;
+  int lpt = 32;  // lines per tile
+  __host__ __device__ int nth_lines() const { return s.nth; }
   __device__ void set_tile(int tile) {
-    i0 = (tile % nbx) * 32;
+    i0 = (tile % nbx) * lpt;
     m2 = s.m2_0 + tile / nbx;
   }
   __device__ bool line_active(int l) const { return i0 + l < s.nth; }
   __device__ const double *gptr(int l, int e) const { return s.in + ((i0 + l) + s.s2 * m2 + s.se * (s.e0 + e)); }
+  // origin of the tile in the ghosted (nth, nr+3, nz+3) array of `in`
+  __device__ void tma_xyz(int &x, int &y, int &z) const {
+    x = i0;
+    if (s.se == s.nth) {  // lines along r at plane m2
+      y = s.e0;
+      z = m2;
+    } else {  // lines along z at row m2
+      y = m2;
+      z = s.e0;
+    }
+  }
+  // element access of the pipelined form (k_chunk_tma)
+  using OutT = T;
+  __device__ int off(int l, int e) const { return (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e); }
+  __device__ int stride() const { return s.se; }
+  __device__ T *out_ptr(int l, int e) const { return s.out + off(l, e); }
+  __device__ bool has_add() const { return s.add != nullptr; }
+  __device__ const double *add_ptr(int l, int e) const { return s.add + off(l, e); }
+  __device__ bool bc_lo_on() const { return s.bc_lo_on != 0; }
+  __device__ bool bc_hi_on() const { return s.bc_hi_on != 0; }
+  __device__ double bc_lo_val(int l) const { return s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0; }
+  __device__ double bc_hi_val(int l) const { return s.bc_hi ? s.bc_hi[(i0 + l) + s.nth * (m2 - 1)] : 0.0; }
+  // mode 1: slip ghost at j = nr+1 of the z lines of row nr
+  __device__ bool ghost_copy() const { return s.mode == 1 && m2 == s.nr; }
+  __device__ int ghost_off() const { return s.nth; }
+  __device__ double slip() const { return s.slip; }
+  // mode 2: the rows before the first and after the last position of q2's r lines
+  __device__ bool edges() const { return s.mode == 2; }
+  __device__ void edge_lo(int l) const {
+    const int o = off(l, 0) - s.se;
+    s.out[o] = (T)(s.add[o] + 0.0);
+  }
+  __device__ void edge_hi(int l, double v) const { s.out[off(l, n - 1) + s.se] = (T)(0.0 * s.slip * v); }
   // boundary right-hand sides replace rows 0 / n-1 of the z sweeps
   __device__ double fix(int l, int e, double v) const {
     if (e == 0 && s.bc_lo_on) return s.bc_lo ? s.bc_lo[(i0 + l) + s.nth * (m2 - 1)] : 0.0;
@@ -856,8 +892,12 @@ struct MomLine {
   __device__ double Cc(int, int e) const { return __ldg(c + e); }
   __device__ double IB(int, int e) const { return __ldg(ib + e); }
   __device__ void store(int l, int e, double x) const {
-    int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
-    double v = s.add ? s.add[o] + x : x;
+    const int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
+    store_v(l, e, s.add ? s.add[o] + x : x);
+  }
+  // stores the final value v (the added field already included)
+  __device__ void store_v(int l, int e, double v) const {
+    const int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
     s.out[o] = (T)v;
     if (s.mode == 1 && m2 == s.nr) s.out[o + s.nth] = (T)(s.slip * v);
     if (s.mode == 2) {
@@ -879,7 +919,16 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const C
     p.ib = cf.ib;
     p.n = s.n;
     p.nbx = (s.nth + 31) / 32;
-    LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
+    const Geo &g = c->geo;
+    LaunchScope ls(c, s.se == g.nth ? PK_RSWEEP : PK_ZSWEEP);
+    // TMA-pipelined persistent form: 32-line tiles along r, 16-line tiles
+    // along z (lines of up to 544 positions need the narrower tile to keep
+    // three stages in shared memory)
+    cudaError_t e =
+        s.se == g.nth
+            ? run_chunk_tma<32, 16, 17, 3>(p, s.in, g.nth, g.J3, g.K3, 1, nm2, c->nsm, c->d_status, c->stream)
+            : run_chunk_tma<16, 32, 17, 3>(p, s.in, g.nth, g.J3, g.K3, 2, nm2, c->nsm, c->d_status, c->stream);
+    if (e != cudaErrorNotSupported) return e;
     return launch_chunk(p, p.nbx * nm2, c->stream);
   }
   if constexpr (std::is_same<T, double>::value) {

@@ -553,15 +553,42 @@ struct PoisLine {
   static constexpr bool kShortChunks = false;
   static constexpr bool kStageCoef = false;  // the pivots depend on the line's (mode, kz)
   static constexpr bool kStageAC = true;     // aa, cc do not
+  static constexpr bool kLineIB = true;
   __device__ const double *a_ptr() const { return pa; }
   __device__ const double *c_ptr() const { return pc; }
   double *a;
   const double *pa, *pc, *pib;
   int n, nth, nm, nbx, i0, kz;
+  int lpt = 32;  // lines per tile
+  __host__ __device__ int nth_lines() const { return nth; }
   __device__ void set_tile(int tile) {
-    i0 = (tile % nbx) * 32;
+    i0 = (tile % nbx) * lpt;
     kz = tile / nbx;
   }
+  // origin of the tile in the (nth, nr, nz) spectral array
+  __device__ void tma_xyz(int &x, int &y, int &z) const {
+    x = i0;
+    y = 0;
+    z = kz;
+  }
+  // element access of the pipelined form (k_chunk_tma)
+  using OutT = double;
+  __device__ int stride() const { return nth; }
+  __device__ double *out_ptr(int l, int e) const { return a + off(l, e); }
+  __device__ bool has_add() const { return false; }
+  __device__ const double *add_ptr(int, int) const { return nullptr; }
+  __device__ const double *ib_ptr(int l, int e) const { return pib + ((size_t)kz * n + e) * nm + mm(l); }
+  __device__ int ib_stride() const { return nm; }
+  __device__ bool bc_lo_on() const { return false; }
+  __device__ bool bc_hi_on() const { return false; }
+  __device__ double bc_lo_val(int) const { return 0.0; }
+  __device__ double bc_hi_val(int) const { return 0.0; }
+  __device__ bool ghost_copy() const { return false; }
+  __device__ int ghost_off() const { return 0; }
+  __device__ double slip() const { return 0.0; }
+  __device__ bool edges() const { return false; }
+  __device__ void edge_lo(int) const {}
+  __device__ void edge_hi(int, double) const {}
   __device__ bool line_active(int l) const { return i0 + l < nth; }
   __device__ int mm(int l) const { return min((i0 + l + 1) / 2, nm - 1); }
   __device__ size_t off(int l, int e) const { return (size_t)nth * n * kz + (i0 + l) + (size_t)nth * e; }
@@ -695,7 +722,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
     p.nm = g.nth / 2 + 1;
     p.nbx = (N + 31) / 32;
     LaunchScope ls(c, PK_RADIAL);
-    if ((e = launch_chunk(p, p.nbx * g.nz, c->stream))) return e;
+    e = run_chunk_tma<32, 16, 17, 3>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream);
+    if (e == cudaErrorNotSupported) e = launch_chunk(p, p.nbx * g.nz, c->stream);
+    if (e) return e;
   } else if (g.nr <= 640)
     e = run_radial<16, 16>(c);
   else if (g.nr <= 1600)
