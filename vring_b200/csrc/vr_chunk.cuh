@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(32 * NCH, NCH == 16 ? 2 : 1) k_chunk(P p) {
 }
 
 // ---------------------------------------------------------------------------
-// TMA-pipelined form.  Persistent CTAs (one per SM) walk the tiles
+// TMA-pipelined form.  Persistent CTAs (MINB per SM) walk the tiles
 // blockIdx.x, blockIdx.x + gridDim.x, ...; a ring of S shared-memory stages
 // is filled by TMA up to S tiles ahead, so the loads of the next tiles are in
 // flight while the current tile is substituted and stored.  A tile is LPT
@@ -179,15 +179,17 @@ struct TmaTile {
   int nbox, br, ldim;
 };
 
-template <int LPT, int NCH, int MAXCL, int S, class P>
-__global__ void __launch_bounds__(LPT *NCH, 1)
+template <int LPT, int NCH, int MAXCL, int S, int MINB, class P>
+__global__ void __launch_bounds__(LPT *NCH, MINB)
     k_chunk_tma(const __grid_constant__ CUtensorMap tm, P p, int ntiles, TmaTile tt, unsigned *status) {
   constexpr int NP = NCH * MAXCL;  // padded line length
   constexpr int NT = LPT * NCH;
   constexpr bool kLine = P::kLineIB;
   using OutT = typename P::OutT;
   extern __shared__ __align__(128) double stage[];
-  __shared__ double sM[NCH][LPT + 1], sC[NCH][LPT + 1];
+  // chunk maps of the forward and the backward substitution (separate, so
+  // that one tile needs four CTA barriers)
+  __shared__ double sM[NCH][LPT + 1], sC[NCH][LPT + 1], sMb[NCH][LPT + 1], sCb[NCH][LPT + 1];
   __shared__ double2 sAB[kLine ? 1 : NP];  // (a, ib) per position
   __shared__ double sMf[kLine ? 1 : NP];   // -a ib
   __shared__ double sU[kLine ? 1 : NP];    // c ib
@@ -212,6 +214,10 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
                   z + (tt.ldim == 2 ? o : 0), &full[s]);
     }
   };
+  if (smem_u32(stage) & 127u) {  // TMA destinations need 128-byte alignment
+    if (tid == 0) atomicOr(status, 2u);
+    return;
+  }
   if (tid == 0) {
     for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
     mbar_init_fence();
@@ -242,10 +248,6 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
     const int s = k % S;
     p.set_tile(tile);
     const bool ok = mbar_wait(&full[s], (unsigned)(k / S) & 1u);
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
-    }
     const double *buf = stage + (size_t)s * slen + line;
     const bool act = p.line_active(line);
     double v[MAXCL];
@@ -278,14 +280,6 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
 #pragma unroll
       for (int t = 0; t < MAXCL; t++) ibv[t] = (act && (full_chunk || e0 + t < n)) ? __ldg(ip + t * is) : 1.0;
     }
-    __syncthreads();  // stage s has been read by every thread
-    if (tid == 0) {
-      const int nt = tile + S * gridDim.x;
-      if (nt < ntiles) {
-        fence_proxy_async();
-        issue(s, nt);
-      }
-    }
     // forward: chunk map with zero input
     double M = 1.0, C = 0.0;
 #pragma unroll
@@ -303,7 +297,19 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
     }
     sM[c][line] = M;
     sC[c][line] = C;
-    __syncthreads();
+    // every thread has read stage s and written its map; a failed wait ends
+    // the walk for the whole CTA
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0) {
+      const int nt = tile + S * gridDim.x;
+      if (nt < ntiles) {
+        fence_proxy_async();
+        issue(s, nt);
+      }
+    }
     chain_chunks<true, NCH, LPT>(sM, sC, w, lane);
     __syncthreads();
     double y = sC[c][line];
@@ -328,13 +334,12 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
       C = v[t] - u * C;
       M = -u * M;
     }
-    __syncthreads();  // every thread has read its forward input
-    sM[c][line] = M;
-    sC[c][line] = C;
+    sMb[c][line] = M;
+    sCb[c][line] = C;
     __syncthreads();
-    chain_chunks<false, NCH, LPT>(sM, sC, w, lane);
+    chain_chunks<false, NCH, LPT>(sMb, sCb, w, lane);
     __syncthreads();
-    double x = sC[c][line];
+    double x = sCb[c][line];
 #pragma unroll
     for (int t = MAXCL - 1; t >= 0; t--) {
       const int e = e0 + t;
@@ -391,7 +396,7 @@ __global__ void __launch_bounds__(LPT *NCH, 1)
 // lines run along; (d0, d1, d2) the array's extents.  cudaErrorNotSupported
 // when it does not apply (odd theta extent, long lines, encoding refused), so
 // the caller can fall back to k_chunk.
-template <int LPT, int NCH, int MAXCL, int S, class P>
+template <int LPT, int NCH, int MAXCL, int S, int MINB, class P>
 cudaError_t run_chunk_tma(P p, const void *base, int d0, int d1, int d2, int ldim, int nm2, int nsm,
                           unsigned *status, cudaStream_t st) {
   if (p.n < 1 || p.n > NCH * MAXCL || (d0 & 1)) return cudaErrorNotSupported;
@@ -399,17 +404,24 @@ cudaError_t run_chunk_tma(P p, const void *base, int d0, int d1, int d2, int ldi
   tt.ldim = ldim;
   tt.nbox = (p.n + 255) / 256;
   tt.br = (p.n + tt.nbox - 1) / tt.nbox;
+  // a TMA destination in shared memory starts on a 128-byte boundary: round
+  // the box height so that every box and every stage does
+  constexpr int kRowAlign = LPT * 8 >= 128 ? 1 : 128 / (LPT * 8);
+  static_assert((LPT * 8) % 16 == 0 && (LPT * 8 >= 128 ? (LPT * 8) % 128 == 0 : 128 % (LPT * 8) == 0),
+                "tile rows must tile 128-byte boundaries");
+  tt.br = (tt.br + kRowAlign - 1) / kRowAlign * kRowAlign;
+  if (tt.br > 256 || ((size_t)tt.br * LPT * 8) % 128) return cudaErrorNotSupported;
   const size_t dyn = sizeof(double) * (size_t)S * tt.nbox * tt.br * LPT;
   CUtensorMap tm;
   if (!encode_tmap_f64_3d(&tm, base, d0, d1, d2, LPT, ldim == 1 ? tt.br : 1, ldim == 2 ? tt.br : 1))
     return cudaErrorNotSupported;
-  auto kern = k_chunk_tma<LPT, NCH, MAXCL, S, P>;
+  auto kern = k_chunk_tma<LPT, NCH, MAXCL, S, MINB, P>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e) return e;
   p.lpt = LPT;
   p.nbx = (p.nth_lines() + LPT - 1) / LPT;
   const int ntiles = p.nbx * nm2;
-  const int grid = ntiles < nsm ? ntiles : nsm;
+  const int grid = ntiles < MINB * nsm ? ntiles : MINB * nsm;
   kern<<<grid, LPT * NCH, dyn, st>>>(tm, p, ntiles, tt, status);
   return cudaGetLastError();
 }

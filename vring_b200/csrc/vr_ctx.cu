@@ -932,5 +932,7 @@ extern "C" int vr_check_finite(vr_ctx *c, int64_t *count) {
   std::memcpy(&status, &h[3], sizeof(status));
   if (status & 1u)
     return set_err(c, VR_ERR_TIMEOUT, "a sweep kernel gave up waiting for its tile loads; results are not valid");
+  if (status & 2u)
+    return set_err(c, VR_ERR_CUDA, "a sweep kernel found its tile buffer misaligned and did not run");
   return n ? set_err(c, VR_ERR_NONFINITE, "non-finite values in q1..q3/pres") : VR_OK;
 }

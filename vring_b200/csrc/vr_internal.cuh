@@ -128,7 +128,8 @@ struct vr_ctx {
   // diagnostics scratch
   double *d_red;
   unsigned long long *d_count;
-  // device status word: bit 0 set by a kernel whose bounded wait gave up
+  // device status word: bit 0 set by a kernel whose bounded wait gave up,
+  // bit 1 by a pipelined sweep whose shared tile buffer was misaligned
   unsigned *d_status;
   // CUDA graphs for the fused substeps (one per irk), built lazily
   cudaGraphExec_t graph[4];
