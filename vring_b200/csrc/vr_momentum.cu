@@ -271,10 +271,29 @@ struct RhsSamples {
   double ru1, ru2, ru3, pg1, pg2, pg3;
 };
 
-// hdnl1-3 and the RK right-hand sides of one cell from its samples
-__device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int kc, const RhsSamples &S,
-                                         RhsCell &out) {
+// The radial metric coefficients of row jc that the right-hand side uses
+// (ucoeff, momentum_coef.F90:24-69), irm at jc+1, jc and jm = max(jc-1, 1).
+struct RowCoef {
+  double h1d11, h1d22d, h1d22n, h1dare, s1t11, irmp, irmc, irmm, s1t2n, s1t2s, s1t2c, s3t2n, s3t2s;
+  double h2d11, h2d22p, h2d22m, h2dare, s2t11, s2t2p, s2t2c, s2t2m;
+};
+
+__device__ __forceinline__ RowCoef row_coef(const Geo &g, int jc) {
   const int jm = jc > 1 ? jc - 1 : 1;
+  RowCoef m;
+  m.h1d11 = g.h1d11[jc], m.h1d22d = g.h1d22d[jc], m.h1d22n = g.h1d22n[jc], m.h1dare = g.h1dare[jc];
+  m.s1t11 = g.s1t11[jc], m.irmp = g.irm[jc + 1], m.irmc = g.irm[jc], m.irmm = g.irm[jm];
+  m.s1t2n = g.s1t2n[jc], m.s1t2s = g.s1t2s[jc], m.s1t2c = g.s1t2c[jc], m.s3t2n = g.s3t2n[jc];
+  m.s3t2s = g.s3t2s[jc], m.h2d11 = g.h2d11[jc], m.h2d22p = g.h2d22p[jc], m.h2d22m = g.h2d22m[jc];
+  m.h2dare = g.h2dare[jc], m.s2t11 = g.s2t11[jc], m.s2t2p = g.s2t2p[jc], m.s2t2c = g.s2t2c[jc];
+  m.s2t2m = g.s2t2m[jc];
+  return m;
+}
+
+// hdnl1-3 and the RK right-hand sides of one cell from its samples and the
+// coefficients m of its row
+__device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int kc, const RhsSamples &S,
+                                         const RowCoef &m, RhsCell &out) {
   const double A1 = S.A1, A2 = S.A2, A3 = S.A3, A4 = S.A4, A5 = S.A5, A6 = S.A6, A7 = S.A7, A8 = S.A8, A9 = S.A9;
   const double B1 = S.B1, B2 = S.B2, B3 = S.B3, B4 = S.B4, B5 = S.B5, B6 = S.B6, B7 = S.B7, B8 = S.B8, B9 = S.B9;
   const double C1 = S.C1, C2 = S.C2, C3 = S.C3, C4 = S.C4, C5 = S.C5, C6 = S.C6, C7 = S.C7, C8 = S.C8, C9 = S.C9;
@@ -285,27 +304,27 @@ __device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int
   {  // hdnl1 (momentum_terms_swirl.F90:29-68)
     const double q1c = A1, q1p = A2, q1m = A3;
     double qnn = q1p + q1c, qss = q1m + q1c;
-    const double h11 = (qnn * qnn - qss * qss) * g.h1d11[jc];
+    const double h11 = (qnn * qnn - qss * qss) * m.h1d11;
     const double q2cn = B4, q2mn = B8, q2c = B1, q2m = B3;
     qnn = (q2cn + q2mn) * (A4 + q1c);
     qss = (q1c + A5) * (q2c + q2m);
-    const double h12d = (qnn - qss) * g.h1d22d[jc];
+    const double h12d = (qnn - qss) * m.h1d22d;
     qnn = (q1p + q1c) * (q2cn + q2c);
     qss = (q1c + q1m) * (q2mn + q2m);
-    const double h12n = (qnn + qss) * g.h1d22n[jc];
+    const double h12n = (qnn + qss) * m.h1d22n;
     qnn = 0.25 * (C6 + C8) * (A6 + q1c);
     qss = kc == 1 ? 0.0 : 0.25 * (C1 + C3) * (q1c + A7);
     const double h13 = (qnn - qss) * g.dx3;
-    const double d1q2 = ((q2cn + q2c) - (q2mn + q2m)) * g.h1dare[jc];
+    const double d1q2 = ((q2cn + q2c) - (q2mn + q2m)) * m.h1dare;
     h1 = d1q2 - (h11 + (h12d + h12n) + h13);
   }
   {  // RHS q1 (step.F90:32-63)
     const double qc = A1;
-    const double d11 = (A2 - 2.0 * qc + A3) * g.s1t11[jc];
+    const double d11 = (A2 - 2.0 * qc + A3) * m.s1t11;
     const double d33 = kc == 1 ? 4.0 / 3.0 * (A6 - 3.0 * qc + 2.0 * 0.0) * g.dx3q : (A6 - 2.0 * qc + A7) * g.dx3q;
-    const double qnn = (A4 * g.irm[jc + 1] - qc * g.irm[jc]) * g.s1t2n[jc];
-    const double qss = (qc * g.irm[jc] - A5 * g.irm[jm]) * g.s1t2s[jc];
-    const double d22 = (qnn - qss) * g.s1t2c[jc];
+    const double qnn = (A4 * m.irmp - qc * m.irmc) * m.s1t2n;
+    const double qss = (qc * m.irmc - A5 * m.irmm) * m.s1t2s;
+    const double d22 = (qnn - qss) * m.s1t2c;
     r1 = (rk.gam * h1 + rk.rom * ru1 - rk.alm * pg1 + are * (d11 + d33 + d22)) * g.dt;
   }
   if (do3) {
@@ -313,10 +332,10 @@ __device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int
       const double q3c = C1;
       double qnn = (C4 + q3c) * (B4 + B9);
       double qss = (C5 + q3c) * (B1 + B7);
-      const double h32 = (qnn - qss) * g.h1d22d[jc];
+      const double h32 = (qnn - qss) * m.h1d22d;
       qnn = (q3c + C2) * (A2 + A9);
       qss = (C3 + q3c) * (A1 + A7);
-      const double h31 = (qnn - qss) * g.h1d11[jc];
+      const double h31 = (qnn - qss) * m.h1d11;
       qnn = 0.25 * (q3c + C6) * (q3c + C6);
       qss = 0.25 * (q3c + C7) * (q3c + C7);
       const double h33 = (qnn - qss) * g.dx3;
@@ -324,10 +343,10 @@ __device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int
     }
     // RHS q3 (step.F90:93-116)
     const double qc = C1;
-    const double d11 = (C2 - 2.0 * qc + C3) * g.s1t11[jc];
+    const double d11 = (C2 - 2.0 * qc + C3) * m.s1t11;
     const double d33 = (C6 - 2.0 * qc + C7) * g.dx3q;
-    const double qnn = (C4 - qc) * g.s3t2n[jc];
-    const double qss = (qc - C5) * g.s3t2s[jc];
+    const double qnn = (C4 - qc) * m.s3t2n;
+    const double qss = (qc - C5) * m.s3t2s;
     const double d22 = qnn - qss;
     r3 = (rk.gam * h3 + rk.rom * ru3 - rk.alm * pg3 + are * (d11 + d33 + d22)) * g.dt;
   }
@@ -336,24 +355,24 @@ __device__ __forceinline__ void rhs_eval(const Geo &g, const Rk &rk, int jc, int
       const double q1p = A2, q1pm = A8, q1c = A1, q1cm = A5, q2c = B1;
       double qnn = (q1p + q1pm) * (B2 + q2c);
       double qss = (q1c + q1cm) * (q2c + B3);
-      const double h21 = (qnn - qss) * g.h2d11[jc];
+      const double h21 = (qnn - qss) * m.h2d11;
       qnn = B4 + q2c;
       qss = q2c + B5;
-      const double h22 = qnn * qnn * g.h2d22p[jc] - qss * qss * g.h2d22m[jc];
+      const double h22 = qnn * qnn * m.h2d22p - qss * qss * m.h2d22m;
       qnn = 0.5 * (q1c + q1p);
       qss = 0.5 * (q1cm + q1pm);
       const double h11n = 0.25 * (qnn + qss) * (qnn + qss);
       qnn = 0.25 * (C6 + C9) * (B6 + q2c);
       qss = kc == 1 ? 0.0 : 0.25 * (C1 + C5) * (q2c + B7);
       const double h23 = (qnn - qss) * g.dx3;
-      const double d1q1 = -((q1p + q1pm) - (q1c + q1cm)) * g.h2dare[jc];
+      const double d1q1 = -((q1p + q1pm) - (q1c + q1cm)) * m.h2dare;
       h2 = d1q1 - (h21 + h22 + h23 - h11n);
     }
     // RHS q2 (step.F90:144-165)
     const double qc = B1;
-    const double d11 = (B2 - 2.0 * qc + B3) * g.s2t11[jc];
+    const double d11 = (B2 - 2.0 * qc + B3) * m.s2t11;
     const double d33 = kc == 1 ? 4.0 / 3.0 * (B6 - 3.0 * qc + 2.0 * 0.0) * g.dx3q : (B6 - 2.0 * qc + B7) * g.dx3q;
-    const double d22 = B4 * g.s2t2p[jc] - qc * g.s2t2c[jc] + B5 * g.s2t2m[jc];
+    const double d22 = B4 * m.s2t2p - qc * m.s2t2c + B5 * m.s2t2m;
     r2 = (rk.gam * h2 + rk.rom * ru2 - rk.alm * pg2 + are * (d11 + d33 + d22)) * g.dt;
   }
   out = RhsCell{h1, h2, h3, r1, r2, r3};
@@ -382,7 +401,7 @@ __device__ __forceinline__ void rhs_cell(const Geo &g, const Rk &rk, const RhsAr
   S.ru1 = ldt(a.ru[0] + o), S.ru2 = ldt(a.ru[1] + o), S.ru3 = ldt(a.ru[2] + o);
   S.pg1 = ldt(a.prg + IPRG(g, ic, jc, kc, 1)), S.pg2 = ldt(a.prg + IPRG(g, ic, jc, kc, 2));
   S.pg3 = ldt(a.prg + IPRG(g, ic, jc, kc, 3));
-  rhs_eval(g, rk, jc, kc, S, out);
+  rhs_eval(g, rk, jc, kc, S, row_coef(g, jc), out);
 }
 
 __global__ void __launch_bounds__(128) k_rhs_fused(Geo g, Rk rk, RhsArgs a) {
@@ -624,6 +643,310 @@ static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a)
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// z-marching form of the fused right-hand side and theta solve.  A CTA owns
+// kMRJ r-rows and up to zs consecutive z-planes and walks them in z.  q1..q3
+// of rows j0-1 .. j0+kMRJ at each plane arrive through a ring of kQRing
+// shared-memory slots that TMA fills kQRing-2 planes ahead, so the stencil
+// reads shared memory and every q word crosses HBM once per CTA; each thread
+// prefetches the ru and prg words of its cell one plane ahead into
+// registers.  The row coefficients and theta factorisations stay staged for
+// the whole walk.
+//
+// The right-hand sides of kTB consecutive planes collect in shared memory;
+// then the warps solve their theta lines 32 / kTL at a time (tsolve_group),
+// so the CTA pays one solve phase per kTB planes and the short group scans
+// keep the instruction count per unknown low.
+// ---------------------------------------------------------------------------
+constexpr int kMRJ = 2, kQRing = 5, kMarchZ = 32, kTB = 4;
+
+// Periodic theta solve of one line by a group of kTL consecutive lanes of a
+// warp (the arithmetic of tsolve_warp; lane g of the group owns the EG
+// contiguous inner unknowns [g EG, g EG + EG)), so a warp solves 32 / kTL
+// lines side by side with short scans.  Groups with on = false touch no
+// memory but take part in the shuffles.
+constexpr int kTL = 8;
+
+template <int EG>
+__device__ __forceinline__ void tsolve_group(int N, const double *cinv, const double *cpp, const double *czz,
+                                             const double *rt, double *sl, int gl, bool on) {
+  const double A = rt[0];
+  const int inner = N - 1;
+  const int i0 = gl * EG;
+  int cnt = on ? inner - i0 : 0;
+  cnt = cnt < 0 ? 0 : (cnt > EG ? EG : cnt);
+  double y[EG];
+  Aff acc{1.0, 0.0};
+#pragma unroll
+  for (int e = 0; e < EG; e++) {
+    y[e] = 0.0;
+    if (e < cnt) {
+      const int i = tpad(i0 + e);
+      const double fi = sl[i], iv = cinv[i];
+      y[e] = fi;
+      acc.C = (fi - A * acc.C) * iv;
+      acc.M = -A * iv * acc.M;
+    }
+  }
+#pragma unroll
+  for (int d = 1; d < kTL; d <<= 1) {
+    Aff o{__shfl_up_sync(0xffffffffu, acc.M, d, kTL), __shfl_up_sync(0xffffffffu, acc.C, d, kTL)};
+    if (gl >= d) acc = aff_then(o, acc);
+  }
+  double yin = __shfl_up_sync(0xffffffffu, acc.C, 1, kTL);
+  if (gl == 0) yin = 0.0;
+#pragma unroll
+  for (int e = 0; e < EG; e++) {
+    if (e < cnt) {
+      yin = (y[e] - A * yin) * cinv[tpad(i0 + e)];
+      y[e] = yin;
+    }
+  }
+  acc = Aff{1.0, 0.0};
+#pragma unroll
+  for (int e = EG - 1; e >= 0; e--) {
+    if (e < cnt) {
+      const double pv = cpp[tpad(i0 + e)];
+      acc.C = y[e] - pv * acc.C;
+      acc.M = -pv * acc.M;
+    }
+  }
+#pragma unroll
+  for (int d = 1; d < kTL; d <<= 1) {
+    Aff o{__shfl_down_sync(0xffffffffu, acc.M, d, kTL), __shfl_down_sync(0xffffffffu, acc.C, d, kTL)};
+    if (gl + d < kTL) acc = aff_then(o, acc);
+  }
+  double win = __shfl_down_sync(0xffffffffu, acc.C, 1, kTL);
+  if (gl == kTL - 1) win = 0.0;
+#pragma unroll
+  for (int e = EG - 1; e >= 0; e--) {
+    if (e < cnt) {
+      win = y[e] - cpp[tpad(i0 + e)] * win;
+      y[e] = win;
+    }
+  }
+  // bordering unknown N (step.F90:526-533)
+  const int last_lane = (inner - 1) / EG, last_e = (inner - 1) - last_lane * EG;
+  const double w1 = __shfl_sync(0xffffffffu, y[0], 0, kTL);
+  double wl = 0.0;
+#pragma unroll
+  for (int e = 0; e < EG; e++)
+    if (e == last_e) wl = y[e];
+  wl = __shfl_sync(0xffffffffu, wl, last_lane, kTL);
+  if (on) {
+    const double fN = sl[tpad(N - 1)];
+    const double xN = (fN - rt[1] * w1 - A * wl) / rt[2];
+#pragma unroll
+    for (int e = 0; e < EG; e++)
+      if (e < cnt) sl[tpad(i0 + e)] = y[e] + czz[tpad(i0 + e)] * xN;
+    if (gl == 0) sl[tpad(N - 1)] = xN;
+  }
+}
+
+template <int E, int CPT, class T>
+__global__ void __launch_bounds__(256, 2)
+    k_rhs_march(const __grid_constant__ CUtensorMap tq1, const __grid_constant__ CUtensorMap tq2,
+                const __grid_constant__ CUtensorMap tq3, Geo g, Rk rk, RhsArgsT<T> a, TriPer t13, TriPer t2,
+                int zs, unsigned *status) {
+  extern __shared__ __align__(128) double sm[];
+  const int N = g.nth, SPN = tpad(N) + 1;
+  const int FS = (kMRJ + 2) * N;    // doubles of one field's box
+  const int FSP = (FS + 15) & ~15;  // box slots start on 128-byte boundaries
+  const int SLOT = 3 * FSP;
+  double *ring = sm;                           // [slot][field][row j0-1+rr][i]
+  // line stride of the solve buffers: 8 mod 16 doubles, so the 32 / kTL
+  // groups of a warp fall on disjoint halves of the shared-memory banks
+  const int SPL = ((SPN + 15) & ~15) + 8;
+  double *lines = ring + kQRing * SLOT;        // [plane of batch][comp][r], each SPL
+  double *fac = lines + kTB * 3 * kMRJ * SPL;  // [fam][r][inv, pp, zz], each SPN
+  __shared__ RowCoef rowc[kMRJ];
+  __shared__ double rowt[kMRJ][2][3];  // sub, sup, za2 of each family
+  __shared__ __align__(8) uint64_t full[kQRing];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nzb = (g.nz + zs - 1) / zs;
+  const int j0 = 1 + (int)(blockIdx.x / nzb) * kMRJ;
+  const int kb = 1 + (int)(blockIdx.x % nzb) * zs;
+  const int ke = min(kb + zs, g.nz + 1);  // planes kb .. ke-1 are evaluated
+  const int nplanes = ke - kb + 2;        // planes kb-1 .. ke are loaded
+  if (smem_u32(sm) & 127u) {
+    if (tid == 0) atomicOr(status, 2u);
+    return;
+  }
+  auto issue = [&](int pr) {  // plane kb-1+pr into slot pr % kQRing
+    const int sl = pr % kQRing, kc = kb - 1 + pr;
+    double *dst = ring + (size_t)sl * SLOT;
+    mbar_expect_tx(&full[sl], 3u * (unsigned)FS * 8u);
+    tma_load_3d(dst, &tq1, 0, j0 - 1, kc, &full[sl]);
+    tma_load_3d(dst + FSP, &tq2, 0, j0 - 1, kc, &full[sl]);
+    tma_load_3d(dst + 2 * FSP, &tq3, 0, j0 - 1, kc, &full[sl]);
+  };
+  if (tid == 0) {
+    for (int sl = 0; sl < kQRing; sl++) mbar_init(&full[sl], 1);
+    mbar_init_fence();
+    for (int pr = 0; pr < kQRing && pr < nplanes; pr++) issue(pr);
+  }
+  for (int idx = tid; idx < 2 * kMRJ * N; idx += blockDim.x) {
+    const int i = idx % N, r = (idx / N) % kMRJ, fam = idx / (N * kMRJ), jc = j0 + r;
+    if (jc > g.nr) continue;
+    const double *inv = fam ? t2.inv : t13.inv, *pp = fam ? t2.pp : t13.pp, *zz = fam ? t2.zz : t13.zz;
+    double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPN;
+    cp_async8(f + tpad(i), inv + (size_t)jc * N + i);
+    cp_async8(f + SPN + tpad(i), pp + (size_t)jc * N + i);
+    cp_async8(f + 2 * SPN + tpad(i), zz + (size_t)jc * N + i);
+  }
+  if (tid < kMRJ && j0 + tid <= g.nr) {
+    const int jc = j0 + tid;
+    rowc[tid] = row_coef(g, jc);
+    rowt[tid][0][0] = t13.sub[jc], rowt[tid][0][1] = t13.sup[jc], rowt[tid][0][2] = t13.za2[jc];
+    rowt[tid][1][0] = t2.sub[jc], rowt[tid][1][1] = t2.sup[jc], rowt[tid][1][2] = t2.za2[jc];
+  }
+  // this thread's cells: (r, i) = divmod(tid + 256 q, N)
+  int ci[CPT], cr[CPT];
+  bool cact[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; q++) {
+    const int cell = tid + 256 * q;
+    cr[q] = cell / N;
+    ci[q] = cell % N;
+    cact[q] = cell < kMRJ * N && j0 + cr[q] <= g.nr;
+  }
+  double pru[CPT][3], ppg[CPT][3];
+  auto prefetch = [&](int kc) {
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+      if (!cact[q]) continue;
+      const int jc = j0 + cr[q], o = I3(g, ci[q] + 1, jc, kc);
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        pru[q][m] = ldt(a.ru[m] + o);
+        ppg[q][m] = ldt(a.prg + IPRG(g, ci[q] + 1, jc, kc, m + 1));
+      }
+    }
+  };
+  prefetch(kb);
+  cp_async_wait_all();
+  __syncthreads();
+
+  bool failed = false;
+  int last_pr = 0;
+  for (int kc = kb; kc < ke; kc++) {
+    const int pr = kc - kb + 1;  // relative index of plane kc
+    const int pb = (kc - kb) % kTB;  // plane within the solve batch
+    last_pr = pr;
+    bool ok = true;
+    if (kc == kb) ok = mbar_wait(&full[0], 0u) && mbar_wait(&full[1 % kQRing], 0u);
+    ok = ok && mbar_wait(&full[(pr + 1) % kQRing], (unsigned)((pr + 1) / kQRing) & 1u);
+    double cru[CPT][3], cpg[CPT][3];
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+#pragma unroll
+      for (int m = 0; m < 3; m++) cru[q][m] = pru[q][m], cpg[q][m] = ppg[q][m];
+    if (kc + 1 < ke) prefetch(kc + 1);
+    const double *sp = ring + (size_t)((pr - 1) % kQRing) * SLOT;
+    const double *sc = ring + (size_t)(pr % kQRing) * SLOT;
+    const double *sn = ring + (size_t)((pr + 1) % kQRing) * SLOT;
+    double *lb = lines + (size_t)pb * 3 * kMRJ * SPL;
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+      if (!cact[q]) continue;
+      const int i = ci[q], r = cr[q], jc = j0 + r;
+      const int ip = i + 1 < N ? i + 1 : 0, im = i > 0 ? i - 1 : N - 1;
+      const int rc = (r + 1) * N, rn = (r + 2) * N, rs = r * N;  // rows jc, jc+1, jc-1
+      const int rjm = jc > 1 ? rs : rc;                          // row max(jc-1, 1)
+      const double *p1 = sp, *c1 = sc, *n1 = sn;
+      const double *p2 = sp + FSP, *c2 = sc + FSP, *n2 = sn + FSP;
+      const double *p3 = sp + 2 * FSP, *c3 = sc + 2 * FSP, *n3 = sn + 2 * FSP;
+      RhsSamples S;
+      S.A1 = c1[rc + i], S.A2 = c1[rc + ip], S.A3 = c1[rc + im], S.A4 = c1[rn + i], S.A5 = c1[rjm + i];
+      S.A6 = n1[rc + i], S.A7 = p1[rc + i], S.A8 = c1[rs + ip], S.A9 = p1[rc + ip];
+      S.B1 = c2[rc + i], S.B2 = c2[rc + ip], S.B3 = c2[rc + im], S.B4 = c2[rn + i], S.B5 = c2[rs + i];
+      S.B6 = n2[rc + i], S.B7 = p2[rc + i], S.B8 = c2[rn + im], S.B9 = p2[rn + i];
+      S.C1 = c3[rc + i], S.C2 = c3[rc + ip], S.C3 = c3[rc + im], S.C4 = c3[rn + i], S.C5 = c3[rjm + i];
+      S.C6 = n3[rc + i], S.C7 = p3[rc + i], S.C8 = n3[rc + im], S.C9 = n3[rs + i];
+      S.ru1 = cru[q][0], S.ru2 = cru[q][1], S.ru3 = cru[q][2];
+      S.pg1 = cpg[q][0], S.pg2 = cpg[q][1], S.pg3 = cpg[q][2];
+      RhsCell v;
+      rhs_eval(g, rk, jc, kc, S, rowc[r], v);
+      const int o = I3(g, i + 1, jc, kc);
+      a.ru[0][o] = (T)v.h1;
+      lb[(size_t)(0 * kMRJ + r) * SPL + tpad(i)] = v.r1;
+      if (kc >= 2) {
+        a.ru[2][o] = (T)v.h3;
+        lb[(size_t)(2 * kMRJ + r) * SPL + tpad(i)] = v.r3;
+      }
+      if (jc >= 2) {
+        a.ru[1][o] = (T)v.h2;
+        lb[(size_t)(1 * kMRJ + r) * SPL + tpad(i)] = v.r2;
+      }
+    }
+    // the plane's lines are written and plane kc-1 has been read by all; a
+    // failed wait ends the walk for the whole CTA
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0 && pr - 1 + kQRing < nplanes) {
+      fence_proxy_async();
+      issue(pr - 1 + kQRing);
+    }
+    if (pb == kTB - 1 || kc == ke - 1) {
+      // solve the batch's [plane][comp][r] lines, 32 / kTL per warp
+      constexpr int kGroups = 32 / kTL, kSolveWarps = kTB * 3 * kMRJ / kGroups;
+      static_assert(kTB * 3 * kMRJ % kGroups == 0 && kSolveWarps <= 8, "solve batch does not fit the warps");
+      const int kc0 = kc - pb;
+      if (warp < kSolveWarps) {
+        const int L = warp * kGroups + lane / kTL;
+        const int pl = L / (3 * kMRJ), comp = (L / kMRJ) % 3, r = L % kMRJ, jc = j0 + r, lk = kc0 + pl;
+        const int fam = comp == 1 ? 1 : 0;
+        const double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPN;
+        const bool on = lk <= kc && jc <= g.nr && !(comp == 1 && jc < 2) && !(comp == 2 && lk < 2);
+        tsolve_group<(32 / kTL) * E>(N, f, f + SPN, f + 2 * SPN, &rowt[r][fam][0], lines + (size_t)L * SPL,
+                                     lane % kTL, on);
+        __syncwarp();
+#pragma unroll
+        for (int gq = 0; gq < kGroups; gq++) {
+          const int L2 = warp * kGroups + gq;
+          const int pl2 = L2 / (3 * kMRJ), comp2 = (L2 / kMRJ) % 3, r2 = L2 % kMRJ, jc2 = j0 + r2, lk2 = kc0 + pl2;
+          if (lk2 > kc || jc2 > g.nr || (comp2 == 1 && jc2 < 2) || (comp2 == 2 && lk2 < 2)) continue;
+          double *dst = (comp2 == 0 ? a.qrhs[0] : (comp2 == 1 ? a.qrhs[1] : a.qrhs[2])) + I3(g, 1, jc2, lk2);
+          const double *src = lines + (size_t)L2 * SPL;
+          for (int i = lane; i < N; i += 32) dst[i] = src[tpad(i)];
+        }
+      }
+      __syncthreads();  // the batch's lines are free again
+    }
+  }
+  if (failed && tid == 0) {
+    // record the timeout and let the loads already issued land (bounded)
+    atomicOr(status, 1u);
+    const int hi = min(last_pr + kQRing - 1, nplanes - 1);
+    for (int p = last_pr + 1; p <= hi; p++) (void)mbar_wait(&full[p % kQRing], (unsigned)(p / kQRing) & 1u);
+  }
+}
+
+template <int E, int CPT, class T>
+static cudaError_t run_rhs_march(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) {
+  const Geo &g = c->geo;
+  if ((g.nth & 1) || kMRJ * g.nth > 256 * CPT || g.nth - 1 > 32 * E) return cudaErrorNotSupported;
+  CUtensorMap tm[3];
+  for (int m = 0; m < 3; m++)
+    if (!encode_tmap_f64_3d(&tm[m], c->q[m], g.nth, g.J3, g.K3, g.nth, kMRJ + 2, 1)) return cudaErrorNotSupported;
+  const int SPN = tpad(g.nth) + 1;
+  const int FS = (kMRJ + 2) * g.nth, FSP = (FS + 15) & ~15;
+  const int SPL = ((SPN + 15) & ~15) + 8;
+  const size_t sm = sizeof(double) * ((size_t)kQRing * 3 * FSP + kTB * 3 * kMRJ * SPL + 2 * kMRJ * 3 * SPN);
+  if (sm > 110 * 1024) return cudaErrorNotSupported;  // two CTAs per SM
+  auto kern = k_rhs_march<E, CPT, T>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
+  const int zs = kMarchZ;
+  const int grid = ((g.nr + kMRJ - 1) / kMRJ) * ((g.nz + zs - 1) / zs);
+  LaunchScope ls(c, PK_RHS);
+  kern<<<grid, 256, sm, c->stream>>>(tm[0], tm[1], tm[2], g, rk, a, t13, t2, zs, c->d_status);
+  return cudaGetLastError();
+}
+
 template <class T>
 static cudaError_t launch_rhs_tsweep_t(vr_ctx *c, const Rk &rk) {
   const Geo &g = c->geo;
@@ -636,6 +959,14 @@ static cudaError_t launch_rhs_tsweep_t(vr_ctx *c, const Rk &rk) {
   }
   a.prg = reinterpret_cast<const T *>(c->prg);
   const int E = (g.nth - 1 + 31) / 32;
+  cudaError_t me = cudaErrorNotSupported;
+  if (E <= 1)
+    me = run_rhs_march<1, 1, T>(c, rk, a);
+  else if (E <= 2)
+    me = run_rhs_march<2, 1, T>(c, rk, a);
+  else if (E <= 4)
+    me = run_rhs_march<4, 1, T>(c, rk, a);
+  if (me != cudaErrorNotSupported) return me;
   if (E <= 1) return run_rhs_tsweep<1, T>(c, rk, a);
   if (E <= 2) return run_rhs_tsweep<2, T>(c, rk, a);
   if (E <= 4) return run_rhs_tsweep<4, T>(c, rk, a);
