@@ -810,7 +810,9 @@ __global__ void __launch_bounds__(256, 2)
     ci[q] = cell % N;
     cact[q] = cell < kMRJ * N && j0 + cr[q] <= g.nr;
   }
-  double pru[CPT][3], ppg[CPT][3];
+  // prefetched in the storage type: a conversion right after the load
+  // would wait for it
+  T pru[CPT][3], ppg[CPT][3];
   auto prefetch = [&](int kc) {
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
@@ -818,8 +820,8 @@ __global__ void __launch_bounds__(256, 2)
       const int jc = j0 + cr[q], o = I3(g, ci[q] + 1, jc, kc);
 #pragma unroll
       for (int m = 0; m < 3; m++) {
-        pru[q][m] = ldt(a.ru[m] + o);
-        ppg[q][m] = ldt(a.prg + IPRG(g, ci[q] + 1, jc, kc, m + 1));
+        pru[q][m] = __ldg(a.ru[m] + o);
+        ppg[q][m] = __ldg(a.prg + IPRG(g, ci[q] + 1, jc, kc, m + 1));
       }
     }
   };
@@ -836,7 +838,7 @@ __global__ void __launch_bounds__(256, 2)
     bool ok = true;
     if (kc == kb) ok = mbar_wait(&full[0], 0u) && mbar_wait(&full[1 % kQRing], 0u);
     ok = ok && mbar_wait(&full[(pr + 1) % kQRing], (unsigned)((pr + 1) / kQRing) & 1u);
-    double cru[CPT][3], cpg[CPT][3];
+    T cru[CPT][3], cpg[CPT][3];
 #pragma unroll
     for (int q = 0; q < CPT; q++)
 #pragma unroll
@@ -863,8 +865,8 @@ __global__ void __launch_bounds__(256, 2)
       S.B6 = n2[rc + i], S.B7 = p2[rc + i], S.B8 = c2[rn + im], S.B9 = p2[rn + i];
       S.C1 = c3[rc + i], S.C2 = c3[rc + ip], S.C3 = c3[rc + im], S.C4 = c3[rn + i], S.C5 = c3[rjm + i];
       S.C6 = n3[rc + i], S.C7 = p3[rc + i], S.C8 = n3[rc + im], S.C9 = n3[rs + i];
-      S.ru1 = cru[q][0], S.ru2 = cru[q][1], S.ru3 = cru[q][2];
-      S.pg1 = cpg[q][0], S.pg2 = cpg[q][1], S.pg3 = cpg[q][2];
+      S.ru1 = (double)cru[q][0], S.ru2 = (double)cru[q][1], S.ru3 = (double)cru[q][2];
+      S.pg1 = (double)cpg[q][0], S.pg2 = (double)cpg[q][1], S.pg3 = (double)cpg[q][2];
       RhsCell v;
       rhs_eval(g, rk, jc, kc, S, rowc[r], v);
       const int o = I3(g, i + 1, jc, kc);
