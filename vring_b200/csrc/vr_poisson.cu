@@ -281,6 +281,234 @@ __global__ void __launch_bounds__(256) k_fft_bwd_w(const double *__restrict__ in
   }
 }
 
+// ---------------------------------------------------------------------------
+// theta transforms of length N = 16 T without shuffles.  T consecutive
+// threads of a warp transform a pair of lines (a, b) as a + i b by
+// Cooley-Tukey with N = 16 x T:
+//   X[k1 + 16 k2] = sum_t W_T^{t k2} W_N^{t k1} sum_m x[t + T m] W_16^{m k1}
+// thread t holds the 16 points x[t + T m] and runs the 16-point DFT in
+// registers; after the twiddles W_N^{t k1} one shared-memory transpose gives
+// thread t the k1 values t G .. t G + G - 1 (G = 16 / T) of every t, and the
+// T-point DFTs run in registers too.  A second pass through shared memory
+// pairs X_k with X_{N-k} to separate the two real lines.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int brev_c(int x, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+__host__ __device__ constexpr int log2_c(int x) { return x <= 1 ? 0 : 1 + log2_c(x / 2); }
+
+// Radix-2 decimation-in-frequency DFT of the L points re/im[OFF .. OFF+L) in
+// registers with W_{2h}^q = W_N^{q N / (2h)} from stw (cos, sin pairs);
+// X[k] ends in slot OFF + brev(k).  Multiplications by W^0 = 1 are skipped
+// (they are exact).
+template <int L, int N, int OFF, int R>
+__device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const double *stw) {
+#pragma unroll
+  for (int h = L / 2; h >= 1; h >>= 1) {
+#pragma unroll
+    for (int j = 0; j < L; j++) {
+      if ((j & h) == 0) {
+        const int ja = OFF + j, jb = OFF + j + h;
+        const double ar = re[ja], ai = im[ja], br = re[jb], bi = im[jb];
+        re[ja] = ar + br;
+        im[ja] = ai + bi;
+        const double dr = ar - br, di = ai - bi;
+        const int q = j & (h - 1);
+        if (q == 0) {
+          re[jb] = dr;
+          im[jb] = di;
+        } else {
+          const int p = q * (N / (2 * h));
+          const double c = stw[2 * p], sn = -stw[2 * p + 1];
+          re[jb] = dr * c - di * sn;
+          im[jb] = dr * sn + di * c;
+        }
+      }
+    }
+  }
+}
+
+// The two-stage transform of the pair held as x[t + T m] in re/im[m]; on
+// return sre/sim[k] hold X[k] (natural order) for this pair.
+// Per-pair shared buffer: re at 0, im at PS, pairs 2 PS + 1 doubles apart.
+// The odd pair stride puts the pairs of a half-warp on different banks for
+// the transpose reads and the spectrum accesses (about half the wavefronts
+// of an aligned stride).
+__host__ __device__ constexpr int fft_pair_stride(int T) { return 16 * (T + 1) + 2; }
+
+// gm: the lanes of this pair's group (a group exits as a whole)
+template <int T>
+__device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], const double *stw, double *sre,
+                                           double *sim, int t, unsigned gm) {
+  constexpr int N = 16 * T, G = 16 / T, LT = log2_c(T);
+  reg_dif<16, N, 0, 16>(re, im, stw);
+  // twiddles W_N^{t k1} and the transpose S[k1][t] (row stride T + 1)
+#pragma unroll
+  for (int k1 = 0; k1 < 16; k1++) {
+    const int rg = brev_c(k1, 4);
+    double yr = re[rg], yi = im[rg];
+    if (k1 != 0) {
+      const int p = t * k1;
+      const double c = stw[2 * p], sn = -stw[2 * p + 1];
+      const double xr = yr * c - yi * sn, xi = yr * sn + yi * c;
+      yr = xr;
+      yi = xi;
+    }
+    sre[k1 * (T + 1) + t] = yr;
+    sim[k1 * (T + 1) + t] = yi;
+  }
+  __syncwarp(gm);
+#pragma unroll
+  for (int u = 0; u < G; u++)
+#pragma unroll
+    for (int tt = 0; tt < T; tt++) {
+      re[u * T + tt] = sre[(t * G + u) * (T + 1) + tt];
+      im[u * T + tt] = sim[(t * G + u) * (T + 1) + tt];
+    }
+  __syncwarp(gm);
+  if constexpr (G >= 1) reg_dif<T, N, 0, 16>(re, im, stw);
+  if constexpr (G >= 2) reg_dif<T, N, T, 16>(re, im, stw);
+  if constexpr (G >= 4) {
+    reg_dif<T, N, 2 * T, 16>(re, im, stw);
+    reg_dif<T, N, 3 * T, 16>(re, im, stw);
+  }
+  if constexpr (G >= 8) {
+#pragma unroll
+    for (int u = 4; u < 8; u++) {
+      // G = 8 means T = 2: one butterfly per pair of slots
+      const int ja = u * 2, jb = ja + 1;
+      const double ar = re[ja], ai = im[ja], br = re[jb], bi = im[jb];
+      re[ja] = ar + br;
+      im[ja] = ai + bi;
+      re[jb] = ar - br;
+      im[jb] = ai - bi;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < G; u++)
+#pragma unroll
+    for (int k2 = 0; k2 < T; k2++) {
+      const int k = t * G + u + 16 * k2;
+      sre[k] = re[u * T + brev_c(k2, LT)];
+      sim[k] = im[u * T + brev_c(k2, LT)];
+    }
+  __syncwarp(gm);
+}
+
+template <int T>
+__global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in, double *__restrict__ out,
+                                                   int nlines, const double *__restrict__ tw) {
+  constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
+  extern __shared__ double sm[];
+  double *stw = sm;
+  const int tid = threadIdx.x, t = tid % T, pl = tid / T;
+  double *sre = sm + 2 * N + (size_t)pl * (2 * PS + 1), *sim = sre + PS;
+  for (int i = tid; i < 2 * N; i += 128) stw[i] = __ldg(tw + i);
+  __syncthreads();
+  const int la = (blockIdx.x * NPB + pl) * 2;
+  if (la >= nlines) return;  // no CTA barrier follows; the pair's group leaves together
+  const unsigned gm = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((tid & 31) / T * T));
+  const bool hasb = la + 1 < nlines;
+  const double *pa = in + (size_t)la * N, *pb = pa + N;
+  double re[16], im[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    re[m] = pa[t + T * m];
+    im[m] = hasb ? pb[t + T * m] : 0.0;
+  }
+  pair_fft16<T>(re, im, stw, sre, sim, t, gm);
+  // packed [a0, a1, b1, ...] of both lines (fastfouriertransform.F90:34-43)
+  double *oa = out + (size_t)la * N, *ob = oa + N;
+  const double invn = 1.0 / N;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const int sx = t + T * j;
+    double va, vb;
+    if (sx == 0) {
+      va = sre[0] * invn;
+      vb = sim[0] * invn;
+    } else {
+      const int k = (sx + 1) >> 1, km = (N - k) & (N - 1);
+      const double zr = sre[k], zi = sim[k], mr = sre[km], mi = sim[km];
+      if (sx & 1) {
+        va = (zr + mr) * invn;
+        vb = (zi + mi) * invn;
+      } else {
+        va = -(zi - mi) * invn;
+        vb = (zr - mr) * invn;
+      }
+    }
+    oa[sx] = va;
+    if (hasb) ob[sx] = vb;
+  }
+}
+
+template <int T>
+__global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in, double *__restrict__ dph, Geo g,
+                                                   int nlines, const double *__restrict__ tw) {
+  constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
+  extern __shared__ double sm[];
+  double *stw = sm;
+  const int tid = threadIdx.x, t = tid % T, pl = tid / T;
+  double *sre = sm + 2 * N + (size_t)pl * (2 * PS + 1), *sim = sre + PS;
+  for (int i = tid; i < 2 * N; i += 128) stw[i] = __ldg(tw + i);
+  __syncthreads();
+  const int la = (blockIdx.x * NPB + pl) * 2;
+  if (la >= nlines) return;  // no CTA barrier follows; the pair's group leaves together
+  const unsigned gm = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((tid & 31) / T * T));
+  const bool hasb = la + 1 < nlines;
+  const double *pa = in + (size_t)la * N, *pb = pa + N;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    sre[t + T * j] = pa[t + T * j];
+    sim[t + T * j] = hasb ? pb[t + T * j] : 0.0;
+  }
+  __syncwarp(gm);
+  // Z_k = A_k + i B_k from the packed Hermitian spectra, conjugated: the
+  // inverse transform runs as conj(DFT(conj Z)) (fastfouriertransform.F90:49-87)
+  double re[16], im[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int k = t + T * m;
+    const int kk = k <= N / 2 ? k : N - k;
+    double ar, ai, br, bi;
+    if (kk == 0) {
+      ar = sre[0];
+      ai = 0.0;
+      br = sim[0];
+      bi = 0.0;
+    } else {
+      ar = sre[2 * kk - 1] / 2.0;
+      br = sim[2 * kk - 1] / 2.0;
+      ai = (2 * kk < N) ? -1.0 * sre[2 * kk] / 2.0 : 0.0;
+      bi = (2 * kk < N) ? -1.0 * sim[2 * kk] / 2.0 : 0.0;
+      if (k > N / 2) {
+        ai = -ai;
+        bi = -bi;
+      }
+    }
+    re[m] = ar - bi;
+    im[m] = -(ai + br);
+  }
+  __syncwarp(gm);
+  pair_fft16<T>(re, im, stw, sre, sim, t, gm);
+  const int ja = 1 + la % g.nr, ka = 1 + la / g.nr;
+  double *da = dph + IDP(g, 1, ja, ka);
+  double *db = nullptr;
+  if (hasb) {
+    const int lb = la + 1;
+    db = dph + IDP(g, 1, 1 + lb % g.nr, 1 + lb / g.nr);
+  }
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const int n = t + T * j;
+    da[n] = sre[n];
+    if (hasb) db[n] = -sim[n];
+  }
+}
+
 // z transforms: a CTA stages LT columns (consecutive theta, fixed r) x nz in
 // shared memory with 128-byte row loads; warp w transforms columns 2w, 2w+1
 // as one complex sequence (Makhoul's even/odd reordering turns the DCT into
@@ -642,13 +870,32 @@ static cudaError_t run_fft_w(vr_ctx *c, int dir) {
   return cudaGetLastError();
 }
 
+template <int T>
+static cudaError_t run_fft_s(vr_ctx *c, int dir) {
+  const Geo &g = c->geo;
+  constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
+  const int nlines = g.nr * g.nz;
+  const size_t sm = sizeof(double) * (2 * N + (size_t)NPB * (2 * PS + 1));
+  const int npairs = (nlines + 1) / 2, blocks = (npairs + NPB - 1) / NPB;
+  cudaError_t e;
+  LaunchScope ls(c, PK_FFT);
+  if (dir > 0) {
+    if ((e = cudaFuncSetAttribute(k_fft_fwd_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_fwd_s<T><<<blocks, 128, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th);
+  } else {
+    if ((e = cudaFuncSetAttribute(k_fft_bwd_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    k_fft_bwd_s<T><<<blocks, 128, sm, c->stream>>>(c->spec, c->dph, g, nlines, c->tw_th);
+  }
+  return cudaGetLastError();
+}
+
 static cudaError_t fft_warp_dispatch(vr_ctx *c, int dir, bool *done) {
   *done = true;
   switch (c->geo.nth) {
-    case 32: return run_fft_w<1>(c, dir);
-    case 64: return run_fft_w<2>(c, dir);
-    case 128: return run_fft_w<4>(c, dir);
-    case 256: return run_fft_w<8>(c, dir);
+    case 32: return run_fft_s<2>(c, dir);
+    case 64: return run_fft_s<4>(c, dir);
+    case 128: return run_fft_s<8>(c, dir);
+    case 256: return run_fft_s<16>(c, dir);
     case 512: return run_fft_w<16>(c, dir);
     case 1024: return run_fft_w<32>(c, dir);
     default: *done = false; return cudaSuccess;
