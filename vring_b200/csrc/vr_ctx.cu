@@ -867,8 +867,7 @@ static int enqueue_substep(vr_ctx *c, int irk) {
   }
   VR_CUDA(c, launch_divq(c, rk));
   VR_CUDA(c, launch_poisson(c));
-  VR_CUDA(c, launch_upsol(c, rk));
-  VR_CUDA(c, launch_uppres(c, rk));
+  VR_CUDA(c, launch_upsol_uppres(c, rk));
   return VR_OK;
 }
 

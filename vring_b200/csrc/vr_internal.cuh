@@ -216,6 +216,7 @@ cudaError_t launch_divq(vr_ctx *c, const Rk &rk);
 cudaError_t launch_poisson(vr_ctx *c);
 cudaError_t launch_upsol(vr_ctx *c, const Rk &rk);
 cudaError_t launch_uppres(vr_ctx *c, const Rk &rk);
+cudaError_t launch_upsol_uppres(vr_ctx *c, const Rk &rk);
 cudaError_t launch_maxdiv(vr_ctx *c, double *d_out);
 cudaError_t launch_count_nonfinite(vr_ctx *c, unsigned long long *d_out);
 

@@ -265,12 +265,28 @@ __global__ void __launch_bounds__(128) k_uppres_r(Geo g, double be, const double
 // never used), and each thread prefetches its cell's prg1..3 and pres one
 // plane ahead into registers.
 // ---------------------------------------------------------------------------
+//
+// With UPSOL the same walk also runs upsol (divergence.F90:69-236) from the
+// dph planes in the ring: q1..q3 of the CTA's cells from dq1..q3 (prefetched
+// like prg), plus the rows and the plane upsol covers beyond uppres: the
+// thread of row 1 writes q3 of row 0 on plane 1 and q2 = 0 on row 1, the
+// thread of row nr the slip ghosts of row nrc, and the CTA holding plane nz
+// takes one more step for the north ghost plane nzc (dph read there through
+// the north-ghost map, i.e. plane nz, already in the ring).
 constexpr int kUpRJ = 2, kUpRing = 7, kUpZ = 32;
 
+// The fields upsol reads and writes.
 template <class T>
+struct UpsolArgs {
+  const T *dq1, *dq2, *dq3;
+  double *q1, *q2, *q3;
+  double adt;
+};
+
+template <class T, bool UPSOL>
 __global__ void __launch_bounds__(256, 2)
     k_uppres_march(const __grid_constant__ CUtensorMap tdph, Geo g, double be, T *__restrict__ prg,
-                   T *__restrict__ pres, double *__restrict__ dphw, int zs, unsigned *status) {
+                   T *__restrict__ pres, double *__restrict__ dphw, int zs, unsigned *status, UpsolArgs<T> us) {
   extern __shared__ __align__(128) double sm[];
   const int N = g.nth;
   constexpr int RR = kUpRJ + 3;  // rows j0-2 .. j0+kUpRJ
@@ -306,14 +322,43 @@ __global__ void __launch_bounds__(256, 2)
   // prefetched in the storage type: a conversion right after the load
   // would wait for it
   T pp1 = T(0), pp2 = T(0), pp3 = T(0), pps = T(0);
+  T pd1 = T(0), pd2 = T(0), pd3 = T(0);
   auto prefetch = [&](int kc) {
     if (!act) return;
-    pp1 = prg[IPRG(g, i + 1, jc, kc, 1)];
-    pp2 = jc >= 2 ? prg[IPRG(g, i + 1, jc, kc, 2)] : T(0);
-    pp3 = kc >= 2 ? prg[IPRG(g, i + 1, jc, kc, 3)] : T(0);
-    pps = pres[I3(g, i + 1, jc, kc)];
+    if (kc <= g.nz) {
+      pp1 = prg[IPRG(g, i + 1, jc, kc, 1)];
+      pp2 = jc >= 2 ? prg[IPRG(g, i + 1, jc, kc, 2)] : T(0);
+      pp3 = kc >= 2 ? prg[IPRG(g, i + 1, jc, kc, 3)] : T(0);
+      pps = pres[I3(g, i + 1, jc, kc)];
+    }
+    if constexpr (UPSOL) {
+      const int o = I3(g, i + 1, jc, kc);
+      pd1 = __ldg(us.dq1 + o);
+      pd2 = __ldg(us.dq2 + o);
+      pd3 = __ldg(us.dq3 + o);
+    }
   };
   prefetch(kb);
+  // upsol of cell (i, jc) on plane kc from its dq and the dph planes kc
+  // (Pc, north-ghost mapped) and kc-1 (Pl); rc/rs are the rows jc, jc-1
+  auto upsol_cell = [&](int kc, double d1, double d2, double d3, const double *Pc, const double *Pl, int rc,
+                        int rs) {
+    const int o = I3(g, i + 1, jc, kc);
+    const double v1 = d1 - (us.adt * g.dx1 * m.irmc) * (Pc[rc + i] - Pc[rc + im]);
+    us.q1[o] = v1;
+    if (jc == g.nr) us.q1[o + g.nth] = g.slip * v1;
+    us.q2[o] = jc == 1 ? 0.0 : d2 - us.adt * m.rcc * g.dx2 * (Pc[rc + i] - Pc[rs + i]);
+    if (jc == g.nr) us.q2[o + g.nth] = 0.0;
+    if (kc == 1) {
+      us.q3[o] = d3;  // imposed south value, rows 0 .. nrc
+      if (jc == 1) us.q3[o - g.nth] = (double)__ldg(us.dq3 + o - g.nth);
+      if (jc == g.nr) us.q3[o + g.nth] = (double)__ldg(us.dq3 + o + g.nth);
+    } else {
+      const double v3 = d3 - us.adt * g.dx3 * (Pc[rc + i] - Pl[rc + i]);
+      us.q3[o] = v3;
+      if (jc == g.nr) us.q3[o + g.nth] = g.slip * v3;
+    }
+  };
   __syncthreads();
 
   bool failed = false;
@@ -326,7 +371,8 @@ __global__ void __launch_bounds__(256, 2)
     if (kc == kb) ok = mbar_wait(&full[0], 0u) && mbar_wait(&full[1], 0u) && mbar_wait(&full[2 % kUpRing], 0u);
     ok = ok && mbar_wait(&full[(pr + 1) % kUpRing], (unsigned)((pr + 1) / kUpRing) & 1u);
     const T o1 = pp1, o2 = pp2, o3 = pp3, os = pps;
-    if (kc + 1 < ke) prefetch(kc + 1);
+    const T e1 = pd1, e2 = pd2, e3 = pd3;
+    if (kc + 1 < ke || (UPSOL && kc + 1 == g.nzc)) prefetch(kc + 1);
     if (act) {
       const double *Pll = sm + (size_t)((pr - 2) % kUpRing) * SLOT;
       const double *Pl = sm + (size_t)((pr - 1) % kUpRing) * SLOT;
@@ -347,6 +393,7 @@ __global__ void __launch_bounds__(256, 2)
       if (kc >= 2) prg[IPRG(g, i + 1, jc, kc, 3)] = (T)n3;
       pres[I3(g, i + 1, jc, kc)] = (T)np;
       if (kc == g.nz) dphw[IDP(g, i + 1, jc, g.nzc)] = S.d_c;
+      if constexpr (UPSOL) upsol_cell(kc, (double)e1, (double)e2, (double)e3, Pc, Pl, rc, rs);
     }
     // plane kc-2 has been read by all; a failed wait ends the walk
     if (__syncthreads_or(!ok)) {
@@ -363,10 +410,20 @@ __global__ void __launch_bounds__(256, 2)
     const int hi = min(last_pr + kUpRing - 2, nplanes - 1);
     for (int p = last_pr + 1; p <= hi; p++) (void)mbar_wait(&full[p % kUpRing], (unsigned)(p / kUpRing) & 1u);
   }
+  if constexpr (UPSOL) {
+    // the north ghost plane nzc: dph there is plane nz (the slot of the last
+    // step's plane kc+1), and plane nzc-1 = nz is that step's plane kc
+    if (!failed && act && ke == g.nz + 1) {
+      const int pr = g.nz - kb + 2;
+      const double *Pn = sm + (size_t)((pr + 1) % kUpRing) * SLOT;
+      const double *Pz = sm + (size_t)(pr % kUpRing) * SLOT;
+      upsol_cell(g.nzc, (double)pd1, (double)pd2, (double)pd3, Pn, Pz, rc, rs);
+    }
+  }
 }
 
-template <class T>
-static cudaError_t run_uppres_march(vr_ctx *c, double be) {
+template <class T, bool UPSOL>
+static cudaError_t run_uppres_march(vr_ctx *c, double be, double adt) {
   const Geo &g = c->geo;
   if ((g.nth & 1) || kUpRJ * g.nth > 256) return cudaErrorNotSupported;
   CUtensorMap tm;
@@ -374,13 +431,15 @@ static cudaError_t run_uppres_march(vr_ctx *c, double be) {
     return cudaErrorNotSupported;
   const int SLOT = ((kUpRJ + 3) * g.nth + 15) & ~15;
   const size_t sm = sizeof(double) * (size_t)kUpRing * SLOT;
-  auto kern = k_uppres_march<T>;
+  auto kern = k_uppres_march<T, UPSOL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   const int zs = kUpZ;
   const int grid = ((g.nr + kUpRJ - 1) / kUpRJ) * ((g.nz + zs - 1) / zs);
+  UpsolArgs<T> us{reinterpret_cast<const T *>(c->dq[0]), reinterpret_cast<const T *>(c->dq[1]),
+                  reinterpret_cast<const T *>(c->dq[2]), c->q[0], c->q[1], c->q[2], adt};
   kern<<<grid, 256, sm, c->stream>>>(tm, g, be, reinterpret_cast<T *>(c->prg), reinterpret_cast<T *>(c->pres),
-                                      c->dph, zs, c->d_status);
+                                      c->dph, zs, c->d_status, us);
   return cudaGetLastError();
 }
 
@@ -389,7 +448,8 @@ cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   dim3 b(32, 4), gr((g.nth + 31) / 32, (g.nr + 3) / 4, g.nz);
   double be = 0.5 * (rk.alm * g.dt) / g.re;
   LaunchScope ls(c, PK_UPPRES);
-  const cudaError_t me = c->mixed ? run_uppres_march<float>(c, be) : run_uppres_march<double>(c, be);
+  const cudaError_t me =
+      c->mixed ? run_uppres_march<float, false>(c, be, 0.0) : run_uppres_march<double, false>(c, be, 0.0);
   if (me != cudaErrorNotSupported) return me;
   if (c->mixed)
     k_uppres_r<float><<<gr, b, 0, c->stream>>>(g, be, c->dph, reinterpret_cast<float *>(c->prg),
@@ -397,6 +457,22 @@ cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
   else
     k_uppres_r<double><<<gr, b, 0, c->stream>>>(g, be, c->dph, c->prg, c->pres, c->dph);
   return cudaGetLastError();
+}
+
+// upsol then uppres of one substep: one z-marching pass when it applies
+// (counted as uppres by the per-kernel timing), else the two kernels
+cudaError_t launch_upsol_uppres(vr_ctx *c, const Rk &rk) {
+  const Geo &g = c->geo;
+  const double be = 0.5 * (rk.alm * g.dt) / g.re, adt = rk.alm * g.dt;
+  cudaError_t me;
+  {
+    LaunchScope ls(c, PK_UPPRES);
+    me = c->mixed ? run_uppres_march<float, true>(c, be, adt) : run_uppres_march<double, true>(c, be, adt);
+  }
+  if (me != cudaErrorNotSupported) return me;
+  cudaError_t e = launch_upsol(c, rk);
+  if (e) return e;
+  return launch_uppres(c, rk);
 }
 
 // ---------------------------------------------------------------------------
