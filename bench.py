@@ -49,6 +49,18 @@ WORDS = {"rhs": 15, "tsweep": 6, "rsweep": 7, "zsweep": 8, "divq": 4, "fft": 4, 
 WORDS_PER_CELL_STEP = 3 * sum(WORDS.values())  # 198 words = 1584 B
 
 
+def family_words(fam, prof):
+    """Algorithmic words per cell and substep of a timed kernel family, with the
+    phases fused into it: the fused right-hand side also solves the theta
+    lines (tsweep), the fused pressure update also runs upsol."""
+    w = WORDS[fam]
+    if fam == "rhs" and "tsweep" not in prof:
+        w += WORDS["tsweep"]
+    if fam == "uppres" and "upsol" not in prof:
+        w += WORDS["upsol"]
+    return w
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -337,7 +349,7 @@ def main():
     fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
     tot_ms, nl = prof[fam]
     per_sub = nl / (3 * args.steps)  # launches of this family per substep
-    bytes_per_launch = WORDS[fam] / per_sub * ncell * 8
+    bytes_per_launch = family_words(fam, prof) / per_sub * ncell * 8
     achieved = bytes_per_launch / (tot_ms / nl / 1e3) / 1e9
     traffic = traffic_table().get(fam)
     step_ideal_ms = WORDS_PER_CELL_STEP * 8 * ncell / (peak * 1e9) * 1e3
