@@ -164,8 +164,22 @@ VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
 /* ---- diagnostics --------------------------------------------------------- */
 /* max over cells of |div q| in FP64 (the divq stencil without 1/(alpha dt)) */
 VR_API int vr_max_divergence(vr_ctx *ctx, double *out);
-/* number of non-finite values in q1..q3 and pres; VR_ERR_NONFINITE if any */
+/* number of non-finite values in q1..q3 and pres; VR_ERR_NONFINITE if any.
+ * Also reads the context's device status word: VR_ERR_TIMEOUT when a
+ * pipelined kernel's bounded wait for its tile loads gave up since the last
+ * vr_clear_status (its results are then not valid), VR_ERR_CUDA when one
+ * found its shared tile buffer misaligned and did not run.  No reference
+ * counterpart: the reference stops on NaN only (divergence.F90:396-399). */
 VR_API int vr_check_finite(vr_ctx *ctx, int64_t *count);
+/* clears the device status word read by vr_check_finite */
+VR_API int vr_clear_status(vr_ctx *ctx);
+/* Exercises the bounded-wait path without a fault: one CTA waits on an
+ * mbarrier that nothing completes, gives up after limit_ns nanoseconds
+ * (1e3 .. 1e9), records the timeout in the status word and returns; the
+ * context stays usable.  Returns VR_ERR_TIMEOUT when the wait ran out as
+ * designed (and leaves the status set for vr_check_finite).  No reference
+ * counterpart. */
+VR_API int vr_wait_selftest(vr_ctx *ctx, int64_t limit_ns);
 /* kernels launched by this context so far */
 VR_API int vr_launch_count(const vr_ctx *ctx, int64_t *n);
 /* per-kernel-family event timing on the context's stream: vr_profile(ctx, 1)

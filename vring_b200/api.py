@@ -82,6 +82,8 @@ def lib():
         L.vr_iterate.argtypes = [vp, i32]
         L.vr_max_divergence.argtypes = [vp, C.POINTER(dp)]
         L.vr_check_finite.argtypes = [vp, C.POINTER(i64)]
+        L.vr_clear_status.argtypes = [vp]
+        L.vr_wait_selftest.argtypes = [vp, i64]
         L.vr_set_stream.argtypes = [vp, vp]
         L.vr_get_stream.argtypes = [vp, C.POINTER(vp)]
         L.vr_launch_count.argtypes = [vp, C.POINTER(i64)]
@@ -261,6 +263,15 @@ class Run:
         v = C.c_double()
         self._chk(lib().vr_max_divergence(self._h, C.byref(v)), "max_divergence")
         return v.value
+
+    def clear_status(self):
+        """Clear the device status word (bounded-wait timeouts) of the context."""
+        self._chk(lib().vr_clear_status(self._h), "clear_status")
+
+    def wait_selftest(self, limit_ns: int = 10_000_000) -> int:
+        """Run a kernel whose bounded wait must run out; returns the status code
+        (VR_ERR_TIMEOUT = 5 when the wait gave up as designed)."""
+        return lib().vr_wait_selftest(self._h, int(limit_ns))
 
     def count_nonfinite(self) -> int:
         n = C.c_int64()
