@@ -509,6 +509,63 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
   }
 }
 
+// 512-point forward DFT of one complex sequence by a warp, N = 16 x 32:
+// lane t holds z[t + 32 m] (m = 0..15) in re/im; a 16-point DFT over m in
+// registers, the twiddles W_512^{t k1}, a transpose through the warp's own
+// two tile columns (row(k) = the padded row of the caller's tile; with
+// rows k = t + 32 k1 both the write and the transposed read fall on
+// distinct banks), then for k1 = lane / 2 the 32-point DFT over t split
+// into even (lane even) and odd (lane odd) samples, each a 16-point DFT in
+// registers, combined by one exchange with the partner lane.  On return
+// re/im[q] = X[k1 + 16 (16 h + brev4(q))], h = lane & 1.  The tile columns
+// must no longer be needed by the caller (their inputs are in registers).
+template <class RowFn>
+__device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], const double *__restrict__ tw,
+                                            double *tile, int ca, int cb, int lane, RowFn row) {
+  constexpr int N = 512;
+  reg_dif<16, N, 0, 16>(re, im, tw);
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < 16; k1++) {
+    const int rg = brev_c(k1, 4);
+    double yr = re[rg], yi = im[rg];
+    if (k1 != 0) {
+      const int p = lane * k1;
+      const double c = __ldg(tw + 2 * p), sn = -__ldg(tw + 2 * p + 1);
+      const double xr = yr * c - yi * sn, xi = yr * sn + yi * c;
+      yr = xr;
+      yi = xi;
+    }
+    tile[row(lane + 32 * k1) + ca] = yr;
+    tile[row(lane + 32 * k1) + cb] = yi;
+  }
+  __syncwarp();
+  const int k1 = lane >> 1, h = lane & 1;
+#pragma unroll
+  for (int u = 0; u < 16; u++) {
+    re[u] = tile[row(2 * u + h + 32 * k1) + ca];
+    im[u] = tile[row(2 * u + h + 32 * k1) + cb];
+  }
+  __syncwarp();
+  reg_dif<16, N, 0, 16>(re, im, tw);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
+#pragma unroll
+  for (int k2 = 0; k2 < 16; k2++) {
+    const int rg = brev_c(k2, 4);
+    double ar = re[rg], ai = im[rg];
+    if (h && k2 != 0) {  // W_32^{k2} O[k2]
+      const int p = 16 * k2;
+      const double c = __ldg(tw + 2 * p), sn = -__ldg(tw + 2 * p + 1);
+      const double wr = ar * c - ai * sn, wi = ar * sn + ai * c;
+      ar = wr;
+      ai = wi;
+    }
+    const double br = __shfl_xor_sync(0xffffffffu, ar, 1), bi = __shfl_xor_sync(0xffffffffu, ai, 1);
+    // h = 0: E + W O (own + partner); h = 1: E - W O (partner - own)
+    re[rg] = h ? br - ar : ar + br;
+    im[rg] = h ? bi - ai : ai + bi;
+  }
+}
+
 // z transforms: a CTA stages LT columns (consecutive theta, fixed r) x nz in
 // shared memory with 128-byte row loads; warp w transforms columns 2w, 2w+1
 // as one complex sequence (Makhoul's even/odd reordering turns the DCT into
@@ -548,12 +605,22 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
       im[q] = tile[row(src) + cb];
     }
     __syncwarp();
-    warp_fft_dif<E>(re, im, twz, lane);
+    if constexpr (E == 16) {
+      warp_fft512(re, im, twz, tile, ca, cb, lane, row);
 #pragma unroll
-    for (int q = 0; q < E; q++) {
-      int k = brev_n(lane + 32 * q, LOGN);
-      tile[row(k) + ca] = re[q];
-      tile[row(k) + cb] = im[q];
+      for (int q = 0; q < 16; q++) {
+        const int k = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
+        tile[row(k) + ca] = re[q];
+        tile[row(k) + cb] = im[q];
+      }
+    } else {
+      warp_fft_dif<E>(re, im, twz, lane);
+#pragma unroll
+      for (int q = 0; q < E; q++) {
+        int k = brev_n(lane + 32 * q, LOGN);
+        tile[row(k) + ca] = re[q];
+        tile[row(k) + cb] = im[q];
+      }
     }
     __syncwarp();
     // y_k = 2 Re(e^{-i pi k/(2N)} V_k) / (2N)
@@ -589,14 +656,27 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
       im[q] = -(vai + vbr);   // -Im W (inverse as conj(DFT(conj W)))
     }
     __syncwarp();
-    warp_fft_dif<E>(re, im, twz, lane);
-    // slot of point n holds conj(w_m), m = brev(n); w_m = v^a_m + i v^b_m
+    if constexpr (E == 16) {
+      // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
+      warp_fft512(re, im, twz, tile, ca, cb, lane, row);
+      __syncwarp();
 #pragma unroll
-    for (int q = 0; q < E; q++) {
-      int m = brev_n(lane + 32 * q, LOGN);
-      int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
-      tile[row(o) + ca] = 2.0 * re[q];
-      tile[row(o) + cb] = -2.0 * im[q];
+      for (int q = 0; q < 16; q++) {
+        const int m = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
+        const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+        tile[row(o) + ca] = 2.0 * re[q];
+        tile[row(o) + cb] = -2.0 * im[q];
+      }
+    } else {
+      warp_fft_dif<E>(re, im, twz, lane);
+      // slot of point n holds conj(w_m), m = brev(n); w_m = v^a_m + i v^b_m
+#pragma unroll
+      for (int q = 0; q < E; q++) {
+        int m = brev_n(lane + 32 * q, LOGN);
+        int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+        tile[row(o) + ca] = 2.0 * re[q];
+        tile[row(o) + cb] = -2.0 * im[q];
+      }
     }
   }
   __syncthreads();
