@@ -673,6 +673,10 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
   const double A = rt[0];
   const int inner = N - 1;
   const int i0 = gl * EG;
+  // EG divides 16 and i0 is a multiple of EG, so the padded index of i0 + e
+  // is tpad(i0) + e for every e < EG
+  static_assert(16 % EG == 0, "chunk length must divide the padding period");
+  const int b0 = tpad(i0);
   int cnt = on ? inner - i0 : 0;
   cnt = cnt < 0 ? 0 : (cnt > EG ? EG : cnt);
   double y[EG];
@@ -681,7 +685,7 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
   for (int e = 0; e < EG; e++) {
     y[e] = 0.0;
     if (e < cnt) {
-      const int i = tpad(i0 + e);
+      const int i = b0 + e;
       const double fi = sl[i], iv = cinv[i];
       y[e] = fi;
       acc.C = (fi - A * acc.C) * iv;
@@ -698,7 +702,7 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
 #pragma unroll
   for (int e = 0; e < EG; e++) {
     if (e < cnt) {
-      yin = (y[e] - A * yin) * cinv[tpad(i0 + e)];
+      yin = (y[e] - A * yin) * cinv[b0 + e];
       y[e] = yin;
     }
   }
@@ -706,7 +710,7 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
 #pragma unroll
   for (int e = EG - 1; e >= 0; e--) {
     if (e < cnt) {
-      const double pv = cpp[tpad(i0 + e)];
+      const double pv = cpp[b0 + e];
       acc.C = y[e] - pv * acc.C;
       acc.M = -pv * acc.M;
     }
@@ -721,7 +725,7 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
 #pragma unroll
   for (int e = EG - 1; e >= 0; e--) {
     if (e < cnt) {
-      win = y[e] - cpp[tpad(i0 + e)] * win;
+      win = y[e] - cpp[b0 + e] * win;
       y[e] = win;
     }
   }
@@ -738,7 +742,7 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
     const double xN = (fN - rt[1] * w1 - A * wl) / rt[2];
 #pragma unroll
     for (int e = 0; e < EG; e++)
-      if (e < cnt) sl[tpad(i0 + e)] = y[e] + czz[tpad(i0 + e)] * xN;
+      if (e < cnt) sl[b0 + e] = y[e] + czz[b0 + e] * xN;
     if (gl == 0) sl[tpad(N - 1)] = xN;
   }
 }
