@@ -1525,9 +1525,10 @@ void orc_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const
  * Elementary Functions", 1980): |x| <= 1/2 uses pi/2 - asin(x); |x| > 1/2
  * uses asin(sqrt((1-|x|)/2)).  asin(s), s <= 1/2, is the Maclaurin series
  * sum_n (2n)!/(4^n (n!)^2 (2n+1)) s^(2n+1) truncated after 28 terms (the
- * remainder is below 2^-56 relative).  The same operation sequence (no FMA)
- * runs in the CUDA particle kernel, so theta -- and the cell index derived
- * from it -- is bit-identical on both sides. */
+ * remainder is below 2^-56 relative), evaluated by Horner's scheme with
+ * fused multiply-adds (C99 fma, correctly rounded).  The same operation
+ * sequence runs in the CUDA particle kernel, so theta -- and the cell index
+ * derived from it -- is bit-identical on both sides. */
 static const double ORC_ASIN_C[28] = {
     0.16666666666666666,   0.075,                 0.044642857142857144,  0.030381944444444444,
     0.022372159090909092,  0.017352764423076924,  0.01396484375,         0.011551800896139705,
@@ -1539,7 +1540,7 @@ static const double ORC_ASIN_C[28] = {
 static double vr_asin_small(double s) {
   double t = s * s;
   double p = ORC_ASIN_C[27];
-  for (int n = 26; n >= 0; n--) p = p * t + ORC_ASIN_C[n];
+  for (int n = 26; n >= 0; n--) p = fma(p, t, ORC_ASIN_C[n]);
   return s + s * (t * p);
 }
 double orc_vr_acos(double x) {

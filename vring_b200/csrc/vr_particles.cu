@@ -82,7 +82,7 @@ __device__ __forceinline__ double asin_small(double s) {
   double t = __dmul_rn(s, s);
   double p = kAsinC[27];
 #pragma unroll
-  for (int n = 26; n >= 0; n--) p = __dadd_rn(__dmul_rn(p, t), kAsinC[n]);
+  for (int n = 26; n >= 0; n--) p = __fma_rn(p, t, kAsinC[n]);  // Horner with fused multiply-adds
   return __dadd_rn(s, __dmul_rn(s, __dmul_rn(t, p)));
 }
 
