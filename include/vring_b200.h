@@ -55,7 +55,7 @@ enum vr_status {
  * arrays, the Poisson right-hand side, transforms and dph stay double,
  * so the projected velocity keeps max|div u| at round-off.  Runs through
  * vr_substep/vr_iterate only (the per-routine entry points return
- * VR_ERR_STATE), for ntheta <= 257 and nr, nz <= 543. */
+ * VR_ERR_STATE), for ntheta <= 257. */
 enum vr_precision { VR_FP64 = 0, VR_MIXED = 1 };
 enum vr_theta_wavenumber {
   VR_WTH_EXACT = 0,    /* m^2, the reference's 'wvnex' (poisson_solve.F90:287)   */

@@ -9,8 +9,8 @@
 - the lines longer than the register-resident sweeps and transforms take
   (Ntheta 256, Nz 1024), against the oracle;
 - the head-on collision of two opposite rings at 512 x 256 x 1024 (about
-  134 M cells), run at full size in FP64: the projected velocity stays
-  divergence-free and finite.
+  134 M cells), run at full size in both precision forms: the projected
+  velocity stays divergence-free and finite.
 
 The reference's z boundaries (wall/inflow and convective outflow) replace the
 periodic z of the collision and single-ring descriptions, as everywhere in
@@ -133,11 +133,13 @@ def test_long_theta_and_z_lines_match_oracle():
 
 
 @pytest.mark.gpu
-def test_head_on_collision_512x256x1024_full_size():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_head_on_collision_512x256x1024_full_size(precision):
     import vring_b200 as V
     from vring_b200.synthetic import annulus_particles, ring_fields
     nth, nr, nz = 256, 512, 1024
-    run = V.Run(nth, nr, nz, 4.0, 16.0, 2.5e-4, 5000.0, 1.0, 1.0, theta_wavenumber="modified")
+    run = V.Run(nth, nr, nz, 4.0, 16.0, 2.5e-4, 5000.0, 1.0, 1.0, precision=precision,
+                theta_wavenumber="modified")
     q = ring_fields(nth, nr, nz, 4.0, 16.0, noise=1e-3, seed=3,
                     rings=[(1.0, 0.15, 1.0, 5.0), (1.0, 0.15, -1.0, 11.0)])
     for n, a in zip(("q1", "q2", "q3"), q):

@@ -288,9 +288,9 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
     return VR_ERR_DESC;
   if (!(d.rmax > 0) || !(d.zmax > 0) || !(d.dt > 0) || !(d.re > 0) || !(d.pe > 0)) return VR_ERR_DESC;
   if (d.precision != VR_FP64 && d.precision != VR_MIXED) return VR_ERR_DESC;
-  // the mixed form runs the fused substep only: theta lines up to 257 cells
-  // (fused theta sweep) and r/z lines up to 544 unknowns (register sweep)
-  if (d.precision == VR_MIXED && (d.ntheta > 257 || d.nr > 543 || d.nz > 543)) return VR_ERR_DESC;
+  // the mixed form runs the fused substep only, whose float right-hand side
+  // keeps theta lines of up to 257 cells in shared memory
+  if (d.precision == VR_MIXED && d.ntheta > 257) return VR_ERR_DESC;
   if (d.theta_wavenumber != VR_WTH_EXACT && d.theta_wavenumber != VR_WTH_MODIFIED) return VR_ERR_DESC;
   if (d.inflow != VR_INFLOW_OFF && d.inflow != VR_INFLOW_REFERENCE) return VR_ERR_DESC;
   int64_t cells = (int64_t)d.ntheta * (d.nr + 3) * (d.nz + 3);

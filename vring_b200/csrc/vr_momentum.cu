@@ -1107,8 +1107,8 @@ struct SweepArgsT {
 };
 using SweepArgs = SweepArgsT<double>;
 
-template <int LT, int CH>
-__global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgs s, CoefShared cf) {
+template <int LT, int CH, class T = double>
+__global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgsT<T> s, CoefShared cf) {
   extern __shared__ double smem[];
   const int LD = LT + 1;
   double *tile = smem;
@@ -1141,27 +1141,27 @@ __global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgs s, CoefShared cf
     int o = (i0 + l) + s.s2 * m2 + s.se * (s.e0 + e);
     double x = tile[e * LD + l];
     double v = s.add ? s.add[o] + x : x;
-    s.out[o] = v;
+    s.out[o] = (T)v;
     if (s.mode == 1 && m2 == s.nr)  // dq(ic, nrc, kc) = slip * dq(ic, nr, kc)
-      s.out[o + s.nth] = s.slip * v;
+      s.out[o + s.nth] = (T)(s.slip * v);
     if (s.mode == 2) {
       if (e == 0)  // dq2(ic, 1, kc) = stri(1) + q2(ic, 1, kc) with stri(1) = 0
-        s.out[o - s.se] = s.add[o - s.se] + 0.0;
+        s.out[o - s.se] = (T)(s.add[o - s.se] + 0.0);
       if (e == s.n - 1)  // dq2(ic, nrc, kc) = 0.0*slip*dq2(ic, nr, kc)
-        s.out[o + s.se] = 0.0 * s.slip * v;
+        s.out[o + s.se] = (T)(0.0 * s.slip * v);
     }
   }
 }
 
-template <int LT, int CH>
-static cudaError_t run_linesweep(vr_ctx *c, const SweepArgs &s, const CoefShared &cf, int nm2) {
+template <int LT, int CH, class T = double>
+static cudaError_t run_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const CoefShared &cf, int nm2) {
   size_t sm = sizeof(double) * ((size_t)s.n * (LT + 1) + 2 * LT * CH);
-  cudaError_t e = cudaFuncSetAttribute(k_linesweep<LT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_linesweep<LT, CH, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm);
   if (e) return e;
   dim3 gr((s.nth + LT - 1) / LT, nm2);
   LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);
-  k_linesweep<LT, CH><<<gr, LT * CH, sm, c->stream>>>(s, cf);
+  k_linesweep<LT, CH, T><<<gr, LT * CH, sm, c->stream>>>(s, cf);
   return cudaGetLastError();
 }
 
@@ -1268,13 +1268,9 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const C
     if (e != cudaErrorNotSupported) return e;
     return launch_chunk(p, p.nbx * nm2, c->stream);
   }
-  if constexpr (std::is_same<T, double>::value) {
-    if (s.n <= 640) return run_linesweep<16, 16>(c, s, cf, nm2);
-    if (s.n <= 1600) return run_linesweep<8, 32>(c, s, cf, nm2);
-    return run_linesweep<4, 64>(c, s, cf, nm2);
-  } else {
-    return cudaErrorNotSupported;  // the mixed form runs lines of at most 544 unknowns
-  }
+  if (s.n <= 640) return run_linesweep<16, 16, T>(c, s, cf, nm2);
+  if (s.n <= 1600) return run_linesweep<8, 32, T>(c, s, cf, nm2);
+  return run_linesweep<4, 64, T>(c, s, cf, nm2);
 }
 
 // solqj (step.F90:266-358): lines (ic, kc) along j.
