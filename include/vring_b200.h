@@ -160,6 +160,11 @@ VR_API int vr_substep(vr_ctx *ctx, int32_t irk);
  * kernels enqueued on the context's stream; particle classes attached with
  * vr_part_attach advance before substep 1 (loop.F90:65-68). */
 VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
+/* vr_substep/vr_iterate replay each RK substep's kernels as a CUDA graph
+ * captured on first use (on by default; bypassed while vr_profile is on or
+ * the inflow is on, whose boundary values change every step).  on = 0 issues
+ * the kernels one by one.  No reference counterpart. */
+VR_API int vr_set_graphs(vr_ctx *ctx, int32_t on);
 
 /* ---- diagnostics --------------------------------------------------------- */
 /* max over cells of |div q| in FP64 (the divq stencil without 1/(alpha dt)) */

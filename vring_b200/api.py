@@ -79,6 +79,7 @@ def lib():
                   "laplace_solve", "upsol", "uppres"):
             getattr(L, "vr_" + n).argtypes = [vp]
         L.vr_substep.argtypes = [vp, i32]
+        L.vr_set_graphs.argtypes = [vp, i32]
         L.vr_iterate.argtypes = [vp, i32]
         L.vr_max_divergence.argtypes = [vp, C.POINTER(dp)]
         L.vr_check_finite.argtypes = [vp, C.POINTER(i64)]
@@ -263,6 +264,10 @@ class Run:
         v = C.c_double()
         self._chk(lib().vr_max_divergence(self._h, C.byref(v)), "max_divergence")
         return v.value
+
+    def set_graphs(self, on: bool):
+        """Replay each substep as a captured CUDA graph (default) or launch one by one."""
+        self._chk(lib().vr_set_graphs(self._h, 1 if on else 0), "set_graphs")
 
     def clear_status(self):
         """Clear the device status word (bounded-wait timeouts) of the context."""

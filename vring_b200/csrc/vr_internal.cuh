@@ -131,9 +131,12 @@ struct vr_ctx {
   // device status word: bit 0 set by a kernel whose bounded wait gave up,
   // bit 1 by a pipelined sweep whose shared tile buffer was misaligned
   unsigned *d_status;
-  // CUDA graphs for the fused substeps (one per irk), built lazily
+  // CUDA graphs of the fused substeps (one per irk), captured on first use
+  // when use_graphs is set; graph_launches counts the kernels of each
   cudaGraphExec_t graph[4];
   bool graph_ok[4];
+  int64_t graph_launches[4];
+  bool use_graphs;
   cudaStream_t own_stream;  // the context's stream; `stream` may be a caller's
   // launch accounting and optional per-kernel event timing
   int64_t nlaunch;
