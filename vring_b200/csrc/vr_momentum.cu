@@ -658,7 +658,7 @@ static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a)
 // so the CTA pays one solve phase per kTB planes and the short group scans
 // keep the instruction count per unknown low.
 // ---------------------------------------------------------------------------
-constexpr int kMRJ = 2, kQRing = 5, kMarchZ = 32, kTB = 4;
+constexpr int kMRJ = 2, kQRing = 4, kMarchZ = 32, kTB = 4;
 
 // Periodic theta solve of one line by a group of kTL consecutive lanes of a
 // warp (the arithmetic of tsolve_warp; lane g of the group owns the EG
