@@ -290,7 +290,7 @@ template <class R>
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
                                                double y, double z, R (*cv)[kPartPerBlock], int p,
                                                int (&cell)[3], double &r, double &theta, double &sn,
-                                               double &cs) {
+                                               double &cs, double &ir1o, double &ir2o) {
   constexpr bool DBL = std::is_same<R, double>::value;
   int it, ir, iz;
   part_cell(P, x, y, z, it, ir, iz, r, theta);
@@ -393,10 +393,17 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   const R fz = a[2] + rp * a[6] + two * zp * a[7] + tp * a[8];
   const R ftt = two * a[3], ftr = rp * a[4], ftz = zp * a[8], frt = a[4], frr = two * a[5];
   const R frz = a[6], fzt = a[8], fzr = a[6], fzz = two * a[7];
-  sincos(theta, &sn, &cs);
+  // sin and cos of theta from the coordinates: theta is the arccosine of
+  // x / r (of -x / r, plus pi, below the x axis), so cos theta = x / r and
+  // sin theta = y / r up to rounding (about 1e-16), without a sincos
+  const double ir1d = 1.0 / r, ir2d = 1.0 / (r * r);
+  cs = x * ir1d;
+  sn = y * ir1d;
+  ir1o = ir1d;
+  ir2o = ir2d;
   const R s_ = (R)sn, c_ = (R)cs;
   const R sn2 = two * s_ * c_, cs2 = (c_ - s_) * (c_ + s_);  // sin 2theta, cos 2theta
-  const R ir1 = (R)(1.0 / r), ir2 = (R)(1.0 / (r * r));
+  const R ir1 = (R)ir1d, ir2 = (R)ir2d;
   const R m_snr = -s_ * ir1, m_csr = c_ * ir1;
   const R m30 = sn2 * ir2, m31 = s_ * s_ * ir1, m33 = s_ * s_ * ir2, m34 = -c_ * s_ * ir1, m37 = c_ * c_;
   const R m40 = -cs2 * ir2, m43 = -c_ * s_ * ir2, m44 = -s_ * s_ * ir1, m46 = c_ * c_ * ir1, m47 = c_ * s_;
@@ -422,11 +429,14 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
 // fitted components (part_tools.F90:730-797), in the reference's summation
 // order over components.
 template <class R>
-__device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d, int id,
+__device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d, double ir1d, double ir2d, int id,
                                               const R (*cv)[kPartPerBlock], int p, R &vel, R (&dvel)[3],
                                               R (&ddvel)[3][3]) {
+  // 1/rsd and 1/rsd^2 with rsd = max(r, 1e-6): the component fit's 1/r and
+  // 1/r^2 (the same divisions) except next to the axis
   const double rsd = r > (double)0.000001f ? r : (double)0.000001f;
-  const R irs = (R)(1.0 / rsd), irs2 = (R)(1.0 / (rsd * rsd));
+  const R irs = (R)(r > (double)0.000001f ? ir1d : 1.0 / rsd);
+  const R irs2 = (R)(r > (double)0.000001f ? ir2d : 1.0 / (rsd * rsd));
   const R sn = (R)sn_d, cs = (R)cs_d, two = 2, three = 3;
   const R A1 = sn * (-two * (cs * cs) + sn * sn) * irs2, A2 = -three * cs * (sn * sn) * irs2;
   const R A3 = cs * (cs * cs - two * (sn * sn)) * irs2, A4 = three * (cs * cs) * sn * irs2;
@@ -512,11 +522,12 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ip = 1 + blockIdx.x * kPartPerBlock + p;
   const bool live = ip <= nlast && isfre[ip - 1] == 0;
-  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0;
+  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
   if (live) {
     const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
     int cell[3];
-    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs);
+    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs, ir1,
+                      ir2);
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -528,7 +539,7 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
   double pw = 0.0;
   if (live) {
     R vr_, dvr[3], ddvr[3][3];
-    part_cart_row<R>(r, sn, cs, w, S.cv, p, vr_, dvr, ddvr);
+    part_cart_row<R>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
     const double vel = vr_;
     double dvel[3], ddvel[3][3];
 #pragma unroll
@@ -613,18 +624,18 @@ __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__re
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * kPartPerBlock + p;
   const bool act = i < n;
-  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0;
+  double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
   if (act) {
     const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
     int cell[3];
-    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs);
+    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs, ir1, ir2);
     if (w == 0)
       for (int a = 0; a < 3; a++) cells[3 * (size_t)i + a] = cell[a];
   }
   __syncthreads();
   if (!act) return;
   R vel, dvel[3], ddvel[3][3];
-  part_cart_row<R>(r, sn, cs, w, cv, p, vel, dvel, ddvel);
+  part_cart_row<R>(r, sn, cs, ir1, ir2, w, cv, p, vel, dvel, ddvel);
   double *o = out + 39 * (size_t)i;
   o[w] = vel;
   for (int b = 0; b < 3; b++) o[3 + w + 3 * b] = dvel[b];
