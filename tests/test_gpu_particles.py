@@ -139,6 +139,34 @@ def test_iter_part_matches_oracle(pid, mode):
     gp.close()
 
 
+@pytest.mark.parametrize("scale,mode", [(3e4, 1), (1e8, 0), (1e8, 1)])
+def test_iter_part_full_iteration_matches_oracle(scale, mode):
+    # Velocities scaled until the stencil differences pass the bound below
+    # which the fit's second pass is rounding noise: the reference then runs
+    # its Richardson iteration for several passes (up to 100).  At 3e4 part of
+    # the particles cross the bound, at 1e8 all of them: the main launch
+    # defers them and the full-iteration launch advances them.
+    from oracle import oracle as O
+    import vring_b200 as V
+    nth, nr, nz = 16, 32, 64
+    orc, gpu = make_pair(nth, nr, nz, dt=1e-2 / scale)
+    from vring_b200.synthetic import ring_fields
+    for n, a in zip(("q1", "q2", "q3"), ring_fields(nth, nr, nz, 4.0, 12.0, noise=1e-3, seed=6)):
+        orc.field(n)[...] = scale * a
+        gpu.set(n, scale * a)
+    op = O.OraclePart(orc, 6, 700, mode)
+    gp = V.Part(gpu, 6, 700, mode)
+    _inject_cloud([op, gp], 600, seed=13, out_frac=0.0)
+    u0 = gp.state()[0].copy()
+    for call in range(2):
+        op.iter_part(1)
+        gp.iter_part(1)
+        _compare_parts(op, gp)
+    moved = np.abs(gp.state()[0][:600, 0:3] - u0[:600, 0:3]).max(axis=1)
+    assert (moved > 0).all()  # every particle was advanced
+    gp.close()
+
+
 def test_inject_remove_bookkeeping():
     from oracle import oracle as O
     import vring_b200 as V

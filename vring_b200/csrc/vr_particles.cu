@@ -44,7 +44,8 @@ struct vr_part {
   // device
   double *u, *v;
   int *isfre, *gone;    // gone[ip-1] = substep serial at removal, -1 alive
-  int *d_nremoved;
+  int *d_nremoved;  // [0] removals since the host last read them, [1..2] deferred counts
+  int *d_defer;     // slots deferred to the full least-squares iteration this substep
   // host bookkeeping (part_tools.F90 type part)
   int npart, nlast, nfree, nids;
   std::vector<int> ifree, h_isfre;
@@ -285,13 +286,15 @@ __device__ __noinline__ void ls_more(const PartCoef *__restrict__ Cg, int nth, i
 // and the sample differences are double; with R = float (the mixed form) the
 // fit and the transform run in float and stop after the first pass, which is
 // the exact least-squares solution (the reference's further passes correct
-// rounding, below float resolution).
-template <class R>
+// rounding, below float resolution).  With FULL false the further passes are
+// not taken: need is set instead and the outputs are not to be used.
+template <class R, bool FULL = true>
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
                                                double y, double z, R (*cv)[kPartPerBlock], int p,
                                                int (&cell)[3], double &r, double &theta, double &sn,
-                                               double &cs, double &ir1o, double &ir2o) {
+                                               double &cs, double &ir1o, double &ir2o, bool &need) {
   constexpr bool DBL = std::is_same<R, double>::value;
+  need = false;
   int it, ir, iz;
   part_cell(P, x, y, z, it, ir, iz, r, theta);
   // keep the mesh lookups inside the stored vectors for points off the mesh
@@ -359,7 +362,8 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
     // stop as the reference does (|mp| < 1e-6), or when the second pass is
     // provably a rounding-level change under that tolerance (see ls_fit);
     // NaN/Inf take the full iteration
-    if (!(sqrt(nn) < (double)0.000001f) && !(ym < P.C.ymax_one_pass)) {
+    need = !(sqrt(nn) < (double)0.000001f) && !(ym < P.C.ymax_one_pass);
+    if (FULL && need) {
       double at[9];
 #pragma unroll
       for (int i = 0; i < 9; i++) at[i] = a[i];
@@ -508,26 +512,38 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 
 // One Euler substep of every live particle (part_tools.F90:517-959) and the
 // out-of-range test and removal (:962-987).
+//
+// The FP64 fit stops after its first pass unless the samples are large
+// enough for the reference's second pass to matter (ls_fit); the rare
+// particles that need more passes are not updated by the main launch
+// (FIX false) but listed in defer[], and the launch with FIX true advances
+// exactly those, with the full iteration.  Particles are independent, so the
+// split changes no result; it keeps the full iteration's registers and call
+// out of the main launch.  defer_n[serial & 1] counts this substep's list;
+// the FIX launch clears the other counter for the next substep.
 #ifndef VR_PART_MINB
 #define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
 #endif
-template <class R>
-__global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const double *__restrict__ q1,
-                                                  const double *__restrict__ q2, const double *__restrict__ q3,
-                                                  double *__restrict__ u, double *__restrict__ v,
-                                                  int *__restrict__ isfre, int *__restrict__ gone, int naloc,
-                                                  int nlast, int mode, double inv_st, double partdt, int serial,
-                                                  int *nremoved) {
-  __shared__ PartShared<R> S;
+// Advance the particles in slots ip (1-based; one per lane, the same for
+// the three warps) whose live flag is set.
+template <class R, bool FIX>
+__device__ __forceinline__ void part_advance(const PartGeo &P, const double *__restrict__ q1,
+                                             const double *__restrict__ q2, const double *__restrict__ q3,
+                                             double *__restrict__ u, double *__restrict__ v,
+                                             int *__restrict__ isfre, int *__restrict__ gone, int naloc, int ip,
+                                             bool live, int mode, double inv_st, double partdt, int serial,
+                                             int *nremoved, int *__restrict__ defer, PartShared<R> &S,
+                                             int (&need_s)[3][kPartPerBlock]) {
+  constexpr bool DBL = std::is_same<R, double>::value;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int ip = 1 + blockIdx.x * kPartPerBlock + p;
-  const bool live = ip <= nlast && isfre[ip - 1] == 0;
   double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
   if (live) {
     const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
     int cell[3];
-    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs, ir1,
-                      ir2);
+    bool need;
+    part_component<R, FIX>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs,
+                           ir1, ir2, need);
+    if (DBL && !FIX) need_s[w][p] = need;
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -536,8 +552,16 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
     }
   }
   __syncthreads();
+  bool go = live;
+  if (DBL && !FIX && live && (need_s[0][p] | need_s[1][p] | need_s[2][p])) {
+    go = false;  // left unchanged here, advanced by the FIX launch
+    if (w == 0) {
+      const int k = atomicAdd(nremoved + 1 + (serial & 1), 1);
+      if (k < naloc) defer[k] = ip;
+    }
+  }
   double pw = 0.0;
-  if (live) {
+  if (go) {
     R vr_, dvr[3], ddvr[3][3];
     part_cart_row<R>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
     const double vel = vr_;
@@ -597,19 +621,49 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
     S.pos[w][p] = pw;
   }
   __syncthreads();
-  if (!live) return;
-  // out of the domain: removed (single rank: nothing migrates)
-  const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
-  const double rp = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
-  if ((z > P.zmax) || (z < 0.0) || (rp > P.rmax) || (rp < 0.0)) {
+  if (go) {
+    // out of the domain: removed (single rank: nothing migrates)
+    const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+    const double rp = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
+    if ((z > P.zmax) || (z < 0.0) || (rp > P.rmax) || (rp < 0.0)) {
 #pragma unroll 1
-    for (int iv = 1 + 39 * w; iv <= 39 * (w + 1); iv++) u[PUo(ip, iv)] = 0.0;
-    if (w == 0) {
+      for (int iv = 1 + 39 * w; iv <= 39 * (w + 1); iv++) u[PUo(ip, iv)] = 0.0;
+      if (w == 0) {
 #pragma unroll
-      for (int iv = 0; iv < 3; iv++) v[(size_t)(ip - 1) + (size_t)naloc * iv] = 0.0;
-      isfre[ip - 1] = 1;
-      gone[ip - 1] = serial;
-      atomicAdd(nremoved, 1);
+        for (int iv = 0; iv < 3; iv++) v[(size_t)(ip - 1) + (size_t)naloc * iv] = 0.0;
+        isfre[ip - 1] = 1;
+        gone[ip - 1] = serial;
+        atomicAdd(nremoved, 1);
+      }
+    }
+  }
+}
+
+template <class R, bool FIX>
+__global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const double *__restrict__ q1,
+                                                  const double *__restrict__ q2, const double *__restrict__ q3,
+                                                  double *__restrict__ u, double *__restrict__ v,
+                                                  int *__restrict__ isfre, int *__restrict__ gone, int naloc,
+                                                  int nlast, int mode, double inv_st, double partdt, int serial,
+                                                  int *nremoved, int *__restrict__ defer) {
+  __shared__ PartShared<R> S;
+  __shared__ int need_s[3][kPartPerBlock];
+  const int p = threadIdx.x & 31;
+  if constexpr (!FIX) {
+    const int ip = 1 + blockIdx.x * kPartPerBlock + p;
+    const bool live = ip <= nlast && isfre[ip - 1] == 0;
+    part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st, partdt, serial,
+                           nremoved, defer, S, need_s);
+  } else {
+    int *const defer_n = nremoved + 1;
+    const int nfix = min(*(volatile int *)(defer_n + (serial & 1)), naloc);
+    if (blockIdx.x == 0 && threadIdx.x == 0) defer_n[(serial + 1) & 1] = 0;
+#pragma unroll 1
+    for (int base = blockIdx.x * kPartPerBlock; base < nfix; base += gridDim.x * kPartPerBlock) {
+      const int ip = base + p < nfix ? defer[base + p] : 0;
+      part_advance<R, true>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, ip > 0, mode, inv_st, partdt, serial,
+                            nremoved, defer, S, need_s);
+      __syncthreads();  // S is reused by the next group
     }
   }
 }
@@ -628,7 +682,9 @@ __global__ void __launch_bounds__(96) k_part_probe(PartGeo P, const double *__re
   if (act) {
     const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
     int cell[3];
-    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs, ir1, ir2);
+    bool need;
+    part_component<R>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, x, y, z, cv, p, cell, r, theta, sn, cs, ir1, ir2,
+                      need);
     if (w == 0)
       for (int a = 0; a < 3; a++) cells[3 * (size_t)i + a] = cell[a];
   }
@@ -800,7 +856,8 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
             cudaMalloc(&p->v, nv * sizeof(double)) == cudaSuccess &&
             cudaMalloc(&p->isfre, naloc * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&p->gone, naloc * sizeof(int)) == cudaSuccess &&
-            cudaMalloc(&p->d_nremoved, sizeof(int)) == cudaSuccess;
+            cudaMalloc(&p->d_nremoved, 3 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&p->d_defer, naloc * sizeof(int)) == cudaSuccess;
   if (!ok) {
     vr_part_destroy(p);
     return set_err(c, VR_ERR_OOM, "particle arrays");
@@ -809,7 +866,7 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
   cudaMemset(p->v, 0, nv * sizeof(double));
   cudaMemset(p->isfre, 0, naloc * sizeof(int));
   cudaMemset(p->gone, 0xff, naloc * sizeof(int));
-  cudaMemset(p->d_nremoved, 0, sizeof(int));
+  cudaMemset(p->d_nremoved, 0, 3 * sizeof(int));
   p->ifree.assign(naloc + 2, 0);
   p->h_isfre.assign(naloc + 1, 0);
   p->inflow.assign(c->geo.nr + 2, 0.0);
@@ -833,6 +890,7 @@ extern "C" int vr_part_destroy(vr_part *p) {
   cudaFree(p->isfre);
   cudaFree(p->gone);
   cudaFree(p->d_nremoved);
+  cudaFree(p->d_defer);
   if (p->d_batch) cudaFree(p->d_batch);
   delete p;
   return VR_OK;
@@ -1062,12 +1120,27 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
   double inv_st = 1.0 / p->st;
   for (int s = 0; s < p->nsubdt; s++) {
     if (p->nlast <= 0) break;
-    LaunchScope ls(c, PK_PART, stream);
-    auto kern = c->mixed ? k_iter_part<float> : k_iter_part<double>;
-    kern<<<(p->nlast + kPartPerBlock - 1) / kPartPerBlock, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v,
-                                                              p->isfre, p->gone, p->naloc, p->nlast, p->mode,
-                                                              inv_st, partdt, p->serial++, p->d_nremoved);
+    const int nb = (p->nlast + kPartPerBlock - 1) / kPartPerBlock, serial = p->serial++;
+    {
+      LaunchScope ls(c, PK_PART, stream);
+      if (c->mixed)
+        k_iter_part<float, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
+                                                         p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
+                                                         serial, p->d_nremoved, p->d_defer);
+      else
+        k_iter_part<double, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
+                                                          p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
+                                                          serial, p->d_nremoved, p->d_defer);
+    }
     cudaError_t e = cudaGetLastError();
+    if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
+    if (!c->mixed) {  // the particles the main launch deferred to the full fit
+      LaunchScope ls(c, PK_PART, stream);
+      k_iter_part<double, true><<<std::min(nb, 8 * c->nsm), 96, 0, stream>>>(
+          P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
+          serial, p->d_nremoved, p->d_defer);
+    }
+    e = cudaGetLastError();
     if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
   }
   return VR_OK;
@@ -1242,6 +1315,7 @@ extern "C" int vr_part_restart_load(vr_part *p, const char *path) {
   p->nfree = h.nfree;
   p->nids = h.nids;
   p->serial = h.serial;
+  VR_CUDA(c, cudaMemset(p->d_nremoved + 1, 0, 2 * sizeof(int)));  // the deferred counts follow serial's parity
   p->inflow_on = h.inflow_on != 0;
   p->r0 = h.r0;
   p->rng = h.rng;
