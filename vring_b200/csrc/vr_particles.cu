@@ -362,7 +362,10 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
     // stop as the reference does (|mp| < 1e-6), or when the second pass is
     // provably a rounding-level change under that tolerance (see ls_fit);
     // NaN/Inf take the full iteration
-    need = !(sqrt(nn) < (double)0.000001f) && !(ym < P.C.ymax_one_pass);
+    // (the main launch tests |mp|^2 against a bound just below the square of
+    // the tolerance: the particles in the thin band it adds are deferred, and
+    // the full-iteration launch applies the exact test)
+    need = !(FULL ? sqrt(nn) < (double)0.000001f : nn < 9.9e-13) && !(ym < P.C.ymax_one_pass);
     if (FULL && need) {
       double at[9];
 #pragma unroll
@@ -514,13 +517,14 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 // out-of-range test and removal (:962-987).
 //
 // The FP64 fit stops after its first pass unless the samples are large
-// enough for the reference's second pass to matter (ls_fit); the rare
-// particles that need more passes are not updated by the main launch
-// (FIX false) but listed in defer[], and the launch with FIX true advances
-// exactly those, with the full iteration.  Particles are independent, so the
-// split changes no result; it keeps the full iteration's registers and call
-// out of the main launch.  defer_n[serial & 1] counts this substep's list;
-// the FIX launch clears the other counter for the next substep.
+// enough for the reference's second pass to matter (ls_fit).  A block of the
+// main launch (FIX false) holding a particle that needs more passes (rare)
+// updates none of its particles but lists them in defer[]; the launch with
+// FIX true advances exactly the listed ones, with the full iteration.
+// Particles are independent, so the split changes no result; it keeps the
+// full iteration's registers and call out of the main launch.
+// defer_n[serial & 1] counts this substep's list; the FIX launch clears the
+// other counter for the next substep.
 #ifndef VR_PART_MINB
 #define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
 #endif
@@ -532,18 +536,16 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
                                              double *__restrict__ u, double *__restrict__ v,
                                              int *__restrict__ isfre, int *__restrict__ gone, int naloc, int ip,
                                              bool live, int mode, double inv_st, double partdt, int serial,
-                                             int *nremoved, int *__restrict__ defer, PartShared<R> &S,
-                                             int (&need_s)[3][kPartPerBlock]) {
+                                             int *nremoved, int *__restrict__ defer, PartShared<R> &S) {
   constexpr bool DBL = std::is_same<R, double>::value;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
+  bool need = false;
   if (live) {
     const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
     int cell[3];
-    bool need;
     part_component<R, FIX>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs,
                            ir1, ir2, need);
-    if (DBL && !FIX) need_s[w][p] = need;
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -551,17 +553,21 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
       for (int jk = 0; jk < 9; jk++) S.hes[w + 3 * jk][p] = u[PUo(ip, 25 + w + 3 * jk)];
     }
   }
-  __syncthreads();
-  bool go = live;
-  if (DBL && !FIX && live && (need_s[0][p] | need_s[1][p] | need_s[2][p])) {
-    go = false;  // left unchanged here, advanced by the FIX launch
-    if (w == 0) {
-      const int k = atomicAdd(nremoved + 1 + (serial & 1), 1);
-      if (k < naloc) defer[k] = ip;
+  if (DBL && !FIX) {
+    // a block with any particle that needs the full fit leaves all of its
+    // particles unchanged here: the FIX launch advances them
+    if (__syncthreads_or(need)) {
+      if (w == 0 && live) {
+        const int k = atomicAdd(nremoved + 1 + (serial & 1), 1);
+        if (k < naloc) defer[k] = ip;
+      }
+      return;
     }
+  } else {
+    __syncthreads();
   }
   double pw = 0.0;
-  if (go) {
+  if (live) {
     R vr_, dvr[3], ddvr[3][3];
     part_cart_row<R>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
     const double vel = vr_;
@@ -621,7 +627,7 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
     S.pos[w][p] = pw;
   }
   __syncthreads();
-  if (go) {
+  if (live) {
     // out of the domain: removed (single rank: nothing migrates)
     const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
     const double rp = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
@@ -647,13 +653,12 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
                                                   int nlast, int mode, double inv_st, double partdt, int serial,
                                                   int *nremoved, int *__restrict__ defer) {
   __shared__ PartShared<R> S;
-  __shared__ int need_s[3][kPartPerBlock];
   const int p = threadIdx.x & 31;
   if constexpr (!FIX) {
     const int ip = 1 + blockIdx.x * kPartPerBlock + p;
     const bool live = ip <= nlast && isfre[ip - 1] == 0;
     part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st, partdt, serial,
-                           nremoved, defer, S, need_s);
+                           nremoved, defer, S);
   } else {
     int *const defer_n = nremoved + 1;
     const int nfix = min(*(volatile int *)(defer_n + (serial & 1)), naloc);
@@ -662,7 +667,7 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
     for (int base = blockIdx.x * kPartPerBlock; base < nfix; base += gridDim.x * kPartPerBlock) {
       const int ip = base + p < nfix ? defer[base + p] : 0;
       part_advance<R, true>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, ip > 0, mode, inv_st, partdt, serial,
-                            nremoved, defer, S, need_s);
+                            nremoved, defer, S);
       __syncthreads();  // S is reused by the next group
     }
   }
@@ -1136,7 +1141,7 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
     if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
     if (!c->mixed) {  // the particles the main launch deferred to the full fit
       LaunchScope ls(c, PK_PART, stream);
-      k_iter_part<double, true><<<std::min(nb, 8 * c->nsm), 96, 0, stream>>>(
+      k_iter_part<double, true><<<std::min(nb, 2 * c->nsm), 96, 0, stream>>>(
           P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
           serial, p->d_nremoved, p->d_defer);
     }
