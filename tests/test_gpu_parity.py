@@ -197,3 +197,17 @@ def test_production_transform_sizes(wth):
     gpu.substep(1)
     for n in STATE + ["dph", "rhs"]:
         assert_field_close(gpu, orc, n, rel=1e-11)
+
+
+def test_streamed_z_transform_many_tiles_per_cta():
+    # 128 x 64 x 512: 512 tiles of the TMA-streamed 512-point z transform, so
+    # each persistent CTA takes three or four and its three buffers are reused
+    grid = (128, 64, 512)
+    orc, gpu = _pair(grid, wth="modified")
+    seed_random(orc, gpu, ["rhs"], seed=61)
+    prep(orc, gpu)
+    orc.laplace_solve()
+    gpu.laplace_solve()
+    g = gpu.get("dph")[:, 1:65, 1:513]
+    r = orc.field("dph")[:, 1:65, 1:513]
+    assert np.abs(g - r).max() <= 1e-11 * np.abs(r).max()

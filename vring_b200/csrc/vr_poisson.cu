@@ -509,19 +509,36 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
   }
 }
 
+// Two adjacent columns (ca, ca + 1) of a padded shared-memory tile as the
+// transpose scratch of warp_fft512: entry k at row(k).
+template <class RowFn>
+struct ColPair {
+  double *tile;
+  int ca;
+  RowFn row;
+  __device__ __forceinline__ void st(int k, double r, double i) const {
+    tile[row(k) + ca] = r;
+    tile[row(k) + ca + 1] = i;
+  }
+  __device__ __forceinline__ void ld(int k, double &r, double &i) const {
+    r = tile[row(k) + ca];
+    i = tile[row(k) + ca + 1];
+  }
+};
+
 // 512-point forward DFT of one complex sequence by a warp, N = 16 x 32:
 // lane t holds z[t + 32 m] (m = 0..15) in re/im; a 16-point DFT over m in
-// registers, the twiddles W_512^{t k1}, a transpose through the warp's own
-// two tile columns (row(k) = the padded row of the caller's tile; with
-// rows k = t + 32 k1 both the write and the transposed read fall on
-// distinct banks), then for k1 = lane / 2 the 32-point DFT over t split
-// into even (lane even) and odd (lane odd) samples, each a 16-point DFT in
-// registers, combined by one exchange with the partner lane.  On return
-// re/im[q] = X[k1 + 16 (16 h + brev4(q))], h = lane & 1.  The tile columns
-// must no longer be needed by the caller (their inputs are in registers).
-template <class RowFn>
+// registers, the twiddles W_512^{t k1}, a transpose through the caller's
+// scratch (acc.st / acc.ld of entry k; the entries k = t + 32 k1 written and
+// the entries read back must fall on distinct banks), then for k1 = lane / 2
+// the 32-point DFT over t split into even (lane even) and odd (lane odd)
+// samples, each a 16-point DFT in registers, combined by one exchange with the
+// partner lane.  On return re/im[q] = X[k1 + 16 (16 h + brev4(q))],
+// h = lane & 1.  The scratch must no longer be needed by the caller (its
+// inputs are in registers).
+template <class Acc>
 __device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], const double *__restrict__ tw,
-                                            double *tile, int ca, int cb, int lane, RowFn row) {
+                                            const Acc &acc, int lane) {
   constexpr int N = 512;
   reg_dif<16, N, 0, 16>(re, im, tw);
   __syncwarp();
@@ -536,16 +553,12 @@ __device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], 
       yr = xr;
       yi = xi;
     }
-    tile[row(lane + 32 * k1) + ca] = yr;
-    tile[row(lane + 32 * k1) + cb] = yi;
+    acc.st(lane + 32 * k1, yr, yi);
   }
   __syncwarp();
   const int k1 = lane >> 1, h = lane & 1;
 #pragma unroll
-  for (int u = 0; u < 16; u++) {
-    re[u] = tile[row(2 * u + h + 32 * k1) + ca];
-    im[u] = tile[row(2 * u + h + 32 * k1) + cb];
-  }
+  for (int u = 0; u < 16; u++) acc.ld(2 * u + h + 32 * k1, re[u], im[u]);
   __syncwarp();
   reg_dif<16, N, 0, 16>(re, im, tw);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
 #pragma unroll
@@ -606,7 +619,7 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     }
     __syncwarp();
     if constexpr (E == 16) {
-      warp_fft512(re, im, twz, tile, ca, cb, lane, row);
+      warp_fft512(re, im, twz, ColPair<decltype(row)>{tile, ca, row}, lane);
 #pragma unroll
       for (int q = 0; q < 16; q++) {
         const int k = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
@@ -658,7 +671,7 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     __syncwarp();
     if constexpr (E == 16) {
       // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
-      warp_fft512(re, im, twz, tile, ca, cb, lane, row);
+      warp_fft512(re, im, twz, ColPair<decltype(row)>{tile, ca, row}, lane);
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < 16; q++) {
@@ -683,6 +696,161 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
   for (int idx = threadIdx.x; idx < N * LT; idx += LT * 16) {
     int k = idx / LT, l = idx % LT;
     if (l < nl) base[l + s2 * k] = tile[row(k) + l];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z transforms of length 512 streamed by TMA.  A persistent CTA of eight
+// warps takes tiles of 16 consecutive slots at one radial index (16 columns x
+// 512 planes, 64 KB) in turn; three shared-memory buffers rotate, so that
+// while the warps transform tile s in place, tile s + 1 is loading and tile
+// s - 1 is being stored.  Tiles arrive 128B-swizzled: the 16-byte chunk with
+// columns 2w, 2w + 1 of row k sits at chunk w ^ (k & 7), and warp w moves its
+// (re, im) pairs as 16-byte words on distinct banks.  The arithmetic is that
+// of k_dct_w (Makhoul's reordering, the 16 x 32 warp FFT, the quarter-wave
+// shift), so both give the same bits.
+// ---------------------------------------------------------------------------
+constexpr int kDctTileCols = 16, kDctN = 512, kDctBufs = 3;
+constexpr unsigned kDctTileBytes = kDctTileCols * kDctN * 8;  // 65,536
+
+// chunk w of row r of a swizzled tile (rows of eight 16-byte chunks)
+__device__ __forceinline__ double2 *swz_pair(double2 *b, int r, int w) { return b + r * 8 + (w ^ (r & 7)); }
+
+// Chunk w of a swizzled tile as a scratch of pairs, entry k at row
+// k ^ (X(k)): with X(k) = 2 ((k >> 5) & 3) both the writes (k = t + 32 k1)
+// and the reads (k = 2u + h + 32 k1, k1 = lane / 2) of warp_fft512's transpose
+// meet eight distinct chunks in each quarter warp; with X(k) = 4 ((k >> 8) & 1)
+// so do the writes of the FFT output (k = lane / 2 + 16 (16 h + brev4(q)))
+// and the reads of pairs k, 512 - k (k = lane + 32 q) that follow.
+template <int SEL>
+struct SwzScratch {
+  double2 *b;
+  int w;
+  __device__ __forceinline__ double2 *at(int k) const {
+    const int r = SEL == 0 ? k ^ (((k >> 5) & 3) << 1) : k ^ (((k >> 8) & 1) << 2);
+    return swz_pair(b, r, w);
+  }
+  __device__ __forceinline__ void st(int k, double re, double im) const { *at(k) = make_double2(re, im); }
+  __device__ __forceinline__ void ld(int k, double &re, double &im) const {
+    const double2 v = *at(k);
+    re = v.x;
+    im = v.y;
+  }
+};
+
+template <int DIR>
+__global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUtensorMap tm, int nti, int ntiles,
+                                                    const double *__restrict__ twz, unsigned *status) {
+  constexpr int N = kDctN;
+  extern __shared__ unsigned char dct_dsm[];
+  __shared__ __align__(8) uint64_t full[kDctBufs];
+  double2 *const buf0 = reinterpret_cast<double2 *>(((uintptr_t)dct_dsm + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int bx = blockIdx.x, gx = gridDim.x;
+  const int nmine = ntiles > bx ? (ntiles - 1 - bx) / gx + 1 : 0;
+  auto buf = [&](int s) { return buf0 + (size_t)(s % kDctBufs) * (kDctTileBytes / 16); };
+  auto issue_load = [&](int s) {
+    const int t = bx + s * gx, i0 = (t % nti) * kDctTileCols, j = t / nti;
+    uint64_t *bar = &full[s % kDctBufs];
+    mbar_expect_tx(bar, kDctTileBytes);
+    tma_load_3d(buf(s), &tm, i0, j, 0, bar);
+    tma_load_3d(buf(s) + 256 * 8, &tm, i0, j, 256, bar);
+  };
+  if (tid == 0) {
+    for (int b = 0; b < kDctBufs; b++) mbar_init(&full[b], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < min(nmine, kDctBufs - 1); s++) issue_load(s);
+  const double *shift = twz + 2 * N;  // cos, sin (pi k / (2N))
+  int s = 0;
+  bool failed = false;
+  for (; s < nmine; s++) {
+    const bool ok = mbar_wait(&full[s % kDctBufs], (s / kDctBufs) & 1);
+    if (!__syncthreads_and(ok)) {
+      failed = true;
+      break;
+    }
+    double2 *const b = buf(s);
+    double re[16], im[16];
+    if (DIR > 0) {
+      // z_n = v^a_n + i v^b_n, v_n = x_{2n} (n < N/2), v_{N-1-n} = x_{2n+1}
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int n = lane + 32 * q, src = n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1;
+        const double2 v = *swz_pair(b, src, warp);
+        re[q] = v.x;
+        im[q] = v.y;
+      }
+      __syncwarp();
+      warp_fft512(re, im, twz, SwzScratch<0>{b, warp}, lane);
+      __syncwarp();
+      const SwzScratch<1> out{b, warp};
+#pragma unroll
+      for (int q = 0; q < 16; q++) out.st((lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4)), re[q], im[q]);
+      __syncwarp();
+      // y_k = 2 Re(e^{-i pi k/(2N)} V_k) / (2N)
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int k = lane + 32 * q, km = (N - k) & (N - 1);
+        double zr, zi, mr, mi;
+        out.ld(k, zr, zi);
+        out.ld(km, mr, mi);
+        const double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);  // V^a = (Z_k + conj Z_{N-k}) / 2
+        const double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);  // V^b = -i (Z_k - conj Z_{N-k}) / 2
+        const double c = __ldg(shift + 2 * k), sn = __ldg(shift + 2 * k + 1);
+        re[q] = 2.0 * (var_ * c + vai * sn) / (2.0 * N * 1);
+        im[q] = 2.0 * (vbr * c + vbi * sn) / (2.0 * N * 1);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 16; q++) *swz_pair(b, lane + 32 * q, warp) = make_double2(re[q], im[q]);
+    } else {
+      // W_k = V^a_k + i V^b_k, V_k = e^{i pi k/(2N)} (X_k - i X_{N-k}) / 2
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int k = lane + 32 * q;
+        const double c = __ldg(shift + 2 * k), sn = __ldg(shift + 2 * k + 1);
+        const double2 x = *swz_pair(b, k, warp), y = *swz_pair(b, (N - k) & (N - 1), warp);
+        const double xa = x.x / 2.0, xb = x.y / 2.0;
+        const double ya = k == 0 ? 0.0 : -y.x / 2.0, yb = k == 0 ? 0.0 : -y.y / 2.0;
+        const double var_ = xa * c - ya * sn, vai = xa * sn + ya * c;
+        const double vbr = xb * c - yb * sn, vbi = xb * sn + yb * c;
+        re[q] = var_ - vbi;    // Re W
+        im[q] = -(vai + vbr);  // -Im W (inverse as conj(DFT(conj W)))
+      }
+      __syncwarp();
+      // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
+      warp_fft512(re, im, twz, SwzScratch<0>{b, warp}, lane);
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int m = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
+        const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+        *swz_pair(b, o, warp) = make_double2(2.0 * re[q], -2.0 * im[q]);
+      }
+    }
+    fence_proxy_async();  // the tile's shared-memory writes, before the TMA store reads them
+    __syncthreads();
+    if (tid == 0) {
+      const int t = bx + s * gx, i0 = (t % nti) * kDctTileCols, j = t / nti;
+      tma_store_3d(&tm, i0, j, 0, b);
+      tma_store_3d(&tm, i0, j, 256, b + 256 * 8);
+      bulk_commit();
+      if (s + kDctBufs - 1 < nmine) {
+        bulk_wait_read<1>();  // the store of tile s - 1, in the buffer refilled next, has left it
+        issue_load(s + kDctBufs - 1);
+      }
+    }
+  }
+  if (tid == 0) {
+    if (failed) {
+      atomicOr(status, 1u);
+      // the loads already issued (tiles s, s + 1) land before the CTA leaves
+      for (int t = s; t < min(nmine, s + kDctBufs - 1); t++) mbar_wait(&full[t % kDctBufs], (t / kDctBufs) & 1);
+    }
+    bulk_wait_all();
   }
 }
 
@@ -994,8 +1162,29 @@ static cudaError_t run_dct_w(vr_ctx *c, int dir) {
   return cudaGetLastError();
 }
 
+// the TMA-streamed 512-point transform; NotSupported when the shape or the
+// tensor map does not fit it
+static cudaError_t run_dct_tma(vr_ctx *c, int dir) {
+  const Geo &g = c->geo;
+  if (g.nz != kDctN || g.nth % kDctTileCols) return cudaErrorNotSupported;
+  CUtensorMap tm;
+  if (!encode_tmap_f64_3d(&tm, c->spec, g.nth, g.nr, g.nz, kDctTileCols, 1, 256, true)) return cudaErrorNotSupported;
+  const int nti = g.nth / kDctTileCols, ntiles = nti * g.nr;
+  const size_t sm = (size_t)kDctBufs * kDctTileBytes + 1024;
+  auto kern = dir > 0 ? k_dct_tma<1> : k_dct_tma<-1>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  LaunchScope ls(c, PK_DCT);
+  kern<<<std::min(ntiles, c->nsm), 256, sm, c->stream>>>(tm, nti, ntiles, c->tw_z, c->d_status);
+  return cudaGetLastError();
+}
+
 static cudaError_t dct_warp_dispatch(vr_ctx *c, int dir, bool *done) {
   *done = true;
+  if (c->geo.nz == kDctN) {
+    cudaError_t e = run_dct_tma(c, dir);
+    if (e != cudaErrorNotSupported) return e;
+  }
   switch (c->geo.nz) {
     case 32: return run_dct_w<1, 16>(c, dir);
     case 64: return run_dct_w<2, 16>(c, dir);

@@ -43,7 +43,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 bool encode_tmap_f64_3d(CUtensorMap *tm, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, unsigned b0,
-                        unsigned b1, unsigned b2) {
+                        unsigned b1, unsigned b2, bool swizzle128) {
   auto fn = encode_fn();
   if (!fn) return false;
   if (((uintptr_t)base & 15) || ((d0 * 8) & 15)) return false;
@@ -52,7 +52,8 @@ bool encode_tmap_f64_3d(CUtensorMap *tm, const void *base, uint64_t d0, uint64_t
   const cuuint32_t box[3] = {b0, b1, b2};
   const cuuint32_t es[3] = {1, 1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dims, strides, box, es,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 

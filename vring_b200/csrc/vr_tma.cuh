@@ -1,7 +1,8 @@
-// vr_tma.cuh -- tensor-memory-accelerator (TMA) tile loads and mbarriers.
+// vr_tma.cuh -- tensor-memory-accelerator (TMA) tile loads/stores and mbarriers.
 //
 // Tiles are loaded with cp.async.bulk.tensor (no cluster multicast) into
-// shared memory and completion is tracked by an mbarrier's transaction count.
+// shared memory and completion is tracked by an mbarrier's transaction count;
+// stores are bulk groups of the issuing thread.
 // Every wait is bounded by the global timer: after kWaitLimitNs without
 // completion the wait reports failure and the kernel records VR_ERR_TIMEOUT
 // in the context's device status word instead of spinning on.
@@ -74,11 +75,35 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, in
       : "memory");
 }
 
+// 3-D tiled store of the box at (x, y, z) from src (shared memory), as one
+// bulk group of this thread: x * 8 bytes must be a multiple of 16 and every
+// coordinate non-negative
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *tm, int x, int y, int z, const void *src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                   reinterpret_cast<uint64_t>(tm)),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// until at most N of this thread's bulk groups still read shared memory
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// until every bulk group of this thread has completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // Host: a tensor map of a column-major FP64 array (d0, d1, d2) with boxes of
-// (b0, b1, b2) elements; out-of-range elements of a box read as zero.  False
-// when the driver entry point is missing or the driver rejects the map
-// (base not 16-byte aligned, d0 * 8 not a multiple of 16, box too large).
+// (b0, b1, b2) elements; out-of-range elements of a box read as zero.  With
+// swizzle128 the box rows (b0 * 8 = 128 bytes) land in shared memory with
+// their 16-byte chunks permuted, chunk c of row r at c ^ (r & 7) (the buffer
+// 1024-byte aligned).  False when the driver entry point is missing or the
+// driver rejects the map (base not 16-byte aligned, d0 * 8 not a multiple of
+// 16, box too large).
 bool encode_tmap_f64_3d(CUtensorMap *tm, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, unsigned b0,
-                        unsigned b1, unsigned b2);
+                        unsigned b1, unsigned b2, bool swizzle128 = false);
 
 }  // namespace vr
