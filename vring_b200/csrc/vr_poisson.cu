@@ -299,12 +299,37 @@ __host__ __device__ constexpr int brev_c(int x, int bits) {
 }
 __host__ __device__ constexpr int log2_c(int x) { return x <= 1 ? 0 : 1 + log2_c(x / 2); }
 
-// Radix-2 decimation-in-frequency DFT of the L points re/im[OFF .. OFF+L) in
-// registers with W_{2h}^q = W_N^{q N / (2h)} from stw (cos, sin pairs);
-// X[k] ends in slot OFF + brev(k).  Multiplications by W^0 = 1 are skipped
-// (they are exact).
+// (dr + i di) W_16^k, k = 1..7, with W_16 = e^{-2 pi i / 16}: -i as a swap,
+// W_16^2 and W_16^6 as sums times sqrt(1/2), the others with the constants
+template <int K>
+__device__ __forceinline__ void w16_mul(double dr, double di, double &outr, double &outi) {
+  constexpr double s2 = 0.7071067811865476;
+  if constexpr (K == 4) {
+    outr = di;
+    outi = -dr;
+  } else if constexpr (K == 2) {
+    outr = (dr + di) * s2;
+    outi = (di - dr) * s2;
+  } else if constexpr (K == 6) {
+    outr = (di - dr) * s2;
+    outi = -(dr + di) * s2;
+  } else {
+    constexpr double c = K == 1 ? 0.9238795325112867 : K == 3 ? 0.3826834323650898 : K == 5 ? -0.3826834323650898
+                                                                                         : -0.9238795325112867;
+    constexpr double sn = K == 1 || K == 7 ? -0.3826834323650898 : -0.9238795325112867;  // -sin(2 pi K / 16)
+    outr = dr * c - di * sn;
+    outi = dr * sn + di * c;
+  }
+}
+
+// Radix-2 decimation-in-frequency DFT of the L <= 16 points
+// re/im[OFF .. OFF+L) in registers; X[k] ends in slot OFF + brev(k).  Every
+// twiddle W_{2h}^q (2h <= 16) is a power of W_16, applied with the constants
+// of w16_mul; multiplications by W^0 = 1 are skipped (they are exact).  N is
+// the length of the whole transform the caller builds from these steps.
 template <int L, int N, int OFF, int R>
-__device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const double *stw) {
+__device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const double *) {
+  static_assert(L <= 16, "register DFTs up to 16 points");
 #pragma unroll
   for (int h = L / 2; h >= 1; h >>= 1) {
 #pragma unroll
@@ -315,15 +340,16 @@ __device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const 
         re[ja] = ar + br;
         im[ja] = ai + bi;
         const double dr = ar - br, di = ai - bi;
-        const int q = j & (h - 1);
-        if (q == 0) {
-          re[jb] = dr;
-          im[jb] = di;
-        } else {
-          const int p = q * (N / (2 * h));
-          const double c = stw[2 * p], sn = -stw[2 * p + 1];
-          re[jb] = dr * c - di * sn;
-          im[jb] = dr * sn + di * c;
+        const int k = (j & (h - 1)) * (8 / h);  // W_{2h}^q = W_16^{8 q / h}
+        switch (k) {
+          case 0: re[jb] = dr; im[jb] = di; break;
+          case 1: w16_mul<1>(dr, di, re[jb], im[jb]); break;
+          case 2: w16_mul<2>(dr, di, re[jb], im[jb]); break;
+          case 3: w16_mul<3>(dr, di, re[jb], im[jb]); break;
+          case 4: w16_mul<4>(dr, di, re[jb], im[jb]); break;
+          case 5: w16_mul<5>(dr, di, re[jb], im[jb]); break;
+          case 6: w16_mul<6>(dr, di, re[jb], im[jb]); break;
+          default: w16_mul<7>(dr, di, re[jb], im[jb]); break;
         }
       }
     }
