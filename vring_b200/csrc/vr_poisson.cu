@@ -322,6 +322,23 @@ __device__ __forceinline__ void w16_mul(double dr, double di, double &outr, doub
   }
 }
 
+// (ar + i ai) W_32^K, K = 1..15, W_32 = e^{-2 pi i / 32}, with the constants
+// cos and sin of 2 pi K / 32 (correctly rounded)
+template <int K>
+__device__ __forceinline__ void w32_mul(double ar, double ai, double &outr, double &outi) {
+  if constexpr (K % 2 == 0) {
+    w16_mul<K / 2>(ar, ai, outr, outi);
+  } else {
+    constexpr double c1 = 0.9807852804032304, c3 = 0.8314696123025452, c5 = 0.5555702330196022,
+                     c7 = 0.19509032201612828;
+    constexpr double cs = K == 1 ? c1 : K == 3 ? c3 : K == 5 ? c5 : K == 7 ? c7 : K == 9 ? -c7 : K == 11 ? -c5
+                        : K == 13 ? -c3 : -c1;
+    constexpr double sn = -(K == 1 || K == 15 ? c7 : K == 3 || K == 13 ? c5 : K == 5 || K == 11 ? c3 : c1);
+    outr = ar * cs - ai * sn;
+    outi = ar * sn + ai * cs;
+  }
+}
+
 // Radix-2 decimation-in-frequency DFT of the L <= 16 points
 // re/im[OFF .. OFF+L) in registers; X[k] ends in slot OFF + brev(k).  Every
 // twiddle W_{2h}^q (2h <= 16) is a power of W_16, applied with the constants
@@ -554,7 +571,8 @@ struct ColPair {
 
 // 512-point forward DFT of one complex sequence by a warp, N = 16 x 32:
 // lane t holds z[t + 32 m] (m = 0..15) in re/im; a 16-point DFT over m in
-// registers, the twiddles W_512^{t k1}, a transpose through the caller's
+// registers, the twiddles W_512^{t k1} (twf(k1, c, sn): cos and -sin of
+// 2 pi t k1 / 512 for this lane), a transpose through the caller's
 // scratch (acc.st / acc.ld of entry k; the entries k = t + 32 k1 written and
 // the entries read back must fall on distinct banks), then for k1 = lane / 2
 // the 32-point DFT over t split into even (lane even) and odd (lane odd)
@@ -562,19 +580,19 @@ struct ColPair {
 // partner lane.  On return re/im[q] = X[k1 + 16 (16 h + brev4(q))],
 // h = lane & 1.  The scratch must no longer be needed by the caller (its
 // inputs are in registers).
-template <class Acc>
-__device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], const double *__restrict__ tw,
-                                            const Acc &acc, int lane) {
+template <class TwFn, class Acc>
+__device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], const TwFn &twf, const Acc &acc,
+                                            int lane) {
   constexpr int N = 512;
-  reg_dif<16, N, 0, 16>(re, im, tw);
+  reg_dif<16, N, 0, 16>(re, im, nullptr);
   __syncwarp();
 #pragma unroll
   for (int k1 = 0; k1 < 16; k1++) {
     const int rg = brev_c(k1, 4);
     double yr = re[rg], yi = im[rg];
     if (k1 != 0) {
-      const int p = lane * k1;
-      const double c = __ldg(tw + 2 * p), sn = -__ldg(tw + 2 * p + 1);
+      double c, sn;
+      twf(k1, c, sn);
       const double xr = yr * c - yi * sn, xi = yr * sn + yi * c;
       yr = xr;
       yi = xi;
@@ -586,15 +604,30 @@ __device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], 
 #pragma unroll
   for (int u = 0; u < 16; u++) acc.ld(2 * u + h + 32 * k1, re[u], im[u]);
   __syncwarp();
-  reg_dif<16, N, 0, 16>(re, im, tw);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
+  reg_dif<16, N, 0, 16>(re, im, nullptr);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
 #pragma unroll
   for (int k2 = 0; k2 < 16; k2++) {
     const int rg = brev_c(k2, 4);
     double ar = re[rg], ai = im[rg];
     if (h && k2 != 0) {  // W_32^{k2} O[k2]
-      const int p = 16 * k2;
-      const double c = __ldg(tw + 2 * p), sn = -__ldg(tw + 2 * p + 1);
-      const double wr = ar * c - ai * sn, wi = ar * sn + ai * c;
+      double wr, wi;
+      switch (k2) {
+        case 1: w32_mul<1>(ar, ai, wr, wi); break;
+        case 2: w32_mul<2>(ar, ai, wr, wi); break;
+        case 3: w32_mul<3>(ar, ai, wr, wi); break;
+        case 4: w32_mul<4>(ar, ai, wr, wi); break;
+        case 5: w32_mul<5>(ar, ai, wr, wi); break;
+        case 6: w32_mul<6>(ar, ai, wr, wi); break;
+        case 7: w32_mul<7>(ar, ai, wr, wi); break;
+        case 8: w32_mul<8>(ar, ai, wr, wi); break;
+        case 9: w32_mul<9>(ar, ai, wr, wi); break;
+        case 10: w32_mul<10>(ar, ai, wr, wi); break;
+        case 11: w32_mul<11>(ar, ai, wr, wi); break;
+        case 12: w32_mul<12>(ar, ai, wr, wi); break;
+        case 13: w32_mul<13>(ar, ai, wr, wi); break;
+        case 14: w32_mul<14>(ar, ai, wr, wi); break;
+        default: w32_mul<15>(ar, ai, wr, wi); break;
+      }
       ar = wr;
       ai = wi;
     }
@@ -631,6 +664,11 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
   }
   cp_async_wait_all();
   __syncthreads();
+  auto tw_lane = [&](int k1, double &c, double &sn) {
+    const int p = lane * k1;
+    c = __ldg(twz + 2 * p);
+    sn = -__ldg(twz + 2 * p + 1);
+  };
   const double *shift = twz + 2 * N;  // cos, sin (pi k / (2N))
   const int ca = 2 * warp, cb = ca + 1;
   double re[E], im[E];
@@ -645,7 +683,7 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     }
     __syncwarp();
     if constexpr (E == 16) {
-      warp_fft512(re, im, twz, ColPair<decltype(row)>{tile, ca, row}, lane);
+      warp_fft512(re, im, tw_lane, ColPair<decltype(row)>{tile, ca, row}, lane);
 #pragma unroll
       for (int q = 0; q < 16; q++) {
         const int k = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
@@ -697,7 +735,7 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
     __syncwarp();
     if constexpr (E == 16) {
       // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
-      warp_fft512(re, im, twz, ColPair<decltype(row)>{tile, ca, row}, lane);
+      warp_fft512(re, im, tw_lane, ColPair<decltype(row)>{tile, ca, row}, lane);
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < 16; q++) {
@@ -771,6 +809,10 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
   extern __shared__ unsigned char dct_dsm[];
   __shared__ __align__(8) uint64_t full[kDctBufs];
   double2 *const buf0 = reinterpret_cast<double2 *>(((uintptr_t)dct_dsm + 1023) & ~(uintptr_t)1023);
+  // this CTA's copy of the lane twiddles W_512^{lane k1} (cos, -sin) at
+  // [k1 - 1][lane] and of the shift e^{i pi k / 1024} at [q][lane],
+  // k = lane + 32 q: every read of a warp is 32 consecutive pairs
+  double2 *const twl = buf0 + kDctBufs * (kDctTileBytes / 16), *const shl = twl + 15 * 32;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int bx = blockIdx.x, gx = gridDim.x;
   const int nmine = ntiles > bx ? (ntiles - 1 - bx) / gx + 1 : 0;
@@ -786,10 +828,22 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
     for (int b = 0; b < kDctBufs; b++) mbar_init(&full[b], 1);
     mbar_init_fence();
   }
+  for (int i = tid; i < 15 * 32; i += 256) {
+    const int p = (i & 31) * (i / 32 + 1);
+    twl[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
+  }
+  for (int i = tid; i < 16 * 32; i += 256) {
+    const int k = (i & 31) + 32 * (i / 32);
+    shl[i] = make_double2(__ldg(twz + 2 * N + 2 * k), __ldg(twz + 2 * N + 2 * k + 1));
+  }
   __syncthreads();
   if (tid == 0)
     for (int s = 0; s < min(nmine, kDctBufs - 1); s++) issue_load(s);
-  const double *shift = twz + 2 * N;  // cos, sin (pi k / (2N))
+  auto tw_lane = [&](int k1, double &c, double &sn) {
+    const double2 v = twl[(k1 - 1) * 32 + lane];
+    c = v.x;
+    sn = v.y;
+  };
   int s = 0;
   bool failed = false;
   for (; s < nmine; s++) {
@@ -810,7 +864,7 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
         im[q] = v.y;
       }
       __syncwarp();
-      warp_fft512(re, im, twz, SwzScratch<0>{b, warp}, lane);
+      warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
       __syncwarp();
       const SwzScratch<1> out{b, warp};
 #pragma unroll
@@ -825,7 +879,8 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
         out.ld(km, mr, mi);
         const double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);  // V^a = (Z_k + conj Z_{N-k}) / 2
         const double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);  // V^b = -i (Z_k - conj Z_{N-k}) / 2
-        const double c = __ldg(shift + 2 * k), sn = __ldg(shift + 2 * k + 1);
+        const double2 cs = shl[q * 32 + lane];
+        const double c = cs.x, sn = cs.y;
         re[q] = 2.0 * (var_ * c + vai * sn) / (2.0 * N * 1);
         im[q] = 2.0 * (vbr * c + vbi * sn) / (2.0 * N * 1);
       }
@@ -837,7 +892,8 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
 #pragma unroll
       for (int q = 0; q < 16; q++) {
         const int k = lane + 32 * q;
-        const double c = __ldg(shift + 2 * k), sn = __ldg(shift + 2 * k + 1);
+        const double2 cs = shl[q * 32 + lane];
+        const double c = cs.x, sn = cs.y;
         const double2 x = *swz_pair(b, k, warp), y = *swz_pair(b, (N - k) & (N - 1), warp);
         const double xa = x.x / 2.0, xb = x.y / 2.0;
         const double ya = k == 0 ? 0.0 : -y.x / 2.0, yb = k == 0 ? 0.0 : -y.y / 2.0;
@@ -848,7 +904,7 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
       }
       __syncwarp();
       // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
-      warp_fft512(re, im, twz, SwzScratch<0>{b, warp}, lane);
+      warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < 16; q++) {
@@ -1196,7 +1252,7 @@ static cudaError_t run_dct_tma(vr_ctx *c, int dir) {
   CUtensorMap tm;
   if (!encode_tmap_f64_3d(&tm, c->spec, g.nth, g.nr, g.nz, kDctTileCols, 1, 256, true)) return cudaErrorNotSupported;
   const int nti = g.nth / kDctTileCols, ntiles = nti * g.nr;
-  const size_t sm = (size_t)kDctBufs * kDctTileBytes + 1024;
+  const size_t sm = (size_t)kDctBufs * kDctTileBytes + (15 + 16) * 32 * 16 + 1024;
   auto kern = dir > 0 ? k_dct_tma<1> : k_dct_tma<-1>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
