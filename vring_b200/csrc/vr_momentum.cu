@@ -747,13 +747,18 @@ __device__ __forceinline__ void tsolve_group(int N, const double *cinv, const do
   }
 }
 
-template <int E, int CPT, class T>
+// NT > 0: the theta extent as a compile-time constant (equal to g.nth), so
+// that the shared-memory offsets, line strides and divisions by it fold
+template <int E, int CPT, class T, int NT>
 __global__ void __launch_bounds__(256, 2)
     k_rhs_march(const __grid_constant__ CUtensorMap tq1, const __grid_constant__ CUtensorMap tq2,
                 const __grid_constant__ CUtensorMap tq3, Geo g, Rk rk, RhsArgsT<T> a, TriPer t13, TriPer t2,
                 int zs, unsigned *status) {
   extern __shared__ __align__(128) double sm[];
-  const int N = g.nth, SPN = tpad(N) + 1;
+  const int N = NT > 0 ? NT : g.nth, SPN = tpad(N) + 1;
+  // offsets of the ghosted fields and of prg (I3, IPRG with this N)
+  auto i3 = [&](int i, int j, int k) { return (i - 1) + N * (j + g.J3 * k); };
+  auto iprg = [&](int i, int j, int k, int m) { return (i - 1) + N * ((j - 1) + g.nr * ((k - 1) + g.nz * (m - 1))); };
   const int FS = (kMRJ + 2) * N;    // doubles of one field's box
   const int FSP = (FS + 15) & ~15;  // box slots start on 128-byte boundaries
   const int SLOT = 3 * FSP;
@@ -821,11 +826,11 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
       if (!cact[q]) continue;
-      const int jc = j0 + cr[q], o = I3(g, ci[q] + 1, jc, kc);
+      const int jc = j0 + cr[q], o = i3(ci[q] + 1, jc, kc);
 #pragma unroll
       for (int m = 0; m < 3; m++) {
         pru[q][m] = __ldg(a.ru[m] + o);
-        ppg[q][m] = __ldg(a.prg + IPRG(g, ci[q] + 1, jc, kc, m + 1));
+        ppg[q][m] = __ldg(a.prg + iprg(ci[q] + 1, jc, kc, m + 1));
       }
     }
   };
@@ -873,7 +878,7 @@ __global__ void __launch_bounds__(256, 2)
       S.pg1 = (double)cpg[q][0], S.pg2 = (double)cpg[q][1], S.pg3 = (double)cpg[q][2];
       RhsCell v;
       rhs_eval(g, rk, jc, kc, S, rowc[r], v);
-      const int o = I3(g, i + 1, jc, kc);
+      const int o = i3(i + 1, jc, kc);
       a.ru[0][o] = (T)v.h1;
       lb[(size_t)(0 * kMRJ + r) * SPL + tpad(i)] = v.r1;
       if (kc >= 2) {
@@ -914,7 +919,7 @@ __global__ void __launch_bounds__(256, 2)
           const int L2 = warp * kGroups + gq;
           const int pl2 = L2 / (3 * kMRJ), comp2 = (L2 / kMRJ) % 3, r2 = L2 % kMRJ, jc2 = j0 + r2, lk2 = kc0 + pl2;
           if (lk2 > kc || jc2 > g.nr || (comp2 == 1 && jc2 < 2) || (comp2 == 2 && lk2 < 2)) continue;
-          double *dst = (comp2 == 0 ? a.qrhs[0] : (comp2 == 1 ? a.qrhs[1] : a.qrhs[2])) + I3(g, 1, jc2, lk2);
+          double *dst = (comp2 == 0 ? a.qrhs[0] : (comp2 == 1 ? a.qrhs[1] : a.qrhs[2])) + i3(1, jc2, lk2);
           const double *src = lines + (size_t)L2 * SPL;
           for (int i = lane; i < N; i += 32) dst[i] = src[tpad(i)];
         }
@@ -930,10 +935,11 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-template <int E, int CPT, class T>
+template <int E, int CPT, class T, int NT = 0>
 static cudaError_t run_rhs_march(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) {
   const Geo &g = c->geo;
-  if ((g.nth & 1) || kMRJ * g.nth > 256 * CPT || g.nth - 1 > 32 * E) return cudaErrorNotSupported;
+  if ((g.nth & 1) || kMRJ * g.nth > 256 * CPT || g.nth - 1 > 32 * E || (NT > 0 && g.nth != NT))
+    return cudaErrorNotSupported;
   CUtensorMap tm[3];
   for (int m = 0; m < 3; m++)
     if (!encode_tmap_f64_3d(&tm[m], c->q[m], g.nth, g.J3, g.K3, g.nth, kMRJ + 2, 1)) return cudaErrorNotSupported;
@@ -942,7 +948,7 @@ static cudaError_t run_rhs_march(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) 
   const int SPL = ((SPN + 15) & ~15) + 8;
   const size_t sm = sizeof(double) * ((size_t)kQRing * 3 * FSP + kTB * 3 * kMRJ * SPL + 2 * kMRJ * 3 * SPN);
   if (sm > 110 * 1024) return cudaErrorNotSupported;  // two CTAs per SM
-  auto kern = k_rhs_march<E, CPT, T>;
+  auto kern = k_rhs_march<E, CPT, T, NT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
@@ -970,6 +976,8 @@ static cudaError_t launch_rhs_tsweep_t(vr_ctx *c, const Rk &rk) {
     me = run_rhs_march<1, 1, T>(c, rk, a);
   else if (E <= 2)
     me = run_rhs_march<2, 1, T>(c, rk, a);
+  else if (g.nth == 128)
+    me = run_rhs_march<4, 1, T, 128>(c, rk, a);
   else if (E <= 4)
     me = run_rhs_march<4, 1, T>(c, rk, a);
   if (me != cudaErrorNotSupported) return me;
