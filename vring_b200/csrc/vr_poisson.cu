@@ -374,48 +374,60 @@ __device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const 
 }
 
 // The two-stage transform of the pair held as x[t + T m] in re/im[m]; on
-// return sre/sim[k] hold X[k] (natural order) for this pair.
-// Per-pair shared buffer: re at 0, im at PS, pairs 2 PS + 1 doubles apart.
-// The odd pair stride puts the pairs of a half-warp on different banks for
-// the transpose reads and the spectrum accesses (about half the wavefronts
-// of an aligned stride).
-__host__ __device__ constexpr int fft_pair_stride(int T) { return 16 * (T + 1) + 2; }
+// return sc[k] holds X[k] (natural order) of this pair as (re, im).
+//
+// Shared memory moves (re, im) pairs as 16-byte words.  The transpose
+// S[k1][c] (16 rows of T columns) stores column c of row k at
+// k T + (c ^ swz(k)), swz(k) = (k / G) mod min(T, 8): the writes (row k1,
+// columns t) and the reads (rows t G + u, column tt) of each quarter warp
+// then meet eight distinct 16-byte bank groups.  Pairs lie
+// fft_pair_stride(T) words apart; for T < 8 the stride offsets the pairs that
+// share a quarter warp by T words modulo 8.  twl[(k1 - 1) T + t] holds
+// W_N^{t k1} as (cos, -sin) for thread t.
+__host__ __device__ constexpr int fft_pair_stride(int T) { return 16 * T + (T < 8 ? T : 0); }
+
+template <int T>
+__device__ __forceinline__ int fft_swz(int k) {
+  constexpr int G = 16 / T, M = (T < 8 ? T : 8) - 1;
+  return (k / G) & M;
+}
 
 // gm: the lanes of this pair's group (a group exits as a whole)
 template <int T>
-__device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], const double *stw, double *sre,
-                                           double *sim, int t, unsigned gm) {
+__device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], const double2 *twl, double2 *sc,
+                                           int t, unsigned gm) {
   constexpr int N = 16 * T, G = 16 / T, LT = log2_c(T);
-  reg_dif<16, N, 0, 16>(re, im, stw);
-  // twiddles W_N^{t k1} and the transpose S[k1][t] (row stride T + 1)
+  reg_dif<16, N, 0, 16>(re, im, nullptr);
+  // twiddles W_N^{t k1} and the transpose S[k1][t]
 #pragma unroll
   for (int k1 = 0; k1 < 16; k1++) {
     const int rg = brev_c(k1, 4);
     double yr = re[rg], yi = im[rg];
     if (k1 != 0) {
-      const int p = t * k1;
-      const double c = stw[2 * p], sn = -stw[2 * p + 1];
+      const double2 w = twl[(k1 - 1) * T + t];
+      const double c = w.x, sn = w.y;
       const double xr = yr * c - yi * sn, xi = yr * sn + yi * c;
       yr = xr;
       yi = xi;
     }
-    sre[k1 * (T + 1) + t] = yr;
-    sim[k1 * (T + 1) + t] = yi;
+    sc[k1 * T + (t ^ fft_swz<T>(k1))] = make_double2(yr, yi);
   }
   __syncwarp(gm);
 #pragma unroll
   for (int u = 0; u < G; u++)
 #pragma unroll
     for (int tt = 0; tt < T; tt++) {
-      re[u * T + tt] = sre[(t * G + u) * (T + 1) + tt];
-      im[u * T + tt] = sim[(t * G + u) * (T + 1) + tt];
+      const int k = t * G + u;
+      const double2 v = sc[k * T + (tt ^ fft_swz<T>(k))];
+      re[u * T + tt] = v.x;
+      im[u * T + tt] = v.y;
     }
   __syncwarp(gm);
-  if constexpr (G >= 1) reg_dif<T, N, 0, 16>(re, im, stw);
-  if constexpr (G >= 2) reg_dif<T, N, T, 16>(re, im, stw);
+  if constexpr (G >= 1) reg_dif<T, N, 0, 16>(re, im, nullptr);
+  if constexpr (G >= 2) reg_dif<T, N, T, 16>(re, im, nullptr);
   if constexpr (G >= 4) {
-    reg_dif<T, N, 2 * T, 16>(re, im, stw);
-    reg_dif<T, N, 3 * T, 16>(re, im, stw);
+    reg_dif<T, N, 2 * T, 16>(re, im, nullptr);
+    reg_dif<T, N, 3 * T, 16>(re, im, nullptr);
   }
   if constexpr (G >= 8) {
 #pragma unroll
@@ -434,21 +446,29 @@ __device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], c
 #pragma unroll
     for (int k2 = 0; k2 < T; k2++) {
       const int k = t * G + u + 16 * k2;
-      sre[k] = re[u * T + brev_c(k2, LT)];
-      sim[k] = im[u * T + brev_c(k2, LT)];
+      sc[k] = make_double2(re[u * T + brev_c(k2, LT)], im[u * T + brev_c(k2, LT)]);
     }
   __syncwarp(gm);
+}
+
+// the block's copy of the lane twiddles: twl[(k1 - 1) T + t] = W_N^{t k1}
+template <int T>
+__device__ __forceinline__ void load_lane_twiddles(double2 *twl, const double *__restrict__ tw) {
+  for (int i = threadIdx.x; i < 15 * T; i += blockDim.x) {
+    const int p = (i % T) * (i / T + 1);
+    twl[i] = make_double2(__ldg(tw + 2 * p), -__ldg(tw + 2 * p + 1));
+  }
 }
 
 template <int T>
 __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in, double *__restrict__ out,
                                                    int nlines, const double *__restrict__ tw) {
   constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
-  extern __shared__ double sm[];
-  double *stw = sm;
+  extern __shared__ double2 smv[];
+  double2 *twl = smv;
   const int tid = threadIdx.x, t = tid % T, pl = tid / T;
-  double *sre = sm + 2 * N + (size_t)pl * (2 * PS + 1), *sim = sre + PS;
-  for (int i = tid; i < 2 * N; i += 128) stw[i] = __ldg(tw + i);
+  double2 *sc = smv + 15 * T + (size_t)pl * PS;
+  load_lane_twiddles<T>(twl, tw);
   __syncthreads();
   const int la = (blockIdx.x * NPB + pl) * 2;
   if (la >= nlines) return;  // no CTA barrier follows; the pair's group leaves together
@@ -461,30 +481,32 @@ __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in
     re[m] = pa[t + T * m];
     im[m] = hasb ? pb[t + T * m] : 0.0;
   }
-  pair_fft16<T>(re, im, stw, sre, sim, t, gm);
-  // packed [a0, a1, b1, ...] of both lines (fastfouriertransform.F90:34-43)
+  pair_fft16<T>(re, im, twl, sc, t, gm);
+  // packed [a0, a1, b1, ...] of both lines (fastfouriertransform.F90:34-43):
+  // coefficient k gives entries 2k - 1 and 2k; k = 0 gives entry 0 and the
+  // thread holding it also writes the cosine-only entry N - 1 of k = N / 2
   double *oa = out + (size_t)la * N, *ob = oa + N;
   const double invn = 1.0 / N;
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
-    const int sx = t + T * j;
-    double va, vb;
-    if (sx == 0) {
-      va = sre[0] * invn;
-      vb = sim[0] * invn;
+  for (int jj = 0; jj < N / (2 * T); jj++) {
+    const int k = t + T * jj;
+    if (k == 0) {
+      const double2 z0 = sc[0], zn = sc[N / 2];
+      oa[0] = z0.x * invn;
+      oa[N - 1] = (zn.x + zn.x) * invn;
+      if (hasb) {
+        ob[0] = z0.y * invn;
+        ob[N - 1] = (zn.y + zn.y) * invn;
+      }
     } else {
-      const int k = (sx + 1) >> 1, km = (N - k) & (N - 1);
-      const double zr = sre[k], zi = sim[k], mr = sre[km], mi = sim[km];
-      if (sx & 1) {
-        va = (zr + mr) * invn;
-        vb = (zi + mi) * invn;
-      } else {
-        va = -(zi - mi) * invn;
-        vb = (zr - mr) * invn;
+      const double2 z = sc[k], m = sc[N - k];
+      oa[2 * k - 1] = (z.x + m.x) * invn;
+      oa[2 * k] = -(z.y - m.y) * invn;
+      if (hasb) {
+        ob[2 * k - 1] = (z.y + m.y) * invn;
+        ob[2 * k] = (z.x - m.x) * invn;
       }
     }
-    oa[sx] = va;
-    if (hasb) ob[sx] = vb;
   }
 }
 
@@ -492,22 +514,20 @@ template <int T>
 __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in, double *__restrict__ dph, Geo g,
                                                    int nlines, const double *__restrict__ tw) {
   constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
-  extern __shared__ double sm[];
-  double *stw = sm;
+  extern __shared__ double2 smv[];
+  double2 *twl = smv;
   const int tid = threadIdx.x, t = tid % T, pl = tid / T;
-  double *sre = sm + 2 * N + (size_t)pl * (2 * PS + 1), *sim = sre + PS;
-  for (int i = tid; i < 2 * N; i += 128) stw[i] = __ldg(tw + i);
+  double2 *sc = smv + 15 * T + (size_t)pl * PS;
+  load_lane_twiddles<T>(twl, tw);
   __syncthreads();
   const int la = (blockIdx.x * NPB + pl) * 2;
   if (la >= nlines) return;  // no CTA barrier follows; the pair's group leaves together
   const unsigned gm = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((tid & 31) / T * T));
   const bool hasb = la + 1 < nlines;
   const double *pa = in + (size_t)la * N, *pb = pa + N;
+  // the two packed lines side by side: sc[n] = (a[n], b[n])
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
-    sre[t + T * j] = pa[t + T * j];
-    sim[t + T * j] = hasb ? pb[t + T * j] : 0.0;
-  }
+  for (int j = 0; j < 16; j++) sc[t + T * j] = make_double2(pa[t + T * j], hasb ? pb[t + T * j] : 0.0);
   __syncwarp(gm);
   // Z_k = A_k + i B_k from the packed Hermitian spectra, conjugated: the
   // inverse transform runs as conj(DFT(conj Z)) (fastfouriertransform.F90:49-87)
@@ -518,15 +538,23 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
     const int kk = k <= N / 2 ? k : N - k;
     double ar, ai, br, bi;
     if (kk == 0) {
-      ar = sre[0];
+      const double2 v = sc[0];
+      ar = v.x;
       ai = 0.0;
-      br = sim[0];
+      br = v.y;
       bi = 0.0;
     } else {
-      ar = sre[2 * kk - 1] / 2.0;
-      br = sim[2 * kk - 1] / 2.0;
-      ai = (2 * kk < N) ? -1.0 * sre[2 * kk] / 2.0 : 0.0;
-      bi = (2 * kk < N) ? -1.0 * sim[2 * kk] / 2.0 : 0.0;
+      const double2 c1 = sc[2 * kk - 1];
+      ar = c1.x / 2.0;
+      br = c1.y / 2.0;
+      if (2 * kk < N) {
+        const double2 s1 = sc[2 * kk];
+        ai = -1.0 * s1.x / 2.0;
+        bi = -1.0 * s1.y / 2.0;
+      } else {
+        ai = 0.0;
+        bi = 0.0;
+      }
       if (k > N / 2) {
         ai = -ai;
         bi = -bi;
@@ -536,7 +564,7 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
     im[m] = -(ai + br);
   }
   __syncwarp(gm);
-  pair_fft16<T>(re, im, stw, sre, sim, t, gm);
+  pair_fft16<T>(re, im, twl, sc, t, gm);
   const int ja = 1 + la % g.nr, ka = 1 + la / g.nr;
   double *da = dph + IDP(g, 1, ja, ka);
   double *db = nullptr;
@@ -547,8 +575,9 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
 #pragma unroll
   for (int j = 0; j < 16; j++) {
     const int n = t + T * j;
-    da[n] = sre[n];
-    if (hasb) db[n] = -sim[n];
+    const double2 v = sc[n];
+    da[n] = v.x;
+    if (hasb) db[n] = -v.y;
   }
 }
 
@@ -1203,9 +1232,9 @@ static cudaError_t run_fft_w(vr_ctx *c, int dir) {
 template <int T>
 static cudaError_t run_fft_s(vr_ctx *c, int dir) {
   const Geo &g = c->geo;
-  constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
+  constexpr int NPB = 128 / T, PS = fft_pair_stride(T);
   const int nlines = g.nr * g.nz;
-  const size_t sm = sizeof(double) * (2 * N + (size_t)NPB * (2 * PS + 1));
+  const size_t sm = sizeof(double2) * (15 * T + (size_t)NPB * PS);
   const int npairs = (nlines + 1) / 2, blocks = (npairs + NPB - 1) / NPB;
   cudaError_t e;
   LaunchScope ls(c, PK_FFT);

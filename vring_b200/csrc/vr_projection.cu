@@ -283,11 +283,14 @@ struct UpsolArgs {
   double adt;
 };
 
-template <class T, bool UPSOL>
+// NT > 0: the theta extent as a compile-time constant (equal to g_in.nth)
+template <class T, bool UPSOL, int NT>
 __global__ void __launch_bounds__(256, 2)
-    k_uppres_march(const __grid_constant__ CUtensorMap tdph, Geo g, double be, T *__restrict__ prg,
+    k_uppres_march(const __grid_constant__ CUtensorMap tdph, Geo g_in, double be, T *__restrict__ prg,
                    T *__restrict__ pres, double *__restrict__ dphw, int zs, unsigned *status, UpsolArgs<T> us) {
   extern __shared__ __align__(128) double sm[];
+  Geo g = g_in;
+  if constexpr (NT > 0) g.nth = NT;
   const int N = g.nth;
   constexpr int RR = kUpRJ + 3;  // rows j0-2 .. j0+kUpRJ
   const int SLOT = (RR * N + 15) & ~15;
@@ -422,16 +425,16 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-template <class T, bool UPSOL>
-static cudaError_t run_uppres_march(vr_ctx *c, double be, double adt) {
+template <class T, bool UPSOL, int NT = 0>
+static cudaError_t run_uppres_march_n(vr_ctx *c, double be, double adt) {
   const Geo &g = c->geo;
-  if ((g.nth & 1) || kUpRJ * g.nth > 256) return cudaErrorNotSupported;
+  if ((g.nth & 1) || kUpRJ * g.nth > 256 || (NT > 0 && g.nth != NT)) return cudaErrorNotSupported;
   CUtensorMap tm;
   if (!encode_tmap_f64_3d(&tm, c->dph, g.nth, g.nr + 2, g.nz + 2, g.nth, kUpRJ + 3, 1))
     return cudaErrorNotSupported;
   const int SLOT = ((kUpRJ + 3) * g.nth + 15) & ~15;
   const size_t sm = sizeof(double) * (size_t)kUpRing * SLOT;
-  auto kern = k_uppres_march<T, UPSOL>;
+  auto kern = k_uppres_march<T, UPSOL, NT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
   const int zs = kUpZ;
@@ -441,6 +444,12 @@ static cudaError_t run_uppres_march(vr_ctx *c, double be, double adt) {
   kern<<<grid, 256, sm, c->stream>>>(tm, g, be, reinterpret_cast<T *>(c->prg), reinterpret_cast<T *>(c->pres),
                                       c->dph, zs, c->d_status, us);
   return cudaGetLastError();
+}
+
+template <class T, bool UPSOL>
+static cudaError_t run_uppres_march(vr_ctx *c, double be, double adt) {
+  if (c->geo.nth == 128) return run_uppres_march_n<T, UPSOL, 128>(c, be, adt);
+  return run_uppres_march_n<T, UPSOL>(c, be, adt);
 }
 
 cudaError_t launch_uppres(vr_ctx *c, const Rk &rk) {
