@@ -209,6 +209,9 @@ def main():
                     help="smaller grid for profiling captures (not the benchmark workload)")
     ap.add_argument("--nparticles", type=int, default=None,
                     help="particle count for profiling captures (not the benchmark workload)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="issue the warm-up substeps launch by launch instead of replaying CUDA graphs "
+                         "(the same kernels in the same order; for profiler launch lists)")
     args = ap.parse_args()
     global NR, NTH, NZ, NPART, WORKLOAD
     if args.grid is not None or args.nparticles is not None:
@@ -244,6 +247,8 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     run.set_stream(stream.cuda_stream)
+    if args.no_graphs:
+        run.set_graphs(False)
     ncell = NTH * NR * NZ
 
     for _ in range(args.warmup):
@@ -316,6 +321,8 @@ def main():
         del pu, pv
         pm.attach(True)
         rm_.set_stream(stream.cuda_stream)
+        if args.no_graphs:
+            rm_.set_graphs(False)
         for _ in range(args.warmup):
             rm_.iterate(1)
         torch.cuda.synchronize()
