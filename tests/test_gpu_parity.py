@@ -211,3 +211,18 @@ def test_streamed_z_transform_many_tiles_per_cta():
     g = gpu.get("dph")[:, 1:65, 1:513]
     r = orc.field("dph")[:, 1:65, 1:513]
     assert np.abs(g - r).max() <= 1e-11 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("wth", ["exact", "modified"])
+def test_streamed_z_transform_three_tiles_per_radius(wth):
+    # Ntheta 48: three 16-slot tiles per radial index (the theta transform
+    # takes the direct sums at this length), 7 radii, 512 planes
+    grid = (48, 7, 512)
+    orc, gpu = _pair(grid, wth=wth)
+    seed_random(orc, gpu, ["rhs"], seed=62)
+    prep(orc, gpu)
+    orc.laplace_solve()
+    gpu.laplace_solve()
+    g = gpu.get("dph")[:, 1:8, 1:513]
+    r = orc.field("dph")[:, 1:8, 1:513]
+    assert np.abs(g - r).max() <= 1e-11 * np.abs(r).max()

@@ -342,10 +342,11 @@ __device__ __forceinline__ void w32_mul(double ar, double ai, double &outr, doub
 // Radix-2 decimation-in-frequency DFT of the L <= 16 points
 // re/im[OFF .. OFF+L) in registers; X[k] ends in slot OFF + brev(k).  Every
 // twiddle W_{2h}^q (2h <= 16) is a power of W_16, applied with the constants
-// of w16_mul; multiplications by W^0 = 1 are skipped (they are exact).  N is
-// the length of the whole transform the caller builds from these steps.
+// of w16_mul; multiplications by W^0 = 1 are skipped (they are exact).  N,
+// the length of the whole transform the caller builds from these steps, does
+// not enter the arithmetic.
 template <int L, int N, int OFF, int R>
-__device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R], const double *) {
+__device__ __forceinline__ void reg_dif(double (&re)[R], double (&im)[R]) {
   static_assert(L <= 16, "register DFTs up to 16 points");
 #pragma unroll
   for (int h = L / 2; h >= 1; h >>= 1) {
@@ -397,7 +398,7 @@ template <int T>
 __device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], const double2 *twl, double2 *sc,
                                            int t, unsigned gm) {
   constexpr int N = 16 * T, G = 16 / T, LT = log2_c(T);
-  reg_dif<16, N, 0, 16>(re, im, nullptr);
+  reg_dif<16, N, 0, 16>(re, im);
   // twiddles W_N^{t k1} and the transpose S[k1][t]
 #pragma unroll
   for (int k1 = 0; k1 < 16; k1++) {
@@ -423,11 +424,11 @@ __device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], c
       im[u * T + tt] = v.y;
     }
   __syncwarp(gm);
-  if constexpr (G >= 1) reg_dif<T, N, 0, 16>(re, im, nullptr);
-  if constexpr (G >= 2) reg_dif<T, N, T, 16>(re, im, nullptr);
+  if constexpr (G >= 1) reg_dif<T, N, 0, 16>(re, im);
+  if constexpr (G >= 2) reg_dif<T, N, T, 16>(re, im);
   if constexpr (G >= 4) {
-    reg_dif<T, N, 2 * T, 16>(re, im, nullptr);
-    reg_dif<T, N, 3 * T, 16>(re, im, nullptr);
+    reg_dif<T, N, 2 * T, 16>(re, im);
+    reg_dif<T, N, 3 * T, 16>(re, im);
   }
   if constexpr (G >= 8) {
 #pragma unroll
@@ -613,7 +614,7 @@ template <class TwFn, class Acc>
 __device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], const TwFn &twf, const Acc &acc,
                                             int lane) {
   constexpr int N = 512;
-  reg_dif<16, N, 0, 16>(re, im, nullptr);
+  reg_dif<16, N, 0, 16>(re, im);
   __syncwarp();
 #pragma unroll
   for (int k1 = 0; k1 < 16; k1++) {
@@ -633,7 +634,7 @@ __device__ __forceinline__ void warp_fft512(double (&re)[16], double (&im)[16], 
 #pragma unroll
   for (int u = 0; u < 16; u++) acc.ld(2 * u + h + 32 * k1, re[u], im[u]);
   __syncwarp();
-  reg_dif<16, N, 0, 16>(re, im, nullptr);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
+  reg_dif<16, N, 0, 16>(re, im);  // E[k2] (h = 0) or O[k2] (h = 1) at slot brev(k2)
 #pragma unroll
   for (int k2 = 0; k2 < 16; k2++) {
     const int rg = brev_c(k2, 4);
