@@ -50,6 +50,7 @@ struct vr_part {
   int npart, nlast, nfree, nids;
   std::vector<int> ifree, h_isfre;
   int serial;  // substeps run so far
+  int ncall;   // iter_part calls enqueued (selects the deferred-list counter)
   bool counted;  // included in ctx->nparts
   // injections waiting for one scatter launch, and its device staging buffer
   std::vector<vr::NewPart> pending;
@@ -513,30 +514,38 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 
 #define PUo(ip, iv) ((size_t)((ip) - 1) + (size_t)naloc * ((iv) - 1))
 
-// One Euler substep of every live particle (part_tools.F90:517-959) and the
-// out-of-range test and removal (:962-987).
+// The nsub Euler substeps of one iter_part call for every live particle
+// (part_tools.F90:517-959), each followed by the out-of-range test and
+// removal (:962-987).  The fields do not change during the call and every
+// particle's update reads only its own state, so a block runs all substeps
+// of its 32 particles in turn (the reference runs each substep over all
+// particles): the results are the same, and the stencil samples of a
+// particle's later substeps are still in this SM's L1.  Removals carry the
+// serial of their substep.
 //
 // The FP64 fit stops after its first pass unless the samples are large
-// enough for the reference's second pass to matter (ls_fit).  A block of the
-// main launch (FIX false) holding a particle that needs more passes (rare)
-// updates none of its particles but lists them in defer[]; the launch with
-// FIX true advances exactly the listed ones, with the full iteration.
-// Particles are independent, so the split changes no result; it keeps the
-// full iteration's registers and call out of the main launch.
-// defer_n[serial & 1] counts this substep's list; the FIX launch clears the
-// other counter for the next substep.
+// enough for the reference's second pass to matter (ls_fit).  When a particle
+// of a block of the main launch (FIX false) needs more passes at substep s
+// (rare), the block stops there and lists its live particles with s in
+// defer[]; the launch with FIX true runs the listed particles from their
+// substep s on, with the full iteration.  This keeps the full iteration's
+// registers and call out of the main launch.  defer_n[par] counts this call's
+// list; the FIX launch clears the other counter for the next call.
 #ifndef VR_PART_MINB
 #define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
 #endif
-// Advance the particles in slots ip (1-based; one per lane, the same for
-// the three warps) whose live flag is set.
+// One substep of the particles in slots ip (1-based; one per lane, the same
+// for the three warps) whose live flag is set.  Returns kPartDeferred (for
+// the whole block) when the main launch leaves the block to the FIX launch,
+// else kPartRemoved for a particle that left the domain, else 0.
+constexpr int kPartRemoved = 1, kPartDeferred = 2;
 template <class R, bool FIX>
-__device__ __forceinline__ void part_advance(const PartGeo &P, const double *__restrict__ q1,
-                                             const double *__restrict__ q2, const double *__restrict__ q3,
-                                             double *__restrict__ u, double *__restrict__ v,
-                                             int *__restrict__ isfre, int *__restrict__ gone, int naloc, int ip,
-                                             bool live, int mode, double inv_st, double partdt, int serial,
-                                             int *nremoved, int *__restrict__ defer, PartShared<R> &S) {
+__device__ __forceinline__ int part_advance(const PartGeo &P, const double *__restrict__ q1,
+                                            const double *__restrict__ q2, const double *__restrict__ q3,
+                                            double *__restrict__ u, double *__restrict__ v,
+                                            int *__restrict__ isfre, int *__restrict__ gone, int naloc, int ip,
+                                            bool live, int mode, double inv_st, double partdt, int serial,
+                                            int *nremoved, PartShared<R> &S) {
   constexpr bool DBL = std::is_same<R, double>::value;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
@@ -555,18 +564,13 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
   }
   if (DBL && !FIX) {
     // a block with any particle that needs the full fit leaves all of its
-    // particles unchanged here: the FIX launch advances them
-    if (__syncthreads_or(need)) {
-      if (w == 0 && live) {
-        const int k = atomicAdd(nremoved + 1 + (serial & 1), 1);
-        if (k < naloc) defer[k] = ip;
-      }
-      return;
-    }
+    // particles unchanged from here on: the FIX launch advances them
+    if (__syncthreads_or(need)) return kPartDeferred;
   } else {
     __syncthreads();
   }
   double pw = 0.0;
+  bool removed = false;
   if (live) {
     R vr_, dvr[3], ddvr[3][3];
     part_cart_row<R>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
@@ -632,6 +636,7 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
     const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
     const double rp = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
     if ((z > P.zmax) || (z < 0.0) || (rp > P.rmax) || (rp < 0.0)) {
+      removed = true;
 #pragma unroll 1
       for (int iv = 1 + 39 * w; iv <= 39 * (w + 1); iv++) u[PUo(ip, iv)] = 0.0;
       if (w == 0) {
@@ -643,31 +648,52 @@ __device__ __forceinline__ void part_advance(const PartGeo &P, const double *__r
       }
     }
   }
+  return removed ? kPartRemoved : 0;
 }
+
+// deferred-list entries: slot | (first substep << kDeferShift)
+constexpr int kDeferShift = 26, kDeferSlotMask = (1 << kDeferShift) - 1;
 
 template <class R, bool FIX>
 __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const double *__restrict__ q1,
                                                   const double *__restrict__ q2, const double *__restrict__ q3,
                                                   double *__restrict__ u, double *__restrict__ v,
                                                   int *__restrict__ isfre, int *__restrict__ gone, int naloc,
-                                                  int nlast, int mode, double inv_st, double partdt, int serial,
-                                                  int *nremoved, int *__restrict__ defer) {
+                                                  int nlast, int mode, double inv_st, double partdt, int nsub,
+                                                  int serial0, int par, int *nremoved, int *__restrict__ defer) {
   __shared__ PartShared<R> S;
-  const int p = threadIdx.x & 31;
+  const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int *const defer_n = nremoved + 1;
   if constexpr (!FIX) {
     const int ip = 1 + blockIdx.x * kPartPerBlock + p;
-    const bool live = ip <= nlast && isfre[ip - 1] == 0;
-    part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st, partdt, serial,
-                           nremoved, defer, S);
+    bool live = ip <= nlast && isfre[ip - 1] == 0;
+#pragma unroll 1
+    for (int s = 0; s < nsub; s++) {
+      const int st = part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st,
+                                            partdt, serial0 + s, nremoved, S);
+      if (st == kPartDeferred) {  // the same in every thread of the block
+        if (w == 0 && live) {
+          const int k = atomicAdd(defer_n + par, 1);
+          if (k < naloc) defer[k] = ip | (s << kDeferShift);
+        }
+        break;
+      }
+      live = live && st != kPartRemoved;
+    }
   } else {
-    int *const defer_n = nremoved + 1;
-    const int nfix = min(*(volatile int *)(defer_n + (serial & 1)), naloc);
-    if (blockIdx.x == 0 && threadIdx.x == 0) defer_n[(serial + 1) & 1] = 0;
+    const int nfix = min(*(volatile int *)(defer_n + par), naloc);
+    if (blockIdx.x == 0 && threadIdx.x == 0) defer_n[par ^ 1] = 0;
 #pragma unroll 1
     for (int base = blockIdx.x * kPartPerBlock; base < nfix; base += gridDim.x * kPartPerBlock) {
-      const int ip = base + p < nfix ? defer[base + p] : 0;
-      part_advance<R, true>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, ip > 0, mode, inv_st, partdt, serial,
-                            nremoved, defer, S);
+      const int e = base + p < nfix ? defer[base + p] : 0;
+      const int ip = e & kDeferSlotMask, s0 = e >> kDeferShift;
+      bool live = ip > 0;
+#pragma unroll 1
+      for (int s = 0; s < nsub; s++) {
+        const int st = part_advance<R, true>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live && s >= s0, mode,
+                                             inv_st, partdt, serial0 + s, nremoved, S);
+        live = live && st != kPartRemoved;
+      }
       __syncthreads();  // S is reused by the next group
     }
   }
@@ -833,7 +859,7 @@ static int vr_part_mesh_init(vr_ctx *c) {
 }
 
 extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode, vr_part **out) {
-  if (!c || !out || naloc < 1 || (mode != 0 && mode != 1)) return VR_ERR_ARG;
+  if (!c || !out || naloc < 1 || naloc > kDeferSlotMask || (mode != 0 && mode != 1)) return VR_ERR_ARG;
   *out = nullptr;
   VR_CUDA(c, cudaSetDevice(c->dev));
   if (!c->part_mesh) {
@@ -1116,35 +1142,36 @@ extern "C" int vr_remv_part(vr_part *p, int32_t ip) {
   return VR_OK;
 }
 
-// enqueue the nsubdt substeps of one call of iter_part
+// enqueue the nsubdt substeps of one call of iter_part: one launch for all
+// substeps, then the launch for the particles it deferred (FP64 only)
 int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
   vr_ctx *c = p->ctx;
   PartGeo P;
   part_geo(c, P);
   double partdt = c->d.dt / (double)(float)p->nsubdt;
   double inv_st = 1.0 / p->st;
-  for (int s = 0; s < p->nsubdt; s++) {
-    if (p->nlast <= 0) break;
-    const int nb = (p->nlast + kPartPerBlock - 1) / kPartPerBlock, serial = p->serial++;
-    {
-      LaunchScope ls(c, PK_PART, stream);
-      if (c->mixed)
-        k_iter_part<float, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
-                                                         p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
-                                                         serial, p->d_nremoved, p->d_defer);
-      else
-        k_iter_part<double, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
-                                                          p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
-                                                          serial, p->d_nremoved, p->d_defer);
-    }
-    cudaError_t e = cudaGetLastError();
-    if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
-    if (!c->mixed) {  // the particles the main launch deferred to the full fit
-      LaunchScope ls(c, PK_PART, stream);
-      k_iter_part<double, true><<<std::min(nb, 2 * c->nsm), 96, 0, stream>>>(
-          P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
-          serial, p->d_nremoved, p->d_defer);
-    }
+  if (p->nlast <= 0) return VR_OK;
+  const int nb = (p->nlast + kPartPerBlock - 1) / kPartPerBlock, serial0 = p->serial, par = p->ncall & 1;
+  p->serial += p->nsubdt;
+  p->ncall++;
+  {
+    LaunchScope ls(c, PK_PART, stream);
+    if (c->mixed)
+      k_iter_part<float, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone,
+                                                       p->naloc, p->nlast, p->mode, inv_st, partdt, p->nsubdt,
+                                                       serial0, par, p->d_nremoved, p->d_defer);
+    else
+      k_iter_part<double, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
+                                                        p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
+                                                        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
+  if (!c->mixed) {
+    LaunchScope ls(c, PK_PART, stream);
+    k_iter_part<double, true><<<std::min(nb, 2 * c->nsm), 96, 0, stream>>>(
+        P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
+        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer);
     e = cudaGetLastError();
     if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
   }
