@@ -188,41 +188,6 @@ __device__ __forceinline__ void ls_pass(const PartCoef &C, const double (&y)[27]
   }
 }
 
-// Quadratic coefficients of one component: the reference's Richardson
-// iteration from zero, at most 100 passes, stopping when |mp| < 1e-6
-// (single-precision literal).  mint X = I, so the first pass is already the
-// least-squares solution and the second pass only adds the rounding error of
-// the first, bounded by a multiple of eps |mint| max|y|.  When max|y| is below
-// the bound at which that correction stays under the stop tolerance
-// (C.ymax_one_pass), the reference stops after the second pass with a
-// rounding-level change; the kernel stops after the first.
-__device__ __forceinline__ void ls_fit(const PartCoef &C, const double (&y)[27], double (&a)[9]) {
-  double mp[9];
-  ls_pass<true>(C, y, a, mp);
-  double nn = 0.0;
-#pragma unroll
-  for (int i = 0; i < 9; i++) {
-    a[i] = mp[i];
-    nn += mp[i] * mp[i];
-  }
-  if (sqrt(nn) < (double)0.000001f) return;
-  double ym = 0.0;
-#pragma unroll
-  for (int k = 0; k < 27; k++) ym = fmax(ym, fabs(y[k]));
-  if (ym < C.ymax_one_pass) return;  // NaN/Inf fail the test and take the full loop
-#pragma unroll 1
-  for (int iint = 2; iint <= 100; iint++) {
-    ls_pass<false>(C, y, a, mp);
-    nn = 0.0;
-#pragma unroll
-    for (int i = 0; i < 9; i++) {
-      a[i] = a[i] + mp[i];
-      nn += mp[i] * mp[i];
-    }
-    if (sqrt(nn) < (double)0.000001f) return;
-  }
-}
-
 // ---- three threads per particle ------------------------------------------
 // A block holds 32 particles in three warps; warp w fits component w of the
 // velocity (q1, q2/rc, q3) at the particle, then owns row w of every output:
@@ -256,9 +221,16 @@ __device__ __forceinline__ double stencil_sample(int nth, int J3, const double *
   return kd == 1 ? v * T.irc[f2] : v;
 }
 
-// Passes 2..100 of the reference's iteration when the one-pass bound does not
-// hold: the samples are gathered again (this path is rare, so they are not
-// kept in registers on the common path).
+// The quadratic coefficients of one component follow the reference's
+// Richardson iteration from zero, at most 100 passes, stopping when
+// |mp| < 1e-6 (single-precision literal).  mint X = I, so the first pass is
+// already the least-squares solution and the second pass only adds the
+// rounding error of the first, bounded by a multiple of eps |mint| max|y|.
+// When max|y| is below the bound at which that correction stays under the
+// stop tolerance (C.ymax_one_pass), the reference stops after the second pass
+// with a rounding-level change and the kernel stops after the first.
+// Otherwise this runs passes 2..100: the samples are gathered again (the path
+// is rare, so they are not kept in registers on the common path).
 __device__ __noinline__ void ls_more(const PartCoef *__restrict__ Cg, int nth, int J3, const double *__restrict__ q,
                                      int kd, Stencil T, double y0, double *a9) {
   double y[27], a[9], mp[9];
@@ -361,7 +333,7 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
 #pragma unroll
     for (int i = 0; i < 9; i++) nn += a[i] * a[i];
     // stop as the reference does (|mp| < 1e-6), or when the second pass is
-    // provably a rounding-level change under that tolerance (see ls_fit);
+    // provably a rounding-level change under that tolerance (see ls_more);
     // NaN/Inf take the full iteration
     // (the main launch tests |mp|^2 against a bound just below the square of
     // the tolerance: the particles in the thin band it adds are deferred, and
@@ -524,7 +496,7 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 // serial of their substep.
 //
 // The FP64 fit stops after its first pass unless the samples are large
-// enough for the reference's second pass to matter (ls_fit).  When a particle
+// enough for the reference's second pass to matter (ls_more).  When a particle
 // of a block of the main launch (FIX false) needs more passes at substep s
 // (rare), the block stops there and lists its live particles with s in
 // defer[]; the launch with FIX true runs the listed particles from their
