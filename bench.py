@@ -61,6 +61,24 @@ def family_words(fam, prof):
     return w
 
 
+def roofline(prof, steps, ncell, peak, peak_kind, traffic_tab, ms_per_step):
+    """Roofline of the dominant field family (largest event time among the
+    families with algorithmic words): algorithmic bytes per launch over its
+    mean launch time, against the HBM peak; traffic is the family's DRAM
+    bytes per launch from the committed ncu summaries; step_frac compares the
+    whole step with the HBM floor of all 198 words per cell-step."""
+    fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
+    tot_ms, nl = prof[fam]
+    per_sub = nl / (3 * steps)  # launches of this family per substep
+    bytes_per_launch = family_words(fam, prof) / per_sub * ncell * 8
+    achieved = bytes_per_launch / (tot_ms / nl / 1e3) / 1e9
+    step_ideal_ms = WORDS_PER_CELL_STEP * 8 * ncell / (peak * 1e9) * 1e3
+    return {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": bytes_per_launch, "traffic": traffic_tab.get(fam),
+            "step_frac": step_ideal_ms / ms_per_step}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -353,13 +371,7 @@ def main():
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
-    fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
-    tot_ms, nl = prof[fam]
-    per_sub = nl / (3 * args.steps)  # launches of this family per substep
-    bytes_per_launch = family_words(fam, prof) / per_sub * ncell * 8
-    achieved = bytes_per_launch / (tot_ms / nl / 1e3) / 1e9
-    traffic = traffic_table().get(fam)
-    step_ideal_ms = WORDS_PER_CELL_STEP * 8 * ncell / (peak * 1e9) * 1e3
+    roof = roofline(prof, args.steps, ncell, peak, peak_kind, traffic_table(), ms_max / args.steps)
 
     part_ms = prof.get("part", (0.0, 0))[0]
     counts = part.counts
@@ -378,11 +390,7 @@ def main():
             "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles, "mixed": mixed,
             "e2e": e2e,
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": bytes_per_launch,
-                         "traffic": traffic,
-                         "step_frac": step_ideal_ms / (ms_max / args.steps)},
+            "roofline": roof,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
