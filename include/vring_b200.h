@@ -206,7 +206,8 @@ VR_API int vr_profile_read(vr_ctx *ctx, int32_t kind, double *total_ms, int64_t 
  * VR_ERR_STATE while any exists). */
 typedef struct vr_part vr_part;
 /* init_part (part_tools.F90:228-359): class id 1..8 sets the radius, the
- * Stokes number and nsubdt; mode 0 inertial particles, 1 tracers */
+ * Stokes number and nsubdt; mode 0 inertial particles, 1 tracers; naloc
+ * (slots) from 1 to 2^26 - 1, else VR_ERR_ARG */
 VR_API int vr_part_create(vr_ctx *ctx, int32_t id, int32_t naloc, int32_t mode, vr_part **out);
 VR_API int vr_part_destroy(vr_part *part);
 /* radius, Stokes number, concentration scale and Euler substeps per step */
