@@ -76,6 +76,7 @@ def roofline(prof, steps, ncell, peak, peak_kind, traffic_tab, ms_per_step):
     return {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": bytes_per_launch, "traffic": traffic_tab.get(fam),
+            "traffic_source": traffic_tab.get("_note") if traffic_tab.get(fam) is not None else None,
             "step_frac": step_ideal_ms / ms_per_step}
 
 
@@ -142,6 +143,13 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def bench_config(world=1):
+    """The config dict both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ], "particles": NPART,
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"}
+
+
 def ring_state():
     from vring_b200.synthetic import ring_fields
     return ring_fields(NTH, NR, NZ, RMAX, ZMAX, R=1.0, sigma=0.2, gamma=1.0, z0=3.0, noise=1e-4, seed=0)
@@ -159,18 +167,19 @@ def particle_state(n, seed=0):
     return u, v
 
 
-def cpu_reference(steps, budget_s, q=None, part_sample=65536):
-    """The CPU restatement on the same workload, all host threads.  The field
-    steps run at full size; the particle advance runs on the first
-    part_sample particles of the same cloud and is scaled to 1,048,576.
-    Returns (Mcell-steps/s, steps timed, threads, sample text)."""
+def cpu_reference(steps, budget_s, q=None, part_sample=None):
+    """The CPU restatement on the same workload, all host threads: full-size
+    field steps and the particle advance of all NPART particles (part_sample
+    smaller than NPART advances the first part_sample of the same cloud and
+    scales their time).  Steps stop early once budget_s has passed.  Returns
+    (Mcell-steps/s, steps timed, threads, sample text)."""
     from oracle import oracle as O
     q = q if q is not None else ring_state()
     o = O.Oracle(NTH, NR, NZ, RMAX, ZMAX, DT, RE, 1.0, SLIP, 1, 0, 0)
     for n, a in zip(("q1", "q2", "q3"), q):
         o.field(n)[...] = a
     pu, pv = particle_state(NPART)
-    part_sample = min(part_sample, NPART)
+    part_sample = NPART if part_sample is None else min(part_sample, NPART)
     op = O.OraclePart(o, PART_CLASS, part_sample, PART_MODE)
     op.u[...] = pu[:part_sample]
     op.v[...] = pv[:part_sample]
@@ -188,9 +197,13 @@ def cpu_reference(steps, budget_s, q=None, part_sample=65536):
         if tc - t0 > budget_s:
             break
     step_s = (t_field + t_part * NPART / part_sample) / done
-    sample = ("%d RK3 steps of the full 256x128x512 field workload plus the particle advance of "
-              "%d of the 1,048,576 particles scaled by %d (CPU FP64 restatement, OpenMP, %d threads)"
-              % (done, part_sample, NPART // part_sample, os.cpu_count()))
+    if part_sample == NPART:
+        sample = ("%d RK3 steps of the full %dx%dx%d workload with all %d particles (CPU FP64 "
+                  "restatement, OpenMP, %d threads)" % (done, NR, NTH, NZ, NPART, os.cpu_count()))
+    else:
+        sample = ("%d RK3 steps of the full %dx%dx%d field workload plus the particle advance of "
+                  "%d of the %d particles scaled by %.3g (CPU FP64 restatement, OpenMP, %d threads)"
+                  % (done, NR, NTH, NZ, part_sample, NPART, NPART / part_sample, os.cpu_count()))
     return NTH * NR * NZ / step_s / 1e6, done, os.cpu_count(), sample
 
 
@@ -206,7 +219,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ]},
+            "config": bench_config(1),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -371,7 +384,10 @@ def main():
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
-    roof = roofline(prof, args.steps, ncell, peak, peak_kind, traffic_table(), ms_max / args.steps)
+    # the committed DRAM traffic belongs to the benchmark size; a reduced run reports none
+    reduced = args.grid is not None or args.nparticles is not None
+    roof = roofline(prof, args.steps, ncell, peak, peak_kind, {} if reduced else traffic_table(),
+                    ms_max / args.steps)
 
     part_ms = prof.get("part", (0.0, 0))[0]
     counts = part.counts
@@ -384,9 +400,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid_nr_ntheta_nz": [NR, NTH, NZ],
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "working set ~2.7 GB per replica, every field 137 MB > 126 MB L2"},
+            "config": bench_config(world),
             "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles, "mixed": mixed,
             "e2e": e2e,
             "gpu_launches": launches,

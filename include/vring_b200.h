@@ -10,8 +10,9 @@
  * components are not C-interoperable, so the state lives in an opaque
  * context that owns all device memory; fields cross the boundary as plain
  * double arrays in the reference's Fortran layouts (column-major, theta
- * fastest, the reference's ghost extents).  INTEGRATION.md shows the
- * ISO_C_BINDING module a Fortran caller binds these with.
+ * fastest, the reference's ghost extents).  A Fortran caller binds these
+ * through an ISO_C_BINDING interface module with one bind(C) interface per
+ * entry point.
  *
  * Conventions: every function returns VR_OK (0) or a VR_ERR_* code;
  * vr_last_error() gives a message.  Work is queued on the context's own CUDA
@@ -282,9 +283,13 @@ VR_API int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, 
  * VR_THOM_NOALLOC_MAX doubles (4 MiB) per device inside the library:
  * n * nbatch above that returns VR_ERR_SCRATCH.  The first call on a device
  * looks the array up (and may load the module); make it before any stream
- * capture.  Calls on one device share the array, so calls that may run at the
- * same time race: order them, e.g. on one stream.  The scratch need not start
- * at zero. */
+ * capture.  The address found then is kept for the life of the process: after
+ * cudaDeviceReset on that device (or anything else that destroys its primary
+ * context) this entry point must not be called on it again.  Calls on one
+ * device share the array, so calls that may run at the same time race: order
+ * them, e.g. on one stream.  The scratch need not start at zero.  The return
+ * value reports this call's launch only, not an error an earlier launch left
+ * pending. */
 #define VR_THOM_NOALLOC_MAX (1 << 19)
 VR_API int vr_solve_lap_thom_noalloc(const double *rhs, double *sol, const double *aa, const double *bb,
                                      const double *cc, int32_t n, int32_t nbatch, void *cuda_stream);

@@ -7,15 +7,19 @@ and dumps, per particle visit, the position and the interpolated Cartesian
 velocity (fort.300x), its gradient (fort.310x, dvel(i,j) with j fastest) and
 the three Hessian slices (fort.321x/322x/323x, ddvel(i,j,l) with l fastest),
 x = MPI rank.  This script samples every 25th line of the rank 0, 1 and 3
-dumps into dertest_kat.npz.  It reads the reference tree and is run once,
-in the build container; the tests only read the .npz it writes.
+dumps into dertest_kat.npz.  It reads the reference tree, whose root is its one
+required argument, and is run once; the tests only read the .npz it writes.
+
+    python tests/golden/make_golden.py <reference root>
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <reference root>")
+REF = sys.argv[1]
 SRC = os.path.join(REF, "dertest", "VR2D")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dertest_kat.npz")
 

@@ -416,7 +416,7 @@ cudaError_t run_chunk_tma(P p, const void *base, int d0, int d1, int d2, int ldi
   if (!encode_tmap_f64_3d(&tm, base, d0, d1, d2, LPT, ldim == 1 ? tt.br : 1, ldim == 2 ? tt.br : 1))
     return cudaErrorNotSupported;
   auto kern = k_chunk_tma<LPT, NCH, MAXCL, S, MINB, P>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  cudaError_t e = allow_dyn_smem(kern, dyn);
   if (e) return e;
   p.lpt = LPT;
   p.nbx = (p.nth_lines() + LPT - 1) / LPT;

@@ -5,8 +5,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "vr_internal.cuh"
@@ -18,6 +21,26 @@ namespace vr {
 int set_err(vr_ctx *c, int code, const std::string &msg) {
   if (c) c->err = msg;
   return code;
+}
+
+cudaError_t allow_dyn_smem(const void *kern, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> raised;  // (kernel, device) -> limit
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = raised.find({kern, dev});
+  if (it == raised.end()) {
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, kern))) return e;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+    const size_t lim = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim))) return e;
+    it = raised.emplace(std::make_pair(kern, dev), lim).first;
+  }
+  return bytes <= it->second ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 LaunchScope::LaunchScope(vr_ctx *ctx, int kind, cudaStream_t stream)

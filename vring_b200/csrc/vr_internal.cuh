@@ -172,6 +172,22 @@ int set_err(vr_ctx *c, int code, const std::string &msg);
       return vr::set_err((c), VR_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
   } while (0)
 
+// Dynamic shared memory above 48 KB needs a per-kernel opt-in
+// (cudaFuncAttributeMaxDynamicSharedMemorySize).  That limit belongs to the
+// kernel on a device, not to a launch: every context and every launch already
+// captured into a CUDA graph sees the latest value.  Setting it per call to
+// that call's size lets a later, smaller call lower it below what an earlier
+// captured launch of the same template instance needs, and that node then
+// fails to launch when it is replayed on its own (a profiler's kernel replay).
+// So the limit is raised once per kernel and device, to the most the device
+// allows beside the kernel's static shared memory, and never lowered; a call
+// needing more than that gets cudaErrorInvalidValue.
+cudaError_t allow_dyn_smem(const void *kern, size_t bytes);
+template <class K>
+inline cudaError_t allow_dyn_smem(K *kern, size_t bytes) {
+  return allow_dyn_smem(reinterpret_cast<const void *>(kern), bytes);
+}
+
 // kernel families for vr_profile_read
 enum ProfKind {
   PK_HDNBC = 0, PK_HDNL, PK_RHS, PK_TSWEEP, PK_RSWEEP, PK_ZSWEEP, PK_DIVQ, PK_FFT, PK_DCT,

@@ -635,7 +635,7 @@ static cudaError_t run_rhs_tsweep(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a)
   const Geo &g = c->geo;
   const int SPN = tpad(g.nth) + 1;
   const size_t sm = sizeof(double) * (size_t)SPN * (3 * kRJ * kRK + 2 * kRJ * 3);
-  cudaError_t e = cudaFuncSetAttribute(k_rhs_tsweep<E, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_rhs_tsweep<E, T>, sm);
   if (e) return e;
   const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
   LaunchScope ls(c, PK_RHS);
@@ -949,7 +949,7 @@ static cudaError_t run_rhs_march(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) 
   const size_t sm = sizeof(double) * ((size_t)kQRing * 3 * FSP + kTB * 3 * kMRJ * SPL + 2 * kMRJ * 3 * SPN);
   if (sm > 110 * 1024) return cudaErrorNotSupported;  // two CTAs per SM
   auto kern = k_rhs_march<E, CPT, T, NT>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(kern, sm);
   if (e) return e;
   const TriPer &t13 = c->ttri[c->irk][0], &t2 = c->ttri[c->irk][1];
   const int zs = kMarchZ;
@@ -998,7 +998,7 @@ template <int E>
 static cudaError_t run_tsweep(vr_ctx *c, const TriPer &t, double *f, int jb, int kb, int nj, int nk) {
   const int SPN = tpad(c->geo.nth) + 1;
   size_t sm = sizeof(double) * (size_t)SPN * (3 + 8);
-  cudaError_t e = cudaFuncSetAttribute(k_tsweep<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_tsweep<E>, sm);
   if (e) return e;
   LaunchScope ls(c, PK_TSWEEP);
   k_tsweep<E><<<dim3((nk + 7) / 8, nj), 256, sm, c->stream>>>(c->geo, t, f, jb, kb, nk);
@@ -1164,8 +1164,7 @@ __global__ void __launch_bounds__(LT *CH) k_linesweep(SweepArgsT<T> s, CoefShare
 template <int LT, int CH, class T = double>
 static cudaError_t run_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const CoefShared &cf, int nm2) {
   size_t sm = sizeof(double) * ((size_t)s.n * (LT + 1) + 2 * LT * CH);
-  cudaError_t e = cudaFuncSetAttribute(k_linesweep<LT, CH, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm);
+  cudaError_t e = allow_dyn_smem(k_linesweep<LT, CH, T>, sm);
   if (e) return e;
   dim3 gr((s.nth + LT - 1) / LT, nm2);
   LaunchScope ls(c, s.se == c->geo.nth ? PK_RSWEEP : PK_ZSWEEP);

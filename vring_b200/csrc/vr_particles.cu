@@ -3,8 +3,9 @@
 // State keeps the reference's layout: u(naloc, 117) and v(naloc, 3) are
 // column-major, i.e. one contiguous array per variable over the particles,
 // so a warp reads and writes each variable of 32 particles as one row.
-// One thread advances one particle through one Euler substep
-// (part_tools.F90:505-959): the 27-point least-squares fit of q1, q2/rc and q3
+// A block of three warps advances 32 particles through every Euler substep
+// of one iter_part call in one launch (part_tools.F90:505-959); warp w fits
+// velocity component w: the 27-point least-squares fit of q1, q2/rc and q3
 // around the particle's cell (part_tools.F90:577-625), the quadratic's value
 // and first/second derivatives, the cylindrical -> Cartesian transforms
 // (:653-797), the Stokes-drag ODE for position, velocity, Jacobian and

@@ -1192,7 +1192,7 @@ template <int LT, int CH>
 static cudaError_t run_radial(vr_ctx *c) {
   const Geo &g = c->geo;
   size_t sm = sizeof(double) * ((size_t)g.nr * (LT + 1) + 2 * LT * CH);
-  cudaError_t e = cudaFuncSetAttribute(k_radial<LT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_radial<LT, CH>, sm);
   if (e) return e;
   LaunchScope ls(c, PK_RADIAL);
   k_radial<LT, CH><<<dim3((g.nth + LT - 1) / LT, g.nz), LT * CH, sm, c->stream>>>(c->spec, g, c->pois_a, c->pois_c,
@@ -1204,7 +1204,7 @@ template <int LT>
 static cudaError_t run_dct(vr_ctx *c, int dir) {
   const Geo &g = c->geo;
   size_t sm = sizeof(double) * 3 * LT * g.nz;
-  cudaError_t e = cudaFuncSetAttribute(k_dct<LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_dct<LT>, sm);
   if (e) return e;
   LaunchScope ls(c, PK_DCT);
   k_dct<LT><<<dim3((g.nth + LT - 1) / LT, g.nr), 256, sm, c->stream>>>(c->spec, g, ilog2(g.nz), dir, c->tw_z);
@@ -1221,10 +1221,10 @@ static cudaError_t run_fft_w(vr_ctx *c, int dir) {
   cudaError_t e;
   LaunchScope ls(c, PK_FFT);
   if (dir > 0) {
-    if ((e = cudaFuncSetAttribute(k_fft_fwd_w<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_fwd_w<E>, sm))) return e;
     k_fft_fwd_w<E><<<blocks, 256, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th);
   } else {
-    if ((e = cudaFuncSetAttribute(k_fft_bwd_w<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_bwd_w<E>, sm))) return e;
     k_fft_bwd_w<E><<<blocks, 256, sm, c->stream>>>(c->spec, c->dph, g, nlines, c->tw_th);
   }
   return cudaGetLastError();
@@ -1240,10 +1240,10 @@ static cudaError_t run_fft_s(vr_ctx *c, int dir) {
   cudaError_t e;
   LaunchScope ls(c, PK_FFT);
   if (dir > 0) {
-    if ((e = cudaFuncSetAttribute(k_fft_fwd_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_fwd_s<T>, sm))) return e;
     k_fft_fwd_s<T><<<blocks, 128, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th);
   } else {
-    if ((e = cudaFuncSetAttribute(k_fft_bwd_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_bwd_s<T>, sm))) return e;
     k_fft_bwd_s<T><<<blocks, 128, sm, c->stream>>>(c->spec, c->dph, g, nlines, c->tw_th);
   }
   return cudaGetLastError();
@@ -1267,7 +1267,7 @@ static cudaError_t run_dct_w(vr_ctx *c, int dir) {
   const Geo &g = c->geo;
   constexpr int N = 32 * E;
   size_t sm = sizeof(double) * ((size_t)N * (LT + 1) + N / 16 + 1);
-  cudaError_t e = cudaFuncSetAttribute(k_dct_w<E, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_dct_w<E, LT>, sm);
   if (e) return e;
   LaunchScope ls(c, PK_DCT);
   k_dct_w<E, LT><<<dim3((g.nth + LT - 1) / LT, g.nr), LT * 16, sm, c->stream>>>(c->spec, g, dir, c->tw_z);
@@ -1284,7 +1284,7 @@ static cudaError_t run_dct_tma(vr_ctx *c, int dir) {
   const int nti = g.nth / kDctTileCols, ntiles = nti * g.nr;
   const size_t sm = (size_t)kDctBufs * kDctTileBytes + (15 + 16) * 32 * 16 + 1024;
   auto kern = dir > 0 ? k_dct_tma<1> : k_dct_tma<-1>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(kern, sm);
   if (e) return e;
   LaunchScope ls(c, PK_DCT);
   kern<<<std::min(ntiles, c->nsm), 256, sm, c->stream>>>(tm, nti, ntiles, c->tw_z, c->d_status);
@@ -1319,7 +1319,7 @@ cudaError_t launch_poisson(vr_ctx *c) {
   } else if (is_pow2(N)) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
-    if ((e = cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_fwd, sm))) return e;
     LaunchScope ls(c, PK_FFT);
     k_fft_fwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->rhs, c->spec, N, ilog2(N), lpb, nlines,
                                                                 c->tw_th);
@@ -1376,7 +1376,7 @@ cudaError_t launch_poisson(vr_ctx *c) {
   } else if (is_pow2(N)) {
     int lpb = N >= 1024 ? 1 : 1024 / N;
     size_t sm = sizeof(double) * 2 * lpb * N;
-    if ((e = cudaFuncSetAttribute(k_fft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = allow_dyn_smem(k_fft_bwd, sm))) return e;
     LaunchScope ls(c, PK_FFT);
     k_fft_bwd<<<(nlines + lpb - 1) / lpb, 256, sm, c->stream>>>(c->spec, c->dph, g, ilog2(N), lpb, nlines, c->tw_th);
   } else {

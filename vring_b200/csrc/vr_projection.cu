@@ -435,7 +435,7 @@ static cudaError_t run_uppres_march_n(vr_ctx *c, double be, double adt) {
   const int SLOT = ((kUpRJ + 3) * g.nth + 15) & ~15;
   const size_t sm = sizeof(double) * (size_t)kUpRing * SLOT;
   auto kern = k_uppres_march<T, UPSOL, NT>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(kern, sm);
   if (e) return e;
   const int zs = kUpZ;
   const int grid = ((g.nr + kUpRJ - 1) / kUpRJ) * ((g.nz + zs - 1) / zs);

@@ -148,7 +148,7 @@ __global__ void k_bthom(const double *__restrict__ rhs, double *__restrict__ sol
 cudaError_t launch_bthom_batched(const double *rhs, double *sol, const double *b1, const double *b2,
                                  const double *b3, int m, int n, int nbatch, double *work, cudaStream_t s) {
   size_t sm = sizeof(double) * (3 * (size_t)m * m + m);
-  cudaError_t e = cudaFuncSetAttribute(k_bthom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = allow_dyn_smem(k_bthom, sm);
   if (e) return e;
   k_bthom<<<nbatch, 128, sm, s>>>(rhs, sol, b1, b2, b3, m, n, work);
   return cudaGetLastError();
@@ -194,7 +194,10 @@ extern "C" int vr_solve_lap_thom(const double *rhs, double *sol, const double *a
 // corrupt each other's results, so such calls must be ordered, e.g. on one
 // stream.  The array's address is looked up once per device on the first call
 // (cudaGetSymbolAddress), which may load the module; make that first call
-// before any stream capture.
+// before any stream capture.  The address stays cached for the life of the
+// process: after cudaDeviceReset (or anything else that destroys the device's
+// primary context) the module may load at another address, and this entry
+// point must not be called on that device again.
 static __device__ __align__(256) double g_thom_scratch[VR_THOM_NOALLOC_MAX];
 
 namespace {
@@ -217,9 +220,15 @@ extern "C" int vr_solve_lap_thom_noalloc(const double *rhs, double *sol, const d
     gamm = static_cast<double *>(addr);
     g_thom_scratch_ptr[dev].store(gamm, std::memory_order_release);
   }
+  // cudaLaunchKernel returns the error of this launch alone; an error that an
+  // earlier, unrelated launch left pending on the thread is neither reported
+  // here nor cleared
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
-  k_thomas<<<(nbatch + 127) / 128, 128, 0, s>>>(rhs, sol, aa, bb, cc, gamm, n, nbatch);
-  return cudaGetLastError() == cudaSuccess ? VR_OK : VR_ERR_CUDA;
+  int n_ = n, nb_ = nbatch;
+  void *args[] = {(void *)&rhs, (void *)&sol, (void *)&aa, (void *)&bb, (void *)&cc, (void *)&gamm,
+                  (void *)&n_, (void *)&nb_};
+  cudaError_t e = cudaLaunchKernel((const void *)k_thomas, dim3((nbatch + 127) / 128), dim3(128), args, 0, s);
+  return e == cudaSuccess ? VR_OK : VR_ERR_CUDA;
 }
 
 extern "C" int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
