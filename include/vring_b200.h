@@ -275,6 +275,98 @@ VR_API int vr_solve_lap_thom(const double *rhs, double *sol, const double *aa, c
 VR_API int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
                        const double *b3, int32_t m, int32_t n, int32_t nbatch);
 
+/* ---- axisymmetric pressure solves with Krylov methods (Ntheta = 1) -------- */
+/* No reference counterpart: the reference solves the pressure directly
+ * (poisson_solve.F90:140-179, 270-323).  The operator is the reference's at
+ * Ntheta = 1 -- K phi = -(1/r)(r phi_r)_r - phi_zz on cell centres, Neumann on
+ * the axis, the wall and both z ends, and the Dirichlet wall closure of the
+ * (m, kz) = (0, 0) mode (poisson_solve.F90:305-317) applied to the z mean --
+ * written as conservative finite volumes on radial faces that may be
+ * stretched (the reference mesh is uniform, mesh_tools.F90:325-330; on a
+ * uniform mesh the rows equal poisson.F90:379-381).  Vectors hold nr*nz
+ * doubles, r fastest (index j + nr k).  CG and Jacobi-CG iterate on the
+ * symmetric form S x = V f (V = cell volume / 2 pi), BiCGSTAB on K x = f, and
+ * the learned form is a flexible CG whose preconditioner is a vr_unet. */
+typedef struct vr_k2d vr_k2d;
+typedef struct vr_k2d_desc {
+  int32_t abi_version;  /* VR_ABI_VERSION                                     */
+  int32_t nr, nz;       /* cells in r and z                                   */
+  double zmax;          /* z in [0, zmax], uniform                            */
+  const double *faces;  /* nr+1 radial faces (host), 0 = faces[0] < ... = rmax */
+  int32_t device;       /* CUDA device ordinal                                */
+  int32_t flags;        /* reserved, 0                                        */
+} vr_k2d_desc;
+enum vr_krylov {
+  VR_KRYLOV_CG = 0,           /* plain CG on S x = V f (the judge)            */
+  VR_KRYLOV_PCG_JACOBI = 1,   /* CG with the inverse diagonal of S            */
+  VR_KRYLOV_BICGSTAB = 2,     /* BiCGSTAB on K x = f                          */
+  VR_KRYLOV_FCG_LEARNED = 3   /* flexible CG, preconditioner = the vr_unet set
+                                 with vr_k2d_set_preconditioner               */
+};
+VR_API int vr_k2d_create(const vr_k2d_desc *desc, vr_k2d **out);
+VR_API int vr_k2d_destroy(vr_k2d *k);
+VR_API const char *vr_k2d_last_error(const vr_k2d *k);
+/* nr, nz and the nr+1 faces (any pointer may be NULL) */
+VR_API int vr_k2d_info(const vr_k2d *k, int32_t *nr, int32_t *nz, double *faces);
+/* y = K x on host arrays; the _dev form takes device arrays and applies S
+ * instead when symmetric != 0 */
+VR_API int vr_k2d_apply(vr_k2d *k, const double *x, double *y);
+VR_API int vr_k2d_apply_dev(vr_k2d *k, const double *x, double *y, int32_t symmetric);
+/* K x = f by the direct method (z DCT-II, a radial tridiagonal per z mode,
+ * DCT-III): the reference's fftp solve at Ntheta = 1 on these faces */
+VR_API int vr_k2d_direct(vr_k2d *k, const double *f, double *x);
+VR_API int vr_k2d_direct_dev(vr_k2d *k, const double *f, double *x);
+/* Krylov solve of K x = f to ||b - A x|| <= tol ||b|| (b, A the form the method
+ * iterates on); x holds the initial guess on entry and the solution on
+ * return.  At most maxit iterations (CG and BiCGSTAB run in chunks of 32, so
+ * up to 31 more may run before the cap is seen).  *iters, *relres (true
+ * residual of the returned x) and, for the host form, *ms (device time of the
+ * solve) may be NULL. */
+VR_API int vr_k2d_solve(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,
+                        int32_t *iters, double *relres, double *ms);
+VR_API int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,
+                            int32_t *iters, double *relres);
+
+/* ---- the learned preconditioner: a 4-level U-Net (no reference counterpart)
+ * Input and output are one channel on the nr x nz grid of a vr_k2d (r fastest);
+ * levels l = 0..3 run on (nr/2^l) x (nz/2^l) with ch[l] channels: two 3x3
+ * convolutions per level on the way down (2x2 average pooling between levels),
+ * nearest-neighbour upsampling, concatenation with the level's skip tensor and
+ * two 3x3 convolutions per level on the way up, then a 1x1 convolution to one
+ * channel.  No biases and identity activations, so the network is a linear
+ * map (a valid preconditioner for the flexible CG).  Weights are BF16 (an FP32
+ * master copy is kept for training), activations BF16, every sum accumulates
+ * in FP32.  nr and nz must be multiples of 8; ch[l] multiples of 8, <= 128. */
+typedef struct vr_unet vr_unet;
+typedef struct vr_unet_desc {
+  int32_t abi_version;
+  int32_t nr, nz;
+  int32_t ch[4];
+  int32_t device;
+  int32_t flags;  /* reserved, 0 */
+} vr_unet_desc;
+VR_API int vr_unet_create(const vr_unet_desc *desc, uint64_t seed, vr_unet **out);
+VR_API int vr_unet_destroy(vr_unet *u);
+VR_API const char *vr_unet_last_error(const vr_unet *u);
+VR_API int vr_unet_nparams(const vr_unet *u, int64_t *n);
+/* FP32 master weights (host), in the layer order of the header comment; each
+ * 3x3 layer is [cout][3 (dr)][3 (dz)][cin], the head [cin] */
+VR_API int vr_unet_get_params(const vr_unet *u, float *w);
+VR_API int vr_unet_set_params(vr_unet *u, const float *w);
+/* y = N(x) on host arrays of nr*nz doubles (x is scaled to unit RMS before the
+ * network and the output scaled back, so N is applied as a homogeneous map) */
+VR_API int vr_unet_forward(vr_unet *u, const double *x, double *y);
+/* gradients of L = sum(g * N(x)) for the gradient check: dL/dw (FP32, host,
+ * nparams) and dL/dx (host, nr*nz); the unit-RMS scaling is not applied */
+VR_API int vr_unet_backward(vr_unet *u, const double *x, const double *g, float *dw, double *dx);
+/* One Adam step on a batch of nb residual pairs resident on the device:
+ * r (nb x nr*nz, S-form residuals) with loss
+ * L = mean_b ||S N(r_b) - r_b||^2 / ||r_b||^2 (S of the vr_k2d);
+ * *loss receives L before the step (may be NULL). */
+VR_API int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *r_dev, int32_t nb, float lr, double *loss);
+/* make the network the preconditioner of VR_KRYLOV_FCG_LEARNED (NULL clears) */
+VR_API int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *u);
+
 /* No counterpart in the reference: solve_lap_thom on device arrays that
  * allocates nothing.  rhs, sol, aa, bb, cc are device pointers of the current
  * device (n * nbatch doubles each, the layout of vr_solve_lap_thom); the work

@@ -1,0 +1,113 @@
+"""GPU Krylov solves of the axisymmetric pressure problem (vr_k2d_*) against
+the CPU restatement (oracle/krylov2d.py) and the reference's own direct
+solve at Ntheta = 1 (the oracle's laplace_solve).
+
+Tolerances: the operator and the direct solve to 1e-12 of the scale; every
+Krylov method to a relative residual of 1e-10 in its own form, and its answer
+to 1e-8 of the direct solve's scale (the residual bound does not bound the
+error of an ill-conditioned system more tightly; the measured agreement is
+printed)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _ring_rhs(ax, seed=0):
+    rng = np.random.default_rng(seed)
+    R, Z = np.meshgrid(ax.rm, (np.arange(ax.nz) + 0.5) * ax.dz, indexing="ij")
+    p = -np.exp(-((R - 1.0) ** 2 + (Z - 5.0) ** 2) / 0.04) + 1e-3 * rng.standard_normal((ax.nr, ax.nz))
+    return ax.apply_K(p)
+
+
+def test_operator_and_direct_solve_match_oracle():
+    import vring_b200 as V
+    from oracle import krylov2d as K
+    nr, nz = 96, 160
+    faces = K.stretched_faces(nr, 5.0)
+    ax = K.Axisym(faces, nz, 15.0)
+    k = V.K2d(faces, nz, 15.0)
+    x = np.random.default_rng(3).standard_normal((nr, nz))
+    y = k.apply(x)
+    assert np.abs(y - ax.apply_K(x)).max() <= 1e-12 * np.abs(ax.apply_K(x)).max()
+    f = _ring_rhs(ax)
+    xd = k.direct(f)
+    xo = ax.solve_direct(f)
+    assert np.abs(xd - xo).max() <= 1e-12 * np.abs(xo).max()
+    k.close()
+
+
+@pytest.mark.parametrize("method", ["cg", "pcg", "bicgstab"])
+def test_krylov_converges_to_direct_solve_stretched(method):
+    import vring_b200 as V
+    from oracle import krylov2d as K
+    nr, nz = 128, 256
+    faces = K.stretched_faces(nr, 5.0)
+    ax = K.Axisym(faces, nz, 15.0)
+    k = V.K2d(faces, nz, 15.0)
+    f = _ring_rhs(ax, 1)
+    x, it, rr, ms = k.solve(f, method, tol=1e-10)
+    xo = ax.solve_direct(f)
+    err = np.abs(x - xo).max() / np.abs(xo).max()
+    print("%s 128x256 stretched: %d iterations, relres %.2e, %.1f ms, max err vs direct %.2e"
+          % (method, it, rr, ms, err))
+    assert rr <= 1e-10
+    assert err <= 1e-8
+    # the same iteration count as the numpy restatement (deterministic sums)
+    if method in ("cg", "pcg"):
+        _, it_o, _ = ax.cg(f, 1e-10, jacobi=method == "pcg")
+        assert abs(it - it_o) <= max(3, it_o // 100), (it, it_o)
+    k.close()
+
+
+def test_vr2d_uniform_deck_matches_reference_direct_solve():
+    """512 x 1024 on r in [0, 5], z in [0, 15] (the VR2D deck's grid) with the
+    reference's uniform mesh: plain CG to 1e-10 against the reference's fftp
+    solve at Ntheta = 1 (the oracle's laplace_solve)."""
+    import vring_b200 as V
+    from oracle import krylov2d as K
+    from oracle import oracle as O
+    nr, nz = 512, 1024
+    faces = K.uniform_faces(nr, 5.0)
+    ax = K.Axisym(faces, nz, 15.0)
+    f = _ring_rhs(ax, 2)
+    o = O.Oracle(1, nr, nz, 5.0, 15.0, 1e-3, 2000.0)
+    o.field("rhs")[...] = f.reshape(1, nr, nz)
+    o.laplace_solve()
+    ref = o.field("dph")[0, 1:nr + 1, 1:nz + 1].copy()
+    k = V.K2d(faces, nz, 15.0)
+    for method in ("cg", "bicgstab"):
+        x, it, rr, ms = k.solve(f, method, tol=1e-10)
+        err = np.abs(x - ref).max() / np.abs(ref).max()
+        print("VR2D deck uniform 512x1024 %s: %d iterations, relres %.2e, %.1f ms, vs reference solve %.2e"
+              % (method, it, rr, ms, err))
+        assert rr <= 1e-10 and err <= 1e-8
+    xd = k.direct(f)
+    assert np.abs(xd - ref).max() <= 1e-11 * np.abs(ref).max()
+    k.close()
+
+
+def test_device_entry_points_and_iteration_cap():
+    import torch
+    import vring_b200 as V
+    from oracle import krylov2d as K
+    nr, nz = 64, 128
+    faces = K.stretched_faces(nr, 5.0)
+    ax = K.Axisym(faces, nz, 15.0)
+    k = V.K2d(faces, nz, 15.0)
+    f = _ring_rhs(ax, 4)
+    fd = torch.from_numpy(np.asfortranarray(f).ravel(order="F")).cuda()
+    xd = torch.zeros_like(fd)
+    torch.cuda.synchronize()
+    it, rr = k.solve_dev(fd.data_ptr(), xd.data_ptr(), "cg", tol=1e-10)
+    assert rr <= 1e-10
+    x2, it2, rr2, _ = k.solve(f, "cg", tol=1e-10)
+    assert it == it2
+    assert np.array_equal(xd.cpu().numpy().reshape(nr, nz, order="F"), x2)
+    # a cap below the needed count stops early without converging
+    _, it3, rr3, _ = k.solve(f, "cg", tol=1e-10, maxit=40)
+    assert 40 <= it3 < 40 + 32 and rr3 > 1e-10
+    # a converged warm start needs no iteration
+    _, it4, rr4, _ = k.solve(f, "cg", x0=x2, tol=1e-6)
+    assert it4 == 0
+    k.close()

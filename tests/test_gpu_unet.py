@@ -1,0 +1,105 @@
+"""The learned preconditioner's network (vr_unet_*): the GPU forward pass and
+gradients against the CPU restatement (oracle/unet_ref.py, FP64 with the
+same BF16 rounding points), training through the project's own kernels,
+and the trained network's effect on the VR2D Krylov solve.
+
+Tolerances: forward output and every gradient within 5e-3 relative L2 of the
+oracle's (the GPU accumulates in FP32; an FP32 sum that lands on the other
+side of a BF16 rounding boundary changes that element by one BF16 ulp,
+2^-8)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CH = (8, 16, 16, 24)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def test_forward_matches_oracle():
+    import vring_b200 as V
+    from oracle import unet_ref as U
+    nr, nz = 32, 64
+    net = V.UNet(nr, nz, CH, seed=5)
+    assert net.nparams == U.nparams(CH)
+    w = net.get_params()
+    x = np.random.default_rng(0).standard_normal((nr, nz))
+    s = np.sqrt(np.mean(x ** 2))
+    y = net.forward(x)
+    yo = s * U.forward(w, CH, x / s)
+    print("forward rel L2 vs oracle %.2e" % _rel(y, yo))
+    assert _rel(y, yo) <= 5e-3
+    # homogeneous: N(3 x) = 3 N(x)
+    assert _rel(net.forward(3 * x), 3 * y) <= 1e-12
+    net.close()
+
+
+def test_gradients_match_oracle():
+    import vring_b200 as V
+    from oracle import unet_ref as U
+    nr, nz = 32, 64
+    net = V.UNet(nr, nz, CH, seed=6)
+    w = net.get_params()
+    rng = np.random.default_rng(1)
+    x, g = rng.standard_normal((nr, nz)), rng.standard_normal((nr, nz))
+    dw, dx = net.backward(x, g)
+    dwo, dxo = U.backward(w, CH, x, g)
+    off = 0
+    for i, (ci, co, _) in enumerate(U.layers(CH) + [(CH[0], 1, 0)]):
+        n = ci * co * (9 if i < 14 else 1)
+        e = _rel(dw[off:off + n], dwo[off:off + n])
+        assert e <= 5e-3, (i, e)
+        off += n
+    print("dw rel L2 %.2e, dx rel L2 %.2e" % (_rel(dw, dwo), _rel(dx, dxo)))
+    assert _rel(dx, dxo) <= 5e-3
+    net.close()
+
+
+def test_training_reduces_the_loss():
+    import torch
+    import vring_b200 as V
+    from vring_b200 import learned as Lr
+    nr, nz = 64, 128
+    k = V.K2d(Lr.tanh_faces(nr), nz, 15.0)
+    net = V.UNet(nr, nz, CH, seed=7)
+    rng = np.random.default_rng(2)
+    r = torch.from_numpy(rng.standard_normal((4, nr * nz))).cuda()
+    torch.cuda.synchronize()
+    l0 = net.train_step(k, r.data_ptr(), 4, 3e-3)
+    for _ in range(30):
+        l1 = net.train_step(k, r.data_ptr(), 4, 3e-3)
+    print("loss %.4e -> %.4e" % (l0, l1))
+    assert np.isfinite(l1) and l1 < 0.5 * l0
+    net.close()
+    k.close()
+
+
+def test_learned_fcg_converges_to_the_same_field():
+    """The flexible CG with the (possibly untrained) network converges to the
+    plain CG's answer; with the committed trained weights it needs at least
+    3x fewer iterations than plain CG on the 512 x 1024 stretched grid."""
+    import vring_b200 as V
+    from vring_b200 import learned as Lr
+    trained = os.path.exists(Lr.WEIGHTS)
+    nr, nz = (Lr.NR, Lr.NZ) if trained else (64, 128)
+    k = V.K2d(Lr.tanh_faces(nr), nz, Lr.ZMAX)
+    net = V.UNet(nr, nz, Lr.CHANNELS, seed=1)
+    if trained:
+        Lr.load_weights(net)
+    seq = Lr.RingSequence(2, k.faces, nz, Lr.ZMAX)
+    f, p_prev, p = Lr.triple(k, seq, 500)
+    res = Lr.compare(k, net, f, x0=p_prev, tol=1e-10)
+    for m, (it, rr, ms, x) in res.items():
+        print("%s: %d iterations, relres %.2e, %.1f ms, max|x - direct| / max|direct| %.2e"
+              % (m, it, rr, ms, np.abs(x - p).max() / np.abs(p).max()))
+        assert rr <= 1e-10
+        assert np.abs(x - p).max() <= 1e-8 * np.abs(p).max()
+    if trained:
+        assert res["cg"][0] >= 3 * res["learned"][0]
+    net.close()
+    k.close()

@@ -48,6 +48,19 @@ class Desc(C.Structure):
                 ("device", C.c_int32), ("flags", C.c_int32)]
 
 
+class K2dDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("nr", C.c_int32), ("nz", C.c_int32), ("zmax", C.c_double),
+                ("faces", C.c_void_p), ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+class UnetDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("nr", C.c_int32), ("nz", C.c_int32), ("ch", C.c_int32 * 4),
+                ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+KRYLOV = {"cg": 0, "pcg": 1, "jacobi": 1, "bicgstab": 2, "fcg": 3, "learned": 3}
+
+
 def declared_symbols(header: str = HEADER) -> list[str]:
     """Every entry point ``include/vring_b200.h`` declares with VR_API."""
     txt = open(header).read()
@@ -113,6 +126,28 @@ def lib():
         L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
         L.vr_solve_lap_thom_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, i32, vp]
+        L.vr_k2d_create.argtypes = [C.POINTER(K2dDesc), C.POINTER(vp)]
+        L.vr_k2d_destroy.argtypes = [vp]
+        L.vr_k2d_last_error.restype = C.c_char_p
+        L.vr_k2d_last_error.argtypes = [vp]
+        L.vr_k2d_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), vp]
+        L.vr_k2d_apply.argtypes = [vp, vp, vp]
+        L.vr_k2d_apply_dev.argtypes = [vp, vp, vp, i32]
+        L.vr_k2d_direct.argtypes = [vp, vp, vp]
+        L.vr_k2d_direct_dev.argtypes = [vp, vp, vp]
+        L.vr_k2d_solve.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp), C.POINTER(dp)]
+        L.vr_k2d_solve_dev.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp)]
+        L.vr_k2d_set_preconditioner.argtypes = [vp, vp]
+        L.vr_unet_create.argtypes = [C.POINTER(UnetDesc), C.c_uint64, C.POINTER(vp)]
+        L.vr_unet_destroy.argtypes = [vp]
+        L.vr_unet_last_error.restype = C.c_char_p
+        L.vr_unet_last_error.argtypes = [vp]
+        L.vr_unet_nparams.argtypes = [vp, C.POINTER(i64)]
+        L.vr_unet_get_params.argtypes = [vp, vp]
+        L.vr_unet_set_params.argtypes = [vp, vp]
+        L.vr_unet_forward.argtypes = [vp, vp, vp]
+        L.vr_unet_backward.argtypes = [vp, vp, vp, vp, vp]
+        L.vr_unet_train_step.argtypes = [vp, vp, vp, i32, C.c_float, C.POINTER(dp)]
         _lib = L
     return _lib
 
@@ -439,3 +474,139 @@ def format_e16_8(x: float) -> str:
     if rc:
         raise VrError(rc, "vr_format_e16_8")
     return buf.value.decode()
+
+
+class K2d:
+    """The axisymmetric (Ntheta = 1) pressure operator on radial faces
+    ``faces`` (nr+1 values, 0 .. rmax) and nz uniform cells on [0, zmax], with
+    its GPU solvers (``vr_k2d_*``).  Host vectors are (nr, nz) arrays indexed
+    [j, k], stored r fastest."""
+
+    def __init__(self, faces, nz: int, zmax: float, device: int = 0):
+        self.faces = np.ascontiguousarray(faces, dtype=np.float64)
+        self.nr, self.nz, self.zmax = self.faces.size - 1, int(nz), float(zmax)
+        d = K2dDesc(VR_ABI_VERSION, self.nr, self.nz, self.zmax, self.faces.ctypes.data, device, 0)
+        self._h = C.c_void_p()
+        rc = lib().vr_k2d_create(C.byref(d), C.byref(self._h))
+        if rc:
+            raise VrError(rc, "vr_k2d_create")
+
+    def _chk(self, rc, what):
+        if rc:
+            raise VrError(rc, "%s: %s" % (what, (lib().vr_k2d_last_error(self._h) or b"").decode()))
+
+    def close(self):
+        if self._h:
+            lib().vr_k2d_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _vec(self, a):
+        return np.asfortranarray(np.asarray(a, dtype=np.float64).reshape(self.nr, self.nz, order="F"))
+
+    def apply(self, x) -> np.ndarray:
+        x = self._vec(x)
+        y = np.empty_like(x)
+        self._chk(lib().vr_k2d_apply(self._h, _p(x), _p(y)), "k2d_apply")
+        return y
+
+    def direct(self, f) -> np.ndarray:
+        f = self._vec(f)
+        x = np.empty_like(f)
+        self._chk(lib().vr_k2d_direct(self._h, _p(f), _p(x)), "k2d_direct")
+        return x
+
+    def solve(self, f, method="cg", x0=None, tol=1e-10, maxit=1000000):
+        """(x, iterations, relative residual, device ms)."""
+        f = self._vec(f)
+        x = np.zeros_like(f) if x0 is None else self._vec(x0).copy()
+        it, rr, ms = C.c_int32(), C.c_double(), C.c_double()
+        self._chk(lib().vr_k2d_solve(self._h, KRYLOV[method], _p(f), _p(x), tol, maxit, C.byref(it),
+                                     C.byref(rr), C.byref(ms)), "k2d_solve")
+        return x, it.value, rr.value, ms.value
+
+    def solve_dev(self, f_ptr: int, x_ptr: int, method="cg", tol=1e-10, maxit=1000000):
+        it, rr = C.c_int32(), C.c_double()
+        self._chk(lib().vr_k2d_solve_dev(self._h, KRYLOV[method], C.c_void_p(f_ptr), C.c_void_p(x_ptr), tol,
+                                         maxit, C.byref(it), C.byref(rr)), "k2d_solve_dev")
+        return it.value, rr.value
+
+    def direct_dev(self, f_ptr: int, x_ptr: int) -> None:
+        self._chk(lib().vr_k2d_direct_dev(self._h, C.c_void_p(f_ptr), C.c_void_p(x_ptr)), "k2d_direct_dev")
+
+    def apply_dev(self, x_ptr: int, y_ptr: int, symmetric: bool = False) -> None:
+        self._chk(lib().vr_k2d_apply_dev(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), 1 if symmetric else 0),
+                  "k2d_apply_dev")
+
+    def set_preconditioner(self, net) -> None:
+        self._chk(lib().vr_k2d_set_preconditioner(self._h, net._h if net is not None else None),
+                  "k2d_set_preconditioner")
+
+
+class UNet:
+    """The learned preconditioner (``vr_unet_*``): a 4-level linear U-Net with
+    BF16 weights and activations and FP32 accumulation on an (nr, nz) grid."""
+
+    def __init__(self, nr: int, nz: int, ch=(16, 32, 48, 64), seed: int = 0, device: int = 0):
+        self.nr, self.nz, self.ch = int(nr), int(nz), tuple(int(c) for c in ch)
+        d = UnetDesc(VR_ABI_VERSION, self.nr, self.nz, (C.c_int32 * 4)(*self.ch), device, 0)
+        self._h = C.c_void_p()
+        rc = lib().vr_unet_create(C.byref(d), seed, C.byref(self._h))
+        if rc:
+            raise VrError(rc, "vr_unet_create")
+        n = C.c_int64()
+        self._chk(lib().vr_unet_nparams(self._h, C.byref(n)), "unet_nparams")
+        self.nparams = n.value
+
+    def _chk(self, rc, what):
+        if rc:
+            raise VrError(rc, "%s: %s" % (what, (lib().vr_unet_last_error(self._h) or b"").decode()))
+
+    def close(self):
+        if self._h:
+            lib().vr_unet_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        w = np.empty(self.nparams, dtype=np.float32)
+        self._chk(lib().vr_unet_get_params(self._h, _p(w)), "unet_get_params")
+        return w
+
+    def set_params(self, w) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        assert w.size == self.nparams
+        self._chk(lib().vr_unet_set_params(self._h, _p(w)), "unet_set_params")
+
+    def _vec(self, a):
+        return np.asfortranarray(np.asarray(a, dtype=np.float64).reshape(self.nr, self.nz, order="F"))
+
+    def forward(self, x) -> np.ndarray:
+        x = self._vec(x)
+        y = np.empty_like(x)
+        self._chk(lib().vr_unet_forward(self._h, _p(x), _p(y)), "unet_forward")
+        return y
+
+    def backward(self, x, g):
+        """(dL/dw float32 (nparams,), dL/dx (nr, nz)) of L = sum(g * N(x))."""
+        x, g = self._vec(x), self._vec(g)
+        dw = np.empty(self.nparams, dtype=np.float32)
+        dx = np.empty_like(x)
+        self._chk(lib().vr_unet_backward(self._h, _p(x), _p(g), _p(dw), _p(dx)), "unet_backward")
+        return dw, dx
+
+    def train_step(self, k2d: K2d, r_ptr: int, nb: int, lr: float) -> float:
+        loss = C.c_double()
+        self._chk(lib().vr_unet_train_step(self._h, k2d._h, C.c_void_p(r_ptr), nb, lr, C.byref(loss)),
+                  "unet_train_step")
+        return loss.value

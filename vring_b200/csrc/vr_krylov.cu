@@ -1,0 +1,956 @@
+// vr_krylov.cu -- the axisymmetric (Ntheta = 1) pressure problem on a
+// radially stretched grid, solved on the GPU by Krylov methods: plain CG and
+// diagonally preconditioned CG on the symmetric form S x = V f, BiCGSTAB on
+// the unsymmetric form K x = f, and a flexible CG that applies a learned
+// preconditioner (vr_unet.cu).  A direct solve (z DCT-II, one radial
+// tridiagonal per z mode, DCT-III: the reference's fftp method at Ntheta = 1,
+// poisson_solve.F90:140-179, 270-323, generalised to stretched radial faces)
+// judges the Krylov answers and generates training pairs.
+//
+// Operator (cell centres (rm_j, zm_k), vectors stored r fastest, i = j + nr k):
+//   S x = aw_j (x - x_{j-1}) + ae_j (x - x_{j+1}) + az_j (2x - x_{k-1} - x_{k+1})
+//         + [j = nr-1] gam mean_k x(nr-1, k)
+// with missing neighbours dropped (Neumann on the axis, the wall and both z
+// ends), aw_j = rc_j dz / (rm_j - rm_{j-1}), ae_j = rc_{j+1} dz / (rm_{j+1} -
+// rm_j), az_j = rm_j dr_j / dz, V_j = rm_j dr_j dz and gam = 2 rc_{nr+1} dz /
+// dr_nr: the Dirichlet closure that poisson_solve.F90:305-317 gives the
+// (m, kz) = (0, 0) mode, written for the z mean in physical space.  K = S / V.
+// On a uniform grid these rows are the reference's aa/bb/cc
+// (poisson.F90:379-381).
+//
+// Every reduction is deterministic: vector kernels write one partial sum per
+// block, and a one-block kernel adds the partials in a fixed order into the
+// scalars the next vector kernel reads.  Iterations are issued in chunks
+// captured as CUDA graphs; a device flag set at convergence turns the rest of
+// a chunk into early returns, and the host reads the flag between chunks.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "vr_internal.cuh"
+#include "vr_learned.cuh"
+
+namespace vr {
+
+constexpr int kK2dThreads = 256;
+constexpr int kK2dMaxBlocks = 1024;
+constexpr int kK2dChunk = 32;  // iterations per captured graph (even)
+
+// scalar slots
+enum K2dScal {
+  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_PQ, SC_N
+};
+// partial-sum slots
+enum K2dPart { PT_A = 0, PT_B, PT_C, PT_D, PT_N };
+// flags: [0] done, [1] iterations
+}  // namespace vr
+
+struct vr_k2d {
+  int nr = 0, nz = 0, n = 0, dev = 0, nb = 0;
+  cudaStream_t stream = nullptr;
+  double *coef = nullptr;  // aw, ae, az, vol, dinv (per j; dinv per cell)
+  double gam = 0.0;
+  double *vec[12] = {};
+  double *part = nullptr;   // PT_N x kK2dMaxBlocks
+  double *sc = nullptr;     // SC_N
+  int *flags = nullptr;     // done, iterations
+  // direct solve: forward / inverse z transforms (nz x nz, row-major [kz][k]
+  // and [k][kz]) and the radial Thomas factorisation per z mode
+  double *dct_f = nullptr, *dct_i = nullptr, *tlo = nullptr, *tup = nullptr, *tib = nullptr;
+  double *tmp = nullptr;
+  cudaGraphExec_t graph[4] = {};
+  bool graph_ok[4] = {};
+  std::string err;
+  const vr_unet *net = nullptr;  // learned preconditioner for VR_KRYLOV_FCG_LEARNED
+  std::vector<double> h_faces;
+};
+
+namespace vr {
+
+struct K2dOp {
+  int nr, nz, n;
+  const double *aw, *ae, *az, *vol, *dinv;
+  double gam;
+};
+
+static K2dOp op_of(const vr_k2d *k) {
+  K2dOp o;
+  o.nr = k->nr;
+  o.nz = k->nz;
+  o.n = k->n;
+  o.aw = k->coef;
+  o.ae = k->coef + k->nr;
+  o.az = k->coef + 2 * k->nr;
+  o.vol = k->coef + 3 * k->nr;
+  o.dinv = k->coef + 4 * k->nr;
+  o.gam = k->gam;
+  return o;
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sh[i];
+  return s;  // valid in thread 0
+}
+
+// mean over k of x(nr-1, k), computed by every block in the same order
+__device__ double last_row_mean(const K2dOp &o, const double *__restrict__ x, double *sh) {
+  double v = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) v += x[(o.nr - 1) + (size_t)o.nr * k];
+  double s = block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[32] = s / o.nz;
+  __syncthreads();
+  return sh[32];
+}
+
+__device__ __forceinline__ double apply_S_at(const K2dOp &o, const double *__restrict__ x, int i, double mean) {
+  const int j = i % o.nr, k = i / o.nr;
+  const double xc = x[i];
+  double y = 0.0;
+  if (j > 0) y += o.aw[j] * (xc - x[i - 1]);
+  if (j < o.nr - 1) y += o.ae[j] * (xc - x[i + 1]);
+  else y += o.gam * mean;
+  const double az = o.az[j];
+  if (k > 0) y += az * (xc - x[i - o.nr]);
+  if (k < o.nz - 1) y += az * (xc - x[i + o.nr]);
+  return y;
+}
+
+// y = S x (form 0) or K x (form 1); with part, part[b] = sum over the block of w . y
+__global__ void __launch_bounds__(kK2dThreads) k2d_apply(K2dOp o, const double *__restrict__ x, double *__restrict__ y,
+                                                       int form, const double *__restrict__ w, double *part,
+                                                       const int *flags) {
+  __shared__ double sh[40];
+  if (flags && flags[0]) return;
+  const double mean = last_row_mean(o, x, sh);
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    double v = apply_S_at(o, x, i, mean);
+    if (form) v /= o.vol[i % o.nr];
+    y[i] = v;
+    if (w) acc += w[i] * v;
+  }
+  if (part) {
+    double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+  }
+}
+
+// generic fused vector update: out = a*X + b*Y (+ partials of two dot products)
+// used for initialisation steps
+__global__ void __launch_bounds__(kK2dThreads) k2d_axpby(int n, double a, const double *__restrict__ X, double b,
+                                                       const double *__restrict__ Y, double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = a * X[i] + (Y ? b * Y[i] : 0.0);
+}
+
+__global__ void __launch_bounds__(kK2dThreads) k2d_dots(int n, const double *__restrict__ a1,
+                                                      const double *__restrict__ b1, const double *__restrict__ a2,
+                                                      const double *__restrict__ b2, double *part1, double *part2) {
+  __shared__ double sh[40];
+  double s1 = 0.0, s2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    s1 += a1[i] * b1[i];
+    if (a2) s2 += a2[i] * b2[i];
+  }
+  double t = block_sum(s1, sh);
+  if (threadIdx.x == 0) part1[blockIdx.x] = t;
+  if (a2) {
+    __syncthreads();
+    t = block_sum(s2, sh);
+    if (threadIdx.x == 0) part2[blockIdx.x] = t;
+  }
+}
+
+// b = V f (or f for the unsymmetric form), element-wise scale by the cell volume
+__global__ void k2d_scale_vol(K2dOp o, const double *__restrict__ f, double *__restrict__ b, int inv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double v = o.vol[i % o.nr];
+    b[i] = inv ? f[i] / v : f[i] * v;
+  }
+}
+
+__device__ __forceinline__ double sum_part(const double *p, int nb, double *sh) {
+  // one block: fixed-order sums of a strided set, then a fixed tree
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += p[i];
+  double s = block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[33] = s;
+  __syncthreads();
+  return sh[33];
+}
+
+// one-block scalar steps
+enum K2dScalarOp {
+  SO_CG_INIT = 0,   // bb, rz, rr from partials A (b.b), B (r.z), C (r.r)
+  SO_CG_ALPHA,      // alpha = rz / (p.q) [A]
+  SO_CG_BETA,       // rz_new [B], rr [C]: beta, convergence
+  SO_BI_INIT,       // bb [A], rho_new = rh.r [B], rr [C]
+  SO_BI_BETA,       // beta from rho_new, rho, alpha, omega
+  SO_BI_ALPHA,      // alpha = rho / rh.v [A]
+  SO_BI_OMEGA,      // omega = t.s [A] / t.t [B]
+  SO_BI_CONV,       // rho_new = rh.r [A], rr [B]
+  SO_FCG_BETA,      // beta = z.q_old [A] / pq_old
+  SO_FCG_ALPHA,     // alpha = p.r [A] / p.q [B]; stores pq
+  SO_FCG_CONV,      // rr [A]
+  SO_NORM,          // rr [A] only (sc[SC_RR])
+  SO_NORM_BB        // bb [A] only (sc[SC_BB])
+};
+
+__global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, int nb, double *sc, int *flags) {
+  __shared__ double sh[40];
+  if (flags[0] && op != SO_NORM && op != SO_NORM_BB && op != SO_CG_INIT && op != SO_BI_INIT) return;
+  const double *pA = part, *pB = part + kK2dMaxBlocks, *pC = part + 2 * kK2dMaxBlocks;
+  double a = sum_part(pA, nb, sh);
+  double b = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT || op == SO_BI_OMEGA ||
+              op == SO_BI_CONV || op == SO_FCG_ALPHA)
+                 ? sum_part(pB, nb, sh)
+                 : 0.0;
+  double c = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT) ? sum_part(pC, nb, sh) : 0.0;
+  if (threadIdx.x != 0) return;
+  switch (op) {
+    case SO_CG_INIT:
+      sc[SC_BB] = a;
+      sc[SC_RZ] = b;
+      sc[SC_RR] = c;
+      flags[0] = (c <= sc[SC_TOL2] * a) ? 1 : 0;
+      flags[1] = 0;
+      break;
+    case SO_CG_ALPHA:
+      sc[SC_ALPHA] = sc[SC_RZ] / a;
+      break;
+    case SO_CG_BETA:
+      sc[SC_BETA] = b / sc[SC_RZ];
+      sc[SC_RZ] = b;
+      sc[SC_RR] = c;
+      flags[1] += 1;
+      if (c <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
+      break;
+    case SO_BI_INIT:
+      sc[SC_BB] = a;
+      sc[SC_RHO_NEW] = b;
+      sc[SC_RR] = c;
+      sc[SC_RHO] = 1.0;
+      sc[SC_ALPHA] = 1.0;
+      sc[SC_OMEGA] = 1.0;
+      flags[0] = (c <= sc[SC_TOL2] * a) ? 1 : 0;
+      flags[1] = 0;
+      break;
+    case SO_BI_BETA:
+      sc[SC_BETA] = (sc[SC_RHO_NEW] / sc[SC_RHO]) * (sc[SC_ALPHA] / sc[SC_OMEGA]);
+      sc[SC_RHO] = sc[SC_RHO_NEW];
+      break;
+    case SO_BI_ALPHA:
+      sc[SC_ALPHA] = sc[SC_RHO] / a;
+      break;
+    case SO_BI_OMEGA:
+      sc[SC_OMEGA] = b != 0.0 ? a / b : 0.0;
+      break;
+    case SO_BI_CONV:
+      sc[SC_RHO_NEW] = a;
+      sc[SC_RR] = b;
+      flags[1] += 1;
+      if (b <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
+      break;
+    case SO_FCG_BETA:
+      sc[SC_BETA] = sc[SC_PQ] != 0.0 ? a / sc[SC_PQ] : 0.0;
+      break;
+    case SO_FCG_ALPHA:
+      sc[SC_ALPHA] = a / b;
+      sc[SC_PQ] = b;
+      break;
+    case SO_FCG_CONV:
+      sc[SC_RR] = a;
+      flags[1] += 1;
+      if (a <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
+      break;
+    case SO_NORM:
+      sc[SC_RR] = a;
+      break;
+    case SO_NORM_BB:
+      sc[SC_BB] = a;
+      break;
+  }
+  // iteration cap (flags[2]): stop as not converged
+  if ((op == SO_CG_BETA || op == SO_BI_CONV || op == SO_FCG_CONV) && !flags[0] && flags[1] >= flags[2]) flags[0] = 2;
+}
+
+// CG: x += alpha p; r -= alpha q; z = M r (identity or Jacobi); partials r.z [B], r.r [C]
+__global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, double *__restrict__ x,
+                                                       double *__restrict__ r, double *__restrict__ z,
+                                                       const double *__restrict__ p, const double *__restrict__ q,
+                                                       const double *sc, double *part, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double al = sc[SC_ALPHA];
+  double rz = 0.0, rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    x[i] += al * p[i];
+    const double ri = r[i] - al * q[i];
+    r[i] = ri;
+    const double zi = jacobi ? ri * o.dinv[i] : ri;
+    if (jacobi) z[i] = zi;
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  double s = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = s;
+  __syncthreads();
+  s = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[2 * kK2dMaxBlocks + blockIdx.x] = s;
+}
+
+// p = z + beta p  (runs only while not converged)
+__global__ void __launch_bounds__(kK2dThreads) k2d_cg_p(int n, double *__restrict__ p, const double *__restrict__ z,
+                                                      const double *sc, const int *flags) {
+  if (flags[0]) return;
+  const double be = sc[SC_BETA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + be * p[i];
+}
+
+// BiCGSTAB p = r + beta (p - omega v)
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_p(int n, double *__restrict__ p, const double *__restrict__ r,
+                                                      const double *__restrict__ v, const double *sc,
+                                                      const int *flags) {
+  if (flags[0]) return;
+  const double be = sc[SC_BETA], om = sc[SC_OMEGA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = r[i] + be * (p[i] - om * v[i]);
+}
+
+// s = r - alpha v
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_s(int n, double *__restrict__ s, const double *__restrict__ r,
+                                                      const double *__restrict__ v, const double *sc,
+                                                      const int *flags) {
+  if (flags[0]) return;
+  const double al = sc[SC_ALPHA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s[i] = r[i] - al * v[i];
+}
+
+// x += alpha p + omega s; r = s - omega t; partials rh.r [A], r.r [B]
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr(int n, double *__restrict__ x, double *__restrict__ r,
+                                                       const double *__restrict__ p, const double *__restrict__ s,
+                                                       const double *__restrict__ t, const double *__restrict__ rh,
+                                                       const double *sc, double *part, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double al = sc[SC_ALPHA], om = sc[SC_OMEGA];
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += al * p[i] + om * s[i];
+    const double ri = s[i] - om * t[i];
+    r[i] = ri;
+    a += rh[i] * ri;
+    b += ri * ri;
+  }
+  double t1 = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t1;
+  __syncthreads();
+  t1 = block_sum(b, sh);
+  if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = t1;
+}
+
+// FCG: p = z - beta p
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_p(int n, double *__restrict__ p, const double *__restrict__ z,
+                                                       const double *sc, const int *flags, int first) {
+  if (flags[0]) return;
+  const double be = first ? 0.0 : sc[SC_BETA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] - be * p[i];
+}
+
+// FCG: x += alpha p; r -= alpha q; partial r.r [A]
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_xr(int n, double *__restrict__ x, double *__restrict__ r,
+                                                        const double *__restrict__ p, const double *__restrict__ q,
+                                                        const double *sc, double *part, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double al = sc[SC_ALPHA];
+  double rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += al * p[i];
+    const double ri = r[i] - al * q[i];
+    r[i] = ri;
+    rr += ri * ri;
+  }
+  double s = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// ---- direct solve -----------------------------------------------------------
+// C[row-major m x n] = A (m x k, column-major: A[i + m l]) times B^T where B is
+// row-major (n x k): C(i, c) = sum_l A(i, l) B(c, l); C stored column-major
+// (i + m c).  64 x 64 tiles, 16 x 16 threads, 4 x 4 outputs per thread.
+__global__ void __launch_bounds__(256) k2d_gemm_abt(int m, int n, int kk, const double *__restrict__ A,
+                                                  const double *__restrict__ B, double *__restrict__ C) {
+  __shared__ double sa[16][65], sb[16][65];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int i0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  double acc[4][4] = {};
+  for (int l0 = 0; l0 < kk; l0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      const int l = e / 64, ii = e % 64;
+      const int gi = i0 + ii, gl = l0 + l;
+      sa[l][ii] = (gi < m && gl < kk) ? A[gi + (size_t)m * gl] : 0.0;
+    }
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      const int cc = e / 16, l = e % 16;
+      const int gc = c0 + cc, gl = l0 + l;
+      sb[l][cc] = (gc < n && gl < kk) ? B[(size_t)gc * kk + gl] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < 16; l++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        a[u] = sa[l][tx + 16 * u];
+        b[u] = sb[l][ty + 16 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int gi = i0 + tx + 16 * u, gc = c0 + ty + 16 * v;
+      if (gi < m && gc < n) C[gi + (size_t)m * gc] = acc[u][v];
+    }
+}
+
+// one thread per z mode: the radial tridiagonal of that mode (contiguous in j)
+__global__ void k2d_radial_thomas(int nr, int nz, double *__restrict__ a, const double *__restrict__ lo,
+                                  const double *__restrict__ up, const double *__restrict__ ib) {
+  const int kz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kz >= nz) return;
+  double *x = a + (size_t)nr * kz;
+  const double *piv = ib + (size_t)nr * kz;
+  double g = x[0] * piv[0];
+  x[0] = g;
+  for (int j = 1; j < nr; j++) {
+    g = (x[j] - lo[j] * g) * piv[j];
+    x[j] = g;
+  }
+  double xn = x[nr - 1];
+  for (int j = nr - 2; j >= 0; j--) {
+    xn = x[j] - up[j] * piv[j] * xn;
+    x[j] = xn;
+  }
+}
+
+}  // namespace vr
+
+using namespace vr;
+
+static int k2d_err(vr_k2d *k, int code, const std::string &m) {
+  if (k) k->err = m;
+  return code;
+}
+#define K2D_CUDA(k, call)                                                                     \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return k2d_err((k), VR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+enum { V_B = 0, V_X, V_R, V_P, V_Q, V_Z, V_RH, V_V, V_S, V_T, V_W1, V_W2 };
+
+extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
+  if (!d || !out) return VR_ERR_ARG;
+  *out = nullptr;
+  if (d->abi_version != VR_ABI_VERSION || !d->faces) return VR_ERR_DESC;
+  const int nr = d->nr, nz = d->nz;
+  if (nr < 4 || nz < 4 || nr > 8192 || nz > 8192 || (int64_t)nr * nz > ((int64_t)1 << 26) || !(d->zmax > 0))
+    return VR_ERR_DESC;
+  const double *f = d->faces;
+  if (f[0] != 0.0) return VR_ERR_DESC;
+  for (int j = 0; j < nr; j++)
+    if (!(f[j + 1] > f[j])) return VR_ERR_DESC;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || d->device < 0 || d->device >= ndev)
+    return VR_ERR_NODEVICE;
+  vr_k2d *k = new (std::nothrow) vr_k2d();
+  if (!k) return VR_ERR_OOM;
+  auto fail = [&](int code) {
+    vr_k2d_destroy(k);
+    return code;
+  };
+  k->nr = nr;
+  k->nz = nz;
+  k->n = nr * nz;
+  k->dev = d->device;
+  k->h_faces.assign(f, f + nr + 1);
+  if (cudaSetDevice(k->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&k->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, k->dev);
+  k->nb = std::min(kK2dMaxBlocks, std::max(1, std::min(2 * nsm, (k->n + kK2dThreads - 1) / kK2dThreads)));
+  // host coefficients
+  const double dz = d->zmax / nz;
+  std::vector<double> rm(nr), dr(nr), aw(nr, 0.0), ae(nr, 0.0), az(nr), vol(nr);
+  for (int j = 0; j < nr; j++) {
+    dr[j] = f[j + 1] - f[j];
+    rm[j] = 0.5 * (f[j] + f[j + 1]);
+    az[j] = rm[j] * dr[j] / dz;
+    vol[j] = rm[j] * dr[j] * dz;
+  }
+  for (int j = 1; j < nr; j++) {
+    const double h = rm[j] - rm[j - 1];
+    aw[j] = f[j] * dz / h;
+    ae[j - 1] = f[j] * dz / h;
+  }
+  k->gam = 2.0 * f[nr] * dz / dr[nr - 1];
+  std::vector<double> coef((size_t)4 * nr + (size_t)nr * nz);
+  for (int j = 0; j < nr; j++) {
+    coef[j] = aw[j];
+    coef[nr + j] = ae[j];
+    coef[2 * nr + j] = az[j];
+    coef[3 * nr + j] = vol[j];
+  }
+  for (int kk = 0; kk < nz; kk++)
+    for (int j = 0; j < nr; j++) {
+      double dg = aw[j] + ae[j] + (kk > 0 ? az[j] : 0.0) + (kk < nz - 1 ? az[j] : 0.0);
+      if (j == nr - 1) dg += k->gam / nz;
+      coef[4 * nr + j + (size_t)nr * kk] = 1.0 / dg;
+    }
+  // direct solve tables: DCT-II scaled 1/(2 nz) (REDFT10) and DCT-III (REDFT01)
+  const double pi = std::acos(-1.0);
+  std::vector<double> cf((size_t)nz * nz), ci((size_t)nz * nz);
+  for (int q = 0; q < nz; q++)
+    for (int kk = 0; kk < nz; kk++) {
+      const double c = std::cos(pi * q * (2.0 * kk + 1.0) / (2.0 * nz));
+      cf[(size_t)q * nz + kk] = c / nz;                 // [kz][k]
+      ci[(size_t)kk * nz + q] = q == 0 ? 1.0 : 2.0 * c;  // [k][kz]
+    }
+  // radial Thomas per z mode on K rows: lo = -aw/V, up = -ae/V
+  std::vector<double> lo(nr), up(nr), ib((size_t)nr * nz);
+  for (int j = 0; j < nr; j++) {
+    lo[j] = -aw[j] / vol[j];
+    up[j] = -ae[j] / vol[j];
+  }
+  for (int q = 0; q < nz; q++) {
+    const double wz = 2.0 / (dz * dz) * (1.0 - std::cos(q * pi / nz));
+    double prev_piv = 0.0;
+    for (int j = 0; j < nr; j++) {
+      double dg = (aw[j] + ae[j]) / vol[j] + wz;
+      if (q == 0 && j == nr - 1) dg += k->gam / vol[j];
+      double beta = j == 0 ? dg : dg - up[j - 1] * lo[j] * prev_piv;
+      prev_piv = 1.0 / beta;
+      ib[(size_t)nr * q + j] = prev_piv;
+    }
+  }
+  const size_t N = (size_t)k->n;
+  if (cudaMalloc(&k->coef, sizeof(double) * coef.size()) != cudaSuccess) return fail(VR_ERR_OOM);
+  for (auto &v : k->vec)
+    if (cudaMalloc(&v, sizeof(double) * N) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->part, sizeof(double) * PT_N * kK2dMaxBlocks) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->sc, sizeof(double) * SC_N) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->flags, sizeof(int) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->dct_f, sizeof(double) * cf.size()) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->dct_i, sizeof(double) * ci.size()) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->tlo, sizeof(double) * nr) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->tup, sizeof(double) * nr) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->tib, sizeof(double) * ib.size()) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->tmp, sizeof(double) * N) != cudaSuccess) return fail(VR_ERR_OOM);
+  struct {
+    double *d;
+    const std::vector<double> *h;
+  } up_[] = {{k->coef, &coef}, {k->dct_f, &cf}, {k->dct_i, &ci}, {k->tlo, &lo}, {k->tup, &up}, {k->tib, &ib}};
+  for (auto &u : up_)
+    if (cudaMemcpy(u.d, u.h->data(), sizeof(double) * u.h->size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(VR_ERR_CUDA);
+  if (cudaMemset(k->part, 0, sizeof(double) * PT_N * kK2dMaxBlocks) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaMemset(k->flags, 0, sizeof(int) * 4) != cudaSuccess) return fail(VR_ERR_CUDA);
+  *out = k;
+  return VR_OK;
+}
+
+extern "C" int vr_k2d_destroy(vr_k2d *k) {
+  if (!k) return VR_OK;
+  cudaSetDevice(k->dev);
+  if (k->stream) cudaStreamSynchronize(k->stream);
+  for (int i = 0; i < 4; i++)
+    if (k->graph_ok[i]) cudaGraphExecDestroy(k->graph[i]);
+  for (double *v : k->vec)
+    if (v) cudaFree(v);
+  double *ps[] = {k->coef, k->part, k->sc, k->dct_f, k->dct_i, k->tlo, k->tup, k->tib, k->tmp};
+  for (double *p : ps)
+    if (p) cudaFree(p);
+  if (k->flags) cudaFree(k->flags);
+  if (k->stream) cudaStreamDestroy(k->stream);
+  delete k;
+  return VR_OK;
+}
+
+extern "C" const char *vr_k2d_last_error(const vr_k2d *k) { return k ? k->err.c_str() : "null solver"; }
+
+extern "C" int vr_k2d_info(const vr_k2d *k, int32_t *nr, int32_t *nz, double *faces) {
+  if (!k) return VR_ERR_ARG;
+  if (nr) *nr = k->nr;
+  if (nz) *nz = k->nz;
+  if (faces) std::memcpy(faces, k->h_faces.data(), sizeof(double) * (k->nr + 1));
+  return VR_OK;
+}
+
+static int k2d_grid(const vr_k2d *k) { return k->nb; }
+
+// y = K x (form 1) or S x (form 0) on device arrays
+static cudaError_t k2d_apply_dev(vr_k2d *k, const double *x, double *y, int form, const double *w, double *part,
+                                 const int *flags) {
+  k2d_apply<<<k2d_grid(k), kK2dThreads, 0, k->stream>>>(op_of(k), x, y, form, w, part, flags);
+  return cudaGetLastError();
+}
+
+extern "C" int vr_k2d_apply_dev(vr_k2d *k, const double *x, double *y, int32_t symmetric) {
+  if (!k || !x || !y) return VR_ERR_ARG;
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  K2D_CUDA(k, k2d_apply_dev(k, x, y, symmetric ? 0 : 1, nullptr, nullptr, nullptr));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  return VR_OK;
+}
+
+extern "C" int vr_k2d_apply(vr_k2d *k, const double *x, double *y) {
+  if (!k || !x || !y) return VR_ERR_ARG;
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  const size_t bytes = sizeof(double) * k->n;
+  K2D_CUDA(k, cudaMemcpyAsync(k->vec[V_W1], x, bytes, cudaMemcpyHostToDevice, k->stream));
+  K2D_CUDA(k, k2d_apply_dev(k, k->vec[V_W1], k->vec[V_W2], 1, nullptr, nullptr, nullptr));
+  K2D_CUDA(k, cudaMemcpyAsync(y, k->vec[V_W2], bytes, cudaMemcpyDeviceToHost, k->stream));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  return VR_OK;
+}
+
+// direct solve K x = f on device arrays (x may alias f)
+static cudaError_t k2d_direct_dev(vr_k2d *k, const double *f, double *x) {
+  const int nr = k->nr, nz = k->nz;
+  dim3 g1((nr + 63) / 64, (nz + 63) / 64);
+  // fh(j, kz) = sum_k f(j, k) cf[kz][k]
+  k2d_gemm_abt<<<g1, 256, 0, k->stream>>>(nr, nz, nz, f, k->dct_f, k->tmp);
+  k2d_radial_thomas<<<(nz + 127) / 128, 128, 0, k->stream>>>(nr, nz, k->tmp, k->tlo, k->tup, k->tib);
+  // x(j, k) = sum_kz sol(j, kz) ci[k][kz]
+  k2d_gemm_abt<<<g1, 256, 0, k->stream>>>(nr, nz, nz, k->tmp, k->dct_i, x);
+  return cudaGetLastError();
+}
+
+extern "C" int vr_k2d_direct_dev(vr_k2d *k, const double *f, double *x) {
+  if (!k || !f || !x) return VR_ERR_ARG;
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  K2D_CUDA(k, k2d_direct_dev(k, f, x));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  return VR_OK;
+}
+
+extern "C" int vr_k2d_direct(vr_k2d *k, const double *f, double *x) {
+  if (!k || !f || !x) return VR_ERR_ARG;
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  const size_t bytes = sizeof(double) * k->n;
+  K2D_CUDA(k, cudaMemcpyAsync(k->vec[V_W1], f, bytes, cudaMemcpyHostToDevice, k->stream));
+  K2D_CUDA(k, k2d_direct_dev(k, k->vec[V_W1], k->vec[V_W2]));
+  K2D_CUDA(k, cudaMemcpyAsync(x, k->vec[V_W2], bytes, cudaMemcpyDeviceToHost, k->stream));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  return VR_OK;
+}
+
+// ---- Krylov drivers ------------------------------------------------------------
+static cudaError_t enqueue_cg_iter(vr_k2d *k, int jacobi) {
+  const K2dOp o = op_of(k);
+  const int gb = k2d_grid(k);
+  double *P = k->part;
+  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *q = k->vec[V_Q];
+  double *z = jacobi ? k->vec[V_Z] : r;
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_ALPHA, P, gb, k->sc, k->flags);
+  k2d_cg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o, jacobi, x, r, z, p, q, k->sc, P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_BETA, P, gb, k->sc, k->flags);
+  k2d_cg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags);
+  return cudaGetLastError();
+}
+
+static cudaError_t enqueue_bicg_iter(vr_k2d *k) {
+  const K2dOp o = op_of(k);
+  const int gb = k2d_grid(k);
+  double *P = k->part;
+  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *v = k->vec[V_V], *s = k->vec[V_S],
+         *t = k->vec[V_T], *rh = k->vec[V_RH];
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_BETA, P, gb, k->sc, k->flags);
+  k2d_bi_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, v, k->sc, k->flags);
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, v, 1, rh, P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_ALPHA, P, gb, k->sc, k->flags);
+  k2d_bi_s<<<gb, kK2dThreads, 0, k->stream>>>(o.n, s, r, v, k->sc, k->flags);
+  // t = K s with partials t.s [A]; t.t [B] from a dots pass
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, s, t, 1, s, P, k->flags);
+  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, t, t, nullptr, nullptr, P + kK2dMaxBlocks, nullptr);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_OMEGA, P, gb, k->sc, k->flags);
+  k2d_bi_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, s, t, rh, k->sc, P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_CONV, P, gb, k->sc, k->flags);
+  return cudaGetLastError();
+}
+
+// runs chunks of captured iterations until the device flag says converged or
+// maxit iterations have run; slot selects the cached graph
+static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), int arg, int maxit, int *iters) {
+  if (!k->graph_ok[slot]) {
+    cudaGraph_t gr = nullptr;
+    K2D_CUDA(k, cudaStreamBeginCapture(k->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < kK2dChunk && e == cudaSuccess; i++) e = enq(k, arg);
+    cudaError_t e2 = cudaStreamEndCapture(k->stream, &gr);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&k->graph[slot], gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return k2d_err(k, VR_ERR_CUDA, std::string("krylov graph: ") + cudaGetErrorString(e));
+    k->graph_ok[slot] = true;
+  }
+  int h[2] = {0, 0};
+  for (int done = 0; done < maxit; done += kK2dChunk) {
+    K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
+    K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+    if (h[0] || h[1] >= maxit) break;
+    K2D_CUDA(k, cudaGraphLaunch(k->graph[slot], k->stream));
+  }
+  K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  *iters = h[1];
+  return VR_OK;
+}
+
+static cudaError_t enq_cg(vr_k2d *k, int jacobi) { return enqueue_cg_iter(k, jacobi); }
+static cudaError_t enq_bicg(vr_k2d *k, int) { return enqueue_bicg_iter(k); }
+
+// FCG with the learned preconditioner: z = |r| N(r / |r|), p = z - beta p_old
+// with beta = (z . q_old) / (p_old . q_old) (Notay's flexible CG, one
+// direction kept), alpha = (p . r) / (p . q).  Host-driven (the network is a
+// sequence of launches); scalars stay on the device.
+static int run_fcg(vr_k2d *k, int maxit, int *iters) {
+  const K2dOp o = op_of(k);
+  const int gb = k2d_grid(k);
+  double *P = k->part;
+  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *q = k->vec[V_Q], *z = k->vec[V_Z];
+  int h[2] = {0, 0};
+  for (int it = 0; it < maxit; it++) {
+    if (it % 8 == 0) {
+      K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
+      K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+      if (h[0]) break;
+    }
+    int rc = unet_precondition(k->net, r, z, k->sc + SC_RR, k->flags, k->stream);
+    if (rc) return k2d_err(k, rc, std::string("learned preconditioner: ") + vr_unet_last_error(k->net));
+    if (it > 0) {
+      k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, q, nullptr, nullptr, P, nullptr);
+      k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_BETA, P, gb, k->sc, k->flags);
+    }
+    k2d_fcg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags, it == 0);
+    k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P + kK2dMaxBlocks, k->flags);
+    k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, nullptr, nullptr, P, nullptr);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_ALPHA, P, gb, k->sc, k->flags);
+    k2d_fcg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, q, k->sc, P, k->flags);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_CONV, P, gb, k->sc, k->flags);
+    K2D_CUDA(k, cudaGetLastError());
+  }
+  K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  *iters = h[1];
+  return VR_OK;
+}
+
+extern "C" int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *net) {
+  if (!k) return VR_ERR_ARG;
+  if (net) {
+    int nr = 0, nz = 0;
+    unet_dims(net, &nr, &nz);
+    if (nr != k->nr || nz != k->nz) return k2d_err(k, VR_ERR_ARG, "network and operator grids differ");
+  }
+  k->net = net;
+  return VR_OK;
+}
+
+// z = D^-1 r (Jacobi) and the initial partials b.b [A], r.z [B], r.r [C]
+__global__ void __launch_bounds__(kK2dThreads) k2d_init_dots(K2dOp o, int jacobi, const double *__restrict__ b,
+                                                           const double *__restrict__ r, double *__restrict__ z,
+                                                           double *part) {
+  __shared__ double sh[40];
+  double bb = 0.0, rz = 0.0, rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double ri = r[i];
+    const double zi = jacobi ? ri * o.dinv[i] : ri;
+    if (z) z[i] = zi;
+    bb += b[i] * b[i];
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  double t = block_sum(bb, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  __syncthreads();
+  t = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = t;
+  __syncthreads();
+  t = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[2 * kK2dMaxBlocks + blockIdx.x] = t;
+}
+
+// solve K x = f on device arrays of nr*nz doubles (r fastest); x holds the
+// initial guess on entry and the solution on return
+extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,
+                                int32_t *iters, double *relres) {
+  if (!k || !f || !x || !(tol > 0) || maxit < 1) return VR_ERR_ARG;
+  if (method < VR_KRYLOV_CG || method > VR_KRYLOV_FCG_LEARNED) return VR_ERR_ARG;
+  if (method == VR_KRYLOV_FCG_LEARNED && !k->net) return k2d_err(k, VR_ERR_STATE, "no learned preconditioner set");
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  const K2dOp o = op_of(k);
+  const int gb = k2d_grid(k);
+  const size_t bytes = sizeof(double) * k->n;
+  double *P = k->part;
+  double *B = k->vec[V_B], *X = k->vec[V_X], *R = k->vec[V_R], *Pv = k->vec[V_P];
+  const bool sym = method != VR_KRYLOV_BICGSTAB;
+  const double tol2 = tol * tol;
+  K2D_CUDA(k, cudaMemcpyAsync(k->sc + SC_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, k->stream));
+  const int hf[3] = {0, 0, maxit};
+  K2D_CUDA(k, cudaMemcpyAsync(k->flags, hf, sizeof(hf), cudaMemcpyHostToDevice, k->stream));
+  K2D_CUDA(k, cudaMemcpyAsync(X, x, bytes, cudaMemcpyDeviceToDevice, k->stream));
+  // b = V f (symmetric form) or f; r = b - A x
+  if (sym)
+    k2d_scale_vol<<<gb, kK2dThreads, 0, k->stream>>>(o, f, B, 0);
+  else
+    K2D_CUDA(k, cudaMemcpyAsync(B, f, bytes, cudaMemcpyDeviceToDevice, k->stream));
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, X, R, sym ? 0 : 1, nullptr, nullptr, nullptr);
+  k2d_axpby<<<gb, kK2dThreads, 0, k->stream>>>(k->n, 1.0, B, -1.0, R, R);
+  K2D_CUDA(k, cudaGetLastError());
+  int it = 0, rc = VR_OK;
+  if (method == VR_KRYLOV_CG || method == VR_KRYLOV_PCG_JACOBI) {
+    const int jac = method == VR_KRYLOV_PCG_JACOBI;
+    double *z = jac ? k->vec[V_Z] : R;
+    k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, jac, B, R, jac ? z : nullptr, P);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
+    K2D_CUDA(k, cudaMemcpyAsync(Pv, z, bytes, cudaMemcpyDeviceToDevice, k->stream));
+    K2D_CUDA(k, cudaGetLastError());
+    rc = run_chunks(k, jac, enq_cg, jac, maxit, &it);
+  } else if (method == VR_KRYLOV_BICGSTAB) {
+    K2D_CUDA(k, cudaMemcpyAsync(k->vec[V_RH], R, bytes, cudaMemcpyDeviceToDevice, k->stream));
+    K2D_CUDA(k, cudaMemsetAsync(Pv, 0, bytes, k->stream));
+    K2D_CUDA(k, cudaMemsetAsync(k->vec[V_V], 0, bytes, k->stream));
+    // partials: b.b [A], rh.r = r.r [B], r.r [C]
+    k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_INIT, P, gb, k->sc, k->flags);
+    K2D_CUDA(k, cudaGetLastError());
+    rc = run_chunks(k, 2, enq_bicg, 0, maxit, &it);
+  } else {
+    k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
+    K2D_CUDA(k, cudaGetLastError());
+    rc = run_fcg(k, maxit, &it);
+  }
+  if (rc) return rc;
+  // true residual of the returned x, in the form the method iterated on
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, X, R, sym ? 0 : 1, nullptr, nullptr, nullptr);
+  k2d_axpby<<<gb, kK2dThreads, 0, k->stream>>>(k->n, 1.0, B, -1.0, R, R);
+  k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_NORM, P + 2 * kK2dMaxBlocks, gb, k->sc, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_NORM_BB, P, gb, k->sc, k->flags);
+  double hs[SC_N];
+  K2D_CUDA(k, cudaMemcpyAsync(x, X, bytes, cudaMemcpyDeviceToDevice, k->stream));
+  K2D_CUDA(k, cudaMemcpyAsync(hs, k->sc, sizeof(hs), cudaMemcpyDeviceToHost, k->stream));
+  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+  if (iters) *iters = it;
+  if (relres) *relres = hs[SC_BB] > 0 ? std::sqrt(hs[SC_RR] / hs[SC_BB]) : 0.0;
+  return VR_OK;
+}
+
+// ---- training support for the learned preconditioner ---------------------------
+namespace vr {
+__global__ void __launch_bounds__(kK2dThreads) k2d_loss_a(K2dOp o, const float *__restrict__ y,
+                                                        const double *__restrict__ x, double *__restrict__ yd,
+                                                        double *__restrict__ e, double *part) {
+  // e = S y - x with y widened; partial e.e
+  __shared__ double sh[40];
+  // widen y first (the stencil reads neighbours): done by the caller's pass
+  const double mean = last_row_mean(o, yd, sh);
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double v = apply_S_at(o, yd, i, mean) - x[i];
+    e[i] = v;
+    acc += v * v;
+  }
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  (void)y;
+}
+
+__global__ void k2d_widen(int n, const float *__restrict__ y, double *__restrict__ yd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) yd[i] = (double)y[i];
+}
+
+// gy = 2 S e / xx (float); loss_acc += e.e / xx
+__global__ void __launch_bounds__(kK2dThreads) k2d_loss_b(K2dOp o, const double *__restrict__ e, double inv_xx,
+                                                        float *__restrict__ gy) {
+  __shared__ double sh[40];
+  const double mean = last_row_mean(o, e, sh);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x)
+    gy[i] = (float)(2.0 * inv_xx * apply_S_at(o, e, i, mean));
+}
+
+__global__ void __launch_bounds__(1024) k2d_sum_into(const double *part, int nb, double scale, double *acc,
+                                                   int overwrite) {
+  __shared__ double sh[40];
+  const double a = sum_part(part, nb, sh);
+  if (threadIdx.x == 0) *acc = overwrite ? a * scale : *acc + a * scale;
+}
+
+cudaError_t k2d_loss_grad(vr_k2d *k, const float *y, const double *x, double xx, float *gy, double *loss_acc,
+                          cudaStream_t s) {
+  const K2dOp o = op_of(k);
+  const int gb = k2d_grid(k);
+  double *yd = k->vec[V_W1], *e = k->vec[V_W2];
+  k2d_widen<<<gb, kK2dThreads, 0, s>>>(o.n, y, yd);
+  k2d_loss_a<<<gb, kK2dThreads, 0, s>>>(o, y, x, yd, e, k->part + 3 * kK2dMaxBlocks);
+  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 3 * kK2dMaxBlocks, gb, 1.0 / xx, loss_acc, 0 /*accumulate*/);
+  k2d_loss_b<<<gb, kK2dThreads, 0, s>>>(o, e, 1.0 / xx, gy);
+  return cudaGetLastError();
+}
+
+cudaError_t k2d_dot_self(vr_k2d *k, const double *x, double *rr, cudaStream_t s) {
+  const int gb = k2d_grid(k);
+  k2d_dots<<<gb, kK2dThreads, 0, s>>>(k->n, x, x, nullptr, nullptr, k->part + 3 * kK2dMaxBlocks, nullptr);
+  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 3 * kK2dMaxBlocks, gb, 1.0, rr, 1);
+  return cudaGetLastError();
+}
+}  // namespace vr
+
+extern "C" int vr_k2d_solve(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,
+                            int32_t *iters, double *relres, double *ms) {
+  if (!k || !f || !x) return VR_ERR_ARG;
+  K2D_CUDA(k, cudaSetDevice(k->dev));
+  const size_t bytes = sizeof(double) * k->n;
+  K2D_CUDA(k, cudaMemcpyAsync(k->vec[V_W1], f, bytes, cudaMemcpyHostToDevice, k->stream));
+  K2D_CUDA(k, cudaMemcpyAsync(k->vec[V_W2], x, bytes, cudaMemcpyHostToDevice, k->stream));
+  cudaEvent_t e0, e1;
+  K2D_CUDA(k, cudaEventCreate(&e0));
+  K2D_CUDA(k, cudaEventCreate(&e1));
+  cudaEventRecord(e0, k->stream);
+  int rc = vr_k2d_solve_dev(k, method, k->vec[V_W1], k->vec[V_W2], tol, maxit, iters, relres);
+  cudaEventRecord(e1, k->stream);
+  if (rc == VR_OK) {
+    K2D_CUDA(k, cudaMemcpyAsync(x, k->vec[V_W2], bytes, cudaMemcpyDeviceToHost, k->stream));
+    K2D_CUDA(k, cudaStreamSynchronize(k->stream));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}

@@ -1,0 +1,747 @@
+// vr_unet.cu -- the learned preconditioner of the axisymmetric Krylov solve:
+// a 4-level U-Net with BF16 weights and activations and FP32 accumulation,
+// with its own forward, backward (data and weight gradients) and Adam kernels.
+//
+// Layout: activations are channels-last on the (nr_l x nz_l) grid of level l,
+// pixel p = j + nr_l k (r fastest), element p * C + c.  A 3x3 layer's weights
+// are [cout][tap][cin] with tap = 3 * dr + dz, dr, dz in {0, 1, 2} meaning the
+// neighbour (j + dr - 1, k + dz - 1); zero padding at the grid edges.
+//
+// Network (no biases, identity activations, so the map is linear):
+//   level 0..2 down: two 3x3 convs (cin -> c_l -> c_l), the second's output is
+//   the skip tensor e_l; 2x2 average pooling to the next level;
+//   level 3: two 3x3 convs (c_2 -> c_3 -> c_3);
+//   level 2..0 up: nearest 2x upsampling of the level below, concatenated with
+//   e_l (upsampled channels first), two 3x3 convs (-> c_l -> c_l);
+//   head: 1x1 conv c_0 -> 1, FP32 output.
+//
+// Convolutions (forward and data gradient) run one output pixel per thread
+// over 16 x 16 pixel tiles: the input tile (18 x 18 pixels x 16 channels) and
+// the weights of those 16 input channels are staged in shared memory as FP32,
+// and each thread keeps all of its pixel's output channels in registers.  The
+// data gradient is the same convolution with the weights flipped and
+// transposed ([cin][8 - tap][cout]).  Weight gradients reduce over pixels per
+// 16 x 16 (cout, cin) tile and are added with FP32 atomics.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "vr_internal.cuh"
+#include "vr_learned.cuh"
+
+namespace vr {
+
+constexpr int kUnetLayers = 15;  // 14 3x3 layers + the 1x1 head
+
+struct UnetLayer {
+  int cin, cout, level, taps;
+  size_t woff;  // offset in the parameter vector
+};
+
+}  // namespace vr
+
+struct vr_unet {
+  int nr = 0, nz = 0, dev = 0;
+  int ch[4] = {};
+  std::string err;
+  vr::UnetLayer L[vr::kUnetLayers];
+  size_t nparam = 0;
+  // parameters: FP32 master, BF16 copy, FP32 copy for the kernels, flipped
+  // copy for the data gradient, gradient, Adam moments
+  float *w32 = nullptr, *wk = nullptr, *wflip = nullptr, *gw = nullptr, *m1 = nullptr, *m2 = nullptr;
+  __nv_bfloat16 *w16 = nullptr;
+  int64_t adam_t = 0;
+  // activations (bf16) and their gradients (fp32), one per tensor slot
+  __nv_bfloat16 *x0 = nullptr;            // input, 1 channel
+  __nv_bfloat16 *a[20] = {};              // layer outputs, pooled and concatenated tensors
+  float *g[20] = {};
+  float *gx0 = nullptr;                   // input gradient (gradient check only)
+  float *y = nullptr, *gy = nullptr;      // head output and its gradient
+  double *xs = nullptr;                   // normalised input (double) for the loss
+  double *dscal = nullptr;                // device scalars: loss accumulator, rr
+  cudaStream_t stream = nullptr;
+};
+
+namespace vr {
+
+__device__ __forceinline__ float tof(float v) { return v; }
+__device__ __forceinline__ float tof(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <class T>
+__device__ __forceinline__ T fromf(float v);
+template <>
+__device__ __forceinline__ float fromf<float>(float v) {
+  return v;
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 fromf<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+
+// out[p][co] (=|+=) sum_{tap, ci} in[p + off(tap)][ci] w[co][tap][ci]
+template <class TI, class TO, int CO>
+__global__ void __launch_bounds__(256) k_conv3(const TI *__restrict__ in, int H, int W, int cin,
+                                             const float *__restrict__ w, int cout, TO *__restrict__ out,
+                                             int accumulate) {
+  extern __shared__ float sm[];
+  float *tin = sm;                 // [18*18][17]
+  float *tw = sm + 18 * 18 * 17;   // [CO][9][16]
+  const int tj = threadIdx.x & 15, tk = threadIdx.x >> 4;
+  const int j0 = blockIdx.x * 16, k0 = blockIdx.y * 16;
+  float acc[CO];
+#pragma unroll
+  for (int c = 0; c < CO; c++) acc[c] = 0.f;
+  for (int c0 = 0; c0 < cin; c0 += 16) {
+    const int cc = min(16, cin - c0);
+    for (int e = threadIdx.x; e < 18 * 18 * 16; e += 256) {
+      const int ci = e & 15, pix = e >> 4;
+      const int pj = pix % 18, pk = pix / 18;
+      const int gj = j0 + pj - 1, gk = k0 + pk - 1;
+      float v = 0.f;
+      if (ci < cc && gj >= 0 && gj < H && gk >= 0 && gk < W) v = tof(in[((size_t)gj + (size_t)H * gk) * cin + c0 + ci]);
+      tin[pix * 17 + ci] = v;
+    }
+    for (int e = threadIdx.x; e < CO * 9 * 16; e += 256) {
+      const int ci = e & 15, t = (e >> 4) % 9, co = e / 144;
+      float v = 0.f;
+      if (co < cout && ci < cc) v = w[((size_t)co * 9 + t) * cin + c0 + ci];
+      tw[e] = v;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int t = 0; t < 9; t++) {
+      const int dr = t / 3, dz = t % 3;
+      const float *ip = tin + ((tj + dr) + 18 * (tk + dz)) * 17;
+      float xin[16];
+#pragma unroll
+      for (int ci = 0; ci < 16; ci++) xin[ci] = ip[ci];
+#pragma unroll
+      for (int co = 0; co < CO; co++) {
+        const float4 *wp = reinterpret_cast<const float4 *>(tw + (co * 9 + t) * 16);
+        const float4 a = wp[0], b = wp[1], c = wp[2], d = wp[3];
+        float s = acc[co];
+        s = fmaf(xin[0], a.x, s);
+        s = fmaf(xin[1], a.y, s);
+        s = fmaf(xin[2], a.z, s);
+        s = fmaf(xin[3], a.w, s);
+        s = fmaf(xin[4], b.x, s);
+        s = fmaf(xin[5], b.y, s);
+        s = fmaf(xin[6], b.z, s);
+        s = fmaf(xin[7], b.w, s);
+        s = fmaf(xin[8], c.x, s);
+        s = fmaf(xin[9], c.y, s);
+        s = fmaf(xin[10], c.z, s);
+        s = fmaf(xin[11], c.w, s);
+        s = fmaf(xin[12], d.x, s);
+        s = fmaf(xin[13], d.y, s);
+        s = fmaf(xin[14], d.z, s);
+        s = fmaf(xin[15], d.w, s);
+        acc[co] = s;
+      }
+    }
+    __syncthreads();
+  }
+  const int gj = j0 + tj, gk = k0 + tk;
+  if (gj < H && gk < W) {
+    TO *op = out + ((size_t)gj + (size_t)H * gk) * cout;
+#pragma unroll
+    for (int co = 0; co < CO; co++)
+      if (co < cout) op[co] = fromf<TO>(accumulate ? acc[co] + tof(op[co]) : acc[co]);
+  }
+}
+
+// dw[co][tap][ci] += sum_p dout[p][co] in[p + off(tap)][ci]; one block per
+// (16-channel cin group, 16-channel cout group, pixel range)
+template <class TI>
+__global__ void __launch_bounds__(256) k_wgrad3(const float *__restrict__ dout, int H, int W, int cout,
+                                              const TI *__restrict__ in, int cin, float *__restrict__ dw,
+                                              int pix_per_block) {
+  __shared__ float sd[32][17];       // dout rows of 32 pixels
+  __shared__ float si[9][32][17];    // in at the 9 taps of those pixels
+  const int ci = threadIdx.x & 15, co = threadIdx.x >> 4;
+  const int ci0 = blockIdx.x * 16, co0 = blockIdx.y * 16;
+  const int P = H * W;
+  const int pbeg = blockIdx.z * pix_per_block, pend = min(P, pbeg + pix_per_block);
+  float acc[9];
+#pragma unroll
+  for (int t = 0; t < 9; t++) acc[t] = 0.f;
+  for (int pb = pbeg; pb < pend; pb += 32) {
+    for (int e = threadIdx.x; e < 32 * 16; e += 256) {
+      const int pl = e >> 4, c = e & 15, p = pb + pl;
+      sd[pl][c] = (p < pend && co0 + c < cout) ? dout[(size_t)p * cout + co0 + c] : 0.f;
+    }
+    for (int e = threadIdx.x; e < 9 * 32 * 16; e += 256) {
+      const int c = e & 15, pl = (e >> 4) & 31, t = e >> 9;
+      const int p = pb + pl;
+      float v = 0.f;
+      if (p < pend && ci0 + c < cin) {
+        const int j = p % H + t / 3 - 1, k = p / H + t % 3 - 1;
+        if (j >= 0 && j < H && k >= 0 && k < W) v = tof(in[((size_t)j + (size_t)H * k) * cin + ci0 + c]);
+      }
+      si[t][pl][c] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int pl = 0; pl < 32; pl++) {
+      const float d = sd[pl][co];
+#pragma unroll
+      for (int t = 0; t < 9; t++) acc[t] = fmaf(d, si[t][pl][ci], acc[t]);
+    }
+    __syncthreads();
+  }
+  if (co0 + co < cout && ci0 + ci < cin)
+#pragma unroll
+    for (int t = 0; t < 9; t++) atomicAdd(dw + ((size_t)(co0 + co) * 9 + t) * cin + ci0 + ci, acc[t]);
+}
+
+// 2x2 average pooling and its gradient
+__global__ void k_pool(const __nv_bfloat16 *__restrict__ in, int H, int W, int c, __nv_bfloat16 *__restrict__ out) {
+  const int H2 = H / 2, W2 = W / 2;
+  const size_t n = (size_t)H2 * W2 * c;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % c);
+    const size_t p = e / c;
+    const int J = (int)(p % H2), K = (int)(p / H2);
+    const size_t b = ((size_t)2 * J + (size_t)H * 2 * K) * c + ch;
+    const float s = tof(in[b]) + tof(in[b + c]) + tof(in[b + (size_t)H * c]) + tof(in[b + (size_t)H * c + c]);
+    out[e] = __float2bfloat16_rn(0.25f * s);
+  }
+}
+// gin[p][c] += 0.25 gout[parent(p)][c]
+__global__ void k_pool_bwd(const float *__restrict__ gout, int H, int W, int c, float *__restrict__ gin) {
+  const size_t n = (size_t)H * W * c;
+  const int H2 = H / 2;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % c);
+    const size_t p = e / c;
+    const int j = (int)(p % H), k = (int)(p / H);
+    gin[e] += 0.25f * gout[((size_t)(j / 2) + (size_t)H2 * (k / 2)) * c + ch];
+  }
+}
+// out[p] = [coarse[parent(p)] (ca channels), skip[p] (cb channels)]
+__global__ void k_upcat(const __nv_bfloat16 *__restrict__ coarse, int ca, const __nv_bfloat16 *__restrict__ skip,
+                        int cb, int H, int W, __nv_bfloat16 *__restrict__ out) {
+  const int c = ca + cb, H2 = H / 2;
+  const size_t n = (size_t)H * W * c;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % c);
+    const size_t p = e / c;
+    const int j = (int)(p % H), k = (int)(p / H);
+    out[e] = ch < ca ? coarse[((size_t)(j / 2) + (size_t)H2 * (k / 2)) * ca + ch] : skip[p * cb + ch - ca];
+  }
+}
+// gradient of k_upcat: gcoarse = sum over the 4 children, gskip += the skip part
+__global__ void k_upcat_bwd(const float *__restrict__ gout, int ca, int cb, int H, int W, float *__restrict__ gcoarse,
+                            float *__restrict__ gskip) {
+  const int c = ca + cb, H2 = H / 2, W2 = W / 2;
+  const size_t nc = (size_t)H2 * W2 * ca;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nc; e += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % ca);
+    const size_t P = e / ca;
+    const int J = (int)(P % H2), K = (int)(P / H2);
+    const size_t b = ((size_t)2 * J + (size_t)H * 2 * K) * c + ch;
+    gcoarse[e] = gout[b] + gout[b + c] + gout[b + (size_t)H * c] + gout[b + (size_t)H * c + c];
+  }
+  const size_t ns = (size_t)H * W * cb;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ns; e += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % cb);
+    const size_t p = e / cb;
+    gskip[e] += gout[p * c + ca + ch];
+  }
+}
+// head: y[p] = sum_c in[p][c] w[c]
+__global__ void k_head(const __nv_bfloat16 *__restrict__ in, int P, int c, const float *__restrict__ w,
+                       float *__restrict__ y) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int ch = 0; ch < c; ch++) s = fmaf(tof(in[(size_t)p * c + ch]), w[ch], s);
+    y[p] = s;
+  }
+}
+// head gradient: gin[p][c] = gy[p] w[c]; gw[c] += sum_p gy[p] in[p][c]
+__global__ void __launch_bounds__(256) k_head_bwd(const __nv_bfloat16 *__restrict__ in, int P, int c,
+                                                const float *__restrict__ w, const float *__restrict__ gy,
+                                                float *__restrict__ gin, float *__restrict__ gw) {
+  __shared__ float red[8][64];
+  float acc[64];
+  for (int ch = 0; ch < 64; ch++) acc[ch] = 0.f;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const float g = gy[p];
+    for (int ch = 0; ch < c; ch++) {
+      gin[(size_t)p * c + ch] = g * w[ch];
+      acc[ch] = fmaf(g, tof(in[(size_t)p * c + ch]), acc[ch]);
+    }
+  }
+  for (int ch = 0; ch < c; ch++) {
+    float v = acc[ch];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][ch] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < c) {
+    float s = 0.f;
+    for (int i = 0; i < 8; i++) s += red[i][threadIdx.x];
+    atomicAdd(gw + threadIdx.x, s);
+  }
+}
+// input: x[p] * inv (double) -> bf16; keeps the scaled double copy
+__global__ void k_in(const double *__restrict__ x, int n, const double *__restrict__ rr, double inv_host,
+                     __nv_bfloat16 *__restrict__ xb, double *__restrict__ xs, const int *flags) {
+  if (flags && flags[0]) return;
+  const double inv = rr ? (*rr > 0 ? 1.0 / sqrt(*rr / n) : 0.0) : inv_host;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = x[i] * inv;
+    if (xs) xs[i] = v;
+    xb[i] = __float2bfloat16_rn((float)v);
+  }
+}
+// output: z = s y
+__global__ void k_out(const float *__restrict__ y, int n, const double *__restrict__ rr, double s_host,
+                      double *__restrict__ z, const int *flags) {
+  if (flags && flags[0]) return;
+  const double s = rr ? sqrt(*rr / n) : s_host;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = s * (double)y[i];
+}
+// weights: bf16 copy, the rounded FP32 copy used by the kernels, the flipped
+// transposed copy for the data gradient of every 3x3 layer
+__global__ void k_wprep(const float *__restrict__ w32, size_t n, __nv_bfloat16 *__restrict__ w16,
+                        float *__restrict__ wk) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(w32[i]);
+    w16[i] = b;
+    wk[i] = __bfloat162float(b);
+  }
+}
+__global__ void k_wflip(const float *__restrict__ w, int cin, int cout, float *__restrict__ wf) {
+  const int n = cin * cout * 9;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int co = e % cout, t = (e / cout) % 9, ci = e / (9 * cout);
+    wf[e] = w[((size_t)co * 9 + (8 - t)) * cin + ci];  // wf[ci][t][co]
+  }
+}
+// Adam (Kingma & Ba 2015) on the FP32 master weights, gradient scaled by gs
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       size_t n, float lr, float gs, float b1, float b2, float c1, float c2, float eps) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i] * gs;
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+template <class TI, class TO>
+static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, int cout, TO *out, int acc,
+                         cudaStream_t s) {
+  const size_t smb = sizeof(float) * (18 * 18 * 17);
+  dim3 g((H + 15) / 16, (W + 15) / 16);
+  cudaError_t e;
+#define VR_CONV_CASE(C)                                                                  \
+  if (cout <= C) {                                                                       \
+    const size_t sm = smb + sizeof(float) * C * 9 * 16;                                  \
+    if ((e = allow_dyn_smem(k_conv3<TI, TO, C>, sm))) return e;                          \
+    k_conv3<TI, TO, C><<<g, 256, sm, s>>>(in, H, W, cin, w, cout, out, acc);             \
+    return cudaGetLastError();                                                           \
+  }
+  VR_CONV_CASE(8)
+  VR_CONV_CASE(16)
+  VR_CONV_CASE(32)
+  VR_CONV_CASE(48)
+  VR_CONV_CASE(64)
+  VR_CONV_CASE(80)
+  VR_CONV_CASE(96)
+  VR_CONV_CASE(112)
+  VR_CONV_CASE(128)
+#undef VR_CONV_CASE
+  return cudaErrorInvalidValue;
+}
+
+template <class TI>
+static cudaError_t wgrad3(const float *dout, int H, int W, int cout, const TI *in, int cin, float *dw,
+                          cudaStream_t s) {
+  const int P = H * W;
+  const int ppb = 4096;
+  dim3 g((cin + 15) / 16, (cout + 15) / 16, (P + ppb - 1) / ppb);
+  k_wgrad3<TI><<<g, 256, 0, s>>>(dout, H, W, cout, in, cin, dw, ppb);
+  return cudaGetLastError();
+}
+
+static int grid_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+}  // namespace vr
+
+using namespace vr;
+
+static int unet_err(vr_unet *u, int code, const std::string &m) {
+  if (u) u->err = m;
+  return code;
+}
+#define U_CUDA(u, call)                                                                        \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return unet_err((u), VR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+// activation slots: id, level, channels (filled at create)
+enum Slot {
+  S_E0A, S_E0, S_P1, S_E1A, S_E1, S_P2, S_E2A, S_E2, S_P3, S_B3A, S_B3,
+  S_U2, S_D2A, S_D2, S_U1, S_D1A, S_D1, S_U0, S_D0A, S_D0, S_NSLOT
+};
+}  // namespace
+
+struct UnetShapes {
+  int lev[S_NSLOT], ch[S_NSLOT];
+};
+
+static UnetShapes shapes_of(const vr_unet *u) {
+  UnetShapes s;
+  const int *c = u->ch;
+  const int L[S_NSLOT] = {0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 2, 2, 2, 1, 1, 1, 0, 0, 0};
+  const int C[S_NSLOT] = {c[0], c[0], c[0], c[1], c[1], c[1], c[2], c[2], c[2], c[3], c[3],
+                          c[3] + c[2], c[2], c[2], c[2] + c[1], c[1], c[1], c[1] + c[0], c[0], c[0]};
+  for (int i = 0; i < S_NSLOT; i++) {
+    s.lev[i] = L[i];
+    s.ch[i] = C[i];
+  }
+  return s;
+}
+
+// the 14 3x3 layers: (input slot or -1 for x0, output slot)
+static const int kConvIn[14] = {-1, S_E0A, S_P1, S_E1A, S_P2, S_E2A, S_P3, S_B3A, S_U2, S_D2A, S_U1, S_D1A, S_U0, S_D0A};
+static const int kConvOut[14] = {S_E0A, S_E0, S_E1A, S_E1, S_E2A, S_E2, S_B3A, S_B3, S_D2A, S_D2, S_D1A, S_D1, S_D0A, S_D0};
+
+static_assert(S_NSLOT <= 20, "tensor slots");
+
+extern "C" int vr_unet_destroy(vr_unet *u);
+
+extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **out) {
+  if (!d || !out) return VR_ERR_ARG;
+  *out = nullptr;
+  if (d->abi_version != VR_ABI_VERSION) return VR_ERR_DESC;
+  if (d->nr < 8 || d->nz < 8 || d->nr % 8 || d->nz % 8 || (int64_t)d->nr * d->nz > ((int64_t)1 << 24)) return VR_ERR_DESC;
+  for (int l = 0; l < 4; l++)
+    if (d->ch[l] < 8 || d->ch[l] > 128 || d->ch[l] % 8) return VR_ERR_DESC;
+  if (d->ch[0] > 64) return VR_ERR_DESC;  // the head's gradient keeps c0 sums per thread
+  if (d->ch[3] + d->ch[2] > 128 || d->ch[2] + d->ch[1] > 128 || d->ch[1] + d->ch[0] > 128) return VR_ERR_DESC;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || d->device < 0 || d->device >= ndev)
+    return VR_ERR_NODEVICE;
+  vr_unet *u = new (std::nothrow) vr_unet();
+  if (!u) return VR_ERR_OOM;
+  auto fail = [&](int code) {
+    vr_unet_destroy(u);
+    return code;
+  };
+  u->nr = d->nr;
+  u->nz = d->nz;
+  u->dev = d->device;
+  for (int l = 0; l < 4; l++) u->ch[l] = d->ch[l];
+  if (cudaSetDevice(u->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
+  const UnetShapes sh = shapes_of(u);
+  size_t off = 0;
+  for (int i = 0; i < 14; i++) {
+    const int cin = kConvIn[i] < 0 ? 1 : sh.ch[kConvIn[i]];
+    const int cout = sh.ch[kConvOut[i]];
+    u->L[i] = UnetLayer{cin, cout, sh.lev[kConvOut[i]], 9, off};
+    off += (size_t)cin * cout * 9;
+  }
+  u->L[14] = UnetLayer{u->ch[0], 1, 0, 1, off};
+  off += u->ch[0];
+  u->nparam = off;
+  // He-style initialisation scaled for a linear network: each 3x3 layer
+  // preserves the variance of its input (std = 1 / sqrt(9 cin)), from a
+  // splitmix64 stream (Box-Muller)
+  std::vector<float> w(u->nparam);
+  uint64_t st = seed;
+  auto next = [&]() {
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  auto unif = [&]() { return ((next() >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+  const double pi = std::acos(-1.0);
+  for (int i = 0; i < kUnetLayers; i++) {
+    const double sd = 1.0 / std::sqrt((double)u->L[i].cin * u->L[i].taps);
+    const size_t n = (size_t)u->L[i].cin * u->L[i].cout * u->L[i].taps;
+    for (size_t e = 0; e < n; e++)
+      w[u->L[i].woff + e] = (float)(sd * std::sqrt(-2.0 * std::log(unif())) * std::cos(2.0 * pi * unif()));
+  }
+  const size_t P0 = (size_t)u->nr * u->nz;
+  size_t maxflip = 0;
+  for (int i = 0; i < 14; i++) maxflip = std::max(maxflip, (size_t)u->L[i].cin * u->L[i].cout * 9);
+  float **fp[] = {&u->w32, &u->wk, &u->gw, &u->m1, &u->m2};
+  for (float **p : fp)
+    if (cudaMalloc(p, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->wflip, sizeof(float) * maxflip) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->w16, sizeof(__nv_bfloat16) * u->nparam) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->x0, sizeof(__nv_bfloat16) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->y, sizeof(float) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->gy, sizeof(float) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->xs, sizeof(double) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->dscal, sizeof(double) * 8) != cudaSuccess) return fail(VR_ERR_OOM);
+  vr_unet *x = u;
+  for (int i = 0; i < S_NSLOT; i++) {
+    const size_t n = (P0 >> (2 * sh.lev[i])) * sh.ch[i];
+    if (cudaMalloc(&x->a[i], sizeof(__nv_bfloat16) * n) != cudaSuccess) return fail(VR_ERR_OOM);
+    if (cudaMalloc(&x->g[i], sizeof(float) * n) != cudaSuccess) return fail(VR_ERR_OOM);
+  }
+  if (cudaMalloc(&x->gx0, sizeof(float) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMemcpy(u->w32, w.data(), sizeof(float) * u->nparam, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(VR_ERR_CUDA);
+  if (cudaMemset(u->m1, 0, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaMemset(u->m2, 0, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_CUDA);
+  k_wprep<<<grid_for(u->nparam), 256, 0, u->stream>>>(u->w32, u->nparam, u->w16, u->wk);
+  if (cudaStreamSynchronize(u->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
+  *out = u;
+  return VR_OK;
+}
+
+extern "C" int vr_unet_destroy(vr_unet *u) {
+  if (!u) return VR_OK;
+  cudaSetDevice(u->dev);
+  if (u->stream) cudaStreamSynchronize(u->stream);
+  for (int i = 0; i < S_NSLOT; i++) {
+    if (u->a[i]) cudaFree(u->a[i]);
+    if (u->g[i]) cudaFree(u->g[i]);
+  }
+  if (u->gx0) cudaFree(u->gx0);
+  float *fp[] = {u->w32, u->wk, u->gw, u->m1, u->m2, u->wflip, u->y, u->gy};
+  for (float *p : fp)
+    if (p) cudaFree(p);
+  if (u->w16) cudaFree(u->w16);
+  if (u->x0) cudaFree(u->x0);
+  if (u->xs) cudaFree(u->xs);
+  if (u->dscal) cudaFree(u->dscal);
+  if (u->stream) cudaStreamDestroy(u->stream);
+  delete u;
+  return VR_OK;
+}
+
+extern "C" const char *vr_unet_last_error(const vr_unet *u) { return u ? u->err.c_str() : "null network"; }
+
+extern "C" int vr_unet_nparams(const vr_unet *u, int64_t *n) {
+  if (!u || !n) return VR_ERR_ARG;
+  *n = (int64_t)u->nparam;
+  return VR_OK;
+}
+
+extern "C" int vr_unet_get_params(const vr_unet *u, float *w) {
+  if (!u || !w) return VR_ERR_ARG;
+  if (cudaSetDevice(u->dev) != cudaSuccess) return VR_ERR_CUDA;
+  if (cudaMemcpy(w, u->w32, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost) != cudaSuccess) return VR_ERR_CUDA;
+  return VR_OK;
+}
+
+extern "C" int vr_unet_set_params(vr_unet *u, const float *w) {
+  if (!u || !w) return VR_ERR_ARG;
+  U_CUDA(u, cudaSetDevice(u->dev));
+  U_CUDA(u, cudaMemcpyAsync(u->w32, w, sizeof(float) * u->nparam, cudaMemcpyHostToDevice, u->stream));
+  k_wprep<<<grid_for(u->nparam), 256, 0, u->stream>>>(u->w32, u->nparam, u->w16, u->wk);
+  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, cudaStreamSynchronize(u->stream));
+  return VR_OK;
+}
+
+namespace vr {
+
+// forward from u->x0 (bf16 input) to u->y (fp32)
+static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
+  const UnetShapes sh = shapes_of(u);
+  const vr_unet *x = u;
+  cudaError_t e;
+  auto HW = [&](int lev, int &H, int &W) {
+    H = u->nr >> lev;
+    W = u->nz >> lev;
+  };
+  int H, W;
+  auto conv = [&](int li) -> cudaError_t {
+    const UnetLayer &L = u->L[li];
+    HW(L.level, H, W);
+    const __nv_bfloat16 *in = kConvIn[li] < 0 ? u->x0 : x->a[kConvIn[li]];
+    return conv3<__nv_bfloat16, __nv_bfloat16>(in, H, W, L.cin, u->wk + L.woff, L.cout, x->a[kConvOut[li]], 0, s);
+  };
+  auto pool = [&](int src, int dst) {
+    HW(sh.lev[src], H, W);
+    const size_t n = (size_t)(H / 2) * (W / 2) * sh.ch[src];
+    k_pool<<<grid_for(n), 256, 0, s>>>(x->a[src], H, W, sh.ch[src], x->a[dst]);
+    return cudaGetLastError();
+  };
+  auto upcat = [&](int coarse, int skip, int dst) {
+    HW(sh.lev[skip], H, W);
+    const size_t n = (size_t)H * W * sh.ch[dst];
+    k_upcat<<<grid_for(n), 256, 0, s>>>(x->a[coarse], sh.ch[coarse], x->a[skip], sh.ch[skip], H, W, x->a[dst]);
+    return cudaGetLastError();
+  };
+  if ((e = conv(0)) || (e = conv(1)) || (e = pool(S_E0, S_P1))) return e;
+  if ((e = conv(2)) || (e = conv(3)) || (e = pool(S_E1, S_P2))) return e;
+  if ((e = conv(4)) || (e = conv(5)) || (e = pool(S_E2, S_P3))) return e;
+  if ((e = conv(6)) || (e = conv(7))) return e;
+  if ((e = upcat(S_B3, S_E2, S_U2)) || (e = conv(8)) || (e = conv(9))) return e;
+  if ((e = upcat(S_D2, S_E1, S_U1)) || (e = conv(10)) || (e = conv(11))) return e;
+  if ((e = upcat(S_D1, S_E0, S_U0)) || (e = conv(12)) || (e = conv(13))) return e;
+  const int P0 = u->nr * u->nz;
+  k_head<<<grid_for(P0), 256, 0, s>>>(x->a[S_D0], P0, u->ch[0], u->wk + u->L[14].woff, u->y);
+  return cudaGetLastError();
+}
+
+// backward from u->gy; accumulates parameter gradients into u->gw and, with
+// want_dx, the input gradient into ext->gx0
+static cudaError_t unet_bwd(const vr_unet *u, bool want_dx, cudaStream_t s) {
+  const UnetShapes sh = shapes_of(u);
+  const vr_unet *x = u;
+  cudaError_t e;
+  int H, W;
+  auto HW = [&](int lev) {
+    H = u->nr >> lev;
+    W = u->nz >> lev;
+  };
+  for (int i = 0; i < S_NSLOT; i++) {
+    HW(sh.lev[i]);
+    if ((e = cudaMemsetAsync(x->g[i], 0, sizeof(float) * (size_t)H * W * sh.ch[i], s))) return e;
+  }
+  const int P0 = u->nr * u->nz;
+  k_head_bwd<<<std::min(P0 / 256 + 1, 148 * 4), 256, 0, s>>>(x->a[S_D0], P0, u->ch[0], u->wk + u->L[14].woff, u->gy,
+                                                            x->g[S_D0], u->gw + u->L[14].woff);
+  if ((e = cudaGetLastError())) return e;
+  // conv layer li: gradient of its output is in g[out]; adds the input
+  // gradient into g[in] (or gx0) and the weight gradient into gw
+  auto conv_bwd = [&](int li) -> cudaError_t {
+    const UnetLayer &L = u->L[li];
+    HW(L.level);
+    const int so = kConvOut[li], si = kConvIn[li];
+    const __nv_bfloat16 *in = si < 0 ? u->x0 : x->a[si];
+    cudaError_t er = wgrad3<__nv_bfloat16>(x->g[so], H, W, L.cout, in, L.cin, u->gw + L.woff, s);
+    if (er) return er;
+    if (si < 0 && !want_dx) return cudaSuccess;
+    k_wflip<<<grid_for((size_t)L.cin * L.cout * 9), 256, 0, s>>>(u->wk + L.woff, L.cin, L.cout, u->wflip);
+    float *gin = si < 0 ? x->gx0 : x->g[si];
+    return conv3<float, float>(x->g[so], H, W, L.cout, u->wflip, L.cin, gin, si < 0 ? 0 : 1, s);
+  };
+  auto upcat_bwd = [&](int coarse, int skip, int dst) {
+    HW(sh.lev[skip]);
+    const size_t n = (size_t)H * W * sh.ch[skip];
+    k_upcat_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], sh.ch[coarse], sh.ch[skip], H, W, x->g[coarse], x->g[skip]);
+    return cudaGetLastError();
+  };
+  auto pool_bwd = [&](int src, int dst) {
+    HW(sh.lev[src]);
+    const size_t n = (size_t)H * W * sh.ch[src];
+    k_pool_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], H, W, sh.ch[src], x->g[src]);
+    return cudaGetLastError();
+  };
+  if ((e = conv_bwd(13)) || (e = conv_bwd(12)) || (e = upcat_bwd(S_D1, S_E0, S_U0))) return e;
+  if ((e = conv_bwd(11)) || (e = conv_bwd(10)) || (e = upcat_bwd(S_D2, S_E1, S_U1))) return e;
+  if ((e = conv_bwd(9)) || (e = conv_bwd(8)) || (e = upcat_bwd(S_B3, S_E2, S_U2))) return e;
+  if ((e = conv_bwd(7)) || (e = conv_bwd(6)) || (e = pool_bwd(S_E2, S_P3))) return e;
+  if ((e = conv_bwd(5)) || (e = conv_bwd(4)) || (e = pool_bwd(S_E1, S_P2))) return e;
+  if ((e = conv_bwd(3)) || (e = conv_bwd(2)) || (e = pool_bwd(S_E0, S_P1))) return e;
+  if ((e = conv_bwd(1)) || (e = conv_bwd(0))) return e;
+  return cudaSuccess;
+}
+
+void unet_dims(const vr_unet *u, int *nr, int *nz) {
+  *nr = u->nr;
+  *nz = u->nz;
+}
+
+int unet_precondition(const vr_unet *u, const double *r, double *z, const double *rr, const int *flags,
+                      cudaStream_t s) {
+  const int n = u->nr * u->nz;
+  k_in<<<grid_for(n), 256, 0, s>>>(r, n, rr, 0.0, u->x0, nullptr, flags);
+  if (cudaGetLastError() != cudaSuccess) return VR_ERR_CUDA;
+  if (unet_fwd(u, s) != cudaSuccess) return VR_ERR_CUDA;
+  k_out<<<grid_for(n), 256, 0, s>>>(u->y, n, rr, 0.0, z, flags);
+  return cudaGetLastError() == cudaSuccess ? VR_OK : VR_ERR_CUDA;
+}
+
+}  // namespace vr
+
+extern "C" int vr_unet_forward(vr_unet *u, const double *xh, double *yh) {
+  if (!u || !xh || !yh) return VR_ERR_ARG;
+  U_CUDA(u, cudaSetDevice(u->dev));
+  const int n = u->nr * u->nz;
+  double ss = 0.0;
+  for (int i = 0; i < n; i++) ss += xh[i] * xh[i];
+  const double s = std::sqrt(ss / n);
+  U_CUDA(u, cudaMemcpyAsync(u->xs, xh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
+  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, s > 0 ? 1.0 / s : 0.0, u->x0, nullptr, nullptr);
+  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, unet_fwd(u, u->stream));
+  k_out<<<grid_for(n), 256, 0, u->stream>>>(u->y, n, nullptr, s, u->xs, nullptr);
+  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, cudaMemcpyAsync(yh, u->xs, sizeof(double) * n, cudaMemcpyDeviceToHost, u->stream));
+  U_CUDA(u, cudaStreamSynchronize(u->stream));
+  return VR_OK;
+}
+
+__global__ static void k_f2d(const float *a, double *b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+__global__ static void k_d2f(const double *a, float *b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+extern "C" int vr_unet_backward(vr_unet *u, const double *xh, const double *gh, float *dw, double *dx) {
+  if (!u || !xh || !gh) return VR_ERR_ARG;
+  U_CUDA(u, cudaSetDevice(u->dev));
+  const int n = u->nr * u->nz;
+  U_CUDA(u, cudaMemcpyAsync(u->xs, xh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
+  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, 1.0, u->x0, nullptr, nullptr);
+  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, unet_fwd(u, u->stream));
+  U_CUDA(u, cudaMemcpyAsync(u->xs, gh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
+  k_d2f<<<grid_for(n), 256, 0, u->stream>>>(u->xs, u->gy, n);
+  U_CUDA(u, cudaMemsetAsync(u->gw, 0, sizeof(float) * u->nparam, u->stream));
+  U_CUDA(u, unet_bwd(u, dx != nullptr, u->stream));
+  if (dw) U_CUDA(u, cudaMemcpyAsync(dw, u->gw, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost, u->stream));
+  if (dx) {
+    k_f2d<<<grid_for(n), 256, 0, u->stream>>>(u->gx0, u->xs, n);
+    U_CUDA(u, cudaMemcpyAsync(dx, u->xs, sizeof(double) * n, cudaMemcpyDeviceToHost, u->stream));
+  }
+  U_CUDA(u, cudaStreamSynchronize(u->stream));
+  return VR_OK;
+}
+
+extern "C" int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *r_dev, int32_t nb, float lr, double *loss) {
+  if (!u || !k || !r_dev || nb < 1 || !(lr > 0)) return VR_ERR_ARG;
+  int32_t knr = 0, knz = 0;
+  vr_k2d_info(k, &knr, &knz, nullptr);
+  if (knr != u->nr || knz != u->nz) return unet_err(u, VR_ERR_ARG, "network and operator grids differ");
+  U_CUDA(u, cudaSetDevice(u->dev));
+  const int n = u->nr * u->nz;
+  cudaStream_t s = u->stream;
+  U_CUDA(u, cudaMemsetAsync(u->gw, 0, sizeof(float) * u->nparam, s));
+  U_CUDA(u, cudaMemsetAsync(u->dscal, 0, sizeof(double) * 8, s));
+  for (int b = 0; b < nb; b++) {
+    const double *r = r_dev + (size_t)b * n;
+    // x = r / rms(r) (double kept for the loss); ||x||^2 = n
+    U_CUDA(u, k2d_dot_self(k, r, u->dscal + 1, s));
+    k_in<<<grid_for(n), 256, 0, s>>>(r, n, u->dscal + 1, 0.0, u->x0, u->xs, nullptr);
+    U_CUDA(u, cudaGetLastError());
+    U_CUDA(u, unet_fwd(u, s));
+    U_CUDA(u, k2d_loss_grad(k, u->y, u->xs, (double)n, u->gy, u->dscal, s));
+    U_CUDA(u, unet_bwd(u, false, s));
+  }
+  // Adam with the batch-mean gradient
+  u->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)u->adam_t), c2 = 1.f - std::pow(b2, (float)u->adam_t);
+  k_adam<<<grid_for(u->nparam), 256, 0, s>>>(u->w32, u->gw, u->m1, u->m2, u->nparam, lr, 1.f / nb, b1, b2, c1, c2,
+                                            1e-8f);
+  k_wprep<<<grid_for(u->nparam), 256, 0, s>>>(u->w32, u->nparam, u->w16, u->wk);
+  U_CUDA(u, cudaGetLastError());
+  double h = 0.0;
+  U_CUDA(u, cudaMemcpyAsync(&h, u->dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
+  U_CUDA(u, cudaStreamSynchronize(s));
+  if (loss) *loss = h / nb;
+  return VR_OK;
+}
