@@ -207,6 +207,57 @@ def cpu_reference(steps, budget_s, q=None, part_sample=None):
     return NTH * NR * NZ / step_s / 1e6, done, os.cpu_count(), sample
 
 
+def ensemble_bench(local, steps):
+    """The ensemble workload (64 rings drawn from seed 1, 65,536 tracers each,
+    mixed form): the rings stepped as one ensemble (one graph launch per RK
+    substep, sweep tiles from the autotuner) against the same rings stepped
+    one context after another.  Host wall time around K steps with the device
+    synchronised on both sides (the ensemble's streams are internal)."""
+    import vring_b200 as V
+    from vring_b200 import ensemble as E
+    specs = E.ensemble_specs(64, seed=1)
+    rings = [E.make_ring(s, device=local) for s in specs]
+    runs = [r for r, _ in rings]
+    ncell = sum(E.cells(s) for s in specs)
+    # per-context loop (each ring's own substep graphs, rings in turn)
+    for r in runs:
+        r.iterate(1)
+    for r in runs:
+        r.sync()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for r in runs:
+            r.iterate(1)
+    for r in runs:
+        r.sync()
+    t_loop = time.perf_counter() - t0
+    ens = V.Ensemble(runs)
+    ens.autotune()
+    tiles = sorted({(s["nth"], s["nr"], s["nz"]): V.autotune(r) for s, r in zip(specs, runs)}.items())
+    ens.iterate(1)
+    ens.sync()
+    n0 = ens.launch_count
+    t0 = time.perf_counter()
+    ens.iterate(steps)
+    ens.sync()
+    t_ens = time.perf_counter() - t0
+    kernels = (ens.launch_count - n0) / steps
+    maxdiv = max(r.max_divergence() for r in runs)
+    out = {"rings": len(specs), "particles_per_ring": E.NPART, "cells": ncell, "steps": steps,
+           "precision": "mixed", "value": ncell * steps / t_ens / 1e6, "unit": UNIT,
+           "per_context_loop": ncell * steps / t_loop / 1e6,
+           "speedup_vs_loop": t_loop / t_ens, "graph_launches_per_step": 3,
+           "field_kernels_per_step": kernels, "max_div_u": maxdiv,
+           "tiles_r_z_by_grid": [[list(k), list(v)] for k, v in tiles],
+           "timing": "host wall time of K steps, device synchronised on both sides"}
+    ens.close()
+    for r, p in rings:
+        p.attach(False)
+        p.close()
+        r.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -236,6 +287,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-ring ensemble timing")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NR", "NTHETA", "NZ"), default=None,
                     help="smaller grid for profiling captures (not the benchmark workload)")
     ap.add_argument("--nparticles", type=int, default=None,
@@ -308,6 +360,11 @@ def main():
     value = replicas.throughput(ncell * args.steps, world, ms_max / 1e3) / 1e6
     maxdiv = run.max_divergence()
     nonfinite = run.count_nonfinite()
+    # the FP64 state after warm-up + timed steps, for the mixed form's per-field error
+    ref_fields = None
+    if not args.no_mixed:
+        ref_fields = {n: run.get(n) for n in ("q1", "q2", "q3", "pres")}
+        ref_fields["xyz"] = part.state()[0][:, 0:3].copy()
 
     # ---- end to end: per step, velocity in from pinned host memory, one step
     # through the C ABI, velocity back to pinned host memory ------------------
@@ -371,21 +428,38 @@ def main():
         prof_m = rm_.profile_read()
         rm_.profile(False)
         clk_m = clocks_m.stop()
+        # error per field against the FP64 form after the same steps (the FP64
+        # form matches the oracle to 1e-13 per step at this size)
+        import numpy as np
+        uscale = max(float(np.abs(ref_fields[n]).max()) for n in ("q1", "q2", "q3"))
+        field_err = {
+            "velocity": max(float(np.abs(rm_.get(n) - ref_fields[n]).max()) for n in ("q1", "q2", "q3")) / uscale,
+            "pressure": float(np.abs(rm_.get("pres") - ref_fields["pres"]).max() / np.abs(ref_fields["pres"]).max()),
+            "particle_positions": float(np.abs(pm.state()[0][:, 0:3] - ref_fields["xyz"]).max() / ZMAX),
+            "after_steps": args.warmup + args.steps,
+            "norm": "max |mixed - fp64| / max |fp64| per field; positions over the domain length"}
+        del ref_fields
         value_m = replicas.throughput(ncell * args.steps, world, ms_m / 1e3) / 1e6
         mixed = {"value": value_m, "unit": UNIT, "ms_per_step": ms_m / args.steps,
                  "vs_fp64": value_m / value, "max_div_u": rm_.max_divergence(),
                  "storage": "float: dq, ru, prg, pres; double: q, sweep work arrays, Poisson "
                             "right-hand side, transforms, dph",
                  "tolerance": "max|u_mixed - u_fp64| <= 2e-6 max|u| after 5 steps (tests/test_gpu_mixed.py)",
+                 "error_vs_fp64": field_err,
                  "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof_m.items())},
                  "clocks": clk_m}
         pm.close()
         rm_.close()
 
-    # ---- roofline of the dominant kernel family -------------------------------
-    peak, peak_kind = peaks()
     # the committed DRAM traffic belongs to the benchmark size; a reduced run reports none
     reduced = args.grid is not None or args.nparticles is not None
+    # ---- the 64-ring ensemble workload -----------------------------------------
+    ensemble = None
+    if not args.no_ensemble and not reduced and world == 1:
+        ensemble = ensemble_bench(local, 5)
+
+    # ---- roofline of the dominant kernel family -------------------------------
+    peak, peak_kind = peaks()
     roof = roofline(prof, args.steps, ncell, peak, peak_kind, {} if reduced else traffic_table(),
                     ms_max / args.steps)
 
@@ -402,6 +476,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": bench_config(world),
             "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles, "mixed": mixed,
+            "ensemble": ensemble,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,

@@ -275,6 +275,39 @@ VR_API int vr_solve_lap_thom(const double *rhs, double *sol, const double *aa, c
 VR_API int vr_solve_lap_bthom(const double *rhs, double *sol, const double *b1, const double *b2,
                        const double *b3, int32_t m, int32_t n, int32_t nbatch);
 
+/* ---- ensembles of independent rings and the tile autotuner --------------- */
+/* No reference counterpart (the reference runs one ring per MPI job).  An
+ * ensemble steps rings of any grids resident on one device: each RK substep of
+ * all rings is one CUDA graph launch whose branches are the rings' own fused
+ * substeps, each ring on its own stream, so small rings run side by side.  A
+ * ring's results are bit-identical to stepping it alone.  The contexts stay
+ * owned by the caller and must outlive the ensemble; their inflow must be off
+ * (the boundary values then do not change between steps) and per-kernel
+ * profiling off.  Particle classes attached to a ring advance before substep 1
+ * as in vr_iterate.  Work queued on a ring's own stream before vr_ens_iterate
+ * runs first, and work queued on it afterwards runs after the ensemble's. */
+typedef struct vr_ens vr_ens;
+VR_API int vr_ens_create(vr_ctx *const *rings, int32_t n, vr_ens **out);
+VR_API int vr_ens_destroy(vr_ens *e);
+VR_API const char *vr_ens_last_error(const vr_ens *e);
+VR_API int vr_ens_iterate(vr_ens *e, int32_t nsteps);
+VR_API int vr_ens_sync(vr_ens *e);
+/* kernels launched through the ensemble's graphs so far */
+VR_API int vr_ens_launch_count(const vr_ens *e, int64_t *n);
+/* vr_autotune for every ring; each grid class (ntheta, nr, nz, precision) is
+ * timed once per process (force != 0 re-times each class once) */
+VR_API int vr_ens_autotune(vr_ens *e, int32_t force);
+/* Times the candidate tile shapes of the r and z sweeps on this context's grid
+ * (r: 16-line TMA tiles, 8-line TMA tiles, register chunks; z: 8-line TMA,
+ * 16-line TMA, register chunks; variants a line length does not fit fall back
+ * to register chunks), keeps the fastest pair and caches it per grid class for
+ * the process.  The context's fields and clock are restored afterwards (the
+ * trials need a temporary device copy of the state).  choice (may be NULL)
+ * receives {r variant, z variant}. */
+VR_API int vr_autotune(vr_ctx *ctx, int32_t force, int32_t choice[2]);
+/* set the sweep tile variants by hand (0 = the default shapes) */
+VR_API int vr_set_tiles(vr_ctx *ctx, int32_t r_variant, int32_t z_variant);
+
 /* ---- axisymmetric pressure solves with Krylov methods (Ntheta = 1) -------- */
 /* No reference counterpart: the reference solves the pressure directly
  * (poisson_solve.F90:140-179, 270-323).  The operator is the reference's at

@@ -126,6 +126,16 @@ def lib():
         L.vr_solve_lap_thom.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.vr_solve_lap_bthom.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32]
         L.vr_solve_lap_thom_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, i32, vp]
+        L.vr_ens_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
+        L.vr_ens_destroy.argtypes = [vp]
+        L.vr_ens_last_error.restype = C.c_char_p
+        L.vr_ens_last_error.argtypes = [vp]
+        L.vr_ens_iterate.argtypes = [vp, i32]
+        L.vr_ens_sync.argtypes = [vp]
+        L.vr_ens_launch_count.argtypes = [vp, C.POINTER(i64)]
+        L.vr_ens_autotune.argtypes = [vp, i32]
+        L.vr_autotune.argtypes = [vp, i32, C.POINTER(i32)]
+        L.vr_set_tiles.argtypes = [vp, i32, i32]
         L.vr_k2d_create.argtypes = [C.POINTER(K2dDesc), C.POINTER(vp)]
         L.vr_k2d_destroy.argtypes = [vp]
         L.vr_k2d_last_error.restype = C.c_char_p
@@ -610,3 +620,57 @@ class UNet:
         self._chk(lib().vr_unet_train_step(self._h, k2d._h, C.c_void_p(r_ptr), nb, lr, C.byref(loss)),
                   "unet_train_step")
         return loss.value
+
+
+class Ensemble:
+    """Independent rings (Run objects on one device) stepped together: one
+    CUDA graph launch per RK substep covering every ring (``vr_ens_*``)."""
+
+    def __init__(self, runs):
+        self.runs = list(runs)
+        arr = (C.c_void_p * len(self.runs))(*[r._h.value for r in self.runs])
+        self._h = C.c_void_p()
+        rc = lib().vr_ens_create(arr, len(self.runs), C.byref(self._h))
+        if rc:
+            raise VrError(rc, "vr_ens_create")
+
+    def _chk(self, rc, what):
+        if rc:
+            raise VrError(rc, "%s: %s" % (what, (lib().vr_ens_last_error(self._h) or b"").decode()))
+
+    def close(self):
+        if self._h:
+            lib().vr_ens_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self, nsteps: int) -> None:
+        self._chk(lib().vr_ens_iterate(self._h, nsteps), "ens_iterate")
+
+    def sync(self) -> None:
+        self._chk(lib().vr_ens_sync(self._h), "ens_sync")
+
+    def autotune(self, force: bool = False) -> None:
+        self._chk(lib().vr_ens_autotune(self._h, 1 if force else 0), "ens_autotune")
+
+    @property
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._chk(lib().vr_ens_launch_count(self._h, C.byref(n)), "ens_launch_count")
+        return n.value
+
+
+def autotune(run: Run, force: bool = False):
+    """``vr_autotune``: the fastest (r, z) sweep tile variants for run's grid."""
+    ch = (C.c_int32 * 2)()
+    run._chk(lib().vr_autotune(run._h, 1 if force else 0, ch), "autotune")
+    return ch[0], ch[1]
+
+
+def set_tiles(run: Run, r_variant: int, z_variant: int) -> None:
+    run._chk(lib().vr_set_tiles(run._h, r_variant, z_variant), "set_tiles")

@@ -532,6 +532,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
   for (auto &o : fl) {
     if (cudaMalloc(o.p, o.w * o.n) != cudaSuccess) return fail(VR_ERR_OOM);
     if (cudaMemsetAsync(*o.p, 0, o.w * o.n, c->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
+    c->state.emplace_back(*o.p, o.w * o.n);
   }
   if (cudaMalloc(&c->d_count, sizeof(unsigned long long) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMemsetAsync(c->d_count, 0, sizeof(unsigned long long) * 4, c->stream) != cudaSuccess)
@@ -874,7 +875,7 @@ extern "C" int vr_uppres(vr_ctx *c) {
 // ---------------------------------------------------------------------------
 // fused substep
 // ---------------------------------------------------------------------------
-static int enqueue_substep(vr_ctx *c, int irk) {
+int vr::enqueue_substep(vr_ctx *c, int irk) {
   c->irk = irk;
   Rk rk = rk_of(c);
   double cs, cor;

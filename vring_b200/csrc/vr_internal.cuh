@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/vring_b200.h"
@@ -153,6 +154,12 @@ struct vr_ctx {
   // analysis: para%stat (run.F90:365-374), zm on the device, block partials
   double stat[20];
   double *ana_zm, *ana_part;
+  // every device field with its size in bytes (the autotuner's snapshot)
+  std::vector<std::pair<void *, size_t>> state;
+  // sweep tile variants picked by the autotuner (0 = the default shapes):
+  // r: 0 TMA 16-line tiles, 1 TMA 8-line tiles, 2 register chunks;
+  // z: 0 TMA 8-line tiles, 1 TMA 16-line tiles, 2 register chunks
+  int tune_r, tune_z;
 };
 
 namespace vr {
@@ -214,6 +221,10 @@ bool rec_write(FILE *f, const void *buf, size_t n);
 bool rec_read(FILE *f, void *buf, size_t n);
 bool data_write(FILE *f, const double *p, size_t n);
 bool data_read(FILE *f, double *p, size_t n);
+
+// the launch sequence of one fused RK substep on the context's current stream
+// (vr_ctx.cu); no graph, no host synchronisation
+int enqueue_substep(vr_ctx *c, int irk);
 
 // enqueue the nsubdt Euler substeps of one particle class on stream s
 // (vr_particles.cu)

@@ -1265,13 +1265,19 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const C
     p.nbx = (s.nth + 31) / 32;
     const Geo &g = c->geo;
     LaunchScope ls(c, s.se == g.nth ? PK_RSWEEP : PK_ZSWEEP);
-    // TMA-pipelined persistent form, two 256-thread CTAs per SM: 16-line
-    // tiles along r, 8-line tiles along z (lines of up to 544 positions need
-    // the narrower tile to keep two stages per CTA in shared memory)
-    cudaError_t e =
-        s.se == g.nth
-            ? run_chunk_tma<16, 16, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, 1, nm2, c->nsm, c->d_status, c->stream)
-            : run_chunk_tma<8, 32, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, 2, nm2, c->nsm, c->d_status, c->stream);
+    // TMA-pipelined persistent form, two 256-thread CTAs per SM: by default
+    // 16-line tiles along r, 8-line tiles along z (lines of up to 544
+    // positions need the narrower tile to keep two stages per CTA in shared
+    // memory); the autotuner may pick the other tile or the register form
+    const bool along_r = s.se == g.nth;
+    const int v = along_r ? c->tune_r : c->tune_z;
+    const int ldim = along_r ? 1 : 2;
+    cudaError_t e = cudaErrorNotSupported;
+    if (v == 2) {
+    } else if ((v == 0) == along_r)
+      e = run_chunk_tma<16, 16, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+    else
+      e = run_chunk_tma<8, 32, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
     if (e != cudaErrorNotSupported) return e;
     return launch_chunk(p, p.nbx * nm2, c->stream);
   }
