@@ -6,7 +6,8 @@ Tolerances: the operator and the direct solve to 1e-12 of the scale; every
 Krylov method to a relative residual of 1e-10 in its own form, and its answer
 to 1e-8 of the direct solve's scale (the residual bound does not bound the
 error of an ill-conditioned system more tightly; the measured agreement is
-printed)."""
+printed).  Solved to 1e-12, plain CG agrees with the reference's direct solve
+to 1e-10."""
 import numpy as np
 import pytest
 
@@ -76,12 +77,15 @@ def test_vr2d_uniform_deck_matches_reference_direct_solve():
     o.laplace_solve()
     ref = o.field("dph")[0, 1:nr + 1, 1:nz + 1].copy()
     k = V.K2d(faces, nz, 15.0)
-    for method in ("cg", "bicgstab"):
-        x, it, rr, ms = k.solve(f, method, tol=1e-10)
+    # to 1e-10 the answers sit within 3e-8 of the reference's; to 1e-12 within
+    # 1e-10 (CG) and 1e-9 (BiCGSTAB on the unsymmetric form)
+    for method, tol, bound in (("cg", 1e-10, 1e-8), ("cg", 1e-12, 1e-10), ("bicgstab", 1e-10, 1e-7),
+                               ("bicgstab", 1e-12, 1e-9)):
+        x, it, rr, ms = k.solve(f, method, tol=tol)
         err = np.abs(x - ref).max() / np.abs(ref).max()
-        print("VR2D deck uniform 512x1024 %s: %d iterations, relres %.2e, %.1f ms, vs reference solve %.2e"
-              % (method, it, rr, ms, err))
-        assert rr <= 1e-10 and err <= 1e-8
+        print("VR2D deck uniform 512x1024 %s to %.0e: %d iterations, relres %.2e, %.1f ms, vs reference solve %.2e"
+              % (method, tol, it, rr, ms, err))
+        assert rr <= tol and err <= bound
     xd = k.direct(f)
     assert np.abs(xd - ref).max() <= 1e-11 * np.abs(ref).max()
     k.close()
