@@ -369,15 +369,21 @@ VR_API int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, double *
  * channel.  No biases and identity activations, so the network is a linear
  * map (a valid preconditioner for the flexible CG).  Weights are BF16 (an FP32
  * master copy is kept for training), activations BF16, every sum accumulates
- * in FP32.  nr and nz must be multiples of 8; ch[l] multiples of 8, <= 128. */
+ * in FP32.  nr and nz must be multiples of 8; ch[l] multiples of 8, ch[0] and
+ * every 3x3 layer's output at most 64, its input at most 128. */
 typedef struct vr_unet vr_unet;
 typedef struct vr_unet_desc {
   int32_t abi_version;
   int32_t nr, nz;
   int32_t ch[4];
   int32_t device;
-  int32_t flags;  /* reserved, 0 */
+  int32_t flags;  /* 0, or VR_UNET_CUDA_CORES */
 } vr_unet_desc;
+/* The forward 3x3 convolutions run on the tensor cores (tcgen05, BF16 x BF16
+ * -> FP32 in tensor memory) by default; this flag runs them on the CUDA cores
+ * instead (same rounding points, FP32 sums in another order).  The gradients
+ * always run on the CUDA cores. */
+#define VR_UNET_CUDA_CORES 1
 VR_API int vr_unet_create(const vr_unet_desc *desc, uint64_t seed, vr_unet **out);
 VR_API int vr_unet_destroy(vr_unet *u);
 VR_API const char *vr_unet_last_error(const vr_unet *u);

@@ -39,6 +39,29 @@ def test_forward_matches_oracle():
     net.close()
 
 
+@pytest.mark.parametrize("grid", [(32, 64), (64, 128)])
+def test_tensor_core_forward_matches_cuda_core_forward_and_oracle(grid):
+    """The tcgen05 implicit-GEMM convolutions against the CUDA-core ones and
+    the oracle, on the network the preconditioner uses (16, 32, 48, 64)."""
+    import vring_b200 as V
+    from oracle import unet_ref as U
+    nr, nz = grid
+    ch = (16, 32, 48, 64)
+    tc = V.UNet(nr, nz, ch, seed=9)
+    cc = V.UNet(nr, nz, ch, seed=9, flags=V.UNet.CUDA_CORES)
+    w = tc.get_params()
+    assert np.array_equal(w, cc.get_params())
+    x = np.random.default_rng(4).standard_normal((nr, nz))
+    s = np.sqrt(np.mean(x ** 2))
+    yt, yc = tc.forward(x), cc.forward(x)
+    yo = s * U.forward(w, ch, x / s)
+    print("%s: tensor cores vs oracle %.2e, CUDA cores vs oracle %.2e, between %.2e"
+          % (grid, _rel(yt, yo), _rel(yc, yo), _rel(yt, yc)))
+    assert _rel(yt, yo) <= 5e-3 and _rel(yc, yo) <= 5e-3
+    tc.close()
+    cc.close()
+
+
 def test_gradients_match_oracle():
     import vring_b200 as V
     from oracle import unet_ref as U

@@ -562,9 +562,13 @@ class UNet:
     """The learned preconditioner (``vr_unet_*``): a 4-level linear U-Net with
     BF16 weights and activations and FP32 accumulation on an (nr, nz) grid."""
 
-    def __init__(self, nr: int, nz: int, ch=(16, 32, 48, 64), seed: int = 0, device: int = 0):
+    CUDA_CORES = 1
+
+    def __init__(self, nr: int, nz: int, ch=(16, 32, 48, 64), seed: int = 0, device: int = 0, flags: int = 0):
+        """flags = UNet.CUDA_CORES runs the forward convolutions on the CUDA
+        cores instead of the tensor cores."""
         self.nr, self.nz, self.ch = int(nr), int(nz), tuple(int(c) for c in ch)
-        d = UnetDesc(VR_ABI_VERSION, self.nr, self.nz, (C.c_int32 * 4)(*self.ch), device, 0)
+        d = UnetDesc(VR_ABI_VERSION, self.nr, self.nz, (C.c_int32 * 4)(*self.ch), device, flags)
         self._h = C.c_void_p()
         rc = lib().vr_unet_create(C.byref(d), seed, C.byref(self._h))
         if rc:

@@ -33,6 +33,7 @@
 
 #include "vr_internal.cuh"
 #include "vr_learned.cuh"
+#include "vr_umma.cuh"
 
 namespace vr {
 
@@ -55,6 +56,10 @@ struct vr_unet {
   // copy for the data gradient, gradient, Adam moments
   float *w32 = nullptr, *wk = nullptr, *wflip = nullptr, *gw = nullptr, *m1 = nullptr, *m2 = nullptr;
   __nv_bfloat16 *w16 = nullptr;
+  __nv_bfloat16 *wpk = nullptr;  // per 3x3 layer [nout][9][cinp] BF16, zero padded (tensor-core form)
+  size_t wpk_off[14] = {};
+  bool cuda_cores = false;       // forward convolutions on CUDA cores instead of tensor cores
+  unsigned *status = nullptr;    // bit 0: a bounded tensor-core wait gave up
   int64_t adam_t = 0;
   // activations (bf16) and their gradients (fp32), one per tensor slot
   __nv_bfloat16 *x0 = nullptr;            // input, 1 channel
@@ -151,6 +156,135 @@ __global__ void __launch_bounds__(256) k_conv3(const TI *__restrict__ in, int H,
 #pragma unroll
     for (int co = 0; co < CO; co++)
       if (co < cout) op[co] = fromf<TO>(accumulate ? acc[co] + tof(op[co]) : acc[co]);
+  }
+}
+
+// The same 3x3 convolution on the tensor cores (BF16 in, FP32 accumulate):
+// an implicit GEMM with M = 128 output pixels per CTA (the rows of A are the
+// CTA's pixels, its columns the 9 taps x CINP input channels of their
+// neighbourhoods), N = NOUT output channels and K = 9 CINP, where CINP and NOUT
+// are cin and cout rounded up to 16.  K runs in blocks of 64 columns through
+// two shared-memory stages that all 128 threads fill -- the im2col gather of A
+// and the packed weights B, both K-major with the 128-byte swizzle -- while
+// the tensor cores work on the other stage; one thread issues the four
+// K-steps of a block and commits them to the stage's mbarrier.  The FP32
+// accumulator stays in tensor memory (128 lanes = pixels, NOUT columns) until
+// the epilogue, where each warp loads its 32 lanes and stores BF16.  Every
+// mbarrier wait is bounded; a wait that gives up sets bit 0 of *status, and
+// the CTA still waits (bounded) for its MMAs and frees its tensor memory.
+template <int CINP, int NOUT>
+__global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W, int cin,
+                                                const __nv_bfloat16 *__restrict__ wpk, int cout,
+                                                __nv_bfloat16 *__restrict__ out, unsigned *status) {
+  static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
+  constexpr int K = 9 * CINP;
+  constexpr int KB = (K + 63) / 64;
+  constexpr int ABYTES = 128 * 128, BBYTES = NOUT * 128, STAGE = ABYTES + BBYTES;
+  constexpr uint32_t NCOLS = NOUT <= 32 ? 32 : 64;
+  constexpr uint32_t IDESC = umma_idesc_bf16_f32(128, NOUT);
+  static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzle");
+  extern __shared__ uint8_t smraw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  __shared__ uint64_t bar[2];
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    tmem_alloc(&tbase, NCOLS);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+  const int P = H * W;
+  const int p = blockIdx.x * 128 + tid;  // this thread's row of A and of D
+  const int pj = p % H, pk = p / H;
+  const bool pin = p < P;
+  bool ok = true;
+  for (int kb = 0; kb < KB; kb++) {
+    const int s = kb & 1;
+    uint8_t *As = sm + s * STAGE;
+    uint8_t *Bs = As + ABYTES;
+    // the MMAs of block kb - 2 read this stage: wait for their commit
+    if (kb >= 2 && !mbar_wait(&bar[s], (unsigned)((kb - 2) >> 1) & 1u)) ok = false;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int k0 = kb * 64 + c * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (pin && k0 < K) {
+        const int t = k0 / CINP, ci = k0 % CINP;  // 8 columns inside one tap (CINP % 16 == 0)
+        const int j = pj + t / 3 - 1, k = pk + t % 3 - 1;
+        if (ci < cin && j >= 0 && j < H && k >= 0 && k < W) {
+          const __nv_bfloat16 *src = in + ((size_t)j + (size_t)H * k) * cin + ci;
+          if ((cin & 7) == 0) {
+            v = *reinterpret_cast<const uint4 *>(src);
+          } else {
+            __nv_bfloat16 e[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) e[q] = (ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
+            v = *reinterpret_cast<const uint4 *>(e);
+          }
+        }
+      }
+      *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = v;
+    }
+    for (int e = tid; e < NOUT * 8; e += 128) {
+      const int n = e >> 3, c = e & 7, k0 = kb * 64 + c * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (k0 < K) v = *reinterpret_cast<const uint4 *>(wpk + (size_t)n * K + k0);
+      *reinterpret_cast<uint4 *>(Bs + sw128_off(n, c)) = v;
+    }
+    fence_proxy_async();  // the generic-proxy stores above, before the tensor cores read them
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(Bs);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        if (kb * 64 + kk * 16 < K) umma_bf16(tmem, ad + (uint64_t)(2 * kk), bd + (uint64_t)(2 * kk), IDESC, (kb | kk) ? 1u : 0u);
+      umma_commit(&bar[s]);
+    }
+  }
+  // the last commit arrives once every MMA of the CTA is done
+  if (!mbar_wait(&bar[(KB - 1) & 1], (unsigned)((KB - 1) >> 1) & 1u)) ok = false;
+  tc_fence_after();
+#pragma unroll
+  for (int c0 = 0; c0 < NOUT; c0 += 16) {
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+    if (pin && ok && c0 < cout) {
+      __nv_bfloat16 *dst = out + (size_t)p * cout + c0;
+      if (c0 + 16 <= cout) {
+        __align__(16) __nv_bfloat16 b[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) b[i] = __float2bfloat16_rn(v[i]);
+        reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(b)[0];
+        reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(b)[1];
+      } else {
+        for (int i = 0; i < 16 && c0 + i < cout; i++) dst[i] = __float2bfloat16_rn(v[i]);
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicOr(status, 1u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+}
+
+// packed tensor-core weights: wpk[n][tap][ci] = bf16(w[n][tap][ci]) for
+// n < cout, ci < cin, zero elsewhere
+__global__ void k_wpack(const float *__restrict__ w, int cin, int cout, int cinp, int nout,
+                        __nv_bfloat16 *__restrict__ wpk) {
+  const int n_el = nout * 9 * cinp;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += gridDim.x * blockDim.x) {
+    const int ci = e % cinp, t = (e / cinp) % 9, n = e / (9 * cinp);
+    const float v = (n < cout && ci < cin) ? w[((size_t)n * 9 + t) * cin + ci] : 0.f;
+    wpk[e] = __float2bfloat16_rn(v);
   }
 }
 
@@ -362,6 +496,47 @@ static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, in
   return cudaErrorInvalidValue;
 }
 
+template <int CINP, int NOUT>
+static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
+                              __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
+  const size_t sm = 1024 + 2 * (size_t)(128 * 128 + NOUT * 128);
+  cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
+  if (e) return e;
+  const int P = H * W;
+  k_conv3_tc<CINP, NOUT><<<(P + 127) / 128, 128, sm, s>>>(in, H, W, cin, wpk, cout, out, status);
+  return cudaGetLastError();
+}
+
+template <int CINP>
+static cudaError_t conv3_tc_c(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
+                              __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
+  switch ((cout + 15) / 16) {
+    case 1: return conv3_tc_n<CINP, 16>(in, H, W, cin, wpk, cout, out, status, s);
+    case 2: return conv3_tc_n<CINP, 32>(in, H, W, cin, wpk, cout, out, status, s);
+    case 3: return conv3_tc_n<CINP, 48>(in, H, W, cin, wpk, cout, out, status, s);
+    case 4: return conv3_tc_n<CINP, 64>(in, H, W, cin, wpk, cout, out, status, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// tensor-core 3x3 convolution: cin up to 128, cout up to 64
+static cudaError_t conv3_tc(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
+                            __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
+  switch ((cin + 15) / 16) {
+    case 1: return conv3_tc_c<16>(in, H, W, cin, wpk, cout, out, status, s);
+    case 2: return conv3_tc_c<32>(in, H, W, cin, wpk, cout, out, status, s);
+    case 3: return conv3_tc_c<48>(in, H, W, cin, wpk, cout, out, status, s);
+    case 4: return conv3_tc_c<64>(in, H, W, cin, wpk, cout, out, status, s);
+    case 5: return conv3_tc_c<80>(in, H, W, cin, wpk, cout, out, status, s);
+    case 6: return conv3_tc_c<96>(in, H, W, cin, wpk, cout, out, status, s);
+    case 7: return conv3_tc_c<112>(in, H, W, cin, wpk, cout, out, status, s);
+    case 8: return conv3_tc_c<128>(in, H, W, cin, wpk, cout, out, status, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static int round16(int x) { return (x + 15) / 16 * 16; }
+
 template <class TI>
 static cudaError_t wgrad3(const float *dout, int H, int W, int cout, const TI *in, int cin, float *dw,
                           cudaStream_t s) {
@@ -373,6 +548,20 @@ static cudaError_t wgrad3(const float *dout, int H, int W, int cout, const TI *i
 }
 
 static int grid_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+
+// BF16 copy, rounded FP32 copy and the packed tensor-core weights of every
+// 3x3 layer, from the FP32 master weights
+static cudaError_t unet_prep_weights(vr_unet *u, cudaStream_t s) {
+  k_wprep<<<grid_for(u->nparam), 256, 0, s>>>(u->w32, u->nparam, u->w16, u->wk);
+  for (int i = 0; i < 14; i++) {
+    const UnetLayer &L = u->L[i];
+    const int cinp = round16(L.cin), nout = round16(L.cout);
+    k_wpack<<<grid_for((size_t)nout * 9 * cinp), 256, 0, s>>>(u->wk + L.woff, L.cin, L.cout, cinp, nout,
+                                                             u->wpk + u->wpk_off[i]);
+  }
+  return cudaGetLastError();
+}
 
 }  // namespace vr
 
@@ -427,7 +616,7 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
   if (d->abi_version != VR_ABI_VERSION) return VR_ERR_DESC;
   if (d->nr < 8 || d->nz < 8 || d->nr % 8 || d->nz % 8 || (int64_t)d->nr * d->nz > ((int64_t)1 << 24)) return VR_ERR_DESC;
   for (int l = 0; l < 4; l++)
-    if (d->ch[l] < 8 || d->ch[l] > 128 || d->ch[l] % 8) return VR_ERR_DESC;
+    if (d->ch[l] < 8 || d->ch[l] > 64 || d->ch[l] % 8) return VR_ERR_DESC;  // a 3x3 layer's output <= 64
   if (d->ch[0] > 64) return VR_ERR_DESC;  // the head's gradient keeps c0 sums per thread
   if (d->ch[3] + d->ch[2] > 128 || d->ch[2] + d->ch[1] > 128 || d->ch[1] + d->ch[0] > 128) return VR_ERR_DESC;
   int ndev = 0;
@@ -483,6 +672,15 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
     if (cudaMalloc(p, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&u->wflip, sizeof(float) * maxflip) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&u->w16, sizeof(__nv_bfloat16) * u->nparam) != cudaSuccess) return fail(VR_ERR_OOM);
+  size_t npk = 0;
+  for (int i = 0; i < 14; i++) {
+    u->wpk_off[i] = npk;
+    npk += (size_t)round16(u->L[i].cout) * 9 * round16(u->L[i].cin);
+  }
+  if (cudaMalloc(&u->wpk, sizeof(__nv_bfloat16) * npk) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&u->status, sizeof(unsigned)) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMemset(u->status, 0, sizeof(unsigned)) != cudaSuccess) return fail(VR_ERR_CUDA);
+  u->cuda_cores = (d->flags & VR_UNET_CUDA_CORES) != 0;
   if (cudaMalloc(&u->x0, sizeof(__nv_bfloat16) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&u->y, sizeof(float) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&u->gy, sizeof(float) * P0) != cudaSuccess) return fail(VR_ERR_OOM);
@@ -499,7 +697,7 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
     return fail(VR_ERR_CUDA);
   if (cudaMemset(u->m1, 0, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_CUDA);
   if (cudaMemset(u->m2, 0, sizeof(float) * u->nparam) != cudaSuccess) return fail(VR_ERR_CUDA);
-  k_wprep<<<grid_for(u->nparam), 256, 0, u->stream>>>(u->w32, u->nparam, u->w16, u->wk);
+  if (unet_prep_weights(u, u->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
   if (cudaStreamSynchronize(u->stream) != cudaSuccess) return fail(VR_ERR_CUDA);
   *out = u;
   return VR_OK;
@@ -518,6 +716,8 @@ extern "C" int vr_unet_destroy(vr_unet *u) {
   for (float *p : fp)
     if (p) cudaFree(p);
   if (u->w16) cudaFree(u->w16);
+  if (u->wpk) cudaFree(u->wpk);
+  if (u->status) cudaFree(u->status);
   if (u->x0) cudaFree(u->x0);
   if (u->xs) cudaFree(u->xs);
   if (u->dscal) cudaFree(u->dscal);
@@ -545,8 +745,7 @@ extern "C" int vr_unet_set_params(vr_unet *u, const float *w) {
   if (!u || !w) return VR_ERR_ARG;
   U_CUDA(u, cudaSetDevice(u->dev));
   U_CUDA(u, cudaMemcpyAsync(u->w32, w, sizeof(float) * u->nparam, cudaMemcpyHostToDevice, u->stream));
-  k_wprep<<<grid_for(u->nparam), 256, 0, u->stream>>>(u->w32, u->nparam, u->w16, u->wk);
-  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, unet_prep_weights(u, u->stream));
   U_CUDA(u, cudaStreamSynchronize(u->stream));
   return VR_OK;
 }
@@ -567,7 +766,9 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
     const UnetLayer &L = u->L[li];
     HW(L.level, H, W);
     const __nv_bfloat16 *in = kConvIn[li] < 0 ? u->x0 : x->a[kConvIn[li]];
-    return conv3<__nv_bfloat16, __nv_bfloat16>(in, H, W, L.cin, u->wk + L.woff, L.cout, x->a[kConvOut[li]], 0, s);
+    if (u->cuda_cores)
+      return conv3<__nv_bfloat16, __nv_bfloat16>(in, H, W, L.cin, u->wk + L.woff, L.cout, x->a[kConvOut[li]], 0, s);
+    return conv3_tc(in, H, W, L.cin, u->wpk + u->wpk_off[li], L.cout, x->a[kConvOut[li]], u->status, s);
   };
   auto pool = [&](int src, int dst) {
     HW(sh.lev[src], H, W);
@@ -737,8 +938,7 @@ extern "C" int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *r_dev, in
   const float c1 = 1.f - std::pow(b1, (float)u->adam_t), c2 = 1.f - std::pow(b2, (float)u->adam_t);
   k_adam<<<grid_for(u->nparam), 256, 0, s>>>(u->w32, u->gw, u->m1, u->m2, u->nparam, lr, 1.f / nb, b1, b2, c1, c2,
                                             1e-8f);
-  k_wprep<<<grid_for(u->nparam), 256, 0, s>>>(u->w32, u->nparam, u->w16, u->wk);
-  U_CUDA(u, cudaGetLastError());
+  U_CUDA(u, unet_prep_weights(u, s));
   double h = 0.0;
   U_CUDA(u, cudaMemcpyAsync(&h, u->dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
   U_CUDA(u, cudaStreamSynchronize(s));
