@@ -207,6 +207,28 @@ def cpu_reference(steps, budget_s, q=None, part_sample=None):
     return NTH * NR * NZ / step_s / 1e6, done, os.cpu_count(), sample
 
 
+def inertial_bench(run, stream, e0, e1, calls=3):
+    import vring_b200 as V
+    run.set_stream(stream.cuda_stream)
+    p = V.Part(run, 1, NPART, 0)
+    pu, pv = particle_state(NPART)
+    p.set_state(pu, pv, None, NPART)
+    del pu, pv
+    p.iter_part(1)
+    run.sync()
+    e0.record(stream)
+    for _ in range(calls):
+        p.iter_part(1)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    out = {"n": NPART, "mode": "inertial", "class": 1, "nsubdt": p.nsubdt, "ms_per_step": ms,
+           "value": NPART / (ms / 1e3), "unit": "particle-steps/s (iter_part alone, CUDA events)",
+           "substeps_per_s": NPART * p.nsubdt / (ms / 1e3), "live_after": p.counts["npart"]}
+    p.close()
+    return out
+
+
 def ensemble_bench(local, steps):
     """The ensemble workload (64 rings drawn from seed 1, 65,536 tracers each,
     mixed form): the rings stepped as one ensemble (one graph launch per RK
@@ -471,6 +493,11 @@ def main():
                  "value": NPART * args.steps / (part_ms / 1e3) if part_ms > 0 else None,
                  "unit": "particle-steps/s (particle kernel time)",
                  "substeps_per_s": NPART * part.nsubdt * args.steps / (part_ms / 1e3) if part_ms > 0 else None}
+    # the reference's inertial particles (class 1: Stokes drag, the 117-word
+    # state with Jacobian and Hessian rates; part_tools.F90:241-251, 847-870)
+    # on the same field and cloud, timed alone over a few iter_part calls
+    if not reduced:
+        particles["inertial"] = inertial_bench(run, stream, e0, e1)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
