@@ -398,11 +398,16 @@ VR_API int vr_unet_forward(vr_unet *u, const double *x, double *y);
 /* gradients of L = sum(g * N(x)) for the gradient check: dL/dw (FP32, host,
  * nparams) and dL/dx (host, nr*nz); the unit-RMS scaling is not applied */
 VR_API int vr_unet_backward(vr_unet *u, const double *x, const double *g, float *dw, double *dx);
-/* One Adam step on a batch of nb residual pairs resident on the device:
- * r (nb x nr*nz, S-form residuals) with loss
- * L = mean_b ||S N(r_b) - r_b||^2 / ||r_b||^2 (S of the vr_k2d);
- * *loss receives L before the step (may be NULL). */
-VR_API int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *r_dev, int32_t nb, float lr, double *loss);
+/* One Adam step on a batch of nb errors e_b resident on the device (nb x
+ * nr*nz): with r_b = S e_b (S of the vr_k2d, the symmetric form), D the inverse
+ * square root of S's diagonal and s_b the RMS of D r_b, the preconditioner's
+ * answer is y_b = s_b D N(D r_b / s_b) and the loss its error in S's energy
+ * norm, L = mean_b (y_b - e_b)' S (y_b - e_b) / (e_b' S e_b).  *loss receives
+ * L before the step (may be NULL).  The flexible CG applies the network the
+ * same way: z = s D N(D r / s). */
+VR_API int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *e_dev, int32_t nb, float lr, double *loss);
+/* diag(S) of the symmetric form (host, nr*nz) */
+VR_API int vr_k2d_diag(const vr_k2d *k, double *d);
 /* make the network the preconditioner of VR_KRYLOV_FCG_LEARNED (NULL clears) */
 VR_API int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *u);
 

@@ -148,6 +148,7 @@ def lib():
         L.vr_k2d_solve.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp), C.POINTER(dp)]
         L.vr_k2d_solve_dev.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp)]
         L.vr_k2d_set_preconditioner.argtypes = [vp, vp]
+        L.vr_k2d_diag.argtypes = [vp, vp]
         L.vr_unet_create.argtypes = [C.POINTER(UnetDesc), C.c_uint64, C.POINTER(vp)]
         L.vr_unet_destroy.argtypes = [vp]
         L.vr_unet_last_error.restype = C.c_char_p
@@ -553,6 +554,12 @@ class K2d:
         self._chk(lib().vr_k2d_apply_dev(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), 1 if symmetric else 0),
                   "k2d_apply_dev")
 
+    def diag(self) -> np.ndarray:
+        """diag(S) of the symmetric form, (nr, nz)."""
+        d = np.empty((self.nr, self.nz), dtype=np.float64, order="F")
+        self._chk(lib().vr_k2d_diag(self._h, _p(d)), "k2d_diag")
+        return d
+
     def set_preconditioner(self, net) -> None:
         self._chk(lib().vr_k2d_set_preconditioner(self._h, net._h if net is not None else None),
                   "k2d_set_preconditioner")
@@ -619,9 +626,11 @@ class UNet:
         self._chk(lib().vr_unet_backward(self._h, _p(x), _p(g), _p(dw), _p(dx)), "unet_backward")
         return dw, dx
 
-    def train_step(self, k2d: K2d, r_ptr: int, nb: int, lr: float) -> float:
+    def train_step(self, k2d: K2d, e_ptr: int, nb: int, lr: float) -> float:
+        """One Adam step on nb device-resident errors (nb x nr*nz doubles);
+        returns the energy-norm loss before the step."""
         loss = C.c_double()
-        self._chk(lib().vr_unet_train_step(self._h, k2d._h, C.c_void_p(r_ptr), nb, lr, C.byref(loss)),
+        self._chk(lib().vr_unet_train_step(self._h, k2d._h, C.c_void_p(e_ptr), nb, lr, C.byref(loss)),
                   "unet_train_step")
         return loss.value
 

@@ -42,7 +42,7 @@ constexpr int kK2dChunk = 32;  // iterations per captured graph (even)
 
 // scalar slots
 enum K2dScal {
-  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_PQ, SC_N
+  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_PQ, SC_SS, SC_ER, SC_N
 };
 // partial-sum slots
 enum K2dPart { PT_A = 0, PT_B, PT_C, PT_D, PT_N };
@@ -52,7 +52,7 @@ enum K2dPart { PT_A = 0, PT_B, PT_C, PT_D, PT_N };
 struct vr_k2d {
   int nr = 0, nz = 0, n = 0, dev = 0, nb = 0;
   cudaStream_t stream = nullptr;
-  double *coef = nullptr;  // aw, ae, az, vol, dinv (per j; dinv per cell)
+  double *coef = nullptr;  // aw, ae, az, vol (per j), then per cell 1/diag(S) and diag(S)^-1/2
   double gam = 0.0;
   double *vec[12] = {};
   double *part = nullptr;   // PT_N x kK2dMaxBlocks
@@ -206,7 +206,8 @@ enum K2dScalarOp {
   SO_FCG_ALPHA,     // alpha = p.r [A] / p.q [B]; stores pq
   SO_FCG_CONV,      // rr [A]
   SO_NORM,          // rr [A] only (sc[SC_RR])
-  SO_NORM_BB        // bb [A] only (sc[SC_BB])
+  SO_NORM_BB,       // bb [A] only (sc[SC_BB])
+  SO_SS             // (D r).(D r) [A] into sc[SC_SS] (the preconditioner's input scale)
 };
 
 __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, int nb, double *sc, int *flags) {
@@ -281,6 +282,9 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       break;
     case SO_NORM_BB:
       sc[SC_BB] = a;
+      break;
+    case SO_SS:
+      sc[SC_SS] = a;
       break;
   }
   // iteration cap (flags[2]): stop as not converged
@@ -368,6 +372,21 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_fcg_p(int n, double *__restri
   if (flags[0]) return;
   const double be = first ? 0.0 : sc[SC_BETA];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] - be * p[i];
+}
+
+// partial sum of (D r)^2 [A] (the learned preconditioner's input scale)
+__global__ void __launch_bounds__(kK2dThreads) k2d_dscaled(int n, const double *__restrict__ r,
+                                                         const double *__restrict__ dh, double *part,
+                                                         const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  double a = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = dh[i] * r[i];
+    a += x * x;
+  }
+  double t = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 // FCG: x += alpha p; r -= alpha q; partial r.r [A]
@@ -515,7 +534,7 @@ extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
     ae[j - 1] = f[j] * dz / h;
   }
   k->gam = 2.0 * f[nr] * dz / dr[nr - 1];
-  std::vector<double> coef((size_t)4 * nr + (size_t)nr * nz);
+  std::vector<double> coef((size_t)4 * nr + 2 * (size_t)nr * nz);
   for (int j = 0; j < nr; j++) {
     coef[j] = aw[j];
     coef[nr + j] = ae[j];
@@ -527,6 +546,7 @@ extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
       double dg = aw[j] + ae[j] + (kk > 0 ? az[j] : 0.0) + (kk < nz - 1 ? az[j] : 0.0);
       if (j == nr - 1) dg += k->gam / nz;
       coef[4 * nr + j + (size_t)nr * kk] = 1.0 / dg;
+      coef[4 * nr + (size_t)nr * nz + j + (size_t)nr * kk] = 1.0 / std::sqrt(dg);
     }
   // direct solve tables: DCT-II scaled 1/(2 nz) (REDFT10) and DCT-III (REDFT01)
   const double pi = std::acos(-1.0);
@@ -598,6 +618,16 @@ extern "C" int vr_k2d_destroy(vr_k2d *k) {
 }
 
 extern "C" const char *vr_k2d_last_error(const vr_k2d *k) { return k ? k->err.c_str() : "null solver"; }
+
+extern "C" int vr_k2d_diag(const vr_k2d *k, double *d) {
+  if (!k || !d) return VR_ERR_ARG;
+  std::vector<double> inv((size_t)k->n);
+  if (cudaSetDevice(k->dev) != cudaSuccess) return VR_ERR_CUDA;
+  if (cudaMemcpy(inv.data(), k->coef + 4 * k->nr, sizeof(double) * k->n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return VR_ERR_CUDA;
+  for (int i = 0; i < k->n; i++) d[i] = 1.0 / inv[i];
+  return VR_OK;
+}
 
 extern "C" int vr_k2d_info(const vr_k2d *k, int32_t *nr, int32_t *nz, double *faces) {
   if (!k) return VR_ERR_ARG;
@@ -748,7 +778,9 @@ static int run_fcg(vr_k2d *k, int maxit, int *iters) {
       K2D_CUDA(k, cudaStreamSynchronize(k->stream));
       if (h[0]) break;
     }
-    int rc = unet_precondition(k->net, r, z, k->sc + SC_RR, k->flags, k->stream);
+    k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, r, k2d_dhalf(k), P, k->flags);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
+    int rc = unet_precondition(k->net, r, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream);
     if (rc) return k2d_err(k, rc, std::string("learned preconditioner: ") + vr_unet_last_error(k->net));
     if (it > 0) {
       k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, q, nullptr, nullptr, P, nullptr);
@@ -872,62 +904,93 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
 
 // ---- training support for the learned preconditioner ---------------------------
 namespace vr {
-__global__ void __launch_bounds__(kK2dThreads) k2d_loss_a(K2dOp o, const float *__restrict__ y,
-                                                        const double *__restrict__ x, double *__restrict__ yd,
-                                                        double *__restrict__ e, double *part) {
-  // e = S y - x with y widened; partial e.e
-  __shared__ double sh[40];
-  // widen y first (the stencil reads neighbours): done by the caller's pass
-  const double mean = last_row_mean(o, yd, sh);
-  double acc = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
-    const double v = apply_S_at(o, yd, i, mean) - x[i];
-    e[i] = v;
-    acc += v * v;
-  }
-  double t = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
-  (void)y;
-}
 
-__global__ void k2d_widen(int n, const float *__restrict__ y, double *__restrict__ yd) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) yd[i] = (double)y[i];
-}
+const double *k2d_dhalf(const vr_k2d *k) { return k->coef + 4 * k->nr + (size_t)k->n; }
 
-// gy = 2 S e / xx (float); loss_acc += e.e / xx
-__global__ void __launch_bounds__(kK2dThreads) k2d_loss_b(K2dOp o, const double *__restrict__ e, double inv_xx,
-                                                        float *__restrict__ gy) {
+// r = S e; partials (D r)^2 [C], e . r [D]
+__global__ void __launch_bounds__(kK2dThreads) k2d_tin(K2dOp o, const double *__restrict__ e,
+                                                     double *__restrict__ r, const double *__restrict__ dh,
+                                                     double *part) {
   __shared__ double sh[40];
   const double mean = last_row_mean(o, e, sh);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x)
-    gy[i] = (float)(2.0 * inv_xx * apply_S_at(o, e, i, mean));
+  double ss = 0.0, er = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double ri = apply_S_at(o, e, i, mean);
+    r[i] = ri;
+    const double x = dh[i] * ri;
+    ss += x * x;
+    er += e[i] * ri;
+  }
+  double t = block_sum(ss, sh);
+  if (threadIdx.x == 0) part[2 * kK2dMaxBlocks + blockIdx.x] = t;
+  __syncthreads();
+  t = block_sum(er, sh);
+  if (threadIdx.x == 0) part[3 * kK2dMaxBlocks + blockIdx.x] = t;
 }
 
-__global__ void __launch_bounds__(1024) k2d_sum_into(const double *part, int nb, double scale, double *acc,
-                                                   int overwrite) {
+__global__ void __launch_bounds__(1024) k2d_sum_into(const double *part, int nb, double *acc, int add,
+                                                   const double *div) {
   __shared__ double sh[40];
   const double a = sum_part(part, nb, sh);
-  if (threadIdx.x == 0) *acc = overwrite ? a * scale : *acc + a * scale;
+  if (threadIdx.x == 0) {
+    const double v = div ? a / *div : a;
+    *acc = add ? *acc + v : v;
+  }
 }
 
-cudaError_t k2d_loss_grad(vr_k2d *k, const float *y, const double *x, double xx, float *gy, double *loss_acc,
-                          cudaStream_t s) {
+// y = s D yhat
+__global__ void k2d_tscale(int n, const float *__restrict__ yh, const double *__restrict__ dh,
+                           const double *__restrict__ ss, double *__restrict__ y) {
+  const double sc = sqrt(*ss / n);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = sc * dh[i] * (double)yh[i];
+}
+
+// res = S y - r; partial (y - e) . res [C]
+__global__ void __launch_bounds__(kK2dThreads) k2d_tres(K2dOp o, const double *__restrict__ y,
+                                                      const double *__restrict__ r, const double *__restrict__ e,
+                                                      double *__restrict__ res, double *part) {
+  __shared__ double sh[40];
+  const double mean = last_row_mean(o, y, sh);
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double v = apply_S_at(o, y, i, mean) - r[i];
+    res[i] = v;
+    acc += (y[i] - e[i]) * v;
+  }
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[2 * kK2dMaxBlocks + blockIdx.x] = t;
+}
+
+// gyhat = 2 s D res / er
+__global__ void k2d_tgrad(int n, const double *__restrict__ res, const double *__restrict__ dh,
+                          const double *__restrict__ ss, const double *__restrict__ er, float *__restrict__ g) {
+  const double sc = 2.0 * sqrt(*ss / n) / *er;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    g[i] = (float)(sc * dh[i] * res[i]);
+}
+
+cudaError_t k2d_train_in(vr_k2d *k, const double *e, double *r, double *ss, double *er, cudaStream_t s) {
   const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
-  double *yd = k->vec[V_W1], *e = k->vec[V_W2];
-  k2d_widen<<<gb, kK2dThreads, 0, s>>>(o.n, y, yd);
-  k2d_loss_a<<<gb, kK2dThreads, 0, s>>>(o, y, x, yd, e, k->part + 3 * kK2dMaxBlocks);
-  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 3 * kK2dMaxBlocks, gb, 1.0 / xx, loss_acc, 0 /*accumulate*/);
-  k2d_loss_b<<<gb, kK2dThreads, 0, s>>>(o, e, 1.0 / xx, gy);
+  k2d_tin<<<gb, kK2dThreads, 0, s>>>(o, e, r, k2d_dhalf(k), k->part);
+  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 2 * kK2dMaxBlocks, gb, ss, 0, nullptr);
+  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 3 * kK2dMaxBlocks, gb, er, 0, nullptr);
   return cudaGetLastError();
 }
 
-cudaError_t k2d_dot_self(vr_k2d *k, const double *x, double *rr, cudaStream_t s) {
+cudaError_t k2d_train_grad(vr_k2d *k, const float *yhat, const double *e, const double *r, const double *ss,
+                           const double *er, float *gyhat, double *loss_acc, cudaStream_t s) {
+  const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
-  k2d_dots<<<gb, kK2dThreads, 0, s>>>(k->n, x, x, nullptr, nullptr, k->part + 3 * kK2dMaxBlocks, nullptr);
-  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 3 * kK2dMaxBlocks, gb, 1.0, rr, 1);
+  double *y = k->vec[V_W1], *res = k->vec[V_W2];
+  k2d_tscale<<<gb, kK2dThreads, 0, s>>>(o.n, yhat, k2d_dhalf(k), ss, y);
+  k2d_tres<<<gb, kK2dThreads, 0, s>>>(o, y, r, e, res, k->part);
+  k2d_sum_into<<<1, 1024, 0, s>>>(k->part + 2 * kK2dMaxBlocks, gb, loss_acc, 1, er);
+  k2d_tgrad<<<gb, kK2dThreads, 0, s>>>(o.n, res, k2d_dhalf(k), ss, er, gyhat);
   return cudaGetLastError();
 }
+
 }  // namespace vr
 
 extern "C" int vr_k2d_solve(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,

@@ -8,21 +8,25 @@
 
 namespace vr {
 
-// z = s N(r / s) with s = sqrt(*rr / n) read on the device (rr = r . r),
-// r and z device arrays of nr*nz doubles; does nothing once flags[0] is set
-int unet_precondition(const vr_unet *u, const double *r, double *z, const double *rr, const int *flags,
-                      cudaStream_t s);
+// z = s D N(D r / s), D = dscale (per cell, may be NULL for 1) and
+// s = sqrt(*ss / n) with ss = sum (D r)^2 read on the device; r and z device
+// arrays of nr*nz doubles; does nothing once flags[0] is set
+int unet_precondition(const vr_unet *u, const double *r, double *z, const double *dscale, const double *ss,
+                      const int *flags, cudaStream_t s);
 
 // grid of a network (nr, nz)
 void unet_dims(const vr_unet *u, int *nr, int *nz);
 
-// The training loss of one sample through the operator of k:
-//   e = S y - x, loss = ||e||^2 / ||x||^2, gy = 2 S e / ||x||^2
-// y (float, the network output) and x (double) device arrays of nr*nz;
-// ||x||^2 is given (xx); adds loss to *loss_acc (device double).
-cudaError_t k2d_loss_grad(vr_k2d *k, const float *y, const double *x, double xx, float *gy, double *loss_acc,
-                          cudaStream_t s);
-// rr[0] = x . x for a device array of nr*nz doubles (deterministic)
-cudaError_t k2d_dot_self(vr_k2d *k, const double *x, double *rr, cudaStream_t s);
+// D^-1/2 of the symmetric operator's diagonal, per cell (device)
+const double *k2d_dhalf(const vr_k2d *k);
+
+// Training pair of one sample: r = S e, ss = sum (D r)^2, er = e . r
+// (device scalars); r a device array of nr*nz
+cudaError_t k2d_train_in(vr_k2d *k, const double *e, double *r, double *ss, double *er, cudaStream_t s);
+// Energy-norm loss of the network output yhat (float) for the pair (e, r):
+//   y = s D yhat, res = S y - r, loss_acc += (y - e) . res / er,
+//   gyhat = 2 s D res / er  (the gradient of the loss with respect to yhat)
+cudaError_t k2d_train_grad(vr_k2d *k, const float *yhat, const double *e, const double *r, const double *ss,
+                           const double *er, float *gyhat, double *loss_acc, cudaStream_t s);
 
 }  // namespace vr

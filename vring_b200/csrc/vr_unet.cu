@@ -67,8 +67,8 @@ struct vr_unet {
   float *g[20] = {};
   float *gx0 = nullptr;                   // input gradient (gradient check only)
   float *y = nullptr, *gy = nullptr;      // head output and its gradient
-  double *xs = nullptr;                   // normalised input (double) for the loss
-  double *dscal = nullptr;                // device scalars: loss accumulator, rr
+  double *xs = nullptr;                   // host-staging and training residual (double)
+  double *dscal = nullptr;                // device scalars: loss accumulator, ss, e.r
   cudaStream_t stream = nullptr;
 };
 
@@ -422,23 +422,24 @@ __global__ void __launch_bounds__(256) k_head_bwd(const __nv_bfloat16 *__restric
     atomicAdd(gw + threadIdx.x, s);
   }
 }
-// input: x[p] * inv (double) -> bf16; keeps the scaled double copy
-__global__ void k_in(const double *__restrict__ x, int n, const double *__restrict__ rr, double inv_host,
-                     __nv_bfloat16 *__restrict__ xb, double *__restrict__ xs, const int *flags) {
+// input: x[p] * D[p] / s -> bf16 (D = dscale or 1; s = sqrt(*ss / n) when ss is
+// given, else 1 / inv_host)
+__global__ void k_in(const double *__restrict__ x, int n, const double *__restrict__ ss, double inv_host,
+                     const double *__restrict__ dscale, __nv_bfloat16 *__restrict__ xb, const int *flags) {
   if (flags && flags[0]) return;
-  const double inv = rr ? (*rr > 0 ? 1.0 / sqrt(*rr / n) : 0.0) : inv_host;
+  const double inv = ss ? (*ss > 0 ? 1.0 / sqrt(*ss / n) : 0.0) : inv_host;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double v = x[i] * inv;
-    if (xs) xs[i] = v;
+    const double v = x[i] * inv * (dscale ? dscale[i] : 1.0);
     xb[i] = __float2bfloat16_rn((float)v);
   }
 }
-// output: z = s y
-__global__ void k_out(const float *__restrict__ y, int n, const double *__restrict__ rr, double s_host,
-                      double *__restrict__ z, const int *flags) {
+// output: z = s D y
+__global__ void k_out(const float *__restrict__ y, int n, const double *__restrict__ ss, double s_host,
+                      const double *__restrict__ dscale, double *__restrict__ z, const int *flags) {
   if (flags && flags[0]) return;
-  const double s = rr ? sqrt(*rr / n) : s_host;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = s * (double)y[i];
+  const double s = ss ? sqrt(*ss / n) : s_host;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    z[i] = s * (double)y[i] * (dscale ? dscale[i] : 1.0);
 }
 // weights: bf16 copy, the rounded FP32 copy used by the kernels, the flipped
 // transposed copy for the data gradient of every 3x3 layer
@@ -854,13 +855,13 @@ void unet_dims(const vr_unet *u, int *nr, int *nz) {
   *nz = u->nz;
 }
 
-int unet_precondition(const vr_unet *u, const double *r, double *z, const double *rr, const int *flags,
-                      cudaStream_t s) {
+int unet_precondition(const vr_unet *u, const double *r, double *z, const double *dscale, const double *ss,
+                      const int *flags, cudaStream_t s) {
   const int n = u->nr * u->nz;
-  k_in<<<grid_for(n), 256, 0, s>>>(r, n, rr, 0.0, u->x0, nullptr, flags);
+  k_in<<<grid_for(n), 256, 0, s>>>(r, n, ss, 0.0, dscale, u->x0, flags);
   if (cudaGetLastError() != cudaSuccess) return VR_ERR_CUDA;
   if (unet_fwd(u, s) != cudaSuccess) return VR_ERR_CUDA;
-  k_out<<<grid_for(n), 256, 0, s>>>(u->y, n, rr, 0.0, z, flags);
+  k_out<<<grid_for(n), 256, 0, s>>>(u->y, n, ss, 0.0, dscale, z, flags);
   return cudaGetLastError() == cudaSuccess ? VR_OK : VR_ERR_CUDA;
 }
 
@@ -874,10 +875,10 @@ extern "C" int vr_unet_forward(vr_unet *u, const double *xh, double *yh) {
   for (int i = 0; i < n; i++) ss += xh[i] * xh[i];
   const double s = std::sqrt(ss / n);
   U_CUDA(u, cudaMemcpyAsync(u->xs, xh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
-  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, s > 0 ? 1.0 / s : 0.0, u->x0, nullptr, nullptr);
+  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, s > 0 ? 1.0 / s : 0.0, nullptr, u->x0, nullptr);
   U_CUDA(u, cudaGetLastError());
   U_CUDA(u, unet_fwd(u, u->stream));
-  k_out<<<grid_for(n), 256, 0, u->stream>>>(u->y, n, nullptr, s, u->xs, nullptr);
+  k_out<<<grid_for(n), 256, 0, u->stream>>>(u->y, n, nullptr, s, nullptr, u->xs, nullptr);
   U_CUDA(u, cudaGetLastError());
   U_CUDA(u, cudaMemcpyAsync(yh, u->xs, sizeof(double) * n, cudaMemcpyDeviceToHost, u->stream));
   U_CUDA(u, cudaStreamSynchronize(u->stream));
@@ -896,7 +897,7 @@ extern "C" int vr_unet_backward(vr_unet *u, const double *xh, const double *gh, 
   U_CUDA(u, cudaSetDevice(u->dev));
   const int n = u->nr * u->nz;
   U_CUDA(u, cudaMemcpyAsync(u->xs, xh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
-  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, 1.0, u->x0, nullptr, nullptr);
+  k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, 1.0, nullptr, u->x0, nullptr);
   U_CUDA(u, cudaGetLastError());
   U_CUDA(u, unet_fwd(u, u->stream));
   U_CUDA(u, cudaMemcpyAsync(u->xs, gh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
@@ -912,24 +913,25 @@ extern "C" int vr_unet_backward(vr_unet *u, const double *xh, const double *gh, 
   return VR_OK;
 }
 
-extern "C" int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *r_dev, int32_t nb, float lr, double *loss) {
-  if (!u || !k || !r_dev || nb < 1 || !(lr > 0)) return VR_ERR_ARG;
+extern "C" int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *e_dev, int32_t nb, float lr, double *loss) {
+  if (!u || !k || !e_dev || nb < 1 || !(lr > 0)) return VR_ERR_ARG;
   int32_t knr = 0, knz = 0;
   vr_k2d_info(k, &knr, &knz, nullptr);
   if (knr != u->nr || knz != u->nz) return unet_err(u, VR_ERR_ARG, "network and operator grids differ");
   U_CUDA(u, cudaSetDevice(u->dev));
   const int n = u->nr * u->nz;
   cudaStream_t s = u->stream;
+  const double *dh = k2d_dhalf(k);
   U_CUDA(u, cudaMemsetAsync(u->gw, 0, sizeof(float) * u->nparam, s));
   U_CUDA(u, cudaMemsetAsync(u->dscal, 0, sizeof(double) * 8, s));
   for (int b = 0; b < nb; b++) {
-    const double *r = r_dev + (size_t)b * n;
-    // x = r / rms(r) (double kept for the loss); ||x||^2 = n
-    U_CUDA(u, k2d_dot_self(k, r, u->dscal + 1, s));
-    k_in<<<grid_for(n), 256, 0, s>>>(r, n, u->dscal + 1, 0.0, u->x0, u->xs, nullptr);
+    const double *e = e_dev + (size_t)b * n;
+    // r = S e; the network sees D r / s (s its RMS), its output maps back as s D yhat
+    U_CUDA(u, k2d_train_in(k, e, u->xs, u->dscal + 1, u->dscal + 2, s));
+    k_in<<<grid_for(n), 256, 0, s>>>(u->xs, n, u->dscal + 1, 0.0, dh, u->x0, nullptr);
     U_CUDA(u, cudaGetLastError());
     U_CUDA(u, unet_fwd(u, s));
-    U_CUDA(u, k2d_loss_grad(k, u->y, u->xs, (double)n, u->gy, u->dscal, s));
+    U_CUDA(u, k2d_train_grad(k, u->y, e, u->xs, u->dscal + 1, u->dscal + 2, u->gy, u->dscal, s));
     U_CUDA(u, unet_bwd(u, false, s));
   }
   // Adam with the batch-mean gradient

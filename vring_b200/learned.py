@@ -11,12 +11,16 @@ pressure low travelling along z with a slowly drifting radius, core size and
 strength plus smooth seeded perturbations; the right-hand side of step t is
 K applied to that step's pressure field, and the converged pressure is the
 plain solver's answer (the direct DCT/radial-Thomas solve, which the Krylov
-solves agree with to their tolerance).  The network sees the residual the
-previous step's pressure leaves, r = V f_t - S p_{t-1} (the warm start's
-residual), and is trained to invert S on it:
-L = mean_b ||S N(r_b) - r_b||^2 / ||r_b||^2.  A quarter of each batch is white
-noise and a quarter S times a random smooth field, so that the map also
-covers the rougher residuals a Krylov iteration produces.
+solves agree with to their tolerance).  What the preconditioner must undo is
+the error of the warm start, e = p_t - p_{t-1}, whose residual is r = S e.
+The network is applied with the symmetric Jacobi scaling, y = s D N(D r / s)
+(D = diag(S)^-1/2, s the RMS of D r), which takes out the operator's strong
+variation with the radius so that one translation-invariant network fits the
+whole grid, and it is trained on the error in S's energy norm,
+L = (y - e)' S (y - e) / e' S e, the norm CG minimises.  Half of each batch
+is triple increments; a quarter random smooth fields and a quarter white
+noise in the scaled variables (e = D w), so that the map also covers the
+rougher errors a Krylov iteration leaves.
 
 Everything runs on the GPU through the library (vr_k2d_*, vr_unet_*); torch
 only holds device buffers.
@@ -114,10 +118,10 @@ def triple(k2d: K2d, seq: RingSequence, t: int):
     return f, p_prev, p
 
 
-def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, log=None,
-          lr_final: float = 1e-4):
-    """Adam on batches of residuals: half warm-start residuals of the triple
-    sequences, a quarter S x (random smooth field), a quarter white noise."""
+def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 3e-3, seed: int = 0, log=None,
+          lr_final: float = 3e-4):
+    """Adam on batches of errors: half warm-start errors of the triple
+    sequences, a quarter random smooth fields, a quarter scaled white noise."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = np.random.default_rng(seed)
@@ -125,8 +129,7 @@ def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 1e-3, see
     n = k2d.nr * k2d.nz
     buf = torch.empty((batch, n), dtype=torch.float64, device=dev)
     rm, zm = cell_centres(k2d.faces, k2d.nz, k2d.zmax)
-    dz = k2d.zmax / k2d.nz
-    vol = rm * np.diff(k2d.faces) * dz
+    dhalf = 1.0 / np.sqrt(k2d.diag())
     losses = []
     for it in range(steps):
         for b in range(batch):
@@ -134,20 +137,17 @@ def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 1e-3, see
             if kind < 2:
                 seq = seqs[rng.integers(len(seqs))]
                 t = int(rng.integers(1, STEPS_PER_SEED))
-                f, p_prev, _ = triple(k2d, seq, t)
-                # the warm start's residual r = V f - S p_prev = V (f - K p_prev)
-                r = (f - k2d.apply(p_prev)) * vol[:, None]
+                _, p_prev, p = triple(k2d, seq, t)
+                e = p - p_prev
             elif kind == 2:
-                # S x random smooth field (cosine modes with decaying amplitude)
-                kr = rng.integers(0, 64, 8)
-                kzz = rng.integers(0, 128, 8)
+                kr = rng.integers(0, k2d.nr // 2, 8)
+                kzz = rng.integers(0, k2d.nz // 2, 8)
                 a = rng.normal(size=8) / (1.0 + kr + kzz)
-                x = sum(ai * np.cos(np.pi * ki * rm[:, None] / k2d.faces[-1]) * np.cos(np.pi * kj * zm[None, :] / k2d.zmax)
+                e = sum(ai * np.cos(np.pi * ki * rm[:, None] / k2d.faces[-1]) * np.cos(np.pi * kj * zm[None, :] / k2d.zmax)
                         for ai, ki, kj in zip(a, kr, kzz))
-                r = k2d.apply(x) * vol[:, None]
             else:
-                r = rng.standard_normal((k2d.nr, k2d.nz))
-            buf[b].copy_(torch.from_numpy(np.asfortranarray(r).ravel(order="F")))
+                e = rng.standard_normal((k2d.nr, k2d.nz)) * dhalf
+            buf[b].copy_(torch.from_numpy(np.asfortranarray(e).ravel(order="F")))
         frac = it / max(1, steps - 1)
         lr_t = lr * (lr_final / lr) ** frac
         torch.cuda.synchronize()  # the library's streams do not wait for torch's
@@ -158,14 +158,14 @@ def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 1e-3, see
     return losses
 
 
-def compare(k2d: K2d, net: UNet, f, x0=None, tol: float = 1e-10):
+def compare(k2d: K2d, net: UNet, f, x0=None, tol: float = 1e-10, maxit: int = 40000):
     """Plain CG, Jacobi CG and the learned flexible CG on one right-hand side:
-    {method: (iterations, relres, ms, x)}."""
+    {method: (iterations, relres, ms, x)}; each stops after maxit iterations."""
     out = {}
     for m in ("cg", "pcg", "learned"):
         if m == "learned":
             k2d.set_preconditioner(net)
-        x, it, rr, ms = k2d.solve(f, m, x0=x0, tol=tol)
+        x, it, rr, ms = k2d.solve(f, m, x0=x0, tol=tol, maxit=maxit)
         out[m] = (it, rr, ms, x)
     k2d.set_preconditioner(None)
     return out
