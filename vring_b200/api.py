@@ -535,7 +535,8 @@ class K2d:
     def solve(self, f, method="cg", x0=None, tol=1e-10, maxit=1000000):
         """(x, iterations, relative residual, device ms)."""
         f = self._vec(f)
-        x = np.zeros_like(f) if x0 is None else self._vec(x0).copy()
+        # the library reads r fastest: keep the copy in Fortran order
+        x = np.zeros_like(f) if x0 is None else np.array(self._vec(x0), order="F", copy=True)
         it, rr, ms = C.c_int32(), C.c_double(), C.c_double()
         self._chk(lib().vr_k2d_solve(self._h, KRYLOV[method], _p(f), _p(x), tol, maxit, C.byref(it),
                                      C.byref(rr), C.byref(ms)), "k2d_solve")

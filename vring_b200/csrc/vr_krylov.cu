@@ -149,8 +149,8 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_apply(K2dOp o, const double *
 
 // generic fused vector update: out = a*X + b*Y (+ partials of two dot products)
 // used for initialisation steps
-__global__ void __launch_bounds__(kK2dThreads) k2d_axpby(int n, double a, const double *__restrict__ X, double b,
-                                                       const double *__restrict__ Y, double *__restrict__ out) {
+__global__ void __launch_bounds__(kK2dThreads) k2d_axpby(int n, double a, const double *X, double b, const double *Y,
+                                                       double *out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[i] = a * X[i] + (Y ? b * Y[i] : 0.0);
 }
