@@ -86,6 +86,8 @@ def lib():
         L.vr_field_extents.argtypes = [vp, i32, C.POINTER(i64)]
         L.vr_set_field.argtypes = [vp, i32, vp, C.POINTER(i64)]
         L.vr_get_field.argtypes = [vp, i32, vp, C.POINTER(i64)]
+        L.vr_set_field_async.argtypes = [vp, i32, vp, C.POINTER(i64), vp]
+        L.vr_get_field_async.argtypes = [vp, i32, vp, C.POINTER(i64), vp]
         L.vr_set_clock.argtypes = [vp, i32, dp, i64]
         L.vr_get_clock.argtypes = [vp, C.POINTER(i32), C.POINTER(dp), C.POINTER(i64)]
         for n in ("ucoeff", "coesys", "hdnbc", "hdnl1", "hdnl2", "hdnl3", "step", "divq",
@@ -236,6 +238,20 @@ class Run:
         ext = (C.c_int64 * 4)()
         self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
         self._chk(lib().vr_get_field(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext), "get " + name)
+
+    def set_async(self, name: str, host_ptr: int, cuda_stream: int) -> None:
+        """vr_set_field_async from pinned host memory on a caller's stream."""
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        self._chk(lib().vr_set_field_async(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext,
+                                           C.c_void_p(cuda_stream)), "set_async " + name)
+
+    def get_async(self, name: str, host_ptr: int, cuda_stream: int) -> None:
+        """vr_get_field_async into pinned host memory on a caller's stream."""
+        ext = (C.c_int64 * 4)()
+        self._chk(lib().vr_field_extents(self._h, FIELD_ID[name], ext), "extents " + name)
+        self._chk(lib().vr_get_field_async(self._h, FIELD_ID[name], C.c_void_p(host_ptr), ext,
+                                           C.c_void_p(cuda_stream)), "get_async " + name)
 
     def set_stream(self, cuda_stream_handle: int) -> None:
         """Queue the context's work on a caller's CUDA stream; 0 (which is also

@@ -560,6 +560,9 @@ extern "C" int vr_destroy(vr_ctx *c) {
   if (c->ana_zm) cudaFree(c->ana_zm);
   if (c->ana_part) cudaFree(c->ana_part);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  if (c->xfer_ev) cudaEventDestroy(c->xfer_ev);
+  for (cudaEvent_t e : c->get_ev)
+    if (e) cudaEventDestroy(e);
   delete[] c->h_rc;
   delete[] c->h_rm;
   delete[] c->h_da;
@@ -690,6 +693,7 @@ extern "C" int vr_set_field(vr_ctx *c, int32_t f, const double *host, const int6
   int rc = check_ext(c, f, ext, &p, &n);
   if (rc) return rc;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  if ((rc = wait_pending_gets(c))) return rc;
   if (float_field(c, f)) {
     std::vector<float> t(host, host + n);
     VR_CUDA(c, cudaMemcpyAsync(p, t.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
@@ -717,6 +721,68 @@ extern "C" int vr_get_field(vr_ctx *c, int32_t f, double *host, const int64_t ex
   }
   VR_CUDA(c, cudaMemcpyAsync(host, p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   VR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return VR_OK;
+}
+
+// Asynchronous transfers.  A get leaves a pending event per field: a later set
+// of the same field waits for it (the device field may be overwritten once it
+// has been read), and the context's next fused step or substep waits for all
+// of them before its kernels write the fields again.  A set makes the
+// context's stream wait for its copy at once (everything after reads it).
+static int xfer_ev(vr_ctx *c, cudaEvent_t *ev) {
+  if (!*ev) VR_CUDA(c, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  return VR_OK;
+}
+
+int vr::wait_pending_gets(vr_ctx *c) {
+  for (int f = 0; f < kXferFields; f++)
+    if (c->get_pending[f]) {
+      VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->get_ev[f], 0));
+      c->get_pending[f] = false;
+    }
+  return VR_OK;
+}
+
+extern "C" int vr_get_field_async(vr_ctx *c, int32_t f, double *host, const int64_t ext[4], void *stream) {
+  if (!c || !host || !stream) return VR_ERR_ARG;
+  double *p;
+  size_t n;
+  int rc = check_ext(c, f, ext, &p, &n);
+  if (rc) return rc;
+  if (float_field(c, f) || f < 0 || f >= kXferFields)
+    return set_err(c, VR_ERR_STATE, "vr_get_field_async: the field is stored as float");
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  if ((rc = xfer_ev(c, &c->xfer_ev)) || (rc = xfer_ev(c, &c->get_ev[f]))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // after the context's work so far
+  VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
+  VR_CUDA(c, cudaMemcpyAsync(host, p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  VR_CUDA(c, cudaEventRecord(c->get_ev[f], s));
+  c->get_pending[f] = true;
+  return VR_OK;
+}
+
+extern "C" int vr_set_field_async(vr_ctx *c, int32_t f, const double *host, const int64_t ext[4], void *stream) {
+  if (!c || !host || !stream) return VR_ERR_ARG;
+  double *p;
+  size_t n;
+  int rc = check_ext(c, f, ext, &p, &n);
+  if (rc) return rc;
+  if (float_field(c, f) || f < 0 || f >= kXferFields)
+    return set_err(c, VR_ERR_STATE, "vr_set_field_async: the field is stored as float");
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  if ((rc = xfer_ev(c, &c->xfer_ev))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (c->get_pending[f]) {
+    // the last get of this field read it after all earlier work on it
+    VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[f], 0));
+  } else {
+    VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // the context's earlier reads come first
+    VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
+  }
+  VR_CUDA(c, cudaMemcpyAsync(p, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  VR_CUDA(c, cudaEventRecord(c->xfer_ev, s));
+  VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->xfer_ev, 0));  // the context's later work reads the new values
   return VR_OK;
 }
 
@@ -942,12 +1008,14 @@ extern "C" int vr_set_graphs(vr_ctx *c, int32_t on) {
 extern "C" int vr_substep(vr_ctx *c, int32_t irk) {
   if (!c || irk < 1 || irk > 3) return VR_ERR_ARG;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  if (int rc = wait_pending_gets(c)) return rc;
   return run_substep(c, irk);
 }
 
 extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
   if (!c || nsteps < 0) return VR_ERR_ARG;
   VR_CUDA(c, cudaSetDevice(c->dev));
+  if (int rc = wait_pending_gets(c)) return rc;
   for (int s = 0; s < nsteps; s++) {
     c->ntime = c->d.dt + c->ntime;
     // loop.F90:54-58: inflow injection every inj = 10 steps

@@ -160,6 +160,11 @@ struct vr_ctx {
   // r: 0 TMA 16-line tiles, 1 TMA 8-line tiles, 2 register chunks;
   // z: 0 TMA 8-line tiles, 1 TMA 16-line tiles, 2 register chunks
   int tune_r, tune_z;
+  // ordering of vr_get_field_async / vr_set_field_async with the context's
+  // stream: a scratch event and one pending-get event per field id
+  cudaEvent_t xfer_ev;
+  cudaEvent_t get_ev[32];
+  bool get_pending[32];
 };
 
 namespace vr {
@@ -221,6 +226,11 @@ bool rec_write(FILE *f, const void *buf, size_t n);
 bool rec_read(FILE *f, void *buf, size_t n);
 bool data_write(FILE *f, const double *p, size_t n);
 bool data_read(FILE *f, double *p, size_t n);
+
+// field ids the asynchronous transfers track, and the wait of the context's
+// stream for the device->host copies still pending (vr_ctx.cu)
+constexpr int kXferFields = 32;
+int wait_pending_gets(vr_ctx *c);
 
 // the launch sequence of one fused RK substep on the context's current stream
 // (vr_ctx.cu); no graph, no host synchronisation
