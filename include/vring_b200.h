@@ -376,20 +376,23 @@ VR_API int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, double *
 
 /* ---- the learned preconditioner: a 4-level U-Net (no reference counterpart)
  * Input and output are one channel on the nr x nz grid of a vr_k2d (r fastest);
- * levels l = 0..3 run on (nr/2^l) x (nz/2^l) with ch[l] channels: two 3x3
- * convolutions per level on the way down (2x2 average pooling between levels),
- * nearest-neighbour upsampling, concatenation with the level's skip tensor and
+ * levels l = 0..3 run on (nr/F^l) x (nz/F^l) with ch[l] channels, F the
+ * pooling factor: two 3x3 convolutions per level on the way down (F x F
+ * average pooling between levels), nearest-neighbour upsampling by F,
+ * concatenation with the level's skip tensor and
  * two 3x3 convolutions per level on the way up, then a 1x1 convolution to one
  * channel.  No biases and identity activations, so the network is a linear
  * map (a valid preconditioner for the flexible CG).  Weights are BF16 (an FP32
  * master copy is kept for training), activations BF16, every sum accumulates
- * in FP32.  nr and nz must be multiples of 8; ch[l] multiples of 8, ch[0] and
- * every 3x3 layer's output at most 64, its input at most 128. */
+ * in FP32.  ch[l] multiples of 8, ch[0] and every 3x3 layer's output at most
+ * 64, its input at most 128. */
 typedef struct vr_unet vr_unet;
 typedef struct vr_unet_desc {
   int32_t abi_version;
   int32_t nr, nz;
   int32_t ch[4];
+  int32_t pool;   /* pooling factor between levels: 2 or 4 (0 means 2); nr and
+                     nz must be multiples of pool^3 */
   int32_t device;
   int32_t flags;  /* 0, or VR_UNET_CUDA_CORES */
 } vr_unet_desc;

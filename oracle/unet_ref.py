@@ -76,20 +76,25 @@ def conv3_bwd(x, w, gy):
     return gw, gx
 
 
-def pool(x):
-    return 0.25 * (x[0::2, 0::2] + x[1::2, 0::2] + x[0::2, 1::2] + x[1::2, 1::2])
+def pool(x, F=2):
+    """F x F average: children summed r fastest (dz outer, dr inner), then / F^2."""
+    s = np.zeros((x.shape[0] // F, x.shape[1] // F) + x.shape[2:])
+    for dz in range(F):
+        for dr in range(F):
+            s = s + x[dr::F, dz::F]
+    return s / (F * F)
 
 
-def pool_bwd(g):
-    return 0.25 * np.repeat(np.repeat(g, 2, axis=0), 2, axis=1)
+def pool_bwd(g, F=2):
+    return np.repeat(np.repeat(g, F, axis=0), F, axis=1) / (F * F)
 
 
-def upcat(coarse, skip):
-    up = np.repeat(np.repeat(coarse, 2, axis=0), 2, axis=1)
+def upcat(coarse, skip, F=2):
+    up = np.repeat(np.repeat(coarse, F, axis=0), F, axis=1)
     return np.concatenate([up, skip], axis=2)
 
 
-def forward(w, ch, x, keep=False, rnd=None):
+def forward(w, ch, x, keep=False, rnd=None, F=2):
     """N(x) for x (nr, nz); BF16 rounding where the GPU stores BF16 (rnd
     replaces the rounding, e.g. the identity for a finite-difference check)."""
     bf16 = rnd if rnd is not None else globals()["bf16"]
@@ -99,58 +104,58 @@ def forward(w, ch, x, keep=False, rnd=None):
     a["x0"] = bf16(x)[:, :, None]
     a["e0a"] = bf16(conv3(a["x0"], Wr[0]))
     a["e0"] = bf16(conv3(a["e0a"], Wr[1]))
-    a["p1"] = bf16(pool(a["e0"]))
+    a["p1"] = bf16(pool(a["e0"], F))
     a["e1a"] = bf16(conv3(a["p1"], Wr[2]))
     a["e1"] = bf16(conv3(a["e1a"], Wr[3]))
-    a["p2"] = bf16(pool(a["e1"]))
+    a["p2"] = bf16(pool(a["e1"], F))
     a["e2a"] = bf16(conv3(a["p2"], Wr[4]))
     a["e2"] = bf16(conv3(a["e2a"], Wr[5]))
-    a["p3"] = bf16(pool(a["e2"]))
+    a["p3"] = bf16(pool(a["e2"], F))
     a["b3a"] = bf16(conv3(a["p3"], Wr[6]))
     a["b3"] = bf16(conv3(a["b3a"], Wr[7]))
-    a["u2"] = upcat(a["b3"], a["e2"])
+    a["u2"] = upcat(a["b3"], a["e2"], F)
     a["d2a"] = bf16(conv3(a["u2"], Wr[8]))
     a["d2"] = bf16(conv3(a["d2a"], Wr[9]))
-    a["u1"] = upcat(a["d2"], a["e1"])
+    a["u1"] = upcat(a["d2"], a["e1"], F)
     a["d1a"] = bf16(conv3(a["u1"], Wr[10]))
     a["d1"] = bf16(conv3(a["d1a"], Wr[11]))
-    a["u0"] = upcat(a["d1"], a["e0"])
+    a["u0"] = upcat(a["d1"], a["e0"], F)
     a["d0a"] = bf16(conv3(a["u0"], Wr[12]))
     a["d0"] = bf16(conv3(a["d0a"], Wr[13]))
     y = a["d0"] @ Wr[14]
     return (y, a, Wr) if keep else y
 
 
-def backward(w, ch, x, g, rnd=None):
+def backward(w, ch, x, g, rnd=None, F=2):
     """(dL/dw, dL/dx) of L = sum(g * N(x)) through the same graph."""
-    y, a, Wr = forward(w, ch, x, keep=True, rnd=rnd)
+    y, a, Wr = forward(w, ch, x, keep=True, rnd=rnd, F=F)
     gw = [None] * 15
     gw[14] = np.einsum("hw,hwc->c", g, a["d0"])
     gd0 = g[:, :, None] * Wr[14][None, None, :]
     gw[13], gd0a = conv3_bwd(a["d0a"], Wr[13], gd0)
     gw[12], gu0 = conv3_bwd(a["u0"], Wr[12], gd0a)
     c1 = ch[1]
-    gd1 = pool(gu0[:, :, :c1]) * 4.0
+    gd1 = pool(gu0[:, :, :c1], F) * (F * F)
     ge0 = gu0[:, :, c1:].copy()
     gw[11], gd1a = conv3_bwd(a["d1a"], Wr[11], gd1)
     gw[10], gu1 = conv3_bwd(a["u1"], Wr[10], gd1a)
     c2 = ch[2]
-    gd2 = pool(gu1[:, :, :c2]) * 4.0
+    gd2 = pool(gu1[:, :, :c2], F) * (F * F)
     ge1 = gu1[:, :, c2:].copy()
     gw[9], gd2a = conv3_bwd(a["d2a"], Wr[9], gd2)
     gw[8], gu2 = conv3_bwd(a["u2"], Wr[8], gd2a)
     c3 = ch[3]
-    gb3 = pool(gu2[:, :, :c3]) * 4.0
+    gb3 = pool(gu2[:, :, :c3], F) * (F * F)
     ge2 = gu2[:, :, c3:].copy()
     gw[7], gb3a = conv3_bwd(a["b3a"], Wr[7], gb3)
     gw[6], gp3 = conv3_bwd(a["p3"], Wr[6], gb3a)
-    ge2 += pool_bwd(gp3)
+    ge2 += pool_bwd(gp3, F)
     gw[5], ge2a = conv3_bwd(a["e2a"], Wr[5], ge2)
     gw[4], gp2 = conv3_bwd(a["p2"], Wr[4], ge2a)
-    ge1 += pool_bwd(gp2)
+    ge1 += pool_bwd(gp2, F)
     gw[3], ge1a = conv3_bwd(a["e1a"], Wr[3], ge1)
     gw[2], gp1 = conv3_bwd(a["p1"], Wr[2], ge1a)
-    ge0 += pool_bwd(gp1)
+    ge0 += pool_bwd(gp1, F)
     gw[1], ge0a = conv3_bwd(a["e0a"], Wr[1], ge0)
     gw[0], gx0 = conv3_bwd(a["x0"], Wr[0], ge0a)
     flat = np.concatenate([gw[i].ravel() for i in range(15)])

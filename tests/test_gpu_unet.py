@@ -49,14 +49,15 @@ def test_tensor_core_forward_matches_cuda_core_forward_and_oracle(grid):
     from oracle import unet_ref as U
     nr, nz = grid
     ch = (16, 32, 48, 64)
-    tc = V.UNet(nr, nz, ch, seed=9)
-    cc = V.UNet(nr, nz, ch, seed=9, flags=V.UNet.CUDA_CORES)
+    pool = 2 if nr < 64 else 4
+    tc = V.UNet(nr, nz, ch, seed=9, pool=pool)
+    cc = V.UNet(nr, nz, ch, seed=9, flags=V.UNet.CUDA_CORES, pool=pool)
     w = tc.get_params()
     assert np.array_equal(w, cc.get_params())
     x = np.random.default_rng(4).standard_normal((nr, nz))
     s = np.sqrt(np.mean(x ** 2))
     yt, yc = tc.forward(x), cc.forward(x)
-    yo = s * U.forward(w, ch, x / s)
+    yo = s * U.forward(w, ch, x / s, F=pool)
     print("%s: tensor cores vs oracle %.2e, CUDA cores vs oracle %.2e, between %.2e"
           % (grid, _rel(yt, yo), _rel(yc, yo), _rel(yt, yc)))
     assert _rel(yt, yo) <= 5e-3 and _rel(yc, yo) <= 5e-3
@@ -64,16 +65,17 @@ def test_tensor_core_forward_matches_cuda_core_forward_and_oracle(grid):
     cc.close()
 
 
-def test_gradients_match_oracle():
+@pytest.mark.parametrize("pool", [2, 4])
+def test_gradients_match_oracle(pool):
     import vring_b200 as V
     from oracle import unet_ref as U
-    nr, nz = 32, 64
-    net = V.UNet(nr, nz, CH, seed=6)
+    nr, nz = (32, 64) if pool == 2 else (64, 128)
+    net = V.UNet(nr, nz, CH, seed=6, pool=pool)
     w = net.get_params()
     rng = np.random.default_rng(1)
     x, g = rng.standard_normal((nr, nz)), rng.standard_normal((nr, nz))
     dw, dx = net.backward(x, g)
-    dwo, dxo = U.backward(w, CH, x, g)
+    dwo, dxo = U.backward(w, CH, x, g, F=pool)
     off = 0
     for i, (ci, co, _) in enumerate(U.layers(CH) + [(CH[0], 1, 0)]):
         n = ci * co * (9 if i < 14 else 1)
@@ -115,7 +117,7 @@ def test_training_on_solver_triples_cuts_iterations_small_grid():
     from vring_b200 import learned as Lr
     nr, nz = 64, 128
     k = V.K2d(Lr.tanh_faces(nr), nz, Lr.ZMAX)
-    net = V.UNet(nr, nz, Lr.CHANNELS, seed=1)
+    net = V.UNet(nr, nz, Lr.CHANNELS, seed=1, pool=2)
     losses = Lr.train(net, k, 300, batch=4, lr=3e-3, lr_final=3e-4)
     print("loss %.3e -> %.3e" % (losses[0], np.mean(losses[-20:])))
     assert np.mean(losses[-20:]) < 0.5 * losses[0]
@@ -141,7 +143,7 @@ def test_trained_network_cuts_vr2d_iterations_3x():
     import vring_b200 as V
     from vring_b200 import learned as Lr
     k = V.K2d(Lr.tanh_faces(Lr.NR), Lr.NZ, Lr.ZMAX)
-    net = V.UNet(Lr.NR, Lr.NZ, Lr.CHANNELS, seed=1)
+    net = Lr.make_net()
     Lr.load_weights(net)
     seq = Lr.RingSequence(2, k.faces, Lr.NZ, Lr.ZMAX)
     f, p_prev, p = Lr.triple(k, seq, 500)

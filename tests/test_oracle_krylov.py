@@ -92,3 +92,21 @@ def test_bf16_rounding_is_nearest_even():
     assert U.bf16(-2.5) == -2.5
     v = struct.unpack("f", struct.pack("I", 0x3F808001))[0]
     assert U.bf16(v) == 1.0 + 2.0 ** -7
+
+
+def test_unet_reverse_pass_with_4x4_pooling():
+    from oracle import unet_ref as U
+    ch = (8, 8, 8, 8)
+    rng = np.random.default_rng(5)
+    w = rng.standard_normal(U.nparams(ch)) * 0.2
+    x, g = rng.standard_normal((64, 64)), rng.standard_normal((64, 64))
+    ident = lambda a: np.asarray(a, dtype=np.float64)  # noqa: E731
+    gw, gx = U.backward(w, ch, x, g, rnd=ident, F=4)
+    L = lambda w_, x_: np.sum(g * U.forward(w_, ch, x_, rnd=ident, F=4))  # noqa: E731
+    for idx in rng.choice(w.size, 8, replace=False):
+        e = np.zeros_like(w)
+        e[idx] = 1e-4
+        assert abs((L(w + e, x) - L(w - e, x)) / 2e-4 - gw[idx]) <= 1e-6 * max(1.0, abs(gw[idx]))
+    e = np.zeros_like(x)
+    e[17, 40] = 1e-4
+    assert abs((L(w, x + e) - L(w, x - e)) / 2e-4 - gx[17, 40]) <= 1e-6 * max(1.0, abs(gx[17, 40]))

@@ -55,7 +55,7 @@ class K2dDesc(C.Structure):
 
 class UnetDesc(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("nr", C.c_int32), ("nz", C.c_int32), ("ch", C.c_int32 * 4),
-                ("device", C.c_int32), ("flags", C.c_int32)]
+                ("pool", C.c_int32), ("device", C.c_int32), ("flags", C.c_int32)]
 
 
 KRYLOV = {"cg": 0, "pcg": 1, "jacobi": 1, "bicgstab": 2, "fcg": 3, "learned": 3}
@@ -588,11 +588,13 @@ class UNet:
 
     CUDA_CORES = 1
 
-    def __init__(self, nr: int, nz: int, ch=(16, 32, 48, 64), seed: int = 0, device: int = 0, flags: int = 0):
-        """flags = UNet.CUDA_CORES runs the forward convolutions on the CUDA
-        cores instead of the tensor cores."""
-        self.nr, self.nz, self.ch = int(nr), int(nz), tuple(int(c) for c in ch)
-        d = UnetDesc(VR_ABI_VERSION, self.nr, self.nz, (C.c_int32 * 4)(*self.ch), device, flags)
+    def __init__(self, nr: int, nz: int, ch=(16, 32, 48, 64), seed: int = 0, device: int = 0, flags: int = 0,
+                 pool: int = 2):
+        """pool: the pooling factor between levels (2 or 4); flags =
+        UNet.CUDA_CORES runs the forward convolutions on the CUDA cores
+        instead of the tensor cores."""
+        self.nr, self.nz, self.ch, self.pool = int(nr), int(nz), tuple(int(c) for c in ch), int(pool)
+        d = UnetDesc(VR_ABI_VERSION, self.nr, self.nz, (C.c_int32 * 4)(*self.ch), self.pool, device, flags)
         self._h = C.c_void_p()
         rc = lib().vr_unet_create(C.byref(d), seed, C.byref(self._h))
         if rc:

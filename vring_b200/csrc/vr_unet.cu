@@ -49,6 +49,7 @@ struct UnetLayer {
 struct vr_unet {
   int nr = 0, nz = 0, dev = 0;
   int ch[4] = {};
+  int pool = 2;  // pooling factor between levels
   std::string err;
   vr::UnetLayer L[vr::kUnetLayers];
   size_t nparam = 0;
@@ -332,53 +333,60 @@ __global__ void __launch_bounds__(256) k_wgrad3(const float *__restrict__ dout, 
     for (int t = 0; t < 9; t++) atomicAdd(dw + ((size_t)(co0 + co) * 9 + t) * cin + ci0 + ci, acc[t]);
 }
 
-// 2x2 average pooling and its gradient
-__global__ void k_pool(const __nv_bfloat16 *__restrict__ in, int H, int W, int c, __nv_bfloat16 *__restrict__ out) {
-  const int H2 = H / 2, W2 = W / 2;
+// F x F average pooling (children summed in FP32, r fastest, then scaled by
+// 1 / F^2) and its gradient
+__global__ void k_pool(const __nv_bfloat16 *__restrict__ in, int H, int W, int c, int F,
+                       __nv_bfloat16 *__restrict__ out) {
+  const int H2 = H / F, W2 = W / F;
   const size_t n = (size_t)H2 * W2 * c;
+  const float inv = 1.f / (float)(F * F);
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int ch = (int)(e % c);
     const size_t p = e / c;
     const int J = (int)(p % H2), K = (int)(p / H2);
-    const size_t b = ((size_t)2 * J + (size_t)H * 2 * K) * c + ch;
-    const float s = tof(in[b]) + tof(in[b + c]) + tof(in[b + (size_t)H * c]) + tof(in[b + (size_t)H * c + c]);
-    out[e] = __float2bfloat16_rn(0.25f * s);
+    float s = 0.f;
+    for (int dz = 0; dz < F; dz++)
+      for (int dr = 0; dr < F; dr++) s += tof(in[((size_t)F * J + dr + (size_t)H * ((size_t)F * K + dz)) * c + ch]);
+    out[e] = __float2bfloat16_rn(inv * s);
   }
 }
-// gin[p][c] += 0.25 gout[parent(p)][c]
-__global__ void k_pool_bwd(const float *__restrict__ gout, int H, int W, int c, float *__restrict__ gin) {
+// gin[p][c] += gout[parent(p)][c] / F^2
+__global__ void k_pool_bwd(const float *__restrict__ gout, int H, int W, int c, int F, float *__restrict__ gin) {
   const size_t n = (size_t)H * W * c;
-  const int H2 = H / 2;
+  const int H2 = H / F;
+  const float inv = 1.f / (float)(F * F);
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int ch = (int)(e % c);
     const size_t p = e / c;
     const int j = (int)(p % H), k = (int)(p / H);
-    gin[e] += 0.25f * gout[((size_t)(j / 2) + (size_t)H2 * (k / 2)) * c + ch];
+    gin[e] += inv * gout[((size_t)(j / F) + (size_t)H2 * (k / F)) * c + ch];
   }
 }
 // out[p] = [coarse[parent(p)] (ca channels), skip[p] (cb channels)]
 __global__ void k_upcat(const __nv_bfloat16 *__restrict__ coarse, int ca, const __nv_bfloat16 *__restrict__ skip,
-                        int cb, int H, int W, __nv_bfloat16 *__restrict__ out) {
-  const int c = ca + cb, H2 = H / 2;
+                        int cb, int H, int W, int F, __nv_bfloat16 *__restrict__ out) {
+  const int c = ca + cb, H2 = H / F;
   const size_t n = (size_t)H * W * c;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int ch = (int)(e % c);
     const size_t p = e / c;
     const int j = (int)(p % H), k = (int)(p / H);
-    out[e] = ch < ca ? coarse[((size_t)(j / 2) + (size_t)H2 * (k / 2)) * ca + ch] : skip[p * cb + ch - ca];
+    out[e] = ch < ca ? coarse[((size_t)(j / F) + (size_t)H2 * (k / F)) * ca + ch] : skip[p * cb + ch - ca];
   }
 }
-// gradient of k_upcat: gcoarse = sum over the 4 children, gskip += the skip part
-__global__ void k_upcat_bwd(const float *__restrict__ gout, int ca, int cb, int H, int W, float *__restrict__ gcoarse,
-                            float *__restrict__ gskip) {
-  const int c = ca + cb, H2 = H / 2, W2 = W / 2;
+// gradient of k_upcat: gcoarse = sum over the F^2 children, gskip += the skip part
+__global__ void k_upcat_bwd(const float *__restrict__ gout, int ca, int cb, int H, int W, int F,
+                            float *__restrict__ gcoarse, float *__restrict__ gskip) {
+  const int c = ca + cb, H2 = H / F, W2 = W / F;
   const size_t nc = (size_t)H2 * W2 * ca;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nc; e += (size_t)gridDim.x * blockDim.x) {
     const int ch = (int)(e % ca);
     const size_t P = e / ca;
     const int J = (int)(P % H2), K = (int)(P / H2);
-    const size_t b = ((size_t)2 * J + (size_t)H * 2 * K) * c + ch;
-    gcoarse[e] = gout[b] + gout[b + c] + gout[b + (size_t)H * c] + gout[b + (size_t)H * c + c];
+    float s = 0.f;
+    for (int dz = 0; dz < F; dz++)
+      for (int dr = 0; dr < F; dr++) s += gout[((size_t)F * J + dr + (size_t)H * ((size_t)F * K + dz)) * c + ch];
+    gcoarse[e] = s;
   }
   const size_t ns = (size_t)H * W * cb;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ns; e += (size_t)gridDim.x * blockDim.x) {
@@ -615,7 +623,11 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
   if (!d || !out) return VR_ERR_ARG;
   *out = nullptr;
   if (d->abi_version != VR_ABI_VERSION) return VR_ERR_DESC;
-  if (d->nr < 8 || d->nz < 8 || d->nr % 8 || d->nz % 8 || (int64_t)d->nr * d->nz > ((int64_t)1 << 24)) return VR_ERR_DESC;
+  const int F = d->pool == 0 ? 2 : d->pool;
+  if (F != 2 && F != 4) return VR_ERR_DESC;
+  const int F3 = F * F * F;
+  if (d->nr < F3 || d->nz < F3 || d->nr % F3 || d->nz % F3 || (int64_t)d->nr * d->nz > ((int64_t)1 << 24))
+    return VR_ERR_DESC;
   for (int l = 0; l < 4; l++)
     if (d->ch[l] < 8 || d->ch[l] > 64 || d->ch[l] % 8) return VR_ERR_DESC;  // a 3x3 layer's output <= 64
   if (d->ch[0] > 64) return VR_ERR_DESC;  // the head's gradient keeps c0 sums per thread
@@ -631,6 +643,7 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
   };
   u->nr = d->nr;
   u->nz = d->nz;
+  u->pool = F;
   u->dev = d->device;
   for (int l = 0; l < 4; l++) u->ch[l] = d->ch[l];
   if (cudaSetDevice(u->dev) != cudaSuccess) return fail(VR_ERR_CUDA);
@@ -689,7 +702,9 @@ extern "C" int vr_unet_create(const vr_unet_desc *d, uint64_t seed, vr_unet **ou
   if (cudaMalloc(&u->dscal, sizeof(double) * 8) != cudaSuccess) return fail(VR_ERR_OOM);
   vr_unet *x = u;
   for (int i = 0; i < S_NSLOT; i++) {
-    const size_t n = (P0 >> (2 * sh.lev[i])) * sh.ch[i];
+    size_t div = 1;
+    for (int l = 0; l < sh.lev[i]; l++) div *= (size_t)u->pool * u->pool;
+    const size_t n = (P0 / div) * sh.ch[i];
     if (cudaMalloc(&x->a[i], sizeof(__nv_bfloat16) * n) != cudaSuccess) return fail(VR_ERR_OOM);
     if (cudaMalloc(&x->g[i], sizeof(float) * n) != cudaSuccess) return fail(VR_ERR_OOM);
   }
@@ -759,8 +774,9 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
   const vr_unet *x = u;
   cudaError_t e;
   auto HW = [&](int lev, int &H, int &W) {
-    H = u->nr >> lev;
-    W = u->nz >> lev;
+    H = u->nr;
+    W = u->nz;
+    for (int l = 0; l < lev; l++) H /= u->pool, W /= u->pool;
   };
   int H, W;
   auto conv = [&](int li) -> cudaError_t {
@@ -773,14 +789,15 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
   };
   auto pool = [&](int src, int dst) {
     HW(sh.lev[src], H, W);
-    const size_t n = (size_t)(H / 2) * (W / 2) * sh.ch[src];
-    k_pool<<<grid_for(n), 256, 0, s>>>(x->a[src], H, W, sh.ch[src], x->a[dst]);
+    const size_t n = (size_t)(H / u->pool) * (W / u->pool) * sh.ch[src];
+    k_pool<<<grid_for(n), 256, 0, s>>>(x->a[src], H, W, sh.ch[src], u->pool, x->a[dst]);
     return cudaGetLastError();
   };
   auto upcat = [&](int coarse, int skip, int dst) {
     HW(sh.lev[skip], H, W);
     const size_t n = (size_t)H * W * sh.ch[dst];
-    k_upcat<<<grid_for(n), 256, 0, s>>>(x->a[coarse], sh.ch[coarse], x->a[skip], sh.ch[skip], H, W, x->a[dst]);
+    k_upcat<<<grid_for(n), 256, 0, s>>>(x->a[coarse], sh.ch[coarse], x->a[skip], sh.ch[skip], H, W, u->pool,
+                                        x->a[dst]);
     return cudaGetLastError();
   };
   if ((e = conv(0)) || (e = conv(1)) || (e = pool(S_E0, S_P1))) return e;
@@ -803,8 +820,9 @@ static cudaError_t unet_bwd(const vr_unet *u, bool want_dx, cudaStream_t s) {
   cudaError_t e;
   int H, W;
   auto HW = [&](int lev) {
-    H = u->nr >> lev;
-    W = u->nz >> lev;
+    H = u->nr;
+    W = u->nz;
+    for (int l = 0; l < lev; l++) H /= u->pool, W /= u->pool;
   };
   for (int i = 0; i < S_NSLOT; i++) {
     HW(sh.lev[i]);
@@ -831,13 +849,14 @@ static cudaError_t unet_bwd(const vr_unet *u, bool want_dx, cudaStream_t s) {
   auto upcat_bwd = [&](int coarse, int skip, int dst) {
     HW(sh.lev[skip]);
     const size_t n = (size_t)H * W * sh.ch[skip];
-    k_upcat_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], sh.ch[coarse], sh.ch[skip], H, W, x->g[coarse], x->g[skip]);
+    k_upcat_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], sh.ch[coarse], sh.ch[skip], H, W, u->pool, x->g[coarse],
+                                            x->g[skip]);
     return cudaGetLastError();
   };
   auto pool_bwd = [&](int src, int dst) {
     HW(sh.lev[src]);
     const size_t n = (size_t)H * W * sh.ch[src];
-    k_pool_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], H, W, sh.ch[src], x->g[src]);
+    k_pool_bwd<<<grid_for(n), 256, 0, s>>>(x->g[dst], H, W, sh.ch[src], u->pool, x->g[src]);
     return cudaGetLastError();
   };
   if ((e = conv_bwd(13)) || (e = conv_bwd(12)) || (e = upcat_bwd(S_D1, S_E0, S_U0))) return e;

@@ -3,7 +3,11 @@
 Grid (the axisymmetric deck, r in [0, 5], z in [0, 15], 512 x 1024 cells) with
 the radial faces clustered toward the ring radius r = 1 by a tanh map of
 strength beta = 2: the index coordinate xi = A + B tanh(beta (r - 1) / 5)
-runs uniformly from 0 to 1.
+runs uniformly from 0 to 1.  The network pools 4 x 4 between its four levels
+(512 x 1024 down to 8 x 16), so its coarsest level sees the whole domain: with
+2 x 2 pooling the coarsest level is 64 x 128 cells, a preconditioner of that
+reach cannot act on the domain-wide modes, and the flexible CG stalled on
+this grid.
 
 Training data: (right-hand side, previous-step pressure, converged pressure)
 triples from seeded synthetic sequences (seeds 2-21): a Gaussian-core ring
@@ -36,6 +40,7 @@ from .api import K2d, UNet
 NR, NZ, RMAX, ZMAX = 512, 1024, 5.0, 15.0
 BETA, RCLUST = 2.0, 1.0
 CHANNELS = (16, 32, 48, 64)
+POOL = 4  # 4 x 4 pooling: levels of 512 x 1024, 128 x 256, 32 x 64 and 8 x 16 cells
 SEEDS = tuple(range(2, 22))
 STEPS_PER_SEED = 1000
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "unet_vr2d_512x1024.npz")
@@ -94,18 +99,19 @@ def make_solver(device: int = 0, nr: int = NR, nz: int = NZ) -> K2d:
     return K2d(tanh_faces(nr), nz, ZMAX, device=device)
 
 
-def make_net(device: int = 0, nr: int = NR, nz: int = NZ, seed: int = 1, ch=CHANNELS) -> UNet:
-    return UNet(nr, nz, ch, seed=seed, device=device)
+def make_net(device: int = 0, nr: int = NR, nz: int = NZ, seed: int = 1, ch=CHANNELS, pool: int = POOL) -> UNet:
+    return UNet(nr, nz, ch, seed=seed, device=device, pool=pool)
 
 
 def save_weights(net: UNet, path: str = WEIGHTS, **meta) -> None:
     os.makedirs(os.path.dirname(path), exist_ok=True)
-    np.savez(path, w=net.get_params(), ch=np.array(net.ch), nr=net.nr, nz=net.nz, **meta)
+    np.savez(path, w=net.get_params(), ch=np.array(net.ch), nr=net.nr, nz=net.nz, pool=net.pool, **meta)
 
 
 def load_weights(net: UNet, path: str = WEIGHTS) -> dict:
     d = np.load(path)
     assert tuple(d["ch"]) == net.ch and int(d["nr"]) == net.nr and int(d["nz"]) == net.nz
+    assert int(d["pool"]) == net.pool
     net.set_params(d["w"])
     return {k: d[k] for k in d.files if k not in ("w",)}
 
