@@ -38,7 +38,8 @@ namespace vr {
 
 constexpr int kK2dThreads = 256;
 constexpr int kK2dMaxBlocks = 1024;
-constexpr int kK2dChunk = 32;  // iterations per captured graph (even)
+constexpr int kK2dChunk = 32;        // iterations per captured graph
+constexpr int kK2dChunkLearned = 4;  // for the learned flexible CG (each iteration runs the network)
 
 // scalar slots
 enum K2dScal {
@@ -368,9 +369,9 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr(int n, double *__restri
 
 // FCG: p = z - beta p
 __global__ void __launch_bounds__(kK2dThreads) k2d_fcg_p(int n, double *__restrict__ p, const double *__restrict__ z,
-                                                       const double *sc, const int *flags, int first) {
+                                                       const double *sc, const int *flags) {
   if (flags[0]) return;
-  const double be = first ? 0.0 : sc[SC_BETA];
+  const double be = flags[1] == 0 ? 0.0 : sc[SC_BETA];  // the first direction is z itself
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] - be * p[i];
 }
 
@@ -738,7 +739,8 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
     cudaGraph_t gr = nullptr;
     K2D_CUDA(k, cudaStreamBeginCapture(k->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < kK2dChunk && e == cudaSuccess; i++) e = enq(k, arg);
+    const int chunk = slot == 3 ? kK2dChunkLearned : kK2dChunk;
+    for (int i = 0; i < chunk && e == cudaSuccess; i++) e = enq(k, arg);
     cudaError_t e2 = cudaStreamEndCapture(k->stream, &gr);
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&k->graph[slot], gr, 0);
@@ -747,7 +749,8 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
     k->graph_ok[slot] = true;
   }
   int h[2] = {0, 0};
-  for (int done = 0; done < maxit; done += kK2dChunk) {
+  const int chunk = slot == 3 ? kK2dChunkLearned : kK2dChunk;
+  for (int done = 0; done < maxit; done += chunk) {
     K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
     K2D_CUDA(k, cudaStreamSynchronize(k->stream));
     if (h[0] || h[1] >= maxit) break;
@@ -762,43 +765,33 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
 static cudaError_t enq_cg(vr_k2d *k, int jacobi) { return enqueue_cg_iter(k, jacobi); }
 static cudaError_t enq_bicg(vr_k2d *k, int) { return enqueue_bicg_iter(k); }
 
-// FCG with the learned preconditioner: z = |r| N(r / |r|), p = z - beta p_old
+// One iteration of the flexible CG with the learned preconditioner:
+// z = s D N(D r / s) (D = diag(S)^-1/2, s the RMS of D r), p = z - beta p_old
 // with beta = (z . q_old) / (p_old . q_old) (Notay's flexible CG, one
-// direction kept), alpha = (p . r) / (p . q).  Host-driven (the network is a
-// sequence of launches); scalars stay on the device.
-static int run_fcg(vr_k2d *k, int maxit, int *iters) {
+// direction kept; beta = 0 on the first iteration), alpha = (p . r) / (p . q).
+// Everything stays on the device, so chunks of iterations, the network's
+// launches included, are captured as graphs like the other methods.
+static cudaError_t enqueue_fcg_iter(vr_k2d *k) {
   const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
   double *P = k->part;
   double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *q = k->vec[V_Q], *z = k->vec[V_Z];
-  int h[2] = {0, 0};
-  for (int it = 0; it < maxit; it++) {
-    if (it % 8 == 0) {
-      K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
-      K2D_CUDA(k, cudaStreamSynchronize(k->stream));
-      if (h[0]) break;
-    }
-    k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, r, k2d_dhalf(k), P, k->flags);
-    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
-    int rc = unet_precondition(k->net, r, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream);
-    if (rc) return k2d_err(k, rc, std::string("learned preconditioner: ") + vr_unet_last_error(k->net));
-    if (it > 0) {
-      k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, q, nullptr, nullptr, P, nullptr);
-      k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_BETA, P, gb, k->sc, k->flags);
-    }
-    k2d_fcg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags, it == 0);
-    k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P + kK2dMaxBlocks, k->flags);
-    k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, nullptr, nullptr, P, nullptr);
-    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_ALPHA, P, gb, k->sc, k->flags);
-    k2d_fcg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, q, k->sc, P, k->flags);
-    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_CONV, P, gb, k->sc, k->flags);
-    K2D_CUDA(k, cudaGetLastError());
-  }
-  K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
-  K2D_CUDA(k, cudaStreamSynchronize(k->stream));
-  *iters = h[1];
-  return VR_OK;
+  k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, r, k2d_dhalf(k), P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
+  if (unet_precondition(k->net, r, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream) != VR_OK)
+    return cudaErrorLaunchFailure;
+  // beta against the previous direction (ignored on the first iteration)
+  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, q, nullptr, nullptr, P, nullptr);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_BETA, P, gb, k->sc, k->flags);
+  k2d_fcg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags);
+  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P + kK2dMaxBlocks, k->flags);
+  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, nullptr, nullptr, P, nullptr);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_ALPHA, P, gb, k->sc, k->flags);
+  k2d_fcg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, q, k->sc, P, k->flags);
+  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_CONV, P, gb, k->sc, k->flags);
+  return cudaGetLastError();
 }
+static cudaError_t enq_fcg(vr_k2d *k, int) { return enqueue_fcg_iter(k); }
 
 extern "C" int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *net) {
   if (!k) return VR_ERR_ARG;
@@ -806,6 +799,10 @@ extern "C" int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *net) {
     int nr = 0, nz = 0;
     unet_dims(net, &nr, &nz);
     if (nr != k->nr || nz != k->nz) return k2d_err(k, VR_ERR_ARG, "network and operator grids differ");
+  }
+  if (k->net != net && k->graph_ok[3]) {
+    cudaGraphExecDestroy(k->graph[3]);
+    k->graph_ok[3] = false;
   }
   k->net = net;
   return VR_OK;
@@ -884,7 +881,7 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
     k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
     k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
     K2D_CUDA(k, cudaGetLastError());
-    rc = run_fcg(k, maxit, &it);
+    rc = run_chunks(k, 3, enq_fcg, 0, maxit, &it);
   }
   if (rc) return rc;
   // true residual of the returned x, in the form the method iterated on
