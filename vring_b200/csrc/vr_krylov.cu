@@ -40,10 +40,11 @@ constexpr int kK2dThreads = 256;
 constexpr int kK2dMaxBlocks = 1024;
 constexpr int kK2dChunk = 32;        // iterations per captured graph
 constexpr int kK2dChunkLearned = 4;  // for the learned flexible CG (each iteration runs the network)
+constexpr int kFcgKeep = 8;          // directions the flexible CG keeps (truncated FCG(m), Notay 2000)
 
 // scalar slots
 enum K2dScal {
-  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_PQ, SC_SS, SC_ER, SC_N
+  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_SS, SC_N
 };
 // partial-sum slots
 enum K2dPart { PT_A = 0, PT_B, PT_C, PT_D, PT_N };
@@ -68,6 +69,9 @@ struct vr_k2d {
   std::string err;
   const vr_unet *net = nullptr;  // learned preconditioner for VR_KRYLOV_FCG_LEARNED
   std::vector<double> h_faces;
+  // the flexible CG's kept directions p_i and q_i = S p_i (a ring of
+  // kFcgKeep slots each), their p_i . q_i, the betas, and partial sums
+  double *fp = nullptr, *fq = nullptr, *fpq = nullptr, *fbeta = nullptr, *fpart = nullptr;
 };
 
 namespace vr {
@@ -203,8 +207,6 @@ enum K2dScalarOp {
   SO_BI_ALPHA,      // alpha = rho / rh.v [A]
   SO_BI_OMEGA,      // omega = t.s [A] / t.t [B]
   SO_BI_CONV,       // rho_new = rh.r [A], rr [B]
-  SO_FCG_BETA,      // beta = z.q_old [A] / pq_old
-  SO_FCG_ALPHA,     // alpha = p.r [A] / p.q [B]; stores pq
   SO_FCG_CONV,      // rr [A]
   SO_NORM,          // rr [A] only (sc[SC_RR])
   SO_NORM_BB,       // bb [A] only (sc[SC_BB])
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
   const double *pA = part, *pB = part + kK2dMaxBlocks, *pC = part + 2 * kK2dMaxBlocks;
   double a = sum_part(pA, nb, sh);
   double b = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT || op == SO_BI_OMEGA ||
-              op == SO_BI_CONV || op == SO_FCG_ALPHA)
+              op == SO_BI_CONV)
                  ? sum_part(pB, nb, sh)
                  : 0.0;
   double c = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT) ? sum_part(pC, nb, sh) : 0.0;
@@ -265,13 +267,6 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       sc[SC_RR] = b;
       flags[1] += 1;
       if (b <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
-      break;
-    case SO_FCG_BETA:
-      sc[SC_BETA] = sc[SC_PQ] != 0.0 ? a / sc[SC_PQ] : 0.0;
-      break;
-    case SO_FCG_ALPHA:
-      sc[SC_ALPHA] = a / b;
-      sc[SC_PQ] = b;
       break;
     case SO_FCG_CONV:
       sc[SC_RR] = a;
@@ -367,14 +362,6 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr(int n, double *__restri
   if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = t1;
 }
 
-// FCG: p = z - beta p
-__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_p(int n, double *__restrict__ p, const double *__restrict__ z,
-                                                       const double *sc, const int *flags) {
-  if (flags[0]) return;
-  const double be = flags[1] == 0 ? 0.0 : sc[SC_BETA];  // the first direction is z itself
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] - be * p[i];
-}
-
 // partial sum of (D r)^2 [A] (the learned preconditioner's input scale)
 __global__ void __launch_bounds__(kK2dThreads) k2d_dscaled(int n, const double *__restrict__ r,
                                                          const double *__restrict__ dh, double *part,
@@ -390,22 +377,125 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_dscaled(int n, const double *
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// FCG: x += alpha p; r -= alpha q; partial r.r [A]
-__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_xr(int n, double *__restrict__ x, double *__restrict__ r,
-                                                        const double *__restrict__ p, const double *__restrict__ q,
-                                                        const double *sc, double *part, const int *flags) {
+// ---- truncated flexible CG with kFcgKeep directions ---------------------------
+// kept = min(iteration, kFcgKeep); the new direction goes to slot iteration % kFcgKeep
+__device__ __forceinline__ int fcg_kept(const int *flags) { return min(flags[1], kFcgKeep); }
+__device__ __forceinline__ int fcg_slot(const int *flags) { return flags[1] % kFcgKeep; }
+
+// partials of z . q_i for the kept directions
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_zq(int n, const double *__restrict__ z,
+                                                        const double *__restrict__ fq, double *fpart,
+                                                        const int *flags) {
   __shared__ double sh[40];
   if (flags[0]) return;
+  const int kept = fcg_kept(flags);
+  double acc[kFcgKeep];
+#pragma unroll
+  for (int i = 0; i < kFcgKeep; i++) acc[i] = 0.0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const double zi = z[e];
+#pragma unroll
+    for (int i = 0; i < kFcgKeep; i++)
+      if (i < kept) acc[i] += zi * fq[(size_t)i * n + e];
+  }
+  for (int i = 0; i < kept; i++) {
+    const double t = block_sum(acc[i], sh);
+    if (threadIdx.x == 0) fpart[(size_t)i * kK2dMaxBlocks + blockIdx.x] = t;
+    __syncthreads();
+  }
+}
+
+// beta_i = (z . q_i) / (p_i . q_i)
+__global__ void __launch_bounds__(1024) k2d_fcg_betas(const double *fpart, int nb, const double *fpq, double *fbeta,
+                                                    const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const int kept = fcg_kept(flags);
+  for (int i = 0; i < kept; i++) {
+    const double a = sum_part(fpart + (size_t)i * kK2dMaxBlocks, nb, sh);
+    if (threadIdx.x == 0) fbeta[i] = fpq[i] != 0.0 ? a / fpq[i] : 0.0;
+  }
+}
+
+// p = z - sum_i beta_i p_i, written to the new slot (which may be the oldest
+// kept direction: each element is read before it is overwritten)
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_pm(int n, const double *__restrict__ z, double *fp,
+                                                        const double *__restrict__ fbeta, const int *flags) {
+  if (flags[0]) return;
+  const int kept = fcg_kept(flags), slot = fcg_slot(flags);
+  double b[kFcgKeep];
+#pragma unroll
+  for (int i = 0; i < kFcgKeep; i++) b[i] = i < kept ? fbeta[i] : 0.0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    double v = z[e];
+#pragma unroll
+    for (int i = 0; i < kFcgKeep; i++)
+      if (i < kept) v -= b[i] * fp[(size_t)i * n + e];
+    fp[(size_t)slot * n + e] = v;
+  }
+}
+
+// q = S p for the new slot, partial p . q [B]
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_apply(K2dOp o, const double *fp, double *fq, double *part,
+                                                           const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const int slot = fcg_slot(flags);
+  const double *x = fp + (size_t)slot * o.n;
+  double *y = fq + (size_t)slot * o.n;
+  const double mean = last_row_mean(o, x, sh);
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double v = apply_S_at(o, x, i, mean);
+    y[i] = v;
+    acc += x[i] * v;
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = t;
+}
+
+// partial p . r [A] of the new slot
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_pr(int n, const double *__restrict__ fp,
+                                                        const double *__restrict__ r, double *part, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double *p = fp + (size_t)fcg_slot(flags) * n;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += p[i] * r[i];
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// alpha = (p . r) / (p . q); p . q kept for the slot
+__global__ void __launch_bounds__(1024) k2d_fcg_alpha(const double *part, int nb, double *sc, double *fpq,
+                                                    const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double pr = sum_part(part, nb, sh);
+  const double pq = sum_part(part + kK2dMaxBlocks, nb, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_ALPHA] = pq != 0.0 ? pr / pq : 0.0;
+    fpq[fcg_slot(flags)] = pq;
+  }
+}
+
+// x += alpha p; r -= alpha q; partial r.r [A]
+__global__ void __launch_bounds__(kK2dThreads) k2d_fcg_xrm(int n, double *__restrict__ x, double *__restrict__ r,
+                                                         const double *__restrict__ fp, const double *__restrict__ fq,
+                                                         const double *sc, double *part, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const size_t so = (size_t)fcg_slot(flags) * n;
   const double al = sc[SC_ALPHA];
   double rr = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] += al * p[i];
-    const double ri = r[i] - al * q[i];
+    x[i] += al * fp[so + i];
+    const double ri = r[i] - al * fq[so + i];
     r[i] = ri;
     rr += ri * ri;
   }
-  double s = block_sum(rr, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  const double t = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 // ---- direct solve -----------------------------------------------------------
@@ -609,7 +699,8 @@ extern "C" int vr_k2d_destroy(vr_k2d *k) {
     if (k->graph_ok[i]) cudaGraphExecDestroy(k->graph[i]);
   for (double *v : k->vec)
     if (v) cudaFree(v);
-  double *ps[] = {k->coef, k->part, k->sc, k->dct_f, k->dct_i, k->tlo, k->tup, k->tib, k->tmp};
+  double *ps[] = {k->coef, k->part, k->sc, k->dct_f, k->dct_i, k->tlo, k->tup, k->tib, k->tmp,
+                  k->fp, k->fq, k->fpq, k->fbeta, k->fpart};
   for (double *p : ps)
     if (p) cudaFree(p);
   if (k->flags) cudaFree(k->flags);
@@ -766,28 +857,31 @@ static cudaError_t enq_cg(vr_k2d *k, int jacobi) { return enqueue_cg_iter(k, jac
 static cudaError_t enq_bicg(vr_k2d *k, int) { return enqueue_bicg_iter(k); }
 
 // One iteration of the flexible CG with the learned preconditioner:
-// z = s D N(D r / s) (D = diag(S)^-1/2, s the RMS of D r), p = z - beta p_old
-// with beta = (z . q_old) / (p_old . q_old) (Notay's flexible CG, one
-// direction kept; beta = 0 on the first iteration), alpha = (p . r) / (p . q).
+// z = s D N(D r / s) (D = diag(S)^-1/2, s the RMS of D r); the new direction
+// is z made S-orthogonal to the last kFcgKeep directions,
+// p = z - sum_i (z . q_i) / (p_i . q_i) p_i (Notay's truncated FCG: the
+// network is not a symmetric map, so one kept direction, which plain CG's
+// recurrence amounts to, loses the S-orthogonality the method relies on);
+// alpha = (p . r) / (p . q).
 // Everything stays on the device, so chunks of iterations, the network's
 // launches included, are captured as graphs like the other methods.
 static cudaError_t enqueue_fcg_iter(vr_k2d *k) {
   const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
   double *P = k->part;
-  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *q = k->vec[V_Q], *z = k->vec[V_Z];
+  double *x = k->vec[V_X], *r = k->vec[V_R], *z = k->vec[V_Z];
   k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, r, k2d_dhalf(k), P, k->flags);
   k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
   if (unet_precondition(k->net, r, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream) != VR_OK)
     return cudaErrorLaunchFailure;
-  // beta against the previous direction (ignored on the first iteration)
-  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, q, nullptr, nullptr, P, nullptr);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_BETA, P, gb, k->sc, k->flags);
-  k2d_fcg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags);
-  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P + kK2dMaxBlocks, k->flags);
-  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, nullptr, nullptr, P, nullptr);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_ALPHA, P, gb, k->sc, k->flags);
-  k2d_fcg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, q, k->sc, P, k->flags);
+  // orthogonalise z against the kept directions in S's inner product
+  k2d_fcg_zq<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, k->fq, k->fpart, k->flags);
+  k2d_fcg_betas<<<1, 1024, 0, k->stream>>>(k->fpart, gb, k->fpq, k->fbeta, k->flags);
+  k2d_fcg_pm<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, k->fp, k->fbeta, k->flags);
+  k2d_fcg_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, k->fp, k->fq, P, k->flags);
+  k2d_fcg_pr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, k->fp, r, P, k->flags);
+  k2d_fcg_alpha<<<1, 1024, 0, k->stream>>>(P, gb, k->sc, k->fpq, k->flags);
+  k2d_fcg_xrm<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, k->fp, k->fq, k->sc, P, k->flags);
   k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_FCG_CONV, P, gb, k->sc, k->flags);
   return cudaGetLastError();
 }
@@ -878,6 +972,14 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
     K2D_CUDA(k, cudaGetLastError());
     rc = run_chunks(k, 2, enq_bicg, 0, maxit, &it);
   } else {
+    if (!k->fp) {
+      const size_t kb = sizeof(double) * kFcgKeep * (size_t)k->n;
+      if (cudaMalloc(&k->fp, kb) != cudaSuccess || cudaMalloc(&k->fq, kb) != cudaSuccess ||
+          cudaMalloc(&k->fpq, sizeof(double) * kFcgKeep) != cudaSuccess ||
+          cudaMalloc(&k->fbeta, sizeof(double) * kFcgKeep) != cudaSuccess ||
+          cudaMalloc(&k->fpart, sizeof(double) * kFcgKeep * kK2dMaxBlocks) != cudaSuccess)
+        return k2d_err(k, VR_ERR_OOM, "flexible CG directions");
+    }
     k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
     k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
     K2D_CUDA(k, cudaGetLastError());
