@@ -347,8 +347,11 @@ enum vr_krylov {
   VR_KRYLOV_CG = 0,           /* plain CG on S x = V f (the judge)            */
   VR_KRYLOV_PCG_JACOBI = 1,   /* CG with the inverse diagonal of S            */
   VR_KRYLOV_BICGSTAB = 2,     /* BiCGSTAB on K x = f                          */
-  VR_KRYLOV_FCG_LEARNED = 3   /* flexible CG, preconditioner = the vr_unet set
-                                 with vr_k2d_set_preconditioner               */
+  VR_KRYLOV_FCG_LEARNED = 3,  /* flexible CG, preconditioner = the vr_unet set
+                                 with vr_k2d_set_preconditioner, between the
+                                 damped-Jacobi steps of vr_k2d_set_smoothing */
+  VR_KRYLOV_FCG_JACOBI = 4    /* the same flexible CG with the Jacobi steps
+                                 alone (the method without the network)      */
 };
 VR_API int vr_k2d_create(const vr_k2d_desc *desc, vr_k2d **out);
 VR_API int vr_k2d_destroy(vr_k2d *k);
@@ -427,6 +430,11 @@ VR_API int vr_unet_train_step(vr_unet *u, vr_k2d *k, const double *e_dev, int32_
 VR_API int vr_k2d_diag(const vr_k2d *k, double *d);
 /* make the network the preconditioner of VR_KRYLOV_FCG_LEARNED (NULL clears) */
 VR_API int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *u);
+/* The flexible CG's preconditioner is z0 = w D^-1 r, z = z0 + N(r - S z0),
+ * z += w D^-1 (r - S z) (D the diagonal of S, N the network): a two-level step
+ * with the network as the correction between damped-Jacobi steps.  w in
+ * [0, 1], default 2/3; w = 0 applies the network alone. */
+VR_API int vr_k2d_set_smoothing(vr_k2d *k, double omega);
 
 /* No counterpart in the reference: solve_lap_thom on device arrays that
  * allocates nothing.  rhs, sol, aa, bb, cc are device pointers of the current

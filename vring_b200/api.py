@@ -58,7 +58,7 @@ class UnetDesc(C.Structure):
                 ("pool", C.c_int32), ("device", C.c_int32), ("flags", C.c_int32)]
 
 
-KRYLOV = {"cg": 0, "pcg": 1, "jacobi": 1, "bicgstab": 2, "fcg": 3, "learned": 3}
+KRYLOV = {"cg": 0, "pcg": 1, "jacobi": 1, "bicgstab": 2, "fcg": 3, "learned": 3, "fcg_jacobi": 4}
 
 
 def declared_symbols(header: str = HEADER) -> list[str]:
@@ -150,6 +150,7 @@ def lib():
         L.vr_k2d_solve.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp), C.POINTER(dp)]
         L.vr_k2d_solve_dev.argtypes = [vp, i32, vp, vp, dp, i32, C.POINTER(i32), C.POINTER(dp)]
         L.vr_k2d_set_preconditioner.argtypes = [vp, vp]
+        L.vr_k2d_set_smoothing.argtypes = [vp, C.c_double]
         L.vr_k2d_diag.argtypes = [vp, vp]
         L.vr_unet_create.argtypes = [C.POINTER(UnetDesc), C.c_uint64, C.POINTER(vp)]
         L.vr_unet_destroy.argtypes = [vp]
@@ -576,6 +577,10 @@ class K2d:
         d = np.empty((self.nr, self.nz), dtype=np.float64, order="F")
         self._chk(lib().vr_k2d_diag(self._h, _p(d)), "k2d_diag")
         return d
+
+    def set_smoothing(self, omega: float) -> None:
+        """Weight of the damped-Jacobi steps around the network (0: off)."""
+        self._chk(lib().vr_k2d_set_smoothing(self._h, omega), "k2d_set_smoothing")
 
     def set_preconditioner(self, net) -> None:
         self._chk(lib().vr_k2d_set_preconditioner(self._h, net._h if net is not None else None),

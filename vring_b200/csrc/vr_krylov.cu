@@ -64,14 +64,16 @@ struct vr_k2d {
   // and [k][kz]) and the radial Thomas factorisation per z mode
   double *dct_f = nullptr, *dct_i = nullptr, *tlo = nullptr, *tup = nullptr, *tib = nullptr;
   double *tmp = nullptr;
-  cudaGraphExec_t graph[4] = {};
-  bool graph_ok[4] = {};
+  cudaGraphExec_t graph[5] = {};  // CG, Jacobi CG, BiCGSTAB, learned FCG, Jacobi-only FCG
+  bool graph_ok[5] = {};
   std::string err;
   const vr_unet *net = nullptr;  // learned preconditioner for VR_KRYLOV_FCG_LEARNED
   std::vector<double> h_faces;
   // the flexible CG's kept directions p_i and q_i = S p_i (a ring of
   // kFcgKeep slots each), their p_i . q_i, the betas, and partial sums
   double *fp = nullptr, *fq = nullptr, *fpq = nullptr, *fbeta = nullptr, *fpart = nullptr;
+  // weight of the damped-Jacobi steps around the network (0: the network alone)
+  double omega = 2.0 / 3.0;
 };
 
 namespace vr {
@@ -498,6 +500,37 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_fcg_xrm(int n, double *__rest
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+// ---- the preconditioner's damped-Jacobi steps -----------------------------------
+// z0 = omega D^-1 r (D^-1 = dinv), t = r - S z0
+__global__ void __launch_bounds__(kK2dThreads) k2d_jac_pre(int n, double omega, const double *__restrict__ dinv,
+                                                         const double *__restrict__ r, double *__restrict__ z0,
+                                                         const int *flags) {
+  if (flags[0]) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z0[i] = omega * dinv[i] * r[i];
+}
+__global__ void __launch_bounds__(kK2dThreads) k2d_resid(K2dOp o, const double *__restrict__ x,
+                                                       const double *__restrict__ r, double *__restrict__ t,
+                                                       const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double mean = last_row_mean(o, x, sh);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x)
+    t[i] = r[i] - apply_S_at(o, x, i, mean);
+}
+// z += z0 (the network's correction on top of the pre-smoothing)
+__global__ void __launch_bounds__(kK2dThreads) k2d_addv(int n, double *__restrict__ z, const double *__restrict__ z0,
+                                                      const int *flags) {
+  if (flags[0]) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] += z0[i];
+}
+// z += omega D^-1 t (t = r - S z, the post-smoothing)
+__global__ void __launch_bounds__(kK2dThreads) k2d_jac_post(int n, double omega, const double *__restrict__ dinv,
+                                                          const double *__restrict__ t, double *__restrict__ z,
+                                                          const int *flags) {
+  if (flags[0]) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] += omega * dinv[i] * t[i];
+}
+
 // ---- direct solve -----------------------------------------------------------
 // C[row-major m x n] = A (m x k, column-major: A[i + m l]) times B^T where B is
 // row-major (n x k): C(i, c) = sum_l A(i, l) B(c, l); C stored column-major
@@ -695,7 +728,7 @@ extern "C" int vr_k2d_destroy(vr_k2d *k) {
   if (!k) return VR_OK;
   cudaSetDevice(k->dev);
   if (k->stream) cudaStreamSynchronize(k->stream);
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 5; i++)
     if (k->graph_ok[i]) cudaGraphExecDestroy(k->graph[i]);
   for (double *v : k->vec)
     if (v) cudaFree(v);
@@ -830,7 +863,7 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
     cudaGraph_t gr = nullptr;
     K2D_CUDA(k, cudaStreamBeginCapture(k->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
-    const int chunk = slot == 3 ? kK2dChunkLearned : kK2dChunk;
+    const int chunk = slot >= 3 ? kK2dChunkLearned : kK2dChunk;
     for (int i = 0; i < chunk && e == cudaSuccess; i++) e = enq(k, arg);
     cudaError_t e2 = cudaStreamEndCapture(k->stream, &gr);
     if (e == cudaSuccess) e = e2;
@@ -840,7 +873,7 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
     k->graph_ok[slot] = true;
   }
   int h[2] = {0, 0};
-  const int chunk = slot == 3 ? kK2dChunkLearned : kK2dChunk;
+  const int chunk = slot >= 3 ? kK2dChunkLearned : kK2dChunk;
   for (int done = 0; done < maxit; done += chunk) {
     K2D_CUDA(k, cudaMemcpyAsync(h, k->flags, sizeof(h), cudaMemcpyDeviceToHost, k->stream));
     K2D_CUDA(k, cudaStreamSynchronize(k->stream));
@@ -870,10 +903,33 @@ static cudaError_t enqueue_fcg_iter(vr_k2d *k) {
   const int gb = k2d_grid(k);
   double *P = k->part;
   double *x = k->vec[V_X], *r = k->vec[V_R], *z = k->vec[V_Z];
-  k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, r, k2d_dhalf(k), P, k->flags);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
-  if (unet_precondition(k->net, r, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream) != VR_OK)
-    return cudaErrorLaunchFailure;
+  // z = M r: with omega > 0 the network is the middle of a two-level step,
+  //   z0 = omega D^-1 r;  z = z0 + N(r - S z0);  z += omega D^-1 (r - S z)
+  // (damped-Jacobi steps before and after the network's correction, so the
+  // rough error components the network does not resolve are damped); without
+  // a network only the two Jacobi steps remain (the method the network is
+  // compared against)
+  const double om = k->omega;
+  double *z0 = k->vec[V_S], *t = k->vec[V_T];
+  const double *rin = r;
+  if (om > 0.0) {
+    k2d_jac_pre<<<gb, kK2dThreads, 0, k->stream>>>(o.n, om, o.dinv, r, z0, k->flags);
+    k2d_resid<<<gb, kK2dThreads, 0, k->stream>>>(o, z0, r, t, k->flags);
+    rin = t;
+  }
+  if (k->net) {
+    k2d_dscaled<<<gb, kK2dThreads, 0, k->stream>>>(o.n, rin, k2d_dhalf(k), P, k->flags);
+    k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_SS, P, gb, k->sc, k->flags);
+    if (unet_precondition(k->net, rin, z, k2d_dhalf(k), k->sc + SC_SS, k->flags, k->stream) != VR_OK)
+      return cudaErrorLaunchFailure;
+    if (om > 0.0) k2d_addv<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, z0, k->flags);
+  } else {
+    cudaMemcpyAsync(z, z0, sizeof(double) * o.n, cudaMemcpyDeviceToDevice, k->stream);
+  }
+  if (om > 0.0) {
+    k2d_resid<<<gb, kK2dThreads, 0, k->stream>>>(o, z, r, t, k->flags);
+    k2d_jac_post<<<gb, kK2dThreads, 0, k->stream>>>(o.n, om, o.dinv, t, z, k->flags);
+  }
   // orthogonalise z against the kept directions in S's inner product
   k2d_fcg_zq<<<gb, kK2dThreads, 0, k->stream>>>(o.n, z, k->fq, k->fpart, k->flags);
   k2d_fcg_betas<<<1, 1024, 0, k->stream>>>(k->fpart, gb, k->fpq, k->fbeta, k->flags);
@@ -886,6 +942,18 @@ static cudaError_t enqueue_fcg_iter(vr_k2d *k) {
   return cudaGetLastError();
 }
 static cudaError_t enq_fcg(vr_k2d *k, int) { return enqueue_fcg_iter(k); }
+
+extern "C" int vr_k2d_set_smoothing(vr_k2d *k, double omega) {
+  if (!k || !(omega >= 0.0) || omega > 1.0) return VR_ERR_ARG;
+  if (omega != k->omega)
+    for (int i = 3; i < 5; i++)
+      if (k->graph_ok[i]) {
+        cudaGraphExecDestroy(k->graph[i]);
+        k->graph_ok[i] = false;
+      }
+  k->omega = omega;
+  return VR_OK;
+}
 
 extern "C" int vr_k2d_set_preconditioner(vr_k2d *k, const vr_unet *net) {
   if (!k) return VR_ERR_ARG;
@@ -931,8 +999,10 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_init_dots(K2dOp o, int jacobi
 extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, double *x, double tol, int32_t maxit,
                                 int32_t *iters, double *relres) {
   if (!k || !f || !x || !(tol > 0) || maxit < 1) return VR_ERR_ARG;
-  if (method < VR_KRYLOV_CG || method > VR_KRYLOV_FCG_LEARNED) return VR_ERR_ARG;
+  if (method < VR_KRYLOV_CG || method > VR_KRYLOV_FCG_JACOBI) return VR_ERR_ARG;
   if (method == VR_KRYLOV_FCG_LEARNED && !k->net) return k2d_err(k, VR_ERR_STATE, "no learned preconditioner set");
+  if (method == VR_KRYLOV_FCG_JACOBI && !(k->omega > 0.0))
+    return k2d_err(k, VR_ERR_STATE, "the Jacobi-only flexible CG needs a smoothing weight > 0");
   K2D_CUDA(k, cudaSetDevice(k->dev));
   const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
@@ -983,7 +1053,11 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
     k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
     k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
     K2D_CUDA(k, cudaGetLastError());
-    rc = run_chunks(k, 3, enq_fcg, 0, maxit, &it);
+    // the graph bakes in whether the network runs: one slot per form
+    const vr_unet *keep = k->net;
+    if (method == VR_KRYLOV_FCG_JACOBI) k->net = nullptr;
+    rc = run_chunks(k, method == VR_KRYLOV_FCG_JACOBI ? 4 : 3, enq_fcg, 0, maxit, &it);
+    k->net = keep;
   }
   if (rc) return rc;
   // true residual of the returned x, in the form the method iterated on

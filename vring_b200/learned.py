@@ -165,10 +165,11 @@ def train(net: UNet, k2d: K2d, steps: int, batch: int = 8, lr: float = 3e-3, see
 
 
 def compare(k2d: K2d, net: UNet, f, x0=None, tol: float = 1e-10, maxit: int = 40000):
-    """Plain CG, Jacobi CG and the learned flexible CG on one right-hand side:
+    """Plain CG, Jacobi CG, the flexible CG with the Jacobi steps alone and
+    with the network between them, on one right-hand side:
     {method: (iterations, relres, ms, x)}; each stops after maxit iterations."""
     out = {}
-    for m in ("cg", "pcg", "learned"):
+    for m in ("cg", "pcg", "fcg_jacobi", "learned"):
         if m == "learned":
             k2d.set_preconditioner(net)
         x, it, rr, ms = k2d.solve(f, m, x0=x0, tol=tol, maxit=maxit)
