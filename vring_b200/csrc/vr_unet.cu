@@ -160,24 +160,42 @@ __global__ void __launch_bounds__(256) k_conv3(const TI *__restrict__ in, int H,
   }
 }
 
+// 16-byte asynchronous global -> shared copy; bytes < 16 zero-fills the rest
+// (0: no global read, the destination becomes zeros)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, unsigned bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // The same 3x3 convolution on the tensor cores (BF16 in, FP32 accumulate):
 // an implicit GEMM with M = 128 output pixels per CTA (the rows of A are the
 // CTA's pixels, its columns the 9 taps x CINP input channels of their
 // neighbourhoods), N = NOUT output channels and K = 9 CINP, where CINP and NOUT
 // are cin and cout rounded up to 16.  K runs in blocks of 64 columns through
-// two shared-memory stages that all 128 threads fill -- the im2col gather of A
-// and the packed weights B, both K-major with the 128-byte swizzle -- while
-// the tensor cores work on the other stage; one thread issues the four
-// K-steps of a block and commits them to the stage's mbarrier.  The FP32
+// kConvStages shared-memory stages, both operands K-major with the 128-byte
+// swizzle: every thread issues the asynchronous 16-byte copies of its pixel's
+// row of the im2col gather (A) and of a share of the packed weights (B) for
+// the blocks ahead, zero-filling taps outside the grid, so the gathers of
+// several blocks are in flight while the tensor cores work; one thread issues
+// the four K-steps of a block and commits them to the stage's mbarrier, whose
+// completion frees the stage for the block kConvStages later.  The FP32
 // accumulator stays in tensor memory (128 lanes = pixels, NOUT columns) until
 // the epilogue, where each warp loads its 32 lanes and stores BF16.  Every
 // mbarrier wait is bounded; a wait that gives up sets bit 0 of *status, and
 // the CTA still waits (bounded) for its MMAs and frees its tensor memory.
+constexpr int kConvStages = 3;
+
 template <int CINP, int NOUT>
 __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W, int cin,
                                                 const __nv_bfloat16 *__restrict__ wpk, int cout,
                                                 __nv_bfloat16 *__restrict__ out, unsigned *status) {
   static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
+  constexpr int S = kConvStages;
   constexpr int K = 9 * CINP;
   constexpr int KB = (K + 63) / 64;
   constexpr int ABYTES = 128 * 128, BBYTES = NOUT * 128, STAGE = ABYTES + BBYTES;
@@ -186,7 +204,7 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
   static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzle");
   extern __shared__ uint8_t smraw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t bar[2];
+  __shared__ uint64_t bar[S];
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
@@ -194,8 +212,7 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
     tmem_relinquish();
   }
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int i = 0; i < S; i++) mbar_init(&bar[i], 1);
     mbar_init_fence();
   }
   tc_fence_before();
@@ -207,52 +224,59 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
   const int pj = p % H, pk = p / H;
   const bool pin = p < P;
   bool ok = true;
-  for (int kb = 0; kb < KB; kb++) {
-    const int s = kb & 1;
-    uint8_t *As = sm + s * STAGE;
+  // the copies of K block kb into its stage (kb % S)
+  auto gather = [&](int kb) {
+    uint8_t *As = sm + (kb % S) * STAGE;
     uint8_t *Bs = As + ABYTES;
-    // the MMAs of block kb - 2 read this stage: wait for their commit
-    if (kb >= 2 && !mbar_wait(&bar[s], (unsigned)((kb - 2) >> 1) & 1u)) ok = false;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       const int k0 = kb * 64 + c * 8;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (pin && k0 < K) {
-        const int t = k0 / CINP, ci = k0 % CINP;  // 8 columns inside one tap (CINP % 16 == 0)
-        const int j = pj + t / 3 - 1, k = pk + t % 3 - 1;
-        if (ci < cin && j >= 0 && j < H && k >= 0 && k < W) {
-          const __nv_bfloat16 *src = in + ((size_t)j + (size_t)H * k) * cin + ci;
-          if ((cin & 7) == 0) {
-            v = *reinterpret_cast<const uint4 *>(src);
-          } else {
-            __nv_bfloat16 e[8];
+      const int t = k0 / CINP, ci = k0 % CINP;  // 8 columns inside one tap (CINP % 16 == 0)
+      const int j = pj + t / 3 - 1, k = pk + t % 3 - 1;
+      const bool live = pin && k0 < K && ci < cin && j >= 0 && j < H && k >= 0 && k < W;
+      const __nv_bfloat16 *src = live ? in + ((size_t)j + (size_t)H * k) * cin + ci : in;
+      if ((cin & 7) == 0) {
+        cp_async16(As + sw128_off(tid, c), src, live ? 16u : 0u);
+      } else {
+        __align__(16) __nv_bfloat16 e[8];
 #pragma unroll
-            for (int q = 0; q < 8; q++) e[q] = (ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
-            v = *reinterpret_cast<const uint4 *>(e);
-          }
-        }
+        for (int q = 0; q < 8; q++) e[q] = (live && ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
+        *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = *reinterpret_cast<const uint4 *>(e);
       }
-      *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = v;
     }
     for (int e = tid; e < NOUT * 8; e += 128) {
       const int n = e >> 3, c = e & 7, k0 = kb * 64 + c * 8;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (k0 < K) v = *reinterpret_cast<const uint4 *>(wpk + (size_t)n * K + k0);
-      *reinterpret_cast<uint4 *>(Bs + sw128_off(n, c)) = v;
+      cp_async16(Bs + sw128_off(n, c), k0 < K ? wpk + (size_t)n * K + k0 : wpk, k0 < K ? 16u : 0u);
     }
-    fence_proxy_async();  // the generic-proxy stores above, before the tensor cores read them
+  };
+#pragma unroll
+  for (int kb = 0; kb < S - 1; kb++) {
+    if (kb < KB) gather(kb);
+    cp_async_commit();
+  }
+  for (int kb = 0; kb < KB; kb++) {
+    cp_async_wait<S - 2>();  // this thread's copies of block kb have landed
+    fence_proxy_async();     // and, like the plain stores, are visible to the tensor cores
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(Bs);
+      uint8_t *As = sm + (kb % S) * STAGE;
+      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(As + ABYTES);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++)
         if (kb * 64 + kk * 16 < K) umma_bf16(tmem, ad + (uint64_t)(2 * kk), bd + (uint64_t)(2 * kk), IDESC, (kb | kk) ? 1u : 0u);
-      umma_commit(&bar[s]);
+      umma_commit(&bar[kb % S]);
     }
+    // block kb + S - 1 refills the stage that block kb - 1 used: wait for its MMAs
+    const int nb = kb + S - 1;
+    if (nb < KB) {
+      if (kb >= 1 && !mbar_wait(&bar[(kb - 1) % S], (unsigned)((kb - 1) / S) & 1u)) ok = false;
+      gather(nb);
+    }
+    cp_async_commit();
   }
   // the last commit arrives once every MMA of the CTA is done
-  if (!mbar_wait(&bar[(KB - 1) & 1], (unsigned)((KB - 1) >> 1) & 1u)) ok = false;
+  if (!mbar_wait(&bar[(KB - 1) % S], (unsigned)((KB - 1) / S) & 1u)) ok = false;
   tc_fence_after();
 #pragma unroll
   for (int c0 = 0; c0 < NOUT; c0 += 16) {
@@ -508,7 +532,7 @@ static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, in
 template <int CINP, int NOUT>
 static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
                               __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
-  const size_t sm = 1024 + 2 * (size_t)(128 * 128 + NOUT * 128);
+  const size_t sm = 1024 + kConvStages * (size_t)(128 * 128 + NOUT * 128);
   cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
   if (e) return e;
   const int P = H * W;
