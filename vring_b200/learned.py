@@ -176,3 +176,35 @@ def compare(k2d: K2d, net: UNet, f, x0=None, tol: float = 1e-10, maxit: int = 40
         out[m] = (it, rr, ms, x)
     k2d.set_preconditioner(None)
     return out
+
+
+def main(argv=None):
+    """Train the VR2D preconditioner on the GPU and write its weights:
+    python -m vring_b200.learned [--steps 800] [--batch 8] [--out path]
+    (the committed weights came from the defaults), then compare the solvers
+    on one triple of each of seeds 2, 7 and 21."""
+    import argparse
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=800)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--lr-final", type=float, default=3e-4)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args(argv)
+    k = make_solver()
+    net = make_net()
+    t0 = time.time()
+    train(net, k, a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final,
+          log=lambda s: print(s, "%.0fs" % (time.time() - t0), flush=True))
+    save_weights(net, a.out, steps=a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final)
+    for seed, t in ((2, 500), (7, 250), (21, 900)):
+        seq = RingSequence(seed, k.faces, k.nz, k.zmax)
+        f, p_prev, p = triple(k, seq, t)
+        for m, (it, rr, ms, x) in compare(k, net, f, x0=p_prev).items():
+            print("seed %d t %d %-10s %6d iterations  relres %.2e  %8.1f ms  max|x - direct| / max|direct| %.2e"
+                  % (seed, t, m, it, rr, ms, np.abs(x - p).max() / np.abs(p).max()), flush=True)
+
+
+if __name__ == "__main__":
+    main()
