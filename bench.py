@@ -280,6 +280,36 @@ def ensemble_bench(local, steps):
     return out
 
 
+def vr2d_bench():
+    """The VR2D axisymmetric pressure solve (512 x 1024, tanh-stretched radial
+    grid) on one triple of seed 2: iterations and device time of plain CG,
+    Jacobi CG, the flexible CG with the Jacobi steps alone and with the
+    committed trained network between them, each to 1e-10 from the previous
+    step's pressure; and the agreement of each answer with the direct solve."""
+    import numpy as np
+    from vring_b200 import learned as Lr
+    import os as _os
+    if not _os.path.exists(Lr.WEIGHTS):
+        return None
+    k = Lr.make_solver()
+    net = Lr.make_net()
+    Lr.load_weights(net)
+    seq = Lr.RingSequence(2, k.faces, Lr.NZ, Lr.ZMAX)
+    f, p_prev, p = Lr.triple(k, seq, 500)
+    Lr.compare(k, net, f, x0=p_prev, maxit=200)  # capture the graphs outside the timing
+    res = Lr.compare(k, net, f, x0=p_prev)
+    out = {"grid_nr_nz": [Lr.NR, Lr.NZ], "tol": 1e-10, "start": "previous step's pressure",
+           "params": net.nparams, "pool": net.pool}
+    for m, (it, rr, ms, x) in res.items():
+        out[m] = {"iterations": it, "relres": rr, "ms": ms,
+                  "max_err_vs_direct": float(np.abs(x - p).max() / np.abs(p).max())}
+    out["iterations_cg_over_learned"] = res["cg"][0] / max(1, res["learned"][0])
+    out["iterations_fcg_jacobi_over_learned"] = res["fcg_jacobi"][0] / max(1, res["learned"][0])
+    net.close()
+    k.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -493,6 +523,7 @@ def main():
     ensemble = None
     if not args.no_ensemble and not reduced and world == 1:
         ensemble = ensemble_bench(local, 5)
+    vr2d = vr2d_bench() if not reduced and world == 1 else None
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
@@ -517,7 +548,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": bench_config(world),
             "max_div_u": maxdiv, "nonfinite": nonfinite, "particles": particles, "mixed": mixed,
-            "ensemble": ensemble,
+            "ensemble": ensemble, "vr2d_krylov": vr2d,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,
