@@ -115,15 +115,16 @@ VR_API int vr_get_field(vr_ctx *ctx, int32_t field, double *host, const int64_t 
 /* Asynchronous transfers of a double-stored field (q1..q3 in either form)
  * between host memory (pinned, for the copy to overlap) and the device, on a
  * caller's stream; the calls return at once.  A get starts after the
- * context's work queued so far; a later set of the same field, and the next
- * vr_iterate / vr_substep / vr_set_field, wait for it.  A set waits for the
- * last get of that field (or the context's earlier work) and the context's
- * later work waits for the set.  The caller synchronises `stream` before it
- * touches the host buffer, and orders a get and a set that share a host
- * buffer itself (e.g. the get of step n before the set of step n+1).  With one
- * stream per direction the device->host copy of one field runs beside the
- * host->device copy of another.  VR_ERR_STATE for a field stored as float.  No
- * reference counterpart. */
+ * context's work queued so far and copies the field in 4 pieces; the next
+ * vr_iterate / vr_substep / vr_set_field waits for it, and a later set of the
+ * same field waits for it piece by piece, so a host buffer that a get fills
+ * and the next set of the same field reads is safe and the two directions
+ * overlap within the field.  Otherwise a set waits for the context's earlier
+ * work; the context's later work waits for the set.  The caller synchronises
+ * `stream` before it touches the host buffer itself.  With one stream per
+ * direction the device->host copy of one piece runs beside the host->device
+ * copy of another.  VR_ERR_STATE for a field stored as float.  No reference
+ * counterpart. */
 VR_API int vr_get_field_async(vr_ctx *ctx, int32_t field, double *host, const int64_t ext[4], void *stream);
 VR_API int vr_set_field_async(vr_ctx *ctx, int32_t field, const double *host, const int64_t ext[4], void *stream);
 /* para%irkstep, para%ntime, para%nstep (loop.F90:51-53, :65) */

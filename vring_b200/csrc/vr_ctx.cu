@@ -561,8 +561,9 @@ extern "C" int vr_destroy(vr_ctx *c) {
   if (c->ana_part) cudaFree(c->ana_part);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->xfer_ev) cudaEventDestroy(c->xfer_ev);
-  for (cudaEvent_t e : c->get_ev)
-    if (e) cudaEventDestroy(e);
+  for (auto &row : c->get_ev)
+    for (cudaEvent_t e : row)
+      if (e) cudaEventDestroy(e);
   delete[] c->h_rc;
   delete[] c->h_rm;
   delete[] c->h_da;
@@ -737,7 +738,7 @@ static int xfer_ev(vr_ctx *c, cudaEvent_t *ev) {
 int vr::wait_pending_gets(vr_ctx *c) {
   for (int f = 0; f < kXferFields; f++)
     if (c->get_pending[f]) {
-      VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->get_ev[f], 0));
+      VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->get_ev[f][kXferChunks - 1], 0));
       c->get_pending[f] = false;
     }
   return VR_OK;
@@ -752,12 +753,19 @@ extern "C" int vr_get_field_async(vr_ctx *c, int32_t f, double *host, const int6
   if (float_field(c, f) || f < 0 || f >= kXferFields)
     return set_err(c, VR_ERR_STATE, "vr_get_field_async: the field is stored as float");
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if ((rc = xfer_ev(c, &c->xfer_ev)) || (rc = xfer_ev(c, &c->get_ev[f]))) return rc;
+  if ((rc = xfer_ev(c, &c->xfer_ev))) return rc;
+  for (int q = 0; q < kXferChunks; q++)
+    if ((rc = xfer_ev(c, &c->get_ev[f][q]))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // after the context's work so far
   VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
-  VR_CUDA(c, cudaMemcpyAsync(host, p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-  VR_CUDA(c, cudaEventRecord(c->get_ev[f], s));
+  // in pieces, each with its event, so that a set of the same field can
+  // follow piece by piece (the two directions then overlap within a field)
+  for (int q = 0; q < kXferChunks; q++) {
+    const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
+    VR_CUDA(c, cudaMemcpyAsync(host + b, p + b, (e - b) * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VR_CUDA(c, cudaEventRecord(c->get_ev[f][q], s));
+  }
   c->get_pending[f] = true;
   return VR_OK;
 }
@@ -773,14 +781,17 @@ extern "C" int vr_set_field_async(vr_ctx *c, int32_t f, const double *host, cons
   VR_CUDA(c, cudaSetDevice(c->dev));
   if ((rc = xfer_ev(c, &c->xfer_ev))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (c->get_pending[f]) {
-    // the last get of this field read it after all earlier work on it
-    VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[f], 0));
-  } else {
+  const bool after_get = c->get_pending[f];
+  if (!after_get) {
     VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // the context's earlier reads come first
     VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
   }
-  VR_CUDA(c, cudaMemcpyAsync(p, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  for (int q = 0; q < kXferChunks; q++) {
+    const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
+    // the last get of this field read each piece after all earlier work on it
+    if (after_get) VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[f][q], 0));
+    VR_CUDA(c, cudaMemcpyAsync(p + b, host + b, (e - b) * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
   VR_CUDA(c, cudaEventRecord(c->xfer_ev, s));
   VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->xfer_ev, 0));  // the context's later work reads the new values
   return VR_OK;

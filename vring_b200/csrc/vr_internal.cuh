@@ -163,7 +163,7 @@ struct vr_ctx {
   // ordering of vr_get_field_async / vr_set_field_async with the context's
   // stream: a scratch event and one pending-get event per field id
   cudaEvent_t xfer_ev;
-  cudaEvent_t get_ev[32];
+  cudaEvent_t get_ev[32][4];  // [field][chunk]: a get copies a field in kXferChunks pieces
   bool get_pending[32];
 };
 
@@ -230,6 +230,7 @@ bool data_read(FILE *f, double *p, size_t n);
 // field ids the asynchronous transfers track, and the wait of the context's
 // stream for the device->host copies still pending (vr_ctx.cu)
 constexpr int kXferFields = 32;
+constexpr int kXferChunks = 4;
 int wait_pending_gets(vr_ctx *c);
 
 // the launch sequence of one fused RK substep on the context's current stream
