@@ -173,29 +173,36 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // The same 3x3 convolution on the tensor cores (BF16 in, FP32 accumulate):
-// an implicit GEMM with M = 128 output pixels per CTA (the rows of A are the
-// CTA's pixels, its columns the 9 taps x CINP input channels of their
-// neighbourhoods), N = NOUT output channels and K = 9 CINP, where CINP and NOUT
-// are cin and cout rounded up to 16.  K runs in blocks of 64 columns through
-// kConvStages shared-memory stages, both operands K-major with the 128-byte
-// swizzle: every thread issues the asynchronous 16-byte copies of its pixel's
-// row of the im2col gather (A) and of a share of the packed weights (B) for
-// the blocks ahead, zero-filling taps outside the grid, so the gathers of
-// several blocks are in flight while the tensor cores work; one thread issues
-// the four K-steps of a block and commits them to the stage's mbarrier, whose
-// completion frees the stage for the block kConvStages later.  The FP32
-// accumulator stays in tensor memory (128 lanes = pixels, NOUT columns) until
-// the epilogue, where each warp loads its 32 lanes and stores BF16.  Every
-// mbarrier wait is bounded; a wait that gives up sets bit 0 of *status, and
-// the CTA still waits (bounded) for its MMAs and frees its tensor memory.
-constexpr int kConvStages = 3;
+// an implicit GEMM over a patch of 16 (r) x 8 (z) output pixels per CTA:
+// M = 128 pixels, N = NOUT output channels and K = 9 CINP, where CINP and NOUT
+// are cin and cout rounded up to 16.  The CTA first copies its input halo
+// (18 x 10 pixels x CINP channels, zero outside the grid) into shared memory
+// with asynchronous copies, once; every K block of 64 columns (taps x
+// channels) of the im2col matrix A is then built from that halo by
+// shared-to-shared copies, so each input pixel crosses L2 about 1.4 times
+// instead of 9.  A and B (the packed weights) sit in kConvStages stages, both
+// K-major with the 128-byte swizzle; one thread issues the four K steps of a
+// block and commits them to the stage's mbarrier, whose completion frees the
+// stage for the block kConvStages later, so building one block overlaps the
+// MMAs of the previous one.  The FP32 accumulator stays in tensor memory
+// (128 lanes = pixels, NOUT columns) until the epilogue, where each warp
+// loads its 32 lanes and stores BF16.  Every mbarrier wait is bounded; a wait
+// that gives up sets bit 0 of *status, and the CTA still waits (bounded) for
+// its MMAs and frees its tensor memory.
+constexpr int kConvStages = 2;
+constexpr int kConvTR = 16, kConvTZ = 8;  // pixel patch of a CTA (r x z)
+
+template <int CINP>
+__host__ __device__ constexpr int conv_halo_bytes() {
+  return (kConvTR + 2) * (kConvTZ + 2) * CINP * 2;
+}
 
 template <int CINP, int NOUT>
 __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W, int cin,
                                                 const __nv_bfloat16 *__restrict__ wpk, int cout,
                                                 __nv_bfloat16 *__restrict__ out, unsigned *status) {
   static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
-  constexpr int S = kConvStages;
+  constexpr int S = kConvStages, HR = kConvTR + 2, HZ = kConvTZ + 2;
   constexpr int K = 9 * CINP;
   constexpr int KB = (K + 63) / 64;
   constexpr int ABYTES = 128 * 128, BBYTES = NOUT * 128, STAGE = ABYTES + BBYTES;
@@ -204,6 +211,7 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
   static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzle");
   extern __shared__ uint8_t smraw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  uint8_t *halo = sm + S * STAGE;  // [hz][hr][CINP] BF16
   __shared__ uint64_t bar[S];
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -215,75 +223,77 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
     for (int i = 0; i < S; i++) mbar_init(&bar[i], 1);
     mbar_init_fence();
   }
+  const int j0 = blockIdx.x * kConvTR, k0 = blockIdx.y * kConvTZ;
+  // the halo: pixels (j0 - 1 .. j0 + 16, k0 - 1 .. k0 + 8), chunks of 8 channels
+  constexpr int CC = CINP / 8;
+  for (int e = tid; e < HR * HZ * CC; e += 128) {
+    const int cc = e % CC, pix = e / CC, hr = pix % HR, hz = pix / HR;
+    const int j = j0 + hr - 1, k = k0 + hz - 1, ci = cc * 8;
+    const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < cin;
+    uint8_t *dst = halo + ((size_t)(hz * HR + hr) * CINP + ci) * 2;
+    const __nv_bfloat16 *src = live ? in + ((size_t)j + (size_t)H * k) * cin + ci : in;
+    if ((cin & 7) == 0) {
+      cp_async16(dst, src, live ? 16u : 0u);
+    } else {
+      __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = (live && ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
+      *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(v);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
-  const int P = H * W;
-  const int p = blockIdx.x * 128 + tid;  // this thread's row of A and of D
-  const int pj = p % H, pk = p / H;
-  const bool pin = p < P;
+  const int mr = tid % kConvTR, mz = tid / kConvTR;  // this thread's row of A and of D
   bool ok = true;
-  // the copies of K block kb into its stage (kb % S)
-  auto gather = [&](int kb) {
-    uint8_t *As = sm + (kb % S) * STAGE;
+  for (int kb = 0; kb < KB; kb++) {
+    const int s = kb % S;
+    uint8_t *As = sm + s * STAGE;
     uint8_t *Bs = As + ABYTES;
+    // the MMAs of block kb - S read this stage: wait for their commit
+    if (kb >= S && !mbar_wait(&bar[s], (unsigned)((kb - S) / S) & 1u)) ok = false;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-      const int k0 = kb * 64 + c * 8;
-      const int t = k0 / CINP, ci = k0 % CINP;  // 8 columns inside one tap (CINP % 16 == 0)
-      const int j = pj + t / 3 - 1, k = pk + t % 3 - 1;
-      const bool live = pin && k0 < K && ci < cin && j >= 0 && j < H && k >= 0 && k < W;
-      const __nv_bfloat16 *src = live ? in + ((size_t)j + (size_t)H * k) * cin + ci : in;
-      if ((cin & 7) == 0) {
-        cp_async16(As + sw128_off(tid, c), src, live ? 16u : 0u);
-      } else {
-        __align__(16) __nv_bfloat16 e[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) e[q] = (live && ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
-        *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = *reinterpret_cast<const uint4 *>(e);
+      const int kc = kb * 64 + c * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (kc < K) {
+        const int t = kc / CINP, ci = kc % CINP;  // tap t: neighbour (j + t / 3 - 1, k + t % 3 - 1)
+        v = *reinterpret_cast<const uint4 *>(halo + ((size_t)((mz + t % 3) * HR + mr + t / 3) * CINP + ci) * 2);
       }
+      *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = v;
     }
     for (int e = tid; e < NOUT * 8; e += 128) {
-      const int n = e >> 3, c = e & 7, k0 = kb * 64 + c * 8;
-      cp_async16(Bs + sw128_off(n, c), k0 < K ? wpk + (size_t)n * K + k0 : wpk, k0 < K ? 16u : 0u);
+      const int n = e >> 3, c = e & 7, kc = kb * 64 + c * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (kc < K) v = *reinterpret_cast<const uint4 *>(wpk + (size_t)n * K + kc);
+      *reinterpret_cast<uint4 *>(Bs + sw128_off(n, c)) = v;
     }
-  };
-#pragma unroll
-  for (int kb = 0; kb < S - 1; kb++) {
-    if (kb < KB) gather(kb);
-    cp_async_commit();
-  }
-  for (int kb = 0; kb < KB; kb++) {
-    cp_async_wait<S - 2>();  // this thread's copies of block kb have landed
-    fence_proxy_async();     // and, like the plain stores, are visible to the tensor cores
+    fence_proxy_async();  // the generic-proxy stores above, before the tensor cores read them
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      uint8_t *As = sm + (kb % S) * STAGE;
-      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(As + ABYTES);
+      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(Bs);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++)
         if (kb * 64 + kk * 16 < K) umma_bf16(tmem, ad + (uint64_t)(2 * kk), bd + (uint64_t)(2 * kk), IDESC, (kb | kk) ? 1u : 0u);
-      umma_commit(&bar[kb % S]);
+      umma_commit(&bar[s]);
     }
-    // block kb + S - 1 refills the stage that block kb - 1 used: wait for its MMAs
-    const int nb = kb + S - 1;
-    if (nb < KB) {
-      if (kb >= 1 && !mbar_wait(&bar[(kb - 1) % S], (unsigned)((kb - 1) / S) & 1u)) ok = false;
-      gather(nb);
-    }
-    cp_async_commit();
   }
   // the last commit arrives once every MMA of the CTA is done
   if (!mbar_wait(&bar[(KB - 1) % S], (unsigned)((KB - 1) / S) & 1u)) ok = false;
   tc_fence_after();
+  const int j = j0 + mr, k = k0 + mz;
+  const bool pin = j < H && k < W;
+  const size_t p = (size_t)j + (size_t)H * k;
 #pragma unroll
   for (int c0 = 0; c0 < NOUT; c0 += 16) {
     float v[16];
     tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
     if (pin && ok && c0 < cout) {
-      __nv_bfloat16 *dst = out + (size_t)p * cout + c0;
+      __nv_bfloat16 *dst = out + p * cout + c0;
       if (c0 + 16 <= cout) {
         __align__(16) __nv_bfloat16 b[16];
 #pragma unroll
@@ -532,11 +542,11 @@ static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, in
 template <int CINP, int NOUT>
 static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
                               __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
-  const size_t sm = 1024 + kConvStages * (size_t)(128 * 128 + NOUT * 128);
+  const size_t sm = 1024 + kConvStages * (size_t)(128 * 128 + NOUT * 128) + conv_halo_bytes<CINP>();
   cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
   if (e) return e;
-  const int P = H * W;
-  k_conv3_tc<CINP, NOUT><<<(P + 127) / 128, 128, sm, s>>>(in, H, W, cin, wpk, cout, out, status);
+  dim3 grid((H + kConvTR - 1) / kConvTR, (W + kConvTZ - 1) / kConvTZ);
+  k_conv3_tc<CINP, NOUT><<<grid, 128, sm, s>>>(in, H, W, cin, wpk, cout, out, status);
   return cudaGetLastError();
 }
 
