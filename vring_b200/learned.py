@@ -182,7 +182,9 @@ def main(argv=None):
     """Train the VR2D preconditioner on the GPU and write its weights:
     python -m vring_b200.learned [--steps 800] [--batch 8] [--out path]
     (the committed weights came from the defaults), then compare the solvers
-    on one triple of each of seeds 2, 7 and 21."""
+    on one triple of each of seeds 2, 7 and 21.  With --forward N it only
+    runs N forward passes of an untrained network on a seeded random field
+    (the case the convolution profiles are taken on) and exits."""
     import argparse
     import time
     ap = argparse.ArgumentParser()
@@ -191,7 +193,15 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--lr-final", type=float, default=3e-4)
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--forward", type=int, default=0)
     a = ap.parse_args(argv)
+    if a.forward:
+        net = make_net()
+        x = np.random.default_rng(0).standard_normal((NR, NZ))
+        for _ in range(a.forward):
+            y = net.forward(x)
+        print("forward passes %d, max|y| %.6g" % (a.forward, float(np.abs(y).max())))
+        return
     k = make_solver()
     net = make_net()
     t0 = time.time()
