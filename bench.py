@@ -207,10 +207,14 @@ def cpu_reference(steps, budget_s, q=None, part_sample=None):
     return NTH * NR * NZ / step_s / 1e6, done, os.cpu_count(), sample
 
 
-def inertial_bench(run, stream, e0, e1, calls=3):
+def particle_alone_ms(run, stream, e0, e1, pid, mode, order, calls=3):
+    """ms per iter_part call of NPART particles of class pid on the run's
+    current field, walked in cell order (order 1) or slot order (0); the
+    first, untimed call builds the order.  Returns (ms, particle class)."""
     import vring_b200 as V
     run.set_stream(stream.cuda_stream)
-    p = V.Part(run, 1, NPART, 0)
+    p = V.Part(run, pid, NPART, mode)
+    p.set_order(order)
     pu, pv = particle_state(NPART)
     p.set_state(pu, pv, None, NPART)
     del pu, pv
@@ -222,11 +226,19 @@ def inertial_bench(run, stream, e0, e1, calls=3):
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / calls
-    out = {"n": NPART, "mode": "inertial", "class": 1, "nsubdt": p.nsubdt, "ms_per_step": ms,
-           "value": NPART / (ms / 1e3), "unit": "particle-steps/s (iter_part alone, CUDA events)",
-           "substeps_per_s": NPART * p.nsubdt / (ms / 1e3), "live_after": p.counts["npart"]}
+    live = p.counts["npart"]
+    nsub = p.nsubdt
     p.close()
-    return out
+    return ms, nsub, live
+
+
+def inertial_bench(run, stream, e0, e1, calls=3):
+    ms, nsub, live = particle_alone_ms(run, stream, e0, e1, 1, 0, 1, calls)
+    ms_slot, _, _ = particle_alone_ms(run, stream, e0, e1, 1, 0, 0, calls)
+    return {"n": NPART, "mode": "inertial", "class": 1, "nsubdt": nsub, "ms_per_step": ms,
+            "value": NPART / (ms / 1e3), "unit": "particle-steps/s (iter_part alone, CUDA events)",
+            "substeps_per_s": NPART * nsub / (ms / 1e3), "live_after": live,
+            "slot_order_ms_per_step": ms_slot}
 
 
 def ensemble_bench(local, steps):
@@ -539,6 +551,10 @@ def main():
     # on the same field and cloud, timed alone over a few iter_part calls
     if not reduced:
         particles["inertial"] = inertial_bench(run, stream, e0, e1)
+        # the tracers alone, walked in cell order (the default) and in slot order
+        particles["alone_ms_per_step"] = {
+            "cell_order": particle_alone_ms(run, stream, e0, e1, PART_CLASS, PART_MODE, 1)[0],
+            "slot_order": particle_alone_ms(run, stream, e0, e1, PART_CLASS, PART_MODE, 0)[0]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",

@@ -360,3 +360,60 @@ def test_iterate_writes_dumps_every_expstp(tmp_path):
                      "trajectory_size02.dat"]
     p.attach(False)
     p.close()
+
+
+def _cloud_state(naloc, n, seed, vel_scale=1.0):
+    """u (naloc, 117) with n particles at random points of the ring domain,
+    some of them fast enough to leave it; v = 0."""
+    rng = np.random.default_rng(seed)
+    u = np.zeros((naloc, 117))
+    r = rng.uniform(0.05, 3.95, n)
+    r[n // 100:n // 50] = 4.0005  # just beyond r = rmax: removed after one substep
+    th = rng.uniform(0, 2 * np.pi, n)
+    u[:n, 0], u[:n, 1], u[:n, 2] = r * np.cos(th), r * np.sin(th), rng.uniform(0.05, 11.95, n)
+    u[:n, 3:6] = vel_scale * rng.uniform(-0.5, 0.5, (n, 3))
+    u[:n // 100, 2] = 11.97
+    u[:n // 100, 5] = 60.0 * vel_scale  # inertial: these leave through z = zmax
+    return u, np.zeros((naloc, 3))
+
+
+@pytest.mark.parametrize("mode,scale", [(1, 1.0), (0, 1.0), (1, 3e4)])
+def test_walk_order_changes_no_result(mode, scale):
+    # The main launch walks the slots grouped by cell bucket (order 1) or in
+    # slot order (order 0): every particle's update reads only its own state,
+    # so both must leave the same bits.  Covers removals, slots injected above
+    # the sorted range and, at the scaled velocity, blocks that defer to the
+    # full-iteration launch after carrying positions through some substeps.
+    import vring_b200 as V
+    from vring_b200.synthetic import ring_fields
+    nth, nr, nz = 32, 64, 128
+    naloc, n = 40000, 30000
+    runs, parts = [], []
+    for order in (0, 1):
+        gpu = V.Run(nth, nr, nz, 4.0, 12.0, 1e-3 / scale, 1000.0, 1.0, 1.0)
+        for nm, a in zip(("q1", "q2", "q3"), ring_fields(nth, nr, nz, 4.0, 12.0, noise=1e-3, seed=3)):
+            gpu.set(nm, scale * a)
+        gp = V.Part(gpu, 6, naloc, mode)
+        gp.set_order(order)
+        u, v = _cloud_state(naloc, n, seed=21, vel_scale=scale)
+        gp.set_state(u, v, nlast=n)
+        runs.append(gpu)
+        parts.append(gp)
+    for call in range(4):
+        for gp in parts:
+            gp.iter_part(1)
+        if call == 1:
+            rng = np.random.default_rng(5)
+            pts = rng.uniform(0.5, 2.5, (1000, 3))
+            for gp in parts:  # free slots first, then slots above nlast
+                for x, y, z in pts:
+                    gp.injc(x, y, z, 0.1, -0.1, 0.2)
+        sa, sb = parts[0].state(), parts[1].state()
+        assert sa[3] == sb[3]
+        np.testing.assert_array_equal(sa[2], sb[2])
+        np.testing.assert_array_equal(sa[0], sb[0])
+        np.testing.assert_array_equal(sa[1], sb[1])
+    assert sa[3]["npart"] < n + 1000  # some left the domain
+    assert sa[3]["nlast"] > n  # and some injections went above the first nlast
+    for gp in parts:
+        gp.close()

@@ -122,6 +122,7 @@ def lib():
         L.vr_part_set_inflow.argtypes = [vp, dp, C.c_uint64, i32]
         L.vr_iter_part.argtypes = [vp, i32]
         L.vr_part_attach.argtypes = [vp, i32]
+        L.vr_part_set_order.argtypes = [vp, i32]
         L.vr_part_set_state.argtypes = [vp, vp, vp, vp, i32]
         L.vr_part_get_state.argtypes = [vp, vp, vp, vp, C.POINTER(i32)]
         L.vr_part_probe.argtypes = [vp, vp, i32, vp, vp]
@@ -414,6 +415,10 @@ class Part:
 
     def iter_part(self, irk: int = 1) -> None:
         self._chk(lib().vr_iter_part(self._h, irk), "iter_part")
+
+    def set_order(self, order: int) -> None:
+        """1: walk the slots grouped by cell (default); 0: slot order."""
+        self._chk(lib().vr_part_set_order(self._h, order), "part_set_order")
 
     def inlt(self, r0: float, rng_state: int):
         """inlt_part (part_tools.F90:95-142); returns (injected, new rng state)."""

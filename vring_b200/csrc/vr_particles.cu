@@ -47,6 +47,11 @@ struct vr_part {
   int *isfre, *gone;    // gone[ip-1] = substep serial at removal, -1 alive
   int *d_nremoved;  // [0] removals since the host last read them, [1..2] deferred counts
   int *d_defer;     // slots deferred to the full least-squares iteration this substep
+  // walk order of the main launch: d_perm[0..nsorted) holds the slots
+  // 1..nsorted grouped by the cell bucket d_key[slot-1] they were in at the
+  // last substep of the previous call (order 1), or nsorted = 0 (slot order)
+  int *d_key, *d_perm, *d_bcnt;
+  int nbucket, nsorted, order;
   // host bookkeeping (part_tools.F90 type part)
   int npart, nlast, nfree, nids;
   std::vector<int> ifree, h_isfre;
@@ -512,22 +517,38 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 // the whole block) when the main launch leaves the block to the FIX launch,
 // else kPartRemoved for a particle that left the domain, else 0.
 constexpr int kPartRemoved = 1, kPartDeferred = 2;
+//
+// The main launch (FIX false) carries the positions from one substep to the
+// next in S.pos and writes the position, the tracer velocity and the fluid
+// velocity with its derivatives (rows 1-6 and 79-117) to u at its last substep
+// only (first/last: substep 0 / nsub-1 of the call); the values are the ones
+// the reference leaves after the call.  A deferring block writes the
+// positions it has reached first.  The inertial ODE rows 4-78 are written at
+// every substep.  At the last substep warp 0 records the particle's cell
+// bucket in key[] for the next call's walk order.
 template <class R, bool FIX>
 __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__restrict__ q1,
                                             const double *__restrict__ q2, const double *__restrict__ q3,
                                             double *__restrict__ u, double *__restrict__ v,
                                             int *__restrict__ isfre, int *__restrict__ gone, int naloc, int ip,
                                             bool live, int mode, double inv_st, double partdt, int serial,
-                                            int *nremoved, PartShared<R> &S) {
+                                            int *nremoved, PartShared<R> &S, bool first = true, bool last = true,
+                                            int *__restrict__ key = nullptr) {
   constexpr bool DBL = std::is_same<R, double>::value;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   double r = 0.0, theta = 0.0, sn = 0.0, cs = 0.0, ir1 = 0.0, ir2 = 0.0;
   bool need = false;
+  const bool carry = !FIX && !first;  // positions from the previous substep in S.pos
   if (live) {
-    const double px = u[PUo(ip, 1)], py = u[PUo(ip, 2)], pz = u[PUo(ip, 3)];
+    const double px = carry ? S.pos[0][p] : u[PUo(ip, 1)], py = carry ? S.pos[1][p] : u[PUo(ip, 2)],
+                 pz = carry ? S.pos[2][p] : u[PUo(ip, 3)];
     int cell[3];
     part_component<R, FIX>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs,
                            ir1, ir2, need);
+    if (!FIX && last && w == 0 && key) {
+      const int jb = ((P.g.nr + 2) >> 2) + 1;
+      key[ip - 1] = cell[2] * jb + (cell[1] >> 2);
+    }
     if (mode != 1) {
 #pragma unroll
       for (int j = 0; j < 3; j++) S.jac[w + 3 * j][p] = u[PUo(ip, 7 + w + 3 * j)];
@@ -537,8 +558,12 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
   }
   if (DBL && !FIX) {
     // a block with any particle that needs the full fit leaves all of its
-    // particles unchanged from here on: the FIX launch advances them
-    if (__syncthreads_or(need)) return kPartDeferred;
+    // particles unchanged from here on: the FIX launch advances them from
+    // the positions reached so far
+    if (__syncthreads_or(need)) {
+      if (live && carry) u[PUo(ip, 1 + w)] = S.pos[w][p];
+      return kPartDeferred;
+    }
   } else {
     __syncthreads();
   }
@@ -555,17 +580,20 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
 #pragma unroll
       for (int l = 0; l < 3; l++) ddvel[j][l] = ddvr[j][l];
     }
-    pw = u[PUo(ip, 1 + w)];
+    const bool store = FIX || last;  // rows written at this substep
+    pw = carry ? S.pos[w][p] : u[PUo(ip, 1 + w)];
     if (mode == 1) {  // tracer: dx/dt = u(x)
       pw = pw + vel * partdt;
-      u[PUo(ip, 1 + w)] = pw;
-      u[PUo(ip, 4 + w)] = vel;
+      if (store) {
+        u[PUo(ip, 1 + w)] = pw;
+        u[PUo(ip, 4 + w)] = vel;
+      }
     } else {
       // Stokes drag on position, velocity, Jacobian and Hessian
       // (part_tools.F90:836-870), explicit Euler (:926-930), row w
       const double pv = u[PUo(ip, 4 + w)];
       pw = pw + pv * partdt;
-      u[PUo(ip, 1 + w)] = pw;
+      if (store) u[PUo(ip, 1 + w)] = pw;
       u[PUo(ip, 4 + w)] = pv + (inv_st * (vel - pv)) * partdt;
 #pragma unroll
       for (int j = 0; j < 3; j++) {
@@ -594,13 +622,15 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
         }
     }
     // fluid velocity and its derivatives at the particle (part_tools.F90:940-958)
-    u[PUo(ip, 79 + w)] = vel;
+    if (store) {
+      u[PUo(ip, 79 + w)] = vel;
 #pragma unroll
-    for (int j = 0; j < 3; j++) u[PUo(ip, 82 + w + 3 * j)] = dvel[j];
+      for (int j = 0; j < 3; j++) u[PUo(ip, 82 + w + 3 * j)] = dvel[j];
 #pragma unroll
-    for (int k = 0; k < 3; k++)
+      for (int k = 0; k < 3; k++)
 #pragma unroll
-      for (int j = 0; j < 3; j++) u[PUo(ip, 91 + w + 3 * j + 9 * k)] = ddvel[j][k];
+        for (int j = 0; j < 3; j++) u[PUo(ip, 91 + w + 3 * j + 9 * k)] = ddvel[j][k];
+    }
     S.pos[w][p] = pw;
   }
   __syncthreads();
@@ -618,6 +648,7 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
         isfre[ip - 1] = 1;
         gone[ip - 1] = serial;
         atomicAdd(nremoved, 1);
+        if (key) key[ip - 1] = (P.g.nz + 2) * (((P.g.nr + 2) >> 2) + 1);  // empty slots sort last
       }
     }
   }
@@ -633,17 +664,22 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
                                                   double *__restrict__ u, double *__restrict__ v,
                                                   int *__restrict__ isfre, int *__restrict__ gone, int naloc,
                                                   int nlast, int mode, double inv_st, double partdt, int nsub,
-                                                  int serial0, int par, int *nremoved, int *__restrict__ defer) {
+                                                  int serial0, int par, int *nremoved, int *__restrict__ defer,
+                                                  const int *__restrict__ perm, int nsorted, int *__restrict__ key) {
   __shared__ PartShared<R> S;
   const int p = threadIdx.x & 31, w = threadIdx.x >> 5;
   int *const defer_n = nremoved + 1;
   if constexpr (!FIX) {
-    const int ip = 1 + blockIdx.x * kPartPerBlock + p;
-    bool live = ip <= nlast && isfre[ip - 1] == 0;
+    // position t of the walk: the sorted slots first, then any slot above
+    // the sorted range in slot order (the grid covers max(nlast, nsorted))
+    const int t = blockIdx.x * kPartPerBlock + p;
+    const int ip = t < nsorted ? perm[t] : t + 1;
+    bool live = ip >= 1 && ip <= nlast && isfre[ip - 1] == 0;
+    if (w == 0 && !live && ip >= 1 && ip <= nlast) key[ip - 1] = (P.g.nz + 2) * (((P.g.nr + 2) >> 2) + 1);
 #pragma unroll 1
     for (int s = 0; s < nsub; s++) {
       const int st = part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st,
-                                            partdt, serial0 + s, nremoved, S);
+                                            partdt, serial0 + s, nremoved, S, s == 0, s == nsub - 1, key);
       if (st == kPartDeferred) {  // the same in every thread of the block
         if (w == 0 && live) {
           const int k = atomicAdd(defer_n + par, 1);
@@ -669,6 +705,73 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
       }
       __syncthreads();  // S is reused by the next group
     }
+  }
+}
+
+// ---- walk order: slots grouped by cell bucket (a counting sort) ----------
+// A bucket is four radial rows of one z plane, all theta: the stencils of the
+// particles of one block then share their rows of q1..q3 in L1, and the
+// blocks resident at a time cover a few neighbouring z planes.  The order
+// changes no result (every particle's update reads only its own state); it
+// is rebuilt after every call from the buckets the particles were in.
+__global__ void k_bucket_count(const int *__restrict__ key, int n, int nb, int *__restrict__ cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int b = min(max(key[t], 0), nb);
+    atomicAdd(cnt + b, 1);
+  }
+}
+
+// exclusive scan of cnt[0..n) in place, one block of 1024 threads
+__global__ void __launch_bounds__(1024) k_bucket_scan(int *__restrict__ cnt, int n) {
+  __shared__ int warp_sum[32];
+  __shared__ int carry;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024 * 8) {
+    int v[8], sum = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int e = base + tid * 8 + i;
+      v[i] = e < n ? cnt[e] : 0;
+      sum += v[i];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int o = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += o;
+    }
+    if (lane == 31) warp_sum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int ws = warp_sum[lane], wi = ws;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, wi, d);
+        if (lane >= d) wi += o;
+      }
+      warp_sum[lane] = wi - ws;  // exclusive over warps
+    }
+    __syncthreads();
+    int run = carry + warp_sum[wid] + incl - sum;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int e = base + tid * 8 + i;
+      if (e < n) cnt[e] = run;
+      run += v[i];
+    }
+    __syncthreads();  // every thread has read carry and warp_sum
+    if (tid == 1023) carry = run;
+    __syncthreads();
+  }
+}
+
+__global__ void k_bucket_scatter(const int *__restrict__ key, int n, int nb, int *__restrict__ off,
+                                 int *__restrict__ perm) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int b = min(max(key[t], 0), nb);
+    perm[atomicAdd(off + b, 1)] = t + 1;
   }
 }
 
@@ -862,6 +965,12 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
             cudaMalloc(&p->gone, naloc * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&p->d_nremoved, 3 * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&p->d_defer, naloc * sizeof(int)) == cudaSuccess;
+  p->nbucket = (c->geo.nz + 2) * (((c->geo.nr + 2) >> 2) + 1);
+  ok = ok && cudaMalloc(&p->d_key, naloc * sizeof(int)) == cudaSuccess &&
+       cudaMalloc(&p->d_perm, naloc * sizeof(int)) == cudaSuccess &&
+       cudaMalloc(&p->d_bcnt, (p->nbucket + 1) * sizeof(int)) == cudaSuccess;
+  p->nsorted = 0;
+  p->order = 1;
   if (!ok) {
     vr_part_destroy(p);
     return set_err(c, VR_ERR_OOM, "particle arrays");
@@ -871,6 +980,7 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
   cudaMemset(p->isfre, 0, naloc * sizeof(int));
   cudaMemset(p->gone, 0xff, naloc * sizeof(int));
   cudaMemset(p->d_nremoved, 0, 3 * sizeof(int));
+  cudaMemset(p->d_key, 0, naloc * sizeof(int));
   p->ifree.assign(naloc + 2, 0);
   p->h_isfre.assign(naloc + 1, 0);
   p->inflow.assign(c->geo.nr + 2, 0.0);
@@ -895,6 +1005,9 @@ extern "C" int vr_part_destroy(vr_part *p) {
   cudaFree(p->gone);
   cudaFree(p->d_nremoved);
   cudaFree(p->d_defer);
+  cudaFree(p->d_key);
+  cudaFree(p->d_perm);
+  cudaFree(p->d_bcnt);
   if (p->d_batch) cudaFree(p->d_batch);
   delete p;
   return VR_OK;
@@ -1124,7 +1237,9 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
   double partdt = c->d.dt / (double)(float)p->nsubdt;
   double inv_st = 1.0 / p->st;
   if (p->nlast <= 0) return VR_OK;
-  const int nb = (p->nlast + kPartPerBlock - 1) / kPartPerBlock, serial0 = p->serial, par = p->ncall & 1;
+  const int nsorted = std::min(p->nsorted, p->naloc);
+  const int nwalk = std::max(p->nlast, nsorted);
+  const int nb = (nwalk + kPartPerBlock - 1) / kPartPerBlock, serial0 = p->serial, par = p->ncall & 1;
   p->serial += p->nsubdt;
   p->ncall++;
   {
@@ -1132,11 +1247,13 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
     if (c->mixed)
       k_iter_part<float, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone,
                                                        p->naloc, p->nlast, p->mode, inv_st, partdt, p->nsubdt,
-                                                       serial0, par, p->d_nremoved, p->d_defer);
+                                                       serial0, par, p->d_nremoved, p->d_defer, p->d_perm,
+                                                       nsorted, p->d_key);
     else
       k_iter_part<double, false><<<nb, 96, 0, stream>>>(P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre,
                                                         p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
-                                                        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer);
+                                                        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer,
+                                                        p->d_perm, nsorted, p->d_key);
   }
   cudaError_t e = cudaGetLastError();
   if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
@@ -1144,10 +1261,34 @@ int vr::vr_part_enqueue(vr_part *p, cudaStream_t stream) {
     LaunchScope ls(c, PK_PART, stream);
     k_iter_part<double, true><<<std::min(nb, 2 * c->nsm), 96, 0, stream>>>(
         P, c->q[0], c->q[1], c->q[2], p->u, p->v, p->isfre, p->gone, p->naloc, p->nlast, p->mode, inv_st, partdt,
-        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer);
+        p->nsubdt, serial0, par, p->d_nremoved, p->d_defer, p->d_perm, nsorted, p->d_key);
     e = cudaGetLastError();
     if (e) return set_err(c, VR_ERR_CUDA, std::string("k_iter_part: ") + cudaGetErrorString(e));
   }
+  // the next call's walk order: slots 1..nlast by the bucket recorded above
+  // (slots deferred or injected since keep an older bucket; any order is
+  // correct, this one only keeps the gathers of a block close together)
+  if (p->order) {
+    LaunchScope ls(c, PK_PART, stream);
+    const int n = p->nlast, g = std::min((n + 255) / 256, 4 * c->nsm);
+    VR_CUDA(c, cudaMemsetAsync(p->d_bcnt, 0, sizeof(int) * (p->nbucket + 1), stream));
+    k_bucket_count<<<g, 256, 0, stream>>>(p->d_key, n, p->nbucket, p->d_bcnt);
+    k_bucket_scan<<<1, 1024, 0, stream>>>(p->d_bcnt, p->nbucket + 1);
+    k_bucket_scatter<<<g, 256, 0, stream>>>(p->d_key, n, p->nbucket, p->d_bcnt, p->d_perm);
+    c->nlaunch += 2;  // three kernels in this scope
+    e = cudaGetLastError();
+    if (e) return set_err(c, VR_ERR_CUDA, std::string("walk order: ") + cudaGetErrorString(e));
+    p->nsorted = n;
+  } else {
+    p->nsorted = 0;
+  }
+  return VR_OK;
+}
+
+extern "C" int vr_part_set_order(vr_part *p, int32_t order) {
+  if (!p || order < 0 || order > 1) return VR_ERR_ARG;
+  p->order = order;
+  if (!order) p->nsorted = 0;
   return VR_OK;
 }
 
@@ -1181,6 +1322,7 @@ extern "C" int vr_part_set_state(vr_part *p, const double *u, const double *v, c
   VR_CUDA(c, cudaMemset(p->gone, 0xff, sizeof(int) * p->naloc));
   VR_CUDA(c, cudaMemset(p->d_nremoved, 0, sizeof(int)));
   p->nlast = nlast;
+  p->nsorted = 0;
   p->nfree = 0;
   p->npart = 0;
   for (int i = 0; i < p->naloc; i++) {
@@ -1317,6 +1459,7 @@ extern "C" int vr_part_restart_load(vr_part *p, const char *path) {
   if (!ok) return set_err(c, VR_ERR_IO, std::string("particle restart: bad file ") + path);
   p->npart = h.npart;
   p->nlast = h.nlast;
+  p->nsorted = 0;
   p->nfree = h.nfree;
   p->nids = h.nids;
   p->serial = h.serial;
