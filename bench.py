@@ -233,12 +233,12 @@ def particle_alone_ms(run, stream, e0, e1, pid, mode, order, calls=3):
 
 
 def inertial_bench(run, stream, e0, e1, calls=3):
-    ms, nsub, live = particle_alone_ms(run, stream, e0, e1, 1, 0, 1, calls)
-    ms_slot, _, _ = particle_alone_ms(run, stream, e0, e1, 1, 0, 0, calls)
+    ms, nsub, live = particle_alone_ms(run, stream, e0, e1, 1, 0, 0, calls)
+    ms_cell, _, _ = particle_alone_ms(run, stream, e0, e1, 1, 0, 1, calls)
     return {"n": NPART, "mode": "inertial", "class": 1, "nsubdt": nsub, "ms_per_step": ms,
             "value": NPART / (ms / 1e3), "unit": "particle-steps/s (iter_part alone, CUDA events)",
             "substeps_per_s": NPART * nsub / (ms / 1e3), "live_after": live,
-            "slot_order_ms_per_step": ms_slot}
+            "cell_order_ms_per_step": ms_cell}
 
 
 def ensemble_bench(local, steps):
@@ -551,7 +551,7 @@ def main():
     # on the same field and cloud, timed alone over a few iter_part calls
     if not reduced:
         particles["inertial"] = inertial_bench(run, stream, e0, e1)
-        # the tracers alone, walked in cell order (the default) and in slot order
+        # the tracers alone, walked in slot order (the default) and in cell order
         particles["alone_ms_per_step"] = {
             "cell_order": particle_alone_ms(run, stream, e0, e1, PART_CLASS, PART_MODE, 1)[0],
             "slot_order": particle_alone_ms(run, stream, e0, e1, PART_CLASS, PART_MODE, 0)[0]}

@@ -253,10 +253,11 @@ VR_API int vr_part_set_inflow(vr_part *part, double r0, uint64_t seed, int32_t o
  * that reads or changes it. */
 VR_API int vr_iter_part(vr_part *part, int32_t irkstep);
 /* The order in which the device walks the slots (no reference counterpart;
- * the results and the state layout are the same either way): 1 (default)
- * groups the slots by the cell each particle was in at the end of the
- * previous call, so neighbouring particles share their stencil rows in
- * cache; 0 walks them in slot order. */
+ * the results and the state layout are the same either way): 0 (default)
+ * walks them in slot order; 1 groups the slots by the cell each particle was
+ * in at the end of the previous call, so neighbouring particles share their
+ * stencil rows in cache but every state row a block reads or writes
+ * scatters over 32 sectors (slower at 1,048,576 particles). */
 VR_API int vr_part_set_order(vr_part *part, int32_t order);
 /* on != 0: vr_iterate advances this class once per time step */
 VR_API int vr_part_attach(vr_part *part, int32_t on);

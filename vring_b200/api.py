@@ -417,7 +417,7 @@ class Part:
         self._chk(lib().vr_iter_part(self._h, irk), "iter_part")
 
     def set_order(self, order: int) -> None:
-        """1: walk the slots grouped by cell (default); 0: slot order."""
+        """0: walk the slots in slot order (default); 1: grouped by cell."""
         self._chk(lib().vr_part_set_order(self._h, order), "part_set_order")
 
     def inlt(self, r0: float, rng_state: int):

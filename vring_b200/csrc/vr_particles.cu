@@ -47,9 +47,14 @@ struct vr_part {
   int *isfre, *gone;    // gone[ip-1] = substep serial at removal, -1 alive
   int *d_nremoved;  // [0] removals since the host last read them, [1..2] deferred counts
   int *d_defer;     // slots deferred to the full least-squares iteration this substep
-  // walk order of the main launch: d_perm[0..nsorted) holds the slots
+  // walk order of the main launch: nsorted = 0 walks the slots in order
+  // (order 0, the default); with order 1 d_perm[0..nsorted) holds the slots
   // 1..nsorted grouped by the cell bucket d_key[slot-1] they were in at the
-  // last substep of the previous call (order 1), or nsorted = 0 (slot order)
+  // last substep of the previous call.  Measured at 1,048,576 particles the
+  // grouped walk is slower (tracers 2.50 against 1.78 ms per call, inertial
+  // 82.6 against 10.0): in the slot-major state u(naloc, 117) a block's rows
+  // then scatter over 32 sectors each, which costs more than the gathers of
+  // the stencils save.
   int *d_key, *d_perm, *d_bcnt;
   int nbucket, nsorted, order;
   // host bookkeeping (part_tools.F90 type part)
@@ -713,7 +718,9 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
 // particles of one block then share their rows of q1..q3 in L1, and the
 // blocks resident at a time cover a few neighbouring z planes.  The order
 // changes no result (every particle's update reads only its own state); it
-// is rebuilt after every call from the buckets the particles were in.
+// is rebuilt after every call from the buckets the particles were in.  Off
+// by default (vr_part_set_order): the scattered state rows cost more than the
+// shared stencil rows save.
 __global__ void k_bucket_count(const int *__restrict__ key, int n, int nb, int *__restrict__ cnt) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int b = min(max(key[t], 0), nb);
@@ -970,7 +977,7 @@ extern "C" int vr_part_create(vr_ctx *c, int32_t id, int32_t naloc, int32_t mode
        cudaMalloc(&p->d_perm, naloc * sizeof(int)) == cudaSuccess &&
        cudaMalloc(&p->d_bcnt, (p->nbucket + 1) * sizeof(int)) == cudaSuccess;
   p->nsorted = 0;
-  p->order = 1;
+  p->order = 0;
   if (!ok) {
     vr_part_destroy(p);
     return set_err(c, VR_ERR_OOM, "particle arrays");
