@@ -114,17 +114,19 @@ VR_API int vr_set_field(vr_ctx *ctx, int32_t field, const double *host, const in
 VR_API int vr_get_field(vr_ctx *ctx, int32_t field, double *host, const int64_t ext[4]);
 /* Asynchronous transfers of a double-stored field (q1..q3 in either form)
  * between host memory (pinned, for the copy to overlap) and the device, on a
- * caller's stream; the calls return at once.  A get starts after the
- * context's work queued so far and copies the field in 4 pieces; the next
- * vr_iterate / vr_substep / vr_set_field waits for it, and a later set of the
- * same field waits for it piece by piece, so a host buffer that a get fills
- * and the next set of the same field reads is safe and the two directions
- * overlap within the field.  Otherwise a set waits for the context's earlier
- * work; the context's later work waits for the set.  The caller synchronises
- * `stream` before it touches the host buffer itself.  With one stream per
- * direction the device->host copy of one piece runs beside the host->device
- * copy of another.  VR_ERR_STATE for a field stored as float.  No reference
- * counterpart. */
+ * caller's stream; the calls return at once.  Both go through device staging
+ * buffers of the field's size (allocated on the field's first transfer): a
+ * get copies the field into its buffer at this point of the context's stream
+ * and the device->host copy runs from there on `stream`; a set copies the
+ * host values into its buffer on `stream` and the context's stream moves them
+ * into the field at this point.  So the host copies of one step overlap the
+ * computation of the neighbouring steps, and the fields read and written are
+ * those of the stream order of the calls.  Each direction copies 4 pieces; a
+ * set whose host memory overlaps the host memory of an earlier get waits for
+ * that get (piece by piece for the same field and buffer), so a buffer that a
+ * get fills and the next set reads is safe.  The caller synchronises `stream`
+ * before it touches the host buffer itself.  VR_ERR_STATE for a field stored
+ * as float.  No reference counterpart. */
 VR_API int vr_get_field_async(vr_ctx *ctx, int32_t field, double *host, const int64_t ext[4], void *stream);
 VR_API int vr_set_field_async(vr_ctx *ctx, int32_t field, const double *host, const int64_t ext[4], void *stream);
 /* para%irkstep, para%ntime, para%nstep (loop.F90:51-53, :65) */

@@ -561,9 +561,15 @@ extern "C" int vr_destroy(vr_ctx *c) {
   if (c->ana_part) cudaFree(c->ana_part);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->xfer_ev) cudaEventDestroy(c->xfer_ev);
-  for (auto &row : c->get_ev)
-    for (cudaEvent_t e : row)
+  for (int f = 0; f < kXferFields; f++) {
+    for (int q = 0; q < kXferChunks; q++)
+      for (cudaEvent_t e : {c->in_ready[f][q], c->out_ready[f][q], c->get_ev[f][q]})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {c->in_free[f], c->out_free[f]})
       if (e) cudaEventDestroy(e);
+    if (c->stage_in[f]) cudaFree(c->stage_in[f]);
+    if (c->stage_out[f]) cudaFree(c->stage_out[f]);
+  }
   delete[] c->h_rc;
   delete[] c->h_rm;
   delete[] c->h_da;
@@ -694,7 +700,6 @@ extern "C" int vr_set_field(vr_ctx *c, int32_t f, const double *host, const int6
   int rc = check_ext(c, f, ext, &p, &n);
   if (rc) return rc;
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if ((rc = wait_pending_gets(c))) return rc;
   if (float_field(c, f)) {
     std::vector<float> t(host, host + n);
     VR_CUDA(c, cudaMemcpyAsync(p, t.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
@@ -725,22 +730,27 @@ extern "C" int vr_get_field(vr_ctx *c, int32_t f, double *host, const int64_t ex
   return VR_OK;
 }
 
-// Asynchronous transfers.  A get leaves a pending event per field: a later set
-// of the same field waits for it (the device field may be overwritten once it
-// has been read), and the context's next fused step or substep waits for all
-// of them before its kernels write the fields again.  A set makes the
-// context's stream wait for its copy at once (everything after reads it).
+// Asynchronous transfers through device staging buffers.  A get copies the
+// field into its stage_out buffer on the context's stream, in stream order,
+// and the device->host copy leaves from there on the caller's stream; a set
+// lands in stage_in on the caller's stream and the context's stream copies it
+// into the field at the point of the call.  The host copies thus never touch
+// a field the context's kernels use: a set for the next step can run while
+// the current step computes, and the get of a step while the next one does.
+// Each direction copies 4 pieces with an event each; a set whose host memory
+// overlaps the host memory of a pending get waits for that get (piece by
+// piece when it is the same field and buffer), so a buffer that a get fills
+// and the next set reads is safe and the two directions overlap within it.
 static int xfer_ev(vr_ctx *c, cudaEvent_t *ev) {
   if (!*ev) VR_CUDA(c, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
   return VR_OK;
 }
 
-int vr::wait_pending_gets(vr_ctx *c) {
-  for (int f = 0; f < kXferFields; f++)
-    if (c->get_pending[f]) {
-      VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->get_ev[f][kXferChunks - 1], 0));
-      c->get_pending[f] = false;
-    }
+static int stage_buf(vr_ctx *c, double **buf, size_t n) {
+  if (!*buf && cudaMalloc(buf, n * sizeof(double)) != cudaSuccess) {
+    *buf = nullptr;
+    return set_err(c, VR_ERR_OOM, "transfer staging buffer");
+  }
   return VR_OK;
 }
 
@@ -753,20 +763,32 @@ extern "C" int vr_get_field_async(vr_ctx *c, int32_t f, double *host, const int6
   if (float_field(c, f) || f < 0 || f >= kXferFields)
     return set_err(c, VR_ERR_STATE, "vr_get_field_async: the field is stored as float");
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if ((rc = xfer_ev(c, &c->xfer_ev))) return rc;
-  for (int q = 0; q < kXferChunks; q++)
+  if ((rc = stage_buf(c, &c->stage_out[f], n))) return rc;
+  if ((rc = xfer_ev(c, &c->out_free[f]))) return rc;
+  for (int q = 0; q < kXferChunks; q++) {
+    if ((rc = xfer_ev(c, &c->out_ready[f][q]))) return rc;
     if ((rc = xfer_ev(c, &c->get_ev[f][q]))) return rc;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // after the context's work so far
-  VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
-  // in pieces, each with its event, so that a set of the same field can
-  // follow piece by piece (the two directions then overlap within a field)
+  double *st = c->stage_out[f];
+  // the previous get of this field has left the staging buffer
+  if (c->out_used[f]) VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->out_free[f], 0));
   for (int q = 0; q < kXferChunks; q++) {
     const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
-    VR_CUDA(c, cudaMemcpyAsync(host + b, p + b, (e - b) * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VR_CUDA(c, cudaMemcpyAsync(st + b, p + b, (e - b) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    VR_CUDA(c, cudaEventRecord(c->out_ready[f][q], c->stream));
+  }
+  for (int q = 0; q < kXferChunks; q++) {
+    const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
+    VR_CUDA(c, cudaStreamWaitEvent(s, c->out_ready[f][q], 0));
+    VR_CUDA(c, cudaMemcpyAsync(host + b, st + b, (e - b) * sizeof(double), cudaMemcpyDeviceToHost, s));
     VR_CUDA(c, cudaEventRecord(c->get_ev[f][q], s));
   }
+  VR_CUDA(c, cudaEventRecord(c->out_free[f], s));
+  c->out_used[f] = true;
   c->get_pending[f] = true;
+  c->get_host[f] = reinterpret_cast<const char *>(host);
+  c->get_bytes[f] = n * sizeof(double);
   return VR_OK;
 }
 
@@ -779,21 +801,40 @@ extern "C" int vr_set_field_async(vr_ctx *c, int32_t f, const double *host, cons
   if (float_field(c, f) || f < 0 || f >= kXferFields)
     return set_err(c, VR_ERR_STATE, "vr_set_field_async: the field is stored as float");
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if ((rc = xfer_ev(c, &c->xfer_ev))) return rc;
+  if ((rc = stage_buf(c, &c->stage_in[f], n))) return rc;
+  if ((rc = xfer_ev(c, &c->in_free[f]))) return rc;
+  for (int q = 0; q < kXferChunks; q++)
+    if ((rc = xfer_ev(c, &c->in_ready[f][q]))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool after_get = c->get_pending[f];
-  if (!after_get) {
-    VR_CUDA(c, cudaEventRecord(c->xfer_ev, c->stream));  // the context's earlier reads come first
-    VR_CUDA(c, cudaStreamWaitEvent(s, c->xfer_ev, 0));
+  double *st = c->stage_in[f];
+  // the context has copied the previous set of this field out of stage_in
+  if (c->in_used[f]) VR_CUDA(c, cudaStreamWaitEvent(s, c->in_free[f], 0));
+  // pending gets that write host memory this set reads
+  const char *h0 = reinterpret_cast<const char *>(host), *h1 = h0 + n * sizeof(double);
+  bool piecewise = false;
+  for (int g = 0; g < kXferFields; g++) {
+    if (!c->get_pending[g]) continue;
+    const char *g0 = c->get_host[g], *g1 = g0 + c->get_bytes[g];
+    if (g1 <= h0 || h1 <= g0) continue;
+    if (g == f && g0 == h0)
+      piecewise = true;
+    else
+      VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[g][kXferChunks - 1], 0));
   }
   for (int q = 0; q < kXferChunks; q++) {
     const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
-    // the last get of this field read each piece after all earlier work on it
-    if (after_get) VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[f][q], 0));
-    VR_CUDA(c, cudaMemcpyAsync(p + b, host + b, (e - b) * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (piecewise) VR_CUDA(c, cudaStreamWaitEvent(s, c->get_ev[f][q], 0));
+    VR_CUDA(c, cudaMemcpyAsync(st + b, host + b, (e - b) * sizeof(double), cudaMemcpyHostToDevice, s));
+    VR_CUDA(c, cudaEventRecord(c->in_ready[f][q], s));
   }
-  VR_CUDA(c, cudaEventRecord(c->xfer_ev, s));
-  VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->xfer_ev, 0));  // the context's later work reads the new values
+  // into the field at this point of the context's stream, piece by piece
+  for (int q = 0; q < kXferChunks; q++) {
+    const size_t b = n * q / kXferChunks, e = n * (q + 1) / kXferChunks;
+    VR_CUDA(c, cudaStreamWaitEvent(c->stream, c->in_ready[f][q], 0));
+    VR_CUDA(c, cudaMemcpyAsync(p + b, st + b, (e - b) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  VR_CUDA(c, cudaEventRecord(c->in_free[f], c->stream));
+  c->in_used[f] = true;
   return VR_OK;
 }
 
@@ -1019,14 +1060,12 @@ extern "C" int vr_set_graphs(vr_ctx *c, int32_t on) {
 extern "C" int vr_substep(vr_ctx *c, int32_t irk) {
   if (!c || irk < 1 || irk > 3) return VR_ERR_ARG;
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if (int rc = wait_pending_gets(c)) return rc;
   return run_substep(c, irk);
 }
 
 extern "C" int vr_iterate(vr_ctx *c, int32_t nsteps) {
   if (!c || nsteps < 0) return VR_ERR_ARG;
   VR_CUDA(c, cudaSetDevice(c->dev));
-  if (int rc = wait_pending_gets(c)) return rc;
   for (int s = 0; s < nsteps; s++) {
     c->ntime = c->d.dt + c->ntime;
     // loop.F90:54-58: inflow injection every inj = 10 steps

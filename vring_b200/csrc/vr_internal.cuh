@@ -160,11 +160,18 @@ struct vr_ctx {
   // r: 0 TMA 16-line tiles, 1 TMA 8-line tiles, 2 register chunks;
   // z: 0 TMA 8-line tiles, 1 TMA 16-line tiles, 2 register chunks
   int tune_r, tune_z;
-  // ordering of vr_get_field_async / vr_set_field_async with the context's
-  // stream: a scratch event and one pending-get event per field id
-  cudaEvent_t xfer_ev;
-  cudaEvent_t get_ev[32][4];  // [field][chunk]: a get copies a field in kXferChunks pieces
-  bool get_pending[32];
+  // vr_get_field_async / vr_set_field_async, per field id (32) and piece
+  // (kXferChunks = 4): host copies go through device staging buffers, so they
+  // never touch the field while the context's kernels run
+  cudaEvent_t xfer_ev;               // scratch
+  double *stage_in[32], *stage_out[32];  // allocated on a field's first transfer
+  cudaEvent_t in_ready[32][4];      // host->device copy of a piece landed in stage_in
+  cudaEvent_t out_ready[32][4];     // the field's piece copied into stage_out
+  cudaEvent_t get_ev[32][4];        // device->host copy of a piece done
+  cudaEvent_t in_free[32], out_free[32];  // the staging buffer may be refilled
+  bool in_used[32], out_used[32], get_pending[32];
+  const char *get_host[32];         // host range of the field's latest get
+  size_t get_bytes[32];
 };
 
 namespace vr {
@@ -227,11 +234,9 @@ bool rec_read(FILE *f, void *buf, size_t n);
 bool data_write(FILE *f, const double *p, size_t n);
 bool data_read(FILE *f, double *p, size_t n);
 
-// field ids the asynchronous transfers track, and the wait of the context's
-// stream for the device->host copies still pending (vr_ctx.cu)
+// field ids and pieces of the asynchronous transfers (vr_ctx.cu)
 constexpr int kXferFields = 32;
 constexpr int kXferChunks = 4;
-int wait_pending_gets(vr_ctx *c);
 
 // the launch sequence of one fused RK substep on the context's current stream
 // (vr_ctx.cu); no graph, no host synchronisation
