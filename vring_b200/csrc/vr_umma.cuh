@@ -32,6 +32,15 @@ __device__ __forceinline__ uint64_t umma_desc_k128(const void *smem_tile) {
   return a | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
+// Descriptor of a K-major tile without swizzle: core matrices of 8 rows x 16
+// bytes (8 BF16 of K), the 8 rows at consecutive 16-byte addresses; lbo is the
+// byte distance between core matrices adjacent in K, sbo between core
+// matrices adjacent in M (or N).  The start needs 16-byte alignment only.
+__device__ __forceinline__ uint64_t umma_desc_plain(const void *smem_start, uint32_t lbo, uint32_t sbo) {
+  const uint64_t a = (uint64_t)((smem_u32(smem_start) & 0x3FFFFu) >> 4);
+  return a | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) | ((uint64_t)1 << 46);
+}
+
 __host__ __device__ constexpr uint32_t umma_idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }

@@ -173,28 +173,33 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // The same 3x3 convolution on the tensor cores (BF16 in, FP32 accumulate):
-// an implicit GEMM over a patch of 16 (r) x 8 (z) output pixels per CTA:
-// M = 128 pixels, N = NOUT output channels and K = 9 CINP, where CINP and NOUT
-// are cin and cout rounded up to 16.  The CTA first copies its input halo
-// (18 x 10 pixels x CINP channels, zero outside the grid) into shared memory
-// with asynchronous copies, once; every K block of 64 columns (taps x
-// channels) of the im2col matrix A is then built from that halo by
-// shared-to-shared copies, so each input pixel crosses L2 about 1.4 times
-// instead of 9.  A and B (the packed weights) sit in kConvStages stages, both
-// K-major with the 128-byte swizzle; one thread issues the four K steps of a
-// block and commits them to the stage's mbarrier, whose completion frees the
-// stage for the block kConvStages later, so building one block overlaps the
-// MMAs of the previous one.  The FP32 accumulator stays in tensor memory
-// (128 lanes = pixels, NOUT columns) until the epilogue, where each warp
-// loads its 32 lanes and stores BF16.  Every mbarrier wait is bounded; a wait
-// that gives up sets bit 0 of *status, and the CTA still waits (bounded) for
-// its MMAs and frees its tensor memory.
-constexpr int kConvStages = 2;
-constexpr int kConvTR = 16, kConvTZ = 8;  // pixel patch of a CTA (r x z)
+// an implicit GEMM over a patch of 8 (r) x 16 (z) output pixels per CTA,
+// M = 128 pixels (row m = r + 8 z), N = NOUT output channels, K = 9 CINP
+// (CINP, NOUT: cin and cout rounded up to 16).  The CTA copies its input halo
+// (10 x 18 pixels x CINP channels, zero outside the grid) into shared memory
+// once, as 16-byte chunks of 8 channels at ((hz CC + cc) 10 + hr) 16 bytes
+// (CC = CINP / 8).  In that order the 8 pixels (hr .. hr + 7, hz) of one
+// chunk column are 8 consecutive 16-byte rows: a K-major operand without
+// swizzle (core matrices of 8 rows x 16 bytes, 160 bytes apart in K and
+// CC 160 bytes apart in M).  So for tap (dr, dz) the A operand of the whole
+// patch is the halo itself, read from the start chunk (dz CC + cc) 10 + dr:
+// no im2col matrix is built.  The weights of the 9 taps are staged once in
+// the same form (wpk [tap][cc][n][8]).  One thread issues the 9 x CINP / 16
+// MMAs (M 128, N NOUT, K 16) and commits them to an mbarrier; the FP32
+// accumulator stays in tensor memory (128 lanes = pixels, NOUT columns) until
+// the epilogue, where each warp loads its 32 lanes and stores BF16.  The wait
+// is bounded; one that gives up sets bit 0 of *status, and the CTA still
+// waits (bounded) for its MMAs and frees its tensor memory.
+constexpr int kConvTR = 8, kConvTZ = 16;  // pixel patch of a CTA (r x z)
+constexpr int kConvHR = kConvTR + 2, kConvHZ = kConvTZ + 2;
 
 template <int CINP>
 __host__ __device__ constexpr int conv_halo_bytes() {
-  return (kConvTR + 2) * (kConvTZ + 2) * CINP * 2;
+  return kConvHR * kConvHZ * CINP * 2;
+}
+template <int CINP, int NOUT>
+__host__ __device__ constexpr int conv_wstage_bytes() {
+  return 9 * CINP * NOUT * 2;
 }
 
 template <int CINP, int NOUT>
@@ -202,17 +207,14 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
                                                 const __nv_bfloat16 *__restrict__ wpk, int cout,
                                                 __nv_bfloat16 *__restrict__ out, unsigned *status) {
   static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
-  constexpr int S = kConvStages, HR = kConvTR + 2, HZ = kConvTZ + 2;
-  constexpr int K = 9 * CINP;
-  constexpr int KB = (K + 63) / 64;
-  constexpr int ABYTES = 128 * 128, BBYTES = NOUT * 128, STAGE = ABYTES + BBYTES;
+  constexpr int CC = CINP / 8, HR = kConvHR, HZ = kConvHZ;
   constexpr uint32_t NCOLS = NOUT <= 32 ? 32 : 64;
   constexpr uint32_t IDESC = umma_idesc_bf16_f32(128, NOUT);
-  static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzle");
   extern __shared__ uint8_t smraw[];
-  uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  uint8_t *halo = sm + S * STAGE;  // [hz][hr][CINP] BF16
-  __shared__ uint64_t bar[S];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
+  uint8_t *halo = sm;                           // [hz][cc][hr] 16-byte chunks
+  uint8_t *wst = sm + conv_halo_bytes<CINP>();  // [tap][cc][n] 16-byte chunks
+  __shared__ uint64_t bar;
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
@@ -220,17 +222,17 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
     tmem_relinquish();
   }
   if (tid == 0) {
-    for (int i = 0; i < S; i++) mbar_init(&bar[i], 1);
+    mbar_init(&bar, 1);
     mbar_init_fence();
   }
   const int j0 = blockIdx.x * kConvTR, k0 = blockIdx.y * kConvTZ;
-  // the halo: pixels (j0 - 1 .. j0 + 16, k0 - 1 .. k0 + 8), chunks of 8 channels
-  constexpr int CC = CINP / 8;
+  // the halo, pixels (j0 - 1 .. j0 + 8, k0 - 1 .. k0 + 16): consecutive
+  // threads take consecutive chunks of a pixel, then the next pixel in r
   for (int e = tid; e < HR * HZ * CC; e += 128) {
     const int cc = e % CC, pix = e / CC, hr = pix % HR, hz = pix / HR;
     const int j = j0 + hr - 1, k = k0 + hz - 1, ci = cc * 8;
     const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < cin;
-    uint8_t *dst = halo + ((size_t)(hz * HR + hr) * CINP + ci) * 2;
+    uint8_t *dst = halo + (size_t)((hz * CC + cc) * HR + hr) * 16;
     const __nv_bfloat16 *src = live ? in + ((size_t)j + (size_t)H * k) * cin + ci : in;
     if ((cin & 7) == 0) {
       cp_async16(dst, src, live ? 16u : 0u);
@@ -241,50 +243,31 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
       *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(v);
     }
   }
+  // the packed weights are already in the staged order
+  for (int e = tid; e < 9 * CC * NOUT; e += 128) cp_async16(wst + (size_t)e * 16, wpk + (size_t)e * 8, 16u);
   cp_async_commit();
   cp_async_wait<0>();
+  fence_proxy_async();  // the halo and weights, before the tensor cores read them
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
-  const int mr = tid % kConvTR, mz = tid / kConvTR;  // this thread's row of A and of D
-  bool ok = true;
-  for (int kb = 0; kb < KB; kb++) {
-    const int s = kb % S;
-    uint8_t *As = sm + s * STAGE;
-    uint8_t *Bs = As + ABYTES;
-    // the MMAs of block kb - S read this stage: wait for their commit
-    if (kb >= S && !mbar_wait(&bar[s], (unsigned)((kb - S) / S) & 1u)) ok = false;
+  if (tid == 0) {
+#pragma unroll 1
+    for (int t = 0; t < 9; t++) {
+      const int dr = t / 3, dz = t % 3;  // tap t: neighbour (j + dr - 1, k + dz - 1)
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int kc = kb * 64 + c * 8;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (kc < K) {
-        const int t = kc / CINP, ci = kc % CINP;  // tap t: neighbour (j + t / 3 - 1, k + t % 3 - 1)
-        v = *reinterpret_cast<const uint4 *>(halo + ((size_t)((mz + t % 3) * HR + mr + t / 3) * CINP + ci) * 2);
+      for (int ks = 0; ks < CINP / 16; ks++) {
+        const uint64_t ad = umma_desc_plain(halo + (size_t)((dz * CC + 2 * ks) * HR + dr) * 16, HR * 16, CC * HR * 16);
+        const uint64_t bd = umma_desc_plain(wst + (size_t)((t * CC + 2 * ks) * NOUT) * 16, NOUT * 16, 128);
+        umma_bf16(tmem, ad, bd, IDESC, (t | ks) ? 1u : 0u);
       }
-      *reinterpret_cast<uint4 *>(As + sw128_off(tid, c)) = v;
     }
-    for (int e = tid; e < NOUT * 8; e += 128) {
-      const int n = e >> 3, c = e & 7, kc = kb * 64 + c * 8;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (kc < K) v = *reinterpret_cast<const uint4 *>(wpk + (size_t)n * K + kc);
-      *reinterpret_cast<uint4 *>(Bs + sw128_off(n, c)) = v;
-    }
-    fence_proxy_async();  // the generic-proxy stores above, before the tensor cores read them
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint64_t ad = umma_desc_k128(As), bd = umma_desc_k128(Bs);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++)
-        if (kb * 64 + kk * 16 < K) umma_bf16(tmem, ad + (uint64_t)(2 * kk), bd + (uint64_t)(2 * kk), IDESC, (kb | kk) ? 1u : 0u);
-      umma_commit(&bar[s]);
-    }
+    umma_commit(&bar);
   }
-  // the last commit arrives once every MMA of the CTA is done
-  if (!mbar_wait(&bar[(KB - 1) % S], (unsigned)((KB - 1) / S) & 1u)) ok = false;
+  const bool ok = mbar_wait(&bar, 0u);
   tc_fence_after();
+  const int mr = tid % kConvTR, mz = tid / kConvTR;  // this thread's row of D: pixel (j0 + mr, k0 + mz)
   const int j = j0 + mr, k = k0 + mz;
   const bool pin = j < H && k < W;
   const size_t p = (size_t)j + (size_t)H * k;
@@ -305,19 +288,25 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
       }
     }
   }
-  if (!ok && tid == 0) atomicOr(status, 1u);
+  if (!ok) {
+    if (tid == 0) atomicOr(status, 1u);
+    // the MMAs may still be reading shared memory and writing tensor memory
+    (void)mbar_wait(&bar, 0u);
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
 
-// packed tensor-core weights: wpk[n][tap][ci] = bf16(w[n][tap][ci]) for
-// n < cout, ci < cin, zero elsewhere
+// packed tensor-core weights in the order the convolution stages them:
+// wpk[((tap CC + cc) nout + n) 8 + q] = bf16(w[n][tap][8 cc + q]) for n < cout,
+// 8 cc + q < cin, zero elsewhere (CC = cinp / 8)
 __global__ void k_wpack(const float *__restrict__ w, int cin, int cout, int cinp, int nout,
                         __nv_bfloat16 *__restrict__ wpk) {
-  const int n_el = nout * 9 * cinp;
+  const int n_el = nout * 9 * cinp, cc_n = cinp / 8;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += gridDim.x * blockDim.x) {
-    const int ci = e % cinp, t = (e / cinp) % 9, n = e / (9 * cinp);
+    const int q = e % 8, n = (e / 8) % nout, cc = (e / (8 * nout)) % cc_n, t = e / (8 * nout * cc_n);
+    const int ci = 8 * cc + q;
     const float v = (n < cout && ci < cin) ? w[((size_t)n * 9 + t) * cin + ci] : 0.f;
     wpk[e] = __float2bfloat16_rn(v);
   }
@@ -542,7 +531,7 @@ static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, in
 template <int CINP, int NOUT>
 static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
                               __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
-  const size_t sm = 1024 + kConvStages * (size_t)(128 * 128 + NOUT * 128) + conv_halo_bytes<CINP>();
+  const size_t sm = 128 + (size_t)conv_halo_bytes<CINP>() + conv_wstage_bytes<CINP, NOUT>();
   cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
   if (e) return e;
   dim3 grid((H + kConvTR - 1) / kConvTR, (W + kConvTZ - 1) / kConvTZ);
