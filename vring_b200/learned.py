@@ -184,7 +184,9 @@ def main(argv=None):
     (the committed weights came from the defaults), then compare the solvers
     on one triple of each of seeds 2, 7 and 21.  With --forward N it only
     runs N forward passes of an untrained network on a seeded random field
-    (the case the convolution profiles are taken on) and exits."""
+    (the case the convolution profiles are taken on) and exits; with
+    --solve N it runs N iterations of the learned flexible CG with the
+    committed weights on the triple of seed 2, step 500, and exits."""
     import argparse
     import time
     ap = argparse.ArgumentParser()
@@ -194,7 +196,19 @@ def main(argv=None):
     ap.add_argument("--lr-final", type=float, default=3e-4)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--forward", type=int, default=0)
+    ap.add_argument("--solve", type=int, default=0)
     a = ap.parse_args(argv)
+    if a.solve:
+        k = make_solver()
+        net = make_net()
+        load_weights(net)
+        seq = RingSequence(2, k.faces, k.nz, k.zmax)
+        f, p_prev, _ = triple(k, seq, 500)
+        k.set_preconditioner(net)
+        _, it, rr, ms = k.solve(f, "learned", x0=p_prev, tol=1e-30, maxit=a.solve)
+        k.set_preconditioner(None)
+        print("learned flexible CG: %d iterations, relres %.3e, %.2f ms" % (it, rr, ms))
+        return
     if a.forward:
         net = make_net()
         x = np.random.default_rng(0).standard_normal((NR, NZ))
