@@ -190,6 +190,12 @@ __device__ __forceinline__ void cp_async_wait() {
 // the epilogue, where each warp loads its 32 lanes and stores BF16.  The wait
 // is bounded; one that gives up sets bit 0 of *status, and the CTA still
 // waits (bounded) for its MMAs and frees its tensor memory.
+//
+// With skip set, the input is the decoder's concatenation, read where it
+// lies instead of from a copy: channels [0, cin) are the coarse level `in`
+// (H/F x W/F pixels, nearest upsampling by F) and channels
+// [cin, cin + cskip) the skip tensor at full resolution.  Both channel counts
+// are multiples of 8, so every 16-byte chunk comes from one of them.
 constexpr int kConvTR = 8, kConvTZ = 16;  // pixel patch of a CTA (r x z)
 constexpr int kConvHR = kConvTR + 2, kConvHZ = kConvTZ + 2;
 
@@ -204,6 +210,7 @@ __host__ __device__ constexpr int conv_wstage_bytes() {
 
 template <int CINP, int NOUT>
 __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W, int cin,
+                                                const __nv_bfloat16 *__restrict__ skip, int cskip, int F,
                                                 const __nv_bfloat16 *__restrict__ wpk, int cout,
                                                 __nv_bfloat16 *__restrict__ out, unsigned *status) {
   static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
@@ -228,13 +235,22 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
   const int j0 = blockIdx.x * kConvTR, k0 = blockIdx.y * kConvTZ;
   // the halo, pixels (j0 - 1 .. j0 + 8, k0 - 1 .. k0 + 16): consecutive
   // threads take consecutive chunks of a pixel, then the next pixel in r
+  const int ctot = skip ? cin + cskip : cin, H2 = H / F;
   for (int e = tid; e < HR * HZ * CC; e += 128) {
     const int cc = e % CC, pix = e / CC, hr = pix % HR, hz = pix / HR;
     const int j = j0 + hr - 1, k = k0 + hz - 1, ci = cc * 8;
-    const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < cin;
+    const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < ctot;
     uint8_t *dst = halo + (size_t)((hz * CC + cc) * HR + hr) * 16;
-    const __nv_bfloat16 *src = live ? in + ((size_t)j + (size_t)H * k) * cin + ci : in;
-    if ((cin & 7) == 0) {
+    const __nv_bfloat16 *src = in;
+    if (live) {
+      if (!skip)
+        src = in + ((size_t)j + (size_t)H * k) * cin + ci;
+      else if (ci < cin)
+        src = in + ((size_t)(j / F) + (size_t)H2 * (k / F)) * cin + ci;
+      else
+        src = skip + ((size_t)j + (size_t)H * k) * cskip + (ci - cin);
+    }
+    if ((ctot & 7) == 0) {
       cp_async16(dst, src, live ? 16u : 0u);
     } else {
       __align__(16) __nv_bfloat16 v[8];
@@ -529,40 +545,48 @@ static cudaError_t conv3(const TI *in, int H, int W, int cin, const float *w, in
 }
 
 template <int CINP, int NOUT>
-static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
-                              __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
+static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *skip, int cskip,
+                              int F, const __nv_bfloat16 *wpk, int cout, __nv_bfloat16 *out, unsigned *status,
+                              cudaStream_t s) {
   const size_t sm = 128 + (size_t)conv_halo_bytes<CINP>() + conv_wstage_bytes<CINP, NOUT>();
   cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
   if (e) return e;
   dim3 grid((H + kConvTR - 1) / kConvTR, (W + kConvTZ - 1) / kConvTZ);
-  k_conv3_tc<CINP, NOUT><<<grid, 128, sm, s>>>(in, H, W, cin, wpk, cout, out, status);
+  k_conv3_tc<CINP, NOUT><<<grid, 128, sm, s>>>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status);
   return cudaGetLastError();
 }
 
 template <int CINP>
-static cudaError_t conv3_tc_c(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
-                              __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
+static cudaError_t conv3_tc_c(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *skip, int cskip,
+                              int F, const __nv_bfloat16 *wpk, int cout, __nv_bfloat16 *out, unsigned *status,
+                              cudaStream_t s) {
   switch ((cout + 15) / 16) {
-    case 1: return conv3_tc_n<CINP, 16>(in, H, W, cin, wpk, cout, out, status, s);
-    case 2: return conv3_tc_n<CINP, 32>(in, H, W, cin, wpk, cout, out, status, s);
-    case 3: return conv3_tc_n<CINP, 48>(in, H, W, cin, wpk, cout, out, status, s);
-    case 4: return conv3_tc_n<CINP, 64>(in, H, W, cin, wpk, cout, out, status, s);
+    case 1: return conv3_tc_n<CINP, 16>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status, s);
+    case 2: return conv3_tc_n<CINP, 32>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status, s);
+    case 3: return conv3_tc_n<CINP, 48>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status, s);
+    case 4: return conv3_tc_n<CINP, 64>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
-// tensor-core 3x3 convolution: cin up to 128, cout up to 64
+// tensor-core 3x3 convolution: cin (+ cskip) up to 128, cout up to 64; with
+// skip, the input is the concatenation of `in` upsampled by F and `skip`
 static cudaError_t conv3_tc(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *wpk, int cout,
-                            __nv_bfloat16 *out, unsigned *status, cudaStream_t s) {
-  switch ((cin + 15) / 16) {
-    case 1: return conv3_tc_c<16>(in, H, W, cin, wpk, cout, out, status, s);
-    case 2: return conv3_tc_c<32>(in, H, W, cin, wpk, cout, out, status, s);
-    case 3: return conv3_tc_c<48>(in, H, W, cin, wpk, cout, out, status, s);
-    case 4: return conv3_tc_c<64>(in, H, W, cin, wpk, cout, out, status, s);
-    case 5: return conv3_tc_c<80>(in, H, W, cin, wpk, cout, out, status, s);
-    case 6: return conv3_tc_c<96>(in, H, W, cin, wpk, cout, out, status, s);
-    case 7: return conv3_tc_c<112>(in, H, W, cin, wpk, cout, out, status, s);
-    case 8: return conv3_tc_c<128>(in, H, W, cin, wpk, cout, out, status, s);
+                            __nv_bfloat16 *out, unsigned *status, cudaStream_t s,
+                            const __nv_bfloat16 *skip = nullptr, int cskip = 0, int F = 1) {
+  if (skip && ((cin & 7) || (cskip & 7))) return cudaErrorInvalidValue;
+  const int ctot = cin + (skip ? cskip : 0);
+  switch ((ctot + 15) / 16) {
+#define VR_CONV_TC(CP) return conv3_tc_c<CP>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status, s)
+    case 1: VR_CONV_TC(16);
+    case 2: VR_CONV_TC(32);
+    case 3: VR_CONV_TC(48);
+    case 4: VR_CONV_TC(64);
+    case 5: VR_CONV_TC(80);
+    case 6: VR_CONV_TC(96);
+    case 7: VR_CONV_TC(112);
+    case 8: VR_CONV_TC(128);
+#undef VR_CONV_TC
     default: return cudaErrorInvalidValue;
   }
 }
@@ -792,7 +816,10 @@ extern "C" int vr_unet_set_params(vr_unet *u, const float *w) {
 namespace vr {
 
 // forward from u->x0 (bf16 input) to u->y (fp32)
-static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
+// infer: the decoder's concatenations are read by the tensor-core
+// convolutions where they lie (no upsampled copy); training keeps the copies,
+// which the backward pass reads
+static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s, bool infer = false) {
   const UnetShapes sh = shapes_of(u);
   const vr_unet *x = u;
   cudaError_t e;
@@ -802,6 +829,7 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
     for (int l = 0; l < lev; l++) H /= u->pool, W /= u->pool;
   };
   int H, W;
+  const bool fuse = infer && !u->cuda_cores;
   auto conv = [&](int li) -> cudaError_t {
     const UnetLayer &L = u->L[li];
     HW(L.level, H, W);
@@ -809,6 +837,13 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
     if (u->cuda_cores)
       return conv3<__nv_bfloat16, __nv_bfloat16>(in, H, W, L.cin, u->wk + L.woff, L.cout, x->a[kConvOut[li]], 0, s);
     return conv3_tc(in, H, W, L.cin, u->wpk + u->wpk_off[li], L.cout, x->a[kConvOut[li]], u->status, s);
+  };
+  // the first convolution of a decoder level, on concat(upsample(coarse), skip)
+  auto conv_cat = [&](int li, int coarse, int skip) -> cudaError_t {
+    const UnetLayer &L = u->L[li];
+    HW(L.level, H, W);
+    return conv3_tc(x->a[coarse], H, W, sh.ch[coarse], u->wpk + u->wpk_off[li], L.cout, x->a[kConvOut[li]],
+                    u->status, s, x->a[skip], sh.ch[skip], u->pool);
   };
   auto pool = [&](int src, int dst) {
     HW(sh.lev[src], H, W);
@@ -827,9 +862,15 @@ static cudaError_t unet_fwd(const vr_unet *u, cudaStream_t s) {
   if ((e = conv(2)) || (e = conv(3)) || (e = pool(S_E1, S_P2))) return e;
   if ((e = conv(4)) || (e = conv(5)) || (e = pool(S_E2, S_P3))) return e;
   if ((e = conv(6)) || (e = conv(7))) return e;
-  if ((e = upcat(S_B3, S_E2, S_U2)) || (e = conv(8)) || (e = conv(9))) return e;
-  if ((e = upcat(S_D2, S_E1, S_U1)) || (e = conv(10)) || (e = conv(11))) return e;
-  if ((e = upcat(S_D1, S_E0, S_U0)) || (e = conv(12)) || (e = conv(13))) return e;
+  if (fuse) {
+    if ((e = conv_cat(8, S_B3, S_E2)) || (e = conv(9))) return e;
+    if ((e = conv_cat(10, S_D2, S_E1)) || (e = conv(11))) return e;
+    if ((e = conv_cat(12, S_D1, S_E0)) || (e = conv(13))) return e;
+  } else {
+    if ((e = upcat(S_B3, S_E2, S_U2)) || (e = conv(8)) || (e = conv(9))) return e;
+    if ((e = upcat(S_D2, S_E1, S_U1)) || (e = conv(10)) || (e = conv(11))) return e;
+    if ((e = upcat(S_D1, S_E0, S_U0)) || (e = conv(12)) || (e = conv(13))) return e;
+  }
   const int P0 = u->nr * u->nz;
   k_head<<<grid_for(P0), 256, 0, s>>>(x->a[S_D0], P0, u->ch[0], u->wk + u->L[14].woff, u->y);
   return cudaGetLastError();
@@ -902,7 +943,7 @@ int unet_precondition(const vr_unet *u, const double *r, double *z, const double
   const int n = u->nr * u->nz;
   k_in<<<grid_for(n), 256, 0, s>>>(r, n, ss, 0.0, dscale, u->x0, flags);
   if (cudaGetLastError() != cudaSuccess) return VR_ERR_CUDA;
-  if (unet_fwd(u, s) != cudaSuccess) return VR_ERR_CUDA;
+  if (unet_fwd(u, s, true) != cudaSuccess) return VR_ERR_CUDA;
   k_out<<<grid_for(n), 256, 0, s>>>(u->y, n, ss, 0.0, dscale, z, flags);
   return cudaGetLastError() == cudaSuccess ? VR_OK : VR_ERR_CUDA;
 }
@@ -919,7 +960,7 @@ extern "C" int vr_unet_forward(vr_unet *u, const double *xh, double *yh) {
   U_CUDA(u, cudaMemcpyAsync(u->xs, xh, sizeof(double) * n, cudaMemcpyHostToDevice, u->stream));
   k_in<<<grid_for(n), 256, 0, u->stream>>>(u->xs, n, nullptr, s > 0 ? 1.0 / s : 0.0, nullptr, u->x0, nullptr);
   U_CUDA(u, cudaGetLastError());
-  U_CUDA(u, unet_fwd(u, u->stream));
+  U_CUDA(u, unet_fwd(u, u->stream, true));
   k_out<<<grid_for(n), 256, 0, u->stream>>>(u->y, n, nullptr, s, nullptr, u->xs, nullptr);
   U_CUDA(u, cudaGetLastError());
   U_CUDA(u, cudaMemcpyAsync(yh, u->xs, sizeof(double) * n, cudaMemcpyDeviceToHost, u->stream));
