@@ -186,7 +186,9 @@ def main(argv=None):
     runs N forward passes of an untrained network on a seeded random field
     (the case the convolution profiles are taken on) and exits; with
     --solve N it runs N iterations of the learned flexible CG with the
-    committed weights on the triple of seed 2, step 500, and exits."""
+    committed weights on the triple of seed 2, step 500, and exits; with
+    --compare it skips the training and compares the solvers with the
+    committed weights."""
     import argparse
     import time
     ap = argparse.ArgumentParser()
@@ -197,6 +199,7 @@ def main(argv=None):
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--forward", type=int, default=0)
     ap.add_argument("--solve", type=int, default=0)
+    ap.add_argument("--compare", action="store_true")
     a = ap.parse_args(argv)
     if a.solve:
         k = make_solver()
@@ -218,10 +221,13 @@ def main(argv=None):
         return
     k = make_solver()
     net = make_net()
-    t0 = time.time()
-    train(net, k, a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final,
-          log=lambda s: print(s, "%.0fs" % (time.time() - t0), flush=True))
-    save_weights(net, a.out, steps=a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final)
+    if a.compare:
+        load_weights(net)
+    else:
+        t0 = time.time()
+        train(net, k, a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final,
+              log=lambda s: print(s, "%.0fs" % (time.time() - t0), flush=True))
+        save_weights(net, a.out, steps=a.steps, batch=a.batch, lr=a.lr, lr_final=a.lr_final)
     for seed, t in ((2, 500), (7, 250), (21, 900)):
         seq = RingSequence(seed, k.faces, k.nz, k.zmax)
         f, p_prev, p = triple(k, seq, t)
