@@ -27,7 +27,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -174,34 +173,30 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // The same 3x3 convolution on the tensor cores (BF16 in, FP32 accumulate):
-// an implicit GEMM over patches of 8 (r) x 16 (z) output pixels, M = 128
-// pixels (row m = r + 8 z), N = NOUT output channels, K = 9 CINP (CINP,
-// NOUT: cin and cout rounded up to 16).  A patch's input halo (10 x 18 pixels
-// x CINP channels, zero outside the grid) sits in shared memory as 16-byte
-// chunks of 8 channels at ((hz CC + cc) 10 + hr) 16 bytes (CC = CINP / 8).
-// In that order the 8 pixels (hr .. hr + 7, hz) of one chunk column are 8
-// consecutive 16-byte rows: a K-major operand without swizzle (core
-// matrices of 8 rows x 16 bytes, 160 bytes apart in K and CC 160 bytes apart
-// in M).  So for tap (dr, dz) the A operand of the whole patch is the halo
-// itself, read from the start chunk (dz CC + cc) 10 + dr: no im2col matrix
-// is built.  The weights of the 9 taps are staged once per CTA in the same
-// form (wpk [tap][cc][n][8]).
-//
-// A CTA walks the patches blockIdx.x, + gridDim.x, ... with two halo
-// buffers: the asynchronous copies of the next patch's halo are in flight
-// while one thread issues the current patch's 9 x CINP / 16 MMAs (M 128,
-// N NOUT, K 16), commits them to an mbarrier, and the warps move the FP32
-// accumulator from tensor memory (128 lanes = pixels, NOUT columns) to BF16
-// stores.  Every wait is bounded; one that gives up sets bit 0 of *status and
-// ends the walk, after a second bounded wait for the MMAs in flight, and the
-// CTA frees its tensor memory.
+// an implicit GEMM over a patch of 8 (r) x 16 (z) output pixels per CTA,
+// M = 128 pixels (row m = r + 8 z), N = NOUT output channels, K = 9 CINP
+// (CINP, NOUT: cin and cout rounded up to 16).  The CTA copies its input halo
+// (10 x 18 pixels x CINP channels, zero outside the grid) into shared memory
+// once, as 16-byte chunks of 8 channels at ((hz CC + cc) 10 + hr) 16 bytes
+// (CC = CINP / 8).  In that order the 8 pixels (hr .. hr + 7, hz) of one
+// chunk column are 8 consecutive 16-byte rows: a K-major operand without
+// swizzle (core matrices of 8 rows x 16 bytes, 160 bytes apart in K and
+// CC 160 bytes apart in M).  So for tap (dr, dz) the A operand of the whole
+// patch is the halo itself, read from the start chunk (dz CC + cc) 10 + dr:
+// no im2col matrix is built.  The weights of the 9 taps are staged once in
+// the same form (wpk [tap][cc][n][8]).  One thread issues the 9 x CINP / 16
+// MMAs (M 128, N NOUT, K 16) and commits them to an mbarrier; the FP32
+// accumulator stays in tensor memory (128 lanes = pixels, NOUT columns) until
+// the epilogue, where each warp loads its 32 lanes and stores BF16.  The wait
+// is bounded; one that gives up sets bit 0 of *status, and the CTA still
+// waits (bounded) for its MMAs and frees its tensor memory.
 //
 // With skip set, the input is the decoder's concatenation, read where it
 // lies instead of from a copy: channels [0, cin) are the coarse level `in`
 // (H/F x W/F pixels, nearest upsampling by F) and channels
 // [cin, cin + cskip) the skip tensor at full resolution.  Both channel counts
 // are multiples of 8, so every 16-byte chunk comes from one of them.
-constexpr int kConvTR = 8, kConvTZ = 16;  // pixel patch (r x z)
+constexpr int kConvTR = 8, kConvTZ = 16;  // pixel patch of a CTA (r x z)
 constexpr int kConvHR = kConvTR + 2, kConvHZ = kConvTZ + 2;
 
 template <int CINP>
@@ -219,17 +214,16 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
                                                 const __nv_bfloat16 *__restrict__ wpk, int cout,
                                                 __nv_bfloat16 *__restrict__ out, unsigned *status) {
   static_assert(CINP % 16 == 0 && NOUT % 16 == 0 && NOUT <= 64, "tile shape");
-  constexpr int CC = CINP / 8, HR = kConvHR, HZ = kConvHZ, HB = conv_halo_bytes<CINP>();
+  constexpr int CC = CINP / 8, HR = kConvHR, HZ = kConvHZ;
   constexpr uint32_t NCOLS = NOUT <= 32 ? 32 : 64;
   constexpr uint32_t IDESC = umma_idesc_bf16_f32(128, NOUT);
   extern __shared__ uint8_t smraw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-  uint8_t *wst = sm;  // [tap][cc][n] 16-byte chunks
-  uint8_t *halo0 = sm + conv_wstage_bytes<CINP, NOUT>();  // two buffers of [hz][cc][hr] chunks
+  uint8_t *halo = sm;                           // [hz][cc][hr] 16-byte chunks
+  uint8_t *wst = sm + conv_halo_bytes<CINP>();  // [tap][cc][n] 16-byte chunks
   __shared__ uint64_t bar;
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int nbx = (H + kConvTR - 1) / kConvTR, npatch = nbx * ((W + kConvTZ - 1) / kConvTZ);
   if (warp == 0) {
     tmem_alloc(&tbase, NCOLS);
     tmem_relinquish();
@@ -238,107 +232,83 @@ __global__ void __launch_bounds__(128) k_conv3_tc(const __nv_bfloat16 *__restric
     mbar_init(&bar, 1);
     mbar_init_fence();
   }
+  const int j0 = blockIdx.x * kConvTR, k0 = blockIdx.y * kConvTZ;
+  // the halo, pixels (j0 - 1 .. j0 + 8, k0 - 1 .. k0 + 16): consecutive
+  // threads take consecutive chunks of a pixel, then the next pixel in r
   const int ctot = skip ? cin + cskip : cin, H2 = H / F;
-  // the halo of patch pt into buffer b: consecutive threads take consecutive
-  // chunks of a pixel, then the next pixel in r
-  auto load_halo = [&](int pt, int b) {
-    const int j0 = (pt % nbx) * kConvTR, k0 = (pt / nbx) * kConvTZ;
-    uint8_t *halo = halo0 + b * HB;
-    for (int e = tid; e < HR * HZ * CC; e += 128) {
-      const int cc = e % CC, pix = e / CC, hr = pix % HR, hz = pix / HR;
-      const int j = j0 + hr - 1, k = k0 + hz - 1, ci = cc * 8;
-      const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < ctot;
-      uint8_t *dst = halo + (size_t)((hz * CC + cc) * HR + hr) * 16;
-      const __nv_bfloat16 *src = in;
-      if (live) {
-        if (!skip)
-          src = in + ((size_t)j + (size_t)H * k) * cin + ci;
-        else if (ci < cin)
-          src = in + ((size_t)(j / F) + (size_t)H2 * (k / F)) * cin + ci;
-        else
-          src = skip + ((size_t)j + (size_t)H * k) * cskip + (ci - cin);
-      }
-      if ((ctot & 7) == 0) {
-        cp_async16(dst, src, live ? 16u : 0u);
-      } else {
-        __align__(16) __nv_bfloat16 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) v[q] = (live && ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
-        *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(v);
-      }
+  for (int e = tid; e < HR * HZ * CC; e += 128) {
+    const int cc = e % CC, pix = e / CC, hr = pix % HR, hz = pix / HR;
+    const int j = j0 + hr - 1, k = k0 + hz - 1, ci = cc * 8;
+    const bool live = j >= 0 && j < H && k >= 0 && k < W && ci < ctot;
+    uint8_t *dst = halo + (size_t)((hz * CC + cc) * HR + hr) * 16;
+    const __nv_bfloat16 *src = in;
+    if (live) {
+      if (!skip)
+        src = in + ((size_t)j + (size_t)H * k) * cin + ci;
+      else if (ci < cin)
+        src = in + ((size_t)(j / F) + (size_t)H2 * (k / F)) * cin + ci;
+      else
+        src = skip + ((size_t)j + (size_t)H * k) * cskip + (ci - cin);
     }
-  };
+    if ((ctot & 7) == 0) {
+      cp_async16(dst, src, live ? 16u : 0u);
+    } else {
+      __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = (live && ci + q < cin) ? src[q] : __float2bfloat16_rn(0.f);
+      *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(v);
+    }
+  }
   // the packed weights are already in the staged order
   for (int e = tid; e < 9 * CC * NOUT; e += 128) cp_async16(wst + (size_t)e * 16, wpk + (size_t)e * 8, 16u);
-  if ((int)blockIdx.x < npatch) load_halo(blockIdx.x, 0);
   cp_async_commit();
+  cp_async_wait<0>();
+  fence_proxy_async();  // the halo and weights, before the tensor cores read them
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
-  bool ok = true;
-  int it = 0;
-  for (int pt = blockIdx.x; pt < npatch; pt += gridDim.x, it++) {
-    const int nx = pt + gridDim.x;
-    if (nx < npatch) load_halo(nx, (it + 1) & 1);
-    cp_async_commit();  // possibly empty: the group count stays one per patch
-    cp_async_wait<1>();  // this patch's halo (and the weights) have landed
-    fence_proxy_async();  // before the tensor cores read them
-    __syncthreads();
-    const uint8_t *halo = halo0 + (it & 1) * HB;
-    if (tid == 0) {
-      tc_fence_after();
+  if (tid == 0) {
 #pragma unroll 1
-      for (int t = 0; t < 9; t++) {
-        const int dr = t / 3, dz = t % 3;  // tap t: neighbour (j + dr - 1, k + dz - 1)
+    for (int t = 0; t < 9; t++) {
+      const int dr = t / 3, dz = t % 3;  // tap t: neighbour (j + dr - 1, k + dz - 1)
 #pragma unroll
-        for (int ks = 0; ks < CINP / 16; ks++) {
-          const uint64_t ad =
-              umma_desc_plain(halo + (size_t)((dz * CC + 2 * ks) * HR + dr) * 16, HR * 16, CC * HR * 16);
-          const uint64_t bd = umma_desc_plain(wst + (size_t)((t * CC + 2 * ks) * NOUT) * 16, NOUT * 16, 128);
-          umma_bf16(tmem, ad, bd, IDESC, (t | ks) ? 1u : 0u);
-        }
-      }
-      umma_commit(&bar);
-    }
-    // a wait that gives up in any thread ends the walk for the whole CTA
-    if (__syncthreads_or(!mbar_wait(&bar, (unsigned)(it & 1)))) {
-      ok = false;
-      break;
-    }
-    tc_fence_after();
-    const int j0 = (pt % nbx) * kConvTR, k0 = (pt / nbx) * kConvTZ;
-    const int mr = tid % kConvTR, mz = tid / kConvTR;  // this thread's row of D: pixel (j0 + mr, k0 + mz)
-    const int j = j0 + mr, k = k0 + mz;
-    const bool pin = j < H && k < W;
-    const size_t p = (size_t)j + (size_t)H * k;
-#pragma unroll
-    for (int c0 = 0; c0 < NOUT; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-      if (pin && c0 < cout) {
-        __nv_bfloat16 *dst = out + p * cout + c0;
-        if (c0 + 16 <= cout) {
-          __align__(16) __nv_bfloat16 b[16];
-#pragma unroll
-          for (int i = 0; i < 16; i++) b[i] = __float2bfloat16_rn(v[i]);
-          reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(b)[0];
-          reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(b)[1];
-        } else {
-          for (int i = 0; i < 16 && c0 + i < cout; i++) dst[i] = __float2bfloat16_rn(v[i]);
-        }
+      for (int ks = 0; ks < CINP / 16; ks++) {
+        const uint64_t ad = umma_desc_plain(halo + (size_t)((dz * CC + 2 * ks) * HR + dr) * 16, HR * 16, CC * HR * 16);
+        const uint64_t bd = umma_desc_plain(wst + (size_t)((t * CC + 2 * ks) * NOUT) * 16, NOUT * 16, 128);
+        umma_bf16(tmem, ad, bd, IDESC, (t | ks) ? 1u : 0u);
       }
     }
-    // every thread has read the accumulator and the MMAs are done with this
-    // halo buffer before the next patch reuses them
-    tc_fence_before();
-    __syncthreads();
+    umma_commit(&bar);
+  }
+  const bool ok = mbar_wait(&bar, 0u);
+  tc_fence_after();
+  const int mr = tid % kConvTR, mz = tid / kConvTR;  // this thread's row of D: pixel (j0 + mr, k0 + mz)
+  const int j = j0 + mr, k = k0 + mz;
+  const bool pin = j < H && k < W;
+  const size_t p = (size_t)j + (size_t)H * k;
+#pragma unroll
+  for (int c0 = 0; c0 < NOUT; c0 += 16) {
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+    if (pin && ok && c0 < cout) {
+      __nv_bfloat16 *dst = out + p * cout + c0;
+      if (c0 + 16 <= cout) {
+        __align__(16) __nv_bfloat16 b[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) b[i] = __float2bfloat16_rn(v[i]);
+        reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(b)[0];
+        reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(b)[1];
+      } else {
+        for (int i = 0; i < 16 && c0 + i < cout; i++) dst[i] = __float2bfloat16_rn(v[i]);
+      }
+    }
   }
   if (!ok) {
     if (tid == 0) atomicOr(status, 1u);
-    (void)mbar_wait(&bar, (unsigned)(it & 1));  // the MMAs in flight, bounded
+    // the MMAs may still be reading shared memory and writing tensor memory
+    (void)mbar_wait(&bar, 0u);
   }
-  cp_async_wait<0>();
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
@@ -578,24 +548,10 @@ template <int CINP, int NOUT>
 static cudaError_t conv3_tc_n(const __nv_bfloat16 *in, int H, int W, int cin, const __nv_bfloat16 *skip, int cskip,
                               int F, const __nv_bfloat16 *wpk, int cout, __nv_bfloat16 *out, unsigned *status,
                               cudaStream_t s) {
-  const size_t sm = 128 + 2 * (size_t)conv_halo_bytes<CINP>() + conv_wstage_bytes<CINP, NOUT>();
+  const size_t sm = 128 + (size_t)conv_halo_bytes<CINP>() + conv_wstage_bytes<CINP, NOUT>();
   cudaError_t e = allow_dyn_smem(k_conv3_tc<CINP, NOUT>, sm);
   if (e) return e;
-  // resident CTAs: shared memory and tensor memory (512 columns per SM)
-  // bound them; the SM count and occupancy are looked up once per instance
-  static std::once_flag once;
-  static int occ = 0, nsm = 0;
-  static cudaError_t qe = cudaSuccess;
-  std::call_once(once, [&] {
-    int dev = 0;
-    if ((qe = cudaGetDevice(&dev)) || (qe = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) ||
-        (qe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3_tc<CINP, NOUT>, 128, sm)))
-      return;
-    occ = std::max(1, std::min(occ, 512 / (NOUT <= 32 ? 32 : 64)));
-  });
-  if (qe) return qe;
-  const int npatch = ((H + kConvTR - 1) / kConvTR) * ((W + kConvTZ - 1) / kConvTZ);
-  const int grid = std::min(npatch, nsm * occ);
+  dim3 grid((H + kConvTR - 1) / kConvTR, (W + kConvTZ - 1) / kConvTZ);
   k_conv3_tc<CINP, NOUT><<<grid, 128, sm, s>>>(in, H, W, cin, skip, cskip, F, wpk, cout, out, status);
   return cudaGetLastError();
 }
