@@ -126,3 +126,69 @@ def test_fft_transpose_is_conflict_free():
                 for tt in range(T):
                     words = [fft_word(T, base + pl, t * G + u, tt) for pl, t in lanes]
                     assert quarter_warp_degree(words) == 1, (T, u, tt)
+
+
+def fft_natural_word(T, pl, k):
+    """16-byte word of entry k of pair pl in natural order (the transform's
+    output and the inverse transform's staged input)."""
+    return 15 * T + pl * pair_stride(T) + k
+
+
+def packed_slot(T, n):
+    return n ^ ((n >> 3) & 1) if T == 8 else n
+
+
+def test_fft_natural_order_write_is_conflict_free_at_128():
+    # pair_fft16's last write, k = 2 t + u + 16 k2: the lanes t >= 4 of a
+    # pair write the other u in the same instruction; with the same u in
+    # every lane it would be 2-way
+    T, G = 8, 2
+    lanes = [(l // T, l % T) for l in range(32)]
+    for u0 in range(G):
+        for k2 in range(T):
+            words = [fft_natural_word(T, pl, t * G + (u0 ^ int(t >= 4)) + 16 * k2) for pl, t in lanes]
+            assert quarter_warp_degree(words) == 1
+            same_u = [fft_natural_word(T, pl, t * G + u0 + 16 * k2) for pl, t in lanes]
+            assert quarter_warp_degree(same_u) == 2
+    # every entry is written exactly once
+    for t in range(T):
+        ks = sorted(t * G + (u0 ^ int(t >= 4)) + 16 * k2 for u0 in range(G) for k2 in range(T))
+        assert ks == sorted(t * G + u + 16 * k2 for u in range(G) for k2 in range(T))
+
+
+def test_fft_forward_output_reads_are_conflict_free():
+    T, N = 8, 128
+    lanes = [(l // T, l % T) for l in range(32)]
+    for jj in range(N // (2 * T)):
+        ks = [(pl, t + T * jj) for pl, t in lanes]
+        assert quarter_warp_degree_active([fft_natural_word(T, pl, k) if k else None for pl, k in ks]) == 1
+        assert quarter_warp_degree_active([fft_natural_word(T, pl, N - k) if k else None for pl, k in ks]) == 1
+
+
+def quarter_warp_degree_active(words):
+    """quarter_warp_degree over the lanes that take part (None: the lane
+    issues its access in another branch)."""
+    worst = 1
+    for qw in range(4):
+        by_group = {}
+        for wd in set(w for w in words[8 * qw:8 * qw + 8] if w is not None):
+            by_group.setdefault(wd % 8, set()).add(wd)
+        if by_group:
+            worst = max(worst, max(len(v) for v in by_group.values()))
+    return worst
+
+
+def test_fft_inverse_packed_staging_is_conflict_free_at_128():
+    T, N = 8, 128
+    assert sorted(packed_slot(T, n) for n in range(N)) == list(range(N))
+    lanes = [(l // T, l % T) for l in range(32)]
+    for j in range(16):  # staging writes of entries t + T j
+        assert quarter_warp_degree([fft_natural_word(T, pl, packed_slot(T, t + T * j)) for pl, t in lanes]) == 1
+    for m in range(16):  # reads of entries 2 kk - 1 and 2 kk
+        kks = [(pl, (t + T * m) if t + T * m <= N // 2 else N - (t + T * m)) for pl, t in lanes]
+        odd = [fft_natural_word(T, pl, packed_slot(T, 2 * kk - 1)) if kk > 0 else None for pl, kk in kks]
+        even = [fft_natural_word(T, pl, packed_slot(T, 2 * kk)) if 0 < 2 * kk < N else None for pl, kk in kks]
+        assert quarter_warp_degree_active(odd) == 1, m
+        assert quarter_warp_degree_active(even) == 1, m
+        plain = [fft_natural_word(T, pl, 2 * kk) if 0 < 2 * kk < N else None for pl, kk in kks]
+        assert quarter_warp_degree_active(plain) == 2  # the unpermuted layout

@@ -767,7 +767,10 @@ __global__ void __launch_bounds__(256, 2)
   // groups of a warp fall on disjoint halves of the shared-memory banks
   const int SPL = ((SPN + 15) & ~15) + 8;
   double *lines = ring + kQRing * SLOT;        // [plane of batch][comp][r], each SPL
-  double *fac = lines + kTB * 3 * kMRJ * SPL;  // [fam][r][inv, pp, zz], each SPN
+  // the factorisation of each (fam, r), 3 SPL apart: 3 SPL is 8 mod 16
+  // doubles too, so the two groups of a half-warp, which solve rows r = 0, 1
+  // of one family, read disjoint halves of the banks
+  double *fac = lines + kTB * 3 * kMRJ * SPL;  // [fam][r][inv, pp, zz], each SPL
   __shared__ RowCoef rowc[kMRJ];
   __shared__ double rowt[kMRJ][2][3];  // sub, sup, za2 of each family
   __shared__ __align__(8) uint64_t full[kQRing];
@@ -798,10 +801,10 @@ __global__ void __launch_bounds__(256, 2)
     const int i = idx % N, r = (idx / N) % kMRJ, fam = idx / (N * kMRJ), jc = j0 + r;
     if (jc > g.nr) continue;
     const double *inv = fam ? t2.inv : t13.inv, *pp = fam ? t2.pp : t13.pp, *zz = fam ? t2.zz : t13.zz;
-    double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPN;
+    double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPL;
     cp_async8(f + tpad(i), inv + (size_t)jc * N + i);
-    cp_async8(f + SPN + tpad(i), pp + (size_t)jc * N + i);
-    cp_async8(f + 2 * SPN + tpad(i), zz + (size_t)jc * N + i);
+    cp_async8(f + SPL + tpad(i), pp + (size_t)jc * N + i);
+    cp_async8(f + 2 * SPL + tpad(i), zz + (size_t)jc * N + i);
   }
   if (tid < kMRJ && j0 + tid <= g.nr) {
     const int jc = j0 + tid;
@@ -909,9 +912,9 @@ __global__ void __launch_bounds__(256, 2)
         const int L = warp * kGroups + lane / kTL;
         const int pl = L / (3 * kMRJ), comp = (L / kMRJ) % 3, r = L % kMRJ, jc = j0 + r, lk = kc0 + pl;
         const int fam = comp == 1 ? 1 : 0;
-        const double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPN;
+        const double *f = fac + (size_t)(fam * kMRJ + r) * 3 * SPL;
         const bool on = lk <= kc && jc <= g.nr && !(comp == 1 && jc < 2) && !(comp == 2 && lk < 2);
-        tsolve_group<(32 / kTL) * E>(N, f, f + SPN, f + 2 * SPN, &rowt[r][fam][0], lines + (size_t)L * SPL,
+        tsolve_group<(32 / kTL) * E>(N, f, f + SPL, f + 2 * SPL, &rowt[r][fam][0], lines + (size_t)L * SPL,
                                      lane % kTL, on);
         __syncwarp();
 #pragma unroll
@@ -946,7 +949,7 @@ static cudaError_t run_rhs_march(vr_ctx *c, const Rk &rk, const RhsArgsT<T> &a) 
   const int SPN = tpad(g.nth) + 1;
   const int FS = (kMRJ + 2) * g.nth, FSP = (FS + 15) & ~15;
   const int SPL = ((SPN + 15) & ~15) + 8;
-  const size_t sm = sizeof(double) * ((size_t)kQRing * 3 * FSP + kTB * 3 * kMRJ * SPL + 2 * kMRJ * 3 * SPN);
+  const size_t sm = sizeof(double) * ((size_t)kQRing * 3 * FSP + kTB * 3 * kMRJ * SPL + 2 * kMRJ * 3 * SPL);
   if (sm > 110 * 1024) return cudaErrorNotSupported;  // two CTAs per SM
   auto kern = k_rhs_march<E, CPT, T, NT>;
   cudaError_t e = allow_dyn_smem(kern, sm);

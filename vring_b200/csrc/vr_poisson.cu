@@ -442,14 +442,39 @@ __device__ __forceinline__ void pair_fft16(double (&re)[16], double (&im)[16], c
       im[jb] = ai - bi;
     }
   }
+  if constexpr (T == 8) {
+    // k = 2 t + u + 16 k2: with the same u, lanes t and t + 4 would meet one
+    // bank group, so the upper half of the pair's quarter warp writes the
+    // other u in the same instruction
 #pragma unroll
-  for (int u = 0; u < G; u++)
+    for (int u0 = 0; u0 < 2; u0++)
 #pragma unroll
-    for (int k2 = 0; k2 < T; k2++) {
-      const int k = t * G + u + 16 * k2;
-      sc[k] = make_double2(re[u * T + brev_c(k2, LT)], im[u * T + brev_c(k2, LT)]);
-    }
+      for (int k2 = 0; k2 < T; k2++) {
+        const bool hi = t >= 4;
+        const int u = u0 ^ (int)hi, b = brev_c(k2, LT);
+        const double vr = hi ? re[(1 - u0) * T + b] : re[u0 * T + b];
+        const double vi = hi ? im[(1 - u0) * T + b] : im[u0 * T + b];
+        sc[t * G + u + 16 * k2] = make_double2(vr, vi);
+      }
+  } else {
+#pragma unroll
+    for (int u = 0; u < G; u++)
+#pragma unroll
+      for (int k2 = 0; k2 < T; k2++) {
+        const int k = t * G + u + 16 * k2;
+        sc[k] = make_double2(re[u * T + brev_c(k2, LT)], im[u * T + brev_c(k2, LT)]);
+      }
+  }
   __syncwarp(gm);
+}
+
+// Slot of packed entry n of the inverse transform's staged pair: for T = 8
+// bit 3 of n flips bit 0, so the writes of 8 consecutive entries and the
+// reads of entries 2k - 1 and 2k (stride 2 over a quarter warp) both meet
+// eight distinct 16-byte bank groups.
+template <int T>
+__device__ __forceinline__ int fft_packed_slot(int n) {
+  return T == 8 ? n ^ ((n >> 3) & 1) : n;
 }
 
 // the block's copy of the lane twiddles: twl[(k1 - 1) T + t] = W_N^{t k1}
@@ -526,9 +551,10 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
   const unsigned gm = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((tid & 31) / T * T));
   const bool hasb = la + 1 < nlines;
   const double *pa = in + (size_t)la * N, *pb = pa + N;
-  // the two packed lines side by side: sc[n] = (a[n], b[n])
+  // the two packed lines side by side: entry n = (a[n], b[n])
 #pragma unroll
-  for (int j = 0; j < 16; j++) sc[t + T * j] = make_double2(pa[t + T * j], hasb ? pb[t + T * j] : 0.0);
+  for (int j = 0; j < 16; j++)
+    sc[fft_packed_slot<T>(t + T * j)] = make_double2(pa[t + T * j], hasb ? pb[t + T * j] : 0.0);
   __syncwarp(gm);
   // Z_k = A_k + i B_k from the packed Hermitian spectra, conjugated: the
   // inverse transform runs as conj(DFT(conj Z)) (fastfouriertransform.F90:49-87)
@@ -539,17 +565,17 @@ __global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in
     const int kk = k <= N / 2 ? k : N - k;
     double ar, ai, br, bi;
     if (kk == 0) {
-      const double2 v = sc[0];
+      const double2 v = sc[fft_packed_slot<T>(0)];
       ar = v.x;
       ai = 0.0;
       br = v.y;
       bi = 0.0;
     } else {
-      const double2 c1 = sc[2 * kk - 1];
+      const double2 c1 = sc[fft_packed_slot<T>(2 * kk - 1)];
       ar = c1.x / 2.0;
       br = c1.y / 2.0;
       if (2 * kk < N) {
-        const double2 s1 = sc[2 * kk];
+        const double2 s1 = sc[fft_packed_slot<T>(2 * kk)];
         ai = -1.0 * s1.x / 2.0;
         bi = -1.0 * s1.y / 2.0;
       } else {
