@@ -271,8 +271,9 @@ __device__ __noinline__ void ls_more(const PartCoef *__restrict__ Cg, int nth, i
 // fit and the transform run in float and stop after the first pass, which is
 // the exact least-squares solution (the reference's further passes correct
 // rounding, below float resolution).  With FULL false the further passes are
-// not taken: need is set instead and the outputs are not to be used.
-template <class R, bool FULL = true>
+// not taken: need is set instead and the outputs are not to be used.  With
+// DERIV false only ff (row 0) is written: the value, without the derivatives.
+template <class R, bool FULL = true, bool DERIV = true>
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
                                                double y, double z, R (*cv)[kPartPerBlock], int p,
                                                int (&cell)[3], double &r, double &theta, double &sn,
@@ -379,6 +380,15 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   const R tp = (R)dtp, rp = (R)drp, zp = (R)dzp, two = 2;
   const R ff = (R)((double)(tp * a[0] + rp * a[1] + zp * a[2] + tp * tp * a[3] + tp * rp * a[4] + rp * rp * a[5] +
                             rp * zp * a[6] + zp * zp * a[7] + zp * tp * a[8]) + y0);
+  if constexpr (!DERIV) {
+    const double ir1d = 1.0 / r;
+    cs = x * ir1d;
+    sn = y * ir1d;
+    ir1o = ir1d;
+    ir2o = 1.0 / (r * r);
+    cv[13 * kd][p] = ff;
+    return;
+  }
   const R ft = a[0] + two * tp * a[3] + rp * a[4] + zp * a[8];
   const R fr = a[1] + tp * a[4] + two * rp * a[5] + zp * a[6];
   const R fz = a[2] + rp * a[6] + two * zp * a[7] + tp * a[8];
@@ -419,10 +429,21 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
 // Row id of the Cartesian velocity, gradient and Hessian from the three
 // fitted components (part_tools.F90:730-797), in the reference's summation
 // order over components.
-template <class R>
+template <class R, bool DERIV = true>
 __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d, double ir1d, double ir2d, int id,
                                               const R (*cv)[kPartPerBlock], int p, R &vel, R (&dvel)[3],
                                               R (&ddvel)[3][3]) {
+  if constexpr (!DERIV) {  // the velocity alone, in the same order as below
+    const R sn = (R)sn_d, cs = (R)cs_d, zero = 0, one = 1;
+    const R nm0 = id == 0 ? -sn : (id == 1 ? cs : zero);
+    const R nm1 = id == 0 ? cs : (id == 1 ? sn : zero);
+    const R nm2 = id == 2 ? one : zero;
+    vel = 0;
+    vel = vel + cv[0][p] * nm0;
+    vel = vel + cv[13][p] * nm1;
+    vel = vel + cv[26][p] * nm2;
+    return;
+  }
   // 1/rsd and 1/rsd^2 with rsd = max(r, 1e-6): the component fit's 1/r and
   // 1/r^2 (the same divisions) except next to the axis
   const double rsd = r > (double)0.000001f ? r : (double)0.000001f;
@@ -530,8 +551,11 @@ constexpr int kPartRemoved = 1, kPartDeferred = 2;
 // the reference leaves after the call.  A deferring block writes the
 // positions it has reached first.  The inertial ODE rows 4-78 are written at
 // every substep.  At the last substep warp 0 records the particle's cell
-// bucket in key[] for the next call's walk order.
-template <class R, bool FIX>
+// bucket in key[] for the next call's walk order.  DERIV false (tracers,
+// main launch, substeps before the last) fits and transforms the velocity
+// alone: a tracer moves with the velocity, and only the last substep stores
+// the gradient and Hessian.
+template <class R, bool FIX, bool DERIV = true>
 __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__restrict__ q1,
                                             const double *__restrict__ q2, const double *__restrict__ q3,
                                             double *__restrict__ u, double *__restrict__ v,
@@ -548,8 +572,8 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
     const double px = carry ? S.pos[0][p] : u[PUo(ip, 1)], py = carry ? S.pos[1][p] : u[PUo(ip, 2)],
                  pz = carry ? S.pos[2][p] : u[PUo(ip, 3)];
     int cell[3];
-    part_component<R, FIX>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn, cs,
-                           ir1, ir2, need);
+    part_component<R, FIX, DERIV>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn,
+                                  cs, ir1, ir2, need);
     if (!FIX && last && w == 0 && key) {
       const int jb = ((P.g.nr + 2) >> 2) + 1;
       key[ip - 1] = cell[2] * jb + (cell[1] >> 2);
@@ -575,8 +599,8 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
   double pw = 0.0;
   bool removed = false;
   if (live) {
-    R vr_, dvr[3], ddvr[3][3];
-    part_cart_row<R>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
+    R vr_, dvr[3] = {}, ddvr[3][3] = {};
+    part_cart_row<R, DERIV>(r, sn, cs, ir1, ir2, w, S.cv, p, vr_, dvr, ddvr);
     const double vel = vr_;
     double dvel[3], ddvel[3][3];
 #pragma unroll
@@ -683,8 +707,13 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
     if (w == 0 && !live && ip >= 1 && ip <= nlast) key[ip - 1] = (P.g.nz + 2) * (((P.g.nr + 2) >> 2) + 1);
 #pragma unroll 1
     for (int s = 0; s < nsub; s++) {
-      const int st = part_advance<R, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode, inv_st,
-                                            partdt, serial0 + s, nremoved, S, s == 0, s == nsub - 1, key);
+      const bool velocity_only = mode == 1 && s < nsub - 1;  // the same in every thread
+      const int st = velocity_only
+                         ? part_advance<R, false, false>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode,
+                                                         inv_st, partdt, serial0 + s, nremoved, S, s == 0, false, key)
+                         : part_advance<R, false, true>(P, q1, q2, q3, u, v, isfre, gone, naloc, ip, live, mode,
+                                                        inv_st, partdt, serial0 + s, nremoved, S, s == 0,
+                                                        s == nsub - 1, key);
       if (st == kPartDeferred) {  // the same in every thread of the block
         if (w == 0 && live) {
           const int k = atomicAdd(defer_n + par, 1);
