@@ -209,6 +209,19 @@ __device__ __forceinline__ void ls_pass(const PartCoef &C, const double (&y)[27]
 
 constexpr int kPartPerBlock = 32;
 
+// The first-pass coefficients of a component's fit depend on the 27 samples
+// around the particle's cell only, not on where the particle sits in it: the
+// main launch keeps them per (component, particle) with the centre sample
+// and the cell they belong to, and a later substep in the same cell reuses
+// them instead of gathering and fitting again (same samples, same
+// arithmetic, same bits).  Each entry is read and written by its own thread.
+template <class R>
+struct PartFitCache {
+  R a[9][3][kPartPerBlock];
+  double y0[3][kPartPerBlock];
+  int cell[3][kPartPerBlock];  // packed cell index, -1: empty
+};
+
 // R: arithmetic of the fit and the transforms (double; float in the mixed form)
 template <class R>
 struct PartShared {
@@ -216,6 +229,7 @@ struct PartShared {
   double jac[9][kPartPerBlock];   // old Jacobian, m + 3 j
   double hes[27][kPartPerBlock];  // old Hessian, m + 3 j + 9 k
   double pos[3][kPartPerBlock];   // new position
+  PartFitCache<R> fc;             // main launch only
 };
 
 // The 27-point stencil of one component: theta columns (periodic), clamped
@@ -277,7 +291,8 @@ template <class R, bool FULL = true, bool DERIV = true>
 __device__ __forceinline__ void part_component(const PartGeo &P, const double *__restrict__ q, int kd, double x,
                                                double y, double z, R (*cv)[kPartPerBlock], int p,
                                                int (&cell)[3], double &r, double &theta, double &sn,
-                                               double &cs, double &ir1o, double &ir2o, bool &need) {
+                                               double &cs, double &ir1o, double &ir2o, bool &need,
+                                               PartFitCache<R> *fc = nullptr) {
   constexpr bool DBL = std::is_same<R, double>::value;
   need = false;
   int it, ir, iz;
@@ -290,6 +305,16 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   cell[0] = it;
   cell[1] = ir;
   cell[2] = iz;
+  const int ckey = it + (P.g.nth + 2) * (ir + (P.g.nr + 3) * iz);
+  R a[9];
+  double y0;
+  if (fc && fc->cell[kd][p] == ckey) {
+    // a cached fit passed the main launch's test (a block with a particle
+    // that needs the full iteration defers before its next substep)
+#pragma unroll
+    for (int i = 0; i < 9; i++) a[i] = fc->a[i][kd][p];
+    y0 = fc->y0[kd][p];
+  } else {
   Stencil T;
 #pragma unroll
   for (int f = -1; f <= 1; f++) {
@@ -312,8 +337,7 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
   }
   // First pass of the fit (mp = mint y from a = 0), accumulated while the
   // samples arrive; y_k = sample_k - y0 is not kept.
-  const double y0 = stencil_sample(P.g.nth, P.g.J3, q, kd, T, 1, 1, 1);
-  R a[9];
+  y0 = stencil_sample(P.g.nth, P.g.J3, q, kd, T, 1, 1, 1);
 #pragma unroll
   for (int i = 0; i < 9; i++) a[i] = 0;
   double ym = 0.0;
@@ -360,6 +384,13 @@ __device__ __forceinline__ void part_component(const PartGeo &P, const double *_
       for (int i = 0; i < 9; i++) a[i] = at[i];
     }
   }
+  if (fc) {
+#pragma unroll
+    for (int i = 0; i < 9; i++) fc->a[i][kd][p] = a[i];
+    fc->y0[kd][p] = y0;
+    fc->cell[kd][p] = ckey;
+  }
+  }  // fit
   double dtp, drp, dzp;
   if (kd == 0) {
     dtp = theta - __ldg(P.thc + it);
@@ -573,7 +604,7 @@ __device__ __forceinline__ int part_advance(const PartGeo &P, const double *__re
                  pz = carry ? S.pos[2][p] : u[PUo(ip, 3)];
     int cell[3];
     part_component<R, FIX, DERIV>(P, w == 0 ? q1 : (w == 1 ? q2 : q3), w, px, py, pz, S.cv, p, cell, r, theta, sn,
-                                  cs, ir1, ir2, need);
+                                  cs, ir1, ir2, need, FIX ? nullptr : &S.fc);
     if (!FIX && last && w == 0 && key) {
       const int jb = ((P.g.nr + 2) >> 2) + 1;
       key[ip - 1] = cell[2] * jb + (cell[1] >> 2);
@@ -705,6 +736,7 @@ __global__ void __launch_bounds__(96, VR_PART_MINB) k_iter_part(PartGeo P, const
     const int ip = t < nsorted ? perm[t] : t + 1;
     bool live = ip >= 1 && ip <= nlast && isfre[ip - 1] == 0;
     if (w == 0 && !live && ip >= 1 && ip <= nlast) key[ip - 1] = (P.g.nz + 2) * (((P.g.nr + 2) >> 2) + 1);
+    S.fc.cell[w][p] = -1;  // this thread's own entry
 #pragma unroll 1
     for (int s = 0; s < nsub; s++) {
       const bool velocity_only = mode == 1 && s < nsub - 1;  // the same in every thread
