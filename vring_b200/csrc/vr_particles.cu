@@ -554,9 +554,11 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 // removal (:962-987).  The fields do not change during the call and every
 // particle's update reads only its own state, so a block runs all substeps
 // of its 32 particles in turn (the reference runs each substep over all
-// particles): the results are the same, and the stencil samples of a
-// particle's later substeps are still in this SM's L1.  Removals carry the
-// serial of their substep.
+// particles): the results are the same, and a later substep whose particle
+// is still in the same cell takes the fit's coefficients from the block's
+// cache (PartFitCache) instead of gathering the 27 samples again (the
+// stencils of a SM's resident blocks, about 660 KB, do not stay in L1).
+// Removals carry the serial of their substep.
 //
 // The FP64 fit stops after its first pass unless the samples are large
 // enough for the reference's second pass to matter (ls_more).  When a particle
