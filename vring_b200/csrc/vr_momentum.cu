@@ -1276,11 +1276,20 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const C
     const int v = along_r ? c->tune_r : c->tune_z;
     const int ldim = along_r ? 1 : 2;
     cudaError_t e = cudaErrorNotSupported;
+    // chunks of 16 when the line fits them (256 / 512 positions): one
+    // substitution step less on every thread's dependent chain than 17
     if (v == 2) {
-    } else if ((v == 0) == along_r)
-      e = run_chunk_tma<16, 16, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
-    else
-      e = run_chunk_tma<8, 32, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+    } else if ((v == 0) == along_r) {
+      if (p.n <= 16 * 16)
+        e = run_chunk_tma<16, 16, 16, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+      else
+        e = run_chunk_tma<16, 16, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+    } else {
+      if (p.n <= 32 * 16)
+        e = run_chunk_tma<8, 32, 16, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+      else
+        e = run_chunk_tma<8, 32, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+    }
     if (e != cudaErrorNotSupported) return e;
     return launch_chunk(p, p.nbx * nm2, c->stream);
   }

@@ -1376,7 +1376,9 @@ cudaError_t launch_poisson(vr_ctx *c) {
     p.nm = g.nth / 2 + 1;
     p.nbx = (N + 31) / 32;
     LaunchScope ls(c, PK_RADIAL);
-    e = run_chunk_tma<16, 16, 17, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream);
+    e = g.nr <= 16 * 16
+            ? run_chunk_tma<16, 16, 16, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream)
+            : run_chunk_tma<16, 16, 17, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream);
     if (e == cudaErrorNotSupported) e = launch_chunk(p, p.nbx * g.nz, c->stream);
     if (e) return e;
   } else if (g.nr <= 640)
