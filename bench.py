@@ -359,7 +359,17 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="issue the warm-up substeps launch by launch instead of replaying CUDA graphs "
                          "(the same kernels in the same order; for profiler launch lists)")
+    ap.add_argument("--no-vr2d", action="store_true", help="skip the VR2D Krylov solves")
+    ap.add_argument("--no-particles-alone", action="store_true",
+                    help="skip the particle classes timed alone (inertial class, walk orders)")
+    ap.add_argument("--step-only", action="store_true",
+                    help="the headline step alone: implies --no-cpu-baseline --no-mixed --no-ensemble "
+                         "--no-vr2d --no-particles-alone --e2e-steps 0 (for profiler launch lists)")
     args = ap.parse_args()
+    if args.step_only:
+        args.no_cpu_baseline = args.no_mixed = args.no_ensemble = True
+        args.no_vr2d = args.no_particles_alone = True
+        args.e2e_steps = 0
     global NR, NTH, NZ, NPART, WORKLOAD
     if args.grid is not None or args.nparticles is not None:
         if args.grid is not None:
@@ -561,7 +571,7 @@ def main():
     ensemble = None
     if not args.no_ensemble and not reduced and world == 1:
         ensemble = ensemble_bench(local, 5)
-    vr2d = vr2d_bench() if not reduced and world == 1 else None
+    vr2d = vr2d_bench() if not reduced and world == 1 and not args.no_vr2d else None
 
     # ---- roofline of the dominant kernel family -------------------------------
     peak, peak_kind = peaks()
@@ -579,7 +589,7 @@ def main():
     # the reference's inertial particles (class 1: Stokes drag, the 117-word
     # state with Jacobian and Hessian rates; part_tools.F90:241-251, 847-870)
     # on the same field and cloud, timed alone over a few iter_part calls
-    if not reduced:
+    if not reduced and not args.no_particles_alone:
         particles["inertial"] = inertial_bench(run, stream, e0, e1)
         # the tracers alone, walked in slot order (the default) and in cell order
         particles["alone_ms_per_step"] = {
