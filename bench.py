@@ -407,8 +407,10 @@ def main():
     if args.no_graphs:
         run.set_graphs(False)
     ncell = NTH * NR * NZ
-    # the sweep tile shapes the autotuner picks for this grid (state restored)
-    tiles = V.autotune(run)
+    # the sweep tile shapes the autotuner picks for this grid (state restored);
+    # a profiler launch list (--step-only) keeps the default shapes, so that
+    # it holds the step's launches only
+    tiles = (0, 0) if args.step_only else V.autotune(run)
 
     for _ in range(args.warmup):
         run.iterate(1)
