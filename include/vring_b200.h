@@ -354,7 +354,7 @@ typedef struct vr_k2d_desc {
   int32_t flags;        /* reserved, 0                                        */
 } vr_k2d_desc;
 enum vr_krylov {
-  VR_KRYLOV_CG = 0,           /* plain CG on S x = V f (the judge)            */
+  VR_KRYLOV_CG = 0,           /* plain CG on S x = V f (the fallback)         */
   VR_KRYLOV_PCG_JACOBI = 1,   /* CG with the inverse diagonal of S            */
   VR_KRYLOV_BICGSTAB = 2,     /* BiCGSTAB on K x = f                          */
   VR_KRYLOV_FCG_LEARNED = 3,  /* flexible CG, preconditioner = the vr_unet set

@@ -5,7 +5,8 @@
 // preconditioner (vr_unet.cu).  A direct solve (z DCT-II, one radial
 // tridiagonal per z mode, DCT-III: the reference's fftp method at Ntheta = 1,
 // poisson_solve.F90:140-179, 270-323, generalised to stretched radial faces)
-// judges the Krylov answers and generates training pairs.
+// is the reference the Krylov answers are checked against, and generates
+// training pairs.
 //
 // Operator (cell centres (rm_j, zm_k), vectors stored r fastest, i = j + nr k):
 //   S x = aw_j (x - x_{j-1}) + ae_j (x - x_{j+1}) + az_j (2x - x_{k-1} - x_{k+1})
