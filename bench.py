@@ -486,6 +486,27 @@ def main():
 
         e2e_run(False)  # the staging buffers are allocated on first use
         e2e_s = e2e_run(False)
+
+        def copies_only_s(reps=5):
+            """the same bytes each way with no step: both directions at once,
+            in 4 pieces per field on the same two streams (the link's floor)"""
+            dst = [torch.empty(p.numel(), dtype=torch.float64, device="cuda") for p in pin_in[0]]
+            src = [torch.zeros(p.numel(), dtype=torch.float64, device="cuda") for p in pin_in[0]]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                for p_in, p_out, d, sd in zip(pin_in[0], pin_out[1], dst, src):
+                    m = p_in.numel()
+                    for q_ in range(4):
+                        b_, e_ = m * q_ // 4, m * (q_ + 1) // 4
+                        with torch.cuda.stream(h2d):
+                            d[b_:e_].copy_(p_in[b_:e_], non_blocking=True)
+                        with torch.cuda.stream(d2h):
+                            p_out[b_:e_].copy_(sd[b_:e_], non_blocking=True)
+            torch.cuda.synchronize()
+            return (time.perf_counter() - t0) / reps
+
+        copy_s = copies_only_s()
         for p, src in zip(pin_out[0], pin_in[0]):
             p.copy_(src)
         rt_s = e2e_run(True)
@@ -499,6 +520,12 @@ def main():
                        "through the library's staging buffers, so the copies of neighbouring steps "
                        "overlap the step); pressure, RK history and particle state stay resident; "
                        "host wall clock, device synchronised at both ends",
+               "copies_alone": {
+                   "ms_per_step": copy_s * 1e3,
+                   "value_if_the_step_were_free": replicas.throughput(ncell, world, copy_s) / 1e6,
+                   "gb_s_per_direction": bytes_q / copy_s / 1e9,
+                   "what": "the same host<->device bytes with no step, both directions at once: the "
+                           "PCIe floor of the end-to-end loop"},
                "round_trip": {
                    "value": replicas.throughput(ncell * args.e2e_steps, world, rt_s) / 1e6, "unit": UNIT,
                    "what": "the same, with every step's input the previous step's result in the same "
