@@ -52,12 +52,15 @@ WORDS_PER_CELL_STEP = 3 * sum(WORDS.values())  # 198 words = 1584 B
 def family_words(fam, prof):
     """Algorithmic words per cell and substep of a timed kernel family, with the
     phases fused into it: the fused right-hand side also solves the theta
-    lines (tsweep), the fused pressure update also runs upsol."""
+    lines (tsweep), the fused pressure update also runs upsol, the forward
+    theta transform of the fused substep also takes divq."""
     w = WORDS[fam]
     if fam == "rhs" and "tsweep" not in prof:
         w += WORDS["tsweep"]
     if fam == "uppres" and "upsol" not in prof:
         w += WORDS["upsol"]
+    if fam == "fft" and "divq" not in prof:
+        w += WORDS["divq"]
     return w
 
 

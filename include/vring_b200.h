@@ -86,6 +86,9 @@ typedef struct vr_desc {
  *   ghosted 3-D  (nth, 0:nr+2, 0:nz+2): Q1..Q3, DQ1..DQ3, RU1..RU3, PRES
  *   PRG          (nth, nr, nz, 3)
  *   RHS          (nth, nr, nz)        -- divq output / Poisson right-hand side
+ *                                          (vr_divq; the fused substep takes
+ *                                          divq inside its theta transform for
+ *                                          nth 32..256 and leaves RHS alone)
  *   DPH          (nth, 0:nr+1, 0:nz+1)
  *   2-D          (nth, 1:nr+1): CORR3S, CORR3N, CSORT, TCONV
  *                (nth, 0:nr+2): DQ3NO                                         */

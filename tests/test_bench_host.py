@@ -26,6 +26,9 @@ def test_family_words_of_fused_kernels():
     assert bench.family_words("rhs", apart) == 15
     assert bench.family_words("uppres", apart) == 9
     assert bench.family_words("zsweep", fused) == 8
+    # the forward theta transform takes divq from dq when divq is not timed apart
+    assert bench.family_words("fft", {"fft": (1.0, 6)}) == 4 + 4
+    assert bench.family_words("fft", {"fft": (1.0, 6), "divq": (1.0, 3)}) == 4
 
 
 def test_roofline_of_the_dominant_field_family():

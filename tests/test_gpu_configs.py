@@ -127,7 +127,9 @@ def test_long_theta_and_z_lines_match_oracle():
     prep(orc, gpu, 1, 0.0, 0)
     orc.substep(1)
     gpu.substep(1)
-    for n in STATE + ["dph", "rhs"]:
+    # (the fused substep takes divq inside the theta transform and leaves the
+    # rhs array alone; dph is the Poisson solve of that right-hand side)
+    for n in STATE + ["dph"]:
         assert_field_close(gpu, orc, n, rel=1e-11)
     gpu.close()
 

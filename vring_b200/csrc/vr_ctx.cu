@@ -1008,8 +1008,12 @@ int vr::enqueue_substep(vr_ctx *c, int irk) {
     VR_CUDA(c, fe);
     VR_CUDA(c, sweeps(c, true));
   }
-  VR_CUDA(c, launch_divq(c, rk));
-  VR_CUDA(c, launch_poisson(c));
+  if (poisson_takes_dq(c)) {  // divq inside the forward theta transform
+    VR_CUDA(c, launch_poisson(c, &rk));
+  } else {
+    VR_CUDA(c, launch_divq(c, rk));
+    VR_CUDA(c, launch_poisson(c));
+  }
   VR_CUDA(c, launch_upsol_uppres(c, rk));
   return VR_OK;
 }

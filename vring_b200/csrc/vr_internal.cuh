@@ -52,6 +52,23 @@ __host__ __device__ inline int IDP(const Geo &g, int i, int j, int k) {
   return (i - 1) + g.nth * (j + (g.nr + 2) * k);
 }
 __host__ __device__ inline int I2O(const Geo &g, int i, int j) { return (i - 1) + g.nth * (j - 1); }
+
+// divq at cell (ic, jc, kc) (divergence.F90:16-67): -div(dq) / (alpha dt),
+// taken in double from the stored dq (T: double, or float in the mixed form).
+// One expression for the divq kernel and for the theta transform that takes
+// its input straight from dq, so both give the same bits.
+template <class T>
+__device__ __forceinline__ double divq_at(const Geo &g, double inv_adt, const T *__restrict__ dq1,
+                                          const T *__restrict__ dq2, const T *__restrict__ dq3, int ic, int jc,
+                                          int kc) {
+  const int ip = ic < g.nth ? ic + 1 : 1;
+  const int o = I3(g, ic, jc, kc);
+  const double irm = __ldg(g.irm + jc);
+  const double d = ((double)__ldg(dq1 + I3(g, ip, jc, kc)) - (double)__ldg(dq1 + o)) * g.dx1 * g.axsym * irm +
+                   ((double)__ldg(dq2 + o + g.nth) - (double)__ldg(dq2 + o)) * g.dx2 * irm +
+                   ((double)__ldg(dq3 + o + g.pl) - (double)__ldg(dq3 + o)) * g.dx3;
+  return -d * inv_adt;
+}
 __host__ __device__ inline int I2Z(const Geo &g, int i, int j) { return (i - 1) + g.nth * j; }
 
 // asynchronous 8-byte global -> shared copies (cp.async, sm_80+): a CTA puts
@@ -259,7 +276,11 @@ cudaError_t launch_tsweep(vr_ctx *c, int comp);
 cudaError_t launch_rsweep(vr_ctx *c, int comp);
 cudaError_t launch_zsweep(vr_ctx *c, int comp);
 cudaError_t launch_divq(vr_ctx *c, const Rk &rk);
-cudaError_t launch_poisson(vr_ctx *c);
+// with div_rk set and a theta extent of 32..256, the forward theta transform
+// computes divq from dq itself (the rhs array is not written); see
+// poisson_takes_dq
+cudaError_t launch_poisson(vr_ctx *c, const Rk *div_rk = nullptr);
+bool poisson_takes_dq(const vr_ctx *c);
 cudaError_t launch_upsol(vr_ctx *c, const Rk &rk);
 cudaError_t launch_uppres(vr_ctx *c, const Rk &rk);
 cudaError_t launch_upsol_uppres(vr_ctx *c, const Rk &rk);

@@ -486,9 +486,19 @@ __device__ __forceinline__ void load_lane_twiddles(double2 *twl, const double *_
   }
 }
 
-template <int T>
+// the input of the forward transform taken straight from dq: divq of the
+// fused substep (divergence.F90:16-67), the same values the divq kernel
+// would have stored
+template <class TQ>
+struct DivSrc {
+  Geo g;
+  double inv_adt;
+  const TQ *dq1, *dq2, *dq3;
+};
+
+template <int T, class TQ = double, bool DIV = false>
 __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in, double *__restrict__ out,
-                                                   int nlines, const double *__restrict__ tw) {
+                                                   int nlines, const double *__restrict__ tw, DivSrc<TQ> dv) {
   constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
   extern __shared__ double2 smv[];
   double2 *twl = smv;
@@ -500,12 +510,23 @@ __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in
   if (la >= nlines) return;  // no CTA barrier follows; the pair's group leaves together
   const unsigned gm = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((tid & 31) / T * T));
   const bool hasb = la + 1 < nlines;
-  const double *pa = in + (size_t)la * N, *pb = pa + N;
   double re[16], im[16];
+  if constexpr (DIV) {
+    // line la is the theta line (j, k) = (1 + la % nr, 1 + la / nr)
+    const int nr = dv.g.nr, ja = 1 + la % nr, ka = 1 + la / nr;
+    const int jb = 1 + (la + 1) % nr, kb = 1 + (la + 1) / nr;
 #pragma unroll
-  for (int m = 0; m < 16; m++) {
-    re[m] = pa[t + T * m];
-    im[m] = hasb ? pb[t + T * m] : 0.0;
+    for (int m = 0; m < 16; m++) {
+      re[m] = divq_at(dv.g, dv.inv_adt, dv.dq1, dv.dq2, dv.dq3, t + T * m + 1, ja, ka);
+      im[m] = hasb ? divq_at(dv.g, dv.inv_adt, dv.dq1, dv.dq2, dv.dq3, t + T * m + 1, jb, kb) : 0.0;
+    }
+  } else {
+    const double *pa = in + (size_t)la * N, *pb = pa + N;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      re[m] = pa[t + T * m];
+      im[m] = hasb ? pb[t + T * m] : 0.0;
+    }
   }
   pair_fft16<T>(re, im, twl, sc, t, gm);
   // packed [a0, a1, b1, ...] of both lines (fastfouriertransform.F90:34-43):
@@ -1257,7 +1278,7 @@ static cudaError_t run_fft_w(vr_ctx *c, int dir) {
 }
 
 template <int T>
-static cudaError_t run_fft_s(vr_ctx *c, int dir) {
+static cudaError_t run_fft_s(vr_ctx *c, int dir, const Rk *div_rk = nullptr) {
   const Geo &g = c->geo;
   constexpr int NPB = 128 / T, PS = fft_pair_stride(T);
   const int nlines = g.nr * g.nz;
@@ -1265,9 +1286,23 @@ static cudaError_t run_fft_s(vr_ctx *c, int dir) {
   const int npairs = (nlines + 1) / 2, blocks = (npairs + NPB - 1) / NPB;
   cudaError_t e;
   LaunchScope ls(c, PK_FFT);
-  if (dir > 0) {
+  if (dir > 0 && div_rk) {
+    const double inv_adt = 1.0 / (div_rk->alm * g.dt);
+    if (c->mixed) {
+      auto kern = k_fft_fwd_s<T, float, true>;
+      if ((e = allow_dyn_smem(kern, sm))) return e;
+      DivSrc<float> dv{g, inv_adt, reinterpret_cast<const float *>(c->dq[0]),
+                       reinterpret_cast<const float *>(c->dq[1]), reinterpret_cast<const float *>(c->dq[2])};
+      kern<<<blocks, 128, sm, c->stream>>>(nullptr, c->spec, nlines, c->tw_th, dv);
+    } else {
+      auto kern = k_fft_fwd_s<T, double, true>;
+      if ((e = allow_dyn_smem(kern, sm))) return e;
+      DivSrc<double> dv{g, inv_adt, c->dq[0], c->dq[1], c->dq[2]};
+      kern<<<blocks, 128, sm, c->stream>>>(nullptr, c->spec, nlines, c->tw_th, dv);
+    }
+  } else if (dir > 0) {
     if ((e = allow_dyn_smem(k_fft_fwd_s<T>, sm))) return e;
-    k_fft_fwd_s<T><<<blocks, 128, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th);
+    k_fft_fwd_s<T><<<blocks, 128, sm, c->stream>>>(c->rhs, c->spec, nlines, c->tw_th, DivSrc<double>{});
   } else {
     if ((e = allow_dyn_smem(k_fft_bwd_s<T>, sm))) return e;
     k_fft_bwd_s<T><<<blocks, 128, sm, c->stream>>>(c->spec, c->dph, g, nlines, c->tw_th);
@@ -1275,13 +1310,18 @@ static cudaError_t run_fft_s(vr_ctx *c, int dir) {
   return cudaGetLastError();
 }
 
-static cudaError_t fft_warp_dispatch(vr_ctx *c, int dir, bool *done) {
+bool poisson_takes_dq(const vr_ctx *c) {
+  const int n = c->geo.nth;
+  return n == 32 || n == 64 || n == 128 || n == 256;
+}
+
+static cudaError_t fft_warp_dispatch(vr_ctx *c, int dir, bool *done, const Rk *div_rk = nullptr) {
   *done = true;
   switch (c->geo.nth) {
-    case 32: return run_fft_s<2>(c, dir);
-    case 64: return run_fft_s<4>(c, dir);
-    case 128: return run_fft_s<8>(c, dir);
-    case 256: return run_fft_s<16>(c, dir);
+    case 32: return run_fft_s<2>(c, dir, div_rk);
+    case 64: return run_fft_s<4>(c, dir, div_rk);
+    case 128: return run_fft_s<8>(c, dir, div_rk);
+    case 256: return run_fft_s<16>(c, dir, div_rk);
     case 512: return run_fft_w<16>(c, dir);
     case 1024: return run_fft_w<32>(c, dir);
     default: *done = false; return cudaSuccess;
@@ -1334,13 +1374,14 @@ static cudaError_t dct_warp_dispatch(vr_ctx *c, int dir, bool *done) {
   }
 }
 
-cudaError_t launch_poisson(vr_ctx *c) {
+cudaError_t launch_poisson(vr_ctx *c, const Rk *div_rk) {
   const Geo &g = c->geo;
   cudaError_t e;
   const int N = g.nth, nlines = g.nr * g.nz;
-  // theta forward: rhs -> spec
+  if (div_rk && !poisson_takes_dq(c)) return cudaErrorInvalidValue;  // the caller runs divq first
+  // theta forward: rhs (or divq of dq) -> spec
   bool done = false;
-  if ((e = fft_warp_dispatch(c, +1, &done))) return e;
+  if ((e = fft_warp_dispatch(c, +1, &done, div_rk))) return e;
   if (done) {
   } else if (is_pow2(N)) {
     int lpb = N >= 1024 ? 1 : 1024 / N;

@@ -32,13 +32,7 @@ __global__ void k_divq(Geo g, double inv_adt, const T *__restrict__ dq1, const T
   int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   int kc = 1 + blockIdx.z;
   if (ic > g.nth || jc > g.nr) return;
-  int ip = ic < g.nth ? ic + 1 : 1;
-  int o = I3(g, ic, jc, kc);
-  double irm = g.irm[jc];
-  double d = (ldv(dq1 + I3(g, ip, jc, kc)) - ldv(dq1 + o)) * g.dx1 * g.axsym * irm +
-             (ldv(dq2 + o + g.nth) - ldv(dq2 + o)) * g.dx2 * irm +
-             (ldv(dq3 + o + g.pl) - ldv(dq3 + o)) * g.dx3;
-  rhs[IRS(g, ic, jc, kc)] = -d * inv_adt;
+  rhs[IRS(g, ic, jc, kc)] = divq_at(g, inv_adt, dq1, dq2, dq3, ic, jc, kc);
 }
 
 cudaError_t launch_divq(vr_ctx *c, const Rk &rk) {
