@@ -122,7 +122,9 @@ def test_fused_substep_matches_routine_sequence(grid, wth):
     prep(orc, gpu, 1, 2e-3, 0)
     orc.substep(1)
     gpu.substep(1)
-    for n in STATE + ["dph", "rhs"]:
+    # the fused substep takes divq inside the forward theta transform and
+    # leaves the rhs array alone; dph is the Poisson solve of that divq
+    for n in STATE + ["dph"]:
         assert_field_close(gpu, orc, n, rel=1e-11)
 
 
@@ -195,7 +197,9 @@ def test_production_transform_sizes(wth):
     prep(orc, gpu, 1, 5e-4, 0)
     orc.substep(1)
     gpu.substep(1)
-    for n in STATE + ["dph", "rhs"]:
+    # the fused substep takes divq inside the forward theta transform and
+    # leaves the rhs array alone; dph is the Poisson solve of that divq
+    for n in STATE + ["dph"]:
         assert_field_close(gpu, orc, n, rel=1e-11)
 
 
