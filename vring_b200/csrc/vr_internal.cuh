@@ -57,17 +57,22 @@ __host__ __device__ inline int I2O(const Geo &g, int i, int j) { return (i - 1) 
 // taken in double from the stored dq (T: double, or float in the mixed form).
 // One expression for the divq kernel and for the theta transform that takes
 // its input straight from dq, so both give the same bits.
+// from dq1 at theta+1 and at the cell, dq2 at r+1 and at the cell, dq3 at
+// z+1 and at the cell, and 1/r_m of the row
+__device__ __forceinline__ double divq_of(const Geo &g, double inv_adt, double q1p, double q1c, double q2n,
+                                          double q2c, double q3n, double q3c, double irm) {
+  const double d = (q1p - q1c) * g.dx1 * g.axsym * irm + (q2n - q2c) * g.dx2 * irm + (q3n - q3c) * g.dx3;
+  return -d * inv_adt;
+}
 template <class T>
 __device__ __forceinline__ double divq_at(const Geo &g, double inv_adt, const T *__restrict__ dq1,
                                           const T *__restrict__ dq2, const T *__restrict__ dq3, int ic, int jc,
                                           int kc) {
   const int ip = ic < g.nth ? ic + 1 : 1;
   const int o = I3(g, ic, jc, kc);
-  const double irm = __ldg(g.irm + jc);
-  const double d = ((double)__ldg(dq1 + I3(g, ip, jc, kc)) - (double)__ldg(dq1 + o)) * g.dx1 * g.axsym * irm +
-                   ((double)__ldg(dq2 + o + g.nth) - (double)__ldg(dq2 + o)) * g.dx2 * irm +
-                   ((double)__ldg(dq3 + o + g.pl) - (double)__ldg(dq3 + o)) * g.dx3;
-  return -d * inv_adt;
+  return divq_of(g, inv_adt, (double)__ldg(dq1 + I3(g, ip, jc, kc)), (double)__ldg(dq1 + o),
+                 (double)__ldg(dq2 + o + g.nth), (double)__ldg(dq2 + o), (double)__ldg(dq3 + o + g.pl),
+                 (double)__ldg(dq3 + o), __ldg(g.irm + jc));
 }
 __host__ __device__ inline int I2Z(const Geo &g, int i, int j) { return (i - 1) + g.nth * j; }
 

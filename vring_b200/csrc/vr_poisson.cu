@@ -512,13 +512,24 @@ __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in
   const bool hasb = la + 1 < nlines;
   double re[16], im[16];
   if constexpr (DIV) {
-    // line la is the theta line (j, k) = (1 + la % nr, 1 + la / nr)
-    const int nr = dv.g.nr, ja = 1 + la % nr, ka = 1 + la / nr;
+    // line la is the theta line (j, k) = (1 + la % nr, 1 + la / nr); the
+    // pair's two lines by their base cells, the theta neighbour wrapping
+    const Geo &g = dv.g;
+    const int nr = g.nr, ja = 1 + la % nr, ka = 1 + la / nr;
     const int jb = 1 + (la + 1) % nr, kb = 1 + (la + 1) / nr;
+    const int oa = I3(g, 1, ja, ka), ob = I3(g, 1, jb, kb), sj = g.nth, sk = g.pl;
+    const double irma = __ldg(g.irm + ja), irmb = hasb ? __ldg(g.irm + jb) : 0.0;
+    const TQ *a1 = dv.dq1 + oa, *a2 = dv.dq2 + oa, *a3 = dv.dq3 + oa;
+    const TQ *b1 = dv.dq1 + ob, *b2 = dv.dq2 + ob, *b3 = dv.dq3 + ob;
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-      re[m] = divq_at(dv.g, dv.inv_adt, dv.dq1, dv.dq2, dv.dq3, t + T * m + 1, ja, ka);
-      im[m] = hasb ? divq_at(dv.g, dv.inv_adt, dv.dq1, dv.dq2, dv.dq3, t + T * m + 1, jb, kb) : 0.0;
+      const int i = t + T * m, ip = i + 1 < N ? i + 1 : 0;
+      re[m] = divq_of(g, dv.inv_adt, (double)__ldg(a1 + ip), (double)__ldg(a1 + i), (double)__ldg(a2 + i + sj),
+                      (double)__ldg(a2 + i), (double)__ldg(a3 + i + sk), (double)__ldg(a3 + i), irma);
+      im[m] = hasb ? divq_of(g, dv.inv_adt, (double)__ldg(b1 + ip), (double)__ldg(b1 + i),
+                             (double)__ldg(b2 + i + sj), (double)__ldg(b2 + i), (double)__ldg(b3 + i + sk),
+                             (double)__ldg(b3 + i), irmb)
+                   : 0.0;
     }
   } else {
     const double *pa = in + (size_t)la * N, *pb = pa + N;
