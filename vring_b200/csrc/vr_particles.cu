@@ -569,7 +569,10 @@ __device__ __forceinline__ void part_cart_row(double r, double sn_d, double cs_d
 // registers and call out of the main launch.  defer_n[par] counts this call's
 // list; the FIX launch clears the other counter for the next call.
 #ifndef VR_PART_MINB
-#define VR_PART_MINB 8  // resident blocks per SM the register budget is sized for
+// resident blocks per SM the register budget is sized for: with the fit
+// cache, measured at 1,048,576 tracers, 6 (112 registers) 1.087 ms per step,
+// 5: 1.133, 8 (80 registers): 1.146, 10: 1.336
+#define VR_PART_MINB 6
 #endif
 // One substep of the particles in slots ip (1-based; one per lane, the same
 // for the three warps) whose live flag is set.  Returns kPartDeferred (for
