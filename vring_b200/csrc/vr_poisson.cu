@@ -477,6 +477,13 @@ __device__ __forceinline__ int fft_packed_slot(int n) {
   return T == 8 ? n ^ ((n >> 3) & 1) : n;
 }
 
+#ifndef VR_FFT_MINB
+// resident 128-thread blocks per SM the registers are sized for: measured at
+// 256 x 128 x 512 (divq + both theta transforms, ms per step) 4: 0.549,
+// unbounded: 0.575, 5: 0.676, 6: 1.020 (spills)
+#define VR_FFT_MINB 4
+#endif
+
 // the block's copy of the lane twiddles: twl[(k1 - 1) T + t] = W_N^{t k1}
 template <int T>
 __device__ __forceinline__ void load_lane_twiddles(double2 *twl, const double *__restrict__ tw) {
@@ -497,7 +504,7 @@ struct DivSrc {
 };
 
 template <int T, class TQ = double, bool DIV = false>
-__global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in, double *__restrict__ out,
+__global__ void __launch_bounds__(128, VR_FFT_MINB) k_fft_fwd_s(const double *__restrict__ in, double *__restrict__ out,
                                                    int nlines, const double *__restrict__ tw, DivSrc<TQ> dv) {
   constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
   extern __shared__ double2 smv[];
@@ -569,7 +576,7 @@ __global__ void __launch_bounds__(128) k_fft_fwd_s(const double *__restrict__ in
 }
 
 template <int T>
-__global__ void __launch_bounds__(128) k_fft_bwd_s(const double *__restrict__ in, double *__restrict__ dph, Geo g,
+__global__ void __launch_bounds__(128, VR_FFT_MINB) k_fft_bwd_s(const double *__restrict__ in, double *__restrict__ dph, Geo g,
                                                    int nlines, const double *__restrict__ tw) {
   constexpr int N = 16 * T, NPB = 128 / T, PS = fft_pair_stride(T);
   extern __shared__ double2 smv[];
