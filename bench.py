@@ -54,6 +54,8 @@ def family_words(fam, prof):
     phases fused into it: the fused right-hand side also solves the theta
     lines (tsweep), the fused pressure update also runs upsol, the forward
     theta transform of the fused substep also takes divq."""
+    if fam in SLAB_WORDS:
+        return SLAB_WORDS[fam]
     w = WORDS[fam]
     if fam == "rhs" and "tsweep" not in prof:
         w += WORDS["tsweep"]
@@ -64,13 +66,19 @@ def family_words(fam, prof):
     return w
 
 
+# the slab cluster kernels of the fused substep: divq + the forward theta and
+# z transforms, and the two inverse transforms
+SLAB_WORDS = {"pois_fwd": WORDS["divq"] + (WORDS["fft"] + WORDS["dct"]) // 2,
+              "pois_bwd": (WORDS["fft"] + WORDS["dct"]) // 2}
+
+
 def roofline(prof, steps, ncell, peak, peak_kind, traffic_tab, ms_per_step):
     """Roofline of the dominant field family (largest event time among the
     families with algorithmic words): algorithmic bytes per launch over its
     mean launch time, against the HBM peak; traffic is the family's DRAM
     bytes per launch from the committed ncu summaries; step_frac compares the
     whole step with the HBM floor of all 198 words per cell-step."""
-    fam = max((k for k in prof if k in WORDS), key=lambda k: prof[k][0])
+    fam = max((k for k in prof if k in WORDS or k in SLAB_WORDS), key=lambda k: prof[k][0])
     tot_ms, nl = prof[fam]
     per_sub = nl / (3 * steps)  # launches of this family per substep
     bytes_per_launch = family_words(fam, prof) / per_sub * ncell * 8

@@ -230,3 +230,27 @@ def test_streamed_z_transform_three_tiles_per_radius(wth):
     g = gpu.get("dph")[:, 1:8, 1:513]
     r = orc.field("dph")[:, 1:8, 1:513]
     assert np.abs(g - r).max() <= 1e-11 * np.abs(r).max()
+
+
+def test_slab_transforms_match_separate_transforms():
+    # Ntheta 128, Nz 512: the fused substep's transforms as slab cluster
+    # kernels (divq + theta + z forward, z + theta inverse) against the
+    # separate transform kernels; the theta transforms pair other lines, so
+    # the two agree to rounding
+    import vring_b200 as V
+    from vring_b200.synthetic import ring_fields
+    nth, nr, nz = 128, 24, 512
+    q = ring_fields(nth, nr, nz, 4.0, 12.0, noise=1e-3, seed=9)
+    out = []
+    for slab in (True, False):
+        gpu = V.Run(nth, nr, nz, 4.0, 12.0, 5e-4, 3000.0, 1.0, 1.0, theta_wavenumber="modified")
+        gpu.set_slab_transforms(slab)
+        for n, a in zip(("q1", "q2", "q3"), q):
+            gpu.set(n, a)
+        gpu.iterate(2)
+        out.append({n: gpu.get(n) for n in STATE + ["dph"]})
+        gpu.close()
+    for n in STATE + ["dph"]:
+        a, b = out[0][n], out[1][n]
+        scale = max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-12 * scale, (n, np.abs(a - b).max() / scale)

@@ -95,6 +95,7 @@ def lib():
             getattr(L, "vr_" + n).argtypes = [vp]
         L.vr_substep.argtypes = [vp, i32]
         L.vr_set_graphs.argtypes = [vp, i32]
+        L.vr_set_slab_transforms.argtypes = [vp, i32]
         L.vr_iterate.argtypes = [vp, i32]
         L.vr_max_divergence.argtypes = [vp, C.POINTER(dp)]
         L.vr_check_finite.argtypes = [vp, C.POINTER(i64)]
@@ -268,7 +269,7 @@ class Run:
         return n.value
 
     PROFILE_KINDS = ["hdnbc", "hdnl", "rhs", "tsweep", "rsweep", "zsweep", "divq", "fft", "dct",
-                     "radial", "upsol", "uppres", "diag", "part"]
+                     "radial", "upsol", "uppres", "diag", "part", "pois_fwd", "pois_bwd"]
 
     def profile(self, enable: bool) -> None:
         self._chk(lib().vr_profile(self._h, 1 if enable else 0), "profile")
@@ -328,6 +329,10 @@ class Run:
         v = C.c_double()
         self._chk(lib().vr_max_divergence(self._h, C.byref(v)), "max_divergence")
         return v.value
+
+    def set_slab_transforms(self, on: bool):
+        """The fused substep's transforms as slab cluster kernels (default) or apart."""
+        self._chk(lib().vr_set_slab_transforms(self._h, 1 if on else 0), "set_slab_transforms")
 
     def set_graphs(self, on: bool):
         """Replay each substep as a captured CUDA graph (default) or launch one by one."""

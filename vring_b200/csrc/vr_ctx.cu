@@ -336,6 +336,7 @@ extern "C" int vr_create(const vr_desc *desc, vr_ctx **out) {
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VR_ERR_CUDA);
   c->stream = c->own_stream;
   c->use_graphs = true;
+  c->slab_transforms = true;
   c->crkgam[1] = 8.0 / 15.0;
   c->crkgam[2] = 5.0 / 12.0;
   c->crkgam[3] = 3.0 / 4.0;
@@ -1052,6 +1053,19 @@ static int run_substep(vr_ctx *c, int irk) {
   c->irk = irk;
   VR_CUDA(c, cudaGraphLaunch(c->graph[irk], c->stream));
   c->nlaunch += c->graph_launches[irk];
+  return VR_OK;
+}
+
+extern "C" int vr_set_slab_transforms(vr_ctx *c, int32_t on) {
+  if (!c) return VR_ERR_ARG;
+  VR_CUDA(c, cudaSetDevice(c->dev));
+  VR_CUDA(c, cudaStreamSynchronize(c->stream));  // captured substeps may replay the other form
+  for (int i = 0; i < 4; i++)
+    if (c->graph_ok[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph_ok[i] = false;
+    }
+  c->slab_transforms = on != 0;
   return VR_OK;
 }
 

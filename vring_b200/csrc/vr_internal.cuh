@@ -182,6 +182,9 @@ struct vr_ctx {
   // r: 0 TMA 16-line tiles, 1 TMA 8-line tiles, 2 register chunks;
   // z: 0 TMA 8-line tiles, 1 TMA 16-line tiles, 2 register chunks
   int tune_r, tune_z;
+  // the fused substep's transforms as cluster kernels per radial slab
+  // (Ntheta 128, Nz 512); off: the separate theta and z transform kernels
+  bool slab_transforms;
   // vr_get_field_async / vr_set_field_async, per field id (32) and piece
   // (kXferChunks = 4): host copies go through device staging buffers, so they
   // never touch the field while the context's kernels run
@@ -232,7 +235,10 @@ inline cudaError_t allow_dyn_smem(K *kern, size_t bytes) {
 // kernel families for vr_profile_read
 enum ProfKind {
   PK_HDNBC = 0, PK_HDNL, PK_RHS, PK_TSWEEP, PK_RSWEEP, PK_ZSWEEP, PK_DIVQ, PK_FFT, PK_DCT,
-  PK_RADIAL, PK_UPSOL, PK_UPPRES, PK_DIAG, PK_PART, PK_N
+  PK_RADIAL, PK_UPSOL, PK_UPPRES, PK_DIAG, PK_PART,
+  PK_POISF,  // divq + theta + z transforms of a slab (cluster kernel)
+  PK_POISB,  // z + theta inverse transforms of a slab (cluster kernel)
+  PK_N
 };
 
 // Counts one kernel launch; with profiling on, brackets it with events on the

@@ -10,6 +10,7 @@
 // factorisation depends only on (theta mode, z mode) and is built once at
 // vr_create; the solve streams the right-hand side through a shared-memory
 // tile and runs the two substitutions chunk-parallel (see vr_momentum.cu).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "vr_chunk.cuh"
@@ -1032,6 +1033,281 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
 }
 
 // ---------------------------------------------------------------------------
+// The theta transform and the z transform of one radial index in one pass
+// each way, for Ntheta = 128 and Nz = 512: a cluster of 8 CTAs owns the
+// (theta, z) slab of one j.
+//
+// Forward (k_pois_fwd_cl): CTA c takes divq of the 64 theta lines of planes
+// 64c + 1 .. 64c + 64 straight from dq (divq_of, as the fused theta
+// transform does) and transforms them in pairs (pair_fft16, 8 threads per
+// pair); the packed spectra stay in its shared memory, row r (the plane) of
+// 64 slot pairs, slot pair P of row r at P ^ ((r >> 1) & 7) so that the
+// strided row reads below meet eight bank groups per quarter warp.  After a
+// cluster barrier warp w of CTA c gathers slots 16c + 2w, 16c + 2w + 1 of all
+// 512 planes from the 8 CTAs' shared memory (distributed shared memory) in
+// Makhoul's order, a second barrier frees the tiles, and the 512-point z
+// transform runs as in k_dct_tma, its result stored by TMA into the spectral
+// array.  Inverse (k_pois_bwd_cl): the z transform of the CTA's 16 slots
+// first (TMA load, k_dct_tma's inverse), a cluster barrier, then the theta
+// pairs of its 64 planes read their packed entries from the 8 CTAs, a second
+// barrier, and the inverse theta transforms write dph.  The arithmetic is
+// that of k_fft_fwd_s / k_dct_tma / k_fft_bwd_s, so the results are the
+// same bits; the spectral array is written once and read once instead of
+// twice each way.  Every CTA takes every cluster barrier.
+// ---------------------------------------------------------------------------
+constexpr int kClCtas = 8, kClRows = kDctN / kClCtas;  // 64 planes per CTA
+constexpr int kClSlab = 128;                            // theta slots
+
+__device__ __forceinline__ int cl_pair_slot(int r, int P) { return r * (kClSlab / 2) + (P ^ ((r >> 1) & 7)); }
+
+template <class TQ>
+__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, 1)
+    k_pois_fwd_cl(const __grid_constant__ CUtensorMap tm, DivSrc<TQ> dv, const double *__restrict__ tw_th,
+                  const double *__restrict__ twz) {
+  namespace cg = cooperative_groups;
+  constexpr int N = kDctN, T = 8, NT = kClSlab;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ unsigned char dct_dsm[];
+  double2 *const b = reinterpret_cast<double2 *>(((uintptr_t)dct_dsm + 1023) & ~(uintptr_t)1023);  // 64 KB
+  double2 *const twf = b + kDctTileBytes / 16;  // theta lane twiddles [15][8]
+  double2 *const twl = twf + 15 * T;            // z lane twiddles [15][32]
+  double2 *const shl = twl + 15 * 32;           // quarter-wave shift [16][32]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int c = (int)cl.block_rank(), jj = blockIdx.x / kClCtas;  // slab j = jj + 1
+  load_lane_twiddles<T>(twf, tw_th);
+  for (int i = tid; i < 15 * 32; i += 256) {
+    const int p = (i & 31) * (i / 32 + 1);
+    twl[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
+  }
+  for (int i = tid; i < 16 * 32; i += 256) {
+    const int k = (i & 31) + 32 * (i / 32);
+    shl[i] = make_double2(__ldg(twz + 2 * N + 2 * k), __ldg(twz + 2 * N + 2 * k + 1));
+  }
+  __syncthreads();
+  // ---- theta: planes 64 c + 2 g (+1), pair group g of 8 threads
+  {
+    const Geo &g = dv.g;
+    const int grp = tid / T, t = tid % T, ra = 2 * grp;
+    const unsigned gm = 0xffu << ((tid & 31) / T * T);
+    const int jc = jj + 1, ka = kClRows * c + ra + 1;
+    const int oa = I3(g, 1, jc, ka), ob = I3(g, 1, jc, ka + 1), sj = g.nth, sk = g.pl;
+    const double irm = __ldg(g.irm + jc);
+    const TQ *a1 = dv.dq1 + oa, *a2 = dv.dq2 + oa, *a3 = dv.dq3 + oa;
+    const TQ *b1 = dv.dq1 + ob, *b2 = dv.dq2 + ob, *b3 = dv.dq3 + ob;
+    double re[16], im[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int i = t + T * m, ip = i + 1 < NT ? i + 1 : 0;
+      re[m] = divq_of(g, dv.inv_adt, (double)__ldg(a1 + ip), (double)__ldg(a1 + i), (double)__ldg(a2 + i + sj),
+                      (double)__ldg(a2 + i), (double)__ldg(a3 + i + sk), (double)__ldg(a3 + i), irm);
+      im[m] = divq_of(g, dv.inv_adt, (double)__ldg(b1 + ip), (double)__ldg(b1 + i), (double)__ldg(b2 + i + sj),
+                      (double)__ldg(b2 + i), (double)__ldg(b3 + i + sk), (double)__ldg(b3 + i), irm);
+    }
+    double2 *sc = b + grp * (2 * NT / 2);  // rows ra, ra + 1 of the tile: the pair's scratch
+    pair_fft16<T>(re, im, twf, sc, t, gm);
+    // packed [a0, a1, b1, ...] (fastfouriertransform.F90:34-43), read first,
+    // then written over the scratch into rows ra (line a) and ra + 1 (line b)
+    double2 z[NT / (2 * T)], zm[NT / (2 * T)];
+#pragma unroll
+    for (int q = 0; q < NT / (2 * T); q++) {
+      const int k = t + T * q;
+      z[q] = sc[k];
+      zm[q] = sc[k == 0 ? NT / 2 : NT - k];
+    }
+    __syncwarp(gm);
+    double *const rowa = reinterpret_cast<double *>(b), invn = 1.0 / NT;
+    auto put = [&](int r, int slot, double v) {
+      rowa[2 * cl_pair_slot(r, slot >> 1) + (slot & 1)] = v;
+    };
+#pragma unroll
+    for (int q = 0; q < NT / (2 * T); q++) {
+      const int k = t + T * q;
+      if (k == 0) {
+        put(ra, 0, z[q].x * invn);
+        put(ra, NT - 1, (zm[q].x + zm[q].x) * invn);
+        put(ra + 1, 0, z[q].y * invn);
+        put(ra + 1, NT - 1, (zm[q].y + zm[q].y) * invn);
+      } else {
+        put(ra, 2 * k - 1, (z[q].x + zm[q].x) * invn);
+        put(ra, 2 * k, -(z[q].y - zm[q].y) * invn);
+        put(ra + 1, 2 * k - 1, (z[q].y + zm[q].y) * invn);
+        put(ra + 1, 2 * k, (z[q].x - zm[q].x) * invn);
+      }
+    }
+  }
+  cl.sync();  // every CTA's packed planes are in its shared memory
+  // ---- z: slots 16 c + 2 w, + 1 of all 512 planes, Makhoul's order
+  double re[16], im[16];
+  {
+    const int P = (kDctTileCols / 2) * c + warp;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int n = lane + 32 * q, src = n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1;
+      const double2 *peer = cl.map_shared_rank(b, src / kClRows);
+      const double2 v = peer[cl_pair_slot(src % kClRows, P)];
+      re[q] = v.x;
+      im[q] = v.y;
+    }
+  }
+  cl.sync();  // every gather from this CTA's tile is done
+  auto tw_lane = [&](int k1, double &cc, double &sn) {
+    const double2 v = twl[(k1 - 1) * 32 + lane];
+    cc = v.x;
+    sn = v.y;
+  };
+  warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+  __syncwarp();
+  const SwzScratch<1> out{b, warp};
+#pragma unroll
+  for (int q = 0; q < 16; q++) out.st((lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4)), re[q], im[q]);
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int k = lane + 32 * q, km = (N - k) & (N - 1);
+    double zr, zi, mr, mi;
+    out.ld(k, zr, zi);
+    out.ld(km, mr, mi);
+    const double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);
+    const double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);
+    const double2 cs = shl[q * 32 + lane];
+    re[q] = 2.0 * (var_ * cs.x + vai * cs.y) / (2.0 * N * 1);
+    im[q] = 2.0 * (vbr * cs.x + vbi * cs.y) / (2.0 * N * 1);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 16; q++) *swz_pair(b, lane + 32 * q, warp) = make_double2(re[q], im[q]);
+  fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_3d(&tm, kDctTileCols * c, jj, 0, b);
+    tma_store_3d(&tm, kDctTileCols * c, jj, 256, b + 256 * 8);
+    bulk_commit();
+    bulk_wait_all();
+  }
+}
+
+__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, 1)
+    k_pois_bwd_cl(const __grid_constant__ CUtensorMap tm, Geo g, double *__restrict__ dph,
+                  const double *__restrict__ tw_th, const double *__restrict__ twz, unsigned *status) {
+  namespace cg = cooperative_groups;
+  constexpr int N = kDctN, T = 8, NT = kClSlab;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ unsigned char dct_dsm[];
+  __shared__ __align__(8) uint64_t full;
+  double2 *const b = reinterpret_cast<double2 *>(((uintptr_t)dct_dsm + 1023) & ~(uintptr_t)1023);  // 64 KB
+  double2 *const twf = b + kDctTileBytes / 16;
+  double2 *const twl = twf + 15 * T;
+  double2 *const shl = twl + 15 * 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int c = (int)cl.block_rank(), jj = blockIdx.x / kClCtas;
+  if (tid == 0) {
+    mbar_init(&full, 1);
+    mbar_init_fence();
+    mbar_expect_tx(&full, kDctTileBytes);
+    tma_load_3d(b, &tm, kDctTileCols * c, jj, 0, &full);
+    tma_load_3d(b + 256 * 8, &tm, kDctTileCols * c, jj, 256, &full);
+  }
+  load_lane_twiddles<T>(twf, tw_th);
+  for (int i = tid; i < 15 * 32; i += 256) {
+    const int p = (i & 31) * (i / 32 + 1);
+    twl[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
+  }
+  for (int i = tid; i < 16 * 32; i += 256) {
+    const int k = (i & 31) + 32 * (i / 32);
+    shl[i] = make_double2(__ldg(twz + 2 * N + 2 * k), __ldg(twz + 2 * N + 2 * k + 1));
+  }
+  __syncthreads();
+  // a load that does not arrive in time: record it and carry on with the
+  // tile as it is (every CTA must still take every cluster barrier); the
+  // wait below ends before the CTA's shared memory can be reused
+  const bool ok = mbar_wait(&full, 0u);
+  if (!ok && tid == 0) atomicOr(status, 1u);
+  // ---- z: inverse of this CTA's 16 slots (k_dct_tma<-1>)
+  {
+    auto tw_lane = [&](int k1, double &cc, double &sn) {
+      const double2 v = twl[(k1 - 1) * 32 + lane];
+      cc = v.x;
+      sn = v.y;
+    };
+    double re[16], im[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int k = lane + 32 * q;
+      const double2 cs = shl[q * 32 + lane];
+      const double2 x = *swz_pair(b, k, warp), y = *swz_pair(b, (N - k) & (N - 1), warp);
+      const double xa = x.x / 2.0, xb = x.y / 2.0;
+      const double ya = k == 0 ? 0.0 : -y.x / 2.0, yb = k == 0 ? 0.0 : -y.y / 2.0;
+      const double var_ = xa * cs.x - ya * cs.y, vai = xa * cs.y + ya * cs.x;
+      const double vbr = xb * cs.x - yb * cs.y, vbi = xb * cs.y + yb * cs.x;
+      re[q] = var_ - vbi;
+      im[q] = -(vai + vbr);
+    }
+    __syncwarp();
+    warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int m = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
+      const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+      *swz_pair(b, o, warp) = make_double2(2.0 * re[q], -2.0 * im[q]);
+    }
+  }
+  cl.sync();  // every CTA's slots are back in plane order in its shared memory
+  // ---- theta: planes 64 c + 2 g (+1), the packed entries from the 8 CTAs
+  const int grp = tid / T, t = tid % T, za = kClRows * c + 2 * grp;  // 0-based planes za, za + 1
+  const unsigned gm = 0xffu << ((tid & 31) / T * T);
+  auto packed = [&](int z0, int n) -> double {  // entry n of plane z0
+    const double *peer = reinterpret_cast<const double *>(cl.map_shared_rank(b, n / kDctTileCols));
+    const int col = n % kDctTileCols;
+    return peer[2 * (z0 * 8 + ((col >> 1) ^ (z0 & 7))) + (col & 1)];
+  };
+  double re[16], im[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int k = t + T * m;
+    const int kk = k <= NT / 2 ? k : NT - k;
+    double ar, ai, br, bi;
+    if (kk == 0) {
+      ar = packed(za, 0);
+      ai = 0.0;
+      br = packed(za + 1, 0);
+      bi = 0.0;
+    } else {
+      ar = packed(za, 2 * kk - 1) / 2.0;
+      br = packed(za + 1, 2 * kk - 1) / 2.0;
+      if (2 * kk < NT) {
+        ai = -1.0 * packed(za, 2 * kk) / 2.0;
+        bi = -1.0 * packed(za + 1, 2 * kk) / 2.0;
+      } else {
+        ai = 0.0;
+        bi = 0.0;
+      }
+      if (k > NT / 2) {
+        ai = -ai;
+        bi = -bi;
+      }
+    }
+    re[m] = ar - bi;
+    im[m] = -(ai + br);
+  }
+  cl.sync();  // every read of this CTA's tile is done: it becomes pair scratch
+  double2 *sc = b + grp * (2 * NT / 2);
+  pair_fft16<T>(re, im, twf, sc, t, gm);
+  const int jc = jj + 1;
+  double *da = dph + IDP(g, 1, jc, za + 1), *db = dph + IDP(g, 1, jc, za + 2);
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const int n = t + T * j;
+    const double2 v = sc[n];
+    da[n] = v.x;
+    db[n] = -v.y;
+  }
+  // the tile load landed long ago unless its wait gave up; then wait for it
+  // once more (bounded) before the shared memory goes away
+  if (!ok && tid == 0) (void)mbar_wait(&full, 0u);
+}
+
+// ---------------------------------------------------------------------------
 // z transforms on lines (slot, j) of the (nth, nr, nz) spectral array,
 // stride nth*nr; a tile holds LT consecutive slots at fixed j.
 // ---------------------------------------------------------------------------
@@ -1392,11 +1668,58 @@ static cudaError_t dct_warp_dispatch(vr_ctx *c, int dir, bool *done) {
   }
 }
 
+// the fused substep's transforms as slab clusters (k_pois_fwd_cl /
+// k_pois_bwd_cl); NotSupported when the shape or the tensor map does not fit
+static cudaError_t run_slab_fwd(vr_ctx *c, const Rk &rk, const CUtensorMap &tm) {
+  const Geo &g = c->geo;
+  const size_t sm = 1024 + (size_t)kDctTileBytes + (15 * 8 + 15 * 32 + 16 * 32) * sizeof(double2);
+  const double inv_adt = 1.0 / (rk.alm * g.dt);
+  cudaError_t e;
+  LaunchScope ls(c, PK_POISF);
+  if (c->mixed) {
+    auto kern = k_pois_fwd_cl<float>;
+    if ((e = allow_dyn_smem(kern, sm))) return e;
+    DivSrc<float> dv{g, inv_adt, reinterpret_cast<const float *>(c->dq[0]),
+                     reinterpret_cast<const float *>(c->dq[1]), reinterpret_cast<const float *>(c->dq[2])};
+    kern<<<kClCtas * g.nr, 256, sm, c->stream>>>(tm, dv, c->tw_th, c->tw_z);
+  } else {
+    auto kern = k_pois_fwd_cl<double>;
+    if ((e = allow_dyn_smem(kern, sm))) return e;
+    DivSrc<double> dv{g, inv_adt, c->dq[0], c->dq[1], c->dq[2]};
+    kern<<<kClCtas * g.nr, 256, sm, c->stream>>>(tm, dv, c->tw_th, c->tw_z);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t run_slab_bwd(vr_ctx *c, const CUtensorMap &tm) {
+  const Geo &g = c->geo;
+  const size_t sm = 1024 + (size_t)kDctTileBytes + (15 * 8 + 15 * 32 + 16 * 32) * sizeof(double2);
+  cudaError_t e;
+  LaunchScope ls(c, PK_POISB);
+  if ((e = allow_dyn_smem(k_pois_bwd_cl, sm))) return e;
+  k_pois_bwd_cl<<<kClCtas * g.nr, 256, sm, c->stream>>>(tm, g, c->dph, c->tw_th, c->tw_z, c->d_status);
+  return cudaGetLastError();
+}
+
+static bool slab_tmap(vr_ctx *c, CUtensorMap *tm) {
+  const Geo &g = c->geo;
+  if (!c->slab_transforms || g.nth != kClSlab || g.nz != kDctN) return false;
+  return encode_tmap_f64_3d(tm, c->spec, g.nth, g.nr, g.nz, kDctTileCols, 1, 256, true);
+}
+
+static cudaError_t radial_solves(vr_ctx *c);
+
 cudaError_t launch_poisson(vr_ctx *c, const Rk *div_rk) {
   const Geo &g = c->geo;
   cudaError_t e;
   const int N = g.nth, nlines = g.nr * g.nz;
   if (div_rk && !poisson_takes_dq(c)) return cudaErrorInvalidValue;  // the caller runs divq first
+  CUtensorMap stm;
+  if (div_rk && slab_tmap(c, &stm)) {
+    if ((e = run_slab_fwd(c, *div_rk, stm))) return e;
+    if ((e = radial_solves(c))) return e;
+    return run_slab_bwd(c, stm);
+  }
   // theta forward: rhs (or divq of dq) -> spec
   bool done = false;
   if ((e = fft_warp_dispatch(c, +1, &done, div_rk))) return e;
@@ -1423,30 +1746,7 @@ cudaError_t launch_poisson(vr_ctx *c, const Rk *div_rk) {
     k_dct_direct<<<dim3(N, g.nr), 64, sizeof(double) * g.nz, c->stream>>>(c->spec, g, +1);
   }
   if ((e = cudaGetLastError())) return e;
-  // radial solves
-  if (chunk_bucket(g.nr)) {
-    PoisLine p;
-    p.a = c->spec;
-    p.pa = c->pois_a;
-    p.pc = c->pois_c;
-    p.pib = c->pois_ib;
-    p.n = g.nr;
-    p.nth = g.nth;
-    p.nm = g.nth / 2 + 1;
-    p.nbx = (N + 31) / 32;
-    LaunchScope ls(c, PK_RADIAL);
-    e = g.nr <= 16 * 16
-            ? run_chunk_tma<16, 16, 16, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream)
-            : run_chunk_tma<16, 16, 17, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream);
-    if (e == cudaErrorNotSupported) e = launch_chunk(p, p.nbx * g.nz, c->stream);
-    if (e) return e;
-  } else if (g.nr <= 640)
-    e = run_radial<16, 16>(c);
-  else if (g.nr <= 1600)
-    e = run_radial<8, 32>(c);
-  else
-    e = run_radial<4, 64>(c);
-  if (e) return e;
+  if ((e = radial_solves(c))) return e;
   // z backward
   if ((e = dct_warp_dispatch(c, -1, &done))) return e;
   if (done) {
@@ -1471,6 +1771,36 @@ cudaError_t launch_poisson(vr_ctx *c, const Rk *div_rk) {
     k_dft_bwd_direct<<<nlines, 64, 0, c->stream>>>(c->spec, c->dph, g, nlines);
   }
   return cudaGetLastError();
+}
+
+// the radial tridiagonal lines of every (theta mode, z mode)
+static cudaError_t radial_solves(vr_ctx *c) {
+  const Geo &g = c->geo;
+  const int N = g.nth;
+  cudaError_t e = cudaSuccess;
+  if (chunk_bucket(g.nr)) {
+    PoisLine p;
+    p.a = c->spec;
+    p.pa = c->pois_a;
+    p.pc = c->pois_c;
+    p.pib = c->pois_ib;
+    p.n = g.nr;
+    p.nth = g.nth;
+    p.nm = g.nth / 2 + 1;
+    p.nbx = (N + 31) / 32;
+    LaunchScope ls(c, PK_RADIAL);
+    e = g.nr <= 16 * 16
+            ? run_chunk_tma<16, 16, 16, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream)
+            : run_chunk_tma<16, 16, 17, 2, 2>(p, c->spec, g.nth, g.nr, g.nz, 1, g.nz, c->nsm, c->d_status, c->stream);
+    if (e == cudaErrorNotSupported) e = launch_chunk(p, p.nbx * g.nz, c->stream);
+    if (e) return e;
+  } else if (g.nr <= 640)
+    e = run_radial<16, 16>(c);
+  else if (g.nr <= 1600)
+    e = run_radial<8, 32>(c);
+  else
+    e = run_radial<4, 64>(c);
+  return e;
 }
 
 }  // namespace vr
