@@ -253,4 +253,7 @@ def test_slab_transforms_match_separate_transforms():
     for n in STATE + ["dph"]:
         a, b = out[0][n], out[1][n]
         scale = max(np.abs(b).max(), 1e-300)
-        assert np.abs(a - b).max() <= 1e-12 * scale, (n, np.abs(a - b).max() / scale)
+        # dph carries the near-singular low modes' amplification of rounding
+        # (the tolerance of every dph comparison with the oracle)
+        rel = 1e-11 if n == "dph" else 1e-12
+        assert np.abs(a - b).max() <= rel * scale, (n, np.abs(a - b).max() / scale)
