@@ -181,12 +181,13 @@ VR_API int vr_substep(vr_ctx *ctx, int32_t irk);
  * kernels enqueued on the context's stream; particle classes attached with
  * vr_part_attach advance before substep 1 (loop.F90:65-68). */
 VR_API int vr_iterate(vr_ctx *ctx, int32_t nsteps);
-/* The fused substep's transforms for Ntheta 128 and Nz 512: on (default),
- * divq + the theta and z forward transforms and the z and theta inverse
- * transforms of each radial slab run as two cluster kernels (8 CTAs per slab,
- * distributed shared memory); off, as the separate theta and z transform
- * kernels.  The results agree to rounding (the theta transforms pair other
- * lines).  No reference counterpart. */
+/* The fused substep's transforms for Ntheta 128 and Nz 512: on, divq + the
+ * theta and z forward transforms and the z and theta inverse transforms of
+ * each radial slab run as two cluster kernels (8 CTAs per slab, distributed
+ * shared memory); off (default), as the separate theta and z transform
+ * kernels, which measured twice as fast at 256 x 128 x 512.  The results
+ * agree to rounding (the theta transforms pair other lines).  No reference
+ * counterpart. */
 VR_API int vr_set_slab_transforms(vr_ctx *ctx, int32_t on);
 /* vr_substep/vr_iterate replay each RK substep's kernels as a CUDA graph
  * captured on first use (on by default; bypassed while vr_profile is on or

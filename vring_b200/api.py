@@ -331,7 +331,7 @@ class Run:
         return v.value
 
     def set_slab_transforms(self, on: bool):
-        """The fused substep's transforms as slab cluster kernels (default) or apart."""
+        """The fused substep's transforms as slab cluster kernels, or apart (default)."""
         self._chk(lib().vr_set_slab_transforms(self._h, 1 if on else 0), "set_slab_transforms")
 
     def set_graphs(self, on: bool):

@@ -183,7 +183,8 @@ struct vr_ctx {
   // z: 0 TMA 8-line tiles, 1 TMA 16-line tiles, 2 register chunks
   int tune_r, tune_z;
   // the fused substep's transforms as cluster kernels per radial slab
-  // (Ntheta 128, Nz 512); off: the separate theta and z transform kernels
+  // (Ntheta 128, Nz 512); off (default): the separate theta and z transform
+  // kernels, which measured twice as fast
   bool slab_transforms;
   // vr_get_field_async / vr_set_field_async, per field id (32) and piece
   // (kXferChunks = 4): host copies go through device staging buffers, so they

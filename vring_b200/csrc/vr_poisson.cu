@@ -1055,13 +1055,20 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
 // same bits; the spectral array is written once and read once instead of
 // twice each way.  Every CTA takes every cluster barrier.
 // ---------------------------------------------------------------------------
+#ifndef VR_SLAB_MINB
+// resident CTAs per SM the slab kernels' registers are sized for (2: 128
+// registers, no spills; measured 1.94 ms per step for both directions at
+// 256 x 128 x 512 against 2.32 with one CTA per SM and 0.96 for the separate
+// transform kernels, which is why the slab form is off by default)
+#define VR_SLAB_MINB 2
+#endif
 constexpr int kClCtas = 8, kClRows = kDctN / kClCtas;  // 64 planes per CTA
 constexpr int kClSlab = 128;                            // theta slots
 
 __device__ __forceinline__ int cl_pair_slot(int r, int P) { return r * (kClSlab / 2) + (P ^ ((r >> 1) & 7)); }
 
 template <class TQ>
-__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, 1)
+__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, VR_SLAB_MINB)
     k_pois_fwd_cl(const __grid_constant__ CUtensorMap tm, DivSrc<TQ> dv, const double *__restrict__ tw_th,
                   const double *__restrict__ twz) {
   namespace cg = cooperative_groups;
@@ -1186,7 +1193,7 @@ __global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, 1)
   }
 }
 
-__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, 1)
+__global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, VR_SLAB_MINB)
     k_pois_bwd_cl(const __grid_constant__ CUtensorMap tm, Geo g, double *__restrict__ dph,
                   const double *__restrict__ tw_th, const double *__restrict__ twz, unsigned *status) {
   namespace cg = cooperative_groups;
