@@ -61,6 +61,8 @@ struct vr_k2d {
   double *part = nullptr;   // PT_N x kK2dMaxBlocks
   double *sc = nullptr;     // SC_N
   int *flags = nullptr;     // done, iterations
+  unsigned *cnt = nullptr;  // arrival counters of the CG kernels' last-block reductions
+  int cg_parity = 0;        // direction buffer of the next CG iteration being captured
   // direct solve: forward / inverse z transforms (nz x nz, row-major [kz][k]
   // and [k][kz]) and the radial Thomas factorisation per z mode
   double *dct_f = nullptr, *dct_i = nullptr, *tlo = nullptr, *tup = nullptr, *tib = nullptr;
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       sc[SC_BB] = a;
       sc[SC_RZ] = b;
       sc[SC_RR] = c;
+      sc[SC_BETA] = 0.0;  // the first direction is z itself
       flags[0] = (c <= sc[SC_TOL2] * a) ? 1 : 0;
       flags[1] = 0;
       break;
@@ -290,11 +293,83 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
   if ((op == SO_CG_BETA || op == SO_BI_CONV || op == SO_FCG_CONV) && !flags[0] && flags[1] >= flags[2]) flags[0] = 2;
 }
 
-// CG: x += alpha p; r -= alpha q; z = M r (identity or Jacobi); partials r.z [B], r.r [C]
+// A CG iteration is two kernels.  Each ends with a reduction of its blocks'
+// partial sums done by the block that arrives last (an arrival counter, reset
+// by that block), in a fixed order, so the scalars need no one-block kernel
+// and the results do not depend on the blocks' timing.
+__device__ __forceinline__ bool arrived_last(unsigned *counter) {
+  __shared__ bool last;
+  __threadfence();  // this block's partials before its arrival
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+// sum of the nb partials p[0..nb) in the block that arrived last (read
+// through L2: the other blocks wrote them)
+__device__ __forceinline__ double sum_part_l2(const double *p, int nb, double *sh) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += __ldcg(p + i);
+  double s = block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[33] = s;
+  __syncthreads();
+  return sh[33];
+}
+
+// CG, first kernel: the direction p = z + beta p_old (beta 0 at the first
+// iteration), formed where the operator needs it and stored in the other p
+// buffer (the neighbouring blocks still read p_old), q = S p, partials p.q
+// [A]; the last block sets alpha = rz / p.q
+__global__ void __launch_bounds__(kK2dThreads) k2d_cg_pq(K2dOp o, const double *__restrict__ z,
+                                                       const double *__restrict__ pold, double *__restrict__ p,
+                                                       double *__restrict__ q, double *sc, double *part,
+                                                       unsigned *counter, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double be = sc[SC_BETA];
+  auto pv = [&](int j) { return z[j] + be * pold[j]; };
+  double v = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) v += pv((o.nr - 1) + o.nr * k);
+  double ms = block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[32] = ms / o.nz;
+  __syncthreads();
+  const double mean = sh[32];
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const int j = i % o.nr, k = i / o.nr;
+    const double xc = pv(i);
+    double y = 0.0;
+    if (j > 0) y += o.aw[j] * (xc - pv(i - 1));
+    if (j < o.nr - 1) y += o.ae[j] * (xc - pv(i + 1));
+    else y += o.gam * mean;
+    const double az = o.az[j];
+    if (k > 0) y += az * (xc - pv(i - o.nr));
+    if (k < o.nz - 1) y += az * (xc - pv(i + o.nr));
+    p[i] = xc;
+    q[i] = y;
+    acc += xc * y;
+  }
+  __syncthreads();
+  double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (!arrived_last(counter)) return;
+  const double pq = sum_part_l2(part, gridDim.x, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_ALPHA] = sc[SC_RZ] / pq;
+    *counter = 0;
+  }
+}
+
+// CG, second kernel: x += alpha p; r -= alpha q; z = M r (identity or
+// Jacobi); partials r.z [B], r.r [C]; the last block sets beta, rz, rr and
+// the convergence and iteration-cap flags
 __global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, double *__restrict__ x,
                                                        double *__restrict__ r, double *__restrict__ z,
                                                        const double *__restrict__ p, const double *__restrict__ q,
-                                                       const double *sc, double *part, const int *flags) {
+                                                       double *sc, double *part, unsigned *counter, int *flags) {
   __shared__ double sh[40];
   if (flags[0]) return;
   const double al = sc[SC_ALPHA];
@@ -313,14 +388,18 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, do
   __syncthreads();
   s = block_sum(rr, sh);
   if (threadIdx.x == 0) part[2 * kK2dMaxBlocks + blockIdx.x] = s;
-}
-
-// p = z + beta p  (runs only while not converged)
-__global__ void __launch_bounds__(kK2dThreads) k2d_cg_p(int n, double *__restrict__ p, const double *__restrict__ z,
-                                                      const double *sc, const int *flags) {
-  if (flags[0]) return;
-  const double be = sc[SC_BETA];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + be * p[i];
+  if (!arrived_last(counter)) return;
+  const double b = sum_part_l2(part + kK2dMaxBlocks, gridDim.x, sh);
+  const double c = sum_part_l2(part + 2 * kK2dMaxBlocks, gridDim.x, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_BETA] = b / sc[SC_RZ];
+    sc[SC_RZ] = b;
+    sc[SC_RR] = c;
+    flags[1] += 1;
+    if (c <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
+    if (!flags[0] && flags[1] >= flags[2]) flags[0] = 2;  // iteration cap: stop as not converged
+    *counter = 0;
+  }
 }
 
 // BiCGSTAB p = r + beta (p - omega v)
@@ -706,6 +785,8 @@ extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
   if (cudaMalloc(&k->part, sizeof(double) * PT_N * kK2dMaxBlocks) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->sc, sizeof(double) * SC_N) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->flags, sizeof(int) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMalloc(&k->cnt, sizeof(unsigned) * 2) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMemset(k->cnt, 0, sizeof(unsigned) * 2) != cudaSuccess) return fail(VR_ERR_CUDA);
   if (cudaMalloc(&k->dct_f, sizeof(double) * cf.size()) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->dct_i, sizeof(double) * ci.size()) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->tlo, sizeof(double) * nr) != cudaSuccess) return fail(VR_ERR_OOM);
@@ -738,6 +819,7 @@ extern "C" int vr_k2d_destroy(vr_k2d *k) {
   for (double *p : ps)
     if (p) cudaFree(p);
   if (k->flags) cudaFree(k->flags);
+  if (k->cnt) cudaFree(k->cnt);
   if (k->stream) cudaStreamDestroy(k->stream);
   delete k;
   return VR_OK;
@@ -823,17 +905,18 @@ extern "C" int vr_k2d_direct(vr_k2d *k, const double *f, double *x) {
 }
 
 // ---- Krylov drivers ------------------------------------------------------------
-static cudaError_t enqueue_cg_iter(vr_k2d *k, int jacobi) {
+// the direction alternates between two buffers (V_P, then V_V), so an
+// iteration's p and the previous one are apart; kK2dChunk is even, so every
+// captured chunk starts from V_P
+static cudaError_t enqueue_cg_iter(vr_k2d *k, int jacobi, int parity) {
   const K2dOp o = op_of(k);
   const int gb = k2d_grid(k);
   double *P = k->part;
-  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *q = k->vec[V_Q];
+  double *x = k->vec[V_X], *r = k->vec[V_R], *q = k->vec[V_Q];
+  double *pold = parity ? k->vec[V_V] : k->vec[V_P], *p = parity ? k->vec[V_P] : k->vec[V_V];
   double *z = jacobi ? k->vec[V_Z] : r;
-  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, q, 0, p, P, k->flags);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_ALPHA, P, gb, k->sc, k->flags);
-  k2d_cg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o, jacobi, x, r, z, p, q, k->sc, P, k->flags);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_BETA, P, gb, k->sc, k->flags);
-  k2d_cg_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, z, k->sc, k->flags);
+  k2d_cg_pq<<<gb, kK2dThreads, 0, k->stream>>>(o, z, pold, p, q, k->sc, P, k->cnt, k->flags);
+  k2d_cg_xr<<<gb, kK2dThreads, 0, k->stream>>>(o, jacobi, x, r, z, p, q, k->sc, P, k->cnt + 1, k->flags);
   return cudaGetLastError();
 }
 
@@ -887,7 +970,12 @@ static int run_chunks(vr_k2d *k, int slot, cudaError_t (*enq)(vr_k2d *, int), in
   return VR_OK;
 }
 
-static cudaError_t enq_cg(vr_k2d *k, int jacobi) { return enqueue_cg_iter(k, jacobi); }
+static_assert(kK2dChunk % 2 == 0, "CG chunks start from the same direction buffer");
+static cudaError_t enq_cg(vr_k2d *k, int jacobi) {
+  const cudaError_t e = enqueue_cg_iter(k, jacobi, k->cg_parity);
+  k->cg_parity ^= 1;
+  return e;
+}
 static cudaError_t enq_bicg(vr_k2d *k, int) { return enqueue_bicg_iter(k); }
 
 // One iteration of the flexible CG with the learned preconditioner:
