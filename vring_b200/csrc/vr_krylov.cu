@@ -38,6 +38,7 @@
 namespace vr {
 
 constexpr int kK2dThreads = 256;
+constexpr int kK2dCgBlocksPerSm = 6;  // the CG kernels' grid (no per-block row mean)
 constexpr int kK2dMaxBlocks = 1024;
 constexpr int kK2dChunk = 32;        // iterations per captured graph
 constexpr int kK2dChunkLearned = 4;  // for the learned flexible CG (each iteration runs the network)
@@ -45,7 +46,9 @@ constexpr int kFcgKeep = 8;          // directions the flexible CG keeps (trunca
 
 // scalar slots
 enum K2dScal {
-  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_SS, SC_N
+  SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_SS,
+  SC_PMEAN,  // CG: mean over z of the next direction's last radial row
+  SC_N
 };
 // partial-sum slots
 enum K2dPart { PT_A = 0, PT_B, PT_C, PT_D, PT_N };
@@ -63,6 +66,7 @@ struct vr_k2d {
   int *flags = nullptr;     // done, iterations
   unsigned *cnt = nullptr;  // arrival counters of the CG kernels' last-block reductions
   int cg_parity = 0;        // direction buffer of the next CG iteration being captured
+  int nb_cg = 1;            // grid of the CG iteration kernels
   // direct solve: forward / inverse z transforms (nz x nz, row-major [kz][k]
   // and [k][kz]) and the radial Thomas factorisation per z mode
   double *dct_f = nullptr, *dct_i = nullptr, *tlo = nullptr, *tup = nullptr, *tib = nullptr;
@@ -318,6 +322,15 @@ __device__ __forceinline__ double sum_part_l2(const double *p, int nb, double *s
   return sh[33];
 }
 
+// the first direction (z itself): the mean over z of its last radial row
+__global__ void __launch_bounds__(kK2dThreads) k2d_cg_pmean(K2dOp o, const double *__restrict__ z, double *sc) {
+  __shared__ double sh[40];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) v += z[(o.nr - 1) + o.nr * k];
+  const double ms = block_sum(v, sh);
+  if (threadIdx.x == 0) sc[SC_PMEAN] = ms / o.nz;
+}
+
 // CG, first kernel: the direction p = z + beta p_old (beta 0 at the first
 // iteration), formed where the operator needs it and stored in the other p
 // buffer (the neighbouring blocks still read p_old), q = S p, partials p.q
@@ -328,15 +341,8 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_pq(K2dOp o, const double *
                                                        unsigned *counter, const int *flags) {
   __shared__ double sh[40];
   if (flags[0]) return;
-  const double be = sc[SC_BETA];
+  const double be = sc[SC_BETA], mean = sc[SC_PMEAN];
   auto pv = [&](int j) { return z[j] + be * pold[j]; };
-  double v = 0.0;
-  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) v += pv((o.nr - 1) + o.nr * k);
-  double ms = block_sum(v, sh);
-  __syncthreads();
-  if (threadIdx.x == 0) sh[32] = ms / o.nz;
-  __syncthreads();
-  const double mean = sh[32];
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
     const int j = i % o.nr, k = i / o.nr;
@@ -352,7 +358,6 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_pq(K2dOp o, const double *
     q[i] = y;
     acc += xc * y;
   }
-  __syncthreads();
   double s = block_sum(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
   if (!arrived_last(counter)) return;
@@ -370,6 +375,8 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, do
                                                        double *__restrict__ r, double *__restrict__ z,
                                                        const double *__restrict__ p, const double *__restrict__ q,
                                                        double *sc, double *part, unsigned *counter, int *flags) {
+  // (the last block also forms the next direction's last-row mean, so the
+  // first kernel of the next iteration needs no reduction over that row)
   __shared__ double sh[40];
   if (flags[0]) return;
   const double al = sc[SC_ALPHA];
@@ -391,8 +398,16 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, do
   if (!arrived_last(counter)) return;
   const double b = sum_part_l2(part + kK2dMaxBlocks, gridDim.x, sh);
   const double c = sum_part_l2(part + 2 * kK2dMaxBlocks, gridDim.x, sh);
+  const double be = b / sc[SC_RZ];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) {
+    const int j = (o.nr - 1) + o.nr * k;
+    v += __ldcg(z + j) + be * p[j];
+  }
+  const double ms = block_sum(v, sh);
   if (threadIdx.x == 0) {
-    sc[SC_BETA] = b / sc[SC_RZ];
+    sc[SC_PMEAN] = ms / o.nz;
+    sc[SC_BETA] = be;
     sc[SC_RZ] = b;
     sc[SC_RR] = c;
     flags[1] += 1;
@@ -723,6 +738,8 @@ extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, k->dev);
   k->nb = std::min(kK2dMaxBlocks, std::max(1, std::min(2 * nsm, (k->n + kK2dThreads - 1) / kK2dThreads)));
+  k->nb_cg = std::min(kK2dMaxBlocks,
+                      std::max(1, std::min(kK2dCgBlocksPerSm * nsm, (k->n + kK2dThreads - 1) / kK2dThreads)));
   // host coefficients
   const double dz = d->zmax / nz;
   std::vector<double> rm(nr), dr(nr), aw(nr, 0.0), ae(nr, 0.0), az(nr), vol(nr);
@@ -910,7 +927,7 @@ extern "C" int vr_k2d_direct(vr_k2d *k, const double *f, double *x) {
 // captured chunk starts from V_P
 static cudaError_t enqueue_cg_iter(vr_k2d *k, int jacobi, int parity) {
   const K2dOp o = op_of(k);
-  const int gb = k2d_grid(k);
+  const int gb = k->nb_cg;
   double *P = k->part;
   double *x = k->vec[V_X], *r = k->vec[V_R], *q = k->vec[V_Q];
   double *pold = parity ? k->vec[V_V] : k->vec[V_P], *p = parity ? k->vec[V_P] : k->vec[V_V];
@@ -1119,6 +1136,7 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
     k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, jac, B, R, jac ? z : nullptr, P);
     k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_CG_INIT, P, gb, k->sc, k->flags);
     K2D_CUDA(k, cudaMemcpyAsync(Pv, z, bytes, cudaMemcpyDeviceToDevice, k->stream));
+    k2d_cg_pmean<<<1, kK2dThreads, 0, k->stream>>>(o, z, k->sc);
     K2D_CUDA(k, cudaGetLastError());
     rc = run_chunks(k, jac, enq_cg, jac, maxit, &it);
   } else if (method == VR_KRYLOV_BICGSTAB) {
