@@ -47,7 +47,8 @@ constexpr int kFcgKeep = 8;          // directions the flexible CG keeps (trunca
 // scalar slots
 enum K2dScal {
   SC_ALPHA = 0, SC_BETA, SC_RZ, SC_BB, SC_RR, SC_RHO, SC_OMEGA, SC_TOL2, SC_RHO_NEW, SC_SS,
-  SC_PMEAN,  // CG: mean over z of the next direction's last radial row
+  SC_PMEAN,  // CG, BiCGSTAB: mean over z of the next direction's last radial row
+  SC_SMEAN,  // BiCGSTAB: the same for s
   SC_N
 };
 // partial-sum slots
@@ -64,8 +65,9 @@ struct vr_k2d {
   double *part = nullptr;   // PT_N x kK2dMaxBlocks
   double *sc = nullptr;     // SC_N
   int *flags = nullptr;     // done, iterations
-  unsigned *cnt = nullptr;  // arrival counters of the CG kernels' last-block reductions
+  unsigned *cnt = nullptr;  // arrival counters of the CG and BiCGSTAB kernels' last-block reductions
   int cg_parity = 0;        // direction buffer of the next CG iteration being captured
+  int bi_parity = 0;        // p and v buffers of the next BiCGSTAB iteration being captured
   int nb_cg = 1;            // grid of the CG iteration kernels
   // direct solve: forward / inverse z transforms (nz x nz, row-major [kz][k]
   // and [k][kz]) and the radial Thomas factorisation per z mode
@@ -169,24 +171,6 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_axpby(int n, double a, const 
     out[i] = a * X[i] + (Y ? b * Y[i] : 0.0);
 }
 
-__global__ void __launch_bounds__(kK2dThreads) k2d_dots(int n, const double *__restrict__ a1,
-                                                      const double *__restrict__ b1, const double *__restrict__ a2,
-                                                      const double *__restrict__ b2, double *part1, double *part2) {
-  __shared__ double sh[40];
-  double s1 = 0.0, s2 = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    s1 += a1[i] * b1[i];
-    if (a2) s2 += a2[i] * b2[i];
-  }
-  double t = block_sum(s1, sh);
-  if (threadIdx.x == 0) part1[blockIdx.x] = t;
-  if (a2) {
-    __syncthreads();
-    t = block_sum(s2, sh);
-    if (threadIdx.x == 0) part2[blockIdx.x] = t;
-  }
-}
-
 // b = V f (or f for the unsymmetric form), element-wise scale by the cell volume
 __global__ void k2d_scale_vol(K2dOp o, const double *__restrict__ f, double *__restrict__ b, int inv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
@@ -209,13 +193,7 @@ __device__ __forceinline__ double sum_part(const double *p, int nb, double *sh) 
 // one-block scalar steps
 enum K2dScalarOp {
   SO_CG_INIT = 0,   // bb, rz, rr from partials A (b.b), B (r.z), C (r.r)
-  SO_CG_ALPHA,      // alpha = rz / (p.q) [A]
-  SO_CG_BETA,       // rz_new [B], rr [C]: beta, convergence
   SO_BI_INIT,       // bb [A], rho_new = rh.r [B], rr [C]
-  SO_BI_BETA,       // beta from rho_new, rho, alpha, omega
-  SO_BI_ALPHA,      // alpha = rho / rh.v [A]
-  SO_BI_OMEGA,      // omega = t.s [A] / t.t [B]
-  SO_BI_CONV,       // rho_new = rh.r [A], rr [B]
   SO_FCG_CONV,      // rr [A]
   SO_NORM,          // rr [A] only (sc[SC_RR])
   SO_NORM_BB,       // bb [A] only (sc[SC_BB])
@@ -227,11 +205,8 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
   if (flags[0] && op != SO_NORM && op != SO_NORM_BB && op != SO_CG_INIT && op != SO_BI_INIT) return;
   const double *pA = part, *pB = part + kK2dMaxBlocks, *pC = part + 2 * kK2dMaxBlocks;
   double a = sum_part(pA, nb, sh);
-  double b = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT || op == SO_BI_OMEGA ||
-              op == SO_BI_CONV)
-                 ? sum_part(pB, nb, sh)
-                 : 0.0;
-  double c = (op == SO_CG_INIT || op == SO_CG_BETA || op == SO_BI_INIT) ? sum_part(pC, nb, sh) : 0.0;
+  double b = (op == SO_CG_INIT || op == SO_BI_INIT) ? sum_part(pB, nb, sh) : 0.0;
+  double c = (op == SO_CG_INIT || op == SO_BI_INIT) ? sum_part(pC, nb, sh) : 0.0;
   if (threadIdx.x != 0) return;
   switch (op) {
     case SO_CG_INIT:
@@ -242,16 +217,6 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       flags[0] = (c <= sc[SC_TOL2] * a) ? 1 : 0;
       flags[1] = 0;
       break;
-    case SO_CG_ALPHA:
-      sc[SC_ALPHA] = sc[SC_RZ] / a;
-      break;
-    case SO_CG_BETA:
-      sc[SC_BETA] = b / sc[SC_RZ];
-      sc[SC_RZ] = b;
-      sc[SC_RR] = c;
-      flags[1] += 1;
-      if (c <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
-      break;
     case SO_BI_INIT:
       sc[SC_BB] = a;
       sc[SC_RHO_NEW] = b;
@@ -261,22 +226,6 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       sc[SC_OMEGA] = 1.0;
       flags[0] = (c <= sc[SC_TOL2] * a) ? 1 : 0;
       flags[1] = 0;
-      break;
-    case SO_BI_BETA:
-      sc[SC_BETA] = (sc[SC_RHO_NEW] / sc[SC_RHO]) * (sc[SC_ALPHA] / sc[SC_OMEGA]);
-      sc[SC_RHO] = sc[SC_RHO_NEW];
-      break;
-    case SO_BI_ALPHA:
-      sc[SC_ALPHA] = sc[SC_RHO] / a;
-      break;
-    case SO_BI_OMEGA:
-      sc[SC_OMEGA] = b != 0.0 ? a / b : 0.0;
-      break;
-    case SO_BI_CONV:
-      sc[SC_RHO_NEW] = a;
-      sc[SC_RR] = b;
-      flags[1] += 1;
-      if (b <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
       break;
     case SO_FCG_CONV:
       sc[SC_RR] = a;
@@ -294,7 +243,7 @@ __global__ void __launch_bounds__(1024) k2d_scalar(int op, const double *part, i
       break;
   }
   // iteration cap (flags[2]): stop as not converged
-  if ((op == SO_CG_BETA || op == SO_BI_CONV || op == SO_FCG_CONV) && !flags[0] && flags[1] >= flags[2]) flags[0] = 2;
+  if (op == SO_FCG_CONV && !flags[0] && flags[1] >= flags[2]) flags[0] = 2;
 }
 
 // A CG iteration is two kernels.  Each ends with a reduction of its blocks'
@@ -417,35 +366,130 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_cg_xr(K2dOp o, int jacobi, do
   }
 }
 
-// BiCGSTAB p = r + beta (p - omega v)
-__global__ void __launch_bounds__(kK2dThreads) k2d_bi_p(int n, double *__restrict__ p, const double *__restrict__ r,
-                                                      const double *__restrict__ v, const double *sc,
-                                                      const int *flags) {
-  if (flags[0]) return;
-  const double be = sc[SC_BETA], om = sc[SC_OMEGA];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = r[i] + be * (p[i] - om * v[i]);
+// (K x)(i) = (S x)(i) / vol with x given as a function of the index and the
+// mean over z of x's last radial row (the wall term)
+template <class F>
+__device__ __forceinline__ double apply_K_fn(const K2dOp &o, const F &xv, int i, double mean) {
+  const int j = i % o.nr, k = i / o.nr;
+  const double xc = xv(i);
+  double y = 0.0;
+  if (j > 0) y += o.aw[j] * (xc - xv(i - 1));
+  if (j < o.nr - 1) y += o.ae[j] * (xc - xv(i + 1));
+  else y += o.gam * mean;
+  const double az = o.az[j];
+  if (k > 0) y += az * (xc - xv(i - o.nr));
+  if (k < o.nz - 1) y += az * (xc - xv(i + o.nr));
+  return y / o.vol[j];
 }
 
-// s = r - alpha v
-__global__ void __launch_bounds__(kK2dThreads) k2d_bi_s(int n, double *__restrict__ s, const double *__restrict__ r,
-                                                      const double *__restrict__ v, const double *sc,
-                                                      const int *flags) {
+// BiCGSTAB in three kernels per iteration, the scalar steps in the block
+// that arrives last (as for CG).  First: p = r + beta (p_old - omega v_old)
+// formed where the operator needs it, v = K p, both into the other buffers;
+// partials rh.v; the last block: rho = rho_new, alpha = rho / rh.v, and the
+// mean of s = r - alpha v over the last radial row
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_pv(K2dOp o, const double *__restrict__ r,
+                                                       const double *__restrict__ pold,
+                                                       const double *__restrict__ vold, const double *__restrict__ rh,
+                                                       double *__restrict__ p, double *__restrict__ v, double *sc,
+                                                       double *part, unsigned *counter, const int *flags) {
+  __shared__ double sh[40];
   if (flags[0]) return;
-  const double al = sc[SC_ALPHA];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s[i] = r[i] - al * v[i];
+  const double be = sc[SC_BETA], om = sc[SC_OMEGA], mean = sc[SC_PMEAN];
+  auto pv = [&](int j) { return r[j] + be * (pold[j] - om * vold[j]); };
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double y = apply_K_fn(o, pv, i, mean);
+    p[i] = pv(i);
+    v[i] = y;
+    acc += rh[i] * y;
+  }
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  if (!arrived_last(counter)) return;
+  const double rhv = sum_part_l2(part, gridDim.x, sh);
+  const double al = sc[SC_RHO_NEW] / rhv;
+  double m = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) {
+    const int j = (o.nr - 1) + o.nr * k;
+    m += r[j] - al * __ldcg(v + j);
+  }
+  const double ms = block_sum(m, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_RHO] = sc[SC_RHO_NEW];
+    sc[SC_ALPHA] = al;
+    sc[SC_SMEAN] = ms / o.nz;
+    *counter = 0;
+  }
 }
 
-// x += alpha p + omega s; r = s - omega t; partials rh.r [A], r.r [B]
-__global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr(int n, double *__restrict__ x, double *__restrict__ r,
-                                                       const double *__restrict__ p, const double *__restrict__ s,
-                                                       const double *__restrict__ t, const double *__restrict__ rh,
-                                                       const double *sc, double *part, const int *flags) {
+// second: s = r - alpha v formed where the operator needs it, t = K s;
+// partials t.s [A], t.t [B]; the last block: omega = t.s / t.t
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_st(K2dOp o, const double *__restrict__ r,
+                                                       const double *__restrict__ v, double *__restrict__ s,
+                                                       double *__restrict__ t, double *sc, double *part,
+                                                       unsigned *counter, const int *flags) {
+  __shared__ double sh[40];
+  if (flags[0]) return;
+  const double al = sc[SC_ALPHA], mean = sc[SC_SMEAN];
+  auto sv = [&](int j) { return r[j] - al * v[j]; };
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
+    const double y = apply_K_fn(o, sv, i, mean), si = sv(i);
+    s[i] = si;
+    t[i] = y;
+    a += si * y;
+    b += y * y;
+  }
+  double x = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = x;
+  __syncthreads();
+  x = block_sum(b, sh);
+  if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = x;
+  if (!arrived_last(counter)) return;
+  const double ts = sum_part_l2(part, gridDim.x, sh);
+  const double tt = sum_part_l2(part + kK2dMaxBlocks, gridDim.x, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_OMEGA] = tt != 0.0 ? ts / tt : 0.0;
+    *counter = 0;
+  }
+}
+
+// beta of the next direction and the mean over z of its last radial row,
+// from r, p, v and the scalars (the first direction: p = v = 0)
+__device__ __forceinline__ void bi_next(const K2dOp &o, const double *r, const double *p, const double *v,
+                                        double *sc, double *sh) {
+  const double be = (sc[SC_RHO_NEW] / sc[SC_RHO]) * (sc[SC_ALPHA] / sc[SC_OMEGA]), om = sc[SC_OMEGA];
+  double m = 0.0;
+  for (int k = threadIdx.x; k < o.nz; k += blockDim.x) {
+    const int j = (o.nr - 1) + o.nr * k;
+    m += __ldcg(r + j) + be * (p[j] - om * v[j]);
+  }
+  const double ms = block_sum(m, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_BETA] = be;
+    sc[SC_PMEAN] = ms / o.nz;
+  }
+}
+
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_first(K2dOp o, const double *r, const double *p,
+                                                          const double *v, double *sc) {
+  __shared__ double sh[40];
+  bi_next(o, r, p, v, sc, sh);
+}
+
+// third: x += alpha p + omega s; r = s - omega t; partials rh.r [A], r.r [B];
+// the last block: rho_new, rr, the convergence and iteration-cap flags, and
+// the next direction's beta and row mean
+__global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr3(K2dOp o, double *__restrict__ x, double *__restrict__ r,
+                                                        const double *__restrict__ p, const double *__restrict__ v,
+                                                        const double *__restrict__ s, const double *__restrict__ t,
+                                                        const double *__restrict__ rh, double *sc, double *part,
+                                                        unsigned *counter, int *flags) {
   __shared__ double sh[40];
   if (flags[0]) return;
   const double al = sc[SC_ALPHA], om = sc[SC_OMEGA];
   double a = 0.0, b = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) {
     x[i] += al * p[i] + om * s[i];
     const double ri = s[i] - om * t[i];
     r[i] = ri;
@@ -457,6 +501,19 @@ __global__ void __launch_bounds__(kK2dThreads) k2d_bi_xr(int n, double *__restri
   __syncthreads();
   t1 = block_sum(b, sh);
   if (threadIdx.x == 0) part[kK2dMaxBlocks + blockIdx.x] = t1;
+  if (!arrived_last(counter)) return;
+  const double rhr = sum_part_l2(part, gridDim.x, sh);
+  const double rr = sum_part_l2(part + kK2dMaxBlocks, gridDim.x, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_RHO_NEW] = rhr;
+    sc[SC_RR] = rr;
+    flags[1] += 1;
+    if (rr <= sc[SC_TOL2] * sc[SC_BB]) flags[0] = 1;
+    if (!flags[0] && flags[1] >= flags[2]) flags[0] = 2;  // iteration cap: stop as not converged
+  }
+  __syncthreads();
+  bi_next(o, r, p, v, sc, sh);
+  if (threadIdx.x == 0) *counter = 0;
 }
 
 // partial sum of (D r)^2 [A] (the learned preconditioner's input scale)
@@ -802,8 +859,8 @@ extern "C" int vr_k2d_create(const vr_k2d_desc *d, vr_k2d **out) {
   if (cudaMalloc(&k->part, sizeof(double) * PT_N * kK2dMaxBlocks) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->sc, sizeof(double) * SC_N) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->flags, sizeof(int) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
-  if (cudaMalloc(&k->cnt, sizeof(unsigned) * 2) != cudaSuccess) return fail(VR_ERR_OOM);
-  if (cudaMemset(k->cnt, 0, sizeof(unsigned) * 2) != cudaSuccess) return fail(VR_ERR_CUDA);
+  if (cudaMalloc(&k->cnt, sizeof(unsigned) * 4) != cudaSuccess) return fail(VR_ERR_OOM);
+  if (cudaMemset(k->cnt, 0, sizeof(unsigned) * 4) != cudaSuccess) return fail(VR_ERR_CUDA);
   if (cudaMalloc(&k->dct_f, sizeof(double) * cf.size()) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->dct_i, sizeof(double) * ci.size()) != cudaSuccess) return fail(VR_ERR_OOM);
   if (cudaMalloc(&k->tlo, sizeof(double) * nr) != cudaSuccess) return fail(VR_ERR_OOM);
@@ -937,23 +994,18 @@ static cudaError_t enqueue_cg_iter(vr_k2d *k, int jacobi, int parity) {
   return cudaGetLastError();
 }
 
-static cudaError_t enqueue_bicg_iter(vr_k2d *k) {
+// p and v alternate between two buffers each (V_P / V_Q and V_V / V_Z), since
+// an iteration forms its p and v from the previous ones at every stencil point
+static cudaError_t enqueue_bicg_iter(vr_k2d *k, int parity) {
   const K2dOp o = op_of(k);
-  const int gb = k2d_grid(k);
+  const int gb = k->nb_cg;
   double *P = k->part;
-  double *x = k->vec[V_X], *r = k->vec[V_R], *p = k->vec[V_P], *v = k->vec[V_V], *s = k->vec[V_S],
-         *t = k->vec[V_T], *rh = k->vec[V_RH];
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_BETA, P, gb, k->sc, k->flags);
-  k2d_bi_p<<<gb, kK2dThreads, 0, k->stream>>>(o.n, p, r, v, k->sc, k->flags);
-  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, p, v, 1, rh, P, k->flags);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_ALPHA, P, gb, k->sc, k->flags);
-  k2d_bi_s<<<gb, kK2dThreads, 0, k->stream>>>(o.n, s, r, v, k->sc, k->flags);
-  // t = K s with partials t.s [A]; t.t [B] from a dots pass
-  k2d_apply<<<gb, kK2dThreads, 0, k->stream>>>(o, s, t, 1, s, P, k->flags);
-  k2d_dots<<<gb, kK2dThreads, 0, k->stream>>>(o.n, t, t, nullptr, nullptr, P + kK2dMaxBlocks, nullptr);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_OMEGA, P, gb, k->sc, k->flags);
-  k2d_bi_xr<<<gb, kK2dThreads, 0, k->stream>>>(o.n, x, r, p, s, t, rh, k->sc, P, k->flags);
-  k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_CONV, P, gb, k->sc, k->flags);
+  double *x = k->vec[V_X], *r = k->vec[V_R], *s = k->vec[V_S], *t = k->vec[V_T], *rh = k->vec[V_RH];
+  double *pold = parity ? k->vec[V_Q] : k->vec[V_P], *p = parity ? k->vec[V_P] : k->vec[V_Q];
+  double *vold = parity ? k->vec[V_Z] : k->vec[V_V], *v = parity ? k->vec[V_V] : k->vec[V_Z];
+  k2d_bi_pv<<<gb, kK2dThreads, 0, k->stream>>>(o, r, pold, vold, rh, p, v, k->sc, P, k->cnt + 2, k->flags);
+  k2d_bi_st<<<gb, kK2dThreads, 0, k->stream>>>(o, r, v, s, t, k->sc, P, k->cnt + 3, k->flags);
+  k2d_bi_xr3<<<gb, kK2dThreads, 0, k->stream>>>(o, x, r, p, v, s, t, rh, k->sc, P, k->cnt + 1, k->flags);
   return cudaGetLastError();
 }
 
@@ -993,7 +1045,11 @@ static cudaError_t enq_cg(vr_k2d *k, int jacobi) {
   k->cg_parity ^= 1;
   return e;
 }
-static cudaError_t enq_bicg(vr_k2d *k, int) { return enqueue_bicg_iter(k); }
+static cudaError_t enq_bicg(vr_k2d *k, int) {
+  const cudaError_t e = enqueue_bicg_iter(k, k->bi_parity);
+  k->bi_parity ^= 1;
+  return e;
+}
 
 // One iteration of the flexible CG with the learned preconditioner:
 // z = s D N(D r / s) (D = diag(S)^-1/2, s the RMS of D r); the new direction
@@ -1146,6 +1202,7 @@ extern "C" int vr_k2d_solve_dev(vr_k2d *k, int32_t method, const double *f, doub
     // partials: b.b [A], rh.r = r.r [B], r.r [C]
     k2d_init_dots<<<gb, kK2dThreads, 0, k->stream>>>(o, 0, B, R, nullptr, P);
     k2d_scalar<<<1, 1024, 0, k->stream>>>(SO_BI_INIT, P, gb, k->sc, k->flags);
+    k2d_bi_first<<<1, kK2dThreads, 0, k->stream>>>(o, R, Pv, k->vec[V_V], k->sc);
     K2D_CUDA(k, cudaGetLastError());
     rc = run_chunks(k, 2, enq_bicg, 0, maxit, &it);
   } else {
