@@ -38,7 +38,10 @@
 namespace vr {
 
 constexpr int kK2dThreads = 256;
-constexpr int kK2dCgBlocksPerSm = 6;  // the CG kernels' grid (no per-block row mean)
+#ifndef VR_K2D_ITER_BLOCKS
+#define VR_K2D_ITER_BLOCKS 6
+#endif
+constexpr int kK2dCgBlocksPerSm = VR_K2D_ITER_BLOCKS;  // the CG and BiCGSTAB kernels' grid per SM
 constexpr int kK2dMaxBlocks = 1024;
 constexpr int kK2dChunk = 32;        // iterations per captured graph
 constexpr int kK2dChunkLearned = 4;  // for the learned flexible CG (each iteration runs the network)
