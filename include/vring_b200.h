@@ -333,9 +333,10 @@ VR_API int vr_ens_launch_count(const vr_ens *e, int64_t *n);
  * timed once per process (force != 0 re-times each class once) */
 VR_API int vr_ens_autotune(vr_ens *e, int32_t force);
 /* Times the candidate tile shapes of the r and z sweeps on this context's grid
- * (r: 16-line TMA tiles, 8-line TMA tiles, register chunks; z: 8-line TMA,
- * 16-line TMA, register chunks; variants a line length does not fit fall back
- * to register chunks), keeps the fastest pair and caches it per grid class for
+ * (r: 16-line TMA tiles, 8-line TMA tiles, register chunks; z lines of up to
+ * 272 positions: 8-line TMA, 16-line TMA, register chunks; longer z lines:
+ * 16-line TMA, 8-line TMA, register chunks; variants a line length does not
+ * fit fall back to register chunks), keeps the fastest pair and caches it per grid class for
  * the process.  The context's fields and clock are restored afterwards (the
  * trials need a temporary device copy of the state).  choice (may be NULL)
  * receives {r variant, z variant}. */

@@ -67,6 +67,29 @@ def test_every_tile_variant_matches_oracle(rv, zv):
     gpu.close()
 
 
+@pytest.mark.parametrize("rv,zv", [(0, 0), (0, 1), (1, 1)])
+def test_long_line_tile_variants_match_oracle(rv, zv):
+    # radial lines of 300-301 positions and axial lines of 513-514: beyond
+    # the 16 x 17 positions of the 256-thread tiles, so the 16-line tiles run
+    # as 32 chunks in one 512-thread CTA per SM (r and z by default; variant
+    # 1 the 8-line tiles)
+    import vring_b200 as V
+    from vring_b200.synthetic import ring_fields
+    nth, nr, nz = 16, 300, 512
+    orc, gpu = make_pair(nth, nr, nz, dt=1e-3, re=2000.0, slip=1.0)
+    V.set_tiles(gpu, rv, zv)
+    q = ring_fields(nth, nr, nz, 4.0, 12.0, R=1.0, sigma=0.2, noise=1e-3, seed=6)
+    for n, a in zip(("q1", "q2", "q3"), q):
+        orc.field(n)[...] = a
+        gpu.set(n, a)
+    prep(orc, gpu, 2, 0.0, 0)
+    orc.substep(2)
+    gpu.substep(2)
+    for n in STATE + ["dph"]:
+        assert_field_close(gpu, orc, n, rel=1e-11)
+    gpu.close()
+
+
 def test_autotune_restores_state_and_caches():
     import vring_b200 as V
     from vring_b200 import ensemble as E

@@ -1268,22 +1268,32 @@ static cudaError_t dispatch_linesweep(vr_ctx *c, const SweepArgsT<T> &s, const C
     p.nbx = (s.nth + 31) / 32;
     const Geo &g = c->geo;
     LaunchScope ls(c, s.se == g.nth ? PK_RSWEEP : PK_ZSWEEP);
-    // TMA-pipelined persistent form, two 256-thread CTAs per SM: by default
-    // 16-line tiles along r, 8-line tiles along z (lines of up to 544
-    // positions need the narrower tile to keep two stages per CTA in shared
-    // memory); the autotuner may pick the other tile or the register form
+    // TMA-pipelined persistent form.  Wide tiles: 16 lines (128-byte rows),
+    // as 16 chunks in two 256-thread CTAs per SM for lines of up to 272
+    // positions, as 32 chunks in one 512-thread CTA per SM beyond (two stages
+    // of a 544-position tile fill 136 KB).  Narrow tiles: 8 lines (64-byte
+    // rows) as 32 chunks in two 256-thread CTAs per SM.  By default r lines
+    // and z lines beyond 272 positions run wide tiles (the z rows of a wide
+    // tile are twice as long, measured 10 % faster at 513 positions), shorter
+    // z lines narrow ones; variant 1 takes the other shape, variant 2 the
+    // register form, as the autotuner picks
     const bool along_r = s.se == g.nth;
     const int v = along_r ? c->tune_r : c->tune_z;
     const int ldim = along_r ? 1 : 2;
     cudaError_t e = cudaErrorNotSupported;
     // chunks of 16 when the line fits them (256 / 512 positions): one
     // substitution step less on every thread's dependent chain than 17
+    const bool wide = (along_r || p.n > 16 * 17) != (v == 1);
     if (v == 2) {
-    } else if ((v == 0) == along_r) {
+    } else if (wide) {
       if (p.n <= 16 * 16)
         e = run_chunk_tma<16, 16, 16, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
-      else
+      else if (p.n <= 16 * 17)
         e = run_chunk_tma<16, 16, 17, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+      else if (p.n <= 32 * 16)
+        e = run_chunk_tma<16, 32, 16, 2, 1>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
+      else
+        e = run_chunk_tma<16, 32, 17, 2, 1>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
     } else {
       if (p.n <= 32 * 16)
         e = run_chunk_tma<8, 32, 16, 2, 2>(p, s.in, g.nth, g.J3, g.K3, ldim, nm2, c->nsm, c->d_status, c->stream);
