@@ -920,9 +920,12 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
     tma_load_3d(buf(s), &tm, i0, j, 0, bar);
     tma_load_3d(buf(s) + 256 * 8, &tm, i0, j, 256, bar);
   };
+  // the first tiles start loading while the CTA stages its twiddles (the
+  // other threads wait on the barriers only after the CTA barrier below)
   if (tid == 0) {
     for (int b = 0; b < kDctBufs; b++) mbar_init(&full[b], 1);
     mbar_init_fence();
+    for (int s = 0; s < min(nmine, kDctBufs - 1); s++) issue_load(s);
   }
   for (int i = tid; i < 15 * 32; i += 256) {
     const int p = (i & 31) * (i / 32 + 1);
@@ -933,12 +936,20 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
     shl[i] = make_double2(__ldg(twz + 2 * N + 2 * k), __ldg(twz + 2 * N + 2 * k + 1));
   }
   __syncthreads();
-  if (tid == 0)
-    for (int s = 0; s < min(nmine, kDctBufs - 1); s++) issue_load(s);
   auto tw_lane = [&](int k1, double &c, double &sn) {
     const double2 v = twl[(k1 - 1) * 32 + lane];
     c = v.x;
     sn = v.y;
+  };
+  // tile s + 2 loads into the buffer of tile s - 1 once that tile's store
+  // (issued at the end of tile s - 1) has read it out; thread 0 refills it
+  // halfway through tile s, after its warp's FFT, so the load has one and a
+  // half tiles of compute to land instead of one
+  auto refill = [&](int s) {
+    if (tid == 0 && s + kDctBufs - 1 < nmine) {
+      bulk_wait_read<0>();
+      issue_load(s + kDctBufs - 1);
+    }
   };
   int s = 0;
   bool failed = false;
@@ -961,6 +972,7 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
       }
       __syncwarp();
       warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+      refill(s);
       __syncwarp();
       const SwzScratch<1> out{b, warp};
 #pragma unroll
@@ -1001,6 +1013,7 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
       __syncwarp();
       // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
       warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+      refill(s);
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < 16; q++) {
@@ -1016,10 +1029,6 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
       tma_store_3d(&tm, i0, j, 0, b);
       tma_store_3d(&tm, i0, j, 256, b + 256 * 8);
       bulk_commit();
-      if (s + kDctBufs - 1 < nmine) {
-        bulk_wait_read<1>();  // the store of tile s - 1, in the buffer refilled next, has left it
-        issue_load(s + kDctBufs - 1);
-      }
     }
   }
   if (tid == 0) {
