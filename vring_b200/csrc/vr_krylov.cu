@@ -20,8 +20,13 @@
 // (poisson.F90:379-381).
 //
 // Every reduction is deterministic: vector kernels write one partial sum per
-// block, and a one-block kernel adds the partials in a fixed order into the
-// scalars the next vector kernel reads.  Iterations are issued in chunks
+// block, and the partials are added in block order into the scalars the next
+// kernel reads -- by the block that finishes last (a ticket counter after a
+// memory fence) in the CG and BiCGSTAB kernels, which also take the scalar
+// steps there, and by a one-block kernel in the setup and the flexible CG.
+// CG runs two kernels per iteration and BiCGSTAB three: each operator
+// application forms the vector it applies (the new direction, or s) as it
+// reads it.  Iterations are issued in chunks
 // captured as CUDA graphs; a device flag set at convergence turns the rest of
 // a chunk into early returns, and the host reads the flag between chunks.
 #include <cuda_runtime.h>
