@@ -32,7 +32,7 @@ def quarter_warp_degree(chunks):
     return worst
 
 
-# ---- k_dct_tma: 128B-swizzled 16-column tiles, warp w owns chunk w ----------
+# ---- warp_fft512 (the slab kernels): 128B-swizzled 16-column tiles, warp w owns chunk w
 
 def swz_word(r, w):
     """16-byte word of (row r, chunk w) in a 128B-swizzled tile (swz_pair)."""
@@ -192,3 +192,113 @@ def test_fft_inverse_packed_staging_is_conflict_free_at_128():
         assert quarter_warp_degree_active(even) == 1, m
         plain = [fft_natural_word(T, pl, 2 * kk) if 0 < 2 * kk < N else None for pl, kk in kks]
         assert quarter_warp_degree_active(plain) == 2  # the unpermuted layout
+
+
+# ---- k_dct_tma: two warps per column pair, N = 8 x 8 x 8 ----------------------
+# thread u = lane + 32 h of pair p (warps 2p, 2p + 1) owns chunk p of each row
+
+def pfft_k2(u):
+    return ((u >> 5) << 2) | (u & 3)
+
+
+def pfft_c(u):
+    return (u >> 2) & 7
+
+
+def pfft_r2(k2, a, c):
+    return 64 * k2 + 8 * c + (a ^ (((k2 & 3) << 1) | (c & 1)))
+
+
+def pfft_p(m):
+    return m ^ (((m >> 3) & 1) << 2)
+
+
+def mk_row(n):
+    return 2 * n if n < 256 else 1023 - 2 * n
+
+
+def pair_degree(row_of_u, p):
+    """worst quarter-warp degree over the two warps of pair p"""
+    return max(quarter_warp_degree([swz_word(row_of_u(l + 32 * h), p) for l in range(32)]) for h in range(2))
+
+
+def test_pair_fft_maps_are_permutations():
+    assert sorted(64 * k2 + n1 for k2 in range(8) for n1 in range(64)) == list(range(512))
+    assert sorted(pfft_r2(k2, a, c) for k2 in range(8) for a in range(8) for c in range(8)) == list(range(512))
+    assert sorted(pfft_p(m) for m in range(512)) == list(range(512))
+    assert sorted(mk_row(n) for n in range(512)) == list(range(512))
+    # after the FFT every (k2, c) is held by exactly one thread
+    assert sorted(pfft_k2(u) + 8 * pfft_c(u) for u in range(64)) == list(range(64))
+
+
+def test_pair_fft_transposes_are_conflict_free():
+    for p in range(8):
+        for k2 in range(8):  # writes: entry (n1 = u, k2) at row 64 k2 + n1
+            assert pair_degree(lambda u: 64 * k2 + u, p) == 1
+        for b in range(8):  # reads by thread (k2, a) = (u / 8, u % 8) of entry (a + 8 b, k2)
+            assert pair_degree(lambda u: 64 * (u >> 3) + (u & 7) + 8 * b, p) == 1
+        for c in range(8):  # second transpose, writes by thread (u / 8, u % 8)
+            assert pair_degree(lambda u: pfft_r2(u >> 3, u & 7, c), p) == 1
+        for a in range(8):  # reads by thread (pfft_k2, pfft_c)
+            assert pair_degree(lambda u: pfft_r2(pfft_k2(u), a, pfft_c(u)), p) == 1
+
+
+def test_pair_dct_data_rows_degree():
+    for p in range(8):
+        for q in range(4):  # forward loads: lanes with u & 4 take slot q + 4 first
+            assert pair_degree(lambda u: mk_row(u + 64 * (q + 4 if (u >> 2) & 1 else q)), p) == 1
+            assert pair_degree(lambda u: mk_row(u + 64 * (q if (u >> 2) & 1 else q + 4)), p) == 1
+            # without the swap the even rows 2n would be 2-way
+            assert pair_degree(lambda u: mk_row(u + 64 * q), p) == 2
+        for d in range(8):  # forward: X[m] to scratch row pfft_p(m)
+            assert pair_degree(lambda u: pfft_p(pfft_k2(u) + 8 * pfft_c(u) + 64 * d), p) == 1
+        for q in range(8):
+            assert pair_degree(lambda u: pfft_p(u + 64 * q), p) == 1
+            # the partner rows 512 - k cross a block of 8 rows: 2-way
+            assert pair_degree(lambda u: pfft_p((512 - u - 64 * q) & 511), p) == 2
+            assert pair_degree(lambda u: u + 64 * q, p) == 1  # results; inverse loads of k
+            assert pair_degree(lambda u: (512 - u - 64 * q) & 511, p) == 1  # inverse loads of 512 - k
+        for j in range(8):  # inverse outputs: lanes with odd c take slot j ^ 4 first
+            def row(u):
+                d = j ^ 4 if pfft_c(u) & 1 else j
+                return mk_row(pfft_k2(u) + 8 * pfft_c(u) + 64 * d)
+            assert pair_degree(row, p) == 1
+
+
+def test_pair_fft_decomposition_matches_numpy():
+    # the three radix-8 stages with the kernel's index maps, each 8-point DFT
+    # leaving X[k] in slot brev3(k), against numpy's FFT
+    import numpy as np
+    N = 512
+    W = lambda e, n: np.exp(-2j * np.pi * e / n)
+
+    def dft8(v):
+        X = np.fft.fft(v)
+        out = np.empty(8, complex)
+        for k in range(8):
+            out[brev(k, 3)] = X[k]
+        return out
+
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    scratch = np.empty(N, complex)
+    for u in range(64):
+        y = dft8(x[u + 64 * np.arange(8)])
+        for k2 in range(8):
+            scratch[64 * k2 + u] = y[brev(k2, 3)] * W(u * k2, 512)
+    mid = {}
+    for u in range(64):
+        k2, a = u >> 3, u & 7
+        mid[u] = dft8(np.array([scratch[64 * k2 + a + 8 * b] for b in range(8)]))
+    for u in range(64):
+        k2, a = u >> 3, u & 7
+        for c in range(8):
+            scratch[pfft_r2(k2, a, c)] = mid[u][brev(c, 3)] * W(a * c, 64)
+    X = np.empty(N, complex)
+    for u in range(64):
+        k2, c = pfft_k2(u), pfft_c(u)
+        z = dft8(np.array([scratch[pfft_r2(k2, a, c)] for a in range(8)]))
+        for d in range(8):
+            X[k2 + 8 * c + 64 * d] = z[brev(d, 3)]
+    ref = np.fft.fft(x)
+    assert np.abs(X - ref).max() <= 1e-13 * np.abs(ref).max()

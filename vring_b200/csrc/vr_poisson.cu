@@ -860,15 +860,9 @@ __global__ void __launch_bounds__(LT * 16) k_dct_w(double *__restrict__ a, Geo g
 }
 
 // ---------------------------------------------------------------------------
-// z transforms of length 512 streamed by TMA.  A persistent CTA of eight
-// warps takes tiles of 16 consecutive slots at one radial index (16 columns x
-// 512 planes, 64 KB) in turn; three shared-memory buffers rotate, so that
-// while the warps transform tile s in place, tile s + 1 is loading and tile
-// s - 1 is being stored.  Tiles arrive 128B-swizzled: the 16-byte chunk with
-// columns 2w, 2w + 1 of row k sits at chunk w ^ (k & 7), and warp w moves its
-// (re, im) pairs as 16-byte words on distinct banks.  The arithmetic is that
-// of k_dct_w (Makhoul's reordering, the 16 x 32 warp FFT, the quarter-wave
-// shift), so both give the same bits.
+// Shared by the z transforms of length 512: tiles of 16 consecutive slots at
+// one radial index (16 columns x 512 planes, 64 KB) arrive 128B-swizzled, the
+// 16-byte chunk with columns 2w, 2w + 1 of row k at chunk w ^ (k & 7).
 // ---------------------------------------------------------------------------
 constexpr int kDctTileCols = 16, kDctN = 512, kDctBufs = 3;
 constexpr unsigned kDctTileBytes = kDctTileCols * kDctN * 8;  // 65,536
@@ -898,18 +892,109 @@ struct SwzScratch {
   }
 };
 
+// ---------------------------------------------------------------------------
+// z transforms of length 512 streamed by TMA.  A persistent CTA of 16 warps
+// takes the 64 KB tiles in turn; three shared-memory buffers rotate, so that
+// while the warps transform tile s in place, tile s + 1 is loading and tile
+// s - 1 is being stored.  The 64 threads of pair p (warps 2p, 2p + 1; at most
+// 128 registers each) transform columns 2p, 2p + 1 as one complex sequence
+// with N = 8 x 64 = 8 x 8 x 8:
+//   X[k2 + 8 c + 64 d] = sum_a W_8^{a d} W_64^{a c} sum_b W_8^{b c}
+//                        W_512^{n1 k2} sum_n2 x[n1 + 64 n2] W_8^{n2 k2},
+//   n1 = a + 8 b,
+// three radix-8 stages in registers (reg_dif), two transposes through the
+// pair's own chunk column of the tile (rows chosen so that every quarter
+// warp meets eight distinct 16-byte chunks), and a 64-thread named barrier
+// (1 + p) between the phases that share the column.  Around the FFT, Makhoul's
+// even/odd reordering and the quarter-wave shift turn it into the DCT-II
+// (forward, scaled 1 / (2 N)) or the DCT-III (inverse).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(pair + 1) : "memory");
+}
+
+__device__ __forceinline__ void tw_mul(double &r, double &i, double2 w) {  // (r + i i)(w.x + i w.y)
+  const double xr = r * w.x - i * w.y, xi = r * w.y + i * w.x;
+  r = xr;
+  i = xi;
+}
+
+// thread u of a pair after the FFT: k2 = 4 (u / 32) + u % 4, c = (u / 4) % 8
+__device__ __forceinline__ int pfft_k2(int u) { return ((u >> 5) << 2) | (u & 3); }
+__device__ __forceinline__ int pfft_c(int u) { return (u >> 2) & 7; }
+// row of entry (k2, a, c) of the second transpose
+__device__ __forceinline__ int pfft_r2(int k2, int a, int c) {
+  return 64 * k2 + 8 * c + (a ^ (((k2 & 3) << 1) | (c & 1)));
+}
+
+// Forward DFT of x[u + 64 q] held in re/im[q] by thread u of pair `pair`;
+// column `pair` of the swizzled tile b is the scratch (its rows no longer
+// needed: the caller has synchronised the pair after its last read).  On
+// return slot brev3(d) holds X[k2 + 8 c + 64 d] (k2 = pfft_k2(u), c =
+// pfft_c(u)); the scratch is still being read until the pair synchronises.
+// tw1[(k2 - 1) 64 + n1] = W_512^{n1 k2}, tw2[(c - 1) 8 + a] = W_64^{a c}.
+__device__ __forceinline__ void pair_fft512(double (&re)[8], double (&im)[8], double2 *b, int pair, int u,
+                                            const double2 *tw1, const double2 *tw2) {
+  constexpr int N = 512;
+  // 8-point DFTs over n2, then W_512^{n1 k2}; entry (n1, k2) at row 64 k2 + n1
+  reg_dif<8, N, 0, 8>(re, im);
+#pragma unroll
+  for (int k2 = 0; k2 < 8; k2++) {
+    const int rg = brev_c(k2, 3);
+    double yr = re[rg], yi = im[rg];
+    if (k2) tw_mul(yr, yi, tw1[(k2 - 1) * 64 + u]);
+    *swz_pair(b, 64 * k2 + u, pair) = make_double2(yr, yi);
+  }
+  pair_sync(pair);
+  // thread (k2, a) = (u / 8, u % 8): 8-point DFTs over b of Y'[a + 8 b][k2]
+  {
+    const int k2 = u >> 3, a = u & 7;
+#pragma unroll
+    for (int bb = 0; bb < 8; bb++) {
+      const double2 v = *swz_pair(b, 64 * k2 + a + 8 * bb, pair);
+      re[bb] = v.x;
+      im[bb] = v.y;
+    }
+    reg_dif<8, N, 0, 8>(re, im);
+    pair_sync(pair);  // every entry of the first transpose has been read
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int rg = brev_c(c, 3);
+      double yr = re[rg], yi = im[rg];
+      if (c) tw_mul(yr, yi, tw2[(c - 1) * 8 + a]);
+      *swz_pair(b, pfft_r2(k2, a, c), pair) = make_double2(yr, yi);
+    }
+  }
+  pair_sync(pair);
+  // thread (k2, c): 8-point DFTs over a
+  {
+    const int k2 = pfft_k2(u), c = pfft_c(u);
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      const double2 v = *swz_pair(b, pfft_r2(k2, a, c), pair);
+      re[a] = v.x;
+      im[a] = v.y;
+    }
+    reg_dif<8, N, 0, 8>(re, im);
+  }
+}
+
+// Makhoul's source row of sequence index n (v_n = x_{2n}, v_{N-1-n} = x_{2n+1})
+__device__ __forceinline__ int mk_row(int n) { return n < 256 ? 2 * n : 1023 - 2 * n; }
+// scratch row of X[m] between the FFT and the forward post-processing
+__device__ __forceinline__ int pfft_p(int m) { return m ^ (((m >> 3) & 1) << 2); }
+
 template <int DIR>
-__global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUtensorMap tm, int nti, int ntiles,
-                                                    const double *__restrict__ twz, unsigned *status) {
+__global__ void __launch_bounds__(512, 1) k_dct_tma(const __grid_constant__ CUtensorMap tm, int nti, int ntiles,
+                                                     const double *__restrict__ twz, unsigned *status) {
   constexpr int N = kDctN;
   extern __shared__ unsigned char dct_dsm[];
   __shared__ __align__(8) uint64_t full[kDctBufs];
   double2 *const buf0 = reinterpret_cast<double2 *>(((uintptr_t)dct_dsm + 1023) & ~(uintptr_t)1023);
-  // this CTA's copy of the lane twiddles W_512^{lane k1} (cos, -sin) at
-  // [k1 - 1][lane] and of the shift e^{i pi k / 1024} at [q][lane],
-  // k = lane + 32 q: every read of a warp is 32 consecutive pairs
-  double2 *const twl = buf0 + kDctBufs * (kDctTileBytes / 16), *const shl = twl + 15 * 32;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double2 *const tw1 = buf0 + kDctBufs * (kDctTileBytes / 16);  // [k2 - 1][n1]: W_512^{n1 k2}
+  double2 *const tw2 = tw1 + 7 * 64;                              // [c - 1][a]: W_64^{a c}
+  double2 *const shl = tw2 + 7 * 8;                               // [k]: e^{i pi k / 1024}
+  const int tid = threadIdx.x, pair = tid >> 6, u = tid & 63;
   const int bx = blockIdx.x, gx = gridDim.x;
   const int nmine = ntiles > bx ? (ntiles - 1 - bx) / gx + 1 : 0;
   auto buf = [&](int s) { return buf0 + (size_t)(s % kDctBufs) * (kDctTileBytes / 16); };
@@ -920,37 +1005,31 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
     tma_load_3d(buf(s), &tm, i0, j, 0, bar);
     tma_load_3d(buf(s) + 256 * 8, &tm, i0, j, 256, bar);
   };
-  // the first tiles start loading while the CTA stages its twiddles (the
-  // other threads wait on the barriers only after the CTA barrier below)
+  // the first tiles start loading while the CTA stages its twiddles
   if (tid == 0) {
-    for (int b = 0; b < kDctBufs; b++) mbar_init(&full[b], 1);
+    for (int bf = 0; bf < kDctBufs; bf++) mbar_init(&full[bf], 1);
     mbar_init_fence();
     for (int s = 0; s < min(nmine, kDctBufs - 1); s++) issue_load(s);
   }
-  for (int i = tid; i < 15 * 32; i += 256) {
-    const int p = (i & 31) * (i / 32 + 1);
-    twl[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
+  for (int i = tid; i < 7 * 64; i += 512) {
+    const int p = (i & 63) * (i / 64 + 1);
+    tw1[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
   }
-  for (int i = tid; i < 16 * 32; i += 256) {
-    const int k = (i & 31) + 32 * (i / 32);
-    shl[i] = make_double2(__ldg(twz + 2 * N + 2 * k), __ldg(twz + 2 * N + 2 * k + 1));
+  for (int i = tid; i < 7 * 8; i += 512) {
+    const int p = 8 * (i & 7) * (i / 8 + 1);
+    tw2[i] = make_double2(__ldg(twz + 2 * p), -__ldg(twz + 2 * p + 1));
   }
+  for (int i = tid; i < N; i += 512) shl[i] = make_double2(__ldg(twz + 2 * N + 2 * i), __ldg(twz + 2 * N + 2 * i + 1));
   __syncthreads();
-  auto tw_lane = [&](int k1, double &c, double &sn) {
-    const double2 v = twl[(k1 - 1) * 32 + lane];
-    c = v.x;
-    sn = v.y;
-  };
   // tile s + 2 loads into the buffer of tile s - 1 once that tile's store
-  // (issued at the end of tile s - 1) has read it out; thread 0 refills it
-  // halfway through tile s, after its warp's FFT, so the load has one and a
-  // half tiles of compute to land instead of one
+  // has read it out; thread 0 refills it halfway through tile s
   auto refill = [&](int s) {
     if (tid == 0 && s + kDctBufs - 1 < nmine) {
       bulk_wait_read<0>();
       issue_load(s + kDctBufs - 1);
     }
   };
+  const int k2 = pfft_k2(u), cc = pfft_c(u);
   int s = 0;
   bool failed = false;
   for (; s < nmine; s++) {
@@ -960,49 +1039,53 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
       break;
     }
     double2 *const b = buf(s);
-    double re[16], im[16];
+    double re[8], im[8];
     if (DIR > 0) {
-      // z_n = v^a_n + i v^b_n, v_n = x_{2n} (n < N/2), v_{N-1-n} = x_{2n+1}
+      // z_n = v^a_n + i v^b_n for n = u + 64 q; the lanes with u & 4 read
+      // slot q + 4 first, so that each quarter warp meets even and odd rows
+      const bool sw = (u >> 2) & 1;
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int n = lane + 32 * q, src = n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1;
-        const double2 v = *swz_pair(b, src, warp);
-        re[q] = v.x;
-        im[q] = v.y;
+      for (int q = 0; q < 4; q++) {
+        const int nA = u + 64 * (sw ? q + 4 : q), nB = u + 64 * (sw ? q : q + 4);
+        const double2 vA = *swz_pair(b, mk_row(nA), pair), vB = *swz_pair(b, mk_row(nB), pair);
+        re[q] = sw ? vB.x : vA.x;
+        im[q] = sw ? vB.y : vA.y;
+        re[q + 4] = sw ? vA.x : vB.x;
+        im[q + 4] = sw ? vA.y : vB.y;
       }
-      __syncwarp();
-      warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+      pair_sync(pair);
+      pair_fft512(re, im, b, pair, u, tw1, tw2);
       refill(s);
-      __syncwarp();
-      const SwzScratch<1> out{b, warp};
+      pair_sync(pair);
 #pragma unroll
-      for (int q = 0; q < 16; q++) out.st((lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4)), re[q], im[q]);
-      __syncwarp();
+      for (int d = 0; d < 8; d++) {
+        const int rg = brev_c(d, 3);
+        *swz_pair(b, pfft_p(k2 + 8 * cc + 64 * d), pair) = make_double2(re[rg], im[rg]);
+      }
+      pair_sync(pair);
       // y_k = 2 Re(e^{-i pi k/(2N)} V_k) / (2N)
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int k = lane + 32 * q, km = (N - k) & (N - 1);
-        double zr, zi, mr, mi;
-        out.ld(k, zr, zi);
-        out.ld(km, mr, mi);
+      for (int q = 0; q < 8; q++) {
+        const int k = u + 64 * q, km = (N - k) & (N - 1);
+        const double2 z = *swz_pair(b, pfft_p(k), pair), mz = *swz_pair(b, pfft_p(km), pair);
+        const double zr = z.x, zi = z.y, mr = mz.x, mi = mz.y;
         const double var_ = 0.5 * (zr + mr), vai = 0.5 * (zi - mi);  // V^a = (Z_k + conj Z_{N-k}) / 2
         const double vbr = 0.5 * (zi + mi), vbi = -0.5 * (zr - mr);  // V^b = -i (Z_k - conj Z_{N-k}) / 2
-        const double2 cs = shl[q * 32 + lane];
-        const double c = cs.x, sn = cs.y;
-        re[q] = 2.0 * (var_ * c + vai * sn) / (2.0 * N * 1);
-        im[q] = 2.0 * (vbr * c + vbi * sn) / (2.0 * N * 1);
+        const double2 cs = shl[k];
+        re[q] = 2.0 * (var_ * cs.x + vai * cs.y) / (2.0 * N * 1);
+        im[q] = 2.0 * (vbr * cs.x + vbi * cs.y) / (2.0 * N * 1);
       }
-      __syncwarp();
+      pair_sync(pair);
 #pragma unroll
-      for (int q = 0; q < 16; q++) *swz_pair(b, lane + 32 * q, warp) = make_double2(re[q], im[q]);
+      for (int q = 0; q < 8; q++) *swz_pair(b, u + 64 * q, pair) = make_double2(re[q], im[q]);
     } else {
       // W_k = V^a_k + i V^b_k, V_k = e^{i pi k/(2N)} (X_k - i X_{N-k}) / 2
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int k = lane + 32 * q;
-        const double2 cs = shl[q * 32 + lane];
+      for (int q = 0; q < 8; q++) {
+        const int k = u + 64 * q;
+        const double2 cs = shl[k];
         const double c = cs.x, sn = cs.y;
-        const double2 x = *swz_pair(b, k, warp), y = *swz_pair(b, (N - k) & (N - 1), warp);
+        const double2 x = *swz_pair(b, k, pair), y = *swz_pair(b, (N - k) & (N - 1), pair);
         const double xa = x.x / 2.0, xb = x.y / 2.0;
         const double ya = k == 0 ? 0.0 : -y.x / 2.0, yb = k == 0 ? 0.0 : -y.y / 2.0;
         const double var_ = xa * c - ya * sn, vai = xa * sn + ya * c;
@@ -1010,16 +1093,20 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
         re[q] = var_ - vbi;    // Re W
         im[q] = -(vai + vbr);  // -Im W (inverse as conj(DFT(conj W)))
       }
-      __syncwarp();
-      // slot q holds conj(w_m), m = lane/2 + 16 (16 (lane & 1) + brev4(q))
-      warp_fft512(re, im, tw_lane, SwzScratch<0>{b, warp}, lane);
+      pair_sync(pair);
+      pair_fft512(re, im, b, pair, u, tw1, tw2);
       refill(s);
-      __syncwarp();
+      pair_sync(pair);
+      // slot brev3(d) holds conj(w_m), m = k2 + 8 cc + 64 d; the lanes with
+      // odd cc write slot d ^ 4 first, so that each quarter warp meets even
+      // and odd rows
+      const bool sw = cc & 1;
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int m = (lane >> 1) + 16 * (16 * (lane & 1) + brev_c(q, 4));
-        const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
-        *swz_pair(b, o, warp) = make_double2(2.0 * re[q], -2.0 * im[q]);
+      for (int j = 0; j < 8; j++) {
+        const int ra = brev_c(j, 3), rb = brev_c(j ^ 4, 3);
+        const double wr = sw ? re[rb] : re[ra], wi = sw ? im[rb] : im[ra];
+        const int m = k2 + 8 * cc + 64 * (sw ? j ^ 4 : j);
+        *swz_pair(b, mk_row(m), pair) = make_double2(2.0 * wr, -2.0 * wi);
       }
     }
     fence_proxy_async();  // the tile's shared-memory writes, before the TMA store reads them
@@ -1055,13 +1142,14 @@ __global__ void __launch_bounds__(256, 1) k_dct_tma(const __grid_constant__ CUte
 // cluster barrier warp w of CTA c gathers slots 16c + 2w, 16c + 2w + 1 of all
 // 512 planes from the 8 CTAs' shared memory (distributed shared memory) in
 // Makhoul's order, a second barrier frees the tiles, and the 512-point z
-// transform runs as in k_dct_tma, its result stored by TMA into the spectral
-// array.  Inverse (k_pois_bwd_cl): the z transform of the CTA's 16 slots
-// first (TMA load, k_dct_tma's inverse), a cluster barrier, then the theta
-// pairs of its 64 planes read their packed entries from the 8 CTAs, a second
-// barrier, and the inverse theta transforms write dph.  The arithmetic is
-// that of k_fft_fwd_s / k_dct_tma / k_fft_bwd_s, so the results are the
-// same bits; the spectral array is written once and read once instead of
+// transform runs as in k_dct_w (the 16 x 32 warp FFT), its result stored by
+// TMA into the spectral array.  Inverse (k_pois_bwd_cl): the z transform of
+// the CTA's 16 slots first (TMA load, k_dct_w's inverse), a cluster barrier,
+// then the theta pairs of its 64 planes read their packed entries from the 8
+// CTAs, a second barrier, and the inverse theta transforms write dph.  The
+// theta arithmetic is that of k_fft_fwd_s / k_fft_bwd_s and the z arithmetic
+// that of k_dct_w, so the results agree with the separate kernels to
+// round-off; the spectral array is written once and read once instead of
 // twice each way.  Every CTA takes every cluster barrier.
 // ---------------------------------------------------------------------------
 #ifndef VR_SLAB_MINB
@@ -1238,7 +1326,7 @@ __global__ void __cluster_dims__(kClCtas, 1, 1) __launch_bounds__(256, VR_SLAB_M
   // wait below ends before the CTA's shared memory can be reused
   const bool ok = mbar_wait(&full, 0u);
   if (!ok && tid == 0) atomicOr(status, 1u);
-  // ---- z: inverse of this CTA's 16 slots (k_dct_tma<-1>)
+  // ---- z: inverse of this CTA's 16 slots (k_dct_w's inverse)
   {
     auto tw_lane = [&](int k1, double &cc, double &sn) {
       const double2 v = twl[(k1 - 1) * 32 + lane];
@@ -1658,12 +1746,13 @@ static cudaError_t run_dct_tma(vr_ctx *c, int dir) {
   CUtensorMap tm;
   if (!encode_tmap_f64_3d(&tm, c->spec, g.nth, g.nr, g.nz, kDctTileCols, 1, 256, true)) return cudaErrorNotSupported;
   const int nti = g.nth / kDctTileCols, ntiles = nti * g.nr;
-  const size_t sm = (size_t)kDctBufs * kDctTileBytes + (15 + 16) * 32 * 16 + 1024;
+  const size_t sm = (size_t)kDctBufs * kDctTileBytes + (7 * 64 + 7 * 8 + kDctN) * 16 + 1024;
   auto kern = dir > 0 ? k_dct_tma<1> : k_dct_tma<-1>;
+  constexpr int threads = 512;
   cudaError_t e = allow_dyn_smem(kern, sm);
   if (e) return e;
   LaunchScope ls(c, PK_DCT);
-  kern<<<std::min(ntiles, c->nsm), 256, sm, c->stream>>>(tm, nti, ntiles, c->tw_z, c->d_status);
+  kern<<<std::min(ntiles, c->nsm), threads, sm, c->stream>>>(tm, nti, ntiles, c->tw_z, c->d_status);
   return cudaGetLastError();
 }
 
